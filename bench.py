@@ -1,0 +1,470 @@
+"""Benchmark: 2-D TM forward + exact adjoint, FP32, config-2 workload.
+
+Workload (one bench step = one full gradient evaluation):
+  model 512 x 1024 (padded 553 x 1065 with CPML 20, stencil 2), dx = 0.02 m,
+  dt = 0.9 x CFL, nt = 4000, 64 shots (sources on row 10 every 16 cells,
+  256 receivers on row 10 every 4 cells, Ricker 400 MHz), eps_r = 6 layers
+  U[3, 25] + smoothed N(0, 0.5) noise, sigma U[0, 0.01] per layer, seed 2.
+  Loss 0.5 * sum(r^2); gradients w.r.t. eps and sigma.  Snapshots of Ey and
+  curl H are stored on the device (FP32 by default, --storage bf16); the 64
+  shots run in shot batches that fit HBM.
+Metric: cell-updates per second (one padded cell of one shot advanced one
+internal step, forward or adjoint): 2 * 64 * 553 * 1065 * 4000 = 3.02e11 per
+step.
+
+Arms:
+  default          the B200 library through the public tide_b200 API.
+  --impl reference the reference's own CPU backend (compiled from its sources
+                   with OpenMP) on the host cores, on a bounded sample of the
+                   same workload.
+
+Run with torchrun for N > 1 GPUs (weak scaling: every rank evaluates the full
+64-shot gradient; ranks then all-reduce the model gradients over NCCL).
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "tide-gpr_b200"))
+
+import tide_b200 as tide  # noqa: E402
+from tide_b200 import _native as nat  # noqa: E402
+
+METRIC = "2D TM cell-updates/s fwd+adj (% of HBM roofline); served p50/p99 latency"
+UNIT = "cell-updates/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+# ---------------------------------------------------------------- workload
+
+
+def config2(seed: int = 2, shots: int = 64, nt: int = 4000, device="cpu"):
+    """Seeded config-2 model and acquisition (synthetic; no dataset)."""
+    from scipy.ndimage import gaussian_filter
+
+    ny, nx, dx = 512, 1024, 0.02
+    rng = np.random.default_rng(seed)
+    layer_eps = rng.uniform(3.0, 25.0, size=6)
+    layer_sig = rng.uniform(0.0, 0.01, size=6)
+    rows = np.minimum(np.arange(ny) * 6 // ny, 5)
+    eps = layer_eps[rows][:, None] * np.ones((1, nx))
+    sig = layer_sig[rows][:, None] * np.ones((1, nx))
+    eps = eps + gaussian_filter(rng.normal(0.0, 0.5, size=(ny, nx)), sigma=8)
+    eps = np.maximum(eps, 1.0)
+    vmax = tide.C0 / math.sqrt(float(eps.min()))
+    max_dt = 1.0 / math.sqrt(2.0 / dx**2) / vmax
+    dt = 0.9 * max_dt
+    amp = tide.ricker(400e6, nt, dt, dtype=torch.float64).view(1, 1, nt).repeat(shots, 1, 1)
+    src = torch.tensor([[[10, 8 + 16 * i]] for i in range(shots)])
+    rec = torch.tensor([[[10, 2 + 4 * j] for j in range(256)]] * shots)
+    f32 = torch.float32
+    return dict(
+        eps=torch.from_numpy(eps).to(f32).to(device), sig=torch.from_numpy(sig).to(f32).to(device),
+        mu=torch.ones((ny, nx), dtype=f32, device=device), amp=amp.to(f32).to(device),
+        src=src.to(device), rec=rec.to(device), dx=dx, dt=dt, nt=nt, shots=shots, ny=ny, nx=nx,
+        pml=20,
+    )
+
+
+PADDED = (553, 1065)
+
+
+def cell_updates(shots: int, nt: int) -> float:
+    return 2.0 * shots * PADDED[0] * PADDED[1] * nt
+
+
+# ---------------------------------------------------------------- helpers
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
+            )
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path).read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def lib():
+    L = nat.load()
+    L.tide_b200_profile_enable.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.tide_b200_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    L.tide_b200_profile_read.restype = ctypes.c_int
+    L.tide_b200_profile_kind_name.restype = ctypes.c_char_p
+    L.tide_b200_launch_count.restype = ctypes.c_int64
+    return L
+
+
+def read_profile(L) -> dict:
+    ms = (ctypes.c_double * 8)()
+    n = (ctypes.c_int64 * 8)()
+    k = L.tide_b200_profile_read(ms, n, 8)
+    return {L.tide_b200_profile_kind_name(i).decode(): (ms[i], n[i]) for i in range(k)}
+
+
+# Algorithmic bytes per cell (one shot, one step) of each stencil kernel,
+# single sweep: fields each read/written once, model coefficients once per
+# launch (shared by the S shots of a launch), CPML memories only in their
+# strips, snapshot bytes where the kernel stores or reads them.
+def kernel_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho_x: float, rho_y: float) -> float:
+    f = 4.0
+    if kind == "fwd_h":  # read Ey; RMW Hx, Hz; cq; RMW m_ey_x, m_ey_z in strips
+        return 5 * f + f / S + 2 * f * (rho_x + rho_y)
+    if kind == "fwd_e":  # read Hx, Hz; RMW Ey; ca, cb; RMW m_hx_z, m_hz_x; store Ey, curl
+        return 5 * f + 2 * f / S + 2 * f * (rho_x + rho_y) + 2 * snap_bytes
+    if kind == "adj_e":  # read lEy; RMW lHx, lHz; cb; memories; read 2 snapshots; model grads
+        return 5 * f + f / S + 2 * f * (rho_x + rho_y) + 2 * snap_bytes + 4 * f / S
+    if kind == "adj_h":  # read lHx, lHz; RMW lEy; ca, cq; memories
+        return 5 * f + 2 * f / S + 2 * f * (rho_x + rho_y)
+    raise KeyError(kind)
+
+
+# ---------------------------------------------------------------- B200 arm
+
+
+def shot_batches(shots: int, snap_bytes: int, device) -> int:
+    per_shot = 2 * snap_bytes * PADDED[0] * PADDED[1] * 4000
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = int(0.88 * free) - (4 << 30)
+    b = max(1, min(shots, budget // per_shot))
+    while shots % b:
+        b -= 1
+    return b
+
+
+def run_b200(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    L = lib()
+    snap_bytes = 2 if args.storage == "bf16" else 4
+    cfg = config2(shots=args.shots, nt=args.nt)
+    S_total = args.shots
+    batch = args.batch or shot_batches(S_total, snap_bytes, dev)
+    compression = args.storage == "bf16"
+
+    # host (pinned) copies for the end-to-end leg, device copies for `value`
+    host = {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in cfg.items()}
+    dev_in = {k: (v.to(dev) if torch.is_tensor(v) else v) for k, v in cfg.items()}
+
+    def step(inp, copy_in: bool):
+        if copy_in:
+            d = {k: (v.to(dev, non_blocking=True) if torch.is_tensor(v) else v) for k, v in inp.items()}
+        else:
+            d = inp
+        eps = d["eps"].detach().requires_grad_(True)
+        sig = d["sig"].detach().requires_grad_(True)
+        loss_total = torch.zeros((), device=dev)
+        for b0 in range(0, S_total, batch):
+            sl = slice(b0, b0 + batch)
+            out = tide.maxwelltm(
+                eps, sig, d["mu"], d["dx"], d["dt"], d["amp"][sl], d["src"][sl], d["rec"][sl],
+                stencil=2, pml_width=d["pml"], storage_mode="device",
+                storage_compression=compression,
+            )
+            r = out[-1]
+            loss = 0.5 * (r * r).sum()
+            loss.backward()
+            loss_total = loss_total + loss.detach()
+        g = torch.stack([eps.grad, sig.grad])
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.all_reduce(g)
+        return g, loss_total
+
+    def timed(n_steps, copy_in):
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        st = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        h2d = d2h = 0
+        for _ in range(n_steps):
+            g, loss = step(host if copy_in else dev_in, copy_in)
+            if copy_in:
+                h2d = sum(v.numel() * v.element_size() for v in host.values() if torch.is_tensor(v))
+                g_h = g.to("cpu", non_blocking=False)
+                l_h = loss.to("cpu")
+                d2h = g_h.numel() * g_h.element_size() + l_h.numel() * l_h.element_size()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, h2d, d2h
+
+    for _ in range(args.warmup):
+        step(dev_in, False)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(dev.index or 0)
+    clocks.start()
+    L.tide_b200_profile_enable(1, 8)
+    read_profile(L)
+    launches0 = L.tide_b200_launch_count()
+    ms, _, _ = timed(args.steps, copy_in=False)
+    launches = L.tide_b200_launch_count() - launches0
+    L.tide_b200_profile_enable(0, 8)
+    prof = read_profile(L)
+    clk = clocks.stop()
+    e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)
+
+    units = cell_updates(S_total, args.nt) * world
+    value = units * args.steps / (ms / 1e3)
+    e2e_value = units * max(1, args.e2e_steps) / (e2e_ms / 1e3)
+
+    # roofline of the dominant kernel
+    peak, peak_kind = hbm_peak()
+    rho_x, rho_y = 41 / PADDED[1], 41 / PADDED[0]
+    shares = {k: v[0] for k, v in prof.items() if v[1] > 0}
+    dom = max(shares, key=shares.get) if shares else None
+    roof = None
+    if dom:
+        avg_ms = prof[dom][0] / prof[dom][1]
+        bpc = kernel_bytes_per_cell(dom, batch, snap_bytes, rho_x, rho_y)
+        bytes_launch = bpc * batch * PADDED[0] * PADDED[1]
+        achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+        roof = {
+            "kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": None, "algorithmic_bytes_per_launch": bytes_launch,
+            "avg_launch_ms": avg_ms,
+            "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
+        }
+
+    if rank == 0:
+        cpu = cpu_baseline(args) if not args.no_cpu_baseline else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded config-2 model and acquisition)",
+            "config": {
+                "workload": "config2: 2D TM fwd+adj, 512x1024 (553x1065 padded), CPML 20, "
+                            f"stencil 2, nt={args.nt}, {S_total} shots, snapshots {args.storage} on device",
+                "shots": S_total, "shot_batch": batch, "nt": args.nt,
+                "cell_updates_per_step": units, "l2": "per-step working set (snapshot history) >> L2",
+                "parallelism": f"shots-weak-dp{world}",
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- CPU arm
+
+
+def _ref_lib():
+    p = ROOT / "oracle" / "_ref" / "libtide_ref_cpu.so"
+    if p.exists():
+        return ctypes.CDLL(str(p)), "reference"
+    return None, "port"
+
+
+def cpu_sample(n_shots: int, nt: int, threads: int):
+    """Time fwd+adj of the reference CPU backend on a config-2 sample."""
+    from tide_b200.tm2d import prepare_tm2d
+
+    lib, kind = _ref_lib()
+    cfg = config2(shots=n_shots, nt=nt)
+    pb = prepare_tm2d(cfg["eps"], cfg["sig"], cfg["mu"], cfg["dx"], cfg["dt"], cfg["amp"],
+                      cfg["src"], cfg["rec"], stencil=2, pml_width=20)
+    prof = [pb.profiles[n] for n in ("ay", "by", "ayh", "byh", "ax", "bx", "axh", "bxh",
+                                      "ky", "kyh", "kx", "kxh")]
+    P = lambda t: 0 if t is None or t.numel() == 0 else t.data_ptr()  # noqa: E731
+    S, ny, nx = pb.n_shots, pb.ny, pb.nx
+    r = torch.zeros((nt, S, pb.n_rec))
+    ey_st = torch.empty((nt, S, ny, nx))
+    cu_st = torch.empty((nt, S, ny, nx))
+    if lib is None:
+        raise RuntimeError("reference CPU backend not built (oracle/_ref); run build()")
+    fwd = lib.maxwell_tm_2_float_forward_with_storage_cpu
+    fwd.argtypes = nat.argtypes("maxwell_tm_forward_with_storage", "float")
+    bwd = lib.maxwell_tm_2_float_backward_cpu
+    bwd.argtypes = nat.argtypes("maxwell_tm_backward", "float")
+    ey, hx, hz, mex, mez, mhx, mhz = pb.fields
+    t0 = time.perf_counter()
+    fwd(P(pb.ca), P(pb.cb), P(pb.cq), P(pb.f), P(ey), P(hx), P(hz), P(mex), P(mez), P(mhx),
+        P(mhz), P(r), P(ey_st), 0, 0, P(cu_st), 0, 0, *[P(t) for t in prof], P(pb.sources_i),
+        P(pb.receivers_i), pb.rdy, pb.rdx, pb.dt, nt, S, ny, nx, pb.n_src, pb.n_rec, 1, 0, 0,
+        ny * nx * 4, True, True, False, False, False, 0, pb.pml_y0, pb.pml_x0, pb.pml_y1,
+        pb.pml_x1, threads, 0, 0, 0)
+    lam = [torch.zeros((S, ny, nx)) for _ in range(7)]
+    scratch = torch.zeros((4, S, ny, nx))
+    gca, gcb = torch.zeros((ny, nx)), torch.zeros((ny, nx))
+    sca, scb = torch.zeros((S, ny, nx)), torch.zeros((S, ny, nx))
+    gf = torch.zeros((nt, S, pb.n_src))
+    bwd(P(pb.ca), P(pb.cb), P(pb.cq), P(r), *[P(t) for t in lam], P(scratch), P(ey_st), 0, 0,
+        P(cu_st), 0, 0, P(gf), P(gca), P(gcb), P(sca), P(scb), *[P(t) for t in prof],
+        P(pb.sources_i), P(pb.receivers_i), pb.rdy, pb.rdx, pb.dt, nt, S, ny, nx, pb.n_src,
+        pb.n_rec, 1, 0, 0, ny * nx * 4, True, True, False, False, False, nt, pb.pml_y0, pb.pml_x0,
+        pb.pml_y1, pb.pml_x1, threads, 0, 0, 0)
+    sec = time.perf_counter() - t0
+    return cell_updates(n_shots, nt) / sec, sec, kind
+
+
+def cpu_baseline(args) -> dict:
+    threads = os.cpu_count() or 1
+    try:
+        v, sec, kind = cpu_sample(args.cpu_shots, args.cpu_nt, threads)
+    except Exception as exc:  # noqa: BLE001
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"unavailable: {exc}"}
+    return {
+        "value": v, "unit": UNIT, "cores": threads, "kind": kind,
+        "sample": f"reference CPU backend (OpenMP build, {threads} threads), config-2 geometry, "
+                  f"{args.cpu_shots} shots x nt={args.cpu_nt} fwd+adj in {sec:.2f} s",
+    }
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(args.cpu_shots, max(8, args.cpu_nt // 8), threads)
+    vals, secs = [], []
+    kind = "reference"
+    for _ in range(args.steps):
+        v, sec, kind = cpu_sample(args.cpu_shots, args.cpu_nt, threads)
+        vals.append(v)
+        secs.append(sec)
+    value = cell_updates(args.cpu_shots, args.cpu_nt) * len(vals) / sum(secs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded config-2 model and acquisition)",
+        "config": {
+            "workload": "config2 sample: 2D TM fwd+adj on the 553x1065 padded grid, "
+                        f"{args.cpu_shots} shots x nt={args.cpu_nt} per step",
+            "shots": args.cpu_shots, "nt": args.cpu_nt,
+        },
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{args.cpu_shots} shots x nt={args.cpu_nt} per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--nt", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "bf16"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-shots", type=int, default=4)
+    ap.add_argument("--cpu-nt", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+/*
+ * tide_b200.h — C ABI of libtide_b200.so, the B200 (sm_100a) implementation
+ * of TIDE's native TM2D time-stepping path.
+ *
+ * The exported symbols carry the reference backend's names and argument
+ * lists, so the reference's ctypes loader can bind them unchanged:
+ *   symbol naming   src/tide/backend_utils.py:771-787
+ *                   ("{propagator}_{accuracy}_{dtype}_{pass}_{device}")
+ *   argument specs  src/tide/backend_utils.py:227-308 (TM forward,
+ *                   forward_with_storage, backward)
+ * Every pointer is a raw device (or pinned host, where stated) address; sizes
+ * are int64; no torch types cross this boundary.
+ *
+ * Differences from the reference behaviour (all deliberate):
+ *   - No entry point ever exits or aborts the process.  A failed argument
+ *     check or CUDA call records a status readable through
+ *     tide_b200_last_error() and the call returns early.
+ *   - Geometry travels as kernel arguments, never as process-global
+ *     __constant__ state, so concurrent calls with different shapes on
+ *     different streams are safe.
+ *   - backward clears the per-shot accumulators on entry and writes batched
+ *     model gradients straight into grad_ca/grad_cb, as the reference CPU
+ *     backend does (maxwell_tm_inst.cpp:2050-2206).
+ */
+#ifndef TIDE_B200_H
+#define TIDE_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Argument list of maxwell_tm_*_forward_cuda.  Replaces
+ * maxwell_tm_{S}_{dtype}_forward_cuda, src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1281-1368
+ * (argtypes src/tide/backend_utils.py:256-269). */
+#define TIDE_TM_FORWARD_ARGS(T)                                                \
+  T const *ca, T const *cb, T const *cq, T const *f, T *ey, T *hx, T *hz,      \
+      T *m_ey_x, T *m_ey_z, T *m_hx_z, T *m_hz_x, T const *debye_a,            \
+      T const *debye_b, T const *debye_cp, T *polarization, T *ey_prev, T *r,  \
+      int64_t n_poles, T const *ay, T const *by, T const *ayh, T const *byh,  \
+      T const *ax, T const *bx, T const *axh, T const *bxh, T const *ky,       \
+      T const *kyh, T const *kx, T const *kxh, int64_t const *sources_i,       \
+      int64_t const *receivers_i, T rdy, T rdx, T dt, int64_t nt,              \
+      int64_t n_shots, int64_t ny, int64_t nx, int64_t n_sources_per_shot,     \
+      int64_t n_receivers_per_shot, int64_t step_ratio, bool has_dispersion,   \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream
+
+/* Argument list of maxwell_tm_*_forward_with_storage_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1371-1609
+ * (argtypes src/tide/backend_utils.py:271-287).  step_ratio is the gradient
+ * sampling interval k: Ey^t and curl H^t are stored when t % k == 0.
+ * storage_mode: 0 device, 1 cpu (pinned host history, 3-slot device ring),
+ * 2 disk (rejected: not built), 3 none.  storage_format: 0 full, 1 bf16. */
+#define TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)                                   \
+  T const *ca, T const *cb, T const *cq, T const *f, T *ey, T *hx, T *hz,      \
+      T *m_ey_x, T *m_ey_z, T *m_hx_z, T *m_hz_x, T *r, void *ey_store_1,      \
+      void *ey_store_3, char const *const *ey_filenames, void *curl_store_1,   \
+      void *curl_store_3, char const *const *curl_filenames, T const *ay,      \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *ky, T const *kyh, T const *kx,      \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream,                 \
+      void *storage_stream
+
+/* Argument list of maxwell_tm_*_backward_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:2739-2770 (which delegates to
+ * background_vjp_reuse, :2405-2734); argtypes src/tide/backend_utils.py:289-308.
+ * Runs t = start_t-1 down to start_t-nt. */
+#define TIDE_TM_BACKWARD_ARGS(T)                                               \
+  T const *ca, T const *cb, T const *cq, T const *grad_r, T *lambda_ey,        \
+      T *lambda_hx, T *lambda_hz, T *m_lambda_ey_x, T *m_lambda_ey_z,          \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, T *adjoint_memory_scratch,           \
+      void *ey_store_1, void *ey_store_3, char const *const *ey_filenames,     \
+      void *curl_store_1, void *curl_store_3,                                  \
+      char const *const *curl_filenames, T *grad_f, T *grad_ca, T *grad_cb,    \
+      T *grad_ca_shot, T *grad_cb_shot, T const *ay, T const *by,              \
+      T const *ayh, T const *byh, T const *ax, T const *bx, T const *axh,      \
+      T const *bxh, T const *ky, T const *kyh, T const *kx, T const *kxh,      \
+      int64_t const *sources_i, int64_t const *receivers_i, T rdy, T rdx,      \
+      T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx,               \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream,                 \
+      void *storage_stream
+
+#define TIDE_TM_DECLARE(S, T)                                                  \
+  void maxwell_tm_##S##_##T##_forward_cuda(TIDE_TM_FORWARD_ARGS(T));           \
+  void maxwell_tm_##S##_##T##_forward_with_storage_cuda(                       \
+      TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T));                                   \
+  void maxwell_tm_##S##_##T##_backward_cuda(TIDE_TM_BACKWARD_ARGS(T));
+
+/* Stencil orders 2/4/6/8 in float and double, as the reference exports
+ * (src/tide/csrc/tm2d/maxwell_tm_cuda_instantiations.inc). */
+TIDE_TM_DECLARE(2, float)
+TIDE_TM_DECLARE(4, float)
+TIDE_TM_DECLARE(6, float)
+TIDE_TM_DECLARE(8, float)
+TIDE_TM_DECLARE(2, double)
+TIDE_TM_DECLARE(4, double)
+TIDE_TM_DECLARE(6, double)
+TIDE_TM_DECLARE(8, double)
+
+/* Comma-separated CUDA architectures the library was built for ("100a").
+ * Replaces tide_cuda_arches, src/tide/csrc/storage/storage_utils.cu:213. */
+const char *tide_cuda_arches(void);
+
+/* Status of the most recent failed call in this process (0 = none) and its
+ * message.  New: the reference exits the process instead
+ * (src/tide/csrc/common/common_gpu.h:12-31). */
+int tide_b200_last_status(void);
+const char *tide_b200_last_error(void);
+void tide_b200_clear_error(void);
+
+/* Synchronises `device` and returns the device-side error word that kernels
+ * set instead of faulting (e.g. a source index outside its shot), then clears
+ * it.  0 = clean.  New; the reference has no device-side checks. */
+int tide_b200_device_status(int64_t device);
+
+/* Kernel timing for benchmarks (new; no reference counterpart).  When
+ * enabled, every `sample_every`-th time step of each call brackets its stencil
+ * kernels with CUDA events on the launching stream; durations accumulate per
+ * kernel kind until read.  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h. */
+void tide_b200_profile_enable(int on, int sample_every);
+int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds);
+const char *tide_b200_profile_kind_name(int kind);
+
+/* Total kernels this library has launched in this process (monotonic). */
+int64_t tide_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TIDE_B200_H */

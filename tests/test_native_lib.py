@@ -1,0 +1,58 @@
+"""The C-ABI boundary without a GPU: the library builds, loads, exports every
+symbol include/tide_b200.h declares, and its argtypes equal the reference
+loader's (src/tide/backend_utils.py:227-308, captured in golden/abi_specs.json)."""
+
+from __future__ import annotations
+
+import json
+import re
+import subprocess
+
+import pytest
+import torch
+
+from conftest import GOLDEN, REPO
+from tide_b200 import _native as nat
+
+
+def header_symbols() -> set[str]:
+    out = subprocess.run(
+        ["gcc", "-E", "-P", "-x", "c", str(REPO / "include" / "tide_b200.h")],
+        capture_output=True, text=True, check=True,
+    ).stdout
+    return set(re.findall(r"\b((?:maxwell_tm|tide)_\w+)\s*\(", out))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = nat.load()
+    declared = header_symbols()
+    assert set(nat.exported_symbols()) <= declared
+    assert len(declared) >= 29
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_library_metadata_calls_without_gpu():
+    lib = nat.load()
+    assert lib.tide_cuda_arches() == b"100a"
+    lib.tide_b200_clear_error()
+    assert lib.tide_b200_last_status() == 0
+
+
+@pytest.mark.parametrize("pass_name", ["forward", "forward_with_storage", "backward"])
+@pytest.mark.parametrize("dtype", ["float", "double"])
+def test_argtypes_match_reference_loader(pass_name, dtype):
+    specs = json.loads((GOLDEN / "abi_specs.json").read_text())
+    ref = specs[f"maxwell_tm_{pass_name}_{dtype}"]
+    mine = [a.__name__ for a in nat.argtypes(f"maxwell_tm_{pass_name}", dtype)]
+    assert mine == ref
+
+
+def test_symbol_naming_matches_reference():
+    assert nat.symbol_name("maxwell_tm", "backward", 4, "double") == "maxwell_tm_4_double_backward_cuda"
+
+
+def test_cpu_tensors_fail_loudly():
+    """No silent CPU fallback: the product path refuses CPU tensors."""
+    with pytest.raises(nat.NativeError):
+        nat.get_backend_function("maxwell_tm", "forward", 2, torch.float32, torch.device("cpu"))

@@ -1,0 +1,175 @@
+// Process-wide status record and the small metadata entry points.
+#include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <vector>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/tide_b200.h"
+#include "tb_common.cuh"
+
+namespace tb {
+
+namespace {
+std::mutex g_mu;
+std::atomic<int> g_status{0};
+std::string g_message;
+}  // namespace
+
+void set_error(int status, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_status.store(status);
+  g_message = buf;
+}
+
+bool cuda_failed(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return false;
+  set_error(kCudaError, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  return true;
+}
+
+namespace {
+std::atomic<int64_t> g_launches{0};
+std::atomic<int> g_prof_on{0};
+std::atomic<int> g_prof_every{8};
+std::mutex g_prof_mu;
+double g_prof_ms[kKindCount] = {};
+int64_t g_prof_n[kKindCount] = {};
+// Event pool shared by all scopes (events are reused across calls).
+std::mutex g_pool_mu;
+std::vector<cudaEvent_t> g_pool;
+
+cudaEvent_t take_event() {
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool.empty()) {
+      cudaEvent_t e = g_pool.back();
+      g_pool.pop_back();
+      return e;
+    }
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+void give_event(cudaEvent_t e) {
+  if (!e) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  g_pool.push_back(e);
+}
+}  // namespace
+
+void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+ProfileScope::ProfileScope(cudaStream_t st)
+    : st_(st), on_(g_prof_on.load() != 0), every_(std::max(1, g_prof_every.load())) {}
+
+bool ProfileScope::sample(int64_t step) const { return on_ && (step % every_) == 0; }
+
+void ProfileScope::begin(int kind) {
+  if (!on_) return;
+  if (n_ == cap_) {
+    int nc = cap_ ? 2 * cap_ : 256;
+    Pair *np = static_cast<Pair *>(realloc(pairs_, sizeof(Pair) * nc));
+    if (!np) return;
+    pairs_ = np;
+    cap_ = nc;
+  }
+  Pair &p = pairs_[n_];
+  p.a = take_event();
+  p.b = take_event();
+  p.kind = kind;
+  if (!p.a || !p.b) {
+    give_event(p.a);
+    give_event(p.b);
+    return;
+  }
+  cudaEventRecord(p.a, st_);
+  open_kind_ = kind;
+}
+
+void ProfileScope::end(int kind) {
+  if (!on_ || open_kind_ != kind) return;
+  cudaEventRecord(pairs_[n_].b, st_);
+  ++n_;
+  open_kind_ = -1;
+}
+
+ProfileScope::~ProfileScope() {
+  if (!on_) return;
+  double ms[kKindCount] = {};
+  int64_t cnt[kKindCount] = {};
+  if (n_ > 0) cudaEventSynchronize(pairs_[n_ - 1].b);
+  for (int i = 0; i < n_; ++i) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, pairs_[i].a, pairs_[i].b) == cudaSuccess) {
+      ms[pairs_[i].kind] += t;
+      cnt[pairs_[i].kind] += 1;
+    }
+    give_event(pairs_[i].a);
+    give_event(pairs_[i].b);
+  }
+  free(pairs_);
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (int k = 0; k < kKindCount; ++k) {
+    g_prof_ms[k] += ms[k];
+    g_prof_n[k] += cnt[k];
+  }
+}
+
+}  // namespace tb
+
+extern "C" {
+
+void tide_b200_profile_enable(int on, int sample_every) {
+  tb::g_prof_every.store(sample_every > 0 ? sample_every : 1);
+  tb::g_prof_on.store(on ? 1 : 0);
+}
+
+int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds) {
+  std::lock_guard<std::mutex> lk(tb::g_prof_mu);
+  int n = max_kinds < tb::kKindCount ? max_kinds : tb::kKindCount;
+  for (int k = 0; k < n; ++k) {
+    if (ms_out) ms_out[k] = tb::g_prof_ms[k];
+    if (launches_out) launches_out[k] = tb::g_prof_n[k];
+  }
+  for (int k = 0; k < tb::kKindCount; ++k) {
+    tb::g_prof_ms[k] = 0.0;
+    tb::g_prof_n[k] = 0;
+  }
+  return tb::kKindCount;
+}
+
+const char *tide_b200_profile_kind_name(int kind) {
+  static const char *names[] = {"fwd_h", "fwd_e", "adj_e", "adj_h"};
+  return (kind >= 0 && kind < tb::kKindCount) ? names[kind] : "";
+}
+
+int64_t tide_b200_launch_count(void) { return tb::g_launches.load(); }
+
+
+const char *tide_cuda_arches(void) { return "100a"; }
+
+int tide_b200_last_status(void) { return tb::g_status.load(); }
+
+const char *tide_b200_last_error(void) {
+  static thread_local std::string copy;
+  std::lock_guard<std::mutex> lk(tb::g_mu);
+  copy = tb::g_message;
+  return copy.c_str();
+}
+
+void tide_b200_clear_error(void) {
+  std::lock_guard<std::mutex> lk(tb::g_mu);
+  tb::g_status.store(0);
+  tb::g_message.clear();
+}
+
+}  // extern "C"

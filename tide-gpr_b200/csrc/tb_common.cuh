@@ -1,0 +1,64 @@
+// Host-side status reporting shared by every entry point of libtide_b200.so.
+//
+// The reference reports CUDA errors with fprintf and then calls std::exit or
+// abort (src/tide/csrc/common/common_gpu.h:12-31).  Here no entry point ever
+// terminates the process: a failure is recorded as (status, message) and the
+// call returns early; callers read it through tide_b200_last_status() /
+// tide_b200_last_error().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+
+namespace tb {
+
+enum Status : int {
+  kOk = 0,
+  kBadArgument = 1,
+  kCudaError = 2,
+  kNotBuilt = 3,
+};
+
+void set_error(int status, const char *fmt, ...);
+
+// Record a CUDA failure; returns true when `e` is an error.
+bool cuda_failed(cudaError_t e, const char *what, const char *file, int line);
+
+// Launch accounting and optional per-kernel event timing (benchmarks).
+enum KernelKind : int { kKFwdH = 0, kKFwdE = 1, kKAdjE = 2, kKAdjH = 3, kKindCount = 4 };
+void count_launches(int64_t n);
+
+// Brackets sampled launches with events on one stream; accumulates into the
+// process-wide profile when the scope closes (after waiting for its events).
+class ProfileScope {
+ public:
+  explicit ProfileScope(cudaStream_t st);
+  ~ProfileScope();
+  bool sample(int64_t step) const;  // is this time step timed?
+  void begin(int kind);
+  void end(int kind);
+
+ private:
+  cudaStream_t st_;
+  bool on_;
+  int every_;
+  int open_kind_ = -1;
+  struct Pair { cudaEvent_t a, b; int kind; };
+  Pair *pairs_ = nullptr;
+  int n_ = 0, cap_ = 0;
+};
+
+}  // namespace tb
+
+#define TB_CUDA(call)                                                         \
+  (tb::cuda_failed((call), #call, __FILE__, __LINE__))
+
+#define TB_REQUIRE(cond, ...)                                                 \
+  do {                                                                        \
+    if (!(cond)) {                                                            \
+      tb::set_error(tb::kBadArgument, __VA_ARGS__);                           \
+      return;                                                                 \
+    }                                                                         \
+  } while (0)

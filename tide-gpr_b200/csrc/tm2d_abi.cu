@@ -1,0 +1,544 @@
+// extern "C" entry points of the TM2D path: forward, forward_with_storage and
+// backward for stencil orders 2/4/6/8 in float and double, under the
+// reference's symbol names (see include/tide_b200.h for the interface each
+// one replaces).
+//
+// Every call works on the caller's stream (compute_stream; 0 = legacy
+// default) and returns as soon as its work is enqueued, except that the cpu
+// storage mode synchronises its side stream before returning, as the
+// reference does (maxwell_tm_cuda_inst.cu:1601-1604).
+#include <algorithm>
+#include <vector>
+
+#include "../../include/tide_b200.h"
+#include "tb_common.cuh"
+#include "tm2d_kernels.cuh"
+
+namespace tb {
+namespace {
+
+constexpr int kRing = 3;  // device ring slots of the cpu storage mode
+                          // (NUM_BUFFERS, maxwell.cu:45-47)
+
+inline cudaStream_t as_stream(void *h) { return reinterpret_cast<cudaStream_t>(h); }
+
+template <typename T, int ST> struct Launch {
+  TMGeom<T> g;
+  dim3 block{kTileX, kTileY, 1};
+  dim3 grid_dom, grid_full;
+  int tiles_x = 0, tiles_y = 0, n_tiles = 0;
+  bool has_domain = false;
+};
+
+template <typename T, int ST>
+bool make_launch(Launch<T, ST> &L, const T *ay, const T *by, const T *ayh, const T *byh,
+                 const T *ax, const T *bx, const T *axh, const T *bxh, const T *ky,
+                 const T *kyh, const T *kx, const T *kxh, T rdy, T rdx, int64_t n_shots,
+                 int64_t ny, int64_t nx, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,
+                 int64_t pml_x1, bool ca_b, bool cb_b, bool cq_b) {
+  constexpr int P = FD<ST>::P;
+  if (n_shots < 1 || n_shots > 65535 || ny < 1 || nx < 1 || ny > (1 << 30) ||
+      nx > (1 << 30)) {
+    set_error(kBadArgument, "TM2D: unsupported shape n_shots=%lld ny=%lld nx=%lld",
+              (long long)n_shots, (long long)ny, (long long)nx);
+    return false;
+  }
+  if (!ay || !by || !ayh || !byh || !ax || !bx || !axh || !bxh || !ky || !kyh || !kx || !kxh) {
+    set_error(kBadArgument, "TM2D: a CPML profile pointer is null");
+    return false;
+  }
+  TMGeom<T> &g = L.g;
+  g.ay = ay; g.by = by; g.ayh = ayh; g.byh = byh;
+  g.ax = ax; g.bx = bx; g.axh = axh; g.bxh = bxh;
+  g.ky = ky; g.kyh = kyh; g.kx = kx; g.kxh = kxh;
+  g.rdy = rdy; g.rdx = rdx;
+  g.ny = (int)ny; g.nx = (int)nx; g.N = ny * nx; g.n_shots = (int)n_shots;
+  g.pml_y0 = (int)pml_y0; g.pml_y1 = (int)pml_y1;
+  g.pml_x0 = (int)pml_x0; g.pml_x1 = (int)pml_x1;
+  g.pml_y1h = pml_y1 > pml_y0 ? (int)pml_y1 - 1 : (int)pml_y0;
+  g.pml_x1h = pml_x1 > pml_x0 ? (int)pml_x1 - 1 : (int)pml_x0;
+  g.ca_b = ca_b; g.cb_b = cb_b; g.cq_b = cq_b;
+  const int64_t dx = nx - 2 * P + 1, dy = ny - 2 * P + 1;
+  L.has_domain = dx > 0 && dy > 0;
+  L.grid_dom = dim3((unsigned)std::max<int64_t>(1, (dx + kTileX - 1) / kTileX),
+                    (unsigned)std::max<int64_t>(1, (dy + kTileY - 1) / kTileY),
+                    (unsigned)n_shots);
+  L.tiles_x = (int)((nx + kTileX - 1) / kTileX);
+  L.tiles_y = (int)((ny + kTileY - 1) / kTileY);
+  L.grid_full = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y, (unsigned)n_shots);
+  L.n_tiles = L.tiles_x * L.tiles_y * (int)n_shots;
+  return true;
+}
+
+// Per-call scratch: CSR point lists for sources and receivers, allocated from
+// the stream-ordered pool and released at the end of the call.
+struct PointScratch {
+  void *mem = nullptr;
+  cudaStream_t st = nullptr;
+  PointCSR src{nullptr, nullptr, nullptr};
+  PointCSR rec{nullptr, nullptr, nullptr};
+  ~PointScratch() {
+    if (mem) cudaFreeAsync(mem, st);
+  }
+};
+
+bool build_list(const int64_t *idx, int n_per_shot, int n_shots, int64_t N, int nx,
+                int tiles_x, int tiles_y, int n_tiles, int *count, int *start, int *cell,
+                int *ent, cudaStream_t st, PointCSR &out) {
+  const int n = n_per_shot * n_shots;
+  if (TB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * n_tiles, st))) return false;
+  const int thr = 256, blk = (n + thr - 1) / thr;
+  k_points_count<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, count);
+  k_points_scan<<<1, 1024, 0, st>>>(count, start, n_tiles);
+  k_points_fill<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, start,
+                                     cell, ent);
+  if (TB_CUDA(cudaGetLastError())) return false;
+  count_launches(3);
+  out = PointCSR{start, cell, ent};
+  return true;
+}
+
+template <typename T, int ST>
+bool build_points(PointScratch &ps, const Launch<T, ST> &L, const int64_t *sources_i,
+                  int64_t n_src, const int64_t *receivers_i, int64_t n_rec, cudaStream_t st) {
+  ps.st = st;
+  const bool want_s = n_src > 0 && sources_i != nullptr;
+  const bool want_r = n_rec > 0 && receivers_i != nullptr;
+  if (!want_s && !want_r) return true;
+  const int64_t S = L.g.n_shots;
+  if ((want_s && n_src * S > (1 << 30)) || (want_r && n_rec * S > (1 << 30))) {
+    set_error(kBadArgument, "TM2D: too many source/receiver entries");
+    return false;
+  }
+  const size_t nt1 = (size_t)L.n_tiles + 1;
+  const size_t ns = want_s ? (size_t)(n_src * S) : 0, nr = want_r ? (size_t)(n_rec * S) : 0;
+  const size_t words = (want_s ? 2 * nt1 + 2 * ns : 0) + (want_r ? 2 * nt1 + 2 * nr : 0);
+  if (TB_CUDA(cudaMallocAsync(&ps.mem, words * sizeof(int), st))) return false;
+  int *w = static_cast<int *>(ps.mem);
+  if (want_s) {
+    int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
+    if (!build_list(sources_i, (int)n_src, (int)S, L.g.N, L.g.nx, L.tiles_x, L.tiles_y,
+                    L.n_tiles, count, start, cell, ent, st, ps.src))
+      return false;
+    w += 2 * nt1 + 2 * ns;
+  }
+  if (want_r) {
+    int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + nr;
+    if (!build_list(receivers_i, (int)n_rec, (int)S, L.g.N, L.g.nx, L.tiles_x, L.tiles_y,
+                    L.n_tiles, count, start, cell, ent, st, ps.rec))
+      return false;
+  }
+  return true;
+}
+
+struct EventRing {
+  cudaEvent_t ev[kRing]{};
+  bool ok = true;
+  EventRing() {
+    for (auto &e : ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) ok = false;
+  }
+  ~EventRing() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+// ---------------------------------------------------------------------------
+template <typename T, int ST>
+void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
+  (void)dt; (void)step_ratio; (void)n_threads;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0, "TM2D forward: nt must be >= 0");
+  TB_REQUIRE(ca && cb && cq && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z && m_hz_x,
+             "TM2D forward: a field or coefficient pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || f, "TM2D forward: sources without amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D forward: receivers without output");
+  DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
+  if (has_dispersion) {
+    TB_REQUIRE(n_poles >= 1 && debye_a && debye_b && debye_cp && polarization,
+               "TM2D forward: dispersion enabled without Debye coefficients");
+    db = DebyeArgs<T>{debye_a, debye_b, debye_cp, polarization, (int)n_poles};
+  }
+  (void)ey_prev;  // the old Ey lives in a register; the buffer is not needed
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = as_stream(compute_stream);
+  PointScratch ps;
+  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
+                    st))
+    return;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  ProfileScope prof(st);
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    const bool smp = prof.sample(t);
+    if (L.has_domain) {
+      if (smp) prof.begin(kKFwdH);
+      k_fwd_h<T, ST><<<L.grid_dom, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      if (smp) prof.end(kKFwdH);
+    }
+    if (smp) prof.begin(kKFwdE);
+    k_fwd_e<T, ST, T><<<L.grid_full, L.block, 0, st>>>(
+        L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)nullptr, (T *)nullptr, db, ps.src, ps.rec,
+        f ? f + t * fs : nullptr, r ? r + t * rs : nullptr);
+    if (smp) prof.end(kKFwdE);
+  }
+  count_launches(nt * (L.has_domain ? 2 : 1));
+  TB_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, int ST>
+void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
+  (void)dt; (void)n_threads; (void)ey_filenames; (void)curl_filenames;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1, "TM2D forward_with_storage: bad nt/step_ratio");
+  TB_REQUIRE(ca && cb && cq && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z && m_hz_x,
+             "TM2D forward_with_storage: a field or coefficient pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || f, "TM2D forward_with_storage: sources without amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D forward_with_storage: receivers without output");
+  TB_REQUIRE(storage_mode != 2,
+             "TM2D forward_with_storage: disk storage mode is not built in this library");
+  TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "TM2D: unknown storage_mode %lld",
+             (long long)storage_mode);
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
+  const bool want_store = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  if (want_store) {
+    TB_REQUIRE(shot_bytes_uncomp == ny * nx * (int64_t)esz,
+               "TM2D: shot_bytes_uncomp=%lld does not match ny*nx*elem=%lld",
+               (long long)shot_bytes_uncomp, (long long)(ny * nx * (int64_t)esz));
+    TB_REQUIRE((!ca_requires_grad || ey_store_1) && (!cb_requires_grad || curl_store_1),
+               "TM2D: snapshot buffers missing");
+    TB_REQUIRE(storage_mode != 1 ||
+                   ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
+               "TM2D: cpu storage mode needs host snapshot buffers");
+  }
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = as_stream(compute_stream);
+  cudaStream_t ss = as_stream(storage_stream);
+  const bool pipeline = want_store && storage_mode == 1 && ss != nullptr && ss != st;
+  PointScratch ps;
+  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
+                    st))
+    return;
+  EventRing store_done, compute_done;
+  if (pipeline) {
+    if (!store_done.ok || !compute_done.ok) {
+      set_error(kCudaError, "TM2D: event creation failed");
+      return;
+    }
+    for (int k = 0; k < kRing; ++k)
+      if (TB_CUDA(cudaEventRecord(store_done.ev[k], ss))) return;
+  }
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
+  ProfileScope prof(st);
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    const bool smp = prof.sample(t);
+    const bool store_step = want_store && (t % step_ratio) == 0;
+    const int64_t q = t / step_ratio;
+    const int slot = (int)(q % kRing);
+    char *e1 = nullptr, *c1 = nullptr;
+    if (store_step) {
+      const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes : (size_t)slot * step_bytes;
+      if (ca_requires_grad) e1 = (char *)ey_store_1 + off1;
+      if (cb_requires_grad) c1 = (char *)curl_store_1 + off1;
+      if (pipeline && TB_CUDA(cudaStreamWaitEvent(st, store_done.ev[slot], 0))) return;
+    }
+    if (L.has_domain) {
+      if (smp) prof.begin(kKFwdH);
+      k_fwd_h<T, ST><<<L.grid_dom, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      if (smp) prof.end(kKFwdH);
+    }
+    const T *ft = f ? f + t * fs : nullptr;
+    T *rt = r ? r + t * rs : nullptr;
+    if (smp) prof.begin(kKFwdE);
+    if (store_step && bf16) {
+      k_fwd_e<T, ST, __nv_bfloat16><<<L.grid_full, L.block, 0, st>>>(
+          L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db,
+          ps.src, ps.rec, ft, rt);
+    } else {
+      k_fwd_e<T, ST, T><<<L.grid_full, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z,
+                                                          m_hz_x, (T *)e1, (T *)c1, db, ps.src,
+                                                          ps.rec, ft, rt);
+    }
+    if (smp) prof.end(kKFwdE);
+    if (store_step && storage_mode == 1) {
+      cudaStream_t cs = st;
+      if (pipeline) {
+        if (TB_CUDA(cudaEventRecord(compute_done.ev[slot], st))) return;
+        if (TB_CUDA(cudaStreamWaitEvent(ss, compute_done.ev[slot], 0))) return;
+        cs = ss;
+      }
+      const size_t off3 = (size_t)q * step_bytes;
+      if (e1 && TB_CUDA(cudaMemcpyAsync((char *)ey_store_3 + off3, e1, step_bytes,
+                                        cudaMemcpyDeviceToHost, cs)))
+        return;
+      if (c1 && TB_CUDA(cudaMemcpyAsync((char *)curl_store_3 + off3, c1, step_bytes,
+                                        cudaMemcpyDeviceToHost, cs)))
+        return;
+      if (pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss))) return;
+    }
+  }
+  count_launches(nt * (L.has_domain ? 2 : 1));
+  if (TB_CUDA(cudaGetLastError())) return;
+  if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, int ST>
+void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
+  (void)dt; (void)n_threads; (void)ey_filenames; (void)curl_filenames;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1 && start_t - nt >= 0,
+             "TM2D backward: bad nt/step_ratio/start_t");
+  TB_REQUIRE(ca && cb && cq && lambda_ey && lambda_hx && lambda_hz && m_lambda_ey_x &&
+                 m_lambda_ey_z && m_lambda_hx_z && m_lambda_hz_x && adjoint_memory_scratch,
+             "TM2D backward: a field or coefficient pointer is null");
+  TB_REQUIRE(n_receivers_per_shot == 0 || grad_r, "TM2D backward: receivers without grad_r");
+  TB_REQUIRE(storage_mode != 2, "TM2D backward: disk storage mode is not built in this library");
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
+  const bool grads = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  if (grads) {
+    TB_REQUIRE(shot_bytes_uncomp == ny * nx * (int64_t)esz,
+               "TM2D backward: shot_bytes_uncomp does not match ny*nx*elem");
+    TB_REQUIRE((!ca_requires_grad || (ey_store_1 && grad_ca)) &&
+                   (!cb_requires_grad || (curl_store_1 && grad_cb)),
+               "TM2D backward: gradient or snapshot buffers missing");
+    TB_REQUIRE((!ca_requires_grad || ca_batched || grad_ca_shot) &&
+                   (!cb_requires_grad || cb_batched || grad_cb_shot),
+               "TM2D backward: per-shot accumulators missing");
+    TB_REQUIRE(storage_mode != 1 ||
+                   ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
+               "TM2D backward: cpu storage mode needs host snapshot buffers");
+  }
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = as_stream(compute_stream);
+  cudaStream_t ss = as_stream(storage_stream);
+  const bool pipeline = grads && storage_mode == 1 && ss != nullptr && ss != st;
+  const size_t SN = (size_t)n_shots * (size_t)L.g.N;
+  T *acc_ca = ca_requires_grad ? (ca_batched ? grad_ca : grad_ca_shot) : nullptr;
+  T *acc_cb = cb_requires_grad ? (cb_batched ? grad_cb : grad_cb_shot) : nullptr;
+  if (grads) {
+    if (acc_ca && !ca_batched && TB_CUDA(cudaMemsetAsync(acc_ca, 0, SN * sizeof(T), st))) return;
+    if (acc_cb && !cb_batched && TB_CUDA(cudaMemsetAsync(acc_cb, 0, SN * sizeof(T), st))) return;
+  }
+  if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, 4 * SN * sizeof(T), st))) return;
+  PointScratch ps;
+  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
+                    st))
+    return;
+
+  // Store indices consumed by this call, latest first.
+  std::vector<int64_t> qs;
+  if (grads)
+    for (int64_t t = start_t - 1; t >= start_t - nt; --t)
+      if (t % step_ratio == 0) qs.push_back(t / step_ratio);
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  EventRing loaded, consumed;
+  if (pipeline && (!loaded.ok || !consumed.ok)) {
+    set_error(kCudaError, "TM2D: event creation failed");
+    return;
+  }
+  if (pipeline)
+    for (int k = 0; k < kRing; ++k)
+      if (TB_CUDA(cudaEventRecord(consumed.ev[k], st))) return;
+  // Issue the H2D copy of store index qs[n] into its ring slot (cpu mode).
+  auto load = [&](size_t n) -> bool {
+    if (n >= qs.size()) return true;
+    const int64_t q = qs[n];
+    const int slot = (int)(q % kRing);
+    cudaStream_t ls = pipeline ? ss : st;
+    if (pipeline && TB_CUDA(cudaStreamWaitEvent(ss, consumed.ev[slot], 0))) return false;
+    const size_t off1 = (size_t)slot * step_bytes, off3 = (size_t)q * step_bytes;
+    if (ca_requires_grad && TB_CUDA(cudaMemcpyAsync((char *)ey_store_1 + off1,
+                                                    (char *)ey_store_3 + off3, step_bytes,
+                                                    cudaMemcpyHostToDevice, ls)))
+      return false;
+    if (cb_requires_grad && TB_CUDA(cudaMemcpyAsync((char *)curl_store_1 + off1,
+                                                    (char *)curl_store_3 + off3, step_bytes,
+                                                    cudaMemcpyHostToDevice, ls)))
+      return false;
+    if (pipeline && TB_CUDA(cudaEventRecord(loaded.ev[slot], ss))) return false;
+    return true;
+  };
+  size_t next_q = 0;  // position in qs of the next store index to consume
+  if (storage_mode == 1 && grads) {
+    for (size_t n = 0; n < std::min<size_t>(2, qs.size()); ++n)
+      if (!load(n)) return;
+  }
+  // Gradient arguments for store index q; in cpu mode waits for its load.
+  auto grad_args = [&](int64_t q, bool &ok) {
+    ok = true;
+    GradArgs<T, T> ga{nullptr, nullptr, acc_ca, acc_cb, (T)step_ratio};
+    const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
+                                          : (size_t)(q % kRing) * step_bytes;
+    if (ca_requires_grad) ga.ey_st = (const T *)((const char *)ey_store_1 + off1);
+    if (cb_requires_grad) ga.cu_st = (const T *)((const char *)curl_store_1 + off1);
+    if (storage_mode == 1 && pipeline)
+      ok = !TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0));
+    return ga;
+  };
+  auto after_consume = [&](int64_t q) -> bool {
+    ++next_q;
+    if (storage_mode != 1) return true;
+    if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return false;
+    return load(next_q + 1);
+  };
+  const GradArgs<T, T> no_grad{nullptr, nullptr, acc_ca, acc_cb, (T)step_ratio};
+
+  T *cur_ey_x = m_lambda_ey_x, *cur_ey_z = m_lambda_ey_z;
+  T *cur_hx_z = m_lambda_hx_z, *cur_hz_x = m_lambda_hz_x;
+  T *nxt_ey_x = adjoint_memory_scratch, *nxt_ey_z = adjoint_memory_scratch + SN;
+  T *nxt_hx_z = adjoint_memory_scratch + 2 * SN, *nxt_hz_x = adjoint_memory_scratch + 3 * SN;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+
+  auto launch_adj_e = [&](const GradArgs<T, T> &ga) {
+    if (bf16) {
+      GradArgs<T, __nv_bfloat16> gb{(const __nv_bfloat16 *)ga.ey_st,
+                                    (const __nv_bfloat16 *)ga.cu_st, ga.acc_ca, ga.acc_cb,
+                                    ga.kscale};
+      k_adj_e<T, ST, __nv_bfloat16><<<L.grid_dom, L.block, 0, st>>>(
+          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x, gb);
+    } else {
+      k_adj_e<T, ST, T><<<L.grid_dom, L.block, 0, st>>>(
+          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x, ga);
+    }
+  };
+
+  ProfileScope prof(st);
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    const bool smp = prof.sample(t);
+    // Coefficient gradient of step t+1 (imaged in this call) rides on the
+    // E-phase kernel, which still sees the final adjoint of step t+1.
+    const int64_t tp = t + 1;
+    const bool grad_prev = grads && tp < start_t && tp % step_ratio == 0;
+    GradArgs<T, T> ga = no_grad;
+    if (grad_prev) {
+      bool ok;
+      ga = grad_args(tp / step_ratio, ok);
+      if (!ok) return;
+    }
+    if (L.has_domain) {
+      if (smp) prof.begin(kKAdjE);
+      launch_adj_e(ga);
+      if (smp) prof.end(kKAdjE);
+    }
+    if (grad_prev && !after_consume(tp / step_ratio)) return;
+    std::swap(cur_hx_z, nxt_hx_z);
+    std::swap(cur_hz_x, nxt_hz_x);
+    if (smp) prof.begin(kKAdjH);
+    k_adj_h<T, ST><<<L.grid_full, L.block, 0, st>>>(
+        L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
+        ps.rec, ps.src, grad_r ? grad_r + t * rs : nullptr, grad_f ? grad_f + t * fs : nullptr);
+    if (smp) prof.end(kKAdjH);
+    std::swap(cur_ey_x, nxt_ey_x);
+    std::swap(cur_ey_z, nxt_ey_z);
+  }
+  const int64_t t_last = start_t - nt;
+  if (grads && nt > 0 && t_last % step_ratio == 0 && L.has_domain) {
+    bool ok;
+    GradArgs<T, T> ga = grad_args(t_last / step_ratio, ok);
+    if (!ok) return;
+    if (bf16) {
+      GradArgs<T, __nv_bfloat16> gb{(const __nv_bfloat16 *)ga.ey_st,
+                                    (const __nv_bfloat16 *)ga.cu_st, ga.acc_ca, ga.acc_cb,
+                                    ga.kscale};
+      k_coeff_grad<T, ST, __nv_bfloat16><<<L.grid_dom, L.block, 0, st>>>(L.g, lambda_ey, gb);
+    } else {
+      k_coeff_grad<T, ST, T><<<L.grid_dom, L.block, 0, st>>>(L.g, lambda_ey, ga);
+    }
+    if (!after_consume(t_last / step_ratio)) return;
+  }
+  // Leave the final adjoint memories in the caller's arrays
+  // (maxwell_tm_cuda_inst.cu:1256-1277).
+  const size_t nbytes = SN * sizeof(T);
+  if (cur_ey_x != m_lambda_ey_x) {
+    if (TB_CUDA(cudaMemcpyAsync(m_lambda_ey_x, cur_ey_x, nbytes, cudaMemcpyDeviceToDevice, st)))
+      return;
+    if (TB_CUDA(cudaMemcpyAsync(m_lambda_ey_z, cur_ey_z, nbytes, cudaMemcpyDeviceToDevice, st)))
+      return;
+    if (TB_CUDA(cudaMemcpyAsync(m_lambda_hx_z, cur_hx_z, nbytes, cudaMemcpyDeviceToDevice, st)))
+      return;
+    if (TB_CUDA(cudaMemcpyAsync(m_lambda_hz_x, cur_hz_x, nbytes, cudaMemcpyDeviceToDevice, st)))
+      return;
+  }
+  if (grads && L.has_domain) {
+    if (ca_requires_grad && !ca_batched)
+      k_combine<T, ST><<<dim3(L.grid_dom.x, L.grid_dom.y, 1), L.block, 0, st>>>(L.g, grad_ca,
+                                                                               acc_ca);
+    if (cb_requires_grad && !cb_batched)
+      k_combine<T, ST><<<dim3(L.grid_dom.x, L.grid_dom.y, 1), L.block, 0, st>>>(L.g, grad_cb,
+                                                                               acc_cb);
+  }
+  count_launches(nt * (L.has_domain ? 2 : 1) + 3);
+  if (TB_CUDA(cudaGetLastError())) return;
+  if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
+}
+
+}  // namespace
+}  // namespace tb
+
+#define TB_DEFINE(S, T)                                                        \
+  extern "C" void maxwell_tm_##S##_##T##_forward_cuda(TIDE_TM_FORWARD_ARGS(T)) { \
+    tb::tm_forward<T, S>(                                                      \
+        ca, cb, cq, f, ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x, debye_a, debye_b, debye_cp, \
+        polarization, ey_prev, r, n_poles, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx,   \
+        kxh, sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,   \
+        n_receivers_per_shot, step_ratio, has_dispersion, ca_batched, cb_batched, cq_batched, \
+        start_t, pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream);          \
+  }                                                                            \
+  extern "C" void maxwell_tm_##S##_##T##_forward_with_storage_cuda(            \
+      TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {                                  \
+    tb::tm_forward_with_storage<T, S>(                                         \
+        ca, cb, cq, f, ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x, r, ey_store_1, ey_store_3, \
+        ey_filenames, curl_store_1, curl_store_3, curl_filenames, ay, by, ayh, byh, ax, bx,   \
+        axh, bxh, ky, kyh, kx, kxh, sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, \
+        n_sources_per_shot, n_receivers_per_shot, step_ratio, storage_mode, storage_format,   \
+        shot_bytes_uncomp, ca_requires_grad, cb_requires_grad, ca_batched, cb_batched,        \
+        cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device,               \
+        compute_stream, storage_stream);                                       \
+  }                                                                            \
+  extern "C" void maxwell_tm_##S##_##T##_backward_cuda(TIDE_TM_BACKWARD_ARGS(T)) { \
+    tb::tm_backward<T, S>(                                                     \
+        ca, cb, cq, grad_r, lambda_ey, lambda_hx, lambda_hz, m_lambda_ey_x, m_lambda_ey_z,    \
+        m_lambda_hx_z, m_lambda_hz_x, adjoint_memory_scratch, ey_store_1, ey_store_3,         \
+        ey_filenames, curl_store_1, curl_store_3, curl_filenames, grad_f, grad_ca, grad_cb,   \
+        grad_ca_shot, grad_cb_shot, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh,     \
+        sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,        \
+        n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
+        ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,      \
+        pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);   \
+  }
+
+TB_DEFINE(2, float)
+TB_DEFINE(4, float)
+TB_DEFINE(6, float)
+TB_DEFINE(8, float)
+TB_DEFINE(2, double)
+TB_DEFINE(4, double)
+TB_DEFINE(6, double)
+TB_DEFINE(8, double)
+
+extern "C" int tide_b200_device_status(int64_t device) {
+  if (TB_CUDA(cudaSetDevice((int)device))) return -1;
+  if (TB_CUDA(cudaDeviceSynchronize())) return -1;
+  int v = 0;
+  if (TB_CUDA(cudaMemcpyFromSymbol(&v, tb::g_tide_dev_err, sizeof(int)))) return -1;
+  const int zero = 0;
+  if (TB_CUDA(cudaMemcpyToSymbol(tb::g_tide_dev_err, &zero, sizeof(int)))) return -1;
+  return v;
+}

@@ -1,0 +1,45 @@
+"""tide_b200 — B200-native (sm_100a) TM2D time stepping with TIDE's API.
+
+``import tide_b200 as tide`` gives the operator API of the reference
+(``MaxwellTM``, ``EMModel``, ``Experiment``, ``Acquisition``,
+``Discretization``, ``CPML``, ``StorageOptions``, ``operator.linearize``)
+and the functional ``maxwelltm``; all propagation runs in libtide_b200.so.
+"""
+
+from .api import (
+    CPML,
+    Acquisition,
+    BackendPreference,
+    Discretization,
+    EMGradient,
+    EMModel,
+    ExecutionOptions,
+    Experiment,
+    FallbackPolicy,
+    ForwardResult,
+    LinearizedMaxwellTM,
+    MaxwellTM,
+    Observers,
+    TMState,
+)
+from .physics import (
+    C0,
+    EP0,
+    MU0,
+    DebyeDispersion,
+    cfl_condition,
+    downsample,
+    prepare_parameters,
+    ricker,
+    upsample,
+)
+from .storage import StorageMode, StorageOptions
+from .tm2d import CallbackState, maxwelltm, prepare_tm2d, propagate
+
+__all__ = [
+    "CPML", "Acquisition", "BackendPreference", "C0", "CallbackState", "DebyeDispersion",
+    "Discretization", "EMGradient", "EMModel", "EP0", "ExecutionOptions", "Experiment",
+    "FallbackPolicy", "ForwardResult", "LinearizedMaxwellTM", "MU0", "MaxwellTM", "Observers",
+    "StorageMode", "StorageOptions", "TMState", "cfl_condition", "downsample", "maxwelltm",
+    "prepare_parameters", "prepare_tm2d", "propagate", "ricker", "upsample",
+]

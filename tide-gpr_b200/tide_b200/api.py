@@ -1,0 +1,268 @@
+"""Operator-level public API: value objects, MaxwellTM, linearization.
+
+Mirrors src/tide/maxwell/contracts.py:24-201, results.py:12-90,
+operators.py:26-129 and linearization.py:36-232 (the vjp half; the Born jvp
+is not built here).  A user of the reference switches with
+``import tide_b200 as tide``.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Iterable
+from dataclasses import dataclass
+from enum import StrEnum
+from typing import Literal
+
+import torch
+
+from . import physics as ph
+from .storage import StorageOptions
+from .tm2d import Callback, maxwelltm
+
+
+class BackendPreference(StrEnum):
+    AUTO = "auto"
+    NATIVE = "native"
+    REFERENCE = "reference"
+
+
+class FallbackPolicy(StrEnum):
+    ERROR = "error"
+    REFERENCE = "reference"
+
+
+@dataclass(frozen=True, slots=True)
+class CPML:
+    """Convolutional PML boundary configuration."""
+
+    width: int | tuple[int, ...] = 20
+
+    def __post_init__(self) -> None:
+        widths = (self.width,) if isinstance(self.width, int) else self.width
+        if not widths or any(w < 0 for w in widths):
+            raise ValueError("CPML widths must be non-negative.")
+
+
+@dataclass(frozen=True, slots=True)
+class Discretization:
+    spacing: float | tuple[float, ...]
+    dt: float
+    stencil: int = 2
+    boundary: CPML = CPML()
+    max_velocity: float | None = None
+
+    def __post_init__(self) -> None:
+        sp = (self.spacing,) if isinstance(self.spacing, (int, float)) else self.spacing
+        if not sp or any(v <= 0 for v in sp):
+            raise ValueError("Grid spacing must be positive.")
+        if self.dt <= 0:
+            raise ValueError("dt must be positive.")
+        if self.stencil not in {2, 4, 6, 8}:
+            raise ValueError("stencil must be one of 2, 4, 6, or 8.")
+        if self.max_velocity is not None and self.max_velocity <= 0:
+            raise ValueError("max_velocity must be positive when provided.")
+
+
+@dataclass(frozen=True, slots=True)
+class Acquisition:
+    source_location: torch.Tensor | None
+    receiver_location: torch.Tensor | None
+
+    @property
+    def n_shots(self) -> int:
+        for t in (self.source_location, self.receiver_location):
+            if t is not None:
+                return int(t.shape[0])
+        return 1
+
+    @property
+    def n_receivers(self) -> int:
+        return 0 if self.receiver_location is None else int(self.receiver_location.shape[1])
+
+    @property
+    def spatial_ndim(self) -> int | None:
+        for t in (self.source_location, self.receiver_location):
+            if t is not None:
+                return int(t.shape[-1])
+        return None
+
+
+@dataclass(frozen=True, slots=True)
+class Experiment:
+    acquisition: Acquisition
+    source_amplitude: torch.Tensor | None
+    nt: int | None = None
+    source_component: str = "ey"
+    receiver_component: str = "ey"
+
+    def __post_init__(self) -> None:
+        if self.nt is not None and self.nt <= 0:
+            raise ValueError("nt must be positive when provided.")
+        if self.source_amplitude is None and self.nt is None:
+            raise ValueError("nt is required when source_amplitude is absent.")
+
+
+@dataclass(frozen=True, slots=True)
+class EMModel:
+    epsilon: torch.Tensor
+    sigma: torch.Tensor
+    mu: torch.Tensor
+    dispersion: ph.DebyeDispersion | None = None
+
+    def __post_init__(self) -> None:
+        if self.sigma.shape != self.epsilon.shape or self.mu.shape != self.epsilon.shape:
+            raise ValueError("epsilon, sigma, and mu must have the same shape.")
+        if self.sigma.device != self.epsilon.device or self.mu.device != self.epsilon.device:
+            raise ValueError("epsilon, sigma, and mu must be on the same device.")
+        if self.sigma.dtype != self.epsilon.dtype or self.mu.dtype != self.epsilon.dtype:
+            raise ValueError("epsilon, sigma, and mu must have the same dtype.")
+
+
+@dataclass(frozen=True, slots=True)
+class Observers:
+    forward: Callback | None = None
+    backward: Callback | None = None
+    frequency: int = 1
+
+    def __post_init__(self) -> None:
+        if self.frequency <= 0:
+            raise ValueError("Observer frequency must be positive.")
+
+
+@dataclass(frozen=True, slots=True)
+class ExecutionOptions:
+    backend: BackendPreference = BackendPreference.AUTO
+    fallback: FallbackPolicy = FallbackPolicy.ERROR
+    reference_mode: Literal["eager", "jit", "compile"] = "eager"
+    n_threads: int | None = None
+
+
+@dataclass(frozen=True, slots=True)
+class TMState:
+    Ey: torch.Tensor
+    Hx: torch.Tensor
+    Hz: torch.Tensor
+    m_Ey_x: torch.Tensor
+    m_Ey_z: torch.Tensor
+    m_Hx_z: torch.Tensor
+    m_Hz_x: torch.Tensor
+
+    @classmethod
+    def from_tensors(cls, tensors) -> TMState:
+        if len(tensors) != 7:
+            raise ValueError(f"TM state requires 7 tensors, got {len(tensors)}.")
+        return cls(*tensors)
+
+
+@dataclass(frozen=True, slots=True)
+class ForwardResult:
+    receiver_data: torch.Tensor
+    final_state: TMState
+
+
+@dataclass(frozen=True, slots=True)
+class EMGradient:
+    epsilon: torch.Tensor | None
+    sigma: torch.Tensor | None
+    mu: torch.Tensor | None = None
+
+
+class MaxwellTM:
+    """Differentiable 2-D TM Maxwell operator on the B200 native path."""
+
+    def __init__(
+        self,
+        discretization: Discretization,
+        experiment: Experiment,
+        *,
+        execution: ExecutionOptions = ExecutionOptions(),
+        storage: StorageOptions = StorageOptions(),
+        model_gradient_sampling_interval: int = 1,
+    ) -> None:
+        if experiment.acquisition.spatial_ndim not in {None, 2}:
+            raise ValueError("MaxwellTM requires two-dimensional acquisition coordinates.")
+        if execution.backend is BackendPreference.REFERENCE:
+            raise NotImplementedError(
+                "tide_b200 has no reference (torch) backend; the native CUDA path is the product."
+            )
+        self.discretization = discretization
+        self.experiment = experiment
+        self.execution = execution
+        self.storage = storage
+        self.model_gradient_sampling_interval = model_gradient_sampling_interval
+
+    def forward(
+        self, model: EMModel, *, state: TMState | None = None, observers: Observers = Observers()
+    ) -> ForwardResult:
+        if model.epsilon.ndim not in {2, 3}:
+            raise ValueError("MaxwellTM model tensors must be 2-D or batched 3-D tensors.")
+        init = (None,) * 7 if state is None else (
+            state.Ey, state.Hx, state.Hz, state.m_Ey_x, state.m_Ey_z, state.m_Hx_z, state.m_Hz_x)
+        d, e = self.discretization, self.experiment
+        out = maxwelltm(
+            model.epsilon, model.sigma, model.mu,
+            grid_spacing=d.spacing, dt=d.dt, source_amplitude=e.source_amplitude,
+            source_location=e.acquisition.source_location,
+            receiver_location=e.acquisition.receiver_location,
+            stencil=d.stencil, pml_width=d.boundary.width, max_vel=d.max_velocity,
+            Ey_0=init[0], Hx_0=init[1], Hz_0=init[2], m_Ey_x=init[3], m_Ey_z=init[4],
+            m_Hx_z=init[5], m_Hz_x=init[6], nt=e.nt,
+            model_gradient_sampling_interval=self.model_gradient_sampling_interval,
+            forward_callback=observers.forward, backward_callback=observers.backward,
+            callback_frequency=observers.frequency,
+            storage_mode=self.storage.mode.value, storage_compression=self.storage.compression,
+            storage_bytes_limit_device=self.storage.bytes_limit_device,
+            storage_bytes_limit_host=self.storage.bytes_limit_host,
+            dispersion=model.dispersion,
+        )
+        return ForwardResult(receiver_data=out[-1], final_state=TMState.from_tensors(out[:-1]))
+
+    __call__ = forward
+
+    def linearize(
+        self,
+        model: EMModel,
+        *,
+        storage: StorageOptions | None = None,
+        targets: Iterable[str] = ("epsilon", "sigma"),
+    ) -> LinearizedMaxwellTM:
+        return LinearizedMaxwellTM(self, model, storage=storage or self.storage, targets=targets)
+
+
+class LinearizedMaxwellTM:
+    """Linearization of MaxwellTM at a model: primal data and exact VJPs.
+
+    Follows src/tide/maxwell/linearization.py:36-160: the primal runs once
+    with the requested targets differentiable and keeps its autograd graph
+    (snapshots), and each vjp is one native adjoint pass.
+    """
+
+    def __init__(self, operator: MaxwellTM, model: EMModel, *, storage: StorageOptions,
+                 targets: Iterable[str]) -> None:
+        self.operator = operator
+        self.targets = tuple(targets)
+        for t in self.targets:
+            if t not in ("epsilon", "sigma"):
+                raise ValueError(f"unsupported linearization target {t!r}")
+        eps = model.epsilon.detach().requires_grad_("epsilon" in self.targets)
+        sig = model.sigma.detach().requires_grad_("sigma" in self.targets)
+        self._inputs = {"epsilon": eps, "sigma": sig}
+        self.model = EMModel(eps, sig, model.mu.detach(), model.dispersion)
+        op = MaxwellTM(operator.discretization, operator.experiment, execution=operator.execution,
+                       storage=storage,
+                       model_gradient_sampling_interval=operator.model_gradient_sampling_interval)
+        self._result = op(self.model)
+
+    @property
+    def primal(self) -> ForwardResult:
+        return ForwardResult(self._result.receiver_data.detach(), self._result.final_state)
+
+    def vjp(self, cotangent: torch.Tensor, *, retain_graph: bool = True) -> EMGradient:
+        ins = [self._inputs[t] for t in self.targets]
+        grads = torch.autograd.grad(self._result.receiver_data, ins, grad_outputs=cotangent,
+                                    retain_graph=retain_graph, allow_unused=True)
+        g = dict(zip(self.targets, grads))
+        return EMGradient(epsilon=g.get("epsilon"), sigma=g.get("sigma"))
+
+    def jvp(self, direction):  # pragma: no cover - documented gap
+        raise NotImplementedError("Born (jvp) propagation is not built in tide_b200.")

@@ -1,0 +1,173 @@
+"""Snapshot storage policy and buffers for the gradient path.
+
+Modes and formats share the reference's integer codes
+(src/tide/storage.py:18-30, src/tide/csrc/storage/storage_utils.h:9-16):
+
+* ``device`` (0): the whole history ``[n_store, S, ny, nx]`` lives in HBM;
+* ``cpu`` (1): a 3-slot device ring plus a pinned host history
+  ``[n_store, S, ny*nx]``; the native library copies each stored step to the
+  host on a side stream while the next steps compute, and streams it back in
+  the adjoint (pinned-host offload);
+* ``none`` (3): nothing stored (forward only);
+* ``auto``: ``device`` when the history fits the device budget, else ``cpu``.
+
+Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
+(float32 fields only).  Disk spilling (mode 2) is not built in this library.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from enum import StrEnum
+
+import torch
+
+STORAGE_DEVICE = 0
+STORAGE_CPU = 1
+STORAGE_DISK = 2
+STORAGE_NONE = 3
+STORAGE_FORMAT_FULL = 0
+STORAGE_FORMAT_BF16 = 1
+RING_SLOTS = 3
+
+
+class StorageMode(StrEnum):
+    DEVICE = "device"
+    CPU = "cpu"
+    DISK = "disk"
+    NONE = "none"
+    AUTO = "auto"
+
+
+@dataclass(frozen=True, slots=True)
+class StorageOptions:
+    """Snapshot storage policy (src/tide/core/types.py:66-88)."""
+
+    mode: StorageMode = StorageMode.DEVICE
+    path: str = "."
+    compression: bool | str = False
+    bytes_limit_device: int | None = None
+    bytes_limit_host: int | None = None
+    chunk_steps: int = 0
+
+    def __post_init__(self) -> None:
+        for name, v in (("bytes_limit_device", self.bytes_limit_device),
+                        ("bytes_limit_host", self.bytes_limit_host)):
+            if v is not None and v < 0:
+                raise ValueError(f"{name} must be non-negative when provided.")
+        if self.chunk_steps < 0:
+            raise ValueError("storage_chunk_steps must be non-negative.")
+
+
+def compression_format(compression: bool | str | None, dtype: torch.dtype) -> tuple[int, torch.dtype]:
+    """Map the public compression flag to (storage_format, stored dtype)."""
+    if compression is True:
+        kind = "bf16"
+    elif compression is False or compression is None:
+        kind = "none"
+    elif isinstance(compression, str) and compression.strip().lower() in {"none", "false", "off", "0"}:
+        kind = "none"
+    elif isinstance(compression, str) and compression.strip().lower() in {"bf16", "bfloat16"}:
+        kind = "bf16"
+    else:
+        raise ValueError("storage_compression must be False/True or one of 'none' or 'bf16'.")
+    if kind == "none":
+        return STORAGE_FORMAT_FULL, dtype
+    if dtype != torch.float32:
+        raise NotImplementedError("BF16 snapshot storage is only supported for float32.")
+    return STORAGE_FORMAT_BF16, torch.bfloat16
+
+
+def mode_code(mode: str) -> int:
+    m = str(mode).lower()
+    codes = {"device": STORAGE_DEVICE, "cpu": STORAGE_CPU, "disk": STORAGE_DISK, "none": STORAGE_NONE}
+    if m not in codes:
+        raise ValueError(f"storage_mode must be 'device', 'cpu', 'disk', 'none', or 'auto', got {mode!r}")
+    return codes[m]
+
+
+@dataclass(slots=True)
+class SnapshotBuffers:
+    """Device (and host) buffers for the Ey and curl-H histories."""
+
+    mode: int
+    fmt: int
+    dtype: torch.dtype
+    n_store: int
+    shot_bytes: int
+    ey_dev: torch.Tensor
+    ey_host: torch.Tensor
+    curl_dev: torch.Tensor
+    curl_host: torch.Tensor
+    keep: list = field(default_factory=list)
+
+
+def history_bytes(n_store: int, n_shots: int, ny: int, nx: int, itemsize: int, n_arrays: int) -> int:
+    return n_store * n_shots * ny * nx * itemsize * n_arrays
+
+
+def resolve_mode(
+    mode: str,
+    *,
+    device: torch.device,
+    n_store: int,
+    n_shots: int,
+    ny: int,
+    nx: int,
+    itemsize: int,
+    n_arrays: int,
+    bytes_limit_device: int | None,
+    bytes_limit_host: int | None,
+) -> int:
+    m = str(mode).lower()
+    if m != "auto":
+        code = mode_code(m)
+        if code == STORAGE_DISK:
+            raise NotImplementedError(
+                "storage_mode='disk' is not built in tide_b200; use 'device', 'cpu' "
+                "(pinned host offload) or gradient checkpointing."
+            )
+        return code
+    total = history_bytes(n_store, n_shots, ny, nx, itemsize, n_arrays)
+    limit_dev = bytes_limit_device
+    if limit_dev is None:
+        free, _ = torch.cuda.mem_get_info(device)
+        limit_dev = int(0.8 * free)
+    if total <= limit_dev:
+        return STORAGE_DEVICE
+    if bytes_limit_host is not None and total > bytes_limit_host:
+        raise MemoryError(
+            f"snapshot history of {total / 1e9:.1f} GB exceeds both budgets; "
+            "use checkpointing (tide_b200.checkpoint)"
+        )
+    return STORAGE_CPU
+
+
+def allocate(
+    mode: int,
+    fmt_dtype: torch.dtype,
+    fmt: int,
+    n_store: int,
+    n_shots: int,
+    ny: int,
+    nx: int,
+    device: torch.device,
+    want_ey: bool,
+    want_curl: bool,
+) -> SnapshotBuffers:
+    empty = torch.empty(0, device=device, dtype=fmt_dtype)
+    empty_h = torch.empty(0, dtype=fmt_dtype)
+    shot_bytes = ny * nx * fmt_dtype.itemsize
+
+    def one(want: bool) -> tuple[torch.Tensor, torch.Tensor]:
+        if not want or mode == STORAGE_NONE:
+            return empty, empty_h
+        if mode == STORAGE_DEVICE:
+            return torch.empty((n_store, n_shots, ny, nx), device=device, dtype=fmt_dtype), empty_h
+        ring = torch.empty((RING_SLOTS, n_shots, ny, nx), device=device, dtype=fmt_dtype)
+        host = torch.empty((n_store, n_shots, ny * nx), dtype=fmt_dtype, pin_memory=True)
+        return ring, host
+
+    ed, eh = one(want_ey)
+    cd, ch = one(want_curl)
+    return SnapshotBuffers(mode, fmt, fmt_dtype, n_store, shot_bytes, ed, eh, cd, ch)
