@@ -14,6 +14,10 @@
 #include <stdint.h>
 #include <string.h>
 
+/* Gradient shot-reduction order of the backward, see tm2d_oracle_impl.h. */
+static int g_oracle_grad_order = 0;
+void tide_oracle_set_grad_order(int order) { g_oracle_grad_order = order; }
+
 #define REAL float
 #define SFX float
 #include "tm2d_oracle_impl.h"

@@ -425,10 +425,18 @@ void FN(tide_oracle_tm_forward_with_storage)(
 
 /* Exact adjoint with fused coefficient gradient, device storage mode.
  * Interface semantics follow the reference CPU backward
- * (maxwell_tm_inst.cpp:1997-2219: per-shot accumulators cleared on entry,
- * batched models accumulate straight into grad_ca/grad_cb); arithmetic
- * follows the reference CUDA exact adjoint (maxwell_tm_cuda_inst.cu:2405-2734).
- * adjoint_memory_scratch holds the four next-step adjoint memories. */
+ * (maxwell_tm_inst.cpp:1997-2219: batched models accumulate straight into
+ * grad_ca/grad_cb); arithmetic follows the reference CUDA exact adjoint
+ * (maxwell_tm_cuda_inst.cu:2405-2734).  adjoint_memory_scratch holds the four
+ * next-step adjoint memories.
+ *
+ * The shot reduction of the model gradient has two summation orders
+ * (tide_oracle_set_grad_order):
+ *   0 (default) the reference's: per-shot accumulators over time, then a sum
+ *     over shots at the end (maxwell_tm_inst.cpp:2185-2206);
+ *   1 step-major: at every imaged step the shot terms are summed in shot order
+ *     and added to the model gradient (the order the CUDA kernels use).
+ * Both are exact sums of the same terms; they differ only in rounding. */
 void FN(tide_oracle_tm_backward)(
     int stencil, const REAL *ca, const REAL *cb, const REAL *cq,
     const REAL *grad_r, REAL *lam_ey, REAL *lam_hx, REAL *lam_hz,
@@ -448,6 +456,7 @@ void FN(tide_oracle_tm_backward)(
   const int64_t N = ny * nx, SN = n_shots * N;
   const int p = stencil / 2;
   const bool bf16 = storage_format == 1;
+  const bool step_major = g_oracle_grad_order == 1;
   REAL *acc_ca = ca_batched ? grad_ca : grad_ca_shot;
   REAL *acc_cb = cb_batched ? grad_cb : grad_cb_shot;
   if (ca_requires_grad && !ca_batched)
@@ -456,63 +465,75 @@ void FN(tide_oracle_tm_backward)(
     memset(grad_cb_shot, 0, (size_t)SN * sizeof(REAL));
   memset(scratch, 0, (size_t)4 * SN * sizeof(REAL));
   const REAL kscale = (REAL)step_ratio;
+  REAL *cur_ey_x = m_lam_ey_x, *cur_ey_z = m_lam_ey_z;
+  REAL *cur_hx_z = m_lam_hx_z, *cur_hz_x = m_lam_hz_x;
+  REAL *nxt_ey_x = scratch, *nxt_ey_z = scratch + SN;
+  REAL *nxt_hx_z = scratch + 2 * SN, *nxt_hz_x = scratch + 3 * SN;
   int64_t swaps = 0;
-#pragma omp parallel for schedule(static) reduction(max : swaps)
-  for (int64_t s = 0; s < n_shots; ++s) {
-    REAL *cur_ey_x = m_lam_ey_x, *cur_ey_z = m_lam_ey_z;
-    REAL *cur_hx_z = m_lam_hx_z, *cur_hz_x = m_lam_hz_x;
-    REAL *nxt_ey_x = scratch, *nxt_ey_z = scratch + SN;
-    REAL *nxt_hx_z = scratch + 2 * SN, *nxt_hz_x = scratch + 3 * SN;
-    int64_t my_swaps = 0;
-    for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
-      REAL *tmp;
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    REAL *tmp;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < n_shots; ++s)
       FN(adj_e)(&g, cb, lam_ey, lam_hx, lam_hz, cur_hx_z, cur_hz_x, nxt_hx_z,
                 nxt_hz_x, s);
-      tmp = cur_hx_z; cur_hx_z = nxt_hx_z; nxt_hx_z = tmp;
-      tmp = cur_hz_x; cur_hz_x = nxt_hz_x; nxt_hz_x = tmp;
+    tmp = cur_hx_z; cur_hx_z = nxt_hx_z; nxt_hx_z = tmp;
+    tmp = cur_hz_x; cur_hz_x = nxt_hz_x; nxt_hz_x = tmp;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < n_shots; ++s) {
       FN(adj_h)(&g, ca, cq, lam_hx, lam_hz, lam_ey, cur_ey_x, cur_ey_z,
                 nxt_ey_x, nxt_ey_z, s);
-      tmp = cur_ey_x; cur_ey_x = nxt_ey_x; nxt_ey_x = tmp;
-      tmp = cur_ey_z; cur_ey_z = nxt_ey_z; nxt_ey_z = tmp;
-      ++my_swaps;
       if (n_rec > 0)
         FN(inject)(lam_ey, grad_r + t * n_shots * n_rec, receivers_i, n_rec, N,
                    s);
       if (n_src > 0)
         FN(record)(grad_f + t * n_shots * n_src, lam_ey, sources_i, n_src, N,
                    s);
-      if ((t % step_ratio) == 0 && (ca_requires_grad || cb_requires_grad)) {
-        const int64_t off = (t / step_ratio) * SN;
-        for (int64_t y = p; y < ny - p + 1; ++y) {
-          for (int64_t x = p; x < nx - p + 1; ++x) {
-            const int64_t i = s * N + y * nx + x;
-            const REAL lam = lam_ey[i];
-            if (ca_requires_grad) {
-              const REAL e = bf16 ? FN(from_bf16)(((const uint16_t *)ey_store)[off + i])
-                                  : ((const REAL *)ey_store)[off + i];
-              acc_ca[i] += lam * e * kscale;
-            }
-            if (cb_requires_grad) {
-              const REAL c = bf16 ? FN(from_bf16)(((const uint16_t *)curl_store)[off + i])
-                                  : ((const REAL *)curl_store)[off + i];
-              acc_cb[i] += lam * c * kscale;
-            }
+    }
+    tmp = cur_ey_x; cur_ey_x = nxt_ey_x; nxt_ey_x = tmp;
+    tmp = cur_ey_z; cur_ey_z = nxt_ey_z; nxt_ey_z = tmp;
+    ++swaps;
+    if ((t % step_ratio) != 0 || !(ca_requires_grad || cb_requires_grad))
+      continue;
+    const int64_t off = (t / step_ratio) * SN;
+#pragma omp parallel for schedule(static)
+    for (int64_t y = p; y < ny - p + 1; ++y) {
+      for (int64_t x = p; x < nx - p + 1; ++x) {
+        const int64_t j = y * nx + x;
+        for (int pass = 0; pass < 2; ++pass) {
+          const bool want = pass == 0 ? ca_requires_grad : cb_requires_grad;
+          if (!want)
+            continue;
+          const void *store = pass == 0 ? ey_store : curl_store;
+          const bool batched = pass == 0 ? ca_batched : cb_batched;
+          REAL *acc = pass == 0 ? acc_ca : acc_cb;
+          REAL *grad = pass == 0 ? grad_ca : grad_cb;
+          REAL sum = (REAL)0;
+          for (int64_t s = 0; s < n_shots; ++s) {
+            const int64_t i = s * N + j;
+            const REAL v = bf16 ? FN(from_bf16)(((const uint16_t *)store)[off + i])
+                                : ((const REAL *)store)[off + i];
+            const REAL term = lam_ey[i] * v * kscale;
+            if (batched || !step_major)
+              acc[i] += term;
+            else
+              sum = sum + term;
           }
+          if (step_major && !batched)
+            grad[j] = grad[j] + sum;
         }
       }
     }
-    /* Leave the final adjoint memories in the caller's arrays. */
-    if (my_swaps % 2 == 1) {
-      const size_t nb = (size_t)N * sizeof(REAL);
-      memcpy(m_lam_ey_x + s * N, cur_ey_x + s * N, nb);
-      memcpy(m_lam_ey_z + s * N, cur_ey_z + s * N, nb);
-      memcpy(m_lam_hx_z + s * N, cur_hx_z + s * N, nb);
-      memcpy(m_lam_hz_x + s * N, cur_hz_x + s * N, nb);
-    }
-    if (my_swaps > swaps)
-      swaps = my_swaps;
   }
-  (void)swaps;
+  /* Leave the final adjoint memories in the caller's arrays. */
+  if (swaps % 2 == 1) {
+    const size_t nb = (size_t)SN * sizeof(REAL);
+    memcpy(m_lam_ey_x, cur_ey_x, nb);
+    memcpy(m_lam_ey_z, cur_ey_z, nb);
+    memcpy(m_lam_hx_z, cur_hx_z, nb);
+    memcpy(m_lam_hz_x, cur_hz_x, nb);
+  }
+  if (step_major)
+    return;
   for (int pass = 0; pass < 2; ++pass) {
     const bool want = pass == 0 ? (ca_requires_grad && !ca_batched)
                                 : (cb_requires_grad && !cb_batched);

@@ -158,3 +158,9 @@ def rel_l2(a: torch.Tensor, b: torch.Tensor) -> float:
     b = b.detach().double().cpu()
     den = torch.linalg.vector_norm(b)
     return float(torch.linalg.vector_norm(a - b) / (den if den > 0 else 1.0))
+
+
+def set_grad_order(oracle: Oracle, order: int) -> None:
+    """0: reference per-shot-then-shots order; 1: step-major (the CUDA kernels')."""
+    oracle.lib.tide_oracle_set_grad_order.argtypes = [c_int]
+    oracle.lib.tide_oracle_set_grad_order(order)

@@ -22,11 +22,18 @@ constexpr int kRing = 3;  // device ring slots of the cpu storage mode
 
 inline cudaStream_t as_stream(void *h) { return reinterpret_cast<cudaStream_t>(h); }
 
+// Rows per thread of each stencil kernel (see tm2d_kernels.cuh).
+constexpr int kRowsH = 4;   // forward H
+constexpr int kRowsE = 2;   // forward E (+ storage, points)
+constexpr int kRowsAE = 2;  // adjoint E
+
+inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)std::max<int64_t>(1, (a + b - 1) / b); }
+
 template <typename T, int ST> struct Launch {
   TMGeom<T> g;
-  dim3 block{kTileX, kTileY, 1};
-  dim3 grid_dom, grid_full;
-  int tiles_x = 0, tiles_y = 0, n_tiles = 0;
+  dim3 block{kTileX, kBlockY, 1};
+  dim3 grid_h, grid_e, grid_ae, grid_ah;
+  int tiles_x = 0, tiles_y_e = 0, tiles_y_ah = 0;
   bool has_domain = false;
 };
 
@@ -38,7 +45,7 @@ bool make_launch(Launch<T, ST> &L, const T *ay, const T *by, const T *ayh, const
                  int64_t pml_x1, bool ca_b, bool cb_b, bool cq_b) {
   constexpr int P = FD<ST>::P;
   if (n_shots < 1 || n_shots > 65535 || ny < 1 || nx < 1 || ny > (1 << 30) ||
-      nx > (1 << 30)) {
+      nx > (1 << 30) || ny * nx > ((int64_t)1 << 31) - 1) {
     set_error(kBadArgument, "TM2D: unsupported shape n_shots=%lld ny=%lld nx=%lld",
               (long long)n_shots, (long long)ny, (long long)nx);
     return false;
@@ -60,13 +67,14 @@ bool make_launch(Launch<T, ST> &L, const T *ay, const T *by, const T *ayh, const
   g.ca_b = ca_b; g.cb_b = cb_b; g.cq_b = cq_b;
   const int64_t dx = nx - 2 * P + 1, dy = ny - 2 * P + 1;
   L.has_domain = dx > 0 && dy > 0;
-  L.grid_dom = dim3((unsigned)std::max<int64_t>(1, (dx + kTileX - 1) / kTileX),
-                    (unsigned)std::max<int64_t>(1, (dy + kTileY - 1) / kTileY),
-                    (unsigned)n_shots);
-  L.tiles_x = (int)((nx + kTileX - 1) / kTileX);
-  L.tiles_y = (int)((ny + kTileY - 1) / kTileY);
-  L.grid_full = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y, (unsigned)n_shots);
-  L.n_tiles = L.tiles_x * L.tiles_y * (int)n_shots;
+  const unsigned S = (unsigned)n_shots;
+  L.grid_h = dim3(cdiv(dx, kTileX), cdiv(dy, kBlockY * kRowsH), S);
+  L.grid_ae = dim3(cdiv(dx, kTileX), cdiv(dy, kBlockY * kRowsAE), S);
+  L.tiles_x = (int)cdiv(nx, kTileX);
+  L.tiles_y_e = (int)cdiv(ny, kBlockY * kRowsE);
+  L.tiles_y_ah = (int)cdiv(ny, kBlockY);
+  L.grid_e = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_e, S);
+  L.grid_ah = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_ah, 1);
   return true;
 }
 
@@ -83,24 +91,27 @@ struct PointScratch {
 };
 
 bool build_list(const int64_t *idx, int n_per_shot, int n_shots, int64_t N, int nx,
-                int tiles_x, int tiles_y, int n_tiles, int *count, int *start, int *cell,
-                int *ent, cudaStream_t st, PointCSR &out) {
+                int tiles_x, int tiles_y, int tile_h, int n_tiles, int *count, int *start,
+                int *cell, int *ent, cudaStream_t st, PointCSR &out) {
   const int n = n_per_shot * n_shots;
   if (TB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * n_tiles, st))) return false;
   const int thr = 256, blk = (n + thr - 1) / thr;
-  k_points_count<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, count);
+  k_points_count<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y,
+                                      tile_h, count);
   k_points_scan<<<1, 1024, 0, st>>>(count, start, n_tiles);
-  k_points_fill<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, start,
-                                     cell, ent);
+  k_points_fill<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, tile_h,
+                                     start, cell, ent);
   if (TB_CUDA(cudaGetLastError())) return false;
   count_launches(3);
   out = PointCSR{start, cell, ent};
   return true;
 }
 
+// Point lists for tiles of 32 columns x tile_h rows (tiles_y per shot).
 template <typename T, int ST>
-bool build_points(PointScratch &ps, const Launch<T, ST> &L, const int64_t *sources_i,
-                  int64_t n_src, const int64_t *receivers_i, int64_t n_rec, cudaStream_t st) {
+bool build_points(PointScratch &ps, const Launch<T, ST> &L, int tiles_y, int tile_h,
+                  const int64_t *sources_i, int64_t n_src, const int64_t *receivers_i,
+                  int64_t n_rec, cudaStream_t st) {
   ps.st = st;
   const bool want_s = n_src > 0 && sources_i != nullptr;
   const bool want_r = n_rec > 0 && receivers_i != nullptr;
@@ -110,22 +121,23 @@ bool build_points(PointScratch &ps, const Launch<T, ST> &L, const int64_t *sourc
     set_error(kBadArgument, "TM2D: too many source/receiver entries");
     return false;
   }
-  const size_t nt1 = (size_t)L.n_tiles + 1;
+  const int n_tiles = L.tiles_x * tiles_y * (int)S;
+  const size_t nt1 = (size_t)n_tiles + 1;
   const size_t ns = want_s ? (size_t)(n_src * S) : 0, nr = want_r ? (size_t)(n_rec * S) : 0;
   const size_t words = (want_s ? 2 * nt1 + 2 * ns : 0) + (want_r ? 2 * nt1 + 2 * nr : 0);
   if (TB_CUDA(cudaMallocAsync(&ps.mem, words * sizeof(int), st))) return false;
   int *w = static_cast<int *>(ps.mem);
   if (want_s) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
-    if (!build_list(sources_i, (int)n_src, (int)S, L.g.N, L.g.nx, L.tiles_x, L.tiles_y,
-                    L.n_tiles, count, start, cell, ent, st, ps.src))
+    if (!build_list(sources_i, (int)n_src, (int)S, L.g.N, L.g.nx, L.tiles_x, tiles_y, tile_h,
+                    n_tiles, count, start, cell, ent, st, ps.src))
       return false;
     w += 2 * nt1 + 2 * ns;
   }
   if (want_r) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + nr;
-    if (!build_list(receivers_i, (int)n_rec, (int)S, L.g.N, L.g.nx, L.tiles_x, L.tiles_y,
-                    L.n_tiles, count, start, cell, ent, st, ps.rec))
+    if (!build_list(receivers_i, (int)n_rec, (int)S, L.g.N, L.g.nx, L.tiles_x, tiles_y, tile_h,
+                    n_tiles, count, start, cell, ent, st, ps.rec))
       return false;
   }
   return true;
@@ -145,6 +157,15 @@ struct EventRing {
 };
 
 // ---------------------------------------------------------------------------
+template <typename T, int ST, typename S>
+inline void launch_fwd_e(const Launch<T, ST> &L, cudaStream_t st, const T *ca, const T *cb,
+                         const T *hx, const T *hz, T *ey, T *m_hx_z, T *m_hz_x, S *e_st,
+                         S *c_st, const DebyeArgs<T> &db, const PointScratch &ps, const T *ft,
+                         T *rt) {
+  k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
+                                                          e_st, c_st, db, ps.src, ps.rec, ft, rt);
+}
+
 template <typename T, int ST>
 void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads;
@@ -167,8 +188,8 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
     return;
   cudaStream_t st = as_stream(compute_stream);
   PointScratch ps;
-  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
-                    st))
+  if (!build_points(ps, L, L.tiles_y_e, kBlockY * kRowsE, sources_i, n_sources_per_shot,
+                    receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   ProfileScope prof(st);
@@ -176,13 +197,12 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
     const bool smp = prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
-      k_fwd_h<T, ST><<<L.grid_dom, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      k_fwd_h<T, ST, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
       if (smp) prof.end(kKFwdH);
     }
     if (smp) prof.begin(kKFwdE);
-    k_fwd_e<T, ST, T><<<L.grid_full, L.block, 0, st>>>(
-        L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)nullptr, (T *)nullptr, db, ps.src, ps.rec,
-        f ? f + t * fs : nullptr, r ? r + t * rs : nullptr);
+    launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, nullptr, nullptr, db, ps,
+                           f ? f + t * fs : nullptr, r ? r + t * rs : nullptr);
     if (smp) prof.end(kKFwdE);
   }
   count_launches(nt * (L.has_domain ? 2 : 1));
@@ -225,8 +245,8 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   cudaStream_t ss = as_stream(storage_stream);
   const bool pipeline = want_store && storage_mode == 1 && ss != nullptr && ss != st;
   PointScratch ps;
-  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
-                    st))
+  if (!build_points(ps, L, L.tiles_y_e, kBlockY * kRowsE, sources_i, n_sources_per_shot,
+                    receivers_i, n_receivers_per_shot, st))
     return;
   EventRing store_done, compute_done;
   if (pipeline) {
@@ -239,7 +259,7 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   }
   const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
-  DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
+  const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
   ProfileScope prof(st);
   for (int64_t t = start_t; t < start_t + nt; ++t) {
     const bool smp = prof.sample(t);
@@ -255,21 +275,18 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     }
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
-      k_fwd_h<T, ST><<<L.grid_dom, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      k_fwd_h<T, ST, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
       if (smp) prof.end(kKFwdH);
     }
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
     if (smp) prof.begin(kKFwdE);
-    if (store_step && bf16) {
-      k_fwd_e<T, ST, __nv_bfloat16><<<L.grid_full, L.block, 0, st>>>(
-          L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db,
-          ps.src, ps.rec, ft, rt);
-    } else {
-      k_fwd_e<T, ST, T><<<L.grid_full, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z,
-                                                          m_hz_x, (T *)e1, (T *)c1, db, ps.src,
-                                                          ps.rec, ft, rt);
-    }
+    if (store_step && bf16)
+      launch_fwd_e<T, ST, __nv_bfloat16>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
+                                         (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db, ps, ft, rt);
+    else
+      launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)e1, (T *)c1, db, ps,
+                             ft, rt);
     if (smp) prof.end(kKFwdE);
     if (store_step && storage_mode == 1) {
       cudaStream_t cs = st;
@@ -294,9 +311,18 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
 }
 
 // ---------------------------------------------------------------------------
+template <typename T>
+bool zero_band(T *m, const TMGeom<T> &g, int axis, int lo, int hi, cudaStream_t st) {
+  if (hi <= lo) return true;
+  k_zero_band<T><<<1184, 256, 0, st>>>(m, g.n_shots, g.ny, g.nx, axis, lo, hi);
+  count_launches(1);
+  return !TB_CUDA(cudaGetLastError());
+}
+
 template <typename T, int ST>
 void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   (void)dt; (void)n_threads; (void)ey_filenames; (void)curl_filenames;
+  (void)grad_ca_shot; (void)grad_cb_shot;  // gradients are reduced in-kernel (see k_adj_h)
   if (TB_CUDA(cudaSetDevice((int)device))) return;
   TB_REQUIRE(nt >= 0 && step_ratio >= 1 && start_t - nt >= 0,
              "TM2D backward: bad nt/step_ratio/start_t");
@@ -315,9 +341,6 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     TB_REQUIRE((!ca_requires_grad || (ey_store_1 && grad_ca)) &&
                    (!cb_requires_grad || (curl_store_1 && grad_cb)),
                "TM2D backward: gradient or snapshot buffers missing");
-    TB_REQUIRE((!ca_requires_grad || ca_batched || grad_ca_shot) &&
-                   (!cb_requires_grad || cb_batched || grad_cb_shot),
-               "TM2D backward: per-shot accumulators missing");
     TB_REQUIRE(storage_mode != 1 ||
                    ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
                "TM2D backward: cpu storage mode needs host snapshot buffers");
@@ -330,16 +353,17 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   cudaStream_t ss = as_stream(storage_stream);
   const bool pipeline = grads && storage_mode == 1 && ss != nullptr && ss != st;
   const size_t SN = (size_t)n_shots * (size_t)L.g.N;
-  T *acc_ca = ca_requires_grad ? (ca_batched ? grad_ca : grad_ca_shot) : nullptr;
-  T *acc_cb = cb_requires_grad ? (cb_batched ? grad_cb : grad_cb_shot) : nullptr;
-  if (grads) {
-    if (acc_ca && !ca_batched && TB_CUDA(cudaMemsetAsync(acc_ca, 0, SN * sizeof(T), st))) return;
-    if (acc_cb && !cb_batched && TB_CUDA(cudaMemsetAsync(acc_cb, 0, SN * sizeof(T), st))) return;
-  }
+  // Both ping-pong buffers of every CPML memory adjoint hold zeros outside
+  // their strips for the whole call, so the kernels only write strip cells.
   if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, 4 * SN * sizeof(T), st))) return;
+  if (!zero_band(m_lambda_hz_x, L.g, 1, L.g.pml_x0, L.g.pml_x1, st) ||
+      !zero_band(m_lambda_hx_z, L.g, 0, L.g.pml_y0, L.g.pml_y1, st) ||
+      !zero_band(m_lambda_ey_x, L.g, 1, L.g.pml_x0, L.g.pml_x1h, st) ||
+      !zero_band(m_lambda_ey_z, L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
+    return;
   PointScratch ps;
-  if (!build_points(ps, L, sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
-                    st))
+  if (!build_points(ps, L, L.tiles_y_ah, kBlockY, sources_i, n_sources_per_shot, receivers_i,
+                    n_receivers_per_shot, st))
     return;
 
   // Store indices consumed by this call, latest first.
@@ -356,7 +380,8 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   if (pipeline)
     for (int k = 0; k < kRing; ++k)
       if (TB_CUDA(cudaEventRecord(consumed.ev[k], st))) return;
-  // Issue the H2D copy of store index qs[n] into its ring slot (cpu mode).
+  // cpu storage mode: copy store index qs[n] from the pinned host history into
+  // its device ring slot, on the side stream once the slot's last reader ran.
   auto load = [&](size_t n) -> bool {
     if (n >= qs.size()) return true;
     const int64_t q = qs[n];
@@ -375,30 +400,10 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (pipeline && TB_CUDA(cudaEventRecord(loaded.ev[slot], ss))) return false;
     return true;
   };
-  size_t next_q = 0;  // position in qs of the next store index to consume
-  if (storage_mode == 1 && grads) {
+  size_t next_q = 0;
+  if (storage_mode == 1 && grads)
     for (size_t n = 0; n < std::min<size_t>(2, qs.size()); ++n)
       if (!load(n)) return;
-  }
-  // Gradient arguments for store index q; in cpu mode waits for its load.
-  auto grad_args = [&](int64_t q, bool &ok) {
-    ok = true;
-    GradArgs<T, T> ga{nullptr, nullptr, acc_ca, acc_cb, (T)step_ratio};
-    const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
-                                          : (size_t)(q % kRing) * step_bytes;
-    if (ca_requires_grad) ga.ey_st = (const T *)((const char *)ey_store_1 + off1);
-    if (cb_requires_grad) ga.cu_st = (const T *)((const char *)curl_store_1 + off1);
-    if (storage_mode == 1 && pipeline)
-      ok = !TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0));
-    return ga;
-  };
-  auto after_consume = [&](int64_t q) -> bool {
-    ++next_q;
-    if (storage_mode != 1) return true;
-    if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return false;
-    return load(next_q + 1);
-  };
-  const GradArgs<T, T> no_grad{nullptr, nullptr, acc_ca, acc_cb, (T)step_ratio};
 
   T *cur_ey_x = m_lambda_ey_x, *cur_ey_z = m_lambda_ey_z;
   T *cur_hx_z = m_lambda_hx_z, *cur_hz_x = m_lambda_hz_x;
@@ -406,62 +411,50 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   T *nxt_hx_z = adjoint_memory_scratch + 2 * SN, *nxt_hz_x = adjoint_memory_scratch + 3 * SN;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
 
-  auto launch_adj_e = [&](const GradArgs<T, T> &ga) {
-    if (bf16) {
-      GradArgs<T, __nv_bfloat16> gb{(const __nv_bfloat16 *)ga.ey_st,
-                                    (const __nv_bfloat16 *)ga.cu_st, ga.acc_ca, ga.acc_cb,
-                                    ga.kscale};
-      k_adj_e<T, ST, __nv_bfloat16><<<L.grid_dom, L.block, 0, st>>>(
-          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x, gb);
-    } else {
-      k_adj_e<T, ST, T><<<L.grid_dom, L.block, 0, st>>>(
-          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x, ga);
-    }
-  };
-
   ProfileScope prof(st);
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
     const bool smp = prof.sample(t);
-    // Coefficient gradient of step t+1 (imaged in this call) rides on the
-    // E-phase kernel, which still sees the final adjoint of step t+1.
-    const int64_t tp = t + 1;
-    const bool grad_prev = grads && tp < start_t && tp % step_ratio == 0;
-    GradArgs<T, T> ga = no_grad;
-    if (grad_prev) {
-      bool ok;
-      ga = grad_args(tp / step_ratio, ok);
-      if (!ok) return;
-    }
     if (L.has_domain) {
       if (smp) prof.begin(kKAdjE);
-      launch_adj_e(ga);
+      k_adj_e<T, ST, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(
+          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x);
       if (smp) prof.end(kKAdjE);
     }
-    if (grad_prev && !after_consume(tp / step_ratio)) return;
     std::swap(cur_hx_z, nxt_hx_z);
     std::swap(cur_hz_x, nxt_hz_x);
+    const bool grad_step = grads && t % step_ratio == 0;
+    const int64_t q = t / step_ratio;
+    const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
+                                          : (size_t)(q % kRing) * step_bytes;
+    if (grad_step && pipeline &&
+        TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0)))
+      return;
+    const char *es = grad_step && ca_requires_grad ? (const char *)ey_store_1 + off1 : nullptr;
+    const char *cs = grad_step && cb_requires_grad ? (const char *)curl_store_1 + off1 : nullptr;
+    const T *grt = grad_r ? grad_r + t * rs : nullptr;
+    T *gft = grad_f ? grad_f + t * fs : nullptr;
     if (smp) prof.begin(kKAdjH);
-    k_adj_h<T, ST><<<L.grid_full, L.block, 0, st>>>(
-        L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
-        ps.rec, ps.src, grad_r ? grad_r + t * rs : nullptr, grad_f ? grad_f + t * fs : nullptr);
+    if (bf16) {
+      GradArgs<T, __nv_bfloat16> ga{(const __nv_bfloat16 *)es, (const __nv_bfloat16 *)cs,
+                                    grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched};
+      k_adj_h<T, ST, __nv_bfloat16><<<L.grid_ah, L.block, 0, st>>>(
+          L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
+          ps.rec, ps.src, grt, gft, ga);
+    } else {
+      GradArgs<T, T> ga{(const T *)es, (const T *)cs, grad_ca, grad_cb, (T)step_ratio,
+                        ca_batched, cb_batched};
+      k_adj_h<T, ST, T><<<L.grid_ah, L.block, 0, st>>>(
+          L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
+          ps.rec, ps.src, grt, gft, ga);
+    }
     if (smp) prof.end(kKAdjH);
     std::swap(cur_ey_x, nxt_ey_x);
     std::swap(cur_ey_z, nxt_ey_z);
-  }
-  const int64_t t_last = start_t - nt;
-  if (grads && nt > 0 && t_last % step_ratio == 0 && L.has_domain) {
-    bool ok;
-    GradArgs<T, T> ga = grad_args(t_last / step_ratio, ok);
-    if (!ok) return;
-    if (bf16) {
-      GradArgs<T, __nv_bfloat16> gb{(const __nv_bfloat16 *)ga.ey_st,
-                                    (const __nv_bfloat16 *)ga.cu_st, ga.acc_ca, ga.acc_cb,
-                                    ga.kscale};
-      k_coeff_grad<T, ST, __nv_bfloat16><<<L.grid_dom, L.block, 0, st>>>(L.g, lambda_ey, gb);
-    } else {
-      k_coeff_grad<T, ST, T><<<L.grid_dom, L.block, 0, st>>>(L.g, lambda_ey, ga);
+    if (grad_step && storage_mode == 1) {
+      ++next_q;
+      if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
+      if (!load(next_q + 1)) return;
     }
-    if (!after_consume(t_last / step_ratio)) return;
   }
   // Leave the final adjoint memories in the caller's arrays
   // (maxwell_tm_cuda_inst.cu:1256-1277).
@@ -476,15 +469,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (TB_CUDA(cudaMemcpyAsync(m_lambda_hz_x, cur_hz_x, nbytes, cudaMemcpyDeviceToDevice, st)))
       return;
   }
-  if (grads && L.has_domain) {
-    if (ca_requires_grad && !ca_batched)
-      k_combine<T, ST><<<dim3(L.grid_dom.x, L.grid_dom.y, 1), L.block, 0, st>>>(L.g, grad_ca,
-                                                                               acc_ca);
-    if (cb_requires_grad && !cb_batched)
-      k_combine<T, ST><<<dim3(L.grid_dom.x, L.grid_dom.y, 1), L.block, 0, st>>>(L.g, grad_cb,
-                                                                               acc_cb);
-  }
-  count_launches(nt * (L.has_domain ? 2 : 1) + 3);
+  count_launches(nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
   if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
 }

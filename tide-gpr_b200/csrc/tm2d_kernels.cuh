@@ -12,7 +12,7 @@
 // reproduces the exact transpose of src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:954-1165.
 //
 // Sources and receivers are not separate launches.  A per-call setup builds,
-// for each 32x8 tile of each shot, the list of point entries that fall in it
+// for each CTA tile (32 columns x tile_h rows) of each shot, the list of point entries that fall in it
 // (CSR by tile, entries in ascending entry order).  The E-update kernel (and
 // the adjoint H-update kernel) then finishes each cell in registers: it adds
 // the source terms of its cell in entry order, writes the cell once, and
@@ -26,8 +26,7 @@
 
 namespace tb {
 
-constexpr int kTileX = 32;  // CTA tile of the cell kernels (x fastest)
-constexpr int kTileY = 8;
+constexpr int kTileX = 32;  // CTA tile width of the cell kernels (x fastest)
 
 // Staggered-grid coefficients (src/tide/csrc/common/staggered_grid.h:229-417).
 template <int ST> struct FD;
@@ -152,37 +151,67 @@ __device__ __forceinline__ bool point_tile_empty(const PointCSR &a, const PointC
 }
 
 // ---------------------------------------------------------------------------
-// Forward H half-step (maxwell_tm_core.cuh:448-502).  Grid covers the update
-// domain [P, n-P+1)^2 with 32x8 tiles; grid.z = shot.
-template <typename T, int ST>
+// Launch shape shared by the stencil kernels: blocks of 32 (x) x 8 (y)
+// threads; each thread owns one column x and R consecutive rows, so a warp
+// touches 32 consecutive floats of R rows and every thread issues all of its
+// loads before any arithmetic (memory-level parallelism is what bounds these
+// kernels; one cell per thread left the SMs waiting on L1/L2).
+constexpr int kBlockY = 8;
+
+// Forward H half-step (maxwell_tm_core.cuh:448-502).  Grid: x over the update
+// domain [P, nx-P+1), y over row groups, z = shot.
+template <typename T, int ST, int R>
 __global__ void __launch_bounds__(256)
 k_fwd_h(TMGeom<T> g, const T *__restrict__ cq, const T *__restrict__ ey, T *__restrict__ hx,
         T *__restrict__ hz, T *__restrict__ m_ey_x, T *__restrict__ m_ey_z) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x + P;
-  const int y = blockIdx.y * kTileY + threadIdx.y + P;
-  const int s = blockIdx.z;
-  if (x >= g.nx - P + 1 || y >= g.ny - P + 1) return;
-  const int64_t j = (int64_t)y * g.nx + x;
-  const int64_t i = (int64_t)s * g.N + j;
-  const T cqv = g.cq_b ? ldg(cq + i) : ldg(cq + j);
-  if (y < g.ny - P) {
-    T d = d_yh1<T, ST>(ey, i, g.nx, g.rdy);
-    if (y < g.pml_y0 || y >= g.pml_y1h) {
-      const T m = ldg(g.byh + y) * m_ey_z[i] + ldg(g.ayh + y) * d;
-      m_ey_z[i] = m;
-      d = d / ldg(g.kyh + y) + m;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R + P;
+  const int ye = g.ny - P + 1;
+  if (x >= g.nx - P + 1 || y0 >= ye) return;
+  const int64_t base = (int64_t)blockIdx.z * g.N;
+  const bool do_hz = x < g.nx - P;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1h;
+  T cqv[R], dz[R], dx[R], hxv[R], hzv[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (y < ye) {
+      const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+      cqv[r] = g.cq_b ? ldg(cq + i) : ldg(cq + j);
+      if (y < g.ny - P) {
+        dz[r] = d_yh1<T, ST>(ey, i, g.nx, g.rdy);
+        hxv[r] = hx[i];
+      }
+      if (do_hz) {
+        dx[r] = d_xh1<T, ST>(ey, i, g.rdx);
+        hzv[r] = hz[i];
+      }
     }
-    hx[i] = hx[i] - cqv * d;
   }
-  if (x < g.nx - P) {
-    T d = d_xh1<T, ST>(ey, i, g.rdx);
-    if (x < g.pml_x0 || x >= g.pml_x1h) {
-      const T m = ldg(g.bxh + x) * m_ey_x[i] + ldg(g.axh + x) * d;
-      m_ey_x[i] = m;
-      d = d / ldg(g.kxh + x) + m;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (y >= ye) continue;
+    const int64_t i = base + (int64_t)y * g.nx + x;
+    if (y < g.ny - P) {
+      T d = dz[r];
+      if (y < g.pml_y0 || y >= g.pml_y1h) {
+        const T m = ldg(g.byh + y) * m_ey_z[i] + ldg(g.ayh + y) * d;
+        m_ey_z[i] = m;
+        d = d / ldg(g.kyh + y) + m;
+      }
+      hx[i] = hxv[r] - cqv[r] * d;
     }
-    hz[i] = hz[i] + cqv * d;
+    if (do_hz) {
+      T d = dx[r];
+      if (px) {
+        const T m = ldg(g.bxh + x) * m_ey_x[i] + ldg(g.axh + x) * d;
+        m_ey_x[i] = m;
+        d = d / ldg(g.kxh + x) + m;
+      }
+      hz[i] = hzv[r] + cqv[r] * d;
+    }
   }
 }
 
@@ -193,12 +222,22 @@ template <typename T> struct DebyeArgs {
   int n_poles;
 };
 
+template <typename S> __device__ __forceinline__ void store_stream(S *p, S v) { __stcs(p, v); }
+template <> __device__ __forceinline__ void store_stream<__nv_bfloat16>(__nv_bfloat16 *p,
+                                                                       __nv_bfloat16 v) {
+  __stcs(reinterpret_cast<unsigned short *>(p), __bfloat16_as_ushort(v));
+}
+template <typename S> __device__ __forceinline__ S load_stream(const S *p) { return __ldcs(p); }
+template <> __device__ __forceinline__ __nv_bfloat16 load_stream<__nv_bfloat16>(const __nv_bfloat16 *p) {
+  return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short *>(p)));
+}
+
 // Forward E half-step with optional snapshot storage, Debye polarisation,
 // source injection and receiver recording
 // (maxwell_tm_core.cuh:504-599, maxwell_tm_cuda_inst.cu:382-457,
-// maxwell.cu:89-141).  Grid covers the full [0,ny)x[0,nx) grid so that points
-// outside the update domain are still injected and recorded.
-template <typename T, int ST, typename S>
+// maxwell.cu:89-141).  Grid covers the full [0,ny)x[0,nx) grid (tiles of 32 x
+// 8R) so points outside the update domain are still injected and recorded.
+template <typename T, int ST, typename S, int R>
 __global__ void __launch_bounds__(256)
 k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
         const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
@@ -207,63 +246,82 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
         T *__restrict__ r_t) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y = blockIdx.y * kTileY + threadIdx.y;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int s = blockIdx.z;
   const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   const bool pts = !point_tile_empty(src, rec, tile);
-  if (x >= g.nx || y >= g.ny) return;
-  const bool dom = x >= P && y >= P && x < g.nx - P + 1 && y < g.ny - P + 1;
-  if (!dom && !pts) return;
-  const int64_t j = (int64_t)y * g.nx + x;
-  const int64_t i = (int64_t)s * g.N + j;
-  const T e_old = ey[i];
-  T e_new = e_old;
-  if (dom) {
-    const T cav = g.ca_b ? ldg(ca + i) : ldg(ca + j);
-    const T cbv = g.cb_b ? ldg(cb + i) : ldg(cb + j);
-    T dhz_dx = d_x1<T, ST>(hz, i, g.rdx);
-    T dhx_dz = d_y1<T, ST>(hx, i, g.nx, g.rdy);
-    if (x < g.pml_x0 || x >= g.pml_x1) {
-      const T m = ldg(g.bx + x) * m_hz_x[i] + ldg(g.ax + x) * dhz_dx;
-      m_hz_x[i] = m;
-      dhz_dx = dhz_dx / ldg(g.kx + x) + m;
-    }
-    if (y < g.pml_y0 || y >= g.pml_y1) {
-      const T m = ldg(g.by + y) * m_hx_z[i] + ldg(g.ay + y) * dhx_dz;
-      m_hx_z[i] = m;
-      dhx_dz = dhx_dz / ldg(g.ky + y) + m;
-    }
-    const T curl = dhz_dx - dhx_dz;
-    if (ey_store) ey_store[i] = Codec<S, T>::enc(e_old);
-    if (curl_store) curl_store[i] = Codec<S, T>::enc(curl);
-    e_new = cav * e_old + cbv * curl;
-    if (db.n_poles > 0) {
-      T pol_term = (T)0;
-      for (int p = 0; p < db.n_poles; ++p)
-        pol_term = pol_term + ldg(db.cp + (int64_t)p * g.N + j) *
-                                  db.pol[((int64_t)s * db.n_poles + p) * g.N + j];
-      e_new = e_new + pol_term;
+  if (x >= g.nx || y0 >= g.ny) return;
+  const int64_t base = (int64_t)s * g.N;
+  const bool xdom = x >= P && x < g.nx - P + 1;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1;
+  T eo[R], en[R], dhz[R], dhx[R], cav[R], cbv[R];
+  bool dom[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    dom[r] = xdom && y >= P && y < g.ny - P + 1;
+    if (dom[r] || (pts && y < g.ny)) {
+      const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+      eo[r] = ey[i];
+      if (dom[r]) {
+        cav[r] = g.ca_b ? ldg(ca + i) : ldg(ca + j);
+        cbv[r] = g.cb_b ? ldg(cb + i) : ldg(cb + j);
+        dhz[r] = d_x1<T, ST>(hz, i, g.rdx);
+        dhx[r] = d_y1<T, ST>(hx, i, g.nx, g.rdy);
+      }
     }
   }
-  if (pts) e_new = point_accumulate(src, tile, (int)j, f_t, e_new);
-  if (dom || pts) ey[i] = e_new;
-  if (dom && db.n_poles > 0) {
-    const T e_sum = e_new + e_old;
-    for (int p = 0; p < db.n_poles; ++p) {
-      const int64_t c = (int64_t)p * g.N + j;
-      const int64_t pi = ((int64_t)s * db.n_poles + p) * g.N + j;
-      db.pol[pi] = ldg(db.a + c) * db.pol[pi] + ldg(db.b + c) * e_sum;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (!(dom[r] || (pts && y < g.ny))) continue;
+    const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+    T e = eo[r];
+    if (dom[r]) {
+      T dz = dhz[r], dy = dhx[r];
+      if (px) {
+        const T m = ldg(g.bx + x) * m_hz_x[i] + ldg(g.ax + x) * dz;
+        m_hz_x[i] = m;
+        dz = dz / ldg(g.kx + x) + m;
+      }
+      if (y < g.pml_y0 || y >= g.pml_y1) {
+        const T m = ldg(g.by + y) * m_hx_z[i] + ldg(g.ay + y) * dy;
+        m_hx_z[i] = m;
+        dy = dy / ldg(g.ky + y) + m;
+      }
+      const T curl = dz - dy;
+      if (ey_store) store_stream(ey_store + i, Codec<S, T>::enc(e));
+      if (curl_store) store_stream(curl_store + i, Codec<S, T>::enc(curl));
+      e = cav[r] * e + cbv[r] * curl;
+      if (db.n_poles > 0) {
+        T pol_term = (T)0;
+        for (int p = 0; p < db.n_poles; ++p)
+          pol_term = pol_term + ldg(db.cp + (int64_t)p * g.N + j) *
+                                    db.pol[((int64_t)s * db.n_poles + p) * g.N + j];
+        e = e + pol_term;
+      }
     }
+    if (pts) e = point_accumulate(src, tile, (int)j, f_t, e);
+    ey[i] = e;
+    if (dom[r] && db.n_poles > 0) {
+      const T e_sum = e + eo[r];
+      for (int p = 0; p < db.n_poles; ++p) {
+        const int64_t c = (int64_t)p * g.N + j;
+        const int64_t pi = ((int64_t)s * db.n_poles + p) * g.N + j;
+        db.pol[pi] = ldg(db.a + c) * db.pol[pi] + ldg(db.b + c) * e_sum;
+      }
+    }
+    if (pts) point_record(rec, tile, (int)j, r_t, e);
+    en[r] = e;
   }
-  if (pts) point_record(rec, tile, (int)j, r_t, e_new);
+  (void)en;
 }
 
 // ---------------------------------------------------------------------------
-// Exact adjoint, E-phase (maxwell_tm_cuda_inst.cu:954-1027) with the
-// coefficient gradient of the previous (later-in-time) step fused in
-// (maxwell_tm_cuda_inst.cu:834-871).  lam_ey is not modified here, so at
-// iteration t it still holds the final adjoint of step t+1, which is exactly
-// what coeff_grad(t+1) consumes.
+// Exact adjoint, E-phase (maxwell_tm_cuda_inst.cu:954-1027).  The CPML memory
+// adjoints ping-pong between m (current, read) and m_n (next, written); the
+// next buffers are written only in their strips because both buffers hold
+// zeros elsewhere for the whole call (cleared on entry).
 template <typename T, int ST>
 __device__ __forceinline__ T raw_x(const TMGeom<T> &g, const T *cb, const T *lam, const T *m,
                                    int64_t base, int y, int x) {
@@ -287,73 +345,66 @@ __device__ __forceinline__ T raw_y(const TMGeom<T> &g, const T *cb, const T *lam
   return ldg(g.ay + y) * mn - q / ldg(g.ky + y);
 }
 
-template <typename T, typename S> struct GradArgs {
-  const S *ey_st;  // snapshot Ey^t of the step being imaged (nullptr: skip)
-  const S *cu_st;  // snapshot curl H^t
-  T *acc_ca;       // [n_shots, ny, nx] accumulators
-  T *acc_cb;
-  T kscale;        // gradient sampling interval as T
-};
-
-template <typename T, typename S>
-__device__ __forceinline__ void coeff_grad_cell(const GradArgs<T, S> &ga, int64_t i, T lam) {
-  if (ga.ey_st) ga.acc_ca[i] = ga.acc_ca[i] + lam * Codec<S, T>::dec(ga.ey_st[i]) * ga.kscale;
-  if (ga.cu_st) ga.acc_cb[i] = ga.acc_cb[i] + lam * Codec<S, T>::dec(ga.cu_st[i]) * ga.kscale;
-}
-
-template <typename T, int ST, typename S>
+template <typename T, int ST, int R>
 __global__ void __launch_bounds__(256)
 k_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
         T *__restrict__ lam_hx, T *__restrict__ lam_hz, const T *__restrict__ m_hx_z,
-        const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n,
-        GradArgs<T, S> ga) {
+        const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x + P;
-  const int y = blockIdx.y * kTileY + threadIdx.y + P;
-  const int s = blockIdx.z;
-  if (x >= g.nx - P + 1 || y >= g.ny - P + 1) return;
-  const int64_t base = (int64_t)s * g.N;
-  const int64_t j = (int64_t)y * g.nx + x, i = base + j;
-  const T lam = ldg(lam_ey + i);
-  coeff_grad_cell(ga, i, lam);
-  const T q = (g.cb_b ? ldg(cb + i) : ldg(cb + j)) * lam;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R + P;
+  const int ye = g.ny - P + 1;
+  if (x >= g.nx - P + 1 || y0 >= ye) return;
+  const int64_t base = (int64_t)blockIdx.z * g.N;
   const bool px = x < g.pml_x0 || x >= g.pml_x1;
-  const bool py = y < g.pml_y0 || y >= g.pml_y1;
-  m_hz_x_n[i] = px ? ldg(g.bx + x) * ldg(m_hz_x + i) + q : (T)0;
-  m_hx_z_n[i] = py ? ldg(g.by + y) * ldg(m_hx_z + i) - q : (T)0;
-  T ax_ = (T)FD<ST>::c(0) * (raw_x<T, ST>(g, cb, lam_ey, m_hz_x, base, y, x) -
-                            raw_x<T, ST>(g, cb, lam_ey, m_hz_x, base, y, x + 1));
+  // raw_y on rows y0-P+1 .. y0+R-1+P, raw_x on columns x-P+1 .. x+P per row.
+  T ry[R + 2 * P - 1];
 #pragma unroll
-  for (int m = 1; m < P; ++m)
-    ax_ = ax_ + (T)FD<ST>::c(m) * (raw_x<T, ST>(g, cb, lam_ey, m_hz_x, base, y, x - m) -
-                                   raw_x<T, ST>(g, cb, lam_ey, m_hz_x, base, y, x + 1 + m));
-  lam_hz[i] = lam_hz[i] + ax_ * g.rdx;
-  T ay_ = (T)FD<ST>::c(0) * (raw_y<T, ST>(g, cb, lam_ey, m_hx_z, base, y, x) -
-                            raw_y<T, ST>(g, cb, lam_ey, m_hx_z, base, y + 1, x));
+  for (int k = 0; k < R + 2 * P - 1; ++k)
+    ry[k] = raw_y<T, ST>(g, cb, lam_ey, m_hx_z, base, y0 - P + 1 + k, x);
+  T rx[R][2 * P];
+  T lhx[R], lhz[R], qv[R];
 #pragma unroll
-  for (int m = 1; m < P; ++m)
-    ay_ = ay_ + (T)FD<ST>::c(m) * (raw_y<T, ST>(g, cb, lam_ey, m_hx_z, base, y - m, x) -
-                                   raw_y<T, ST>(g, cb, lam_ey, m_hx_z, base, y + 1 + m, x));
-  lam_hx[i] = lam_hx[i] + ay_ * g.rdy;
-}
-
-// Coefficient gradient alone, for the earliest step of a backward call.
-template <typename T, int ST, typename S>
-__global__ void __launch_bounds__(256)
-k_coeff_grad(TMGeom<T> g, const T *__restrict__ lam_ey, GradArgs<T, S> ga) {
-  constexpr int P = FD<ST>::P;
-  const int x = blockIdx.x * kTileX + threadIdx.x + P;
-  const int y = blockIdx.y * kTileY + threadIdx.y + P;
-  const int s = blockIdx.z;
-  if (x >= g.nx - P + 1 || y >= g.ny - P + 1) return;
-  const int64_t i = (int64_t)s * g.N + (int64_t)y * g.nx + x;
-  coeff_grad_cell(ga, i, ldg(lam_ey + i));
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+#pragma unroll
+    for (int k = 0; k < 2 * P; ++k) rx[r][k] = raw_x<T, ST>(g, cb, lam_ey, m_hz_x, base, y, x - P + 1 + k);
+    if (y < ye) {
+      const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+      qv[r] = (g.cb_b ? ldg(cb + i) : ldg(cb + j)) * ldg(lam_ey + i);
+      lhx[r] = lam_hx[i];
+      lhz[r] = lam_hz[i];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (y >= ye) continue;
+    const int64_t i = base + (int64_t)y * g.nx + x;
+    if (px) m_hz_x_n[i] = ldg(g.bx + x) * ldg(m_hz_x + i) + qv[r];
+    if (y < g.pml_y0 || y >= g.pml_y1) m_hx_z_n[i] = ldg(g.by + y) * ldg(m_hx_z + i) - qv[r];
+    // diff_x1_adj: sum_m c_m (raw(x-m) - raw(x+1+m)); rx[r][k] holds raw(x-P+1+k)
+    T ax_ = (T)FD<ST>::c(0) * (rx[r][P - 1] - rx[r][P]);
+#pragma unroll
+    for (int m = 1; m < P; ++m) ax_ = ax_ + (T)FD<ST>::c(m) * (rx[r][P - 1 - m] - rx[r][P + m]);
+    lam_hz[i] = lhz[r] + ax_ * g.rdx;
+    // diff_y1_adj: sum_m c_m (raw(y-m) - raw(y+1+m)); ry[k] holds raw(y0-P+1+k)
+    T ay_ = (T)FD<ST>::c(0) * (ry[r + P - 1] - ry[r + P]);
+#pragma unroll
+    for (int m = 1; m < P; ++m) ay_ = ay_ + (T)FD<ST>::c(m) * (ry[r + P - 1 - m] - ry[r + P + m]);
+    lam_hx[i] = lhx[r] + ay_ * g.rdy;
+  }
 }
 
 // ---------------------------------------------------------------------------
-// Exact adjoint, H-phase (maxwell_tm_cuda_inst.cu:1082-1165), with the
-// adjoint-source injection at receivers and the source-gradient recording
-// (maxwell.cu:107-161) fused as a per-cell epilogue.
+// Exact adjoint, H-phase (maxwell_tm_cuda_inst.cu:1082-1165), fused with the
+// adjoint-source injection at receivers, the source-gradient recording
+// (maxwell.cu:107-161) and the coefficient gradient of this step
+// (maxwell_tm_cuda_inst.cu:834-871): the final adjoint of step t is in a
+// register when the cell is written, so grad_ca += lam * Ey^t * k and
+// grad_cb += lam * curlH^t * k are taken there.  Each thread loops over all
+// shots of the call and sums their image terms before one read-modify-write
+// of the model-shaped gradient (batched models keep one gradient per shot).
 template <typename T, int ST>
 __device__ __forceinline__ T raw_eyz(const TMGeom<T> &g, const T *cq, const T *lhx, const T *m,
                                      int64_t base, int y, int x) {
@@ -377,67 +428,103 @@ __device__ __forceinline__ T raw_eyx(const TMGeom<T> &g, const T *cq, const T *l
   return ldg(g.axh + x) * mn + adj / ldg(g.kxh + x);
 }
 
-template <typename T, int ST>
+template <typename T, typename S> struct GradArgs {
+  const S *ey_st;  // snapshot Ey^t of the step being imaged (nullptr: skip)
+  const S *cu_st;  // snapshot curl H^t
+  T *grad_ca;      // [ny, nx], or [n_shots, ny, nx] when `batched`
+  T *grad_cb;
+  T kscale;        // gradient sampling interval as T
+  bool batched_ca, batched_cb;
+};
+
+template <typename T, int ST, typename S>
 __global__ void __launch_bounds__(256)
 k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
         const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
         const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
         T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src, const T *__restrict__ gr_t,
-        T *__restrict__ gf_t) {
+        T *__restrict__ gf_t, GradArgs<T, S> ga) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y = blockIdx.y * kTileY + threadIdx.y;
-  const int s = blockIdx.z;
-  const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  const bool pts = !point_tile_empty(src, rec, tile);
+  const int y = blockIdx.y * kBlockY + threadIdx.y;
   if (x >= g.nx || y >= g.ny) return;
   const bool dom = x >= P && y >= P && x < g.nx - P + 1 && y < g.ny - P + 1;
-  if (!dom && !pts) return;
-  const int64_t base = (int64_t)s * g.N;
-  const int64_t j = (int64_t)y * g.nx + x, i = base + j;
-  T lam = lam_ey[i];
+  const int64_t j = (int64_t)y * g.nx + x;
+  const int tile_xy = blockIdx.y * gridDim.x + blockIdx.x;
+  const int tiles_per_shot = gridDim.x * gridDim.y;
+  const bool py = y < g.pml_y0 || y >= g.pml_y1h;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1h;
+  const bool wz = dom && y < g.ny - P && py;
+  const bool wx = dom && x < g.nx - P && px;
+  T cav = 0, cqv = 0;
   if (dom) {
-    const T cqv = g.cq_b ? ldg(cq + i) : ldg(cq + j);
-    const bool py = y < g.pml_y0 || y >= g.pml_y1h;
-    const bool px = x < g.pml_x0 || x >= g.pml_x1h;
-    const T adj_y = -cqv * ldg(lam_hx + i);
-    const T adj_x = cqv * ldg(lam_hz + i);
-    m_ey_z_n[i] = (y < g.ny - P && py) ? ldg(g.byh + y) * ldg(m_ey_z + i) + adj_y : (T)0;
-    m_ey_x_n[i] = (x < g.nx - P && px) ? ldg(g.bxh + x) * ldg(m_ey_x + i) + adj_x : (T)0;
-    const T cav = g.ca_b ? ldg(ca + i) : ldg(ca + j);
-    lam = cav * lam;
-    T dz = (T)FD<ST>::c(0) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1, x) -
-                             raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y, x));
-#pragma unroll
-    for (int m = 1; m < P; ++m)
-      dz = dz + (T)FD<ST>::c(m) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1 - m, x) -
-                                   raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y + m, x));
-    T dx = (T)FD<ST>::c(0) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1) -
-                             raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x));
-#pragma unroll
-    for (int m = 1; m < P; ++m)
-      dx = dx + (T)FD<ST>::c(m) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1 - m) -
-                                   raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x + m));
-    lam = lam + (dz * g.rdy + dx * g.rdx);
+    cav = g.ca_b ? (T)0 : ldg(ca + j);
+    cqv = g.cq_b ? (T)0 : ldg(cq + j);
   }
-  if (pts) lam = point_accumulate(rec, tile, (int)j, gr_t, lam);
-  lam_ey[i] = lam;
-  if (pts) point_record(src, tile, (int)j, gf_t, lam);
+  const bool do_grad = dom && (ga.ey_st != nullptr || ga.cu_st != nullptr);
+  T sum_ca = (T)0, sum_cb = (T)0;
+  for (int s = 0; s < g.n_shots; ++s) {
+    const int64_t base = (int64_t)s * g.N, i = base + j;
+    const int tile = s * tiles_per_shot + tile_xy;
+    const bool pts = !point_tile_empty(src, rec, tile);
+    if (!dom && !pts) continue;
+    T lam = lam_ey[i];
+    if (dom) {
+      const T cqs = g.cq_b ? ldg(cq + i) : cqv;
+      const T cas = g.ca_b ? ldg(ca + i) : cav;
+      const T adj_y = -cqs * ldg(lam_hx + i);
+      const T adj_x = cqs * ldg(lam_hz + i);
+      if (wz) m_ey_z_n[i] = ldg(g.byh + y) * ldg(m_ey_z + i) + adj_y;
+      if (wx) m_ey_x_n[i] = ldg(g.bxh + x) * ldg(m_ey_x + i) + adj_x;
+      lam = cas * lam;
+      T dz = (T)FD<ST>::c(0) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1, x) -
+                               raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y, x));
+#pragma unroll
+      for (int m = 1; m < P; ++m)
+        dz = dz + (T)FD<ST>::c(m) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1 - m, x) -
+                                     raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y + m, x));
+      T dx = (T)FD<ST>::c(0) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1) -
+                               raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x));
+#pragma unroll
+      for (int m = 1; m < P; ++m)
+        dx = dx + (T)FD<ST>::c(m) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1 - m) -
+                                     raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x + m));
+      lam = lam + (dz * g.rdy + dx * g.rdx);
+    }
+    if (pts) lam = point_accumulate(rec, tile, (int)j, gr_t, lam);
+    lam_ey[i] = lam;
+    if (pts) point_record(src, tile, (int)j, gf_t, lam);
+    if (do_grad) {
+      if (ga.ey_st) {
+        const T t = lam * Codec<S, T>::dec(load_stream(ga.ey_st + i)) * ga.kscale;
+        if (ga.batched_ca) ga.grad_ca[i] = ga.grad_ca[i] + t;
+        else sum_ca = sum_ca + t;
+      }
+      if (ga.cu_st) {
+        const T t = lam * Codec<S, T>::dec(load_stream(ga.cu_st + i)) * ga.kscale;
+        if (ga.batched_cb) ga.grad_cb[i] = ga.grad_cb[i] + t;
+        else sum_cb = sum_cb + t;
+      }
+    }
+  }
+  if (do_grad) {
+    if (ga.ey_st && !ga.batched_ca) ga.grad_ca[j] = ga.grad_ca[j] + sum_ca;
+    if (ga.cu_st && !ga.batched_cb) ga.grad_cb[j] = ga.grad_cb[j] + sum_cb;
+  }
 }
 
-// Shot reduction of the per-shot accumulators (maxwell_tm_inst.cpp:2185-2206):
-// grad[j] += sum over shots, summed in shot order.
-template <typename T, int ST>
-__global__ void __launch_bounds__(256)
-k_combine(TMGeom<T> g, T *__restrict__ grad, const T *__restrict__ acc) {
-  constexpr int P = FD<ST>::P;
-  const int x = blockIdx.x * kTileX + threadIdx.x + P;
-  const int y = blockIdx.y * kTileY + threadIdx.y + P;
-  if (x >= g.nx - P + 1 || y >= g.ny - P + 1) return;
-  const int64_t j = (int64_t)y * g.nx + x;
-  T sum = (T)0;
-  for (int s = 0; s < g.n_shots; ++s) sum = sum + ldg(acc + (int64_t)s * g.N + j);
-  grad[j] = grad[j] + sum;
+// Clears a CPML memory array outside its absorbing strips along one axis
+// (axis 0: rows [lo, hi) are cleared; axis 1: columns [lo, hi)).
+template <typename T>
+__global__ void k_zero_band(T *__restrict__ m, int n_shots, int ny, int nx, int axis, int lo,
+                            int hi) {
+  const int64_t n = (int64_t)n_shots * ny * nx;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = k % ((int64_t)ny * nx);
+    const int v = axis == 0 ? (int)(c / nx) : (int)(c % nx);
+    if (v >= lo && v < hi) m[k] = (T)0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -445,13 +532,13 @@ k_combine(TMGeom<T> g, T *__restrict__ grad, const T *__restrict__ acc) {
 // skipped as in the reference; an index at or beyond ny*nx sets the device
 // error word and is skipped instead of writing out of bounds.
 __device__ __forceinline__ int point_tile_of(int64_t idx, int s, int nx, int tiles_x,
-                                             int tiles_y) {
+                                             int tiles_y, int tile_h) {
   const int y = (int)(idx / nx), x = (int)(idx % nx);
-  return (s * tiles_y + y / kTileY) * tiles_x + x / kTileX;
+  return (s * tiles_y + y / tile_h) * tiles_x + x / kTileX;
 }
 
 __global__ void k_points_count(const int64_t *__restrict__ idx, int n_per_shot, int n_shots,
-                               int64_t N, int nx, int tiles_x, int tiles_y,
+                               int64_t N, int nx, int tiles_x, int tiles_y, int tile_h,
                                int *__restrict__ count) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_per_shot * n_shots) return;
@@ -461,7 +548,7 @@ __global__ void k_points_count(const int64_t *__restrict__ idx, int n_per_shot, 
     atomicOr(&g_tide_dev_err, 1);
     return;
   }
-  atomicAdd(count + point_tile_of(v, e / n_per_shot, nx, tiles_x, tiles_y), 1);
+  atomicAdd(count + point_tile_of(v, e / n_per_shot, nx, tiles_x, tiles_y, tile_h), 1);
 }
 
 // Exclusive scan of count[0..n) into start[0..n] by one block of 1024 threads.
@@ -492,7 +579,7 @@ __global__ void __launch_bounds__(1024) k_points_scan(const int *__restrict__ co
 // Place each entry at start[tile] + (its rank among earlier entries of the
 // same shot and tile), so every tile lists its entries in ascending order.
 __global__ void k_points_fill(const int64_t *__restrict__ idx, int n_per_shot, int n_shots,
-                              int64_t N, int nx, int tiles_x, int tiles_y,
+                              int64_t N, int nx, int tiles_x, int tiles_y, int tile_h,
                               const int *__restrict__ start, int *__restrict__ cell,
                               int *__restrict__ ent) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -500,11 +587,11 @@ __global__ void k_points_fill(const int64_t *__restrict__ idx, int n_per_shot, i
   const int64_t v = idx[e];
   if (v < 0 || v >= N) return;
   const int s = e / n_per_shot;
-  const int tile = point_tile_of(v, s, nx, tiles_x, tiles_y);
+  const int tile = point_tile_of(v, s, nx, tiles_x, tiles_y, tile_h);
   int rank = 0;
   for (int e2 = s * n_per_shot; e2 < e; ++e2) {
     const int64_t v2 = idx[e2];
-    if (v2 >= 0 && v2 < N && point_tile_of(v2, s, nx, tiles_x, tiles_y) == tile) ++rank;
+    if (v2 >= 0 && v2 < N && point_tile_of(v2, s, nx, tiles_x, tiles_y, tile_h) == tile) ++rank;
   }
   const int pos = start[tile] + rank;
   cell[pos] = (int)v;
