@@ -285,12 +285,12 @@ def run_b200(args) -> None:
 
     clocks = ClockSampler(dev.index or 0)
     clocks.start()
-    L.tide_b200_profile_enable(1, 8)
+    L.tide_b200_profile_enable(1, 32)
     read_profile(L)
     launches0 = L.tide_b200_launch_count()
     ms, _, _ = timed(args.steps, copy_in=False)
     launches = L.tide_b200_launch_count() - launches0
-    L.tide_b200_profile_enable(0, 8)
+    L.tide_b200_profile_enable(0, 32)
     prof = read_profile(L)
     clk = clocks.stop()
     e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)

@@ -132,7 +132,8 @@ int tide_b200_device_status(int64_t device);
 /* Kernel timing for benchmarks (new; no reference counterpart).  When
  * enabled, every `sample_every`-th time step of each call brackets its stencil
  * kernels with CUDA events on the launching stream; durations accumulate per
- * kernel kind until read.  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h. */
+ * kernel kind until read (reading waits for the recorded events; profiled
+ * calls themselves never block).  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h. */
 void tide_b200_profile_enable(int on, int sample_every);
 int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds);
 const char *tide_b200_profile_kind_name(int kind);

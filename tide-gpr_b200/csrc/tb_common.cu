@@ -102,21 +102,38 @@ void ProfileScope::end(int kind) {
   open_kind_ = -1;
 }
 
+// Event pairs of closed scopes wait here until tide_b200_profile_read, so a
+// profiled call never blocks the host.
+std::mutex g_pending_mu;
+std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, int>> g_pending;
+
 ProfileScope::~ProfileScope() {
   if (!on_) return;
-  double ms[kKindCount] = {};
-  int64_t cnt[kKindCount] = {};
-  if (n_ > 0) cudaEventSynchronize(pairs_[n_ - 1].b);
-  for (int i = 0; i < n_; ++i) {
-    float t = 0.f;
-    if (cudaEventElapsedTime(&t, pairs_[i].a, pairs_[i].b) == cudaSuccess) {
-      ms[pairs_[i].kind] += t;
-      cnt[pairs_[i].kind] += 1;
-    }
-    give_event(pairs_[i].a);
-    give_event(pairs_[i].b);
+  {
+    std::lock_guard<std::mutex> lk(g_pending_mu);
+    for (int i = 0; i < n_; ++i) g_pending.push_back({{pairs_[i].a, pairs_[i].b}, pairs_[i].kind});
   }
   free(pairs_);
+}
+
+void resolve_pending() {
+  std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, int>> pend;
+  {
+    std::lock_guard<std::mutex> lk(g_pending_mu);
+    pend.swap(g_pending);
+  }
+  double ms[kKindCount] = {};
+  int64_t cnt[kKindCount] = {};
+  for (auto &p : pend) {
+    float t = 0.f;
+    if (cudaEventSynchronize(p.first.second) == cudaSuccess &&
+        cudaEventElapsedTime(&t, p.first.first, p.first.second) == cudaSuccess) {
+      ms[p.second] += t;
+      cnt[p.second] += 1;
+    }
+    give_event(p.first.first);
+    give_event(p.first.second);
+  }
   std::lock_guard<std::mutex> lk(g_prof_mu);
   for (int k = 0; k < kKindCount; ++k) {
     g_prof_ms[k] += ms[k];
@@ -134,6 +151,7 @@ void tide_b200_profile_enable(int on, int sample_every) {
 }
 
 int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds) {
+  tb::resolve_pending();
   std::lock_guard<std::mutex> lk(tb::g_prof_mu);
   int n = max_kinds < tb::kKindCount ? max_kinds : tb::kKindCount;
   for (int k = 0; k < n; ++k) {

@@ -13,6 +13,7 @@
 #include "../../include/tide_b200.h"
 #include "tb_common.cuh"
 #include "tm2d_kernels.cuh"
+#include "tm2d_s2.cuh"
 
 namespace tb {
 namespace {
@@ -23,9 +24,10 @@ constexpr int kRing = 3;  // device ring slots of the cpu storage mode
 inline cudaStream_t as_stream(void *h) { return reinterpret_cast<cudaStream_t>(h); }
 
 // Rows per thread of each stencil kernel (see tm2d_kernels.cuh).
-constexpr int kRowsH = 4;   // forward H
+constexpr int kRowsH = 1;   // forward H
 constexpr int kRowsE = 2;   // forward E (+ storage, points)
 constexpr int kRowsAE = 2;  // adjoint E
+constexpr int kRowsAH = 1;  // adjoint H (+ points, gradient)
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)std::max<int64_t>(1, (a + b - 1) / b); }
 
@@ -72,7 +74,7 @@ bool make_launch(Launch<T, ST> &L, const T *ay, const T *by, const T *ayh, const
   L.grid_ae = dim3(cdiv(dx, kTileX), cdiv(dy, kBlockY * kRowsAE), S);
   L.tiles_x = (int)cdiv(nx, kTileX);
   L.tiles_y_e = (int)cdiv(ny, kBlockY * kRowsE);
-  L.tiles_y_ah = (int)cdiv(ny, kBlockY);
+  L.tiles_y_ah = (int)cdiv(ny, kBlockY * kRowsAH);
   L.grid_e = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_e, S);
   L.grid_ah = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_ah, 1);
   return true;
@@ -157,13 +159,55 @@ struct EventRing {
 };
 
 // ---------------------------------------------------------------------------
+// Stencil order 2 runs the single-path kernels of tm2d_s2.cuh (Debye media use
+// the generic E kernel); higher orders run the generic kernels.
 template <typename T, int ST, typename S>
 inline void launch_fwd_e(const Launch<T, ST> &L, cudaStream_t st, const T *ca, const T *cb,
                          const T *hx, const T *hz, T *ey, T *m_hx_z, T *m_hz_x, S *e_st,
                          S *c_st, const DebyeArgs<T> &db, const PointScratch &ps, const T *ft,
                          T *rt) {
-  k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
-                                                          e_st, c_st, db, ps.src, ps.rec, ft, rt);
+  if (ST == 2 && db.n_poles == 0)
+    k2_fwd_e<T, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
+                                                         e_st, c_st, ps.src, ps.rec, ft, rt);
+  else
+    k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z,
+                                                            m_hz_x, e_st, c_st, db, ps.src,
+                                                            ps.rec, ft, rt);
+}
+
+template <typename T, int ST>
+inline void launch_fwd_h(const Launch<T, ST> &L, cudaStream_t st, const T *cq, const T *ey,
+                         T *hx, T *hz, T *m_ey_x, T *m_ey_z) {
+  if (ST == 2)
+    k2_fwd_h<T, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+  else
+    k_fwd_h<T, ST, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+}
+
+template <typename T, int ST>
+inline void launch_adj_e(const Launch<T, ST> &L, cudaStream_t st, const T *cb, const T *lam,
+                         T *lhx, T *lhz, const T *mz, const T *mx, T *mz_n, T *mx_n) {
+  if (ST == 2)
+    k2_adj_e<T, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(L.g, cb, lam, lhx, lhz, mz, mx, mz_n,
+                                                        mx_n);
+  else
+    k_adj_e<T, ST, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(L.g, cb, lam, lhx, lhz, mz, mx, mz_n,
+                                                           mx_n);
+}
+
+template <typename T, int ST, typename S>
+inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, const T *cq,
+                         const T *lhx, const T *lhz, T *ley, const T *mex, const T *mez,
+                         T *mex_n, T *mez_n, const PointScratch &ps, const T *grt, T *gft,
+                         const GradArgs<T, S> &ga) {
+  if (ST == 2)
+    k2_adj_h<T, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex, mez,
+                                                           mex_n, mez_n, ps.rec, ps.src, grt, gft,
+                                                           ga);
+  else
+    k_adj_h<T, ST, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex,
+                                                              mez, mex_n, mez_n, ps.rec, ps.src,
+                                                              grt, gft, ga);
 }
 
 template <typename T, int ST>
@@ -197,7 +241,7 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
     const bool smp = prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
-      k_fwd_h<T, ST, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
       if (smp) prof.end(kKFwdH);
     }
     if (smp) prof.begin(kKFwdE);
@@ -275,7 +319,7 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     }
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
-      k_fwd_h<T, ST, kRowsH><<<L.grid_h, L.block, 0, st>>>(L.g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
       if (smp) prof.end(kKFwdH);
     }
     const T *ft = f ? f + t * fs : nullptr;
@@ -362,7 +406,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
       !zero_band(m_lambda_ey_z, L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, L.tiles_y_ah, kBlockY, sources_i, n_sources_per_shot, receivers_i,
+  if (!build_points(ps, L, L.tiles_y_ah, kBlockY * kRowsAH, sources_i, n_sources_per_shot, receivers_i,
                     n_receivers_per_shot, st))
     return;
 
@@ -416,8 +460,8 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     const bool smp = prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKAdjE);
-      k_adj_e<T, ST, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(
-          L.g, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x, nxt_hx_z, nxt_hz_x);
+      launch_adj_e<T, ST>(L, st, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x,
+                          nxt_hx_z, nxt_hz_x);
       if (smp) prof.end(kKAdjE);
     }
     std::swap(cur_hx_z, nxt_hx_z);
@@ -437,15 +481,14 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (bf16) {
       GradArgs<T, __nv_bfloat16> ga{(const __nv_bfloat16 *)es, (const __nv_bfloat16 *)cs,
                                     grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched};
-      k_adj_h<T, ST, __nv_bfloat16><<<L.grid_ah, L.block, 0, st>>>(
-          L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
-          ps.rec, ps.src, grt, gft, ga);
+      launch_adj_h<T, ST, __nv_bfloat16>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey,
+                                         cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft,
+                                         ga);
     } else {
       GradArgs<T, T> ga{(const T *)es, (const T *)cs, grad_ca, grad_cb, (T)step_ratio,
                         ca_batched, cb_batched};
-      k_adj_h<T, ST, T><<<L.grid_ah, L.block, 0, st>>>(
-          L.g, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z,
-          ps.rec, ps.src, grt, gft, ga);
+      launch_adj_h<T, ST, T>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x,
+                             cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft, ga);
     }
     if (smp) prof.end(kKAdjH);
     std::swap(cur_ey_x, nxt_ey_x);

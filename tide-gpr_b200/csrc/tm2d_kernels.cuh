@@ -158,6 +158,46 @@ __device__ __forceinline__ bool point_tile_empty(const PointCSR &a, const PointC
 // kernels; one cell per thread left the SMs waiting on L1/L2).
 constexpr int kBlockY = 8;
 
+// ---------------------------------------------------------------------------
+// Interior fast paths (stencil order 2).  A CTA whose cells and stencil
+// neighbours all lie outside the CPML strips (and so away from the domain
+// edges) needs none of the strip logic; most of the grid is such tiles.  They
+// take a branch-free path: 32-bit offsets from the shot's base pointer,
+// x-neighbours exchanged with warp shuffles (blockDim.x == 32, so threadIdx.x
+// is the lane), y-neighbours reused from registers.  Every value is computed
+// with the same operations in the same order as the general path, so both
+// paths give bit-identical results.  Offsets fit in int32: the host rejects
+// grids with ny * nx >= 2^31.
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T, int R>
+__device__ __forceinline__ void fwd_h_fast(const TMGeom<T> &g, const T *__restrict__ cq,
+                                           const T *__restrict__ ey, T *__restrict__ hx,
+                                           T *__restrict__ hz, int x, int y0) {
+  const int nx = g.nx, j0 = y0 * nx + x;
+  T e[R + 1], c[R], vx[R], vz[R], er[R];
+#pragma unroll
+  for (int r = 0; r <= R; ++r) e[r] = ldg(ey + j0 + r * nx);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    c[r] = ldg(cq + j0 + r * nx);
+    vx[r] = hx[j0 + r * nx];
+    vz[r] = hz[j0 + r * nx];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    er[r] = __shfl_down_sync(kFull, e[r], 1);
+    if (threadIdx.x == 31) er[r] = ldg(ey + j0 + r * nx + 1);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const T dz = (e[r + 1] - e[r]) * g.rdy;
+    const T dx = (er[r] - e[r]) * g.rdx;
+    hx[j0 + r * nx] = vx[r] - c[r] * dz;
+    hz[j0 + r * nx] = vz[r] + c[r] * dx;
+  }
+}
+
 // Forward H half-step (maxwell_tm_core.cuh:448-502).  Grid: x over the update
 // domain [P, nx-P+1), y over row groups, z = shot.
 template <typename T, int ST, int R>
@@ -167,9 +207,18 @@ k_fwd_h(TMGeom<T> g, const T *__restrict__ cq, const T *__restrict__ ey, T *__re
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x + P;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R + P;
+  const int64_t base = (int64_t)blockIdx.z * g.N;
+  if constexpr (ST == 2) {
+    // Interior tile: no strip cell for Hx or Hz (block-uniform test).
+    const int tx0 = blockIdx.x * kTileX + P, ty0 = blockIdx.y * kBlockY * R + P;
+    if (tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1h && ty0 >= g.pml_y0 &&
+        ty0 + kBlockY * R <= g.pml_y1h) {
+      fwd_h_fast<T, R>(g, g.cq_b ? cq + base : cq, ey + base, hx + base, hz + base, x, y0);
+      return;
+    }
+  }
   const int ye = g.ny - P + 1;
   if (x >= g.nx - P + 1 || y0 >= ye) return;
-  const int64_t base = (int64_t)blockIdx.z * g.N;
   const bool do_hz = x < g.nx - P;
   const bool px = x < g.pml_x0 || x >= g.pml_x1h;
   T cqv[R], dz[R], dx[R], hxv[R], hzv[R];
@@ -232,6 +281,47 @@ template <> __device__ __forceinline__ __nv_bfloat16 load_stream<__nv_bfloat16>(
   return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short *>(p)));
 }
 
+// Forward E half-step, interior tile (no strip cell, no Debye); points of the
+// tile are applied per cell exactly as in the general path.
+template <typename T, typename S, int R>
+__device__ __forceinline__ void fwd_e_fast(const TMGeom<T> &g, const T *__restrict__ ca,
+                                           const T *__restrict__ cb, const T *__restrict__ hx,
+                                           const T *__restrict__ hz, T *__restrict__ ey,
+                                           S *__restrict__ est, S *__restrict__ cst, bool pts,
+                                           const PointCSR &src, const PointCSR &rec, int tile,
+                                           const T *__restrict__ f_t, T *__restrict__ r_t, int x,
+                                           int y0) {
+  const int nx = g.nx, j0 = y0 * nx + x;
+  T vx[R + 1], vz[R], vzl[R], eo[R], a[R], b[R];
+#pragma unroll
+  for (int r = 0; r <= R; ++r) vx[r] = ldg(hx + j0 + (r - 1) * nx);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    vz[r] = ldg(hz + j0 + r * nx);
+    eo[r] = ey[j0 + r * nx];
+    a[r] = ldg(ca + j0 + r * nx);
+    b[r] = ldg(cb + j0 + r * nx);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    vzl[r] = __shfl_up_sync(kFull, vz[r], 1);
+    if (threadIdx.x == 0) vzl[r] = ldg(hz + j0 + r * nx - 1);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 + r * nx;
+    const T dz = (vz[r] - vzl[r]) * g.rdx;
+    const T dy = (vx[r + 1] - vx[r]) * g.rdy;
+    const T curl = dz - dy;
+    if (est) store_stream(est + j, Codec<S, T>::enc(eo[r]));
+    if (cst) store_stream(cst + j, Codec<S, T>::enc(curl));
+    T e = a[r] * eo[r] + b[r] * curl;
+    if (pts) e = point_accumulate(src, tile, j, f_t, e);
+    ey[j] = e;
+    if (pts) point_record(rec, tile, j, r_t, e);
+  }
+}
+
 // Forward E half-step with optional snapshot storage, Debye polarisation,
 // source injection and receiver recording
 // (maxwell_tm_core.cuh:504-599, maxwell_tm_cuda_inst.cu:382-457,
@@ -250,8 +340,19 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
   const int s = blockIdx.z;
   const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   const bool pts = !point_tile_empty(src, rec, tile);
-  if (x >= g.nx || y0 >= g.ny) return;
   const int64_t base = (int64_t)s * g.N;
+  if constexpr (ST == 2) {
+    const int tx0 = blockIdx.x * kTileX, ty0 = blockIdx.y * kBlockY * R;
+    if (db.n_poles == 0 && tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1 && ty0 >= g.pml_y0 &&
+        ty0 + kBlockY * R <= g.pml_y1) {
+      fwd_e_fast<T, S, R>(g, g.ca_b ? ca + base : ca, g.cb_b ? cb + base : cb, hx + base,
+                          hz + base, ey + base, ey_store ? ey_store + base : nullptr,
+                          curl_store ? curl_store + base : nullptr, pts, src, rec, tile, f_t,
+                          r_t, x, y0);
+      return;
+    }
+  }
+  if (x >= g.nx || y0 >= g.ny) return;
   const bool xdom = x >= P && x < g.nx - P + 1;
   const bool px = x < g.pml_x0 || x >= g.pml_x1;
   T eo[R], en[R], dhz[R], dhx[R], cav[R], cbv[R];
@@ -345,6 +446,35 @@ __device__ __forceinline__ T raw_y(const TMGeom<T> &g, const T *cb, const T *lam
   return ldg(g.ay + y) * mn - q / ldg(g.ky + y);
 }
 
+// Adjoint E-phase, interior tile: raw_x = q and raw_y = -q with q = cb * lam,
+// no memory adjoint in the strips of these cells or their neighbours.
+template <typename T, int R>
+__device__ __forceinline__ void adj_e_fast(const TMGeom<T> &g, const T *__restrict__ cb,
+                                           const T *__restrict__ lam, T *__restrict__ lhx,
+                                           T *__restrict__ lhz, int x, int y0) {
+  const int nx = g.nx, j0 = y0 * nx + x;
+  T q[R + 1], qr[R], vx[R], vz[R];
+#pragma unroll
+  for (int r = 0; r <= R; ++r) q[r] = ldg(cb + j0 + r * nx) * ldg(lam + j0 + r * nx);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    vx[r] = lhx[j0 + r * nx];
+    vz[r] = lhz[j0 + r * nx];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    qr[r] = __shfl_down_sync(kFull, q[r], 1);
+    if (threadIdx.x == 31) qr[r] = ldg(cb + j0 + r * nx + 1) * ldg(lam + j0 + r * nx + 1);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const T ax_ = (T)1 * (q[r] - qr[r]);
+    lhz[j0 + r * nx] = vz[r] + ax_ * g.rdx;
+    const T ay_ = (T)1 * ((-q[r]) - (-q[r + 1]));
+    lhx[j0 + r * nx] = vx[r] + ay_ * g.rdy;
+  }
+}
+
 template <typename T, int ST, int R>
 __global__ void __launch_bounds__(256)
 k_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
@@ -353,9 +483,19 @@ k_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x + P;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R + P;
+  const int64_t base = (int64_t)blockIdx.z * g.N;
+  if constexpr (ST == 2) {
+    // Interior tile: cells and their +1 neighbours outside the strips.
+    const int tx0 = blockIdx.x * kTileX + P, ty0 = blockIdx.y * kBlockY * R + P;
+    if (tx0 >= g.pml_x0 && tx0 + kTileX < g.pml_x1 && ty0 >= g.pml_y0 &&
+        ty0 + kBlockY * R < g.pml_y1) {
+      adj_e_fast<T, R>(g, g.cb_b ? cb + base : cb, lam_ey + base, lam_hx + base, lam_hz + base,
+                       x, y0);
+      return;
+    }
+  }
   const int ye = g.ny - P + 1;
   if (x >= g.nx - P + 1 || y0 >= ye) return;
-  const int64_t base = (int64_t)blockIdx.z * g.N;
   const bool px = x < g.pml_x0 || x >= g.pml_x1;
   // raw_y on rows y0-P+1 .. y0+R-1+P, raw_x on columns x-P+1 .. x+P per row.
   T ry[R + 2 * P - 1];
@@ -437,7 +577,79 @@ template <typename T, typename S> struct GradArgs {
   bool batched_ca, batched_cb;
 };
 
-template <typename T, int ST, typename S>
+// Adjoint H-phase update of one cell (general path: strips, domain edges).
+template <typename T, int ST>
+__device__ __forceinline__ T adj_h_general(const TMGeom<T> &g, const T *__restrict__ ca,
+                                           const T *__restrict__ cq,
+                                           const T *__restrict__ lam_hx,
+                                           const T *__restrict__ lam_hz,
+                                           const T *__restrict__ m_ey_x,
+                                           const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
+                                           T *__restrict__ m_ey_z_n, int64_t base, int y, int x,
+                                           T lam) {
+  constexpr int P = FD<ST>::P;
+  const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+  const T cqs = g.cq_b ? ldg(cq + i) : ldg(cq + j);
+  const T cas = g.ca_b ? ldg(ca + i) : ldg(ca + j);
+  const bool py = y < g.pml_y0 || y >= g.pml_y1h;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1h;
+  const T adj_y = -cqs * ldg(lam_hx + i);
+  const T adj_x = cqs * ldg(lam_hz + i);
+  if (y < g.ny - P && py) m_ey_z_n[i] = ldg(g.byh + y) * ldg(m_ey_z + i) + adj_y;
+  if (x < g.nx - P && px) m_ey_x_n[i] = ldg(g.bxh + x) * ldg(m_ey_x + i) + adj_x;
+  lam = cas * lam;
+  T dz = (T)FD<ST>::c(0) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1, x) -
+                           raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y, x));
+#pragma unroll
+  for (int m = 1; m < P; ++m)
+    dz = dz + (T)FD<ST>::c(m) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1 - m, x) -
+                                 raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y + m, x));
+  T dx = (T)FD<ST>::c(0) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1) -
+                           raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x));
+#pragma unroll
+  for (int m = 1; m < P; ++m)
+    dx = dx + (T)FD<ST>::c(m) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1 - m) -
+                                 raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x + m));
+  return lam + (dz * g.rdy + dx * g.rdx);
+}
+
+// Adjoint H-phase, interior tile (stencil 2): raw_eyz = -cq * lam_hx and
+// raw_eyx = cq * lam_hz for the cells and their -1 neighbours.
+template <typename T, int R>
+__device__ __forceinline__ void adj_h_fast(const TMGeom<T> &g, const T *__restrict__ ca,
+                                           const T *__restrict__ cq,
+                                           const T *__restrict__ lhx,
+                                           const T *__restrict__ lhz, const T *__restrict__ ley,
+                                           int j0, T (&lam)[R]) {
+  const int nx = g.nx;
+  T rz[R + 1], rx[R], rxl[R], a[R];
+#pragma unroll
+  for (int r = 0; r <= R; ++r) {
+    const int j = j0 + (r - 1) * nx;
+    rz[r] = -ldg(cq + j) * ldg(lhx + j);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 + r * nx;
+    rx[r] = ldg(cq + j) * ldg(lhz + j);
+    a[r] = ldg(ca + j);
+    lam[r] = ley[j];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    rxl[r] = __shfl_up_sync(kFull, rx[r], 1);
+    if (threadIdx.x == 0) rxl[r] = ldg(cq + j0 + r * nx - 1) * ldg(lhz + j0 + r * nx - 1);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const T dz = (T)1 * (rz[r] - rz[r + 1]);
+    const T dx = (T)1 * (rxl[r] - rx[r]);
+    lam[r] = a[r] * lam[r];
+    lam[r] = lam[r] + (dz * g.rdy + dx * g.rdx);
+  }
+}
+
+template <typename T, int ST, typename S, int R>
 __global__ void __launch_bounds__(256)
 k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
         const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
@@ -446,70 +658,77 @@ k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
         T *__restrict__ gf_t, GradArgs<T, S> ga) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y = blockIdx.y * kBlockY + threadIdx.y;
-  if (x >= g.nx || y >= g.ny) return;
-  const bool dom = x >= P && y >= P && x < g.nx - P + 1 && y < g.ny - P + 1;
-  const int64_t j = (int64_t)y * g.nx + x;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int tile_xy = blockIdx.y * gridDim.x + blockIdx.x;
   const int tiles_per_shot = gridDim.x * gridDim.y;
-  const bool py = y < g.pml_y0 || y >= g.pml_y1h;
-  const bool px = x < g.pml_x0 || x >= g.pml_x1h;
-  const bool wz = dom && y < g.ny - P && py;
-  const bool wx = dom && x < g.nx - P && px;
-  T cav = 0, cqv = 0;
-  if (dom) {
-    cav = g.ca_b ? (T)0 : ldg(ca + j);
-    cqv = g.cq_b ? (T)0 : ldg(cq + j);
+  bool fast = false;
+  if constexpr (ST == 2) {
+    // Interior tile: cells and their -1 neighbours outside the strips.
+    const int tx0 = blockIdx.x * kTileX, ty0 = blockIdx.y * kBlockY * R;
+    fast = !g.ca_b && !g.cq_b && tx0 - 1 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1h &&
+           ty0 - 1 >= g.pml_y0 && ty0 + kBlockY * R <= g.pml_y1h;
   }
-  const bool do_grad = dom && (ga.ey_st != nullptr || ga.cu_st != nullptr);
-  T sum_ca = (T)0, sum_cb = (T)0;
+  if (!fast && (x >= g.nx || y0 >= g.ny)) return;
+  const bool imaging = ga.ey_st != nullptr || ga.cu_st != nullptr;
+  T sum_ca[R], sum_cb[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) sum_ca[r] = sum_cb[r] = (T)0;
+  const int j0 = y0 * g.nx + x;
   for (int s = 0; s < g.n_shots; ++s) {
-    const int64_t base = (int64_t)s * g.N, i = base + j;
+    const int64_t base = (int64_t)s * g.N;
     const int tile = s * tiles_per_shot + tile_xy;
     const bool pts = !point_tile_empty(src, rec, tile);
-    if (!dom && !pts) continue;
-    T lam = lam_ey[i];
-    if (dom) {
-      const T cqs = g.cq_b ? ldg(cq + i) : cqv;
-      const T cas = g.ca_b ? ldg(ca + i) : cav;
-      const T adj_y = -cqs * ldg(lam_hx + i);
-      const T adj_x = cqs * ldg(lam_hz + i);
-      if (wz) m_ey_z_n[i] = ldg(g.byh + y) * ldg(m_ey_z + i) + adj_y;
-      if (wx) m_ey_x_n[i] = ldg(g.bxh + x) * ldg(m_ey_x + i) + adj_x;
-      lam = cas * lam;
-      T dz = (T)FD<ST>::c(0) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1, x) -
-                               raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y, x));
+    T lam[R];
+    bool live[R], dom[R];
+    if (fast) {
+      adj_h_fast<T, R>(g, ca, cq, lam_hx + base, lam_hz + base, lam_ey + base, j0, lam);
 #pragma unroll
-      for (int m = 1; m < P; ++m)
-        dz = dz + (T)FD<ST>::c(m) * (raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y - 1 - m, x) -
-                                     raw_eyz<T, ST>(g, cq, lam_hx, m_ey_z, base, y + m, x));
-      T dx = (T)FD<ST>::c(0) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1) -
-                               raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x));
+      for (int r = 0; r < R; ++r) live[r] = dom[r] = true;
+    } else {
 #pragma unroll
-      for (int m = 1; m < P; ++m)
-        dx = dx + (T)FD<ST>::c(m) * (raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x - 1 - m) -
-                                     raw_eyx<T, ST>(g, cq, lam_hz, m_ey_x, base, y, x + m));
-      lam = lam + (dz * g.rdy + dx * g.rdx);
-    }
-    if (pts) lam = point_accumulate(rec, tile, (int)j, gr_t, lam);
-    lam_ey[i] = lam;
-    if (pts) point_record(src, tile, (int)j, gf_t, lam);
-    if (do_grad) {
-      if (ga.ey_st) {
-        const T t = lam * Codec<S, T>::dec(load_stream(ga.ey_st + i)) * ga.kscale;
-        if (ga.batched_ca) ga.grad_ca[i] = ga.grad_ca[i] + t;
-        else sum_ca = sum_ca + t;
+      for (int r = 0; r < R; ++r) {
+        const int y = y0 + r;
+        dom[r] = x >= P && y >= P && x < g.nx - P + 1 && y < g.ny - P + 1;
+        live[r] = y < g.ny && (dom[r] || pts);
+        if (!live[r]) continue;
+        lam[r] = lam_ey[base + (int64_t)y * g.nx + x];
+        if (dom[r])
+          lam[r] = adj_h_general<T, ST>(g, ca, cq, lam_hx, lam_hz, m_ey_x, m_ey_z, m_ey_x_n,
+                                        m_ey_z_n, base, y, x, lam[r]);
       }
-      if (ga.cu_st) {
-        const T t = lam * Codec<S, T>::dec(load_stream(ga.cu_st + i)) * ga.kscale;
-        if (ga.batched_cb) ga.grad_cb[i] = ga.grad_cb[i] + t;
-        else sum_cb = sum_cb + t;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (!live[r]) continue;
+      const int j = j0 + r * g.nx;
+      const int64_t i = base + j;
+      T v = lam[r];
+      if (pts) v = point_accumulate(rec, tile, j, gr_t, v);
+      lam_ey[i] = v;
+      if (pts) point_record(src, tile, j, gf_t, v);
+      if (imaging && dom[r]) {
+        if (ga.ey_st) {
+          const T t = v * Codec<S, T>::dec(load_stream(ga.ey_st + i)) * ga.kscale;
+          if (ga.batched_ca) ga.grad_ca[i] = ga.grad_ca[i] + t;
+          else sum_ca[r] = sum_ca[r] + t;
+        }
+        if (ga.cu_st) {
+          const T t = v * Codec<S, T>::dec(load_stream(ga.cu_st + i)) * ga.kscale;
+          if (ga.batched_cb) ga.grad_cb[i] = ga.grad_cb[i] + t;
+          else sum_cb[r] = sum_cb[r] + t;
+        }
       }
     }
   }
-  if (do_grad) {
-    if (ga.ey_st && !ga.batched_ca) ga.grad_ca[j] = ga.grad_ca[j] + sum_ca;
-    if (ga.cu_st && !ga.batched_cb) ga.grad_cb[j] = ga.grad_cb[j] + sum_cb;
+  if (!imaging) return;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    const bool dom = x >= P && y >= P && x < g.nx - P + 1 && y < g.ny - P + 1;
+    if (!dom) continue;
+    const int j = j0 + r * g.nx;
+    if (ga.ey_st && !ga.batched_ca) ga.grad_ca[j] = ga.grad_ca[j] + sum_ca[r];
+    if (ga.cu_st && !ga.batched_cb) ga.grad_cb[j] = ga.grad_cb[j] + sum_cb[r];
   }
 }
 
