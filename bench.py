@@ -173,21 +173,28 @@ def read_profile(L) -> dict:
 # Algorithmic bytes per cell (one shot, one step) of each stencil kernel,
 # single sweep: fields each read/written once, model coefficients once per
 # launch (shared by the S shots of a launch), CPML memories only in their
-# strips, snapshot bytes where the kernel stores or reads them.
+# strips (read + write), snapshot bytes where the kernel stores or reads them,
+# and the model-shaped gradient read-modify-write once per launch.
 def kernel_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho_x: float, rho_y: float) -> float:
     f = 4.0
-    if kind == "fwd_h":  # read Ey; RMW Hx, Hz; cq; RMW m_ey_x, m_ey_z in strips
-        return 5 * f + f / S + 2 * f * (rho_x + rho_y)
-    if kind == "fwd_e":  # read Hx, Hz; RMW Ey; ca, cb; RMW m_hx_z, m_hz_x; store Ey, curl
-        return 5 * f + 2 * f / S + 2 * f * (rho_x + rho_y) + 2 * snap_bytes
-    if kind == "adj_e":  # read lEy; RMW lHx, lHz; cb; memories; read 2 snapshots; model grads
-        return 5 * f + f / S + 2 * f * (rho_x + rho_y) + 2 * snap_bytes + 4 * f / S
-    if kind == "adj_h":  # read lHx, lHz; RMW lEy; ca, cq; memories
-        return 5 * f + 2 * f / S + 2 * f * (rho_x + rho_y)
+    strips = 2 * f * (rho_x + rho_y)
+    if kind == "fwd_h":  # read Ey; RMW Hx, Hz; cq; m_ey_x, m_ey_z
+        return 5 * f + f / S + strips
+    if kind == "fwd_e":  # read Hx, Hz; RMW Ey; ca, cb; m_hx_z, m_hz_x; store Ey^t, curl H^t
+        return 5 * f + 2 * f / S + strips + 2 * snap_bytes
+    if kind == "adj_e":  # read lEy; RMW lHx, lHz; cb; adjoint memories (read cur, write next)
+        return 5 * f + f / S + strips
+    if kind == "adj_h":  # read lHx, lHz; RMW lEy; ca, cq; memories; 2 snapshots; 2 gradients
+        return 5 * f + 2 * f / S + strips + 2 * snap_bytes + 2 * 2 * f / S
     raise KeyError(kind)
 
 
 # ---------------------------------------------------------------- B200 arm
+
+
+# DRAM bytes per cell moved by each kernel in one ncu capture on the config-2
+# grid (profiles/k2_adj_h_config2_ncu_full.md); None where not captured.
+TRAFFIC_B_PER_CELL = {"adj_h": 24.6}
 
 
 def shot_batches(shots: int, snap_bytes: int, device) -> int:
@@ -313,7 +320,9 @@ def run_b200(args) -> None:
         roof = {
             "kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": None, "algorithmic_bytes_per_launch": bytes_launch,
+            "traffic": (TRAFFIC_B_PER_CELL[dom] * batch * PADDED[0] * PADDED[1]
+                        if dom in TRAFFIC_B_PER_CELL else None),
+            "algorithmic_bytes_per_launch": bytes_launch,
             "avg_launch_ms": avg_ms,
             "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
         }
