@@ -113,6 +113,21 @@ TIDE_TM_DECLARE(4, double)
 TIDE_TM_DECLARE(6, double)
 TIDE_TM_DECLARE(8, double)
 
+/* Allocation-free variant of maxwell_tm_2_float_forward_cuda (same arguments,
+ * same results).  It has no counterpart in the reference.  It is for callers
+ * that must not allocate device memory during the call -- code running inside
+ * an allocator or memory-pool callback, or applications that reserve all
+ * device memory up front: the per-call scratch (the per-tile lists of source
+ * and receiver entries) lives in a fixed 16 MiB device array inside this
+ * library instead of the stream-ordered pool.  Problems needing more scratch
+ * than the array holds (2 (tiles + 1) + 2 entries words per point list,
+ * tiles = n_shots * ceil(nx/32) * ceil(ny/16)) are rejected with a status
+ * message.  All calls on a device share the array, so calls whose GPU work
+ * overlaps race and must be serialised; the first call on each device looks
+ * up the array's address and should come before any stream capture.  Debye
+ * media are not supported by this variant. */
+void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
+
 /* Comma-separated CUDA architectures the library was built for ("100a").
  * Replaces tide_cuda_arches, src/tide/csrc/storage/storage_utils.cu:213. */
 const char *tide_cuda_arches(void);

@@ -8,6 +8,7 @@
 // storage mode synchronises its side stream before returning, as the
 // reference does (maxwell_tm_cuda_inst.cu:1601-1604).
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "../../include/tide_b200.h"
@@ -569,4 +570,114 @@ extern "C" int tide_b200_device_status(int64_t device) {
   const int zero = 0;
   if (TB_CUDA(cudaMemcpyToSymbol(tb::g_tide_dev_err, &zero, sizeof(int)))) return -1;
   return v;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free forward (stencil 2, float).
+//
+// Some callers cannot allocate device memory while they run the solver: code
+// executing inside a custom allocator or memory-pool callback, applications
+// that reserve all device memory up front and forbid further allocation, and
+// embedders whose own allocator is not the CUDA runtime's.  The regular
+// forward allocates a small per-call scratch (the per-tile lists of source and
+// receiver entries) from the stream-ordered pool; this variant instead keeps
+// that scratch in one fixed device array that lives in this library, so the
+// call performs no allocation and no free of any kind.
+//
+// Limits and sharing:
+//  - the array holds kNoAllocScratchWords 32-bit words (16 MiB).  A call
+//    needs 2 (tiles + 1) + 2 entries words per point list (sources and
+//    receivers), tiles = n_shots * ceil(nx / 32) * ceil(ny / 16); larger
+//    problems are rejected with a status message before any GPU work;
+//  - every call on a device uses the same array and leaves its contents
+//    behind; each call clears the counters it needs first.  Calls whose GPU
+//    work overlaps (for example on two streams at once) race on the array and
+//    must be serialised by the caller;
+//  - the first call on each device looks the array's device address up (with
+//    that device current) and caches it; make that first call before any
+//    stream capture.
+namespace tb {
+namespace {
+
+constexpr size_t kNoAllocScratchWords = size_t(1) << 22;
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocScratchWords];
+
+std::mutex g_noalloc_mu;
+int *g_noalloc_ptr[128] = {};
+
+// Device address of the scratch array on the current device (set up once).
+int *noalloc_scratch(int device) {
+  if (device < 0 || device >= 128) {
+    set_error(kBadArgument, "noalloc forward: device index %d out of range", device);
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_ptr[device] == nullptr) {
+    void *p = nullptr;
+    if (TB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch))) return nullptr;
+    g_noalloc_ptr[device] = static_cast<int *>(p);
+  }
+  return g_noalloc_ptr[device];
+}
+
+}  // namespace
+}  // namespace tb
+
+extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float)) {
+  using namespace tb;
+  using T = float;
+  constexpr int ST = 2;
+  (void)dt; (void)step_ratio; (void)n_threads; (void)ey_prev;
+  (void)debye_a; (void)debye_b; (void)debye_cp; (void)polarization; (void)n_poles;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0, "noalloc forward: nt must be >= 0");
+  TB_REQUIRE(!has_dispersion, "noalloc forward: Debye media are not supported by this variant");
+  TB_REQUIRE(ca && cb && cq && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z && m_hz_x,
+             "noalloc forward: a field or coefficient pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || f, "noalloc forward: sources without amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r, "noalloc forward: receivers without output");
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  const bool want_s = n_sources_per_shot > 0 && sources_i != nullptr;
+  const bool want_r = n_receivers_per_shot > 0 && receivers_i != nullptr;
+  const size_t nt1 = (size_t)L.tiles_x * L.tiles_y_e * (size_t)n_shots + 1;
+  const size_t ns = want_s ? (size_t)(n_sources_per_shot * n_shots) : 0;
+  const size_t nr = want_r ? (size_t)(n_receivers_per_shot * n_shots) : 0;
+  const size_t words = (want_s ? 2 * nt1 + 2 * ns : 0) + (want_r ? 2 * nt1 + 2 * nr : 0);
+  TB_REQUIRE(words <= kNoAllocScratchWords,
+             "noalloc forward: problem needs %zu scratch words, the fixed array holds %zu "
+             "(reduce n_shots per call or use maxwell_tm_2_float_forward_cuda)",
+             words, kNoAllocScratchWords);
+  int *scratch = noalloc_scratch((int)device);
+  if (scratch == nullptr) return;
+  cudaStream_t st = as_stream(compute_stream);
+  PointScratch ps;  // ps.mem stays null: nothing is freed at scope exit
+  ps.st = st;
+  const int tile_h = kBlockY * kRowsE;
+  int *w = scratch;
+  if (want_s) {
+    int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
+    if (!build_list(sources_i, (int)n_sources_per_shot, (int)n_shots, L.g.N, L.g.nx, L.tiles_x,
+                    L.tiles_y_e, tile_h, (int)(nt1 - 1), count, start, cell, ent, st, ps.src))
+      return;
+    w += 2 * nt1 + 2 * ns;
+  }
+  if (want_r) {
+    int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + nr;
+    if (!build_list(receivers_i, (int)n_receivers_per_shot, (int)n_shots, L.g.N, L.g.nx,
+                    L.tiles_x, L.tiles_y_e, tile_h, (int)(nt1 - 1), count, start, cell, ent, st,
+                    ps.rec))
+      return;
+  }
+  const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    if (L.has_domain) launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
+    launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, nullptr, nullptr, db, ps,
+                           f ? f + t * fs : nullptr, r ? r + t * rs : nullptr);
+  }
+  count_launches(nt * (L.has_domain ? 2 : 1));
+  TB_CUDA(cudaGetLastError());
 }
