@@ -164,9 +164,9 @@ def lib():
 
 
 def read_profile(L) -> dict:
-    ms = (ctypes.c_double * 8)()
-    n = (ctypes.c_int64 * 8)()
-    k = L.tide_b200_profile_read(ms, n, 8)
+    ms = (ctypes.c_double * 16)()
+    n = (ctypes.c_int64 * 16)()
+    k = L.tide_b200_profile_read(ms, n, 16)
     return {L.tide_b200_profile_kind_name(i).decode(): (ms[i], n[i]) for i in range(k)}
 
 
@@ -177,15 +177,19 @@ def read_profile(L) -> dict:
 # and the model-shaped gradient read-modify-write once per launch.
 def kernel_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho_x: float, rho_y: float) -> float:
     f = 4.0
-    strips = 2 * f * (rho_x + rho_y)
+    strips = 2 * f * (rho_x + rho_y)  # two CPML memories (one per axis), read + write
     if kind == "fwd_h":  # read Ey; RMW Hx, Hz; cq; m_ey_x, m_ey_z
         return 5 * f + f / S + strips
     if kind == "fwd_e":  # read Hx, Hz; RMW Ey; ca, cb; m_hx_z, m_hz_x; store Ey^t, curl H^t
-        return 5 * f + 2 * f / S + strips + 2 * snap_bytes
+        return 4 * f + 2 * f / S + strips + 2 * snap_bytes
+    if kind == "fwd_step":  # fused: read + write Ey, Hx, Hz; ca, cb, cq; four memories; snapshots
+        return 6 * f + 3 * f / S + 2 * strips + 2 * snap_bytes
     if kind == "adj_e":  # read lEy; RMW lHx, lHz; cb; adjoint memories (read cur, write next)
         return 5 * f + f / S + strips
     if kind == "adj_h":  # read lHx, lHz; RMW lEy; ca, cq; memories; 2 snapshots; 2 gradients
-        return 5 * f + 2 * f / S + strips + 2 * snap_bytes + 2 * 2 * f / S
+        return 4 * f + 2 * f / S + strips + 2 * snap_bytes + 2 * 2 * f / S
+    if kind == "adj_step":  # fused adjoint: read + write lEy, lHx, lHz; coefficients; memories;
+        return 6 * f + 3 * f / S + 2 * strips + 2 * snap_bytes + 2 * 2 * f / S  # snapshots; grads
     raise KeyError(kind)
 
 

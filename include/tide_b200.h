@@ -148,13 +148,22 @@ int tide_b200_device_status(int64_t device);
  * enabled, every `sample_every`-th time step of each call brackets its stencil
  * kernels with CUDA events on the launching stream; durations accumulate per
  * kernel kind until read (reading waits for the recorded events; profiled
- * calls themselves never block).  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h. */
+ * calls themselves never block).  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h,
+ * 4 fwd_step (fused forward), 5 adj_step (fused adjoint). */
 void tide_b200_profile_enable(int on, int sample_every);
 int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds);
 const char *tide_b200_profile_kind_name(int kind);
 
 /* Total kernels this library has launched in this process (monotonic). */
 int64_t tide_b200_launch_count(void);
+
+/* Selection between the two stencil-2 FP32 forward implementations (new; no
+ * reference counterpart).  A call whose three field arrays (3 * n_shots * ny
+ * * nx * 4 bytes) exceed `bytes` runs the fused one-launch-per-step kernel;
+ * smaller calls run the H/E kernel pair, whose re-reads then hit L2.  0 = always
+ * fused, negative = never.  Default 64 MiB.  Returns the previous setting;
+ * process-wide, takes effect at the next call. */
+int64_t tide_b200_set_fused_threshold(int64_t bytes);
 
 #ifdef __cplusplus
 }

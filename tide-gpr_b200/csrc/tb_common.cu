@@ -166,7 +166,8 @@ int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds)
 }
 
 const char *tide_b200_profile_kind_name(int kind) {
-  static const char *names[] = {"fwd_h", "fwd_e", "adj_e", "adj_h"};
+  static const char *names[] = {"fwd_h", "fwd_e", "adj_e", "adj_h", "fwd_step",
+                                "adj_step"};
   return (kind >= 0 && kind < tb::kKindCount) ? names[kind] : "";
 }
 

@@ -27,7 +27,15 @@ void set_error(int status, const char *fmt, ...);
 bool cuda_failed(cudaError_t e, const char *what, const char *file, int line);
 
 // Launch accounting and optional per-kernel event timing (benchmarks).
-enum KernelKind : int { kKFwdH = 0, kKFwdE = 1, kKAdjE = 2, kKAdjH = 3, kKindCount = 4 };
+enum KernelKind : int {
+  kKFwdH = 0,     // forward H half step
+  kKFwdE = 1,     // forward E half step (+ snapshots, points)
+  kKAdjE = 2,     // adjoint E-phase
+  kKAdjH = 3,     // adjoint H-phase (+ points, gradient)
+  kKFwdStep = 4,  // fused forward step (stencil 2)
+  kKAdjStep = 5,  // fused adjoint step (stencil 2)
+  kKindCount = 6
+};
 void count_launches(int64_t n);
 
 // Brackets sampled launches with events on one stream; accumulates into the

@@ -8,12 +8,16 @@
 // storage mode synchronises its side stream before returning, as the
 // reference does (maxwell_tm_cuda_inst.cu:1601-1604).
 #include <algorithm>
+#include <atomic>
 #include <mutex>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/tide_b200.h"
 #include "tb_common.cuh"
 #include "tm2d_kernels.cuh"
+#include "tm2d_fused.cuh"
 #include "tm2d_s2.cuh"
 
 namespace tb {
@@ -88,31 +92,30 @@ struct PointScratch {
   cudaStream_t st = nullptr;
   PointCSR src{nullptr, nullptr, nullptr};
   PointCSR rec{nullptr, nullptr, nullptr};
+  const unsigned char *rowf = nullptr;  // per (shot, tile row): any point? (null: none at all)
   ~PointScratch() {
     if (mem) cudaFreeAsync(mem, st);
   }
 };
 
 bool build_list(const int64_t *idx, int n_per_shot, int n_shots, int64_t N, int nx,
-                int tiles_x, int tiles_y, int tile_h, int n_tiles, int *count, int *start,
-                int *cell, int *ent, cudaStream_t st, PointCSR &out) {
+                const PointTiles &pt, int n_tiles, int *count, int *start, int *cell, int *ent,
+                cudaStream_t st, PointCSR &out) {
   const int n = n_per_shot * n_shots;
   if (TB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * n_tiles, st))) return false;
   const int thr = 256, blk = (n + thr - 1) / thr;
-  k_points_count<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y,
-                                      tile_h, count);
+  k_points_count<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, pt, count);
   k_points_scan<<<1, 1024, 0, st>>>(count, start, n_tiles);
-  k_points_fill<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, tiles_x, tiles_y, tile_h,
-                                     start, cell, ent);
+  k_points_fill<<<blk, thr, 0, st>>>(idx, n_per_shot, n_shots, N, nx, pt, start, cell, ent);
   if (TB_CUDA(cudaGetLastError())) return false;
   count_launches(3);
   out = PointCSR{start, cell, ent};
   return true;
 }
 
-// Point lists for tiles of 32 columns x tile_h rows (tiles_y per shot).
+// Point lists for the tiles `pt`.
 template <typename T, int ST>
-bool build_points(PointScratch &ps, const Launch<T, ST> &L, int tiles_y, int tile_h,
+bool build_points(PointScratch &ps, const Launch<T, ST> &L, const PointTiles &pt,
                   const int64_t *sources_i, int64_t n_src, const int64_t *receivers_i,
                   int64_t n_rec, cudaStream_t st) {
   ps.st = st;
@@ -124,26 +127,32 @@ bool build_points(PointScratch &ps, const Launch<T, ST> &L, int tiles_y, int til
     set_error(kBadArgument, "TM2D: too many source/receiver entries");
     return false;
   }
-  const int n_tiles = L.tiles_x * tiles_y * (int)S;
+  const int n_tiles = pt.tiles_x * pt.tiles_y * (int)S;
   const size_t nt1 = (size_t)n_tiles + 1;
   const size_t ns = want_s ? (size_t)(n_src * S) : 0, nr = want_r ? (size_t)(n_rec * S) : 0;
   const size_t words = (want_s ? 2 * nt1 + 2 * ns : 0) + (want_r ? 2 * nt1 + 2 * nr : 0);
-  if (TB_CUDA(cudaMallocAsync(&ps.mem, words * sizeof(int), st))) return false;
+  const int n_rows = pt.tiles_y * (int)S;
+  if (TB_CUDA(cudaMallocAsync(&ps.mem, words * sizeof(int) + (size_t)n_rows, st))) return false;
   int *w = static_cast<int *>(ps.mem);
   if (want_s) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
-    if (!build_list(sources_i, (int)n_src, (int)S, L.g.N, L.g.nx, L.tiles_x, tiles_y, tile_h,
-                    n_tiles, count, start, cell, ent, st, ps.src))
+    if (!build_list(sources_i, (int)n_src, (int)S, L.g.N, L.g.nx, pt, n_tiles, count, start,
+                    cell, ent, st, ps.src))
       return false;
     w += 2 * nt1 + 2 * ns;
   }
   if (want_r) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + nr;
-    if (!build_list(receivers_i, (int)n_rec, (int)S, L.g.N, L.g.nx, L.tiles_x, tiles_y, tile_h,
-                    n_tiles, count, start, cell, ent, st, ps.rec))
+    if (!build_list(receivers_i, (int)n_rec, (int)S, L.g.N, L.g.nx, pt, n_tiles, count, start,
+                    cell, ent, st, ps.rec))
       return false;
   }
-  return true;
+  unsigned char *rowf = reinterpret_cast<unsigned char *>(static_cast<int *>(ps.mem) + words);
+  k_points_rowflags<<<(n_rows + 255) / 256, 256, 0, st>>>(ps.src.start, ps.rec.start, pt.tiles_x,
+                                                          n_rows, rowf);
+  count_launches(1);
+  ps.rowf = rowf;
+  return !TB_CUDA(cudaGetLastError());
 }
 
 struct EventRing {
@@ -211,6 +220,109 @@ inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, c
                                                               grt, gft, ga);
 }
 
+// ---------------------------------------------------------------------------
+// Fused stencil-2 FP32 forward (tm2d_fused.cuh) on a pitched internal copy of
+// the state: two copies of Ey, Hx, Hz, m_ey_x, m_ey_z (ping-pong), one of
+// m_hx_z, m_hz_x (updated in place) and of the coefficients, every array with
+// a guard row before and after it.  The copy is made at the start of a call
+// and the final state copied back at its end.
+struct PitchedFwd {
+  void *mem = nullptr;
+  cudaStream_t st = nullptr;
+  F4Geom q{};
+  int nx = 0;
+  float *cur[5] = {}, *nxt[5] = {}, *mhx = nullptr, *mhz = nullptr;
+  float *ca = nullptr, *cb = nullptr, *cq = nullptr;
+  float *user[7] = {};  // caller's ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x
+  int64_t rows = 0;     // rows of the state arrays (n_shots * ny)
+  ~PitchedFwd() {
+    if (mem) cudaFreeAsync(mem, st);
+  }
+  // Pitched array base points at row 0, pitched column 0 (column x at + padl).
+  bool copy_in(float *dst, const float *src, int64_t nrows) {
+    return !TB_CUDA(cudaMemcpy2DAsync(dst + q.padl, (size_t)q.pitch * 4, src, (size_t)nx * 4,
+                                      (size_t)nx * 4, (size_t)nrows, cudaMemcpyDeviceToDevice,
+                                      st));
+  }
+  bool init(const TMGeom<float> &g, float *const fields[7], const float *ca_u,
+            const float *cb_u, const float *cq_u, cudaStream_t s) {
+    st = s;
+    nx = g.nx;
+    q = f4_geom(g);
+    if (q.pshot > ((int64_t)1 << 31) - 1 - 2 * q.pitch) {
+      set_error(kBadArgument, "TM2D: ny * pitch too large for the fused forward");
+      return false;
+    }
+    rows = (int64_t)g.n_shots * g.ny;
+    const int64_t rc[3] = {(g.ca_b ? g.n_shots : 1) * (int64_t)g.ny,
+                           (g.cb_b ? g.n_shots : 1) * (int64_t)g.ny,
+                           (g.cq_b ? g.n_shots : 1) * (int64_t)g.ny};
+    const size_t state = (size_t)(rows + 2) * q.pitch;
+    size_t total = 12 * state;
+    for (int i = 0; i < 3; ++i) total += (size_t)(rc[i] + 2) * q.pitch;
+    if (TB_CUDA(cudaMallocAsync(&mem, total * sizeof(float), st))) return false;
+    if (TB_CUDA(cudaMemsetAsync(mem, 0, total * sizeof(float), st))) return false;
+    float *p = static_cast<float *>(mem);
+    auto take = [&](size_t n) {
+      float *r = p + q.pitch;  // past the leading guard row
+      p += n;
+      return r;
+    };
+    for (int i = 0; i < 5; ++i) cur[i] = take(state);
+    for (int i = 0; i < 5; ++i) nxt[i] = take(state);
+    mhx = take(state);
+    mhz = take(state);
+    ca = take((size_t)(rc[0] + 2) * q.pitch);
+    cb = take((size_t)(rc[1] + 2) * q.pitch);
+    cq = take((size_t)(rc[2] + 2) * q.pitch);
+    for (int i = 0; i < 7; ++i) user[i] = fields[i];
+    for (int i = 0; i < 5; ++i)
+      if (!copy_in(cur[i], user[i], rows) || !copy_in(nxt[i], user[i], rows)) return false;
+    return copy_in(mhx, user[5], rows) && copy_in(mhz, user[6], rows) &&
+           copy_in(ca, ca_u, rc[0]) && copy_in(cb, cb_u, rc[1]) && copy_in(cq, cq_u, rc[2]);
+  }
+  // State of the next step (old = current copy, new = the other); swaps.
+  FwdState<float> step() {
+    const FwdState<float> fs{cur[0], cur[1], cur[2], cur[3], cur[4], mhx, mhz,
+                             nxt[0], nxt[1], nxt[2], nxt[3], nxt[4], mhx, mhz};
+    for (int i = 0; i < 5; ++i) std::swap(cur[i], nxt[i]);
+    return fs;
+  }
+  bool finish() {
+    const float *fin[7] = {cur[0], cur[1], cur[2], cur[3], cur[4], mhx, mhz};
+    for (int i = 0; i < 7; ++i)
+      if (TB_CUDA(cudaMemcpy2DAsync(user[i], (size_t)nx * 4, fin[i] + q.padl,
+                                    (size_t)q.pitch * 4, (size_t)nx * 4, (size_t)rows,
+                                    cudaMemcpyDeviceToDevice, st)))
+        return false;
+    return true;
+  }
+  // One time step (one launch).
+  template <typename S_>
+  void launch(const TMGeom<float> &g, S_ *e_st, S_ *c_st, const PointScratch &ps,
+              const float *ft, float *rt) {
+    const F4Blocks nb = f4_blocks(q);
+    const dim3 grid((unsigned)(nb.n_side + nb.n_band + nb.n_int), 1, (unsigned)g.n_shots);
+    f4_fwd_step<S_><<<grid, dim3(32, kF4Warps, 1), 0, st>>>(g, q, nb, ca, cb, cq, step(), e_st,
+                                                            c_st, ps.src, ps.rec, ps.rowf, ft,
+                                                            rt);
+  }
+};
+
+template <typename T> constexpr bool is_float() { return std::is_same<T, float>::value; }
+
+// The two-kernel forward re-reads H and Ey between its half steps; while the
+// three fields of a call fit in about half of the 126 MB L2 those re-reads
+// are L2 hits and the two-kernel path is the faster one (measured on the
+// 553 x 1065 grid: 8 shots two-kernel 51.8 us/step vs fused 55.8; 24 shots
+// fused 134 vs two-kernel 171).  Above that the fused step's single HBM
+// sweep wins.
+std::atomic<int64_t> g_fused_min_bytes{(int64_t)64 << 20};  // tide_b200_set_fused_threshold
+inline bool fused_pays(int64_t n_shots, int64_t cells) {
+  const int64_t t = g_fused_min_bytes.load();
+  return t >= 0 && 3 * n_shots * cells * (int64_t)sizeof(float) > t;
+}
+
 template <typename T, int ST>
 void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads;
@@ -232,11 +344,35 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   cudaStream_t st = as_stream(compute_stream);
-  PointScratch ps;
-  if (!build_points(ps, L, L.tiles_y_e, kBlockY * kRowsE, sources_i, n_sources_per_shot,
-                    receivers_i, n_receivers_per_shot, st))
-    return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  if constexpr (is_float<T>() && ST == 2) {
+    if (db.n_poles == 0 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N)) {
+      // Fused one-launch-per-step path.
+      PitchedFwd pf;
+      float *const fields[7] = {ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x};
+      if (!pf.init(L.g, fields, ca, cb, cq, st)) return;
+      PointScratch ps;
+      if (!build_points(ps, L, pf.q.pt, sources_i, n_sources_per_shot, receivers_i,
+                        n_receivers_per_shot, st))
+        return;
+      ProfileScope prof(st);
+      for (int64_t t = start_t; t < start_t + nt; ++t) {
+        const bool smp = prof.sample(t);
+        if (smp) prof.begin(kKFwdStep);
+        pf.launch<float>(L.g, nullptr, nullptr, ps, f ? f + t * fs : nullptr,
+                         r ? r + t * rs : nullptr);
+        if (smp) prof.end(kKFwdStep);
+      }
+      count_launches(nt);
+      if (TB_CUDA(cudaGetLastError())) return;
+      pf.finish();
+      return;
+    }
+  }
+  PointScratch ps;
+  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0}, sources_i,
+                    n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
+    return;
   ProfileScope prof(st);
   for (int64_t t = start_t; t < start_t + nt; ++t) {
     const bool smp = prof.sample(t);
@@ -289,9 +425,18 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   cudaStream_t st = as_stream(compute_stream);
   cudaStream_t ss = as_stream(storage_stream);
   const bool pipeline = want_store && storage_mode == 1 && ss != nullptr && ss != st;
+  // one launch per step (see fused_pays)
+  const bool fused = is_float<T>() && ST == 2 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N);
+  PitchedFwd pf;
+  if constexpr (is_float<T>()) {
+    float *const fields[7] = {ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x};
+    if (fused && !pf.init(L.g, fields, ca, cb, cq, st)) return;
+  }
   PointScratch ps;
-  if (!build_points(ps, L, L.tiles_y_e, kBlockY * kRowsE, sources_i, n_sources_per_shot,
-                    receivers_i, n_receivers_per_shot, st))
+  if (!(fused ? build_points(ps, L, pf.q.pt, sources_i, n_sources_per_shot, receivers_i,
+                             n_receivers_per_shot, st)
+              : build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0}, sources_i,
+                             n_sources_per_shot, receivers_i, n_receivers_per_shot, st)))
     return;
   EventRing store_done, compute_done;
   if (pipeline) {
@@ -318,21 +463,33 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
       if (cb_requires_grad) c1 = (char *)curl_store_1 + off1;
       if (pipeline && TB_CUDA(cudaStreamWaitEvent(st, store_done.ev[slot], 0))) return;
     }
-    if (L.has_domain) {
-      if (smp) prof.begin(kKFwdH);
-      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
-      if (smp) prof.end(kKFwdH);
-    }
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
-    if (smp) prof.begin(kKFwdE);
-    if (store_step && bf16)
-      launch_fwd_e<T, ST, __nv_bfloat16>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
-                                         (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db, ps, ft, rt);
-    else
-      launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)e1, (T *)c1, db, ps,
-                             ft, rt);
-    if (smp) prof.end(kKFwdE);
+    if (fused) {
+      if (smp) prof.begin(kKFwdStep);
+      if constexpr (is_float<T>()) {
+        if (store_step && bf16)
+          pf.launch<__nv_bfloat16>(L.g, (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, ps, ft, rt);
+        else
+          pf.launch<float>(L.g, (float *)e1, (float *)c1, ps, ft, rt);
+      }
+      if (smp) prof.end(kKFwdStep);
+    } else {
+      if (L.has_domain) {
+        if (smp) prof.begin(kKFwdH);
+        launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
+        if (smp) prof.end(kKFwdH);
+      }
+      if (smp) prof.begin(kKFwdE);
+      if (store_step && bf16)
+        launch_fwd_e<T, ST, __nv_bfloat16>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
+                                           (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db, ps, ft,
+                                           rt);
+      else
+        launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)e1, (T *)c1, db,
+                               ps, ft, rt);
+      if (smp) prof.end(kKFwdE);
+    }
     if (store_step && storage_mode == 1) {
       cudaStream_t cs = st;
       if (pipeline) {
@@ -350,8 +507,11 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
       if (pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss))) return;
     }
   }
-  count_launches(nt * (L.has_domain ? 2 : 1));
+  count_launches(fused ? nt : nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
+  if constexpr (is_float<T>()) {
+    if (fused && !pf.finish()) return;
+  }
   if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
 }
 
@@ -407,7 +567,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
       !zero_band(m_lambda_ey_z, L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, L.tiles_y_ah, kBlockY * kRowsAH, sources_i, n_sources_per_shot, receivers_i,
+  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_ah, kTileX, kBlockY * kRowsAH, 0}, sources_i, n_sources_per_shot, receivers_i,
                     n_receivers_per_shot, st))
     return;
 
@@ -562,6 +722,10 @@ TB_DEFINE(4, double)
 TB_DEFINE(6, double)
 TB_DEFINE(8, double)
 
+extern "C" int64_t tide_b200_set_fused_threshold(int64_t bytes) {
+  return tb::g_fused_min_bytes.exchange(bytes < 0 ? -1 : bytes);
+}
+
 extern "C" int tide_b200_device_status(int64_t device) {
   if (TB_CUDA(cudaSetDevice((int)device))) return -1;
   if (TB_CUDA(cudaDeviceSynchronize())) return -1;
@@ -659,16 +823,17 @@ extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(flo
   int *w = scratch;
   if (want_s) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
-    if (!build_list(sources_i, (int)n_sources_per_shot, (int)n_shots, L.g.N, L.g.nx, L.tiles_x,
-                    L.tiles_y_e, tile_h, (int)(nt1 - 1), count, start, cell, ent, st, ps.src))
+    if (!build_list(sources_i, (int)n_sources_per_shot, (int)n_shots, L.g.N, L.g.nx,
+                    PointTiles{L.tiles_x, L.tiles_y_e, kTileX, tile_h, 0}, (int)(nt1 - 1), count,
+                    start, cell, ent, st, ps.src))
       return;
     w += 2 * nt1 + 2 * ns;
   }
   if (want_r) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + nr;
     if (!build_list(receivers_i, (int)n_receivers_per_shot, (int)n_shots, L.g.N, L.g.nx,
-                    L.tiles_x, L.tiles_y_e, tile_h, (int)(nt1 - 1), count, start, cell, ent, st,
-                    ps.rec))
+                    PointTiles{L.tiles_x, L.tiles_y_e, kTileX, tile_h, 0}, (int)(nt1 - 1), count,
+                    start, cell, ent, st, ps.rec))
       return;
   }
   const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};

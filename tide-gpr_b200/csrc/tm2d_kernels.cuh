@@ -750,15 +750,18 @@ __global__ void k_zero_band(T *__restrict__ m, int n_shots, int ny, int nx, int 
 // Point-list construction (once per call).  Entries with a negative index are
 // skipped as in the reference; an index at or beyond ny*nx sets the device
 // error word and is skipped instead of writing out of bounds.
-__device__ __forceinline__ int point_tile_of(int64_t idx, int s, int nx, int tiles_x,
-                                             int tiles_y, int tile_h) {
+// Tile of a cell: tiles of tile_w columns (counted from column -xoff) by
+// tile_h rows, tiles_x x tiles_y per shot.
+struct PointTiles {
+  int tiles_x, tiles_y, tile_w, tile_h, xoff;
+};
+__device__ __forceinline__ int point_tile_of(int64_t idx, int s, int nx, const PointTiles &t) {
   const int y = (int)(idx / nx), x = (int)(idx % nx);
-  return (s * tiles_y + y / tile_h) * tiles_x + x / kTileX;
+  return (s * t.tiles_y + y / t.tile_h) * t.tiles_x + (x + t.xoff) / t.tile_w;
 }
 
 __global__ void k_points_count(const int64_t *__restrict__ idx, int n_per_shot, int n_shots,
-                               int64_t N, int nx, int tiles_x, int tiles_y, int tile_h,
-                               int *__restrict__ count) {
+                               int64_t N, int nx, PointTiles pt, int *__restrict__ count) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_per_shot * n_shots) return;
   const int64_t v = idx[e];
@@ -767,7 +770,20 @@ __global__ void k_points_count(const int64_t *__restrict__ idx, int n_per_shot, 
     atomicOr(&g_tide_dev_err, 1);
     return;
   }
-  atomicAdd(count + point_tile_of(v, e / n_per_shot, nx, tiles_x, tiles_y, tile_h), 1);
+  atomicAdd(count + point_tile_of(v, e / n_per_shot, nx, pt), 1);
+}
+
+// Per tile row i = shot * tiles_y + tile row: does any tile of the row hold a
+// point of either list?  (start arrays are exclusive scans over the tiles.)
+__global__ void k_points_rowflags(const int *__restrict__ s_start, const int *__restrict__ r_start,
+                                  int tiles_x, int n_rows, unsigned char *__restrict__ flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_rows) return;
+  const int t0 = i * tiles_x, t1 = t0 + tiles_x;
+  bool any = false;
+  if (s_start) any = any || s_start[t1] > s_start[t0];
+  if (r_start) any = any || r_start[t1] > r_start[t0];
+  flags[i] = any ? 1 : 0;
 }
 
 // Exclusive scan of count[0..n) into start[0..n] by one block of 1024 threads.
@@ -798,19 +814,19 @@ __global__ void __launch_bounds__(1024) k_points_scan(const int *__restrict__ co
 // Place each entry at start[tile] + (its rank among earlier entries of the
 // same shot and tile), so every tile lists its entries in ascending order.
 __global__ void k_points_fill(const int64_t *__restrict__ idx, int n_per_shot, int n_shots,
-                              int64_t N, int nx, int tiles_x, int tiles_y, int tile_h,
-                              const int *__restrict__ start, int *__restrict__ cell,
+                              int64_t N, int nx, PointTiles pt, const int *__restrict__ start,
+                              int *__restrict__ cell,
                               int *__restrict__ ent) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_per_shot * n_shots) return;
   const int64_t v = idx[e];
   if (v < 0 || v >= N) return;
   const int s = e / n_per_shot;
-  const int tile = point_tile_of(v, s, nx, tiles_x, tiles_y, tile_h);
+  const int tile = point_tile_of(v, s, nx, pt);
   int rank = 0;
   for (int e2 = s * n_per_shot; e2 < e; ++e2) {
     const int64_t v2 = idx[e2];
-    if (v2 >= 0 && v2 < N && point_tile_of(v2, s, nx, tiles_x, tiles_y, tile_h) == tile) ++rank;
+    if (v2 >= 0 && v2 < N && point_tile_of(v2, s, nx, pt) == tile) ++rank;
   }
   const int pos = start[tile] + rank;
   cell[pos] = (int)v;

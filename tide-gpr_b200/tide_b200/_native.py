@@ -129,6 +129,16 @@ def device_status(device: torch.device) -> int:
     return int(lib.tide_b200_device_status(device.index or 0))
 
 
+def set_fused_threshold(nbytes: int) -> int:
+    """Field bytes (3 * shots * ny * nx * 4) above which the stencil-2 FP32
+    forward runs the fused one-launch-per-step kernel (0 = always, negative =
+    never); returns the previous setting."""
+    lib = load()
+    lib.tide_b200_set_fused_threshold.argtypes = [ctypes.c_int64]
+    lib.tide_b200_set_fused_threshold.restype = ctypes.c_int64
+    return int(lib.tide_b200_set_fused_threshold(int(nbytes)))
+
+
 def ptr(t: torch.Tensor | None) -> int:
     if t is None or t.numel() == 0:
         return 0
@@ -149,4 +159,5 @@ def exported_symbols() -> list[str]:
         "tide_b200_last_error",
         "tide_b200_clear_error",
         "tide_b200_device_status",
+        "tide_b200_set_fused_threshold",
     ]
