@@ -212,8 +212,8 @@ inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, c
                          const GradArgs<T, S> &ga) {
   if (ST == 2)
     k2_adj_h<T, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex, mez,
-                                                           mex_n, mez_n, ps.rec, ps.src, grt, gft,
-                                                           ga);
+                                                           mex_n, mez_n, ps.rec, ps.src, ps.rowf,
+                                                           grt, gft, ga);
   else
     k_adj_h<T, ST, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex,
                                                               mez, mex_n, mez_n, ps.rec, ps.src,

@@ -373,8 +373,8 @@ template <typename T, typename S, int R, int U>
 __device__ __forceinline__ void adj_h_interior_group(
     const TMGeom<T> &g, const GradArgs<T, S> &ga, const T *__restrict__ lam_hx,
     const T *__restrict__ lam_hz, T *__restrict__ lam_ey, const PointCSR &rec,
-    const PointCSR &src, const T *__restrict__ gr_t, T *__restrict__ gf_t, int s0,
-    int tiles_per_shot, int tile_xy, int j0, const T (&a)[R], const T (&cz)[R + 1],
+    const PointCSR &src, const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
+    T *__restrict__ gf_t, int s0, int tiles_per_shot, int tile_xy, int j0, const T (&a)[R], const T (&cz)[R + 1],
     const T (&cx)[R], const T (&cl)[R], T (&sa)[R], T (&sb)[R]) {
   const int nx = g.nx;
   T hxz[U][R + 1], hzx[U][R], hzl[U][R], lam[U][R];
@@ -399,7 +399,8 @@ __device__ __forceinline__ void adj_h_interior_group(
     const int s = s0 + u;
     const int64_t base = (int64_t)s * g.N;
     const int tile = s * tiles_per_shot + tile_xy;
-    const bool pts = !point_tile_empty(src, rec, tile);
+    const bool pts = rowf != nullptr && __ldg(rowf + s * gridDim.y + blockIdx.y) != 0 &&
+                     !point_tile_empty(src, rec, tile);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = j0 + r * nx;
@@ -433,7 +434,8 @@ __global__ void __launch_bounds__(256)
 k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
          const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
          const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
-         T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src, const T *__restrict__ gr_t,
+         T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src,
+         const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
          T *__restrict__ gf_t, GradArgs<T, S> ga) {
   const int nx = g.nx, ny = g.ny;
   const int x = blockIdx.x * kTileX + threadIdx.x;
@@ -471,11 +473,13 @@ k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
       constexpr int U = 4;
       int s0 = 0;
       for (; s0 + U <= g.n_shots; s0 += U)
-        adj_h_interior_group<T, S, R, U>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, gr_t, gf_t,
-                                         s0, tiles_per_shot, tile_xy, j0, a, cz, cx, cl, sa, sb);
+        adj_h_interior_group<T, S, R, U>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf, gr_t,
+                                         gf_t, s0, tiles_per_shot, tile_xy, j0, a, cz, cx, cl, sa,
+                                         sb);
       for (; s0 < g.n_shots; ++s0)
-        adj_h_interior_group<T, S, R, 1>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, gr_t, gf_t,
-                                         s0, tiles_per_shot, tile_xy, j0, a, cz, cx, cl, sa, sb);
+        adj_h_interior_group<T, S, R, 1>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf, gr_t,
+                                         gf_t, s0, tiles_per_shot, tile_xy, j0, a, cz, cx, cl, sa,
+                                         sb);
       if (imaging) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -527,7 +531,8 @@ k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
   for (int s = 0; s < g.n_shots; ++s) {
     const int64_t base = (int64_t)s * g.N;
     const int tile = s * tiles_per_shot + tile_xy;
-    const bool pts = !point_tile_empty(src, rec, tile);
+    const bool pts = rowf != nullptr && __ldg(rowf + s * gridDim.y + blockIdx.y) != 0 &&
+                     !point_tile_empty(src, rec, tile);
     const T *lhx = lam_hx + base, *lhz = lam_hz + base, *mex = m_ey_x + base;
     const T *mez = m_ey_z + base;
     T *ley = lam_ey + base;
