@@ -212,18 +212,10 @@ def shot_batches(shots: int, snap_bytes: int, device) -> int:
 
 
 def run_b200(args) -> None:
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    from tide_b200 import distributed as tdist
 
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+    ctx = tdist.init_distributed(device="cuda", timeout_s=600.0)  # NCCL when WORLD_SIZE > 1
+    world, rank, dev = ctx.world_size, ctx.rank, ctx.device
     L = lib()
     snap_bytes = 2 if args.storage == "bf16" else 4
     cfg = config2(shots=args.shots, nt=args.nt)
@@ -254,11 +246,8 @@ def run_b200(args) -> None:
             loss = 0.5 * (r * r).sum()
             loss.backward()
             loss_total = loss_total + loss.detach()
+        tdist.all_reduce_gradients([eps, sig], ctx=ctx)  # the one exchange per gradient
         g = torch.stack([eps.grad, sig.grad])
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.all_reduce(g)
         return g, loss_total
 
     def timed(n_steps, copy_in):
