@@ -1,13 +1,13 @@
 /*
  * tide_b200.h — C ABI of libtide_b200.so, the B200 (sm_100a) implementation
- * of TIDE's native TM2D time-stepping path.
+ * of TIDE's native time-stepping paths: 2-D TM and 3-D Maxwell (Yee).
  *
  * The exported symbols carry the reference backend's names and argument
  * lists, so the reference's ctypes loader can bind them unchanged:
  *   symbol naming   src/tide/backend_utils.py:771-787
  *                   ("{propagator}_{accuracy}_{dtype}_{pass}_{device}")
  *   argument specs  src/tide/backend_utils.py:227-308 (TM forward,
- *                   forward_with_storage, backward)
+ *                   forward_with_storage, backward), :446-556 (3-D)
  * Every pointer is a raw device (or pinned host, where stated) address; sizes
  * are int64; no torch types cross this boundary.
  *
@@ -127,6 +127,110 @@ TIDE_TM_DECLARE(8, double)
  * up the array's address and should come before any stream capture.  Debye
  * media are not supported by this variant. */
 void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
+
+/* ---------------------------------------------------------------- 3-D */
+
+/* Argument list of maxwell_3d_*_forward_cuda.  Replaces
+ * maxwell_3d_{S}_{dtype}_forward_cuda, src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:3012-3288
+ * (argtypes src/tide/backend_utils.py:484-504).  Fields [S, nz, ny, nx];
+ * CPML memories compacted along their own axis as the reference's CUDA
+ * callers allocate them (grid_utils.py:96-150): axis extent
+ * pml_0 + n - max(pml_0, pml_1 - 1).  source/receiver_component 0 x, 1 y, 2 z.
+ * Dispersion (has_dispersion) and execution_backend != 0 are rejected with a
+ * status message. */
+#define TIDE_3D_FORWARD_ARGS(T)                                                \
+  T const *ca, T const *cb, T const *cq, T const *f, T *ex, T *ey, T *ez,      \
+      T *hx, T *hy, T *hz, T *m_hz_y, T *m_hy_z, T *m_hx_z, T *m_hz_x,         \
+      T *m_hy_x, T *m_hx_y, T *m_ey_z, T *m_ez_y, T *m_ez_x, T *m_ex_z,        \
+      T *m_ex_y, T *m_ey_x, T const *debye_a, T const *debye_b,                \
+      T const *debye_cp, T *pol_ex, T *pol_ey, T *pol_ez, T *ex_prev,          \
+      T *ey_prev, T *ez_prev, T *r, int64_t n_poles, T const *az, T const *bz, \
+      T const *azh, T const *bzh, T const *ay, T const *by, T const *ayh,      \
+      T const *byh, T const *ax, T const *bx, T const *axh, T const *bxh,      \
+      T const *kz, T const *kzh, T const *ky, T const *kyh, T const *kx,       \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdz, T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t nz,      \
+      int64_t ny, int64_t nx, int64_t n_sources_per_shot,                      \
+      int64_t n_receivers_per_shot, int64_t step_ratio, bool has_dispersion,   \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream
+
+/* maxwell_3d_*_forward_with_storage_cuda.  Replaces
+ * src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:3290-3880 (argtypes
+ * src/tide/backend_utils.py:506-524).  Stores E^t (3 components) and the
+ * CPML-corrected curl H (3 components) at steps t % step_ratio == 0; each
+ * component has a device buffer (s1), a pinned host history (s3, cpu mode)
+ * and a file-name list (fn, disk mode, rejected). */
+#define TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)                                   \
+  T const *ca, T const *cb, T const *cq, T const *f, T *ex, T *ey, T *ez,      \
+      T *hx, T *hy, T *hz, T *m_hz_y, T *m_hy_z, T *m_hx_z, T *m_hz_x,         \
+      T *m_hy_x, T *m_hx_y, T *m_ey_z, T *m_ez_y, T *m_ez_x, T *m_ex_z,        \
+      T *m_ex_y, T *m_ey_x, T *r, void *ex_s1, void *ex_s3, void *ex_fn,       \
+      void *ey_s1, void *ey_s3, void *ey_fn, void *ez_s1, void *ez_s3,         \
+      void *ez_fn, void *cx_s1, void *cx_s3, void *cx_fn, void *cy_s1,         \
+      void *cy_s3, void *cy_fn, void *cz_s1, void *cz_s3, void *cz_fn,         \
+      T const *az, T const *bz, T const *azh, T const *bzh, T const *ay,       \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *kz, T const *kzh, T const *ky,      \
+      T const *kyh, T const *kx, T const *kxh, int64_t const *sources_i,       \
+      int64_t const *receivers_i, T rdz, T rdy, T rdx, T dt, int64_t nt,       \
+      int64_t n_shots, int64_t nz, int64_t ny, int64_t nx,                     \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream, void *storage_stream
+
+/* maxwell_3d_*_backward_cuda.  Replaces
+ * src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:4542-5240 (argtypes
+ * src/tide/backend_utils.py:537-556).  Exact adjoint over t = start_t-1 down
+ * to start_t-nt; adjoint CPML memories ping-pong with adjoint_memory_scratch
+ * (same compact sizes, the final state lands in the caller's arrays).
+ * grad_ca / grad_cb accumulate; with several unbatched shots the per-shot
+ * sums go to grad_*_shot and are added once at the end in shot order (then
+ * cleared); grad_eps / grad_sigma, when given, receive the conversion of the
+ * final grad_ca / grad_cb (maxwell_3d_cuda_inst.cu:2729-2776). */
+#define TIDE_3D_BACKWARD_ARGS(T)                                               \
+  T const *ca, T const *cb, T const *cq, T const *grad_r, T *lambda_ex,        \
+      T *lambda_ey, T *lambda_ez, T *lambda_hx, T *lambda_hy, T *lambda_hz,    \
+      T *m_lambda_ey_z, T *m_lambda_ez_y, T *m_lambda_ez_x, T *m_lambda_ex_z,  \
+      T *m_lambda_ex_y, T *m_lambda_ey_x, T *m_lambda_hz_y, T *m_lambda_hy_z,  \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, T *m_lambda_hy_x, T *m_lambda_hx_y,  \
+      T *adjoint_memory_scratch, void *ex_s1, void *ex_s3, void *ex_fn,        \
+      void *ey_s1, void *ey_s3, void *ey_fn, void *ez_s1, void *ez_s3,         \
+      void *ez_fn, void *cx_s1, void *cx_s3, void *cx_fn, void *cy_s1,         \
+      void *cy_s3, void *cy_fn, void *cz_s1, void *cz_s3, void *cz_fn,         \
+      T *grad_f, T *grad_ca, T *grad_cb, T *grad_eps, T *grad_sigma,           \
+      T *grad_ca_shot, T *grad_cb_shot, bool zero_grad_on_entry, T const *az,  \
+      T const *bz, T const *azh, T const *bzh, T const *ay, T const *by,       \
+      T const *ayh, T const *byh, T const *ax, T const *bx, T const *axh,      \
+      T const *bxh, T const *kz, T const *kzh, T const *ky, T const *kyh,      \
+      T const *kx, T const *kxh, int64_t const *sources_i,                     \
+      int64_t const *receivers_i, T rdz, T rdy, T rdx, T dt, int64_t nt,       \
+      int64_t n_shots, int64_t nz, int64_t ny, int64_t nx,                     \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream, void *storage_stream
+
+#define TIDE_3D_DECLARE(S, T)                                                  \
+  void maxwell_3d_##S##_##T##_forward_cuda(TIDE_3D_FORWARD_ARGS(T));           \
+  void maxwell_3d_##S##_##T##_forward_with_storage_cuda(                       \
+      TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T));                                   \
+  void maxwell_3d_##S##_##T##_backward_cuda(TIDE_3D_BACKWARD_ARGS(T));
+
+TIDE_3D_DECLARE(2, float)
+TIDE_3D_DECLARE(2, double)
 
 /* Comma-separated CUDA architectures the library was built for ("100a").
  * Replaces tide_cuda_arches, src/tide/csrc/storage/storage_utils.cu:213. */

@@ -1,0 +1,494 @@
+/*
+ * TEST INFRASTRUCTURE ONLY — the CPU oracle for the 3-D Maxwell (Yee) path.
+ *
+ * Included twice by em3d_oracle.c (REAL = float / double, SFX names the
+ * instantiation).  Plain sequential C restating the reference's arithmetic
+ * for stencil order 2:
+ *
+ *   forward H update        src/tide/csrc/em3d/maxwell_3d_inst.cpp:560-632
+ *   forward E update        src/tide/csrc/em3d/maxwell_3d_inst.cpp:646-702
+ *   E with snapshots        src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:755-868
+ *   sources / receivers     src/tide/csrc/em3d/maxwell_3d_inst.cpp:300-348
+ *   exact adjoint, E phase  src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:1478-1695
+ *   exact adjoint, H phase  src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:1748-1829
+ *   coefficient gradient    src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:2301-2368
+ *   shot reduction          src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:2713-2727
+ *   eps / sigma conversion  src/tide/csrc/em3d/maxwell_3d_inst.cpp:376-445
+ *   reverse loop order      src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:4886-5190
+ *
+ * Compiled without FMA contraction and with IEEE division (d / kappa, as the
+ * reference CPU backend and the reference's snapshot-storing CUDA kernel
+ * do), so the float forward equals the reference CPU forward bit for bit.
+ * CPML memories are full [S, nz, ny, nx] arrays here (the CUDA ABI passes
+ * them compacted along their axis; tests convert).
+ *
+ * Field order: ex, ey, ez, hx, hy, hz.  Forward memories (reference ABI
+ * order): m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y, m_ey_z, m_ez_y,
+ * m_ez_x, m_ex_z, m_ex_y, m_ey_x.  Adjoint memories (reference ABI order):
+ * ey_z, ez_y, ez_x, ex_z, ex_y, ey_x, hz_y, hy_z, hx_z, hz_x, hy_x, hx_y.
+ * Profiles: az bz azh bzh ay by ayh byh ax bx axh bxh kz kzh ky kyh kx kxh.
+ * Snapshots (device mode, [n_store, S, nz, ny, nx]): ex ey ez curl_x curl_y
+ * curl_z; fmt 1 = bf16 (round to nearest even).
+ */
+
+#define CAT2_(a, b) a##_##b
+#define CAT2(a, b) CAT2_(a, b)
+#define FN(name) CAT2(name, SFX)
+
+typedef struct {
+  int64_t S, nz, ny, nx, N;
+  REAL rdz, rdy, rdx;
+  int64_t z0, y0, x0, z1, y1, x1;  /* integer-grid strips: c < c0 || c >= c1 */
+  int64_t z1h, y1h, x1h;           /* half-grid strips:    c < c0 || c >= c1h */
+  const REAL *p[18];
+  int ca_b, cb_b, cq_b;
+} FN(g3);
+
+#ifndef EM3D_ORACLE_ENUMS
+#define EM3D_ORACLE_ENUMS
+enum { AZ, BZ, AZH, BZH, AY, BY, AYH, BYH, AX, BX, AXH, BXH, KZ, KZH, KY, KYH, KX, KXH };
+/* Adjoint memories, ABI order. */
+enum { L_EY_Z, L_EZ_Y, L_EZ_X, L_EX_Z, L_EX_Y, L_EY_X, L_HZ_Y, L_HY_Z, L_HX_Z, L_HZ_X, L_HY_X, L_HX_Y };
+#endif
+
+static inline int FN(active)(const FN(g3) * g, int64_t z, int64_t y, int64_t x) {
+  return z >= 1 && z < g->nz && y >= 1 && y < g->ny && x >= 1 && x < g->nx;
+}
+static inline int64_t FN(mi)(const FN(g3) * g, int64_t s, int64_t z, int64_t y, int64_t x) {
+  return ((s * g->nz + z) * g->ny + y) * g->nx + x;
+}
+
+static void FN(step_h)(const FN(g3) * g, const REAL *cq, REAL **F, REAL **M) {
+  REAL *ex = F[0], *ey = F[1], *ez = F[2], *hx = F[3], *hy = F[4], *hz = F[5];
+  REAL *m_ey_z = M[6], *m_ez_y = M[7], *m_ez_x = M[8], *m_ex_z = M[9], *m_ex_y = M[10],
+       *m_ey_x = M[11];
+  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = 1; z < g->nz; ++z)
+      for (int64_t y = 1; y < g->ny; ++y)
+        for (int64_t x = 1; x < g->nx; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL c = cq[g->cq_b ? i : j];
+          const int pz = z < g->z0 || z >= g->z1h, py = y < g->y0 || y >= g->y1h,
+                    px = x < g->x0 || x >= g->x1h;
+          REAL dEy_dz = 0, dEz_dy = 0, dEz_dx = 0, dEx_dz = 0, dEx_dy = 0, dEy_dx = 0;
+          if (z < g->nz - 1) {
+            REAL d = (ey[i + sz] - ey[i]) * g->rdz;
+            if (pz) {
+              m_ey_z[i] = g->p[BZH][z] * m_ey_z[i] + g->p[AZH][z] * d;
+              d = d / g->p[KZH][z] + m_ey_z[i];
+            }
+            dEy_dz = d;
+          }
+          if (y < g->ny - 1) {
+            REAL d = (ez[i + sy] - ez[i]) * g->rdy;
+            if (py) {
+              m_ez_y[i] = g->p[BYH][y] * m_ez_y[i] + g->p[AYH][y] * d;
+              d = d / g->p[KYH][y] + m_ez_y[i];
+            }
+            dEz_dy = d;
+          }
+          if (x < g->nx - 1) {
+            REAL d = (ez[i + 1] - ez[i]) * g->rdx;
+            if (px) {
+              m_ez_x[i] = g->p[BXH][x] * m_ez_x[i] + g->p[AXH][x] * d;
+              d = d / g->p[KXH][x] + m_ez_x[i];
+            }
+            dEz_dx = d;
+          }
+          if (z < g->nz - 1) {
+            REAL d = (ex[i + sz] - ex[i]) * g->rdz;
+            if (pz) {
+              m_ex_z[i] = g->p[BZH][z] * m_ex_z[i] + g->p[AZH][z] * d;
+              d = d / g->p[KZH][z] + m_ex_z[i];
+            }
+            dEx_dz = d;
+          }
+          if (y < g->ny - 1) {
+            REAL d = (ex[i + sy] - ex[i]) * g->rdy;
+            if (py) {
+              m_ex_y[i] = g->p[BYH][y] * m_ex_y[i] + g->p[AYH][y] * d;
+              d = d / g->p[KYH][y] + m_ex_y[i];
+            }
+            dEx_dy = d;
+          }
+          if (x < g->nx - 1) {
+            REAL d = (ey[i + 1] - ey[i]) * g->rdx;
+            if (px) {
+              m_ey_x[i] = g->p[BXH][x] * m_ey_x[i] + g->p[AXH][x] * d;
+              d = d / g->p[KXH][x] + m_ey_x[i];
+            }
+            dEy_dx = d;
+          }
+          hx[i] = hx[i] - c * (dEy_dz - dEz_dy);
+          hy[i] = hy[i] - c * (dEz_dx - dEx_dz);
+          hz[i] = hz[i] - c * (dEx_dy - dEy_dx);
+        }
+}
+
+static inline uint16_t FN(bf16)(REAL v) {
+  float f = (float)v;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) return (uint16_t)((u >> 16) | 0x40);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+static inline REAL FN(unbf16)(uint16_t h) {
+  uint32_t u = (uint32_t)h << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return (REAL)f;
+}
+static inline void FN(put)(void *st, int fmt, int64_t i, REAL v) {
+  if (fmt) ((uint16_t *)st)[i] = FN(bf16)(v);
+  else ((REAL *)st)[i] = v;
+}
+static inline REAL FN(get)(const void *st, int fmt, int64_t i) {
+  return fmt ? FN(unbf16)(((const uint16_t *)st)[i]) : ((const REAL *)st)[i];
+}
+
+/* E update; st[6] (ex, ey, ez, curl x/y/z snapshots of this step) or NULLs. */
+static void FN(step_e)(const FN(g3) * g, const REAL *ca, const REAL *cb, REAL **F, REAL **M,
+                       void **st, int fmt) {
+  REAL *ex = F[0], *ey = F[1], *ez = F[2], *hx = F[3], *hy = F[4], *hz = F[5];
+  REAL *m_hz_y = M[0], *m_hy_z = M[1], *m_hx_z = M[2], *m_hz_x = M[3], *m_hy_x = M[4],
+       *m_hx_y = M[5];
+  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = 1; z < g->nz; ++z)
+      for (int64_t y = 1; y < g->ny; ++y)
+        for (int64_t x = 1; x < g->nx; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL a = ca[g->ca_b ? i : j], b = cb[g->cb_b ? i : j];
+          REAL dHy_dz = (hy[i] - hy[i - sz]) * g->rdz;
+          REAL dHz_dy = (hz[i] - hz[i - sy]) * g->rdy;
+          REAL dHz_dx = (hz[i] - hz[i - 1]) * g->rdx;
+          REAL dHx_dz = (hx[i] - hx[i - sz]) * g->rdz;
+          REAL dHx_dy = (hx[i] - hx[i - sy]) * g->rdy;
+          REAL dHy_dx = (hy[i] - hy[i - 1]) * g->rdx;
+          if (z < g->z0 || z >= g->z1) {
+            m_hy_z[i] = g->p[BZ][z] * m_hy_z[i] + g->p[AZ][z] * dHy_dz;
+            dHy_dz = dHy_dz / g->p[KZ][z] + m_hy_z[i];
+            m_hx_z[i] = g->p[BZ][z] * m_hx_z[i] + g->p[AZ][z] * dHx_dz;
+            dHx_dz = dHx_dz / g->p[KZ][z] + m_hx_z[i];
+          }
+          if (y < g->y0 || y >= g->y1) {
+            m_hz_y[i] = g->p[BY][y] * m_hz_y[i] + g->p[AY][y] * dHz_dy;
+            dHz_dy = dHz_dy / g->p[KY][y] + m_hz_y[i];
+            m_hx_y[i] = g->p[BY][y] * m_hx_y[i] + g->p[AY][y] * dHx_dy;
+            dHx_dy = dHx_dy / g->p[KY][y] + m_hx_y[i];
+          }
+          if (x < g->x0 || x >= g->x1) {
+            m_hz_x[i] = g->p[BX][x] * m_hz_x[i] + g->p[AX][x] * dHz_dx;
+            dHz_dx = dHz_dx / g->p[KX][x] + m_hz_x[i];
+            m_hy_x[i] = g->p[BX][x] * m_hy_x[i] + g->p[AX][x] * dHy_dx;
+            dHy_dx = dHy_dx / g->p[KX][x] + m_hy_x[i];
+          }
+          const REAL cx = dHy_dz - dHz_dy, cy = dHz_dx - dHx_dz, cz = dHx_dy - dHy_dx;
+          if (st && st[0]) {
+            FN(put)(st[0], fmt, i, ex[i]);
+            FN(put)(st[1], fmt, i, ey[i]);
+            FN(put)(st[2], fmt, i, ez[i]);
+          }
+          if (st && st[3]) {
+            FN(put)(st[3], fmt, i, cx);
+            FN(put)(st[4], fmt, i, cy);
+            FN(put)(st[5], fmt, i, cz);
+          }
+          ex[i] = a * ex[i] + b * cx;
+          ey[i] = a * ey[i] + b * cy;
+          ez[i] = a * ez[i] + b * cz;
+        }
+}
+
+static void FN(inject)(REAL *field, const REAL *vals, const int64_t *idx, int64_t S, int64_t n,
+                       int64_t N) {
+  for (int64_t s = 0; s < S; ++s)
+    for (int64_t k = 0; k < n; ++k) {
+      const int64_t c = idx[s * n + k];
+      if (c >= 0) field[s * N + c] = field[s * N + c] + vals[s * n + k];
+    }
+}
+static void FN(record)(REAL *out, const REAL *field, const int64_t *idx, int64_t S, int64_t n,
+                       int64_t N) {
+  for (int64_t s = 0; s < S; ++s)
+    for (int64_t k = 0; k < n; ++k) {
+      const int64_t c = idx[s * n + k];
+      out[s * n + k] = c >= 0 ? field[s * N + c] : (REAL)0;
+    }
+}
+
+static void FN(setup)(FN(g3) * g, const REAL **prof, REAL rdz, REAL rdy, REAL rdx, int64_t S,
+                      int64_t nz, int64_t ny, int64_t nx, const int64_t *pml, int ca_b, int cb_b,
+                      int cq_b) {
+  g->S = S;
+  g->nz = nz;
+  g->ny = ny;
+  g->nx = nx;
+  g->N = nz * ny * nx;
+  g->rdz = rdz;
+  g->rdy = rdy;
+  g->rdx = rdx;
+  g->z0 = pml[0];
+  g->y0 = pml[1];
+  g->x0 = pml[2];
+  g->z1 = pml[3];
+  g->y1 = pml[4];
+  g->x1 = pml[5];
+  g->z1h = g->z1 > g->z0 ? g->z1 - 1 : g->z0;
+  g->y1h = g->y1 > g->y0 ? g->y1 - 1 : g->y0;
+  g->x1h = g->x1 > g->x0 ? g->x1 - 1 : g->x0;
+  for (int k = 0; k < 18; ++k) g->p[k] = prof[k];
+  g->ca_b = ca_b;
+  g->cb_b = cb_b;
+  g->cq_b = cq_b;
+}
+
+/* Forward over steps [start_t, start_t + nt).  store: 6 snapshot histories
+ * (or NULLs), written at steps t % k == 0 into slot t / k. */
+void FN(tide_oracle_em3d_forward)(const REAL *ca, const REAL *cb, const REAL *cq, const REAL *f,
+                                  REAL **F, REAL **M, REAL *r, const REAL **prof,
+                                  const int64_t *src_i, const int64_t *rec_i, REAL rdz, REAL rdy,
+                                  REAL rdx, int64_t nt, int64_t S, int64_t nz, int64_t ny,
+                                  int64_t nx, int64_t n_src, int64_t n_rec, int64_t start_t,
+                                  const int64_t *pml, int ca_b, int cb_b, int cq_b, int src_comp,
+                                  int rec_comp, void **store, int64_t k, int fmt) {
+  FN(g3) g;
+  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
+  const size_t esz = fmt ? 2 : sizeof(REAL);
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    FN(step_h)(&g, cq, F, M);
+    void *st[6] = {0, 0, 0, 0, 0, 0};
+    if (store && k > 0 && t % k == 0)
+      for (int c = 0; c < 6; ++c)
+        if (store[c]) st[c] = (char *)store[c] + (size_t)(t / k) * (size_t)(S * g.N) * esz;
+    FN(step_e)(&g, ca, cb, F, M, store ? st : 0, fmt);
+    if (n_src > 0 && f && src_i) FN(inject)(F[src_comp], f + t * S * n_src, src_i, S, n_src, g.N);
+    if (n_rec > 0 && r && rec_i) FN(record)(r + t * S * n_rec, F[rec_comp], rec_i, S, n_rec, g.N);
+  }
+}
+
+/* Raw adjoint terms at the offset cell o (reference raw_e_side / raw_h_side). */
+static inline REAL FN(raw_e)(const FN(g3) * g, const REAL *coef, int cb_batched, const REAL *lam,
+                             const REAL *mem, int axis, int neg, int64_t s, int64_t z, int64_t y,
+                             int64_t x) {
+  if (!FN(active)(g, z, y, x)) return 0;
+  const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+  REAL q = coef[cb_batched ? i : j] * lam[i];
+  if (neg) q = -q;
+  const int64_t c = axis == 0 ? z : axis == 1 ? y : x;
+  const int64_t lo = axis == 0 ? g->z0 : axis == 1 ? g->y0 : g->x0;
+  const int64_t hi = axis == 0 ? g->z1 : axis == 1 ? g->y1 : g->x1;
+  const REAL *A = g->p[axis == 0 ? AZ : axis == 1 ? AY : AX];
+  const REAL *B = g->p[axis == 0 ? BZ : axis == 1 ? BY : BX];
+  const REAL *K = g->p[axis == 0 ? KZ : axis == 1 ? KY : KX];
+  const REAL m_used = B[c] * mem[i] + q;
+  return (c < lo || c >= hi) ? (A[c] * m_used + q / K[c]) : q;
+}
+static inline REAL FN(raw_h)(const FN(g3) * g, const REAL *coef, int cq_batched, const REAL *lam,
+                             const REAL *mem, int axis, int neg, int64_t s, int64_t z, int64_t y,
+                             int64_t x) {
+  if (!FN(active)(g, z, y, x)) return 0;
+  const int64_t c = axis == 0 ? z : axis == 1 ? y : x;
+  const int64_t n = axis == 0 ? g->nz : axis == 1 ? g->ny : g->nx;
+  if (c >= n - 1) return 0;
+  const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+  REAL q = coef[cq_batched ? i : j] * lam[i];
+  if (neg) q = -q;
+  const int64_t lo = axis == 0 ? g->z0 : axis == 1 ? g->y0 : g->x0;
+  const int64_t hi = axis == 0 ? g->z1h : axis == 1 ? g->y1h : g->x1h;
+  const REAL *A = g->p[axis == 0 ? AZH : axis == 1 ? AYH : AXH];
+  const REAL *B = g->p[axis == 0 ? BZH : axis == 1 ? BYH : BXH];
+  const REAL *K = g->p[axis == 0 ? KZH : axis == 1 ? KYH : KXH];
+  const REAL m_used = B[c] * mem[i] + q;
+  return (c < lo || c >= hi) ? (A[c] * m_used + q / K[c]) : q;
+}
+
+static void FN(adj_e)(const FN(g3) * g, const REAL *cb, REAL **L, REAL **cur, REAL **nxt) {
+  REAL *lex = L[0], *ley = L[1], *lez = L[2], *lhx = L[3], *lhy = L[4], *lhz = L[5];
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = 1; z < g->nz; ++z)
+      for (int64_t y = 1; y < g->ny; ++y)
+        for (int64_t x = 1; x < g->nx; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL c = cb[g->cb_b ? i : j];
+          const REAL qx = c * lex[i], qy = c * ley[i], qz = c * lez[i];
+          const int pz = z < g->z0 || z >= g->z1, py = y < g->y0 || y >= g->y1,
+                    px = x < g->x0 || x >= g->x1;
+          nxt[L_HY_Z][i] = pz ? g->p[BZ][z] * cur[L_HY_Z][i] + qx : (REAL)0;
+          nxt[L_HX_Z][i] = pz ? g->p[BZ][z] * cur[L_HX_Z][i] - qy : (REAL)0;
+          nxt[L_HZ_Y][i] = py ? g->p[BY][y] * cur[L_HZ_Y][i] - qx : (REAL)0;
+          nxt[L_HX_Y][i] = py ? g->p[BY][y] * cur[L_HX_Y][i] + qz : (REAL)0;
+          nxt[L_HZ_X][i] = px ? g->p[BX][x] * cur[L_HZ_X][i] + qy : (REAL)0;
+          nxt[L_HY_X][i] = px ? g->p[BX][x] * cur[L_HY_X][i] - qz : (REAL)0;
+          const int cb_b = g->cb_b;
+#define RE(lam, mem, ax, ng, dz, dy, dx) \
+  FN(raw_e)(g, cb, cb_b, lam, cur[mem], ax, ng, s, z + (dz), y + (dy), x + (dx))
+          const REAL a1 = (RE(ley, L_HX_Z, 0, 1, 0, 0, 0) * (REAL)1 -
+                           RE(ley, L_HX_Z, 0, 1, 1, 0, 0) * (REAL)1) * g->rdz;
+          const REAL a2 = (RE(lez, L_HX_Y, 1, 0, 0, 0, 0) * (REAL)1 -
+                           RE(lez, L_HX_Y, 1, 0, 0, 1, 0) * (REAL)1) * g->rdy;
+          lhx[i] = lhx[i] + (a1 + a2);
+          const REAL b1 = (RE(lex, L_HY_Z, 0, 0, 0, 0, 0) * (REAL)1 -
+                           RE(lex, L_HY_Z, 0, 0, 1, 0, 0) * (REAL)1) * g->rdz;
+          const REAL b2 = (RE(lez, L_HY_X, 2, 1, 0, 0, 0) * (REAL)1 -
+                           RE(lez, L_HY_X, 2, 1, 0, 0, 1) * (REAL)1) * g->rdx;
+          lhy[i] = lhy[i] + (b1 + b2);
+          const REAL c1 = (RE(lex, L_HZ_Y, 1, 1, 0, 0, 0) * (REAL)1 -
+                           RE(lex, L_HZ_Y, 1, 1, 0, 1, 0) * (REAL)1) * g->rdy;
+          const REAL c2 = (RE(ley, L_HZ_X, 2, 0, 0, 0, 0) * (REAL)1 -
+                           RE(ley, L_HZ_X, 2, 0, 0, 0, 1) * (REAL)1) * g->rdx;
+          lhz[i] = lhz[i] + (c1 + c2);
+#undef RE
+        }
+}
+
+static void FN(adj_h)(const FN(g3) * g, const REAL *ca, const REAL *cq, REAL **L, REAL **cur,
+                      REAL **nxt) {
+  REAL *lex = L[0], *ley = L[1], *lez = L[2], *lhx = L[3], *lhy = L[4], *lhz = L[5];
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = 1; z < g->nz; ++z)
+      for (int64_t y = 1; y < g->ny; ++y)
+        for (int64_t x = 1; x < g->nx; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL c = cq[g->cq_b ? i : j];
+          const int pz = z < g->nz - 1 && (z < g->z0 || z >= g->z1h);
+          const int py = y < g->ny - 1 && (y < g->y0 || y >= g->y1h);
+          const int px = x < g->nx - 1 && (x < g->x0 || x >= g->x1h);
+          nxt[L_EY_Z][i] = pz ? g->p[BZH][z] * cur[L_EY_Z][i] - c * lhx[i] : (REAL)0;
+          nxt[L_EX_Z][i] = pz ? g->p[BZH][z] * cur[L_EX_Z][i] + c * lhy[i] : (REAL)0;
+          nxt[L_EZ_Y][i] = py ? g->p[BYH][y] * cur[L_EZ_Y][i] + c * lhx[i] : (REAL)0;
+          nxt[L_EX_Y][i] = py ? g->p[BYH][y] * cur[L_EX_Y][i] - c * lhz[i] : (REAL)0;
+          nxt[L_EZ_X][i] = px ? g->p[BXH][x] * cur[L_EZ_X][i] - c * lhy[i] : (REAL)0;
+          nxt[L_EY_X][i] = px ? g->p[BXH][x] * cur[L_EY_X][i] + c * lhz[i] : (REAL)0;
+          const REAL a = ca[g->ca_b ? i : j];
+          lex[i] = a * lex[i];
+          ley[i] = a * ley[i];
+          lez[i] = a * lez[i];
+          const int cq_b = g->cq_b;
+#define RH(lam, mem, ax, ng, dz, dy, dx) \
+  FN(raw_h)(g, cq, cq_b, lam, cur[mem], ax, ng, s, z + (dz), y + (dy), x + (dx))
+          const REAL e1 = (RH(lhx, L_EY_Z, 0, 1, -1, 0, 0) * (REAL)1 -
+                           RH(lhx, L_EY_Z, 0, 1, 0, 0, 0) * (REAL)1) * g->rdz;
+          const REAL e2 = (RH(lhz, L_EY_X, 2, 0, 0, 0, -1) * (REAL)1 -
+                           RH(lhz, L_EY_X, 2, 0, 0, 0, 0) * (REAL)1) * g->rdx;
+          ley[i] = ley[i] + (e1 + e2);
+          const REAL f1 = (RH(lhy, L_EX_Z, 0, 0, -1, 0, 0) * (REAL)1 -
+                           RH(lhy, L_EX_Z, 0, 0, 0, 0, 0) * (REAL)1) * g->rdz;
+          const REAL f2 = (RH(lhz, L_EX_Y, 1, 1, 0, -1, 0) * (REAL)1 -
+                           RH(lhz, L_EX_Y, 1, 1, 0, 0, 0) * (REAL)1) * g->rdy;
+          lex[i] = lex[i] + (f1 + f2);
+          const REAL h1 = (RH(lhx, L_EZ_Y, 1, 0, 0, -1, 0) * (REAL)1 -
+                           RH(lhx, L_EZ_Y, 1, 0, 0, 0, 0) * (REAL)1) * g->rdy;
+          const REAL h2 = (RH(lhy, L_EZ_X, 2, 1, 0, 0, -1) * (REAL)1 -
+                           RH(lhy, L_EZ_X, 2, 1, 0, 0, 0) * (REAL)1) * g->rdx;
+          lez[i] = lez[i] + (h1 + h2);
+#undef RH
+        }
+}
+
+/* Exact adjoint over t = start_t-1 down to start_t-nt.  lmem: the 12 adjoint
+ * memories (updated in place, ping-pong with internal buffers).  Gradients
+ * accumulate: grad_ca / grad_cb model-shaped (per shot when batched); with
+ * several unbatched shots per-shot sums are kept and added once at the end,
+ * in shot order, as the reference does.  grad_eps / grad_sigma (optional)
+ * receive the conversion of the final grad_ca / grad_cb. */
+void FN(tide_oracle_em3d_backward)(const REAL *ca, const REAL *cb, const REAL *cq,
+                                   const REAL *grad_r, REAL **L, REAL **lmem, void **store,
+                                   REAL *grad_f, REAL *grad_ca, REAL *grad_cb, REAL *grad_eps,
+                                   REAL *grad_sigma, REAL dt, const REAL **prof,
+                                   const int64_t *src_i, const int64_t *rec_i, REAL rdz, REAL rdy,
+                                   REAL rdx, int64_t nt, int64_t S, int64_t nz, int64_t ny,
+                                   int64_t nx, int64_t n_src, int64_t n_rec, int64_t k, int fmt,
+                                   int64_t start_t, const int64_t *pml, int ca_b, int cb_b,
+                                   int cq_b, int src_comp, int rec_comp, int need_ca,
+                                   int need_cb) {
+  FN(g3) g;
+  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
+  const int64_t tot = S * g.N;
+  REAL *scratch = (REAL *)calloc((size_t)(12 * tot), sizeof(REAL));
+  REAL *cur[12], *nxt[12];
+  for (int m = 0; m < 12; ++m) {
+    cur[m] = lmem[m];
+    nxt[m] = scratch + m * tot;
+  }
+  const int shot_ca = need_ca && !ca_b && S > 1, shot_cb = need_cb && !cb_b && S > 1;
+  REAL *gca_s = shot_ca ? (REAL *)calloc((size_t)tot, sizeof(REAL)) : 0;
+  REAL *gcb_s = shot_cb ? (REAL *)calloc((size_t)tot, sizeof(REAL)) : 0;
+  const size_t esz = fmt ? 2 : sizeof(REAL);
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    FN(adj_e)(&g, cb, L, cur, nxt);
+    /* H phase reads the H-phase memories of the current step */
+    FN(adj_h)(&g, ca, cq, L, cur, nxt);
+    if (n_rec > 0 && grad_r && rec_i) FN(inject)(L[rec_comp], grad_r + t * S * n_rec, rec_i, S, n_rec, g.N);
+    if (n_src > 0 && grad_f && src_i) FN(record)(grad_f + t * S * n_src, L[src_comp], src_i, S, n_src, g.N);
+    if (k > 0 && t % k == 0 && store) {
+      const size_t off = (size_t)(t / k) * (size_t)tot * esz;
+      for (int64_t s = 0; s < S; ++s)
+        for (int64_t z = 1; z < nz; ++z)
+          for (int64_t y = 1; y < ny; ++y)
+            for (int64_t x = 1; x < nx; ++x) {
+              const int64_t i = FN(mi)(&g, s, z, y, x), j = i - s * g.N;
+              const REAL lx = L[0][i], ly = L[1][i], lz = L[2][i];
+              if (need_ca && store[0]) {
+                const char *b0 = (const char *)store[0] + off, *b1 = (const char *)store[1] + off,
+                           *b2 = (const char *)store[2] + off;
+                const REAL acc = lx * FN(get)(b0, fmt, i) + ly * FN(get)(b1, fmt, i) +
+                                 lz * FN(get)(b2, fmt, i);
+                const REAL sc = acc * (REAL)k;
+                if (ca_b) grad_ca[i] = grad_ca[i] + sc;
+                else if (S == 1) grad_ca[j] = grad_ca[j] + sc;
+                else gca_s[i] = gca_s[i] + sc;
+              }
+              if (need_cb && store[3]) {
+                const char *b0 = (const char *)store[3] + off, *b1 = (const char *)store[4] + off,
+                           *b2 = (const char *)store[5] + off;
+                const REAL acc = lx * FN(get)(b0, fmt, i) + ly * FN(get)(b1, fmt, i) +
+                                 lz * FN(get)(b2, fmt, i);
+                const REAL sc = acc * (REAL)k;
+                if (cb_b) grad_cb[i] = grad_cb[i] + sc;
+                else if (S == 1) grad_cb[j] = grad_cb[j] + sc;
+                else gcb_s[i] = gcb_s[i] + sc;
+              }
+            }
+    }
+    for (int m = 0; m < 12; ++m) {
+      REAL *tmp = cur[m];
+      cur[m] = nxt[m];
+      nxt[m] = tmp;
+    }
+  }
+  for (int m = 0; m < 12; ++m)
+    if (cur[m] != lmem[m]) memcpy(lmem[m], cur[m], (size_t)tot * sizeof(REAL));
+  for (int w = 0; w < 2; ++w) {
+    REAL *acc = w ? gcb_s : gca_s, *out = w ? grad_cb : grad_ca;
+    if (!acc) continue;
+    for (int64_t j = 0; j < g.N; ++j) {
+      REAL sum = 0;
+      for (int64_t s = 0; s < S; ++s) sum = sum + acc[s * g.N + j];
+      out[j] = out[j] + sum;
+    }
+  }
+  if (grad_eps || grad_sigma) {
+    const REAL inv_dt = (REAL)1 / dt, ep0 = (REAL)8.8541878128e-12;
+    const int64_t n = ca_b ? tot : g.N;
+    for (int64_t o = 0; o < n; ++o) {
+      const int64_t s = ca_b ? o / g.N : 0, j = o - s * g.N;
+      const REAL av = ca[ca_b ? o : j], bv = cb[cb_b ? s * g.N + j : j], bsq = bv * bv;
+      const REAL ga = need_ca && grad_ca ? grad_ca[o] : (REAL)0;
+      const REAL gb = need_cb && grad_cb ? grad_cb[o] : (REAL)0;
+      const REAL dca_de = ((REAL)1 - av) * bv * inv_dt, dcb_de = -bsq * inv_dt;
+      const REAL dca_ds = -((REAL)0.5) * ((REAL)1 + av) * bv, dcb_ds = -((REAL)0.5) * bsq;
+      if (grad_eps) grad_eps[o] = (ga * dca_de + gb * dcb_de) * ep0;
+      if (grad_sigma) grad_sigma[o] = ga * dca_ds + gb * dcb_ds;
+    }
+  }
+  free(scratch);
+  free(gca_s);
+  free(gcb_s);
+}
+
+#undef FN
+#undef CAT2
+#undef CAT2_

@@ -131,11 +131,12 @@ def abi_specs():
     import json
 
     specs = {}
-    for pass_name in ("forward", "forward_with_storage", "backward"):
-        for dt in ("float", "double"):
-            ats = bu._template_argtypes(f"maxwell_tm_{pass_name}", dt)
-            specs[f"maxwell_tm_{pass_name}_{dt}"] = [a.__name__ for a in ats]
-        specs[f"maxwell_tm_{pass_name}_names"] = list(bu.backend_signature("maxwell_tm", pass_name))
+    for prop in ("maxwell_tm", "maxwell_3d"):
+        for pass_name in ("forward", "forward_with_storage", "backward"):
+            for dt in ("float", "double"):
+                ats = bu._template_argtypes(f"{prop}_{pass_name}", dt)
+                specs[f"{prop}_{pass_name}_{dt}"] = [a.__name__ for a in ats]
+            specs[f"{prop}_{pass_name}_names"] = list(bu.backend_signature(prop, pass_name))
     (HERE / "abi_specs.json").write_text(json.dumps(specs, indent=1))
 
 

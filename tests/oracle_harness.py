@@ -164,3 +164,139 @@ def set_grad_order(oracle: Oracle, order: int) -> None:
     """0: reference per-shot-then-shots order; 1: step-major (the CUDA kernels')."""
     oracle.lib.tide_oracle_set_grad_order.argtypes = [c_int]
     oracle.lib.tide_oracle_set_grad_order(order)
+
+
+# --------------------------------------------------------------------- 3-D
+PROFILES_3D = ("az", "bz", "azh", "bzh", "ay", "by", "ayh", "byh", "ax", "bx", "axh", "bxh",
+               "kz", "kzh", "ky", "kyh", "kx", "kxh")
+
+
+def _ptr_array(ts):
+    return (c_void_p * len(ts))(*[_p(t) for t in ts])
+
+
+class Oracle3D:
+    """ctypes binding of the C restatement of the reference 3-D path
+    (tide_oracle_em3d_*).  Memories are full [S, nz, ny, nx] arrays here."""
+
+    def __init__(self):
+        if not ORACLE_SO.exists():
+            build_oracle()
+        self.lib = ctypes.CDLL(str(ORACLE_SO))
+
+    def _fn(self, name, dtype):
+        sfx = "float" if dtype == torch.float32 else "double"
+        fn = getattr(self.lib, f"tide_oracle_em3d_{name}_{sfx}")
+        fn.restype = None
+        return fn, (c_float if dtype == torch.float32 else c_double)
+
+    @staticmethod
+    def full_state(pb):
+        """Full-layout copies of pb's fields and CPML memories (CPU)."""
+        from tide_b200.em3d import MEM_AXES
+
+        fields = [t.detach().cpu().clone() for t in pb.fields]
+        mem = [pb.layout.unpack(m.detach().cpu(), a).contiguous()
+               for m, a in zip(pb.memories, MEM_AXES)]
+        return fields, mem
+
+    def forward(self, pb, ca, cb, f, r, fields, mem, *, store=None, k=1, fmt=0, start_t=0,
+                nt=None):
+        nt = pb.nt if nt is None else nt
+        fn, F = self._fn("forward", pb.dtype)
+        P, I = c_void_p, c_int64
+        pml = (c_int64 * 6)(*pb.pml)
+        fn.argtypes = [P, P, P, P, P, P, P, P, P, P, F, F, F, I, I, I, I, I, I, I, I, P, c_int,
+                       c_int, c_int, c_int, c_int, P, I, c_int]
+        prof = _ptr_array([pb.profiles[n].cpu() for n in PROFILES_3D])
+        st = _ptr_array(list(store)) if store is not None else None
+        fn(_p(ca), _p(cb), _p(pb.cq.cpu()), _p(f), _ptr_array(fields), _ptr_array(mem), _p(r),
+           prof, _p(pb.sources_i.cpu()), _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, nt,
+           pb.n_shots, pb.nz, pb.ny, pb.nx, pb.n_src, pb.n_rec, start_t, pml, int(pb.batched),
+           int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp,
+           st if st is not None else None, k, fmt)
+
+    def backward(self, pb, ca, cb, grad_r, store, *, k=1, fmt=0, need_ca=True, need_cb=True,
+                 need_f=True, start_t=None, nt=None, lam=None, grads=None, eps_sigma=False):
+        """Returns (grad_ca, grad_cb, grad_f, lam_fields, lam_mem[, grad_eps, grad_sigma])."""
+        S, nz, ny, nx = pb.n_shots, pb.nz, pb.ny, pb.nx
+        nt_all = pb.nt
+        nt = nt_all if nt is None else nt
+        start_t = nt_all if start_t is None else start_t
+        dt = pb.dtype
+        if lam is None:
+            lam = ([torch.zeros((S, nz, ny, nx), dtype=dt) for _ in range(6)],
+                   [torch.zeros((S, nz, ny, nx), dtype=dt) for _ in range(12)])
+        mshape = (S, nz, ny, nx) if pb.batched else (nz, ny, nx)
+        if grads is None:
+            grads = (torch.zeros(mshape, dtype=dt), torch.zeros(mshape, dtype=dt),
+                     torch.zeros((nt_all, S, max(pb.n_src, 1)), dtype=dt))
+        gca, gcb, gf = grads
+        geps = torch.zeros(mshape, dtype=dt) if eps_sigma else None
+        gsig = torch.zeros(mshape, dtype=dt) if eps_sigma else None
+        fn, F = self._fn("backward", dt)
+        P, I = c_void_p, c_int64
+        fn.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P, F, P, P, P, F, F, F, I, I, I, I, I,
+                       I, I, I, c_int, I, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int]
+        prof = _ptr_array([pb.profiles[n].cpu() for n in PROFILES_3D])
+        pml = (c_int64 * 6)(*pb.pml)
+        fn(_p(ca), _p(cb), _p(pb.cq.cpu()), _p(grad_r), _ptr_array(lam[0]), _ptr_array(lam[1]),
+           _ptr_array(list(store)), _p(gf) if need_f and pb.n_src else None,
+           _p(gca) if need_ca else None, _p(gcb) if need_cb else None, _p(geps), _p(gsig),
+           pb.dt, prof, _p(pb.sources_i.cpu()), _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy,
+           pb.rdx, nt, S, nz, ny, nx, pb.n_src, pb.n_rec, k, fmt, start_t, pml,
+           int(pb.batched), int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp,
+           int(need_ca), int(need_cb))
+        out = (gca, gcb, gf, lam[0], lam[1])
+        return out + ((geps, gsig) if eps_sigma else ())
+
+
+class OracleEM3D(torch.autograd.Function):
+    """Autograd node over (ca, cb, f) backed by the 3-D C oracle (CPU)."""
+
+    @staticmethod
+    def forward(ctx, ca, cb, f, pb, oracle):
+        S, nz, ny, nx, nt = pb.n_shots, pb.nz, pb.ny, pb.nx, pb.nt
+        r = torch.zeros((nt, S, pb.n_rec), dtype=pb.dtype)
+        store = [torch.zeros((nt, S, nz, ny, nx), dtype=pb.dtype) for _ in range(6)]
+        fields, mem = Oracle3D.full_state(pb)
+        oracle.forward(pb, ca.detach(), cb.detach(), f.detach(), r, fields, mem, store=store)
+        ctx.save_for_backward(ca, cb)
+        ctx.pb, ctx.oracle, ctx.store = pb, oracle, store
+        return r
+
+    @staticmethod
+    def backward(ctx, grad_r):
+        ca, cb = ctx.saved_tensors
+        pb = ctx.pb
+        gca, gcb, gf, _, _ = ctx.oracle.backward(pb, ca.detach(), cb.detach(),
+                                                 grad_r.contiguous(), ctx.store)
+        if not pb.batched:
+            gca, gcb = gca.unsqueeze(0), gcb.unsqueeze(0)
+        return gca, gcb, (gf.reshape(-1) if pb.n_src else None), None, None
+
+
+class RefCPU3D:
+    """The reference's 3-D CPU backend (maxwell_3d_2_{dtype}_forward_cpu);
+    memories are full arrays on this path."""
+
+    def __init__(self, path: pathlib.Path = REF_SO):
+        self.lib = ctypes.CDLL(str(path))
+
+    def forward(self, pb, ca, cb, f, r, fields, mem, n_threads=0):
+        import sys
+
+        sys.path.insert(0, str(REPO / "tide-gpr_b200"))
+        from tide_b200 import _native as nat
+
+        sfx = "float" if pb.dtype == torch.float32 else "double"
+        fn = getattr(self.lib, f"maxwell_3d_2_{sfx}_forward_cpu")
+        fn.argtypes = nat.argtypes("maxwell_3d_forward", sfx)
+        fn.restype = None
+        b = pb.batched
+        fn(_p(ca), _p(cb), _p(pb.cq.cpu()), _p(f), *[_p(t) for t in fields],
+           *[_p(t) for t in mem], *([0] * 9), _p(r), 0,
+           *[_p(pb.profiles[n].cpu()) for n in PROFILES_3D], _p(pb.sources_i.cpu()),
+           _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.nz,
+           pb.ny, pb.nx, pb.n_src, pb.n_rec, 1, False, b, b, b, 0, *pb.pml, pb.src_comp,
+           pb.rec_comp, n_threads, 0, 0, 0)

@@ -20,7 +20,7 @@ def header_symbols() -> set[str]:
         ["gcc", "-E", "-P", "-x", "c", str(REPO / "include" / "tide_b200.h")],
         capture_output=True, text=True, check=True,
     ).stdout
-    return set(re.findall(r"\b((?:maxwell_tm|tide)_\w+)\s*\(", out))
+    return set(re.findall(r"\b((?:maxwell_tm|maxwell_3d|tide)_\w+)\s*\(", out))
 
 
 def test_library_exports_every_declared_symbol():
@@ -39,12 +39,13 @@ def test_library_metadata_calls_without_gpu():
     assert lib.tide_b200_last_status() == 0
 
 
+@pytest.mark.parametrize("prop", ["maxwell_tm", "maxwell_3d"])
 @pytest.mark.parametrize("pass_name", ["forward", "forward_with_storage", "backward"])
 @pytest.mark.parametrize("dtype", ["float", "double"])
-def test_argtypes_match_reference_loader(pass_name, dtype):
+def test_argtypes_match_reference_loader(prop, pass_name, dtype):
     specs = json.loads((GOLDEN / "abi_specs.json").read_text())
-    ref = specs[f"maxwell_tm_{pass_name}_{dtype}"]
-    mine = [a.__name__ for a in nat.argtypes(f"maxwell_tm_{pass_name}", dtype)]
+    ref = specs[f"{prop}_{pass_name}_{dtype}"]
+    mine = [a.__name__ for a in nat.argtypes(f"{prop}_{pass_name}", dtype)]
     assert mine == ref
 
 

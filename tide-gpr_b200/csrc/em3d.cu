@@ -1,0 +1,943 @@
+// 3-D Maxwell (Yee) path, stencil order 2: forward, forward with snapshot
+// storage and exact adjoint with coefficient gradients, behind the
+// reference's maxwell_3d_2_{float,double}_{forward,forward_with_storage,
+// backward}_cuda symbols (declared in include/tide_b200.h).
+//
+// Arithmetic follows the reference's 3-D update and adjoint (forward H/E
+// src/tide/csrc/em3d/maxwell_3d_inst.cpp:560-702; snapshots
+// maxwell_3d_cuda_inst.cu:755-868; adjoint :1478-1829; coefficient gradient
+// :2301-2368; shot reduction :2713-2727; conversion :2729-2776), with IEEE
+// division by kappa everywhere (the reference CPU backend and its storing CUDA
+// kernel divide; its plain CUDA forward multiplies by a reciprocal), so the
+// forward is bit-identical to the reference CPU backend.
+//
+// Layout: fields [S, nz, ny, nx]; CPML memories compacted along their own
+// axis (cells c < c0 and c >= max(c0, c1 - 1) kept) as the reference's CUDA
+// callers allocate them.  Launch: blocks of 32 (x) x 8 (y) threads, each
+// thread walking kZRun consecutive z cells of one (y, x) column; grid z =
+// shot x z-run.
+#include <algorithm>
+#include <utility>
+
+#include <cuda_bf16.h>
+
+#include "../../include/tide_b200.h"
+#include "tb_common.cuh"
+
+namespace tb {
+namespace {
+
+constexpr int kZRun = 4;
+constexpr int kRing3 = 3;  // device ring slots of the cpu storage mode (NUM_BUFFERS)
+
+enum { PAZ, PBZ, PAZH, PBZH, PAY, PBY, PAYH, PBYH, PAX, PBX, PAXH, PBXH,
+       PKZ, PKZH, PKY, PKYH, PKX, PKXH, kNProf };
+
+template <typename T> struct G3 {
+  const T *p[kNProf];
+  T rdz, rdy, rdx;
+  int nz, ny, nx, S;
+  int64_t N;
+  int z0, y0, x0, z1, y1, x1, z1h, y1h, x1h;
+  int ezc, eyc, exc;  // compact extents along z, y, x
+  bool ca_b, cb_b, cq_b;
+};
+
+template <typename T> __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+// Compact memory index of cell (s, z, y, x) for a memory of `axis`.
+template <typename T, int AXIS>
+__device__ __forceinline__ int64_t cidx(const G3<T> &g, int s, int z, int y, int x) {
+  if (AXIS == 0) {
+    const int hs = max(g.z0, g.z1 - 1);
+    const int c = z < g.z0 ? z : (z >= hs ? g.z0 + z - hs : 0);
+    return (((int64_t)s * g.ezc + c) * g.ny + y) * g.nx + x;
+  } else if (AXIS == 1) {
+    const int hs = max(g.y0, g.y1 - 1);
+    const int c = y < g.y0 ? y : (y >= hs ? g.y0 + y - hs : 0);
+    return (((int64_t)s * g.nz + z) * g.eyc + c) * g.nx + x;
+  } else {
+    const int hs = max(g.x0, g.x1 - 1);
+    const int c = x < g.x0 ? x : (x >= hs ? g.x0 + x - hs : 0);
+    return (((int64_t)s * g.nz + z) * g.ny + y) * g.exc + c;
+  }
+}
+
+// d / k for a CPML kappa k > 0; a zero numerator (a field the wave has not
+// reached) divides 1 instead so the division stays on its fast path, and d
+// itself (= d / k, sign included) is returned.
+template <typename T> __device__ __forceinline__ T div_k(T d, T k) {
+  const T q = (d == (T)0 ? (T)1 : d) / k;
+  return d == (T)0 ? d : q;
+}
+
+template <typename S, typename T> struct Snap {
+  __device__ static S enc(T v) { return (S)v; }
+  __device__ static T dec(S v) { return (T)v; }
+};
+template <typename T> struct Snap<__nv_bfloat16, T> {
+  __device__ static __nv_bfloat16 enc(T v) { return __float2bfloat16((float)v); }
+  __device__ static T dec(__nv_bfloat16 v) { return (T)__bfloat162float(v); }
+};
+
+struct Cell {
+  int s, z, y, x, zend;
+  int64_t i, j;  // flat index with and without the shot offset
+};
+template <typename T>
+__device__ __forceinline__ bool first_cell(const G3<T> &g, Cell &c) {
+  const int zruns = (g.nz + kZRun - 1) / kZRun;
+  c.x = blockIdx.x * blockDim.x + threadIdx.x;
+  c.y = blockIdx.y * blockDim.y + threadIdx.y;
+  c.s = blockIdx.z / zruns;
+  c.z = (blockIdx.z - c.s * zruns) * kZRun;
+  c.zend = min(c.z + kZRun, g.nz);
+  if (c.x < 1 || c.x >= g.nx || c.y < 1 || c.y >= g.ny) return false;
+  if (c.z < 1) c.z = 1;
+  return c.z < c.zend;
+}
+__device__ __forceinline__ void set_index(Cell &c, int ny, int nx, int64_t N) {
+  c.j = ((int64_t)c.z * ny + c.y) * nx + c.x;
+  c.i = (int64_t)c.s * N + c.j;
+}
+
+// ---------------------------------------------------------------- forward
+template <typename T>
+__global__ void __launch_bounds__(256)
+k3_fwd_h(G3<T> g, const T *__restrict__ cq, const T *__restrict__ ex, const T *__restrict__ ey,
+         const T *__restrict__ ez, T *__restrict__ hx, T *__restrict__ hy, T *__restrict__ hz,
+         T *__restrict__ m_ey_z, T *__restrict__ m_ez_y, T *__restrict__ m_ez_x,
+         T *__restrict__ m_ex_z, T *__restrict__ m_ex_y, T *__restrict__ m_ey_x) {
+  Cell c;
+  if (!first_cell(g, c)) return;
+  const int64_t sz = (int64_t)g.ny * g.nx, sy = g.nx;
+  const bool py = c.y < g.y0 || c.y >= g.y1h, px = c.x < g.x0 || c.x >= g.x1h;
+  for (; c.z < c.zend; ++c.z) {
+    set_index(c, g.ny, g.nx, g.N);
+    const int64_t i = c.i;
+    const T q = ld(cq + (g.cq_b ? i : c.j));
+    const bool pz = c.z < g.z0 || c.z >= g.z1h;
+    const T e_x = ld(ex + i), e_y = ld(ey + i), e_z = ld(ez + i);
+    T dEy_dz = 0, dEz_dy = 0, dEz_dx = 0, dEx_dz = 0, dEx_dy = 0, dEy_dx = 0;
+    if (c.z < g.nz - 1) {
+      T d = (ld(ey + i + sz) - e_y) * g.rdz;
+      T d2 = (ld(ex + i + sz) - e_x) * g.rdz;
+      if (pz) {
+        const int64_t m = cidx<T, 0>(g, c.s, c.z, c.y, c.x);
+        const T b = ld(g.p[PBZH] + c.z), a = ld(g.p[PAZH] + c.z), k = ld(g.p[PKZH] + c.z);
+        const T m1 = b * m_ey_z[m] + a * d;
+        m_ey_z[m] = m1;
+        d = div_k(d, k) + m1;
+        const T m2 = b * m_ex_z[m] + a * d2;
+        m_ex_z[m] = m2;
+        d2 = div_k(d2, k) + m2;
+      }
+      dEy_dz = d;
+      dEx_dz = d2;
+    }
+    if (c.y < g.ny - 1) {
+      T d = (ld(ez + i + sy) - e_z) * g.rdy;
+      T d2 = (ld(ex + i + sy) - e_x) * g.rdy;
+      if (py) {
+        const int64_t m = cidx<T, 1>(g, c.s, c.z, c.y, c.x);
+        const T b = ld(g.p[PBYH] + c.y), a = ld(g.p[PAYH] + c.y), k = ld(g.p[PKYH] + c.y);
+        const T m1 = b * m_ez_y[m] + a * d;
+        m_ez_y[m] = m1;
+        d = div_k(d, k) + m1;
+        const T m2 = b * m_ex_y[m] + a * d2;
+        m_ex_y[m] = m2;
+        d2 = div_k(d2, k) + m2;
+      }
+      dEz_dy = d;
+      dEx_dy = d2;
+    }
+    if (c.x < g.nx - 1) {
+      T d = (ld(ez + i + 1) - e_z) * g.rdx;
+      T d2 = (ld(ey + i + 1) - e_y) * g.rdx;
+      if (px) {
+        const int64_t m = cidx<T, 2>(g, c.s, c.z, c.y, c.x);
+        const T b = ld(g.p[PBXH] + c.x), a = ld(g.p[PAXH] + c.x), k = ld(g.p[PKXH] + c.x);
+        const T m1 = b * m_ez_x[m] + a * d;
+        m_ez_x[m] = m1;
+        d = div_k(d, k) + m1;
+        const T m2 = b * m_ey_x[m] + a * d2;
+        m_ey_x[m] = m2;
+        d2 = div_k(d2, k) + m2;
+      }
+      dEz_dx = d;
+      dEy_dx = d2;
+    }
+    hx[i] = hx[i] - q * (dEy_dz - dEz_dy);
+    hy[i] = hy[i] - q * (dEz_dx - dEx_dz);
+    hz[i] = hz[i] - q * (dEx_dy - dEy_dx);
+  }
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(256)
+k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restrict__ ex,
+         T *__restrict__ ey, T *__restrict__ ez, const T *__restrict__ hx,
+         const T *__restrict__ hy, const T *__restrict__ hz, T *__restrict__ m_hz_y,
+         T *__restrict__ m_hy_z, T *__restrict__ m_hx_z, T *__restrict__ m_hz_x,
+         T *__restrict__ m_hy_x, T *__restrict__ m_hx_y, S *__restrict__ st_ex,
+         S *__restrict__ st_ey, S *__restrict__ st_ez, S *__restrict__ st_cx,
+         S *__restrict__ st_cy, S *__restrict__ st_cz) {
+  Cell c;
+  if (!first_cell(g, c)) return;
+  const int64_t sz = (int64_t)g.ny * g.nx, sy = g.nx;
+  const bool py = c.y < g.y0 || c.y >= g.y1, px = c.x < g.x0 || c.x >= g.x1;
+  for (; c.z < c.zend; ++c.z) {
+    set_index(c, g.ny, g.nx, g.N);
+    const int64_t i = c.i;
+    const T a = ld(ca + (g.ca_b ? i : c.j)), b = ld(cb + (g.cb_b ? i : c.j));
+    const T h_x = ld(hx + i), h_y = ld(hy + i), h_z = ld(hz + i);
+    T dHy_dz = (h_y - ld(hy + i - sz)) * g.rdz;
+    T dHz_dy = (h_z - ld(hz + i - sy)) * g.rdy;
+    T dHz_dx = (h_z - ld(hz + i - 1)) * g.rdx;
+    T dHx_dz = (h_x - ld(hx + i - sz)) * g.rdz;
+    T dHx_dy = (h_x - ld(hx + i - sy)) * g.rdy;
+    T dHy_dx = (h_y - ld(hy + i - 1)) * g.rdx;
+    if (c.z < g.z0 || c.z >= g.z1) {
+      const int64_t m = cidx<T, 0>(g, c.s, c.z, c.y, c.x);
+      const T bb = ld(g.p[PBZ] + c.z), aa = ld(g.p[PAZ] + c.z), k = ld(g.p[PKZ] + c.z);
+      const T m1 = bb * m_hy_z[m] + aa * dHy_dz;
+      m_hy_z[m] = m1;
+      dHy_dz = div_k(dHy_dz, k) + m1;
+      const T m2 = bb * m_hx_z[m] + aa * dHx_dz;
+      m_hx_z[m] = m2;
+      dHx_dz = div_k(dHx_dz, k) + m2;
+    }
+    if (py) {
+      const int64_t m = cidx<T, 1>(g, c.s, c.z, c.y, c.x);
+      const T bb = ld(g.p[PBY] + c.y), aa = ld(g.p[PAY] + c.y), k = ld(g.p[PKY] + c.y);
+      const T m1 = bb * m_hz_y[m] + aa * dHz_dy;
+      m_hz_y[m] = m1;
+      dHz_dy = div_k(dHz_dy, k) + m1;
+      const T m2 = bb * m_hx_y[m] + aa * dHx_dy;
+      m_hx_y[m] = m2;
+      dHx_dy = div_k(dHx_dy, k) + m2;
+    }
+    if (px) {
+      const int64_t m = cidx<T, 2>(g, c.s, c.z, c.y, c.x);
+      const T bb = ld(g.p[PBX] + c.x), aa = ld(g.p[PAX] + c.x), k = ld(g.p[PKX] + c.x);
+      const T m1 = bb * m_hz_x[m] + aa * dHz_dx;
+      m_hz_x[m] = m1;
+      dHz_dx = div_k(dHz_dx, k) + m1;
+      const T m2 = bb * m_hy_x[m] + aa * dHy_dx;
+      m_hy_x[m] = m2;
+      dHy_dx = div_k(dHy_dx, k) + m2;
+    }
+    const T cx = dHy_dz - dHz_dy, cy = dHz_dx - dHx_dz, cz = dHx_dy - dHy_dx;
+    const T e_x = ex[i], e_y = ey[i], e_z = ez[i];
+    if (st_ex) {
+      st_ex[i] = Snap<S, T>::enc(e_x);
+      st_ey[i] = Snap<S, T>::enc(e_y);
+      st_ez[i] = Snap<S, T>::enc(e_z);
+    }
+    if (st_cx) {
+      st_cx[i] = Snap<S, T>::enc(cx);
+      st_cy[i] = Snap<S, T>::enc(cy);
+      st_cz[i] = Snap<S, T>::enc(cz);
+    }
+    ex[i] = a * e_x + b * cx;
+    ey[i] = a * e_y + b * cy;
+    ez[i] = a * e_z + b * cz;
+  }
+}
+
+// Sources then receivers of one step: one thread per (shot, point).
+template <typename T>
+__global__ void k3_points(T *__restrict__ field_src, const T *__restrict__ f_t,
+                          const int64_t *__restrict__ src_i, int n_src,
+                          const T *__restrict__ field_rec, T *__restrict__ r_t,
+                          const int64_t *__restrict__ rec_i, int n_rec, int S, int64_t N,
+                          int phase) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (phase == 0) {  // inject (duplicates within a shot accumulate in entry order)
+    if (e >= S) return;
+    for (int k = 0; k < n_src; ++k) {
+      const int64_t c = src_i[e * n_src + k];
+      if (c >= 0 && c < N) field_src[(int64_t)e * N + c] += f_t[e * n_src + k];
+    }
+  } else {  // record
+    if (e >= S * n_rec) return;
+    const int s = e / n_rec;
+    const int64_t c = rec_i[e];
+    r_t[e] = (c >= 0 && c < N) ? field_rec[(int64_t)s * N + c] : (T)0;
+  }
+}
+
+// ---------------------------------------------------------------- adjoint
+// Adjoint memories (ABI order).
+enum { LEY_Z, LEZ_Y, LEZ_X, LEX_Z, LEX_Y, LEY_X, LHZ_Y, LHY_Z, LHX_Z, LHZ_X, LHY_X, LHX_Y, kNMem };
+template <typename T> struct Mem12 {
+  T *m[kNMem];
+};
+
+__device__ __forceinline__ bool active3(int z, int y, int x, int nz, int ny, int nx) {
+  return z >= 1 && z < nz && y >= 1 && y < ny && x >= 1 && x < nx;
+}
+
+// E-side raw adjoint at the cell (z, y, x) (maxwell_3d_cuda_inst.cu:1478-1520).
+template <typename T, int AXIS, bool NEG>
+__device__ __forceinline__ T raw_e(const G3<T> &g, const T *cb, const T *lam, const T *mem,
+                                   int s, int z, int y, int x) {
+  if (!active3(z, y, x, g.nz, g.ny, g.nx)) return (T)0;
+  const int64_t j = ((int64_t)z * g.ny + y) * g.nx + x, i = (int64_t)s * g.N + j;
+  T q = ld(cb + (g.cb_b ? i : j)) * ld(lam + i);
+  if (NEG) q = -q;
+  const int c = AXIS == 0 ? z : AXIS == 1 ? y : x;
+  const int lo = AXIS == 0 ? g.z0 : AXIS == 1 ? g.y0 : g.x0;
+  const int hi = AXIS == 0 ? g.z1 : AXIS == 1 ? g.y1 : g.x1;
+  if (!(c < lo || c >= hi)) return q;
+  const int pa = AXIS == 0 ? PAZ : AXIS == 1 ? PAY : PAX;
+  const T m_used = ld(g.p[pa + 1] + c) * ld(mem + cidx<T, AXIS>(g, s, z, y, x)) + q;
+  return ld(g.p[pa] + c) * m_used + q / ld(g.p[PKZ + 2 * AXIS] + c);
+}
+
+// H-side raw adjoint (maxwell_3d_cuda_inst.cu:1522-1575).
+template <typename T, int AXIS, bool NEG>
+__device__ __forceinline__ T raw_h(const G3<T> &g, const T *cq, const T *lam, const T *mem,
+                                   int s, int z, int y, int x) {
+  if (!active3(z, y, x, g.nz, g.ny, g.nx)) return (T)0;
+  const int c = AXIS == 0 ? z : AXIS == 1 ? y : x;
+  const int n = AXIS == 0 ? g.nz : AXIS == 1 ? g.ny : g.nx;
+  if (c >= n - 1) return (T)0;
+  const int64_t j = ((int64_t)z * g.ny + y) * g.nx + x, i = (int64_t)s * g.N + j;
+  T q = ld(cq + (g.cq_b ? i : j)) * ld(lam + i);
+  if (NEG) q = -q;
+  const int lo = AXIS == 0 ? g.z0 : AXIS == 1 ? g.y0 : g.x0;
+  const int hi = AXIS == 0 ? g.z1h : AXIS == 1 ? g.y1h : g.x1h;
+  if (!(c < lo || c >= hi)) return q;
+  const int pa = AXIS == 0 ? PAZH : AXIS == 1 ? PAYH : PAXH;
+  const T m_used = ld(g.p[pa + 1] + c) * ld(mem + cidx<T, AXIS>(g, s, z, y, x)) + q;
+  return ld(g.p[pa] + c) * m_used + q / ld(g.p[PKZH + 2 * AXIS] + c);
+}
+
+// Adjoint of the forward E update (maxwell_3d_cuda_inst.cu:1625-1695):
+// next E-phase memories at the own cell, lambda_H gathers from lambda_E.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
+         const T *__restrict__ ley, const T *__restrict__ lez, T *__restrict__ lhx,
+         T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt) {
+  Cell c;
+  if (!first_cell(g, c)) return;
+  const bool py = c.y < g.y0 || c.y >= g.y1, px = c.x < g.x0 || c.x >= g.x1;
+  for (; c.z < c.zend; ++c.z) {
+    set_index(c, g.ny, g.nx, g.N);
+    const int64_t i = c.i;
+    const int s = c.s, z = c.z, y = c.y, x = c.x;
+    const T b = ld(cb + (g.cb_b ? i : c.j));
+    const T qx = b * ld(lex + i), qy = b * ld(ley + i), qz = b * ld(lez + i);
+    const bool pz = z < g.z0 || z >= g.z1;
+    {
+      const int64_t m = cidx<T, 0>(g, s, z, y, x);
+      const T bz = ld(g.p[PBZ] + z);
+      nxt.m[LHY_Z][m] = pz ? bz * cur.m[LHY_Z][m] + qx : (T)0;
+      nxt.m[LHX_Z][m] = pz ? bz * cur.m[LHX_Z][m] - qy : (T)0;
+    }
+    {
+      const int64_t m = cidx<T, 1>(g, s, z, y, x);
+      const T by = ld(g.p[PBY] + y);
+      nxt.m[LHZ_Y][m] = py ? by * cur.m[LHZ_Y][m] - qx : (T)0;
+      nxt.m[LHX_Y][m] = py ? by * cur.m[LHX_Y][m] + qz : (T)0;
+    }
+    {
+      const int64_t m = cidx<T, 2>(g, s, z, y, x);
+      const T bx = ld(g.p[PBX] + x);
+      nxt.m[LHZ_X][m] = px ? bx * cur.m[LHZ_X][m] + qy : (T)0;
+      nxt.m[LHY_X][m] = px ? bx * cur.m[LHY_X][m] - qz : (T)0;
+    }
+    const T a1 = (raw_e<T, 0, true>(g, cb, ley, cur.m[LHX_Z], s, z, y, x) * (T)1 -
+                  raw_e<T, 0, true>(g, cb, ley, cur.m[LHX_Z], s, z + 1, y, x) * (T)1) * g.rdz;
+    const T a2 = (raw_e<T, 1, false>(g, cb, lez, cur.m[LHX_Y], s, z, y, x) * (T)1 -
+                  raw_e<T, 1, false>(g, cb, lez, cur.m[LHX_Y], s, z, y + 1, x) * (T)1) * g.rdy;
+    lhx[i] = lhx[i] + (a1 + a2);
+    const T b1 = (raw_e<T, 0, false>(g, cb, lex, cur.m[LHY_Z], s, z, y, x) * (T)1 -
+                  raw_e<T, 0, false>(g, cb, lex, cur.m[LHY_Z], s, z + 1, y, x) * (T)1) * g.rdz;
+    const T b2 = (raw_e<T, 2, true>(g, cb, lez, cur.m[LHY_X], s, z, y, x) * (T)1 -
+                  raw_e<T, 2, true>(g, cb, lez, cur.m[LHY_X], s, z, y, x + 1) * (T)1) * g.rdx;
+    lhy[i] = lhy[i] + (b1 + b2);
+    const T c1 = (raw_e<T, 1, true>(g, cb, lex, cur.m[LHZ_Y], s, z, y, x) * (T)1 -
+                  raw_e<T, 1, true>(g, cb, lex, cur.m[LHZ_Y], s, z, y + 1, x) * (T)1) * g.rdy;
+    const T c2 = (raw_e<T, 2, false>(g, cb, ley, cur.m[LHZ_X], s, z, y, x) * (T)1 -
+                  raw_e<T, 2, false>(g, cb, ley, cur.m[LHZ_X], s, z, y, x + 1) * (T)1) * g.rdx;
+    lhz[i] = lhz[i] + (c1 + c2);
+  }
+}
+
+// Adjoint of the forward H update (maxwell_3d_cuda_inst.cu:1748-1829).
+template <typename T>
+__global__ void __launch_bounds__(256)
+k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
+         const T *__restrict__ lhx, const T *__restrict__ lhy, const T *__restrict__ lhz,
+         T *__restrict__ lex, T *__restrict__ ley, T *__restrict__ lez, Mem12<T> cur,
+         Mem12<T> nxt) {
+  Cell c;
+  if (!first_cell(g, c)) return;
+  const bool py = c.y < g.ny - 1 && (c.y < g.y0 || c.y >= g.y1h);
+  const bool px = c.x < g.nx - 1 && (c.x < g.x0 || c.x >= g.x1h);
+  for (; c.z < c.zend; ++c.z) {
+    set_index(c, g.ny, g.nx, g.N);
+    const int64_t i = c.i;
+    const int s = c.s, z = c.z, y = c.y, x = c.x;
+    const T q = ld(cq + (g.cq_b ? i : c.j));
+    const T l_hx = ld(lhx + i), l_hy = ld(lhy + i), l_hz = ld(lhz + i);
+    const bool pz = z < g.nz - 1 && (z < g.z0 || z >= g.z1h);
+    {
+      const int64_t m = cidx<T, 0>(g, s, z, y, x);
+      const T bz = ld(g.p[PBZH] + z);
+      nxt.m[LEY_Z][m] = pz ? bz * cur.m[LEY_Z][m] - q * l_hx : (T)0;
+      nxt.m[LEX_Z][m] = pz ? bz * cur.m[LEX_Z][m] + q * l_hy : (T)0;
+    }
+    {
+      const int64_t m = cidx<T, 1>(g, s, z, y, x);
+      const T by = ld(g.p[PBYH] + y);
+      nxt.m[LEZ_Y][m] = py ? by * cur.m[LEZ_Y][m] + q * l_hx : (T)0;
+      nxt.m[LEX_Y][m] = py ? by * cur.m[LEX_Y][m] - q * l_hz : (T)0;
+    }
+    {
+      const int64_t m = cidx<T, 2>(g, s, z, y, x);
+      const T bx = ld(g.p[PBXH] + x);
+      nxt.m[LEZ_X][m] = px ? bx * cur.m[LEZ_X][m] - q * l_hy : (T)0;
+      nxt.m[LEY_X][m] = px ? bx * cur.m[LEY_X][m] + q * l_hz : (T)0;
+    }
+    const T a = ld(ca + (g.ca_b ? i : c.j));
+    const T v_x = a * lex[i], v_y = a * ley[i], v_z = a * lez[i];
+    const T e1 = (raw_h<T, 0, true>(g, cq, lhx, cur.m[LEY_Z], s, z - 1, y, x) * (T)1 -
+                  raw_h<T, 0, true>(g, cq, lhx, cur.m[LEY_Z], s, z, y, x) * (T)1) * g.rdz;
+    const T e2 = (raw_h<T, 2, false>(g, cq, lhz, cur.m[LEY_X], s, z, y, x - 1) * (T)1 -
+                  raw_h<T, 2, false>(g, cq, lhz, cur.m[LEY_X], s, z, y, x) * (T)1) * g.rdx;
+    ley[i] = v_y + (e1 + e2);
+    const T f1 = (raw_h<T, 0, false>(g, cq, lhy, cur.m[LEX_Z], s, z - 1, y, x) * (T)1 -
+                  raw_h<T, 0, false>(g, cq, lhy, cur.m[LEX_Z], s, z, y, x) * (T)1) * g.rdz;
+    const T f2 = (raw_h<T, 1, true>(g, cq, lhz, cur.m[LEX_Y], s, z, y - 1, x) * (T)1 -
+                  raw_h<T, 1, true>(g, cq, lhz, cur.m[LEX_Y], s, z, y, x) * (T)1) * g.rdy;
+    lex[i] = v_x + (f1 + f2);
+    const T h1 = (raw_h<T, 1, false>(g, cq, lhx, cur.m[LEZ_Y], s, z, y - 1, x) * (T)1 -
+                  raw_h<T, 1, false>(g, cq, lhx, cur.m[LEZ_Y], s, z, y, x) * (T)1) * g.rdy;
+    const T h2 = (raw_h<T, 2, true>(g, cq, lhy, cur.m[LEZ_X], s, z, y, x - 1) * (T)1 -
+                  raw_h<T, 2, true>(g, cq, lhy, cur.m[LEZ_X], s, z, y, x) * (T)1) * g.rdx;
+    lez[i] = v_z + (h1 + h2);
+  }
+}
+
+// Adjoint sources (receivers inject grad_r) then adjoint receivers (sources
+// record grad_f), one step.
+template <typename T>
+__global__ void k3_adj_points(T *__restrict__ lam_rec, const T *__restrict__ gr_t,
+                              const int64_t *__restrict__ rec_i, int n_rec,
+                              const T *__restrict__ lam_src, T *__restrict__ gf_t,
+                              const int64_t *__restrict__ src_i, int n_src, int S, int64_t N,
+                              int phase) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (phase == 0) {
+    if (e >= S) return;
+    for (int k = 0; k < n_rec; ++k) {
+      const int64_t c = rec_i[e * n_rec + k];
+      if (c >= 0 && c < N) lam_rec[(int64_t)e * N + c] += gr_t[e * n_rec + k];
+    }
+  } else {
+    if (e >= S * n_src) return;
+    const int s = e / n_src;
+    const int64_t c = src_i[e];
+    gf_t[e] = (c >= 0 && c < N) ? lam_src[(int64_t)s * N + c] : (T)0;
+  }
+}
+
+// Coefficient gradient of one stored step (maxwell_3d_cuda_inst.cu:2301-2368).
+template <typename T, typename S>
+__global__ void __launch_bounds__(256)
+k3_coeff_grad(G3<T> g, const T *__restrict__ lex, const T *__restrict__ ley,
+              const T *__restrict__ lez, const S *__restrict__ sx, const S *__restrict__ sy,
+              const S *__restrict__ sz_, const S *__restrict__ cx, const S *__restrict__ cy,
+              const S *__restrict__ cz, T *__restrict__ gca, T *__restrict__ gcb,
+              T *__restrict__ gca_shot, T *__restrict__ gcb_shot, T kscale) {
+  Cell c;
+  if (!first_cell(g, c)) return;
+  for (; c.z < c.zend; ++c.z) {
+    set_index(c, g.ny, g.nx, g.N);
+    const int64_t i = c.i;
+    const T l_x = ld(lex + i), l_y = ld(ley + i), l_z = ld(lez + i);
+    if (sx) {
+      const T acc = l_x * Snap<S, T>::dec(sx[i]) + l_y * Snap<S, T>::dec(sy[i]) +
+                    l_z * Snap<S, T>::dec(sz_[i]);
+      const T v = acc * kscale;
+      if (g.ca_b) gca[i] = gca[i] + v;
+      else if (g.S == 1) gca[c.j] = gca[c.j] + v;
+      else gca_shot[i] = gca_shot[i] + v;
+    }
+    if (cx) {
+      const T acc = l_x * Snap<S, T>::dec(cx[i]) + l_y * Snap<S, T>::dec(cy[i]) +
+                    l_z * Snap<S, T>::dec(cz[i]);
+      const T v = acc * kscale;
+      if (g.cb_b) gcb[i] = gcb[i] + v;
+      else if (g.S == 1) gcb[c.j] = gcb[c.j] + v;
+      else gcb_shot[i] = gcb_shot[i] + v;
+    }
+  }
+}
+
+// grad[j] += sum over shots of grad_shot[s, j] (shot order), then clear.
+template <typename T>
+__global__ void k3_combine(T *__restrict__ grad, T *__restrict__ shot, int S, int64_t N) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < N;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    T sum = 0;
+    for (int s = 0; s < S; ++s) {
+      sum = sum + shot[(int64_t)s * N + j];
+      shot[(int64_t)s * N + j] = (T)0;
+    }
+    grad[j] = grad[j] + sum;
+  }
+}
+
+// d/d(eps_r), d/d(sigma) from d/d(ca), d/d(cb) (maxwell_3d_inst.cpp:376-445).
+template <typename T>
+__global__ void k3_convert(const T *__restrict__ ca, const T *__restrict__ cb,
+                           const T *__restrict__ gca, const T *__restrict__ gcb,
+                           T *__restrict__ geps, T *__restrict__ gsig, T dt, int64_t n,
+                           int64_t N, bool ca_b, bool cb_b) {
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = ca_b ? o / N : 0, j = o - s * N;
+    const T av = ca[ca_b ? o : j], bv = cb[cb_b ? s * N + j : j], bsq = bv * bv;
+    const T ga = gca ? gca[o] : (T)0, gb = gcb ? gcb[o] : (T)0;
+    const T inv_dt = (T)1 / dt;
+    const T dca_de = ((T)1 - av) * bv * inv_dt, dcb_de = -bsq * inv_dt;
+    const T dca_ds = -((T)0.5) * ((T)1 + av) * bv, dcb_ds = -((T)0.5) * bsq;
+    if (geps) geps[o] = (ga * dca_de + gb * dcb_de) * (T)8.8541878128e-12;
+    if (gsig) gsig[o] = ga * dca_ds + gb * dcb_ds;
+  }
+}
+
+// ---------------------------------------------------------------- host
+inline cudaStream_t stream_of(void *h) { return reinterpret_cast<cudaStream_t>(h); }
+
+template <typename T> struct Launch3 {
+  G3<T> g;
+  dim3 grid, block{32, 8, 1};
+  int64_t mem_size[3];  // elements of a compact memory along z, y, x
+};
+
+template <typename T>
+bool make3(Launch3<T> &L, const T *const prof[kNProf], T rdz, T rdy, T rdx, int64_t S,
+           int64_t nz, int64_t ny, int64_t nx, int64_t pz0, int64_t py0, int64_t px0,
+           int64_t pz1, int64_t py1, int64_t px1, bool ca_b, bool cb_b, bool cq_b) {
+  if (S < 1 || nz < 2 || ny < 2 || nx < 2 || nz > (1 << 20) || ny > (1 << 20) ||
+      nx > (1 << 20) || nz * ny * nx > ((int64_t)1 << 40) ||
+      S * ((nz + kZRun - 1) / kZRun) > 65535) {
+    set_error(kBadArgument, "3-D: unsupported shape n_shots=%lld nz=%lld ny=%lld nx=%lld",
+              (long long)S, (long long)nz, (long long)ny, (long long)nx);
+    return false;
+  }
+  for (int k = 0; k < kNProf; ++k)
+    if (!prof[k]) {
+      set_error(kBadArgument, "3-D: CPML profile pointer %d is null", k);
+      return false;
+    }
+  auto bad = [](int64_t lo, int64_t hi, int64_t n) { return lo < 0 || hi < lo || hi > n; };
+  if (bad(pz0, pz1, nz) || bad(py0, py1, ny) || bad(px0, px1, nx)) {
+    set_error(kBadArgument, "3-D: CPML bounds outside the grid");
+    return false;
+  }
+  G3<T> &g = L.g;
+  for (int k = 0; k < kNProf; ++k) g.p[k] = prof[k];
+  g.rdz = rdz; g.rdy = rdy; g.rdx = rdx;
+  g.nz = (int)nz; g.ny = (int)ny; g.nx = (int)nx; g.S = (int)S;
+  g.N = nz * ny * nx;
+  g.z0 = (int)pz0; g.y0 = (int)py0; g.x0 = (int)px0;
+  g.z1 = (int)pz1; g.y1 = (int)py1; g.x1 = (int)px1;
+  g.z1h = pz1 > pz0 ? (int)pz1 - 1 : (int)pz0;
+  g.y1h = py1 > py0 ? (int)py1 - 1 : (int)py0;
+  g.x1h = px1 > px0 ? (int)px1 - 1 : (int)px0;
+  g.ezc = (int)(pz0 + nz - std::max(pz0, pz1 - 1));
+  g.eyc = (int)(py0 + ny - std::max(py0, py1 - 1));
+  g.exc = (int)(px0 + nx - std::max(px0, px1 - 1));
+  g.ca_b = ca_b; g.cb_b = cb_b; g.cq_b = cq_b;
+  L.grid = dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8),
+                (unsigned)(S * ((nz + kZRun - 1) / kZRun)));
+  L.mem_size[0] = S * g.ezc * ny * nx;
+  L.mem_size[1] = S * nz * g.eyc * nx;
+  L.mem_size[2] = S * nz * ny * g.exc;
+  return true;
+}
+
+template <typename T> T *field_of(T *ex, T *ey, T *ez, int64_t comp) {
+  return comp == 0 ? ex : comp == 2 ? ez : ey;
+}
+
+template <typename T>
+bool common_checks(const char *what, int64_t n_src, const T *f, int64_t n_rec, const T *r,
+                   int64_t src_c, int64_t rec_c, int64_t exec_backend) {
+  if (n_src > 0 && !f) {
+    set_error(kBadArgument, "%s: sources without amplitudes", what);
+    return false;
+  }
+  if (n_rec > 0 && !r) {
+    set_error(kBadArgument, "%s: receivers without output", what);
+    return false;
+  }
+  if (src_c < 0 || src_c > 2 || rec_c < 0 || rec_c > 2) {
+    set_error(kBadArgument, "%s: component must be 0 (x), 1 (y) or 2 (z)", what);
+    return false;
+  }
+  if (exec_backend != 0) {
+    set_error(kBadArgument, "%s: execution_backend %lld is not built (0 only)", what,
+              (long long)exec_backend);
+    return false;
+  }
+  return true;
+}
+
+template <typename T, typename S>
+void launch_fwd_step(const Launch3<T> &L, cudaStream_t st, const T *ca, const T *cb,
+                     const T *cq, T *F[6], T *M[12], S *const snap[6], const T *f_t,
+                     const int64_t *src_i, int64_t n_src, int64_t src_c, T *r_t,
+                     const int64_t *rec_i, int64_t n_rec, int64_t rec_c) {
+  k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, F[0], F[1], F[2], F[3], F[4], F[5], M[6],
+                                          M[7], M[8], M[9], M[10], M[11]);
+  k3_fwd_e<T, S><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, F[0], F[1], F[2], F[3], F[4], F[5],
+                                             M[0], M[1], M[2], M[3], M[4], M[5], snap[0],
+                                             snap[1], snap[2], snap[3], snap[4], snap[5]);
+  int n = 2;
+  const int S_ = L.g.S;
+  if (n_src > 0 && f_t && src_i) {
+    k3_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(field_of(F[0], F[1], F[2], src_c), f_t, src_i,
+                                                   (int)n_src, nullptr, nullptr, nullptr, 0, S_,
+                                                   L.g.N, 0);
+    ++n;
+  }
+  if (n_rec > 0 && r_t && rec_i) {
+    const int tot = S_ * (int)n_rec;
+    k3_points<T><<<(tot + 127) / 128, 128, 0, st>>>(nullptr, nullptr, nullptr, 0,
+                                                    field_of(F[0], F[1], F[2], rec_c), r_t,
+                                                    rec_i, (int)n_rec, S_, L.g.N, 1);
+    ++n;
+  }
+  count_launches(n);
+}
+
+template <typename T>
+void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
+  (void)dt; (void)step_ratio; (void)n_threads; (void)n_poles;
+  (void)debye_a; (void)debye_b; (void)debye_cp; (void)pol_ex; (void)pol_ey; (void)pol_ez;
+  (void)ex_prev; (void)ey_prev; (void)ez_prev;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0, "3-D forward: nt must be >= 0");
+  TB_REQUIRE(!has_dispersion, "3-D forward: Debye dispersion is not built in this library");
+  TB_REQUIRE(ca && cb && cq && ex && ey && ez && hx && hy && hz,
+             "3-D forward: a field or coefficient pointer is null");
+  T *M[12] = {m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y,
+              m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x};
+  for (T *m : M) TB_REQUIRE(m != nullptr, "3-D forward: a CPML memory pointer is null");
+  if (!common_checks("3-D forward", n_sources_per_shot, f, n_receivers_per_shot, r,
+                     source_component, receiver_component, execution_backend))
+    return;
+  const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
+                           kz, kzh, ky, kyh, kx, kxh};
+  Launch3<T> L;
+  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = stream_of(compute_stream);
+  T *F[6] = {ex, ey, ez, hx, hy, hz};
+  T *const none[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  for (int64_t t = start_t; t < start_t + nt; ++t)
+    launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, none, f ? f + t * fs : nullptr, sources_i,
+                          n_sources_per_shot, source_component, r ? r + t * rs : nullptr,
+                          receivers_i, n_receivers_per_shot, receiver_component);
+  TB_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
+  (void)dt; (void)n_threads; (void)ex_fn; (void)ey_fn; (void)ez_fn; (void)cx_fn; (void)cy_fn;
+  (void)cz_fn;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D forward_with_storage: bad nt/step_ratio");
+  TB_REQUIRE(ca && cb && cq && ex && ey && ez && hx && hy && hz,
+             "3-D forward_with_storage: a field or coefficient pointer is null");
+  TB_REQUIRE(storage_mode != 2,
+             "3-D forward_with_storage: disk storage mode is not built in this library");
+  TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "3-D: unknown storage_mode %lld",
+             (long long)storage_mode);
+  T *M[12] = {m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y,
+              m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x};
+  for (T *m : M) TB_REQUIRE(m != nullptr, "3-D forward_with_storage: a CPML memory is null");
+  if (!common_checks("3-D forward_with_storage", n_sources_per_shot, f, n_receivers_per_shot,
+                     r, source_component, receiver_component, execution_backend))
+    return;
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "3-D: bf16 snapshot storage requires float32 fields");
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  const bool want = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
+  void *s1[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};
+  void *s3[6] = {ex_s3, ey_s3, ez_s3, cx_s3, cy_s3, cz_s3};
+  const bool need[6] = {ca_requires_grad, ca_requires_grad, ca_requires_grad,
+                        cb_requires_grad, cb_requires_grad, cb_requires_grad};
+  if (want) {
+    TB_REQUIRE(shot_bytes_uncomp == nz * ny * nx * (int64_t)esz,
+               "3-D: shot_bytes_uncomp=%lld does not match nz*ny*nx*elem=%lld",
+               (long long)shot_bytes_uncomp, (long long)(nz * ny * nx * (int64_t)esz));
+    for (int c = 0; c < 6; ++c) {
+      TB_REQUIRE(!need[c] || s1[c], "3-D: snapshot buffer %d missing", c);
+      TB_REQUIRE(!need[c] || storage_mode != 1 || s3[c],
+                 "3-D: cpu storage mode needs host snapshot buffer %d", c);
+    }
+  }
+  const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
+                           kz, kzh, ky, kyh, kx, kxh};
+  Launch3<T> L;
+  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = stream_of(compute_stream);
+  T *F[6] = {ex, ey, ez, hx, hy, hz};
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    const bool store = want && (t % step_ratio) == 0;
+    const int64_t q = t / step_ratio;
+    char *dst[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (store)
+      for (int c = 0; c < 6; ++c)
+        if (need[c])
+          dst[c] = (char *)s1[c] +
+                   (storage_mode == 0 ? (size_t)q : (size_t)(q % kRing3)) * step_bytes;
+    const T *ft = f ? f + t * fs : nullptr;
+    T *rt = r ? r + t * rs : nullptr;
+    if (bf16) {
+      __nv_bfloat16 *const sp[6] = {(__nv_bfloat16 *)dst[0], (__nv_bfloat16 *)dst[1],
+                                    (__nv_bfloat16 *)dst[2], (__nv_bfloat16 *)dst[3],
+                                    (__nv_bfloat16 *)dst[4], (__nv_bfloat16 *)dst[5]};
+      launch_fwd_step<T, __nv_bfloat16>(L, st, ca, cb, cq, F, M, sp, ft, sources_i,
+                                        n_sources_per_shot, source_component, rt, receivers_i,
+                                        n_receivers_per_shot, receiver_component);
+    } else {
+      T *const sp[6] = {(T *)dst[0], (T *)dst[1], (T *)dst[2],
+                        (T *)dst[3], (T *)dst[4], (T *)dst[5]};
+      launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, sp, ft, sources_i, n_sources_per_shot,
+                            source_component, rt, receivers_i, n_receivers_per_shot,
+                            receiver_component);
+    }
+    if (store && storage_mode == 1)  // ordered on the compute stream: the ring slot is reused
+      for (int c = 0; c < 6; ++c)
+        if (dst[c] && TB_CUDA(cudaMemcpyAsync((char *)s3[c] + (size_t)q * step_bytes, dst[c],
+                                              step_bytes, cudaMemcpyDeviceToHost, st)))
+          return;
+  }
+  (void)storage_stream;
+  if (TB_CUDA(cudaGetLastError())) return;
+  if (want && storage_mode == 1) TB_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename T>
+void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
+  (void)n_threads; (void)ex_fn; (void)ey_fn; (void)ez_fn; (void)cx_fn; (void)cy_fn; (void)cz_fn;
+  (void)storage_stream;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D backward: bad nt/step_ratio");
+  TB_REQUIRE(start_t - nt >= 0, "3-D backward: start_t - nt must be >= 0");
+  TB_REQUIRE(ca && cb && cq && lambda_ex && lambda_ey && lambda_ez && lambda_hx && lambda_hy &&
+                 lambda_hz && adjoint_memory_scratch,
+             "3-D backward: a field, coefficient or scratch pointer is null");
+  TB_REQUIRE(storage_mode != 2, "3-D backward: disk storage mode is not built in this library");
+  TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "3-D: unknown storage_mode %lld",
+             (long long)storage_mode);
+  T *lm[12] = {m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,
+               m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z,
+               m_lambda_hx_z, m_lambda_hz_x, m_lambda_hy_x, m_lambda_hx_y};
+  for (T *m : lm) TB_REQUIRE(m != nullptr, "3-D backward: an adjoint CPML memory is null");
+  if (!common_checks<T>("3-D backward", 0, nullptr, 0, nullptr, source_component,
+                        receiver_component, execution_backend))
+    return;
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "3-D: bf16 snapshot storage requires float32 fields");
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  const bool need_ca = ca_requires_grad && grad_ca && storage_mode != 3;
+  const bool need_cb = cb_requires_grad && grad_cb && storage_mode != 3;
+  void *s1[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};
+  void *s3[6] = {ex_s3, ey_s3, ez_s3, cx_s3, cy_s3, cz_s3};
+  const bool need[6] = {need_ca, need_ca, need_ca, need_cb, need_cb, need_cb};
+  if (need_ca || need_cb) {
+    TB_REQUIRE(shot_bytes_uncomp == nz * ny * nx * (int64_t)esz,
+               "3-D: shot_bytes_uncomp=%lld does not match nz*ny*nx*elem=%lld",
+               (long long)shot_bytes_uncomp, (long long)(nz * ny * nx * (int64_t)esz));
+    for (int c = 0; c < 6; ++c) {
+      TB_REQUIRE(!need[c] || s1[c], "3-D backward: snapshot buffer %d missing", c);
+      TB_REQUIRE(!need[c] || storage_mode != 1 || s3[c],
+                 "3-D backward: cpu storage mode needs host snapshot buffer %d", c);
+    }
+  }
+  const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
+                           kz, kzh, ky, kyh, kx, kxh};
+  Launch3<T> L;
+  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  const G3<T> &g = L.g;
+  const bool shot_ca = need_ca && !ca_batched && n_shots > 1;
+  const bool shot_cb = need_cb && !cb_batched && n_shots > 1;
+  TB_REQUIRE(!shot_ca || grad_ca_shot, "3-D backward: grad_ca_shot needed for several shots");
+  TB_REQUIRE(!shot_cb || grad_cb_shot, "3-D backward: grad_cb_shot needed for several shots");
+  cudaStream_t st = stream_of(compute_stream);
+  const int64_t tot = n_shots * g.N;
+  const int64_t model_n = g.N;
+  if (zero_grad_on_entry) {
+    if (grad_f && n_sources_per_shot > 0 &&
+        TB_CUDA(cudaMemsetAsync(grad_f, 0, sizeof(T) * nt * n_shots * n_sources_per_shot, st)))
+      return;
+    if (need_ca && TB_CUDA(cudaMemsetAsync(grad_ca, 0, sizeof(T) * (ca_batched ? tot : model_n), st)))
+      return;
+    if (need_cb && TB_CUDA(cudaMemsetAsync(grad_cb, 0, sizeof(T) * (cb_batched ? tot : model_n), st)))
+      return;
+  }
+  if (shot_ca && TB_CUDA(cudaMemsetAsync(grad_ca_shot, 0, sizeof(T) * tot, st))) return;
+  if (shot_cb && TB_CUDA(cudaMemsetAsync(grad_cb_shot, 0, sizeof(T) * tot, st))) return;
+  // Adjoint memory ping-pong: caller arrays and the scratch (same sizes).
+  Mem12<T> cur, nxt;
+  {
+    const int axis_of[12] = {0, 1, 2, 0, 1, 2, 1, 0, 0, 2, 2, 1};
+    int64_t off = 0;
+    for (int m = 0; m < 12; ++m) {
+      cur.m[m] = lm[m];
+      nxt.m[m] = adjoint_memory_scratch + off;
+      off += L.mem_size[axis_of[m]];
+    }
+    if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, sizeof(T) * off, st))) return;
+  }
+  T *lam_src = field_of(lambda_ex, lambda_ey, lambda_ez, source_component);
+  T *lam_rec = field_of(lambda_ex, lambda_ey, lambda_ez, receiver_component);
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  const int S_ = (int)n_shots;
+  int64_t launches = 0;
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    k3_adj_e<T><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez, lambda_hx,
+                                            lambda_hy, lambda_hz, cur, nxt);
+    k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
+                                            lambda_ex, lambda_ey, lambda_ez, cur, nxt);
+    launches += 2;
+    if (n_receivers_per_shot > 0 && grad_r && receivers_i) {
+      k3_adj_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
+          lam_rec, grad_r + t * n_shots * n_receivers_per_shot, receivers_i,
+          (int)n_receivers_per_shot, nullptr, nullptr, nullptr, 0, S_, g.N, 0);
+      ++launches;
+    }
+    if (n_sources_per_shot > 0 && grad_f && sources_i) {
+      const int n = S_ * (int)n_sources_per_shot;
+      k3_adj_points<T><<<(n + 127) / 128, 128, 0, st>>>(
+          nullptr, nullptr, nullptr, 0, lam_src, grad_f + t * n_shots * n_sources_per_shot,
+          sources_i, (int)n_sources_per_shot, S_, g.N, 1);
+      ++launches;
+    }
+    if ((need_ca || need_cb) && (t % step_ratio) == 0) {
+      const int64_t q = t / step_ratio;
+      const char *src[6];
+      for (int c = 0; c < 6; ++c) {
+        src[c] = nullptr;
+        if (!need[c]) continue;
+        if (storage_mode == 1) {  // bring the host history back through a ring slot
+          char *slot = (char *)s1[c] + (size_t)(q % kRing3) * step_bytes;
+          if (TB_CUDA(cudaMemcpyAsync(slot, (const char *)s3[c] + (size_t)q * step_bytes,
+                                      step_bytes, cudaMemcpyHostToDevice, st)))
+            return;
+          src[c] = slot;
+        } else {
+          src[c] = (const char *)s1[c] + (size_t)q * step_bytes;
+        }
+      }
+      const T ks = (T)step_ratio;
+      if (bf16)
+        k3_coeff_grad<T, __nv_bfloat16><<<L.grid, L.block, 0, st>>>(
+            g, lambda_ex, lambda_ey, lambda_ez, (const __nv_bfloat16 *)src[0],
+            (const __nv_bfloat16 *)src[1], (const __nv_bfloat16 *)src[2],
+            (const __nv_bfloat16 *)src[3], (const __nv_bfloat16 *)src[4],
+            (const __nv_bfloat16 *)src[5], grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
+      else
+        k3_coeff_grad<T, T><<<L.grid, L.block, 0, st>>>(
+            g, lambda_ex, lambda_ey, lambda_ez, (const T *)src[0], (const T *)src[1],
+            (const T *)src[2], (const T *)src[3], (const T *)src[4], (const T *)src[5],
+            grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
+      ++launches;
+    }
+    std::swap(cur, nxt);
+  }
+  for (int m = 0; m < 12; ++m)
+    if (cur.m[m] != lm[m]) {
+      const int axis_of[12] = {0, 1, 2, 0, 1, 2, 1, 0, 0, 2, 2, 1};
+      if (TB_CUDA(cudaMemcpyAsync(lm[m], cur.m[m], sizeof(T) * L.mem_size[axis_of[m]],
+                                  cudaMemcpyDeviceToDevice, st)))
+        return;
+    }
+  if (shot_ca) {
+    k3_combine<T><<<592, 256, 0, st>>>(grad_ca, grad_ca_shot, S_, model_n);
+    ++launches;
+  }
+  if (shot_cb) {
+    k3_combine<T><<<592, 256, 0, st>>>(grad_cb, grad_cb_shot, S_, model_n);
+    ++launches;
+  }
+  if ((grad_eps || grad_sigma) && (need_ca || need_cb)) {
+    const int64_t n = ca_batched ? tot : model_n;
+    k3_convert<T><<<592, 256, 0, st>>>(ca, cb, need_ca ? grad_ca : nullptr,
+                                       need_cb ? grad_cb : nullptr, grad_eps, grad_sigma, dt, n,
+                                       model_n, ca_batched, cb_batched);
+    ++launches;
+  }
+  count_launches(launches);
+  if (TB_CUDA(cudaGetLastError())) return;
+  if ((need_ca || need_cb) && storage_mode == 1) TB_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+}  // namespace tb
+
+#define TB3_DEFINE(S, T)                                                                   \
+  extern "C" void maxwell_3d_##S##_##T##_forward_cuda(TIDE_3D_FORWARD_ARGS(T)) {           \
+    tb::em3d_forward<T>(                                                                   \
+        ca, cb, cq, f, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x,     \
+        m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, debye_a, debye_b,          \
+        debye_cp, pol_ex, pol_ey, pol_ez, ex_prev, ey_prev, ez_prev, r, n_poles, az, bz,   \
+        azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh, kz, kzh, ky, kyh, kx, kxh,           \
+        sources_i, receivers_i, rdz, rdy, rdx, dt, nt, n_shots, nz, ny, nx,                \
+        n_sources_per_shot, n_receivers_per_shot, step_ratio, has_dispersion, ca_batched,  \
+        cb_batched, cq_batched, start_t, pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1,   \
+        source_component, receiver_component, n_threads, device, execution_backend,        \
+        compute_stream);                                                                   \
+  }                                                                                        \
+  extern "C" void maxwell_3d_##S##_##T##_forward_with_storage_cuda(                        \
+      TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {                                              \
+    tb::em3d_forward_with_storage<T>(                                                      \
+        ca, cb, cq, f, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x,     \
+        m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, r, ex_s1, ex_s3, ex_fn,    \
+        ey_s1, ey_s3, ey_fn, ez_s1, ez_s3, ez_fn, cx_s1, cx_s3, cx_fn, cy_s1, cy_s3,       \
+        cy_fn, cz_s1, cz_s3, cz_fn, az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,  \
+        kz, kzh, ky, kyh, kx, kxh, sources_i, receivers_i, rdz, rdy, rdx, dt, nt, n_shots, \
+        nz, ny, nx, n_sources_per_shot, n_receivers_per_shot, step_ratio, storage_mode,    \
+        storage_format, shot_bytes_uncomp, ca_requires_grad, cb_requires_grad, ca_batched, \
+        cb_batched, cq_batched, start_t, pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1,   \
+        source_component, receiver_component, n_threads, device, execution_backend,        \
+        compute_stream, storage_stream);                                                   \
+  }                                                                                        \
+  extern "C" void maxwell_3d_##S##_##T##_backward_cuda(TIDE_3D_BACKWARD_ARGS(T)) {         \
+    tb::em3d_backward<T>(                                                                  \
+        ca, cb, cq, grad_r, lambda_ex, lambda_ey, lambda_ez, lambda_hx, lambda_hy,         \
+        lambda_hz, m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,             \
+        m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z, m_lambda_hx_z,         \
+        m_lambda_hz_x, m_lambda_hy_x, m_lambda_hx_y, adjoint_memory_scratch, ex_s1, ex_s3, \
+        ex_fn, ey_s1, ey_s3, ey_fn, ez_s1, ez_s3, ez_fn, cx_s1, cx_s3, cx_fn, cy_s1,       \
+        cy_s3, cy_fn, cz_s1, cz_s3, cz_fn, grad_f, grad_ca, grad_cb, grad_eps, grad_sigma, \
+        grad_ca_shot, grad_cb_shot, zero_grad_on_entry, az, bz, azh, bzh, ay, by, ayh,     \
+        byh, ax, bx, axh, bxh, kz, kzh, ky, kyh, kx, kxh, sources_i, receivers_i, rdz,     \
+        rdy, rdx, dt, nt, n_shots, nz, ny, nx, n_sources_per_shot, n_receivers_per_shot,   \
+        step_ratio, storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad,     \
+        cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t, pml_z0, pml_y0,     \
+        pml_x0, pml_z1, pml_y1, pml_x1, source_component, receiver_component, n_threads,   \
+        device, execution_backend, compute_stream, storage_stream);                        \
+  }
+
+TB3_DEFINE(2, float)
+TB3_DEFINE(2, double)

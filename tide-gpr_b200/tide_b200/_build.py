@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
 ]
-SOURCES = ["tb_common.cu", "tm2d_abi.cu"]
+SOURCES = ["tb_common.cu", "tm2d_abi.cu", "em3d.cu"]
 
 
 def nvcc() -> str:

@@ -53,7 +53,31 @@ SPECS: dict[str, list] = {
     ],
 }
 
+_3D_TAIL = [(_FLOAT, 3), (_FLOAT, 1), (_I, 1), (_I, 1), (_I, 3), (_I, 2), (_I, 1)]
+_3D_FLAGS = [(_B, 3), (_I, 1), (_I, 6), (_I, 2), (_I, 1), (_I, 1), (_I, 1)]
+_3D_STORAGE = [(_I, 3), (_B, 2)]
+_3D_PROFILES = [(_P, 12), (_P, 6), (_P, 2)]
+_3D_FIELDS = [(_P, 6), (_P, 12)]
+SPECS.update({
+    # src/tide/backend_utils.py:484-504
+    "maxwell_3d_forward": [
+        (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 9), (_P, 1), (_I, 1), *_3D_PROFILES, *_3D_TAIL,
+        (_B, 1), *_3D_FLAGS, (_P, 1),
+    ],
+    # src/tide/backend_utils.py:506-524
+    "maxwell_3d_forward_with_storage": [
+        (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), *_3D_PROFILES, *_3D_TAIL,
+        *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
+    ],
+    # src/tide/backend_utils.py:537-556
+    "maxwell_3d_backward": [
+        (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 4), (_P, 2), (_B, 1),
+        *_3D_PROFILES, *_3D_TAIL, *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
+    ],
+})
+
 ACCURACIES = (2, 4, 6, 8)
+ACCURACIES_3D = (2,)
 DTYPES = {torch.float32: "float", torch.float64: "double"}
 PASSES = ("forward", "forward_with_storage", "backward")
 
@@ -102,8 +126,9 @@ def get_backend_function(
         )
     if not torch.cuda.is_available():
         raise NativeError("CUDA is not available; libtide_b200 cannot run.")
-    if accuracy not in ACCURACIES:
-        raise ValueError(f"Unsupported accuracy {accuracy}; supported: {ACCURACIES}")
+    supported = ACCURACIES_3D if propagator == "maxwell_3d" else ACCURACIES
+    if accuracy not in supported:
+        raise ValueError(f"Unsupported accuracy {accuracy} for {propagator}; supported: {supported}")
     if dtype not in DTYPES:
         raise TypeError(f"Unsupported dtype {dtype}")
     lib = load()
@@ -150,6 +175,11 @@ def exported_symbols() -> list[str]:
     names = [
         symbol_name("maxwell_tm", p, a, d)
         for a in ACCURACIES
+        for d in ("float", "double")
+        for p in PASSES
+    ] + [
+        symbol_name("maxwell_3d", p, a, d)
+        for a in ACCURACIES_3D
         for d in ("float", "double")
         for p in PASSES
     ]

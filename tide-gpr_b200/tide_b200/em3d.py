@@ -1,0 +1,386 @@
+"""3-D Maxwell (Yee) propagation on libtide_b200.so (stencil order 2).
+
+Mirrors the reference's 3-D operator path (src/tide/maxwell/maxwell3d.py:
+200-951 and maxwell3d_cuda.py:27-921): coordinate order [z, y, x]; models
+padded by fd_pad + CPML width per side ([p, p-1] per axis, replicate);
+sources / receivers as flat indices on the padded grid; source amplitudes
+scaled by -cb / (dz dy dx) at the source cell; CPML memories held compact
+along their own axis (the layout the native ABI takes); an autograd
+Function whose backward is the library's exact adjoint.  There is no CPU
+path: CPU tensors raise.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Sequence
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _native as nat
+from . import physics as ph
+from . import storage as stg
+
+COMPONENTS = {"ex": 0, "ey": 1, "ez": 2}
+# Axis (0 z, 1 y, 2 x) of each forward CPML memory, ABI order:
+# m_hz_y m_hy_z m_hx_z m_hz_x m_hy_x m_hx_y m_ey_z m_ez_y m_ez_x m_ex_z m_ex_y m_ey_x
+MEM_AXES = (1, 0, 0, 2, 2, 1, 0, 1, 2, 0, 1, 2)
+MEM_NAMES = ("m_hz_y", "m_hy_z", "m_hx_z", "m_hz_x", "m_hy_x", "m_hx_y",
+             "m_ey_z", "m_ez_y", "m_ez_x", "m_ex_z", "m_ex_y", "m_ey_x")
+# Adjoint memories, ABI order: ey_z ez_y ez_x ex_z ex_y ey_x hz_y hy_z hx_z hz_x hy_x hx_y
+ADJ_MEM_AXES = (0, 1, 2, 0, 1, 2, 1, 0, 0, 2, 2, 1)
+PROFILE_ORDER = ("az", "bz", "azh", "bzh", "ay", "by", "ayh", "byh", "ax", "bx", "axh", "bxh",
+                 "kz", "kzh", "ky", "kyh", "kx", "kxh")
+
+
+@dataclass
+class CompactLayout:
+    """CPML memory kept only on cells c < c0 and c >= max(c0, c1 - 1) of its
+    axis (src/tide/grid_utils.py:96-150)."""
+
+    shots: int
+    shape: tuple[int, int, int]
+    bounds: tuple[tuple[int, int], ...]
+
+    def extent(self, axis: int) -> int:
+        lo, hi = self.bounds[axis]
+        return lo + self.shape[axis] - max(lo, hi - 1)
+
+    def full_shape(self) -> tuple[int, ...]:
+        return (self.shots, *self.shape)
+
+    def compact_shape(self, axis: int) -> tuple[int, ...]:
+        s = list(self.full_shape())
+        s[axis + 1] = self.extent(axis)
+        return tuple(s)
+
+    def coords(self, axis: int, device=None) -> torch.Tensor:
+        lo, hi = self.bounds[axis]
+        n = self.shape[axis]
+        return torch.cat([torch.arange(lo, device=device), torch.arange(max(lo, hi - 1), n, device=device)])
+
+    def zeros(self, axis: int, device, dtype) -> torch.Tensor:
+        return torch.zeros(self.compact_shape(axis), device=device, dtype=dtype)
+
+    def pack(self, full: torch.Tensor, axis: int) -> torch.Tensor:
+        return full.index_select(axis + 1, self.coords(axis, full.device)).contiguous()
+
+    def unpack(self, compact: torch.Tensor, axis: int) -> torch.Tensor:
+        out = torch.zeros(self.full_shape(), device=compact.device, dtype=compact.dtype)
+        return out.index_copy(axis + 1, self.coords(axis, compact.device), compact)
+
+
+@dataclass
+class EM3DProblem:
+    """Everything one native 3-D call needs (padded grid)."""
+
+    ca: torch.Tensor
+    cb: torch.Tensor
+    cq: torch.Tensor
+    f: torch.Tensor
+    profiles: dict
+    sources_i: torch.Tensor
+    receivers_i: torch.Tensor
+    fields: list
+    memories: list
+    layout: CompactLayout
+    rdz: float
+    rdy: float
+    rdx: float
+    dt: float
+    nt: int
+    n_shots: int
+    nz: int
+    ny: int
+    nx: int
+    n_src: int
+    n_rec: int
+    pml: tuple  # z0, y0, x0, z1, y1, x1
+    batched: bool
+    src_comp: int
+    rec_comp: int
+    grad_interval: int
+    fd_pad: list
+    pml_width: list
+    dtype: torch.dtype
+    device: torch.device
+    models: dict = field(default_factory=dict)
+
+
+def _widths(pml_width: int | Sequence[int]) -> list[int]:
+    if isinstance(pml_width, int):
+        return [pml_width] * 6
+    w = [int(v) for v in pml_width]
+    if len(w) == 3:
+        return [w[0], w[0], w[1], w[1], w[2], w[2]]
+    if len(w) != 6:
+        raise ValueError("pml_width must be an int or 3 / 6 values [z0, z1, y0, y1, x0, x1]")
+    return w
+
+
+def _spacing(h: float | Sequence[float]) -> list[float]:
+    if isinstance(h, (int, float)):
+        return [float(h)] * 3
+    v = [float(x) for x in h]
+    if len(v) != 3:
+        raise ValueError("grid_spacing must be a float or [dz, dy, dx]")
+    return v
+
+
+def _pad3(t: torch.Tensor, pad: Sequence[int], mode: str) -> torch.Tensor:
+    """Pad a [nz, ny, nx] or [B, nz, ny, nx] tensor by [z0, z1, y0, y1, x0, x1]."""
+    squeeze = t.ndim == 3
+    x = t.unsqueeze(0) if squeeze else t
+    x = torch.nn.functional.pad(x.unsqueeze(1), (pad[4], pad[5], pad[2], pad[3], pad[0], pad[1]),
+                                mode=mode).squeeze(1)
+    return x.squeeze(0) if squeeze else x
+
+
+def prepare_em3d(
+    epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
+    grid_spacing: float | Sequence[float], dt: float,
+    source_amplitude: torch.Tensor | None, source_location: torch.Tensor | None,
+    receiver_location: torch.Tensor | None, *, stencil: int = 2,
+    pml_width: int | Sequence[int] = 20, source_component: str = "ey",
+    receiver_component: str = "ey", model_gradient_sampling_interval: int = 1,
+    nt: int | None = None,
+) -> EM3DProblem:
+    """Pad the model, build coefficients, CPML profiles, point indices and the
+    zero initial state (maxwell3d_cuda.py:310-528)."""
+    if stencil != 2:
+        raise ValueError("the 3-D path is built for stencil order 2")
+    if epsilon.ndim not in (3, 4) or sigma.shape != epsilon.shape or mu.shape != epsilon.shape:
+        raise ValueError("epsilon, sigma, mu must share a [nz, ny, nx] or [S, nz, ny, nx] shape")
+    if source_component not in COMPONENTS or receiver_component not in COMPONENTS:
+        raise ValueError("components must be 'ex', 'ey' or 'ez'")
+    device, dtype = epsilon.device, epsilon.dtype
+    batched = epsilon.ndim == 4
+    dz, dy, dx = _spacing(grid_spacing)
+    widths = _widths(pml_width)
+    fd = [1, 0, 1, 0, 1, 0]
+    pad = [a + b for a, b in zip(fd, widths)]
+    mz, my, mx = epsilon.shape[-3:]
+    nz, ny, nx = mz + pad[0] + pad[1], my + pad[2] + pad[3], mx + pad[4] + pad[5]
+    pml = (fd[0] + widths[0], fd[2] + widths[2], fd[4] + widths[4],
+           nz - fd[1] - widths[1], ny - fd[3] - widths[3], nx - fd[5] - widths[5])
+    eps_p, sig_p, mu_p = (_pad3(t, pad, "replicate") for t in (epsilon, sigma, mu))
+    coef = ph.compile_material_coefficients(eps_p, sig_p, mu_p, dt)
+    ca, cb, cq = coef["ca"], coef["cb"], coef["cq"]
+    if source_amplitude is not None and source_amplitude.numel() > 0:
+        S = source_amplitude.shape[0]
+    elif source_location is not None and source_location.numel() > 0:
+        S = source_location.shape[0]
+    elif receiver_location is not None and receiver_location.numel() > 0:
+        S = receiver_location.shape[0]
+    else:
+        S = epsilon.shape[0] if batched else 1
+    if nt is None:
+        if source_amplitude is None or source_amplitude.numel() == 0:
+            raise ValueError("nt is needed when there are no source amplitudes")
+        nt = int(source_amplitude.shape[-1])
+
+    def flat(loc):
+        if loc is None or loc.numel() == 0:
+            return torch.empty(0, device=device, dtype=torch.long), 0
+        loc = loc.to(device)
+        z, y, x = loc[..., 0] + pad[0], loc[..., 1] + pad[2], loc[..., 2] + pad[4]
+        return ((z * ny + y) * nx + x).long().contiguous(), loc.shape[1]
+
+    sources_i, n_src = flat(source_location)
+    receivers_i, n_rec = flat(receiver_location)
+    if n_src > 0 and source_amplitude is not None and source_amplitude.numel() > 0:
+        cbf = cb.reshape(S if batched else 1, -1).expand(S, -1)
+        cb_at = cbf.gather(1, sources_i)
+        f = (source_amplitude.permute(2, 0, 1) * cb_at[None] * (-1.0 / (dx * dy * dz)))
+        f = f.reshape(-1).contiguous()
+    else:
+        f = torch.empty(0, device=device, dtype=dtype)
+    prof = ph.set_pml_profiles_3d(widths, fd, dt, [dz, dy, dx], dtype, device, nz, ny, nx)
+    layout = CompactLayout(S, (nz, ny, nx), ((pml[0], pml[3]), (pml[1], pml[4]), (pml[2], pml[5])))
+    shape = (S, nz, ny, nx)
+    fields = [torch.zeros(shape, device=device, dtype=dtype) for _ in range(6)]
+    memories = [layout.zeros(a, device, dtype) for a in MEM_AXES]
+    shp = (S, nz, ny, nx) if batched else (1, nz, ny, nx)
+    return EM3DProblem(
+        ca=ca.reshape(shp), cb=cb.reshape(shp), cq=cq.reshape(shp), f=f, profiles=prof,
+        sources_i=sources_i, receivers_i=receivers_i, fields=fields, memories=memories,
+        layout=layout, rdz=1.0 / dz, rdy=1.0 / dy, rdx=1.0 / dx, dt=float(dt), nt=int(nt),
+        n_shots=int(S), nz=nz, ny=ny, nx=nx, n_src=int(n_src), n_rec=int(n_rec), pml=pml,
+        batched=batched, src_comp=COMPONENTS[source_component],
+        rec_comp=COMPONENTS[receiver_component],
+        grad_interval=int(model_gradient_sampling_interval), fd_pad=fd, pml_width=widths,
+        dtype=dtype, device=device, models={"epsilon": eps_p, "sigma": sig_p, "mu": mu_p},
+    )
+
+
+# ----------------------------------------------------------------- native calls
+def _p(t):
+    return nat.ptr(t)
+
+
+def _profile_ptrs(pb: EM3DProblem) -> list[int]:
+    return [_p(pb.profiles[k]) for k in PROFILE_ORDER]
+
+
+def _tail(pb: EM3DProblem, nt: int, step_ratio: int) -> list:
+    return [pb.rdz, pb.rdy, pb.rdx, pb.dt, nt, pb.n_shots, pb.nz, pb.ny, pb.nx, pb.n_src,
+            pb.n_rec, step_ratio]
+
+
+def _flags(pb: EM3DProblem, start_t: int) -> list:
+    b = pb.batched
+    return [b, b, b, start_t, *pb.pml, pb.src_comp, pb.rec_comp, 0,
+            pb.device.index or 0, 0]
+
+
+def native_forward(pb: EM3DProblem, ca, cb, f, r, start_t: int, nt: int) -> None:
+    fn = nat.get_backend_function("maxwell_3d", "forward", 2, pb.dtype, pb.device)
+    stream = torch.cuda.current_stream(pb.device).cuda_stream
+    fn(_p(ca), _p(cb), _p(pb.cq), _p(f), *[_p(t) for t in pb.fields],
+       *[_p(t) for t in pb.memories], *([0] * 9), _p(r), 0, *_profile_ptrs(pb),
+       _p(pb.sources_i), _p(pb.receivers_i), *_tail(pb, nt, 1), False, *_flags(pb, start_t),
+       stream)
+    nat.check("maxwell_3d forward")
+
+
+@dataclass
+class Snapshots3D:
+    mode: int
+    fmt: int
+    n_store: int
+    shot_bytes: int
+    dev: list  # 6 device buffers (or empty)
+    host: list  # 6 pinned host histories (cpu mode)
+
+
+def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need_cb: bool) -> Snapshots3D:
+    k = max(1, pb.grad_interval)
+    n_store = (pb.nt + k - 1) // k
+    sdt = torch.bfloat16 if fmt == 1 else pb.dtype
+    esz = torch.tensor([], dtype=sdt).element_size()
+    shot_bytes = pb.nz * pb.ny * pb.nx * esz
+    empty = torch.empty(0, device=pb.device, dtype=sdt)
+    need = [need_ca] * 3 + [need_cb] * 3
+    dev, host = [], []
+    for c in range(6):
+        if not need[c] or mode == stg.STORAGE_NONE:
+            dev.append(empty)
+            host.append(torch.empty(0, dtype=sdt))
+        elif mode == stg.STORAGE_DEVICE:
+            dev.append(torch.empty((n_store, pb.n_shots, pb.nz, pb.ny, pb.nx), device=pb.device, dtype=sdt))
+            host.append(torch.empty(0, dtype=sdt))
+        else:
+            dev.append(torch.empty((3, pb.n_shots, pb.nz, pb.ny, pb.nx), device=pb.device, dtype=sdt))
+            host.append(torch.empty((n_store, pb.n_shots, pb.nz * pb.ny * pb.nx), dtype=sdt,
+                                    pin_memory=True))
+    return Snapshots3D(mode, fmt, n_store, shot_bytes, dev, host)
+
+
+def _store_ptrs(sn: Snapshots3D) -> list[int]:
+    out = []
+    for c in range(6):
+        out += [_p(sn.dev[c]), _p(sn.host[c]), 0]
+    return out
+
+
+def native_forward_storage(pb: EM3DProblem, ca, cb, f, r, sn: Snapshots3D, need_ca: bool,
+                           need_cb: bool, start_t: int = 0, nt: int | None = None) -> None:
+    nt = pb.nt if nt is None else nt
+    fn = nat.get_backend_function("maxwell_3d", "forward_with_storage", 2, pb.dtype, pb.device)
+    stream = torch.cuda.current_stream(pb.device).cuda_stream
+    fn(_p(ca), _p(cb), _p(pb.cq), _p(f), *[_p(t) for t in pb.fields],
+       *[_p(t) for t in pb.memories], _p(r), *_store_ptrs(sn), *_profile_ptrs(pb),
+       _p(pb.sources_i), _p(pb.receivers_i), *_tail(pb, nt, max(1, pb.grad_interval)),
+       sn.mode, sn.fmt, sn.shot_bytes, need_ca, need_cb, *_flags(pb, start_t), stream, stream)
+    nat.check("maxwell_3d forward_with_storage")
+
+
+def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: bool,
+                    need_cb: bool, need_f: bool, *, grad_eps=None, grad_sigma=None,
+                    lam=None, start_t: int | None = None, nt: int | None = None):
+    """Exact adjoint; returns (grad_ca, grad_cb, grad_f) with grad_ca/cb
+    shaped like ca/cb, grad_f [nt * S * n_src]."""
+    dev, dt_ = pb.device, pb.dtype
+    S, nz, ny, nx = pb.n_shots, pb.nz, pb.ny, pb.nx
+    nt_all = pb.nt
+    nt = nt_all if nt is None else nt
+    start_t = nt_all if start_t is None else start_t
+    shape = (S, nz, ny, nx)
+    if lam is None:
+        lam = {"fields": [torch.zeros(shape, device=dev, dtype=dt_) for _ in range(6)],
+               "mem": [pb.layout.zeros(a, dev, dt_) for a in ADJ_MEM_AXES]}
+    scratch = torch.empty(sum(m.numel() for m in lam["mem"]), device=dev, dtype=dt_)
+    empty = torch.empty(0, device=dev, dtype=dt_)
+    mshape = ca.shape
+    grad_ca = torch.zeros(mshape, device=dev, dtype=dt_) if need_ca else empty
+    grad_cb = torch.zeros(mshape, device=dev, dtype=dt_) if need_cb else empty
+    shot_ca = torch.empty(shape, device=dev, dtype=dt_) if need_ca and not pb.batched and S > 1 else empty
+    shot_cb = torch.empty(shape, device=dev, dtype=dt_) if need_cb and not pb.batched and S > 1 else empty
+    grad_f = (torch.zeros(nt_all * S * pb.n_src, device=dev, dtype=dt_)
+              if need_f and pb.n_src > 0 else empty)
+    fn = nat.get_backend_function("maxwell_3d", "backward", 2, dt_, dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    fn(_p(ca), _p(cb), _p(pb.cq), _p(grad_r), *[_p(t) for t in lam["fields"]],
+       *[_p(t) for t in lam["mem"]], _p(scratch), *_store_ptrs(sn), _p(grad_f), _p(grad_ca),
+       _p(grad_cb), _p(grad_eps), _p(grad_sigma), _p(shot_ca), _p(shot_cb), False,
+       *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
+       *_tail(pb, nt, max(1, pb.grad_interval)), sn.mode, sn.fmt, sn.shot_bytes, need_ca,
+       need_cb, *_flags(pb, start_t), stream, stream)
+    nat.check("maxwell_3d backward")
+    return grad_ca, grad_cb, grad_f
+
+
+class EM3DPropagate(torch.autograd.Function):
+    """Receivers from (ca, cb, f); backward through the exact adjoint."""
+
+    @staticmethod
+    def forward(ctx, ca, cb, f, pb: EM3DProblem, mode: int, fmt: int):
+        need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
+        if need_ca or need_cb or ctx.needs_input_grad[2]:
+            sn = allocate_snapshots(pb, mode, fmt, need_ca, need_cb)
+            native_forward_storage(pb, ca, cb, f, r, sn, need_ca, need_cb)
+            ctx.pb, ctx.sn = pb, sn
+            ctx.flags = (need_ca, need_cb, ctx.needs_input_grad[2])
+            ctx.save_for_backward(ca, cb)
+        else:
+            native_forward(pb, ca, cb, f, r, 0, pb.nt)
+        return r
+
+    @staticmethod
+    def backward(ctx, grad_r):
+        ca, cb = ctx.saved_tensors
+        need_ca, need_cb, need_f = ctx.flags
+        gca, gcb, gf = native_backward(ctx.pb, ca, cb, grad_r.contiguous(), ctx.sn, need_ca,
+                                       need_cb, need_f)
+        return (gca if need_ca else None, gcb if need_cb else None,
+                gf if need_f else None, None, None, None)
+
+
+def maxwell3d(
+    epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
+    grid_spacing: float | Sequence[float], dt: float,
+    source_amplitude: torch.Tensor | None, source_location: torch.Tensor | None,
+    receiver_location: torch.Tensor | None, stencil: int = 2,
+    pml_width: int | Sequence[int] = 20, nt: int | None = None,
+    model_gradient_sampling_interval: int = 1, source_component: str = "ey",
+    receiver_component: str = "ey", storage_mode: str = "device",
+    storage_compression: bool | str = False,
+):
+    """3-D Maxwell solve (src/tide/maxwell/maxwell3d.py:200-951): returns the
+    final Ex, Ey, Ez, Hx, Hy, Hz and the 12 CPML memories on the model + CPML
+    region (outer fd_pad cells removed), then the receiver data [nt, S, n_rec].
+    Differentiable in epsilon, sigma and source_amplitude."""
+    if epsilon.device.type != "cuda":
+        raise nat.NativeError("libtide_b200 runs on CUDA devices only; there is no CPU path.")
+    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
+                      receiver_location, stencil=stencil, pml_width=pml_width,
+                      source_component=source_component, receiver_component=receiver_component,
+                      model_gradient_sampling_interval=model_gradient_sampling_interval, nt=nt)
+    mode = stg.mode_code(storage_mode)
+    fmt = 1 if storage_compression in (True, "bf16") else 0
+    r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt)
+    s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
+    outs = [t[s] for t in pb.fields]
+    outs += [pb.layout.unpack(m, a)[s] for m, a in zip(pb.memories, MEM_AXES)]
+    return (*outs, r)

@@ -209,6 +209,38 @@ def set_pml_profiles(
     return out
 
 
+def set_pml_profiles_3d(
+    pml_width: Sequence[int],
+    fd_pad: Sequence[int],
+    dt: float,
+    grid_spacing: Sequence[float],
+    dtype: torch.dtype,
+    device: torch.device,
+    nz: int,
+    ny: int,
+    nx: int,
+) -> dict[str, torch.Tensor]:
+    """The eighteen 1-D profiles of the 3-D Yee grid (src/tide/staggered.py:
+    188-330): a, b, kappa on integer points and on half points (suffix h) per
+    axis; pml_width and fd_pad are [z0, z1, y0, y1, x0, x1], grid_spacing
+    [dz, dy, dx]."""
+    sizes = (nz, ny, nx)
+    max_pml = max(pml_width[2 * a + s] * grid_spacing[a] for a in range(3) for s in range(2))
+    out: dict[str, torch.Tensor] = {}
+    for a, name in enumerate("zyx"):
+        n = sizes[a]
+        ws = pml_width[2 * a:2 * a + 2]
+        ps = [fd_pad[2 * a] + ws[0], n - 1 - fd_pad[2 * a + 1] - ws[1]]
+        for suffix, start in (("", 0.0), ("h", 0.5)):
+            aa, bb, kk = cpml_profile(
+                ws, ps, max_pml, dt, n, dtype, device, start=start, grid_spacing=grid_spacing[a]
+            )
+            out[f"a{name}{suffix}"] = aa.contiguous()
+            out[f"b{name}{suffix}"] = bb.contiguous()
+            out[f"k{name}{suffix}"] = kk.contiguous()
+    return out
+
+
 # ------------------------------------------------------------------ padding
 
 
