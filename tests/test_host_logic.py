@@ -1,0 +1,54 @@
+"""Host-side policy and helpers of the TM2D / 3-D paths (CPU only)."""
+
+from __future__ import annotations
+
+import pytest
+import torch
+
+from tide_b200 import physics as ph
+from tide_b200 import storage as stg
+from tide_b200 import tm2d
+
+
+@pytest.mark.parametrize("shape,pad", [((5, 7), [2, 3, 1, 4]), ((3, 5, 7), [0, 2, 3, 0]),
+                                       ((4, 5, 6), [1, 2, 0, 3, 2, 1]),
+                                       ((2, 4, 5, 6), [3, 1, 2, 2, 1, 0])])
+def test_replicate_pad_matches_torch_and_is_deterministic(shape, pad):
+    t = torch.randn(shape, dtype=torch.float64, requires_grad=True)
+    nd = len(pad) // 2
+    order = []
+    for i in range(nd - 1, -1, -1):
+        order += [pad[2 * i], pad[2 * i + 1]]
+    x = t.reshape(1, -1, *t.shape[t.ndim - nd:])  # (batch 1, channels, *padded dims)
+    ref = torch.nn.functional.pad(x, order, mode="replicate")
+    ref = ref.reshape(*t.shape[: t.ndim - nd], *ref.shape[-nd:])
+    out = ph.replicate_pad(t, pad)
+    assert torch.equal(out, ref)
+    w = torch.randn(out.shape, dtype=torch.float64)
+    (g,) = torch.autograd.grad((out * w).sum(), t)
+    (g_ref,) = torch.autograd.grad((ref * w).sum(), t)
+    assert torch.allclose(g, g_ref, rtol=1e-13, atol=1e-13)
+
+
+def test_checkpoint_segment_length():
+    assert tm2d.checkpoint_steps(400, 1, 0) == 20  # about sqrt(nt)
+    assert tm2d.checkpoint_steps(400, 3, 10) == 12  # rounded up to the sampling interval
+    assert tm2d.checkpoint_steps(7, 2, 1) == 2
+    assert tm2d.checkpoint_steps(5, 1, 50) == 50
+
+
+def test_storage_modes():
+    assert stg.StorageMode("checkpoint") is stg.StorageMode.CHECKPOINT
+    assert stg.mode_code("cpu") == stg.STORAGE_CPU
+    with pytest.raises(ValueError):
+        stg.mode_code("tape")
+    with pytest.raises(NotImplementedError):
+        stg.resolve_mode("disk", device=torch.device("cpu"), n_store=1, n_shots=1, ny=4, nx=4,
+                         itemsize=4, n_arrays=2, bytes_limit_device=None, bytes_limit_host=None)
+    # auto: device when the history fits the device budget, else pinned host
+    kw = dict(device=torch.device("cpu"), n_store=10, n_shots=2, ny=8, nx=8, itemsize=4, n_arrays=2)
+    total = stg.history_bytes(10, 2, 8, 8, 4, 2)
+    assert stg.resolve_mode("auto", bytes_limit_device=total, bytes_limit_host=None, **kw) == stg.STORAGE_DEVICE
+    assert stg.resolve_mode("auto", bytes_limit_device=total - 1, bytes_limit_host=None, **kw) == stg.STORAGE_CPU
+    with pytest.raises(MemoryError, match="checkpoint"):
+        stg.resolve_mode("auto", bytes_limit_device=0, bytes_limit_host=0, **kw)

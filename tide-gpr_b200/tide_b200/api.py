@@ -213,6 +213,7 @@ class MaxwellTM:
             storage_mode=self.storage.mode.value, storage_compression=self.storage.compression,
             storage_bytes_limit_device=self.storage.bytes_limit_device,
             storage_bytes_limit_host=self.storage.bytes_limit_host,
+            storage_chunk_steps=self.storage.chunk_steps,
             dispersion=model.dispersion,
         )
         return ForwardResult(receiver_data=out[-1], final_state=TMState.from_tensors(out[:-1]))

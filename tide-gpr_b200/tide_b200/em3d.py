@@ -127,15 +127,6 @@ def _spacing(h: float | Sequence[float]) -> list[float]:
     return v
 
 
-def _pad3(t: torch.Tensor, pad: Sequence[int], mode: str) -> torch.Tensor:
-    """Pad a [nz, ny, nx] or [B, nz, ny, nx] tensor by [z0, z1, y0, y1, x0, x1]."""
-    squeeze = t.ndim == 3
-    x = t.unsqueeze(0) if squeeze else t
-    x = torch.nn.functional.pad(x.unsqueeze(1), (pad[4], pad[5], pad[2], pad[3], pad[0], pad[1]),
-                                mode=mode).squeeze(1)
-    return x.squeeze(0) if squeeze else x
-
-
 def prepare_em3d(
     epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
     grid_spacing: float | Sequence[float], dt: float,
@@ -163,7 +154,7 @@ def prepare_em3d(
     nz, ny, nx = mz + pad[0] + pad[1], my + pad[2] + pad[3], mx + pad[4] + pad[5]
     pml = (fd[0] + widths[0], fd[2] + widths[2], fd[4] + widths[4],
            nz - fd[1] - widths[1], ny - fd[3] - widths[3], nx - fd[5] - widths[5])
-    eps_p, sig_p, mu_p = (_pad3(t, pad, "replicate") for t in (epsilon, sigma, mu))
+    eps_p, sig_p, mu_p = (ph.replicate_pad(t, pad).contiguous() for t in (epsilon, sigma, mu))
     coef = ph.compile_material_coefficients(eps_p, sig_p, mu_p, dt)
     ca, cb, cq = coef["ca"], coef["cb"], coef["cq"]
     if source_amplitude is not None and source_amplitude.numel() > 0:

@@ -251,15 +251,35 @@ def _torch_pad_order(pad: Sequence[int]) -> list[int]:
     return out
 
 
+def replicate_pad(t: torch.Tensor, pad: Sequence[int]) -> torch.Tensor:
+    """Replicate-pad the last len(pad)//2 dims of t by pad = [lo0, hi0, lo1,
+    hi1, ...] (first padded dim first).  Built from edge slices, expand and
+    cat, so its backward (sums over the expanded edges) is deterministic on
+    the GPU, unlike the scatter-based backward of the replicate mode of
+    torch.nn.functional.pad; the forward values are the same."""
+    nd = len(pad) // 2
+    for i in range(nd):
+        dim = t.ndim - nd + i
+        lo, hi = int(pad[2 * i]), int(pad[2 * i + 1])
+        if lo == 0 and hi == 0:
+            continue
+        parts = []
+        if lo:
+            edge = t.narrow(dim, 0, 1)
+            parts.append(edge.expand(*[lo if d == dim else -1 for d in range(t.ndim)]))
+        parts.append(t)
+        if hi:
+            edge = t.narrow(dim, t.shape[dim] - 1, 1)
+            parts.append(edge.expand(*[hi if d == dim else -1 for d in range(t.ndim)]))
+        t = torch.cat(parts, dim)
+    return t
+
+
 def pad_model(t: torch.Tensor, pad: Sequence[int]) -> torch.Tensor:
     """Replicate-pad a [ny, nx] or [B, ny, nx] model by [y0, y1, x0, x1]."""
     if max(pad) == 0:
         return t.clone()
-    squeeze = t.ndim == 2
-    if squeeze:
-        t = t.unsqueeze(0)
-    out = torch.nn.functional.pad(t, _torch_pad_order(pad), mode="replicate")
-    return out.squeeze(0) if squeeze else out
+    return replicate_pad(t, pad).contiguous()
 
 
 def pad_field(

@@ -9,7 +9,13 @@ Modes and formats share the reference's integer codes
   host on a side stream while the next steps compute, and streams it back in
   the adjoint (pinned-host offload);
 * ``none`` (3): nothing stored (forward only);
-* ``auto``: ``device`` when the history fits the device budget, else ``cpu``.
+* ``auto``: ``device`` when the history fits the device budget, else ``cpu``;
+* ``checkpoint`` (this library's addition): no history; the forward keeps the
+  full state every ``storage_chunk_steps`` steps (default about sqrt(nt)) and
+  the adjoint recomputes each segment's snapshots into a segment-sized device
+  buffer, last segment first.  Memory falls from nt to about 2 sqrt(nt)
+  snapshots for one extra forward pass; the gradient is bit-identical to the
+  ``device`` mode's.
 
 Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
 (float32 fields only).  Disk spilling (mode 2) is not built in this library.
@@ -37,6 +43,7 @@ class StorageMode(StrEnum):
     DISK = "disk"
     NONE = "none"
     AUTO = "auto"
+    CHECKPOINT = "checkpoint"
 
 
 @dataclass(frozen=True, slots=True)
@@ -125,7 +132,7 @@ def resolve_mode(
         if code == STORAGE_DISK:
             raise NotImplementedError(
                 "storage_mode='disk' is not built in tide_b200; use 'device', 'cpu' "
-                "(pinned host offload) or gradient checkpointing."
+                "(pinned host offload) or 'checkpoint' (recompute segments)."
             )
         return code
     total = history_bytes(n_store, n_shots, ny, nx, itemsize, n_arrays)
@@ -138,7 +145,7 @@ def resolve_mode(
     if bytes_limit_host is not None and total > bytes_limit_host:
         raise MemoryError(
             f"snapshot history of {total / 1e9:.1f} GB exceeds both budgets; "
-            "use checkpointing (tide_b200.checkpoint)"
+            "use storage_mode='checkpoint'"
         )
     return STORAGE_CPU
 

@@ -296,7 +296,17 @@ class TMPropagate(torch.autograd.Function):
         freq = int(opts.get("callback_frequency", 1)) if fwd_cb else 0
         k = pb.grad_interval
         snaps = None
-        if need_ca or need_cb:
+        ckpt = None
+        if (need_ca or need_cb) and str(opts.get("storage_mode", "device")).lower() == "checkpoint":
+            if pb.debye is not None:
+                raise NotImplementedError(
+                    "Debye media: use tide_b200.debye for gradients (the checkpointed path "
+                    "here does not carry the polarisation state)"
+                )
+            seg_len = checkpoint_steps(nt, k, opts.get("storage_chunk_steps"))
+            ckpt = (seg_len, _run_forward_checkpointed(pb, ca, cb, f, r, seg_len, fwd_cb,
+                                                       max(1, freq)))
+        elif need_ca or need_cb:
             fmt, sdtype = stg.compression_format(opts.get("storage_compression", False), dtype)
             n_store = (nt + k - 1) // k
             mode = stg.resolve_mode(
@@ -319,6 +329,8 @@ class TMPropagate(torch.autograd.Function):
             _run_forward_plain(pb, ca, cb, f, r, fwd_cb, freq)
         ctx.pb = pb
         ctx.snaps = snaps
+        ctx.ckpt = ckpt
+        ctx.f = f.detach()
         ctx.opts = opts
         ctx.need = (need_ca, need_cb, need_f)
         ctx.save_for_backward(ca, cb)
@@ -333,9 +345,15 @@ class TMPropagate(torch.autograd.Function):
         ca, cb = ctx.saved_tensors
         need_ca, need_cb, need_f = ctx.need
         grad_r = grads[7]
-        g_ca, g_cb, g_f = _run_backward(pb, ca, cb, grad_r, ctx.snaps, need_ca, need_cb, need_f,
-                                        ctx.opts)
+        if ctx.ckpt is not None:
+            seg_len, ckpts = ctx.ckpt
+            g_ca, g_cb, g_f = _run_backward_checkpointed(pb, ca, cb, ctx.f, grad_r, ckpts, seg_len,
+                                                         need_ca, need_cb, need_f, ctx.opts)
+        else:
+            g_ca, g_cb, g_f = _run_backward(pb, ca, cb, grad_r, ctx.snaps, need_ca, need_cb,
+                                            need_f, ctx.opts)
         ctx.snaps = None
+        ctx.ckpt = None
         return g_ca, g_cb, g_f, None, None
 
 
@@ -357,101 +375,206 @@ def _fwd_state(pb: TMProblem, step: int) -> CallbackState:
     )
 
 
-def _run_forward_storage(pb, ca, cb, f, r, snaps, need_ca, need_cb, fwd_cb, freq):
+def _storage_call(pb, ca, cb, f, r_ptr, ptrs, mode, fmt, shot_bytes, need_ca, need_cb, start, n,
+                  side=None):
+    """One forward_with_storage call over steps [start, start + n); r_ptr and
+    ptrs = (ey_dev, ey_host, curl_dev, curl_host) are raw addresses."""
     fn = nat.get_backend_function(
         "maxwell_tm", "forward_with_storage", pb.stencil, pb.dtype, pb.device
     )
     ey, hx, hz, mex, mez, mhx, mhz = pb.fields
-    comp = _stream_handle(pb.device)
+    fn(
+        nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(f),
+        nat.ptr(ey), nat.ptr(hx), nat.ptr(hz), nat.ptr(mex), nat.ptr(mez), nat.ptr(mhx),
+        nat.ptr(mhz), r_ptr, ptrs[0], ptrs[1], 0, ptrs[2], ptrs[3], 0,
+        *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
+        pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec,
+        pb.grad_interval, mode, fmt, shot_bytes, need_ca, need_cb,
+        pb.batched, pb.batched, pb.batched, start,
+        pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, pb.device.index or 0,
+        _stream_handle(pb.device), int(side.cuda_stream) if side is not None else 0,
+    )
+    nat.check("maxwell_tm forward_with_storage")
+
+
+def _snap_ptrs(snaps, shift_bytes: int = 0):
+    """Raw addresses of a snapshot set; device pointers shifted back by
+    shift_bytes so that a segment-sized buffer receives the slots of a later
+    segment (the native call adds slot * step_bytes)."""
+    d = lambda t: nat.ptr(t) - shift_bytes if t is not None and t.numel() else 0  # noqa: E731
+    return (d(snaps.ey_dev), nat.ptr(snaps.ey_host), d(snaps.curl_dev), nat.ptr(snaps.curl_host))
+
+
+def _run_forward_storage(pb, ca, cb, f, r, snaps, need_ca, need_cb, fwd_cb, freq):
     side = torch.cuda.Stream(pb.device) if snaps.mode == stg.STORAGE_CPU else None
     snaps.keep.append(side)
     nt = pb.nt
     chunk = nt if not fwd_cb else max(1, freq)
     for step in range(0, nt, chunk):
         n = min(chunk, nt - step)
-        fn(
-            nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(f),
-            nat.ptr(ey), nat.ptr(hx), nat.ptr(hz), nat.ptr(mex), nat.ptr(mez), nat.ptr(mhx),
-            nat.ptr(mhz), nat.ptr(r),
-            nat.ptr(snaps.ey_dev), nat.ptr(snaps.ey_host), 0,
-            nat.ptr(snaps.curl_dev), nat.ptr(snaps.curl_host), 0,
-            *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
-            pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec,
-            pb.grad_interval, snaps.mode, snaps.fmt, snaps.shot_bytes, need_ca, need_cb,
-            pb.batched, pb.batched, pb.batched, step,
-            pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, pb.device.index or 0,
-            comp, int(side.cuda_stream) if side is not None else 0,
-        )
-        nat.check("maxwell_tm forward_with_storage")
+        _storage_call(pb, ca, cb, f, nat.ptr(r), _snap_ptrs(snaps), snaps.mode, snaps.fmt,
+                      snaps.shot_bytes, need_ca, need_cb, step, n, side)
         if fwd_cb:
             fwd_cb(_fwd_state(pb, step + n))
 
 
-def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts):
-    device, dtype = pb.device, pb.dtype
-    S, ny, nx, nt = pb.n_shots, pb.ny, pb.nx, pb.nt
-    shape = (S, ny, nx)
-    if grad_r is None or grad_r.numel() == 0:
-        grad_r = torch.zeros((nt, S, pb.n_rec), device=device, dtype=dtype)
-    grad_r = grad_r.contiguous()
-    z = lambda: torch.zeros(shape, device=device, dtype=dtype)  # noqa: E731
-    lam = [z() for _ in range(7)]
-    scratch = torch.empty((4, S, ny, nx), device=device, dtype=dtype)
-    grad_f = (
-        torch.zeros((nt, S, pb.n_src), device=device, dtype=dtype)
-        if pb.n_src > 0
-        else torch.empty(0, device=device, dtype=dtype)
+class _AdjointState:
+    """Adjoint fields, scratch and gradient accumulators of one backward pass
+    (kept across the calls of a chunked or checkpointed backward)."""
+
+    def __init__(self, pb, need_ca, need_cb):
+        device, dtype = pb.device, pb.dtype
+        S, ny, nx, nt = pb.n_shots, pb.ny, pb.nx, pb.nt
+        shape = (S, ny, nx)
+        z = lambda: torch.zeros(shape, device=device, dtype=dtype)  # noqa: E731
+        self.lam = [z() for _ in range(7)]
+        self.scratch = torch.empty((4, S, ny, nx), device=device, dtype=dtype)
+        self.grad_f = (
+            torch.zeros((nt, S, pb.n_src), device=device, dtype=dtype)
+            if pb.n_src > 0
+            else torch.empty(0, device=device, dtype=dtype)
+        )
+        empty = torch.empty(0, device=device, dtype=dtype)
+        model_shape = shape if pb.batched else (ny, nx)
+        self.grad_ca = torch.zeros(model_shape, device=device, dtype=dtype) if need_ca else empty
+        self.grad_cb = torch.zeros(model_shape, device=device, dtype=dtype) if need_cb else empty
+        self.shot_ca = torch.empty(shape, device=device, dtype=dtype) if need_ca and not pb.batched else empty
+        self.shot_cb = torch.empty(shape, device=device, dtype=dtype) if need_cb and not pb.batched else empty
+
+    def result(self, pb, need_ca, need_cb, need_f):
+        g_ca = (self.grad_ca if pb.batched else self.grad_ca.unsqueeze(0)) if need_ca else None
+        g_cb = (self.grad_cb if pb.batched else self.grad_cb.unsqueeze(0)) if need_cb else None
+        g_f = self.grad_f.reshape(-1) if (need_f and pb.n_src > 0) else None
+        return g_ca, g_cb, g_f
+
+
+def _backward_call(pb, ca, cb, grad_r, st: _AdjointState, ptrs, mode, fmt, shot_bytes, need_ca,
+                   need_cb, start_t, n, side=None):
+    """One backward call over t = start_t-1 down to start_t-n."""
+    fn = nat.get_backend_function("maxwell_tm", "backward", pb.stencil, pb.dtype, pb.device)
+    fn(
+        nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(grad_r),
+        *[nat.ptr(t) for t in st.lam], nat.ptr(st.scratch),
+        ptrs[0], ptrs[1], 0, ptrs[2], ptrs[3], 0,
+        nat.ptr(st.grad_f), nat.ptr(st.grad_ca), nat.ptr(st.grad_cb), nat.ptr(st.shot_ca),
+        nat.ptr(st.shot_cb), *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
+        pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec, pb.grad_interval,
+        mode, fmt, shot_bytes, need_ca, need_cb, pb.batched, pb.batched, pb.batched, start_t,
+        pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, pb.device.index or 0,
+        _stream_handle(pb.device), int(side.cuda_stream) if side is not None else 0,
     )
-    empty = torch.empty(0, device=device, dtype=dtype)
-    model_shape = shape if pb.batched else (ny, nx)
-    grad_ca = torch.zeros(model_shape, device=device, dtype=dtype) if need_ca else empty
-    grad_cb = torch.zeros(model_shape, device=device, dtype=dtype) if need_cb else empty
-    shot_ca = torch.empty(shape, device=device, dtype=dtype) if need_ca and not pb.batched else empty
-    shot_cb = torch.empty(shape, device=device, dtype=dtype) if need_cb and not pb.batched else empty
+    nat.check("maxwell_tm backward")
+
+
+def _grad_r(pb, grad_r):
+    if grad_r is None or grad_r.numel() == 0:
+        return torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
+    return grad_r.contiguous()
+
+
+def _adjoint_callback(pb, st: _AdjointState, bwd_cb, step, need_ca, need_cb):
+    names = ("lambda_Ey", "lambda_Hx", "lambda_Hz", "m_lambda_Ey_x", "m_lambda_Ey_z",
+             "m_lambda_Hx_z", "m_lambda_Hz_x")
+    grads = {}
+    if need_ca:
+        grads["ca"] = st.grad_ca
+    if need_cb:
+        grads["cb"] = st.grad_cb
+    bwd_cb(CallbackState(
+        dt=pb.dt, step=step, nt=pb.nt, wavefields=dict(zip(names, st.lam)), models=pb.models,
+        gradients=grads, fd_pad=list(pb.fd_pad), pml_width=list(pb.pml_width), is_backward=True,
+    ))
+
+
+def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts):
+    grad_r = _grad_r(pb, grad_r)
+    nt = pb.nt
+    st = _AdjointState(pb, need_ca, need_cb)
     mode = snaps.mode if snaps is not None else stg.STORAGE_NONE
     fmt = snaps.fmt if snaps is not None else 0
     shot_bytes = snaps.shot_bytes if snaps is not None else 0
-    side = torch.cuda.Stream(device) if mode == stg.STORAGE_CPU else None
-    fn = nat.get_backend_function("maxwell_tm", "backward", pb.stencil, dtype, device)
+    ptrs = _snap_ptrs(snaps) if snaps is not None else (0, 0, 0, 0)
+    side = torch.cuda.Stream(pb.device) if mode == stg.STORAGE_CPU else None
     bwd_cb: Callback | None = opts.get("backward_callback")
-    k = pb.grad_interval
     freq = int(opts.get("callback_frequency", 1)) if bwd_cb else 0
-    # Backward chunks end on storage boundaries so each call images whole steps.
     chunk = nt if not bwd_cb else max(1, freq)
-    ends = list(range(nt, 0, -chunk))
-    for start_t in ends:
+    for start_t in range(nt, 0, -chunk):
         n = min(chunk, start_t)
-        fn(
-            nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(grad_r),
-            *[nat.ptr(t) for t in lam], nat.ptr(scratch),
-            nat.ptr(snaps.ey_dev if snaps else None), nat.ptr(snaps.ey_host if snaps else None), 0,
-            nat.ptr(snaps.curl_dev if snaps else None), nat.ptr(snaps.curl_host if snaps else None), 0,
-            nat.ptr(grad_f), nat.ptr(grad_ca), nat.ptr(grad_cb), nat.ptr(shot_ca), nat.ptr(shot_cb),
-            *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
-            pb.rdy, pb.rdx, pb.dt, n, S, ny, nx, pb.n_src, pb.n_rec, k, mode, fmt, shot_bytes,
-            need_ca and snaps is not None, need_cb and snaps is not None,
-            pb.batched, pb.batched, pb.batched, start_t,
-            pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, device.index or 0,
-            _stream_handle(device), int(side.cuda_stream) if side is not None else 0,
-        )
-        nat.check("maxwell_tm backward")
+        _backward_call(pb, ca, cb, grad_r, st, ptrs, mode, fmt, shot_bytes,
+                       need_ca and snaps is not None, need_cb and snaps is not None, start_t, n,
+                       side)
         if bwd_cb:
-            names = ("lambda_Ey", "lambda_Hx", "lambda_Hz", "m_lambda_Ey_x", "m_lambda_Ey_z",
-                     "m_lambda_Hx_z", "m_lambda_Hz_x")
-            grads = {}
-            if need_ca:
-                grads["ca"] = grad_ca
-            if need_cb:
-                grads["cb"] = grad_cb
-            bwd_cb(CallbackState(
-                dt=pb.dt, step=start_t - n, nt=nt, wavefields=dict(zip(names, lam)),
-                models=pb.models, gradients=grads, fd_pad=list(pb.fd_pad),
-                pml_width=list(pb.pml_width), is_backward=True,
-            ))
-    g_ca = (grad_ca if pb.batched else grad_ca.unsqueeze(0)) if need_ca else None
-    g_cb = (grad_cb if pb.batched else grad_cb.unsqueeze(0)) if need_cb else None
-    g_f = grad_f.reshape(-1) if (need_f and pb.n_src > 0) else None
-    return g_ca, g_cb, g_f
+            _adjoint_callback(pb, st, bwd_cb, start_t - n, need_ca, need_cb)
+    return st.result(pb, need_ca, need_cb, need_f)
+
+
+def checkpoint_steps(nt: int, k: int, requested: int | None) -> int:
+    """Segment length of the checkpointed gradient: a multiple of the
+    gradient sampling interval k, default about sqrt(nt) steps."""
+    seg = int(requested or 0) or max(1, int(round(nt ** 0.5)))
+    return max(k, (seg + k - 1) // k * k)
+
+
+def _run_forward_checkpointed(pb, ca, cb, f, r, seg_len, fwd_cb=None, freq=0):
+    """Plain forward that keeps the full state (fields and CPML memories) at
+    the start of every segment of seg_len steps."""
+    ckpts = []
+    step = 0
+    while step < pb.nt:
+        if step % seg_len == 0:
+            ckpts.append([t.clone() for t in pb.fields])
+        end = min(pb.nt, (step // seg_len + 1) * seg_len)
+        if fwd_cb:
+            end = min(end, (step // freq + 1) * freq)
+        native_forward(pb, ca, cb, f, r, step, end - step)
+        step = end
+        if fwd_cb and (step % freq == 0 or step == pb.nt):
+            fwd_cb(_fwd_state(pb, step))
+    return ckpts
+
+
+def _run_backward_checkpointed(pb, ca, cb, f, grad_r, ckpts, seg_len, need_ca, need_cb, need_f,
+                               opts):
+    """Checkpoint-and-recompute gradient: for each segment, last first, the
+    forward is recomputed from its checkpoint with the segment's snapshots in
+    a segment-sized device buffer, then the adjoint runs over the segment."""
+    grad_r = _grad_r(pb, grad_r)
+    final = [t.clone() for t in pb.fields]
+    st = _AdjointState(pb, need_ca, need_cb)
+    k = pb.grad_interval
+    fmt, sdtype = stg.compression_format(opts.get("storage_compression", False), pb.dtype)
+    n_slots = (seg_len + k - 1) // k
+    snaps = stg.allocate(stg.STORAGE_DEVICE, sdtype, fmt, n_slots, pb.n_shots, pb.ny, pb.nx,
+                         pb.device, need_ca, need_cb)
+    step_bytes = snaps.shot_bytes * pb.n_shots
+    r_seg = torch.empty((seg_len, pb.n_shots, max(pb.n_rec, 1)), device=pb.device, dtype=pb.dtype)
+    r_step_bytes = pb.n_shots * pb.n_rec * r_seg.element_size()
+    bwd_cb: Callback | None = opts.get("backward_callback")
+    freq = max(1, int(opts.get("callback_frequency", 1))) if bwd_cb else 0
+    for idx in range(len(ckpts) - 1, -1, -1):
+        seg = idx * seg_len
+        n = min(seg_len, pb.nt - seg)
+        for dst, src in zip(pb.fields, ckpts[idx]):
+            dst.copy_(src)
+        # the segment's slots and receivers land in segment-sized buffers: the
+        # native call indexes them by absolute step, so their bases move back
+        ptrs = _snap_ptrs(snaps, (seg // k) * step_bytes)
+        r_ptr = nat.ptr(r_seg) - seg * r_step_bytes if pb.n_rec > 0 else 0
+        _storage_call(pb, ca, cb, f, r_ptr, ptrs, stg.STORAGE_DEVICE, fmt, snaps.shot_bytes,
+                      need_ca, need_cb, seg, n)
+        end = seg + n
+        while end > seg:
+            # callbacks fall where the stored-history backward makes them:
+            # every freq steps counted down from nt, and at step 0
+            lo = max(seg, pb.nt - ((pb.nt - end) // freq + 1) * freq) if bwd_cb else seg
+            _backward_call(pb, ca, cb, grad_r, st, ptrs, stg.STORAGE_DEVICE, fmt,
+                           snaps.shot_bytes, need_ca, need_cb, end, end - lo)
+            end = lo
+            if bwd_cb and ((pb.nt - end) % freq == 0 or end == 0):
+                _adjoint_callback(pb, st, bwd_cb, end, need_ca, need_cb)
+    for dst, src in zip(pb.fields, final):
+        dst.copy_(src)
+    return st.result(pb, need_ca, need_cb, need_f)
 
 
 def propagate(pb: TMProblem, opts: dict | None = None):
@@ -499,6 +622,7 @@ def maxwelltm(
     storage_compression: bool | str = False,
     storage_bytes_limit_device: int | None = None,
     storage_bytes_limit_host: int | None = None,
+    storage_chunk_steps: int = 0,
     dispersion: ph.DebyeDispersion | None = None,
     **_unused: Any,
 ):
@@ -536,6 +660,7 @@ def maxwelltm(
         storage_compression=storage_compression,
         storage_bytes_limit_device=storage_bytes_limit_device,
         storage_bytes_limit_host=storage_bytes_limit_host,
+        storage_chunk_steps=storage_chunk_steps,
     )
     fields, r = propagate(pb, opts)
     if ratio > 1 and r.numel() > 0:
