@@ -846,3 +846,6 @@ extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(flo
   count_launches(nt * (L.has_domain ? 2 : 1));
   TB_CUDA(cudaGetLastError());
 }
+
+// Multi-job serving engine (shares this file's launch helpers and tile lists).
+#include "tm2d_serve.cuh"

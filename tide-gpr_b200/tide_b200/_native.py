@@ -171,7 +171,7 @@ def ptr(t: torch.Tensor | None) -> int:
 
 
 def exported_symbols() -> list[str]:
-    """Every symbol include/tide_b200.h declares (used by the load test)."""
+    """Every symbol include/*.h declares (used by the load test)."""
     names = [
         symbol_name("maxwell_tm", p, a, d)
         for a in ACCURACIES
@@ -190,4 +190,16 @@ def exported_symbols() -> list[str]:
         "tide_b200_clear_error",
         "tide_b200_device_status",
         "tide_b200_set_fused_threshold",
+        "tide_b200_launch_count",
+        "tide_b200_profile_enable",
+        "tide_b200_profile_read",
+        "tide_b200_profile_kind_name",
+        "maxwell_tm_2_float_forward_noalloc_cuda",
+        "tide_b200_serve_create",
+        "tide_b200_serve_destroy",
+        "tide_b200_serve_bind",
+        "tide_b200_serve_release",
+        "tide_b200_serve_plan",
+        "tide_b200_serve_run",
+        "tide_b200_serve_launches",
     ]

@@ -594,6 +594,49 @@ def propagate(pb: TMProblem, opts: dict | None = None):
     return list(pb.fields), r
 
 
+def build_problem(
+    epsilon: torch.Tensor,
+    sigma: torch.Tensor,
+    mu: torch.Tensor,
+    grid_spacing: float | Sequence[float],
+    dt: float,
+    source_amplitude: torch.Tensor | None,
+    source_location: torch.Tensor | None,
+    receiver_location: torch.Tensor | None,
+    *,
+    stencil: int = 2,
+    pml_width: int | Sequence[int] = 20,
+    max_vel: float | None = None,
+    initial_state: Sequence[torch.Tensor | None] | None = None,
+    nt: int | None = None,
+    model_gradient_sampling_interval: int = 1,
+    dispersion: ph.DebyeDispersion | None = None,
+) -> tuple[TMProblem, int]:
+    """Bounds checks, CFL sub-stepping and prepare_tm2d, as the functional
+    API does them (src/tide/maxwell/tm2d.py:258-420): returns the prepared
+    problem and the sub-step ratio (receivers are downsampled by it)."""
+    ny_m, nx_m = epsilon.shape[-2:]
+    for name, loc in (("Source", source_location), ("Receiver", receiver_location)):
+        if loc is not None and loc.numel() > 0:
+            if bool((loc[..., 0] >= ny_m).any()) or bool((loc[..., 1] >= nx_m).any()):
+                raise RuntimeError(f"{name} location out of bounds")
+    spacing = ph.normalize_spacing_2d(grid_spacing)
+    if max_vel is None:
+        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
+    inner_dt, ratio = ph.cfl_condition(spacing, dt, max_vel)
+    amp = source_amplitude
+    if ratio > 1 and amp is not None and amp.numel() > 0:
+        amp = ph.upsample(amp, ratio)
+    nt_int = nt * ratio if nt is not None else (amp.shape[-1] if amp is not None else None)
+    pb = prepare_tm2d(
+        epsilon, sigma, mu, spacing, inner_dt, amp, source_location, receiver_location,
+        stencil=stencil, pml_width=pml_width, initial_state=initial_state, nt=nt_int,
+        model_gradient_sampling_interval=model_gradient_sampling_interval,
+        dispersion=dispersion,
+    )
+    return pb, ratio
+
+
 def maxwelltm(
     epsilon: torch.Tensor,
     sigma: torch.Tensor,
@@ -634,24 +677,11 @@ def maxwelltm(
     """
     if callback_frequency <= 0:
         raise ValueError("callback_frequency must be positive")
-    ny_m, nx_m = epsilon.shape[-2:]
-    for name, loc in (("Source", source_location), ("Receiver", receiver_location)):
-        if loc is not None and loc.numel() > 0:
-            if bool((loc[..., 0] >= ny_m).any()) or bool((loc[..., 1] >= nx_m).any()):
-                raise RuntimeError(f"{name} location out of bounds")
-    spacing = ph.normalize_spacing_2d(grid_spacing)
-    if max_vel is None:
-        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
-    inner_dt, ratio = ph.cfl_condition(spacing, dt, max_vel)
-    amp = source_amplitude
-    if ratio > 1 and amp is not None and amp.numel() > 0:
-        amp = ph.upsample(amp, ratio)
-    nt_int = nt * ratio if nt is not None else (amp.shape[-1] if amp is not None else None)
-    pb = prepare_tm2d(
-        epsilon, sigma, mu, spacing, inner_dt, amp, source_location, receiver_location,
-        stencil=stencil, pml_width=pml_width,
-        initial_state=[Ey_0, Hx_0, Hz_0, m_Ey_x, m_Ey_z, m_Hx_z, m_Hz_x],
-        nt=nt_int, model_gradient_sampling_interval=model_gradient_sampling_interval,
+    pb, ratio = build_problem(
+        epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
+        receiver_location, stencil=stencil, pml_width=pml_width, max_vel=max_vel,
+        initial_state=[Ey_0, Hx_0, Hz_0, m_Ey_x, m_Ey_z, m_Hx_z, m_Hz_x], nt=nt,
+        model_gradient_sampling_interval=model_gradient_sampling_interval,
         dispersion=dispersion,
     )
     opts = dict(
@@ -668,4 +698,5 @@ def maxwelltm(
     return (*[pb.crop(t) for t in fields], r)
 
 
-__all__ = ["CallbackState", "TMProblem", "maxwelltm", "prepare_tm2d", "propagate"]
+__all__ = ["CallbackState", "TMProblem", "build_problem", "maxwelltm", "prepare_tm2d",
+           "propagate"]
