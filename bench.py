@@ -12,6 +12,11 @@ Metric: cell-updates per second (one padded cell of one shot advanced one
 internal step, forward or adjoint): 2 * 64 * 553 * 1065 * 4000 = 3.02e11 per
 step.
 
+The default run adds a "serving" object: the first --serve-jobs jobs of the
+seeded mixed-size stream (config 3) through the continuous-batching server
+(tide_b200.serve) and one after another through the per-job API, plus a
+Poisson-arrival run for p50/p99 latency.
+
 Arms:
   default          the B200 library through the public tide_b200 API.
   --impl reference the reference's own CPU backend (compiled from its sources
@@ -320,6 +325,9 @@ def run_b200(args) -> None:
             "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
         }
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_jobs > 0:
+        serving = serve_bench(args)
     if rank == 0:
         cpu = cpu_baseline(args) if not args.no_cpu_baseline else None
         line = {
@@ -337,7 +345,7 @@ def run_b200(args) -> None:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -345,6 +353,80 @@ def run_b200(args) -> None:
 
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- serving
+
+
+def serve_bench(args) -> dict:
+    """Served mixed-size stream (seeded, synthetic): the first `serve_jobs`
+    jobs of the 2000-job stream (nz, nx log-uniform, nt and shots uniform,
+    30 % forward+gradient), unchanged in size.  Three runs: all jobs queued at
+    t = 0 through the server (capacity), the same jobs one after another
+    through the per-job public API with the same plans (plain), and Poisson
+    arrivals at `serve_load` x the served capacity (p50/p99 latency)."""
+    from tide_b200 import serve as sv
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.empty_cache()
+    jobs = sv.mixed_stream(args.serve_jobs, seed=3)
+    cells = sum(j.cell_updates() for j in jobs)
+    L = lib()
+    with sv.TMServer(dev, chunk_steps=args.serve_chunk) as srv:
+        srv.serve([sv.mixed_stream(1, seed=11, nt_scale=0.02)[0]], realtime=False)  # capture
+        torch.cuda.synchronize(dev)
+        l0 = srv.launches()
+        t0 = time.perf_counter()
+        res = srv.serve(jobs, realtime=False)
+        torch.cuda.synchronize(dev)
+        t_served = time.perf_counter() - t0
+        launches = srv.launches() - l0
+        stats = dict(srv.stats)
+        plans = {j.job_id: srv.plan(j) for j in jobs}
+        budget = srv.budget
+    assert len(res) == len(jobs)
+    torch.cuda.empty_cache()
+    n_plain = min(len(jobs), args.serve_plain_jobs)
+    lp0 = L.tide_b200_launch_count()
+    t0 = time.perf_counter()
+    for j in jobs[:n_plain]:
+        sv.run_plain(j, plans[j.job_id], dev)
+    torch.cuda.synchronize(dev)
+    t_plain = time.perf_counter() - t0
+    plain_launches = L.tide_b200_launch_count() - lp0
+    cells_plain = sum(j.cell_updates() for j in jobs[:n_plain])
+    torch.cuda.empty_cache()
+    rate = args.serve_load * len(jobs) / t_served
+    stream = sv.mixed_stream(args.serve_jobs, seed=3, rate=rate)
+    with sv.TMServer(dev, chunk_steps=args.serve_chunk) as srv:
+        srv.serve([sv.mixed_stream(1, seed=11, nt_scale=0.02)[0]], realtime=False)
+        t0 = time.perf_counter()
+        res2 = srv.serve(stream, realtime=True)
+        t_stream = time.perf_counter() - t0
+    lat = [r.latency for r in res2]
+    served = cells / t_served
+    plain = cells_plain / t_plain
+    modes = {}
+    for p in plans.values():
+        modes[p.mode] = modes.get(p.mode, 0) + 1
+    return {
+        "workload": f"served mixed-size 2D TM stream, seed 3, first {len(jobs)} of 2000 jobs "
+                    "(full sizes: nz 128-1024, nx 256-2048 log-uniform, nt 1000-6000, shots 1-32, "
+                    "30 % forward+gradient), CPML 20, stencil 2, FP32",
+        "jobs": len(jobs), "cell_updates": cells,
+        "served_cell_updates_per_s": served, "served_s": t_served,
+        "plain_cell_updates_per_s": plain, "plain_s": t_plain, "plain_jobs": n_plain,
+        "served_over_plain": served / plain,
+        "poisson_rate_jobs_per_s": rate, "load": args.serve_load,
+        "stream_cell_updates_per_s": cells / t_stream,
+        "latency_p50_s": sv.percentile(lat, 50), "latency_p99_s": sv.percentile(lat, 99),
+        "latency_max_s": max(lat),
+        "chunk_steps": args.serve_chunk, "memory_budget_gb": round(budget / 1e9, 1),
+        "max_resident_groups": stats["max_resident"], "chunks": stats["chunks"],
+        "engine_launches": launches, "plain_launches": int(plain_launches), "plans": modes,
+        "timing": "wall clock around host-to-host runs (models and sources in host memory, "
+                  "results copied back), torch.cuda.synchronize at the end",
+    }
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -459,6 +541,11 @@ def main() -> None:
     ap.add_argument("--cpu-shots", type=int, default=4)
     ap.add_argument("--cpu-nt", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=32,
+                    help="jobs of the served mixed-size stream (0: skip the serving runs)")
+    ap.add_argument("--serve-plain-jobs", type=int, default=32)
+    ap.add_argument("--serve-chunk", type=int, default=32)
+    ap.add_argument("--serve-load", type=float, default=0.8)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -11,7 +11,8 @@
  * running its adjoint share the device in the same step.  The per-cell
  * arithmetic is that of the per-call kernels (the same tile functions), so a
  * job's receivers, adjoint fields and gradients are bit-identical to the
- * per-call path whatever else is resident.
+ * per-call path whatever else is resident.  Large jobs run the per-call
+ * kernels themselves on the engine's streams, next to the shared launches.
  *
  * Use: create an engine; bind each admitted job's device buffers to a slot
  * (bind builds the job's source/receiver tile lists once); before each chunk
@@ -57,6 +58,14 @@ typedef struct TideServeJob {
   int64_t storage_format;                        /* the engine's snapshot format */
 } TideServeJob;
 
+/* Plan flags. */
+enum {
+  /* the fields of this forward phase are not read after it (no checkpoint
+   * copy, no later forward from them): a large slot may run it with the
+   * fused pitched step */
+  TIDE_SERVE_FLAG_FUSED = 1
+};
+
 /* Slot phases of a chunk. */
 enum {
   TIDE_SERVE_IDLE = 0,
@@ -80,13 +89,18 @@ int64_t tide_b200_serve_release(void *engine, int64_t slot);
  * memory ping-pong pair). */
 int64_t tide_b200_serve_plan(void *engine, int64_t slot, int64_t phase, int64_t t0,
                              int64_t n_steps, void *ey_store, void *curl_store, int64_t q0,
-                             int64_t adj_parity);
+                             int64_t adj_parity, int64_t flags);
 /* Runs chunk_steps steps of every planned slot (a slot with n_steps < chunk_steps
  * idles after its own steps).  use_graph != 0 replays a captured CUDA graph of
  * the chunk.  Ordered after the work already on `stream` and before later work
  * on it; returns once enqueued. */
 int64_t tide_b200_serve_run(void *engine, int64_t chunk_steps, int64_t use_graph,
                             int64_t stream);
+/* Slots of at least direct_cells shots x cells (bound after this call; < 0:
+ * none) run the per-call kernels on their own streams instead of the shared
+ * tile walk; fused != 0 lets them use the fused forward step when planned
+ * with TIDE_SERVE_FLAG_FUSED.  Defaults: 1 << 20 cells, fused on. */
+int64_t tide_b200_serve_configure(void *engine, int64_t direct_cells, int64_t fused);
 /* Kernel launches issued by the engine so far (graph replays count their nodes). */
 int64_t tide_b200_serve_launches(void *engine);
 

@@ -134,3 +134,26 @@ def test_poisson_arrivals_realtime(cuda_device):
     for r in res:
         assert r.finished >= r.admitted >= r.arrival - 1e-9
         _check(r, ref[r.job_id], f"job {r.job_id} realtime")
+
+
+@pytest.mark.parametrize("fused_threshold", [0, -1])
+def test_direct_slots_match_table_and_plain(cuda_device, fused_threshold):
+    """Groups at or above direct_cells run the per-call kernels (pair, or the
+    fused pitched forward when allowed) on the engine's streams next to the
+    table walk of the small groups: same bits as the table walk and as the
+    per-job path."""
+    from tide_b200 import _native as nat
+
+    jobs = _jobs()
+    ref, plans, _ = _serve(jobs, direct_cells=-1)
+    old = nat.set_fused_threshold(fused_threshold)
+    try:
+        mixed, _, _ = _serve(jobs, direct_cells=3000)
+        alone, _, _ = _serve(jobs[1:2], direct_cells=3000)
+        plain = sv.run_plain(jobs[4], plans[jobs[4].job_id])
+    finally:
+        nat.set_fused_threshold(old)
+    for j in jobs:
+        _check(mixed[j.job_id], ref[j.job_id], f"job {j.job_id} direct vs table")
+    _check(alone[jobs[1].job_id], ref[jobs[1].job_id], "direct alone")
+    _check(mixed[jobs[4].job_id], plain, "direct vs plain")

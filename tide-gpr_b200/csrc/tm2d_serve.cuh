@@ -19,6 +19,16 @@
 // The work table (geometry, pointers, phase, first step, steps this chunk,
 // snapshot bases) is built on the host before each chunk in pinned memory and
 // copied to the device on the engine's stream ahead of the chunk's kernels.
+//
+// Large slots (shots x cells at or above the engine's direct threshold) do
+// not go through the table: their tiles fill the GPU on their own, and the
+// per-call kernels (parameters in the constant bank, fewer registers, and the
+// fused pitched forward step) are faster per cell than the table walk.  Each
+// runs its steps with the per-call launches on one of a pool of streams,
+// concurrently with the table chains and with the other large slots.  A
+// large slot in a forward phase whose fields are not read afterwards (the
+// plan's fused flag) keeps a pitched copy of its state for the fused
+// one-launch step from its first such chunk until it leaves the phase.
 #pragma once
 
 #include "../../include/tide_b200_serve.h"
@@ -148,6 +158,8 @@ __global__ void __launch_bounds__(256, 3) k_srv_adj_h(const SrvTable *__restrict
 
 // Host side -----------------------------------------------------------------
 
+constexpr int kSrvPool = 8;  // streams of the large slots
+
 struct SrvHostSlot {
   bool bound = false;
   SrvSlot s{};          // static part filled at bind; plan fills the rest
@@ -155,6 +167,15 @@ struct SrvHostSlot {
   int tiles[4] = {0, 0, 0, 0};  // tiles of each kind
   bool adjoint = false;
   int64_t nt = 0;
+  // large slots
+  bool direct = false;
+  int pool = 0;
+  Launch<float, 2> L{};
+  bool fused_ok = false;           // plan: fields not read after this forward phase
+  PitchedFwd *pf = nullptr;        // pitched state of the fused forward
+  PointScratch *pf_pts = nullptr;  // tile lists of the fused tiling
+  const int64_t *src_i = nullptr, *rec_i = nullptr;
+  int64_t n_src = 0, n_rec = 0;
 };
 
 struct SrvEngine {
@@ -168,6 +189,10 @@ struct SrvEngine {
   SrvTable *h_table[2] = {nullptr, nullptr};
   int cur = 0;
   int grid[4] = {0, 0, 0, 0};
+  int64_t direct_cells = (int64_t)1 << 20;  // shots x cells of a large slot (< 0: none)
+  bool fused = true;                        // fused forward step for eligible large slots
+  cudaStream_t pool[kSrvPool] = {};
+  cudaEvent_t ev_pool[kSrvPool] = {};
   std::vector<SrvHostSlot> slots;
   std::map<std::tuple<int, bool, bool>, cudaGraphExec_t> graphs;
   std::vector<std::pair<void *, cudaEvent_t>> deferred;  // released tile lists, freed when done
@@ -193,8 +218,16 @@ struct SrvEngine {
     if (sf) cudaStreamSynchronize(sf);
     if (sa) cudaStreamSynchronize(sa);
     sweep(true);
-    for (auto &s : slots)
+    for (auto &s : slots) {
+      delete s.pf;
+      delete s.pf_pts;
       if (s.points) cudaFree(s.points);
+    }
+    for (int i = 0; i < kSrvPool; ++i) {
+      if (pool[i]) cudaStreamSynchronize(pool[i]);
+      if (ev_pool[i]) cudaEventDestroy(ev_pool[i]);
+      if (pool[i]) cudaStreamDestroy(pool[i]);
+    }
     if (d_table) cudaFree(d_table);
     for (auto *h : h_table)
       if (h) cudaFreeHost(h);
@@ -225,6 +258,72 @@ void srv_enqueue(SrvEngine &E, int C, bool fwd, bool adj) {
   }
   if (TB_CUDA(cudaEventRecord(E.ev_join, E.sa))) return;
   TB_CUDA(cudaStreamWaitEvent(E.sf, E.ev_join, 0));
+}
+
+// Steps of one large slot with the per-call kernels on stream st.
+template <typename S>
+bool srv_direct(SrvHostSlot &H, cudaStream_t st, bool fused_enabled, int64_t &launches) {
+  SrvSlot &s = H.s;
+  const Launch<float, 2> &L = H.L;
+  PointScratch pe, pa;  // views of the slot's lists (own no memory)
+  pe.src = s.src_e; pe.rec = s.rec_e;
+  pa.src = s.src_ah; pa.rec = s.rec_ah; pa.rowf = s.rowf_ah;
+  const bool fwd = s.phase == TIDE_SERVE_FORWARD || s.phase == TIDE_SERVE_FORWARD_STORE;
+  const bool fused = fwd && H.fused_ok && fused_enabled && fused_pays(s.g.n_shots, s.g.N);
+  if (H.pf && !fused) {
+    // leaving the fused phase: fields back to the caller's layout when a
+    // forward follows, then the pitched copy goes
+    if (fwd && !H.pf->finish()) return false;
+    delete H.pf;
+    delete H.pf_pts;
+    H.pf = nullptr;
+    H.pf_pts = nullptr;
+  }
+  if (fused && !H.pf) {
+    H.pf = new PitchedFwd();
+    float *const fields[7] = {s.ey, s.hx, s.hz, s.m_ey_x, s.m_ey_z, s.m_hx_z, s.m_hz_x};
+    if (!H.pf->init(L.g, fields, s.ca, s.cb, s.cq, st)) return false;
+    H.pf_pts = new PointScratch();
+    if (!build_points(*H.pf_pts, L, H.pf->q.pt, H.src_i, H.n_src, H.rec_i, H.n_rec, st))
+      return false;
+  }
+  const DebyeArgs<float> db{nullptr, nullptr, nullptr, nullptr, 0};
+  for (int j = 0; j < s.n; ++j) {
+    if (fwd) {
+      const int64_t t = s.t0 + j;
+      const float *ft = s.f ? s.f + t * s.fs : nullptr;
+      float *rt = s.r ? s.r + t * s.rs : nullptr;
+      const bool store = s.phase == TIDE_SERVE_FORWARD_STORE && t % s.k == 0;
+      const int64_t off = store ? (t / s.k - s.q0) * s.shot_cells : 0;
+      S *es = store && s.ey_st ? static_cast<S *>(s.ey_st) + off : nullptr;
+      S *cs = store && s.cu_st ? static_cast<S *>(s.cu_st) + off : nullptr;
+      if (fused) {
+        H.pf->launch<S>(L.g, es, cs, *H.pf_pts, ft, rt);
+        launches += 1;
+      } else {
+        launch_fwd_h<float, 2>(L, st, s.cq, s.ey, s.hx, s.hz, s.m_ey_x, s.m_ey_z);
+        launch_fwd_e<float, 2, S>(L, st, s.ca, s.cb, s.hx, s.hz, s.ey, s.m_hx_z, s.m_hz_x, es,
+                                  cs, db, pe, ft, rt);
+        launches += 2;
+      }
+    } else {
+      const int64_t t = s.t0 - 1 - j;
+      const int c = (s.parity + j) & 1;
+      launch_adj_e<float, 2>(L, st, s.cb, s.lam_ey, s.lam_hx, s.lam_hz, s.mem[2][c], s.mem[3][c],
+                             s.mem[2][c ^ 1], s.mem[3][c ^ 1]);
+      const bool img = (s.ey_st || s.cu_st) && t % s.k == 0;
+      const int64_t off = img ? (t / s.k - s.q0) * s.shot_cells : 0;
+      const S *es = img && s.ey_st ? static_cast<const S *>(s.ey_st) + off : nullptr;
+      const S *cs = img && s.cu_st ? static_cast<const S *>(s.cu_st) + off : nullptr;
+      const GradArgs<float, S> ga{es, cs, s.grad_ca, s.grad_cb, (float)s.k, false, false};
+      launch_adj_h<float, 2, S>(L, st, s.ca, s.cq, s.lam_hx, s.lam_hz, s.lam_ey, s.mem[0][c],
+                                s.mem[1][c], s.mem[0][c ^ 1], s.mem[1][c ^ 1], pa,
+                                s.grad_r ? s.grad_r + t * s.rs : nullptr,
+                                s.grad_f ? s.grad_f + t * s.fs : nullptr, ga);
+      launches += 2;
+    }
+  }
+  return true;
 }
 
 bool srv_points(const int64_t *idx, int64_t n_per_shot, int64_t S, int64_t N, int nx,
@@ -264,6 +363,9 @@ void *tide_b200_serve_create(int64_t device, int64_t max_slots, int64_t storage_
             !TB_CUDA(cudaStreamCreateWithFlags(&E->sa, cudaStreamNonBlocking));
   for (cudaEvent_t *e : {&E->ev_in, &E->ev_fork, &E->ev_join, &E->ev_up[0], &E->ev_up[1]})
     ok = ok && !TB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (int i = 0; ok && i < kSrvPool; ++i)
+    ok = !TB_CUDA(cudaStreamCreateWithFlags(&E->pool[i], cudaStreamNonBlocking)) &&
+         !TB_CUDA(cudaEventCreateWithFlags(&E->ev_pool[i], cudaEventDisableTiming));
   ok = ok && !TB_CUDA(cudaMalloc(&E->d_table, sizeof(SrvTable)));
   for (auto *&h : E->h_table)
     ok = ok && !TB_CUDA(cudaMallocHost(&h, sizeof(SrvTable)));
@@ -367,6 +469,13 @@ int64_t tide_b200_serve_bind(void *engine, const TideServeJob *job, int64_t stre
   }
   H.adjoint = adjoint;
   H.nt = J.nt;
+  H.direct = E->direct_cells >= 0 && s.shot_cells >= E->direct_cells;
+  H.pool = slot % kSrvPool;
+  H.L = L;
+  H.src_i = J.n_src > 0 ? J.sources_i : nullptr;
+  H.rec_i = J.n_rec > 0 ? J.receivers_i : nullptr;
+  H.n_src = J.n_src;
+  H.n_rec = J.n_rec;
   if (adjoint) {
     s.lam_ey = J.lam[0]; s.lam_hx = J.lam[1]; s.lam_hz = J.lam[2];
     const size_t SN = (size_t)s.shot_cells;
@@ -433,6 +542,8 @@ int64_t tide_b200_serve_release(void *engine, int64_t slot) {
   }
   if (TB_CUDA(cudaSetDevice(E->device))) return -1;
   SrvHostSlot &H = E->slots[(size_t)slot];
+  delete H.pf;      // stream-ordered frees on the slot's pool stream
+  delete H.pf_pts;
   if (H.points) {
     // enqueued chunks may still read the slot's tile lists: free them once
     // the engine's stream has passed this point
@@ -451,7 +562,7 @@ int64_t tide_b200_serve_release(void *engine, int64_t slot) {
 
 int64_t tide_b200_serve_plan(void *engine, int64_t slot, int64_t phase, int64_t t0,
                              int64_t n_steps, void *ey_store, void *curl_store, int64_t q0,
-                             int64_t adj_parity) {
+                             int64_t adj_parity, int64_t flags) {
   using namespace tb;
   auto *E = static_cast<SrvEngine *>(engine);
   if (E == nullptr || slot < 0 || slot >= E->max_slots || !E->slots[(size_t)slot].bound) {
@@ -479,6 +590,7 @@ int64_t tide_b200_serve_plan(void *engine, int64_t slot, int64_t phase, int64_t 
   s.cu_st = (phase == TIDE_SERVE_FORWARD_STORE || phase == TIDE_SERVE_ADJOINT) ? curl_store : nullptr;
   s.q0 = (int)q0;
   s.parity = (int)(adj_parity & 1);
+  H.fused_ok = (flags & TIDE_SERVE_FLAG_FUSED) != 0;
   return 0;
 }
 
@@ -499,8 +611,13 @@ int64_t tide_b200_serve_run(void *engine, int64_t chunk_steps, int64_t use_graph
   int n = 0;
   bool any_f = false, any_a = false;
   for (int k = 0; k < 4; ++k) T.pre[k][0] = 0;
+  bool any_direct = false;
   for (auto &H : E->slots) {
     if (!H.bound || H.s.phase == TIDE_SERVE_IDLE || H.s.n <= 0) continue;
+    if (H.direct) {
+      any_direct = true;
+      continue;
+    }
     const bool adj = H.s.phase == TIDE_SERVE_ADJOINT;
     any_f = any_f || !adj;
     any_a = any_a || adj;
@@ -513,12 +630,41 @@ int64_t tide_b200_serve_run(void *engine, int64_t chunk_steps, int64_t use_graph
   }
   T.n_slots = n;
   for (int k = 0; k < 4; ++k) T.total[k] = T.pre[k][n];
-  if (n == 0) return 0;
-  for (auto &H : E->slots)  // steps are consumed: a slot runs again only when re-planned
-    if (H.bound) H.s.n = 0;
+  if (n == 0 && !any_direct) return 0;
   cudaStream_t caller = reinterpret_cast<cudaStream_t>(stream);
   if (TB_CUDA(cudaEventRecord(E->ev_in, caller))) return -1;
   if (TB_CUDA(cudaStreamWaitEvent(E->sf, E->ev_in, 0))) return -1;
+  // large slots: per-call kernels on the pool streams, after the caller's work
+  bool used[kSrvPool] = {};
+  int64_t nl_direct = 0;
+  for (auto &H : E->slots) {
+    if (!H.bound || !H.direct || H.s.phase == TIDE_SERVE_IDLE || H.s.n <= 0) continue;
+    cudaStream_t ps = E->pool[H.pool];
+    if (!used[H.pool]) {
+      if (TB_CUDA(cudaStreamWaitEvent(ps, E->ev_in, 0))) return -1;
+      used[H.pool] = true;
+    }
+    const bool ok = E->fmt ? srv_direct<__nv_bfloat16>(H, ps, E->fused, nl_direct)
+                           : srv_direct<float>(H, ps, E->fused, nl_direct);
+    if (!ok) return -1;
+  }
+  for (auto &H : E->slots)  // steps are consumed: a slot runs again only when re-planned
+    if (H.bound) H.s.n = 0;
+  auto join_pool = [&]() -> bool {
+    for (int i = 0; i < kSrvPool; ++i)
+      if (used[i] && (TB_CUDA(cudaEventRecord(E->ev_pool[i], E->pool[i])) ||
+                      TB_CUDA(cudaStreamWaitEvent(E->sf, E->ev_pool[i], 0))))
+        return false;
+    return true;
+  };
+  E->launches += nl_direct;
+  count_launches(nl_direct);
+  if (n == 0) {
+    if (!join_pool()) return -1;
+    if (TB_CUDA(cudaEventRecord(E->ev_in, E->sf))) return -1;
+    if (TB_CUDA(cudaStreamWaitEvent(caller, E->ev_in, 0))) return -1;
+    return TB_CUDA(cudaGetLastError()) ? -1 : 0;
+  }
   const size_t bytes = offsetof(SrvTable, slot) + (size_t)n * sizeof(SrvSlot);
   if (TB_CUDA(cudaMemcpyAsync(E->d_table, &T, bytes, cudaMemcpyHostToDevice, E->sf))) return -1;
   if (TB_CUDA(cudaEventRecord(E->ev_up[b], E->sf))) return -1;
@@ -547,9 +693,21 @@ int64_t tide_b200_serve_run(void *engine, int64_t chunk_steps, int64_t use_graph
   }
   E->launches += nl;
   count_launches(nl);
+  if (!join_pool()) return -1;
   if (TB_CUDA(cudaGetLastError())) return -1;
   if (TB_CUDA(cudaEventRecord(E->ev_in, E->sf))) return -1;
   if (TB_CUDA(cudaStreamWaitEvent(caller, E->ev_in, 0))) return -1;
+  return 0;
+}
+
+int64_t tide_b200_serve_configure(void *engine, int64_t direct_cells, int64_t fused) {
+  auto *E = static_cast<tb::SrvEngine *>(engine);
+  if (E == nullptr) {
+    tb::set_error(tb::kBadArgument, "serve configure: null engine");
+    return -1;
+  }
+  E->direct_cells = direct_cells;
+  E->fused = fused != 0;
   return 0;
 }
 

@@ -202,4 +202,5 @@ def exported_symbols() -> list[str]:
         "tide_b200_serve_plan",
         "tide_b200_serve_run",
         "tide_b200_serve_launches",
+        "tide_b200_serve_configure",
     ]

@@ -42,8 +42,10 @@ from . import physics as ph
 from . import storage as stg
 from . import tm2d
 
-# Slot phases (include/tide_b200_serve.h).
+# Slot phases and plan flags (include/tide_b200_serve.h).
 IDLE, FORWARD, FORWARD_STORE, ADJOINT = 0, 1, 2, 3
+FLAG_FUSED = 1
+DIRECT_CELLS = 1 << 20  # shots x cells from which a group runs the per-call kernels
 
 
 class _CJob(ctypes.Structure):
@@ -76,7 +78,8 @@ def _lib():
             "tide_b200_serve_destroy": ([P], None),
             "tide_b200_serve_bind": ([P, ctypes.POINTER(_CJob), I], I),
             "tide_b200_serve_release": ([P, I], I),
-            "tide_b200_serve_plan": ([P, I, I, I, I, P, P, I, I], I),
+            "tide_b200_serve_plan": ([P, I, I, I, I, P, P, I, I, I], I),
+            "tide_b200_serve_configure": ([P, I, I], I),
             "tide_b200_serve_run": ([P, I, I, I], I),
             "tide_b200_serve_launches": ([P], I),
         }
@@ -168,12 +171,15 @@ class JobPlan:
 def group_bytes(ny: int, nx: int, S: int, nt: int, n_src: int, n_rec: int, mode: str,
                 seg_len: int, k: int, item: int) -> int:
     """Device bytes of one resident shot group (fields, coefficients,
-    amplitudes, receivers, adjoint state, snapshots or checkpoints, and the
-    padded models kept for the gradient's chain rule)."""
+    amplitudes, receivers, adjoint state, snapshots or checkpoints, the
+    padded models kept for the gradient's chain rule, and the pitched copy of
+    a fused forward)."""
     N = ny * nx
     SN = S * N
     b = 4 * (3 * N + 7 * SN + nt * S * (n_src + n_rec)) + 8 * S * (n_src + n_rec)
     b += 4 * 12 * max(ny, nx) + 4 * 6 * N
+    if mode in ("forward", "device") and SN >= DIRECT_CELLS:
+        b += 4 * (12 * S * (ny + 2) + 3 * (ny + 2)) * (nx + 64)
     if mode == "forward":
         return b
     b += 4 * (11 * SN + nt * S * (n_rec + n_src) + 2 * N) + 4 * 6 * N
@@ -340,13 +346,16 @@ class TMServer:
     chunk (the continuous-batching granularity); use_graphs: replay a
     captured CUDA graph per chunk; storage_compression: BF16 snapshots for
     every gradient job of this server; history_limit / group_limit: planning
-    thresholds (default budget/8 and budget/4).
+    thresholds (default budget/8 and budget/4); direct_cells: shots x cells
+    from which a group runs the per-call kernels on its own stream (and, with
+    fused, the fused forward step) instead of the shared tile walk.
     """
 
     def __init__(self, device: torch.device | str = "cuda", *, memory_budget: int | None = None,
                  max_slots: int = 64, chunk_steps: int = 32, use_graphs: bool = True,
                  storage_compression: bool = False, history_limit: int | None = None,
-                 group_limit: int | None = None, max_bypass: int = 8, depth: int = 2):
+                 group_limit: int | None = None, max_bypass: int = 8, depth: int = 2,
+                 direct_cells: int = DIRECT_CELLS, fused: bool = True):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise nat.NativeError("TMServer runs on a CUDA device only")
@@ -370,6 +379,8 @@ class TMServer:
         nat.check("serve create")
         if not self.engine:
             raise nat.NativeError("serve create failed")
+        self.lib.tide_b200_serve_configure(self.engine, int(direct_cells), int(fused))
+        nat.check("serve configure")
         self.stream = torch.cuda.Stream(self.device)
         self.queue: deque[_Task] = deque()
         self.resident: list[_Task] = []
@@ -585,8 +596,12 @@ class TMServer:
             ey = cu = None
             if seg.phase in (FORWARD_STORE, ADJOINT):
                 ey, cu = (nat.ptr(s) for s in t.out["snaps"])
+            # fields of forward-only and device-history forwards are not read
+            # afterwards (checkpoint segments copy theirs)
+            flags = FLAG_FUSED if (seg.phase != ADJOINT and
+                                   t.plan.mode in ("forward", "device")) else 0
             self.lib.tide_b200_serve_plan(self.engine, t.slot, seg.phase, t0, n, ey, cu, seg.q0,
-                                          t.adj_steps)
+                                          t.adj_steps, flags)
             nat.check("serve plan")
             planned.append((t, n))
         if not planned:
