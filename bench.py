@@ -290,12 +290,12 @@ def run_b200(args) -> None:
 
     clocks = ClockSampler(dev.index or 0)
     clocks.start()
-    L.tide_b200_profile_enable(1, 32)
+    L.tide_b200_profile_enable(1 if args.profile_every > 0 else 0, max(1, args.profile_every))
     read_profile(L)
     launches0 = L.tide_b200_launch_count()
     ms, _, _ = timed(args.steps, copy_in=False)
     launches = L.tide_b200_launch_count() - launches0
-    L.tide_b200_profile_enable(0, 32)
+    L.tide_b200_profile_enable(0, 1)
     prof = read_profile(L)
     clk = clocks.stop()
     e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)
@@ -541,6 +541,9 @@ def main() -> None:
     ap.add_argument("--cpu-shots", type=int, default=4)
     ap.add_argument("--cpu-nt", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-every", type=int, default=32,
+                    help="time every n-th step's kernels with events in the timed region "
+                         "(0: off; the roofline needs it)")
     ap.add_argument("--serve-jobs", type=int, default=32,
                     help="jobs of the served mixed-size stream (0: skip the serving runs)")
     ap.add_argument("--serve-plain-jobs", type=int, default=32)

@@ -19,32 +19,43 @@
 
 namespace tb {
 
-// Block coordinates of a tile: the hardware block index for the per-call
-// kernels, a virtual one for the multi-job kernels of the serving engine.
+// Block coordinates of a tile.  The per-call kernels read them from the
+// hardware block index (HwTile: special registers, re-read where used, so they
+// hold no registers across the body); the multi-job kernels of the serving
+// engine pass a virtual tile (Tile).
 struct Tile {
-  int x, y, z, gx, gy;
+  int x_, y_, z_, gx_, gy_;
+  __device__ __forceinline__ int x() const { return x_; }
+  __device__ __forceinline__ int y() const { return y_; }
+  __device__ __forceinline__ int z() const { return z_; }
+  __device__ __forceinline__ int gx() const { return gx_; }
+  __device__ __forceinline__ int gy() const { return gy_; }
 };
-__device__ __forceinline__ Tile hw_tile() {
-  return Tile{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)gridDim.x, (int)gridDim.y};
-}
+struct HwTile {
+  __device__ __forceinline__ int x() const { return (int)blockIdx.x; }
+  __device__ __forceinline__ int y() const { return (int)blockIdx.y; }
+  __device__ __forceinline__ int z() const { return (int)blockIdx.z; }
+  __device__ __forceinline__ int gx() const { return (int)gridDim.x; }
+  __device__ __forceinline__ int gy() const { return (int)gridDim.y; }
+};
 
 // ---------------------------------------------------------------- forward H
-template <typename T, int R>
+template <typename T, int R, typename TL>
 __device__ __forceinline__ void fwd_h_tile(
-    const Tile &tl, const TMGeom<T> &g,
+    const TL tl, const TMGeom<T> &g,
     const T *__restrict__ cq, const T *__restrict__ ey, T *__restrict__ hx,
     T *__restrict__ hz, T *__restrict__ m_ey_x, T *__restrict__ m_ey_z) {
   const int nx = g.nx, ny = g.ny;
-  const int x = tl.x * kTileX + threadIdx.x + 1;
-  const int y0 = (tl.y * kBlockY + threadIdx.y) * R + 1;
+  const int x = tl.x() * kTileX + threadIdx.x + 1;
+  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R + 1;
   if (y0 >= ny || x >= nx) return;
-  const int64_t base = (int64_t)tl.z * g.N;
+  const int64_t base = (int64_t)tl.z() * g.N;
   ey += base; hx += base; hz += base; m_ey_x += base; m_ey_z += base;
   if (g.cq_b) cq += base;
   const int j0 = y0 * nx + x;
   {
     // Interior tile (block-uniform): no strip cell for H-x or H-z.
-    const int tx0 = tl.x * kTileX + 1, ty0 = tl.y * kBlockY * R + 1;
+    const int tx0 = tl.x() * kTileX + 1, ty0 = tl.y() * kBlockY * R + 1;
     if (tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1h && ty0 >= g.pml_y0 &&
         ty0 + kBlockY * R <= g.pml_y1h) {
       T e[R + 1], er[R], c[R], vx[R], vz[R];
@@ -123,23 +134,23 @@ template <typename T, int R>
 __global__ void __launch_bounds__(256)
 k2_fwd_h(TMGeom<T> g, const T *__restrict__ cq, const T *__restrict__ ey, T *__restrict__ hx,
          T *__restrict__ hz, T *__restrict__ m_ey_x, T *__restrict__ m_ey_z) {
-  fwd_h_tile<T, R>(hw_tile(), g, cq, ey, hx, hz, m_ey_x, m_ey_z);
+  fwd_h_tile<T, R>(HwTile(), g, cq, ey, hx, hz, m_ey_x, m_ey_z);
 }
 
 // ---------------------------------------------------------------- forward E
 // Full-grid tiles (32 x 8R) so point entries outside the domain are served.
-template <typename T, typename S, int R>
+template <typename T, typename S, int R, typename TL>
 __device__ __forceinline__ void fwd_e_tile(
-    const Tile &tl, const TMGeom<T> &g,
+    const TL tl, const TMGeom<T> &g,
     const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
     const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
     T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
     PointCSR src, PointCSR rec, const T *__restrict__ f_t, T *__restrict__ r_t) {
   const int nx = g.nx, ny = g.ny;
-  const int x = tl.x * kTileX + threadIdx.x;
-  const int y0 = (tl.y * kBlockY + threadIdx.y) * R;
-  const int s = tl.z;
-  const int tile = (s * tl.gy + tl.y) * tl.gx + tl.x;
+  const int x = tl.x() * kTileX + threadIdx.x;
+  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R;
+  const int s = tl.z();
+  const int tile = (s * tl.gy() + tl.y()) * tl.gx() + tl.x();
   if (y0 >= ny || x >= nx) return;
   const bool pts = !point_tile_empty(src, rec, tile);
   const int64_t base = (int64_t)s * g.N;
@@ -151,7 +162,7 @@ __device__ __forceinline__ void fwd_e_tile(
   const int j0 = y0 * nx + x;
   {
     // Interior tile (block-uniform): no strip cell, every cell in the domain.
-    const int tx0 = tl.x * kTileX, ty0 = tl.y * kBlockY * R;
+    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * kBlockY * R;
     if (tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1 && ty0 >= g.pml_y0 &&
         ty0 + kBlockY * R <= g.pml_y1) {
       T vx[R + 1], vz[R], vzl[R], eo[R], a[R], b[R];
@@ -247,7 +258,7 @@ k2_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const 
          const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
          T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
          PointCSR src, PointCSR rec, const T *__restrict__ f_t, T *__restrict__ r_t) {
-  fwd_e_tile<T, S, R>(hw_tile(), g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, ey_store, curl_store, src,
+  fwd_e_tile<T, S, R>(HwTile(), g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, ey_store, curl_store, src,
       rec, f_t, r_t);
 }
 
@@ -255,24 +266,24 @@ k2_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const 
 // raw_x(x') = q (x' in [pml_x0, pml_x1)) or ax (bx m + q) + q / kx;
 // raw_y(y') = -q (y' in [pml_y0, pml_y1)) or ay (by m - q) - q / ky; both 0
 // outside the domain (maxwell_tm_cuda_inst.cu:954-994).
-template <typename T, int R>
+template <typename T, int R, typename TL>
 __device__ __forceinline__ void adj_e_tile(
-    const Tile &tl, const TMGeom<T> &g,
+    const TL tl, const TMGeom<T> &g,
     const T *__restrict__ cb, const T *__restrict__ lam_ey,
     T *__restrict__ lam_hx, T *__restrict__ lam_hz, const T *__restrict__ m_hx_z,
     const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
   const int nx = g.nx, ny = g.ny;
-  const int x = tl.x * kTileX + threadIdx.x + 1;
-  const int y0 = (tl.y * kBlockY + threadIdx.y) * R + 1;
+  const int x = tl.x() * kTileX + threadIdx.x + 1;
+  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R + 1;
   if (y0 >= ny || x >= nx) return;
-  const int64_t base = (int64_t)tl.z * g.N;
+  const int64_t base = (int64_t)tl.z() * g.N;
   lam_ey += base; lam_hx += base; lam_hz += base;
   m_hx_z += base; m_hz_x += base; m_hx_z_n += base; m_hz_x_n += base;
   if (g.cb_b) cb += base;
   {
     // Interior tile (block-uniform): cells and their +1 neighbours outside
     // the strips, so raw_x = q and raw_y = -q throughout.
-    const int tx0 = tl.x * kTileX + 1, ty0 = tl.y * kBlockY * R + 1;
+    const int tx0 = tl.x() * kTileX + 1, ty0 = tl.y() * kBlockY * R + 1;
     if (tx0 >= g.pml_x0 && tx0 + kTileX < g.pml_x1 && ty0 >= g.pml_y0 &&
         ty0 + kBlockY * R < g.pml_y1) {
       const int j0 = y0 * nx + x;
@@ -392,7 +403,7 @@ __global__ void __launch_bounds__(256)
 k2_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
          T *__restrict__ lam_hx, T *__restrict__ lam_hz, const T *__restrict__ m_hx_z,
          const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
-  adj_e_tile<T, R>(hw_tile(), g, cb, lam_ey, lam_hx, lam_hz, m_hx_z, m_hz_x, m_hx_z_n, m_hz_x_n);
+  adj_e_tile<T, R>(HwTile(), g, cb, lam_ey, lam_hx, lam_hz, m_hx_z, m_hz_x, m_hx_z_n, m_hz_x_n);
 }
 
 // ---------------------------------------------------------------- adjoint H
@@ -408,7 +419,7 @@ __device__ __forceinline__ void adj_h_interior_group(
     const TMGeom<T> &g, const GradArgs<T, S> &ga, const T *__restrict__ lam_hx,
     const T *__restrict__ lam_hz, T *__restrict__ lam_ey, const PointCSR &rec,
     const PointCSR &src, const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
-    T *__restrict__ gf_t, int s0, int tiles_per_shot, int tile_xy, int j0, const Tile &tl,
+    T *__restrict__ gf_t, int s0, int tiles_per_shot, int tile_xy, int j0, int trow_stride,
     const T (&a)[R], const T (&cz)[R + 1],
     const T (&cx)[R], const T (&cl)[R], T (&sa)[R], T (&sb)[R]) {
   const int nx = g.nx;
@@ -434,7 +445,7 @@ __device__ __forceinline__ void adj_h_interior_group(
     const int s = s0 + u;
     const int64_t base = (int64_t)s * g.N;
     const int tile = s * tiles_per_shot + tile_xy;
-    const bool pts = rowf != nullptr && __ldg(rowf + s * tl.gy + tl.y) != 0 &&
+    const bool pts = rowf != nullptr && __ldg(rowf + s * trow_stride) != 0 &&
                      !point_tile_empty(src, rec, tile);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -464,9 +475,9 @@ __device__ __forceinline__ void adj_h_interior_group(
 // model coefficients are read once, and the image terms lam * Ey^t * k and
 // lam * curlH^t * k of all shots are summed before one read-modify-write of
 // the model gradient (batched models keep one gradient per shot).
-template <typename T, typename S, int R>
+template <typename T, typename S, int R, typename TL>
 __device__ __forceinline__ void adj_h_tile(
-    const Tile &tl, const TMGeom<T> &g,
+    const TL tl, const TMGeom<T> &g,
     const T *__restrict__ ca, const T *__restrict__ cq,
     const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
     const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
@@ -474,11 +485,11 @@ __device__ __forceinline__ void adj_h_tile(
     const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
     T *__restrict__ gf_t, GradArgs<T, S> ga) {
   const int nx = g.nx, ny = g.ny;
-  const int x = tl.x * kTileX + threadIdx.x;
-  const int y0 = (tl.y * kBlockY + threadIdx.y) * R;
+  const int x = tl.x() * kTileX + threadIdx.x;
+  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R;
   if (y0 >= ny || x >= nx) return;
-  const int tile_xy = tl.y * tl.gx + tl.x;
-  const int tiles_per_shot = tl.gx * tl.gy;
+  const int tile_xy = tl.y() * tl.gx() + tl.x();
+  const int tiles_per_shot = tl.gx() * tl.gy();
   const bool xdom = x >= 1;
   const bool rx_ok = x >= 1 && x < nx - 1;  // raw_eyx defined at x
   const bool xs = rx_ok && (x < g.pml_x0 || x >= g.pml_x1h);
@@ -490,7 +501,7 @@ __device__ __forceinline__ void adj_h_tile(
   {
     // Interior tile (block-uniform): cells and their -1 neighbours outside
     // the strips, unbatched coefficients.
-    const int tx0 = tl.x * kTileX, ty0 = tl.y * kBlockY * R;
+    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * kBlockY * R;
     if (!g.ca_b && !g.cq_b && tx0 - 1 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1h &&
         ty0 - 1 >= g.pml_y0 && ty0 + kBlockY * R <= g.pml_y1h) {
       T a[R], cz[R + 1], cx[R], cl[R], sa[R], sb[R];
@@ -507,14 +518,15 @@ __device__ __forceinline__ void adj_h_tile(
       // Shots in groups of U: all loads of a group are issued before its
       // arithmetic so U shots' memory latency overlaps.
       constexpr int U = 4;
+      const unsigned char *rowf_t = rowf ? rowf + tl.y() : nullptr;
       int s0 = 0;
       for (; s0 + U <= g.n_shots; s0 += U)
-        adj_h_interior_group<T, S, R, U>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf, gr_t,
-                                         gf_t, s0, tiles_per_shot, tile_xy, j0, tl, a, cz, cx,
+        adj_h_interior_group<T, S, R, U>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf_t, gr_t,
+                                         gf_t, s0, tiles_per_shot, tile_xy, j0, tl.gy(), a, cz, cx,
                                          cl, sa, sb);
       for (; s0 < g.n_shots; ++s0)
-        adj_h_interior_group<T, S, R, 1>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf, gr_t,
-                                         gf_t, s0, tiles_per_shot, tile_xy, j0, tl, a, cz, cx,
+        adj_h_interior_group<T, S, R, 1>(g, ga, lam_hx, lam_hz, lam_ey, rec, src, rowf_t, gr_t,
+                                         gf_t, s0, tiles_per_shot, tile_xy, j0, tl.gy(), a, cz, cx,
                                          cl, sa, sb);
       if (imaging) {
 #pragma unroll
@@ -567,7 +579,7 @@ __device__ __forceinline__ void adj_h_tile(
   for (int s = 0; s < g.n_shots; ++s) {
     const int64_t base = (int64_t)s * g.N;
     const int tile = s * tiles_per_shot + tile_xy;
-    const bool pts = rowf != nullptr && __ldg(rowf + s * tl.gy + tl.y) != 0 &&
+    const bool pts = rowf != nullptr && __ldg(rowf + s * tl.gy() + tl.y()) != 0 &&
                      !point_tile_empty(src, rec, tile);
     const T *lhx = lam_hx + base, *lhz = lam_hz + base, *mex = m_ey_x + base;
     const T *mez = m_ey_z + base;
@@ -681,14 +693,14 @@ __device__ __forceinline__ void adj_h_tile(
   }
 }
 template <typename T, typename S, int R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
          const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
          const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
          T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src,
          const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
          T *__restrict__ gf_t, GradArgs<T, S> ga) {
-  adj_h_tile<T, S, R>(hw_tile(), g, ca, cq, lam_hx, lam_hz, lam_ey, m_ey_x, m_ey_z, m_ey_x_n,
+  adj_h_tile<T, S, R>(HwTile(), g, ca, cq, lam_hx, lam_hz, lam_ey, m_ey_x, m_ey_z, m_ey_x_n,
       m_ey_z_n, rec, src, rowf, gr_t, gf_t, ga);
 }
 
