@@ -300,3 +300,42 @@ class RefCPU3D:
            _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.nz,
            pb.ny, pb.nx, pb.n_src, pb.n_rec, 1, False, b, b, b, 0, *pb.pml, pb.src_comp,
            pb.rec_comp, n_threads, 0, 0, 0)
+
+
+class OracleDebye:
+    """Debye-medium forward with storage and exact adjoint of the C oracle,
+    driven with the product's argument struct (tide_b200.debye.CDebye) on
+    host tensors; a problem prepared on the CPU by prepare_tm2d."""
+
+    def __init__(self):
+        if not ORACLE_SO.exists():
+            build_oracle()
+        self.lib = ctypes.CDLL(str(ORACLE_SO))
+
+    def _call(self, name, dtype, A):
+        from tide_b200.debye import CDebye
+
+        sfx = "float" if dtype == torch.float32 else "double"
+        fn = getattr(self.lib, f"tide_oracle_tm_debye_{name}_{sfx}")
+        fn.argtypes = [ctypes.POINTER(CDebye)]
+        fn.restype = None
+        fn(ctypes.byref(A))
+
+    def forward(self, pb, ca, cb, f, r, a, b, cp, snaps, start_t=0, nt=None, k=1, fmt=0, q0=0):
+        from tide_b200 import debye as dby
+
+        A = dby.make_args(pb, ca, cb, a, b, cp, f=f, r=r, start_t=start_t, nt=nt, k=k, fmt=fmt,
+                          q0=q0, stream=0)
+        A.pol = _p(dby.polarization(pb))
+        snaps.bind(A)
+        self._call("forward_with_storage", pb.dtype, A)
+
+    def backward(self, pb, ca, cb, a, b, cp, grad_r, st, snaps, start_t, nt, k=1, fmt=0, q0=0):
+        from tide_b200 import debye as dby
+
+        A = dby.make_args(pb, ca, cb, a, b, cp, start_t=start_t, nt=nt, k=k, fmt=fmt, q0=q0,
+                          stream=0)
+        A.grad_r = _p(grad_r)
+        snaps.bind(A)
+        st.bind(A)
+        self._call("backward", pb.dtype, A)

@@ -849,3 +849,6 @@ extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(flo
 
 // Multi-job serving engine (shares this file's launch helpers and tile lists).
 #include "tm2d_serve.cuh"
+
+// Debye-medium forward with storage and adjoint (same launch helpers).
+#include "tm2d_debye.cuh"

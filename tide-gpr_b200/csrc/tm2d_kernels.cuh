@@ -269,6 +269,9 @@ template <typename T> struct DebyeArgs {
   const T *a, *b, *cp;  // [n_poles, ny, nx]
   T *pol;               // [n_shots, n_poles, ny, nx]
   int n_poles;
+  // snapshots of this step (element type S of the kernel), null: not recorded
+  void *pol_st;   // P^t before the update, [n_shots, n_poles, ny, nx]
+  void *esum_st;  // E^{t+1} + E^t, [n_shots, ny, nx]
 };
 
 template <typename S> __device__ __forceinline__ void store_stream(S *p, S v) { __stcs(p, v); }
@@ -396,9 +399,12 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
       e = cav[r] * e + cbv[r] * curl;
       if (db.n_poles > 0) {
         T pol_term = (T)0;
-        for (int p = 0; p < db.n_poles; ++p)
-          pol_term = pol_term + ldg(db.cp + (int64_t)p * g.N + j) *
-                                    db.pol[((int64_t)s * db.n_poles + p) * g.N + j];
+        for (int p = 0; p < db.n_poles; ++p) {
+          const int64_t pi = ((int64_t)s * db.n_poles + p) * g.N + j;
+          const T pv = db.pol[pi];
+          if (db.pol_st) store_stream(static_cast<S *>(db.pol_st) + pi, Codec<S, T>::enc(pv));
+          pol_term = pol_term + ldg(db.cp + (int64_t)p * g.N + j) * pv;
+        }
         e = e + pol_term;
       }
     }
@@ -406,6 +412,7 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
     ey[i] = e;
     if (dom[r] && db.n_poles > 0) {
       const T e_sum = e + eo[r];
+      if (db.esum_st) store_stream(static_cast<S *>(db.esum_st) + i, Codec<S, T>::enc(e_sum));
       for (int p = 0; p < db.n_poles; ++p) {
         const int64_t c = (int64_t)p * g.N + j;
         const int64_t pi = ((int64_t)s * db.n_poles + p) * g.N + j;

@@ -300,8 +300,8 @@ class TMPropagate(torch.autograd.Function):
         if (need_ca or need_cb) and str(opts.get("storage_mode", "device")).lower() == "checkpoint":
             if pb.debye is not None:
                 raise NotImplementedError(
-                    "Debye media: use tide_b200.debye for gradients (the checkpointed path "
-                    "here does not carry the polarisation state)"
+                    "Debye media: gradients run through tide_b200.debye (propagate routes "
+                    "them there)"
                 )
             seg_len = checkpoint_steps(nt, k, opts.get("storage_chunk_steps"))
             ckpt = (seg_len, _run_forward_checkpointed(pb, ca, cb, f, r, seg_len, fwd_cb,
@@ -321,8 +321,8 @@ class TMPropagate(torch.autograd.Function):
             snaps = stg.allocate(mode, sdtype, fmt, n_store, S, pb.ny, pb.nx, device, need_ca, need_cb)
             if pb.debye is not None:
                 raise NotImplementedError(
-                    "Debye media: use tide_b200.debye for gradients (forward-with-storage "
-                    "kernels here do not carry the polarisation state)"
+                    "Debye media: gradients run through tide_b200.debye (propagate routes "
+                    "them there)"
                 )
             _run_forward_storage(pb, ca, cb, f, r, snaps, need_ca, need_cb, fwd_cb, freq)
         else:
@@ -581,6 +581,15 @@ def propagate(pb: TMProblem, opts: dict | None = None):
     """Run the TM2D propagation; returns (7 padded state tensors, receivers [nt, S, n_rec])."""
     opts = opts or {}
     needs_graph = pb.ca.requires_grad or pb.cb.requires_grad or pb.f.requires_grad
+    if pb.debye is not None:
+        d = pb.debye
+        if needs_graph or any(torch.is_tensor(d[n]) and d[n].requires_grad
+                              for n in ("a", "b", "cp")):
+            from .debye import propagate_debye
+
+            if opts.get("forward_callback") or opts.get("backward_callback"):
+                raise NotImplementedError("callbacks are not supported for Debye gradients")
+            return propagate_debye(pb, opts)
     if needs_graph:
         out = TMPropagate.apply(pb.ca, pb.cb, pb.f, pb, opts)
         return list(out[:7]), out[7]
