@@ -38,7 +38,7 @@ def nvcc() -> str:
 def _stale(obj: pathlib.Path, src: pathlib.Path) -> bool:
     if not obj.exists():
         return True
-    deps = [src, *CSRC.glob("*.cuh"), ROOT.parent / "include" / "tide_b200.h", pathlib.Path(__file__)]
+    deps = [src, *CSRC.glob("*.cuh"), *(ROOT.parent / "include").glob("*.h"), pathlib.Path(__file__)]
     return any(d.exists() and d.stat().st_mtime > obj.stat().st_mtime for d in deps)
 
 
