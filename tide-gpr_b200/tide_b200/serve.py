@@ -289,6 +289,8 @@ class _Task:
         self.g = g
         self.lo, self.hi = plan.groups[g]
         self.bytes = plan.group_bytes[g]
+        ny, nx = job.padded_shape()
+        self.cells = (self.hi - self.lo) * ny * nx  # shots x cells of the group
         nt = job.nt
         k = max(1, min(job.model_gradient_sampling_interval, nt)) if nt > 0 else 1
         self.segments = program(plan.mode, nt, k, plan.seg_len)
@@ -305,6 +307,11 @@ class _Task:
     @property
     def finished_stepping(self) -> bool:
         return self.seg >= len(self.segments)
+
+    def remaining_steps(self) -> int:
+        if self.finished_stepping:
+            return 0
+        return sum(s.steps for s in self.segments[self.seg:]) - self.pos
 
     def next_plan(self, C: int) -> tuple[Segment, int, int, bool] | None:
         """(segment, t0 for this chunk, steps this chunk, first chunk of segment)."""
@@ -355,7 +362,8 @@ class TMServer:
                  max_slots: int = 64, chunk_steps: int = 32, use_graphs: bool = True,
                  storage_compression: bool = False, history_limit: int | None = None,
                  group_limit: int | None = None, max_bypass: int = 8, depth: int = 2,
-                 direct_cells: int = DIRECT_CELLS, fused: bool = True):
+                 direct_cells: int = DIRECT_CELLS, fused: bool = True, priority: bool = True,
+                 max_weight: int = 4):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise nat.NativeError("TMServer runs on a CUDA device only")
@@ -381,6 +389,9 @@ class TMServer:
             raise nat.NativeError("serve create failed")
         self.lib.tide_b200_serve_configure(self.engine, int(direct_cells), int(fused))
         nat.check("serve configure")
+        self.direct_cells = int(direct_cells)
+        self.priority = bool(priority)
+        self.max_weight = max(1, int(max_weight))
         self.stream = torch.cuda.Stream(self.device)
         self.queue: deque[_Task] = deque()
         self.resident: list[_Task] = []
@@ -582,11 +593,30 @@ class TMServer:
             for dst, src in zip(fields, o["ckpt"][int(name[8:])]):
                 dst.copy_(src)
 
+    def _weights(self) -> dict:
+        """Steps per chunk of each resident group, in units of chunk_steps:
+        groups on their own streams (per-call kernels) with more remaining
+        steps than the median run up to max_weight chunks' worth, so the
+        longest jobs (checkpointed gradients: three passes) are not left to
+        finish alone after the others."""
+        if not self.priority:
+            return {}
+        rem = sorted(t.remaining_steps() for t in self.resident)
+        if not rem:
+            return {}
+        ref = max(1, rem[len(rem) // 2])
+        w = {}
+        for t in self.resident:
+            if t.cells >= self.direct_cells >= 0:
+                w[id(t)] = max(1, min(self.max_weight, t.remaining_steps() // ref))
+        return w
+
     def _run_chunk(self) -> None:
         C = self.C
         planned = []
+        weights = self._weights()
         for t in self.resident:
-            p = t.next_plan(C)
+            p = t.next_plan(C * weights.get(id(t), 1))
             if p is None:
                 continue
             seg, t0, n, first = p
