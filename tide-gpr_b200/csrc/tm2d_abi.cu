@@ -41,7 +41,15 @@ template <typename T, int ST> struct Launch {
   dim3 block{kTileX, kBlockY, 1};
   dim3 grid_h, grid_e, grid_ae, grid_ah;
   int tiles_x = 0, tiles_y_e = 0, tiles_y_ah = 0;
+  int ah_by = kBlockY;  // warps per block (rows of 32 cells) of the adjoint H kernel
   bool has_domain = false;
+  // Point-list tiles of the adjoint H kernel.
+  PointTiles ah_tiles() const { return PointTiles{tiles_x, tiles_y_ah, kTileX, ah_by * kRowsAH, 0}; }
+  void set_ah_by(int by) {
+    ah_by = by;
+    tiles_y_ah = (int)cdiv(g.ny, by * kRowsAH);
+    grid_ah = dim3((unsigned)tiles_x, (unsigned)tiles_y_ah, 1);
+  }
 };
 
 template <typename T, int ST>
@@ -79,10 +87,40 @@ bool make_launch(Launch<T, ST> &L, const T *ay, const T *by, const T *ayh, const
   L.grid_ae = dim3(cdiv(dx, kTileX), cdiv(dy, kBlockY * kRowsAE), S);
   L.tiles_x = (int)cdiv(nx, kTileX);
   L.tiles_y_e = (int)cdiv(ny, kBlockY * kRowsE);
-  L.tiles_y_ah = (int)cdiv(ny, kBlockY * kRowsAH);
   L.grid_e = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_e, S);
-  L.grid_ah = dim3((unsigned)L.tiles_x, (unsigned)L.tiles_y_ah, 1);
+  L.set_ah_by(kBlockY);
   return true;
+}
+
+// Block height of the stencil-2 adjoint H kernel for one call.  Its blocks
+// each loop over all shots, so its grid is only a few waves deep (553 x 1065:
+// 2380 blocks of 8 warps on 148 x 4 slots = 4.02 waves; 4726 blocks of 4
+// warps on 148 x 8 slots = 3.99).  Picks the height whose last wave is
+// fullest; on that grid 4 warps run 47.1 us per step against 47.7 at 8 shots.
+template <typename T, typename S> void pick_adj_h_rows(Launch<T, 2> &L) {
+  static const std::pair<int, int> occ = [] {
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k2_adj_h<T, S, kRowsAH, 8>, 256, 0) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k2_adj_h<T, S, kRowsAH, 4>, 128, 0) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      return std::pair<int, int>(0, 0);
+    }
+    return std::pair<int, int>(a, b);
+  }();
+  int dev = 0, n_sm = 0;
+  if (occ.first < 1 || occ.second < 1 || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  auto fill = [&](int by, int blocks_per_sm) {
+    const double w =
+        (double)L.tiles_x * (double)cdiv(L.g.ny, by * kRowsAH) / ((double)n_sm * blocks_per_sm);
+    return w / std::ceil(w);
+  };
+  L.set_ah_by(fill(4, occ.second) > fill(8, occ.first) + 0.02 ? 4 : 8);
 }
 
 // Per-call scratch: CSR point lists for sources and receivers, allocated from
@@ -210,10 +248,12 @@ inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, c
                          const T *lhx, const T *lhz, T *ley, const T *mex, const T *mez,
                          T *mex_n, T *mez_n, const PointScratch &ps, const T *grt, T *gft,
                          const GradArgs<T, S> &ga) {
-  if (ST == 2)
-    k2_adj_h<T, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex, mez,
-                                                           mex_n, mez_n, ps.rec, ps.src, ps.rowf,
-                                                           grt, gft, ga);
+  if (ST == 2 && L.ah_by == 4)
+    k2_adj_h<T, S, kRowsAH, 4><<<L.grid_ah, dim3(kTileX, 4, 1), 0, st>>>(
+        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga);
+  else if (ST == 2)
+    k2_adj_h<T, S, kRowsAH, kBlockY><<<L.grid_ah, L.block, 0, st>>>(
+        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga);
   else
     k_adj_h<T, ST, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex,
                                                               mez, mex_n, mez_n, ps.rec, ps.src,
@@ -554,6 +594,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
+  if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
   cudaStream_t st = as_stream(compute_stream);
   cudaStream_t ss = as_stream(storage_stream);
   const bool pipeline = grads && storage_mode == 1 && ss != nullptr && ss != st;
@@ -567,7 +608,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
       !zero_band(m_lambda_ey_z, L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_ah, kTileX, kBlockY * kRowsAH, 0}, sources_i, n_sources_per_shot, receivers_i,
+  if (!build_points(ps, L, L.ah_tiles(), sources_i, n_sources_per_shot, receivers_i,
                     n_receivers_per_shot, st))
     return;
 

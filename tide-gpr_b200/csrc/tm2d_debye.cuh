@@ -209,8 +209,8 @@ void debye_backward(const TideTMDebye &A) {
       !zero_band(lam[4], L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_ah, kTileX, kBlockY * kRowsAH, 0},
-                    A.sources_i, A.n_src, A.receivers_i, A.n_rec, st))
+  if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
+  if (!build_points(ps, L, L.ah_tiles(), A.sources_i, A.n_src, A.receivers_i, A.n_rec, st))
     return;
   const T *ca = static_cast<const T *>(A.ca), *cb = static_cast<const T *>(A.cb);
   const T *cq = static_cast<const T *>(A.cq);

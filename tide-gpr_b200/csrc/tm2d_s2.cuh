@@ -471,11 +471,12 @@ __device__ __forceinline__ void adj_h_interior_group(
   }
 }
 
-// Full-grid tiles (32 x 8R).  Each thread loops over the shots of the call:
-// model coefficients are read once, and the image terms lam * Ey^t * k and
-// lam * curlH^t * k of all shots are summed before one read-modify-write of
-// the model gradient (batched models keep one gradient per shot).
-template <typename T, typename S, int R, typename TL>
+// Full-grid tiles (32 x BY R, BY warps per block).  Each thread loops over the
+// shots of the call: model coefficients are read once, and the image terms
+// lam * Ey^t * k and lam * curlH^t * k of all shots are summed before one
+// read-modify-write of the model gradient (batched models keep one gradient
+// per shot).
+template <typename T, typename S, int R, int BY = kBlockY, typename TL>
 __device__ __forceinline__ void adj_h_tile(
     const TL tl, const TMGeom<T> &g,
     const T *__restrict__ ca, const T *__restrict__ cq,
@@ -486,7 +487,7 @@ __device__ __forceinline__ void adj_h_tile(
     T *__restrict__ gf_t, GradArgs<T, S> ga) {
   const int nx = g.nx, ny = g.ny;
   const int x = tl.x() * kTileX + threadIdx.x;
-  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R;
+  const int y0 = (tl.y() * BY + threadIdx.y) * R;
   if (y0 >= ny || x >= nx) return;
   const int tile_xy = tl.y() * tl.gx() + tl.x();
   const int tiles_per_shot = tl.gx() * tl.gy();
@@ -501,9 +502,9 @@ __device__ __forceinline__ void adj_h_tile(
   {
     // Interior tile (block-uniform): cells and their -1 neighbours outside
     // the strips, unbatched coefficients.
-    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * kBlockY * R;
+    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * BY * R;
     if (!g.ca_b && !g.cq_b && tx0 - 1 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1h &&
-        ty0 - 1 >= g.pml_y0 && ty0 + kBlockY * R <= g.pml_y1h) {
+        ty0 - 1 >= g.pml_y0 && ty0 + BY * R <= g.pml_y1h) {
       T a[R], cz[R + 1], cx[R], cl[R], sa[R], sb[R];
 #pragma unroll
       for (int r = 0; r <= R; ++r) cz[r] = ldg(cq + j0 + (r - 1) * nx);
@@ -692,15 +693,17 @@ __device__ __forceinline__ void adj_h_tile(
     if (ga.cu_st && !ga.batched_cb) ga.grad_cb[j] = ga.grad_cb[j] + sum_cb[r];
   }
 }
-template <typename T, typename S, int R>
-__global__ void __launch_bounds__(256, 4)
+// 64 registers per thread at any block height (4 blocks of 8 warps or 8 of 4
+// per SM); the compiler's own choice spills.
+template <typename T, typename S, int R, int BY>
+__global__ void __launch_bounds__(32 * BY, 32 / BY)
 k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
          const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
          const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
          T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src,
          const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
          T *__restrict__ gf_t, GradArgs<T, S> ga) {
-  adj_h_tile<T, S, R>(HwTile(), g, ca, cq, lam_hx, lam_hz, lam_ey, m_ey_x, m_ey_z, m_ey_x_n,
+  adj_h_tile<T, S, R, BY>(HwTile(), g, ca, cq, lam_hx, lam_hz, lam_ey, m_ey_x, m_ey_z, m_ey_x_n,
       m_ey_z_n, rec, src, rowf, gr_t, gf_t, ga);
 }
 

@@ -490,7 +490,7 @@ int64_t tide_b200_serve_bind(void *engine, const TideServeJob *job, int64_t stre
   }
   // Tile lists: E tiling (forward) and, for the adjoint, adjoint-H tiling.
   const PointTiles pe{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0};
-  const PointTiles ph{L.tiles_x, L.tiles_y_ah, kTileX, kBlockY * kRowsAH, 0};
+  const PointTiles ph = L.ah_tiles();  // 8-warp blocks: the table's tiling
   auto words = [&](const PointTiles &pt, int64_t per) -> size_t {
     if (per <= 0) return 0;
     return 2 * ((size_t)pt.tiles_x * pt.tiles_y * S + 1) + 2 * (size_t)(per * S);
