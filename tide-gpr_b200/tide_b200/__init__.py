@@ -1,9 +1,10 @@
 """tide_b200 — B200-native (sm_100a) TM2D time stepping with TIDE's API.
 
 ``import tide_b200 as tide`` gives the operator API of the reference
-(``MaxwellTM``, ``EMModel``, ``Experiment``, ``Acquisition``,
+(``MaxwellTM``, ``Maxwell3D``, ``EMModel``, ``Experiment``, ``Acquisition``,
 ``Discretization``, ``CPML``, ``StorageOptions``, ``operator.linearize``)
-and the functional ``maxwelltm``; all propagation runs in libtide_b200.so.
+and the functionals ``maxwelltm`` and ``maxwell3d``; all propagation runs in
+libtide_b200.so.
 """
 
 from .api import (
@@ -11,13 +12,16 @@ from .api import (
     Acquisition,
     BackendPreference,
     Discretization,
+    EM3DState,
     EMGradient,
     EMModel,
     ExecutionOptions,
     Experiment,
     FallbackPolicy,
     ForwardResult,
+    LinearizedMaxwell3D,
     LinearizedMaxwellTM,
+    Maxwell3D,
     MaxwellTM,
     Observers,
     TMState,
@@ -34,12 +38,14 @@ from .physics import (
     upsample,
 )
 from .storage import StorageMode, StorageOptions
+from .em3d import maxwell3d
 from .tm2d import CallbackState, maxwelltm, prepare_tm2d, propagate
 
 __all__ = [
     "CPML", "Acquisition", "BackendPreference", "C0", "CallbackState", "DebyeDispersion",
-    "Discretization", "EMGradient", "EMModel", "EP0", "ExecutionOptions", "Experiment",
-    "FallbackPolicy", "ForwardResult", "LinearizedMaxwellTM", "MU0", "MaxwellTM", "Observers",
-    "StorageMode", "StorageOptions", "TMState", "cfl_condition", "downsample", "maxwelltm",
+    "Discretization", "EM3DState", "EMGradient", "EMModel", "EP0", "ExecutionOptions",
+    "Experiment", "FallbackPolicy", "ForwardResult", "LinearizedMaxwell3D",
+    "LinearizedMaxwellTM", "MU0", "Maxwell3D", "MaxwellTM", "Observers",
+    "StorageMode", "StorageOptions", "TMState", "cfl_condition", "downsample", "maxwell3d", "maxwelltm",
     "prepare_parameters", "prepare_tm2d", "propagate", "ricker", "upsample",
 ]

@@ -1,7 +1,7 @@
-"""Operator-level public API: value objects, MaxwellTM, linearization.
+"""Operator-level public API: value objects, MaxwellTM, Maxwell3D, linearization.
 
 Mirrors src/tide/maxwell/contracts.py:24-201, results.py:12-90,
-operators.py:26-129 and linearization.py:36-232 (the vjp half; the Born jvp
+operators.py:26-255 and linearization.py:36-232 (the vjp half; the Born jvp
 is not built here).  A user of the reference switches with
 ``import tide_b200 as tide``.
 """
@@ -18,6 +18,7 @@ import torch
 from . import physics as ph
 from .storage import StorageOptions
 from .tm2d import Callback, maxwelltm
+from . import em3d
 
 
 class BackendPreference(StrEnum):
@@ -155,9 +156,43 @@ class TMState:
 
 
 @dataclass(frozen=True, slots=True)
+class EM3DState:
+    """Final (or initial) 3-D state: six fields and the twelve CPML memories
+    on the model + CPML region (results.py EM3DState)."""
+
+    Ex: torch.Tensor
+    Ey: torch.Tensor
+    Ez: torch.Tensor
+    Hx: torch.Tensor
+    Hy: torch.Tensor
+    Hz: torch.Tensor
+    m_hz_y: torch.Tensor
+    m_hy_z: torch.Tensor
+    m_hx_z: torch.Tensor
+    m_hz_x: torch.Tensor
+    m_hy_x: torch.Tensor
+    m_hx_y: torch.Tensor
+    m_ey_z: torch.Tensor
+    m_ez_y: torch.Tensor
+    m_ez_x: torch.Tensor
+    m_ex_z: torch.Tensor
+    m_ex_y: torch.Tensor
+    m_ey_x: torch.Tensor
+
+    @classmethod
+    def from_tensors(cls, tensors) -> EM3DState:
+        if len(tensors) != 18:
+            raise ValueError(f"EM3D state requires 18 tensors, got {len(tensors)}.")
+        return cls(*tensors)
+
+    def tensors(self) -> tuple:
+        return tuple(getattr(self, n) for n in em3d.STATE_NAMES)
+
+
+@dataclass(frozen=True, slots=True)
 class ForwardResult:
     receiver_data: torch.Tensor
-    final_state: TMState
+    final_state: TMState | EM3DState
 
 
 @dataclass(frozen=True, slots=True)
@@ -192,7 +227,8 @@ class MaxwellTM:
         self.model_gradient_sampling_interval = model_gradient_sampling_interval
 
     def forward(
-        self, model: EMModel, *, state: TMState | None = None, observers: Observers = Observers()
+        self, model: EMModel, *, state: TMState | None = None, observers: Observers = Observers(),
+        retain_history: bool = False,
     ) -> ForwardResult:
         if model.epsilon.ndim not in {2, 3}:
             raise ValueError("MaxwellTM model tensors must be 2-D or batched 3-D tensors.")
@@ -214,7 +250,7 @@ class MaxwellTM:
             storage_bytes_limit_device=self.storage.bytes_limit_device,
             storage_bytes_limit_host=self.storage.bytes_limit_host,
             storage_chunk_steps=self.storage.chunk_steps,
-            dispersion=model.dispersion,
+            dispersion=model.dispersion, retain_history=retain_history,
         )
         return ForwardResult(receiver_data=out[-1], final_state=TMState.from_tensors(out[:-1]))
 
@@ -252,7 +288,7 @@ class LinearizedMaxwellTM:
         op = MaxwellTM(operator.discretization, operator.experiment, execution=operator.execution,
                        storage=storage,
                        model_gradient_sampling_interval=operator.model_gradient_sampling_interval)
-        self._result = op(self.model)
+        self._result = op(self.model, retain_history=True)
 
     @property
     def primal(self) -> ForwardResult:
@@ -267,3 +303,86 @@ class LinearizedMaxwellTM:
 
     def jvp(self, direction):  # pragma: no cover - documented gap
         raise NotImplementedError("Born (jvp) propagation is not built in tide_b200.")
+
+
+class Maxwell3D:
+    """Differentiable full 3-D (Yee) Maxwell operator on the B200 native path
+    (operators.py:132-255)."""
+
+    def __init__(
+        self,
+        discretization: Discretization,
+        experiment: Experiment,
+        *,
+        execution: ExecutionOptions = ExecutionOptions(),
+        storage: StorageOptions = StorageOptions(),
+        model_gradient_sampling_interval: int = 1,
+    ) -> None:
+        if experiment.acquisition.spatial_ndim not in {None, 3}:
+            raise ValueError("Maxwell3D requires three-dimensional acquisition coordinates.")
+        if execution.backend is BackendPreference.REFERENCE:
+            raise NotImplementedError(
+                "tide_b200 has no reference (torch) backend; the native CUDA path is the product."
+            )
+        self.discretization = discretization
+        self.experiment = experiment
+        self.execution = execution
+        self.storage = storage
+        self.model_gradient_sampling_interval = model_gradient_sampling_interval
+
+    def forward(
+        self, model: EMModel, *, state: EM3DState | None = None, observers: Observers = Observers(),
+        retain_history: bool = False,
+    ) -> ForwardResult:
+        if model.epsilon.ndim not in {3, 4}:
+            raise ValueError("Maxwell3D model tensors must be 3-D or batched 4-D tensors.")
+        init = dict(zip(("Ex_0", "Ey_0", "Ez_0", "Hx_0", "Hy_0", "Hz_0") + em3d.MEM_NAMES,
+                        state.tensors() if state is not None else (None,) * 18))
+        d, e = self.discretization, self.experiment
+        out = em3d.maxwell3d(
+            model.epsilon, model.sigma, model.mu,
+            grid_spacing=d.spacing, dt=d.dt, source_amplitude=e.source_amplitude,
+            source_location=e.acquisition.source_location,
+            receiver_location=e.acquisition.receiver_location,
+            stencil=d.stencil, pml_width=d.boundary.width, max_vel=d.max_velocity, nt=e.nt,
+            model_gradient_sampling_interval=self.model_gradient_sampling_interval,
+            source_component=e.source_component, receiver_component=e.receiver_component,
+            forward_callback=observers.forward, backward_callback=observers.backward,
+            callback_frequency=observers.frequency,
+            storage_mode=self.storage.mode.value, storage_compression=self.storage.compression,
+            storage_chunk_steps=self.storage.chunk_steps, dispersion=model.dispersion,
+            retain_history=retain_history, **init,
+        )
+        return ForwardResult(receiver_data=out[-1], final_state=EM3DState.from_tensors(out[:-1]))
+
+    __call__ = forward
+
+    def linearize(
+        self,
+        model: EMModel,
+        *,
+        storage: StorageOptions | None = None,
+        targets: Iterable[str] = ("epsilon", "sigma"),
+    ) -> LinearizedMaxwell3D:
+        return LinearizedMaxwell3D(self, model, storage=storage or self.storage, targets=targets)
+
+
+class LinearizedMaxwell3D(LinearizedMaxwellTM):
+    """Linearization of Maxwell3D at a model: primal data and exact VJPs
+    (linearization.py LinearizedMaxwell3D, the vjp half)."""
+
+    def __init__(self, operator: Maxwell3D, model: EMModel, *, storage: StorageOptions,
+                 targets: Iterable[str]) -> None:
+        self.operator = operator
+        self.targets = tuple(targets)
+        for t in self.targets:
+            if t not in ("epsilon", "sigma"):
+                raise ValueError(f"unsupported linearization target {t!r}")
+        eps = model.epsilon.detach().requires_grad_("epsilon" in self.targets)
+        sig = model.sigma.detach().requires_grad_("sigma" in self.targets)
+        self._inputs = {"epsilon": eps, "sigma": sig}
+        self.model = EMModel(eps, sig, model.mu.detach(), model.dispersion)
+        op = Maxwell3D(operator.discretization, operator.experiment, execution=operator.execution,
+                       storage=storage,
+                       model_gradient_sampling_interval=operator.model_gradient_sampling_interval)
+        self._result = op(self.model, retain_history=True)

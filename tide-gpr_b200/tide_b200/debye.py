@@ -235,6 +235,8 @@ class DebyePropagate(torch.autograd.Function):
                                 q0=s0 // k)
             for dst, src in zip(state, final):
                 dst.copy_(src)
+        if not ctx.opts.get("retain_history"):
+            ctx.plan = None  # release the history (a linearization keeps it)
         g = st.g
         gf = st.grad_f.reshape(-1) if (st.grad_f is not None and ctx.needs_input_grad[2]) else None
         return (g["ca"].unsqueeze(0) if g["ca"] is not None else None,

@@ -134,10 +134,13 @@ def prepare_em3d(
     receiver_location: torch.Tensor | None, *, stencil: int = 2,
     pml_width: int | Sequence[int] = 20, source_component: str = "ey",
     receiver_component: str = "ey", model_gradient_sampling_interval: int = 1,
-    nt: int | None = None,
+    nt: int | None = None, initial_state: Sequence[torch.Tensor | None] | None = None,
 ) -> EM3DProblem:
     """Pad the model, build coefficients, CPML profiles, point indices and the
-    zero initial state (maxwell3d_cuda.py:310-528)."""
+    initial state (maxwell3d_cuda.py:310-528).  initial_state: Ex, Ey, Ez, Hx,
+    Hy, Hz and the 12 CPML memories in MEM_NAMES order, each [nz', ny', nx']
+    or [S, nz', ny', nx'] on the model + CPML region (the shape this module
+    returns) or on the full padded grid; None entries start at zero."""
     if stencil != 2:
         raise ValueError("the 3-D path is built for stencil order 2")
     if epsilon.ndim not in (3, 4) or sigma.shape != epsilon.shape or mu.shape != epsilon.shape:
@@ -189,8 +192,22 @@ def prepare_em3d(
     prof = ph.set_pml_profiles_3d(widths, fd, dt, [dz, dy, dx], dtype, device, nz, ny, nx)
     layout = CompactLayout(S, (nz, ny, nx), ((pml[0], pml[3]), (pml[1], pml[4]), (pml[2], pml[5])))
     shape = (S, nz, ny, nx)
-    fields = [torch.zeros(shape, device=device, dtype=dtype) for _ in range(6)]
-    memories = [layout.zeros(a, device, dtype) for a in MEM_AXES]
+    init = list(initial_state) if initial_state is not None else [None] * 18
+    if len(init) != 18:
+        raise ValueError("initial_state holds 6 fields and 12 CPML memories")
+
+    def padded(t):  # zero fd padding, as create_or_pad(..., mode="constant")
+        if t.ndim == 3:
+            t = t[None].expand(S, -1, -1, -1)
+        t = t.to(device=device, dtype=dtype)
+        if tuple(t.shape) == shape:
+            return t.clone().contiguous()
+        return torch.nn.functional.pad(t, ph._torch_pad_order(fd)).contiguous()
+
+    fields = [padded(t) if t is not None and t.numel() else torch.zeros(shape, device=device, dtype=dtype)
+              for t in init[:6]]
+    memories = [layout.pack(padded(t), a) if t is not None and t.numel() else layout.zeros(a, device, dtype)
+                for t, a in zip(init[6:], MEM_AXES)]
     shp = (S, nz, ny, nx) if batched else (1, nz, ny, nx)
     return EM3DProblem(
         ca=ca.reshape(shp), cb=cb.reshape(shp), cq=cq.reshape(shp), f=f, profiles=prof,
@@ -242,11 +259,13 @@ class Snapshots3D:
     shot_bytes: int
     dev: list  # 6 device buffers (or empty)
     host: list  # 6 pinned host histories (cpu mode)
+    q0: int = 0  # first store slot held by the device buffers (checkpoint segments)
 
 
-def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need_cb: bool) -> Snapshots3D:
+def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need_cb: bool,
+                       n_store: int | None = None) -> Snapshots3D:
     k = max(1, pb.grad_interval)
-    n_store = (pb.nt + k - 1) // k
+    n_store = (pb.nt + k - 1) // k if n_store is None else int(n_store)
     sdt = torch.bfloat16 if fmt == 1 else pb.dtype
     esz = torch.tensor([], dtype=sdt).element_size()
     shot_bytes = pb.nz * pb.ny * pb.nx * esz
@@ -268,9 +287,14 @@ def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need
 
 
 def _store_ptrs(sn: Snapshots3D) -> list[int]:
+    """Raw snapshot addresses; device bases move back by q0 slots so that a
+    segment-sized buffer receives the slots of a later segment (the native
+    call adds slot * step_bytes)."""
     out = []
     for c in range(6):
-        out += [_p(sn.dev[c]), _p(sn.host[c]), 0]
+        d = sn.dev[c]
+        step = d[0].numel() * d.element_size() if d.numel() else 0
+        out += [_p(d) - sn.q0 * step if d.numel() else 0, _p(sn.host[c]), 0]
     return out
 
 
@@ -288,9 +312,10 @@ def native_forward_storage(pb: EM3DProblem, ca, cb, f, r, sn: Snapshots3D, need_
 
 def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: bool,
                     need_cb: bool, need_f: bool, *, grad_eps=None, grad_sigma=None,
-                    lam=None, start_t: int | None = None, nt: int | None = None):
+                    lam=None, start_t: int | None = None, nt: int | None = None, grads=None):
     """Exact adjoint; returns (grad_ca, grad_cb, grad_f) with grad_ca/cb
-    shaped like ca/cb, grad_f [nt * S * n_src]."""
+    shaped like ca/cb, grad_f [nt * S * n_src].  grads: the same triple from
+    an earlier call over later steps, accumulated into (chunked adjoint)."""
     dev, dt_ = pb.device, pb.dtype
     S, nz, ny, nx = pb.n_shots, pb.nz, pb.ny, pb.nx
     nt_all = pb.nt
@@ -303,12 +328,15 @@ def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: b
     scratch = torch.empty(sum(m.numel() for m in lam["mem"]), device=dev, dtype=dt_)
     empty = torch.empty(0, device=dev, dtype=dt_)
     mshape = ca.shape
-    grad_ca = torch.zeros(mshape, device=dev, dtype=dt_) if need_ca else empty
-    grad_cb = torch.zeros(mshape, device=dev, dtype=dt_) if need_cb else empty
+    if grads is not None:
+        grad_ca, grad_cb, grad_f = grads
+    else:
+        grad_ca = torch.zeros(mshape, device=dev, dtype=dt_) if need_ca else empty
+        grad_cb = torch.zeros(mshape, device=dev, dtype=dt_) if need_cb else empty
+        grad_f = (torch.zeros(nt_all * S * pb.n_src, device=dev, dtype=dt_)
+                  if need_f and pb.n_src > 0 else empty)
     shot_ca = torch.empty(shape, device=dev, dtype=dt_) if need_ca and not pb.batched and S > 1 else empty
     shot_cb = torch.empty(shape, device=dev, dtype=dt_) if need_cb and not pb.batched and S > 1 else empty
-    grad_f = (torch.zeros(nt_all * S * pb.n_src, device=dev, dtype=dt_)
-              if need_f and pb.n_src > 0 else empty)
     fn = nat.get_backend_function("maxwell_3d", "backward", 2, dt_, dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     fn(_p(ca), _p(cb), _p(pb.cq), _p(grad_r), *[_p(t) for t in lam["fields"]],
@@ -321,31 +349,101 @@ def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: b
     return grad_ca, grad_cb, grad_f
 
 
+CHECKPOINT = -1  # storage code of the checkpoint-and-recompute gradient (Python-side)
+
+
+def checkpoint_steps(nt: int, k: int, requested: int | None) -> int:
+    """Segment length of the checkpointed gradient: a multiple of the gradient
+    sampling interval k, default about sqrt(nt) steps."""
+    seg = int(requested or 0) or max(1, int(round(nt ** 0.5)))
+    return max(k, (seg + k - 1) // k * k)
+
+
+def _state(pb: EM3DProblem) -> list:
+    return list(pb.fields) + list(pb.memories)
+
+
+def forward_checkpointed(pb: EM3DProblem, ca, cb, f, r, seg: int) -> list:
+    """Plain forward keeping the full state (6 fields, 12 compact memories) at
+    the start of every segment of seg steps."""
+    ckpts = []
+    for t0 in range(0, pb.nt, seg):
+        ckpts.append([t.clone() for t in _state(pb)])
+        native_forward(pb, ca, cb, f, r, t0, min(seg, pb.nt - t0))
+    return ckpts
+
+
+def backward_checkpointed(pb: EM3DProblem, ca, cb, f, grad_r, ckpts: list, seg: int, fmt: int,
+                          need_ca: bool, need_cb: bool, need_f: bool):
+    """Checkpoint-and-recompute gradient: for each segment, last first, the
+    forward is recomputed from its checkpoint with the segment's snapshots in
+    a segment-sized device buffer, then the adjoint runs over the segment and
+    accumulates into the same gradients.  The final forward state is put back
+    at the end."""
+    k = max(1, pb.grad_interval)
+    final = [t.clone() for t in _state(pb)]
+    sn = allocate_snapshots(pb, stg.STORAGE_DEVICE, fmt, need_ca, need_cb, n_store=seg // k)
+    r_scratch = torch.empty((pb.nt, pb.n_shots, max(pb.n_rec, 1)), device=pb.device, dtype=pb.dtype)
+    shape = (pb.n_shots, pb.nz, pb.ny, pb.nx)
+    dev, dt_ = pb.device, pb.dtype
+    lam = {"fields": [torch.zeros(shape, device=dev, dtype=dt_) for _ in range(6)],
+           "mem": [pb.layout.zeros(a, dev, dt_) for a in ADJ_MEM_AXES]}
+    grads = None
+    for idx in range(len(ckpts) - 1, -1, -1):
+        t0 = idx * seg
+        n = min(seg, pb.nt - t0)
+        for dst, src in zip(_state(pb), ckpts[idx]):
+            dst.copy_(src)
+        sn.q0 = t0 // k
+        native_forward_storage(pb, ca, cb, f, r_scratch if pb.n_rec > 0 else r_scratch[:0], sn,
+                               need_ca, need_cb, start_t=t0, nt=n)
+        grads = native_backward(pb, ca, cb, grad_r, sn, need_ca, need_cb, need_f, lam=lam,
+                                start_t=t0 + n, nt=n, grads=grads)
+    for dst, src in zip(_state(pb), final):
+        dst.copy_(src)
+    return grads
+
+
 class EM3DPropagate(torch.autograd.Function):
-    """Receivers from (ca, cb, f); backward through the exact adjoint."""
+    """Receivers from (ca, cb, f); backward through the exact adjoint, from a
+    stored snapshot history (device or pinned host) or by checkpoint segments
+    with recomputation (mode CHECKPOINT)."""
 
     @staticmethod
-    def forward(ctx, ca, cb, f, pb: EM3DProblem, mode: int, fmt: int):
+    def forward(ctx, ca, cb, f, pb: EM3DProblem, mode: int, fmt: int, seg: int, retain: bool):
         need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
-        if need_ca or need_cb or ctx.needs_input_grad[2]:
+        ctx.pb, ctx.mode, ctx.fmt, ctx.seg, ctx.retain = pb, mode, fmt, seg, retain
+        ctx.flags = (need_ca, need_cb, ctx.needs_input_grad[2])
+        if mode == CHECKPOINT and (need_ca or need_cb or ctx.needs_input_grad[2]):
+            ctx.ckpts = forward_checkpointed(pb, ca, cb, f, r, seg)
+            ctx.save_for_backward(ca, cb, f)
+        elif need_ca or need_cb or ctx.needs_input_grad[2]:
             sn = allocate_snapshots(pb, mode, fmt, need_ca, need_cb)
             native_forward_storage(pb, ca, cb, f, r, sn, need_ca, need_cb)
-            ctx.pb, ctx.sn = pb, sn
-            ctx.flags = (need_ca, need_cb, ctx.needs_input_grad[2])
-            ctx.save_for_backward(ca, cb)
+            ctx.sn = sn
+            ctx.save_for_backward(ca, cb, f)
         else:
             native_forward(pb, ca, cb, f, r, 0, pb.nt)
         return r
 
     @staticmethod
     def backward(ctx, grad_r):
-        ca, cb = ctx.saved_tensors
+        ca, cb, f = ctx.saved_tensors
         need_ca, need_cb, need_f = ctx.flags
-        gca, gcb, gf = native_backward(ctx.pb, ca, cb, grad_r.contiguous(), ctx.sn, need_ca,
-                                       need_cb, need_f)
+        if ctx.mode == CHECKPOINT:
+            gca, gcb, gf = backward_checkpointed(ctx.pb, ca, cb, f, grad_r.contiguous(), ctx.ckpts,
+                                                 ctx.seg, ctx.fmt, need_ca, need_cb, need_f)
+        else:
+            gca, gcb, gf = native_backward(ctx.pb, ca, cb, grad_r.contiguous(), ctx.sn, need_ca,
+                                           need_cb, need_f)
+        if not ctx.retain:  # release the history (a linearization keeps it)
+            ctx.ckpts = ctx.sn = None
         return (gca if need_ca else None, gcb if need_cb else None,
-                gf if need_f else None, None, None, None)
+                gf if need_f else None, None, None, None, None, None)
+
+
+STATE_NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") + MEM_NAMES
 
 
 def maxwell3d(
@@ -353,25 +451,75 @@ def maxwell3d(
     grid_spacing: float | Sequence[float], dt: float,
     source_amplitude: torch.Tensor | None, source_location: torch.Tensor | None,
     receiver_location: torch.Tensor | None, stencil: int = 2,
-    pml_width: int | Sequence[int] = 20, nt: int | None = None,
+    pml_width: int | Sequence[int] = 20, max_vel: float | None = None,
+    Ex_0: torch.Tensor | None = None, Ey_0: torch.Tensor | None = None,
+    Ez_0: torch.Tensor | None = None, Hx_0: torch.Tensor | None = None,
+    Hy_0: torch.Tensor | None = None, Hz_0: torch.Tensor | None = None,
+    m_hz_y: torch.Tensor | None = None, m_hy_z: torch.Tensor | None = None,
+    m_hx_z: torch.Tensor | None = None, m_hz_x: torch.Tensor | None = None,
+    m_hy_x: torch.Tensor | None = None, m_hx_y: torch.Tensor | None = None,
+    m_ey_z: torch.Tensor | None = None, m_ez_y: torch.Tensor | None = None,
+    m_ez_x: torch.Tensor | None = None, m_ex_z: torch.Tensor | None = None,
+    m_ex_y: torch.Tensor | None = None, m_ey_x: torch.Tensor | None = None,
+    nt: int | None = None,
     model_gradient_sampling_interval: int = 1, source_component: str = "ey",
     receiver_component: str = "ey", storage_mode: str = "device",
-    storage_compression: bool | str = False,
+    storage_compression: bool | str = False, storage_bytes_limit_device: int | None = None,
+    storage_bytes_limit_host: int | None = None, storage_chunk_steps: int | None = None,
+    forward_callback=None, backward_callback=None, callback_frequency: int = 1,
+    dispersion=None, retain_history: bool = False, **_unused,
 ):
     """3-D Maxwell solve (src/tide/maxwell/maxwell3d.py:200-951): returns the
     final Ex, Ey, Ez, Hx, Hy, Hz and the 12 CPML memories on the model + CPML
     region (outer fd_pad cells removed), then the receiver data [nt, S, n_rec].
-    Differentiable in epsilon, sigma and source_amplitude."""
+    Differentiable in epsilon, sigma and source_amplitude.  The initial state
+    (Ex_0 .. m_ey_x) takes the same shapes.  storage_mode: 'device', 'cpu'
+    (pinned host history), 'none', or 'checkpoint' (segments of
+    storage_chunk_steps steps, default about sqrt(nt), recomputed in the
+    backward pass).  As in the reference (maxwell3d.py:418-440), a dt above
+    the CFL bound for max_vel (default: the model's largest wave speed) runs
+    ceil(dt / dt_max) internal steps per user step, with the source
+    amplitudes upsampled and the receivers downsampled by that ratio.
+    retain_history keeps the history (or checkpoints) after a backward pass
+    for further vjps.  Callbacks and dispersive media are not built for the
+    3-D path and raise."""
     if epsilon.device.type != "cuda":
         raise nat.NativeError("libtide_b200 runs on CUDA devices only; there is no CPU path.")
-    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
+    if forward_callback is not None or backward_callback is not None:
+        raise NotImplementedError("callbacks are not built for the 3-D path")
+    if dispersion is not None:
+        raise NotImplementedError("dispersive media are not built for the 3-D path")
+    if max_vel is None:
+        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
+    inner_dt, ratio = ph.cfl_condition(_spacing(grid_spacing), dt, max_vel)
+    amp = source_amplitude
+    if ratio > 1 and amp is not None and amp.numel() > 0:
+        amp = ph.upsample(amp, ratio)
+    nt_int = nt * ratio if nt is not None else None
+    init = [Ex_0, Ey_0, Ez_0, Hx_0, Hy_0, Hz_0, m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y,
+            m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x]
+    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, inner_dt, amp, source_location,
                       receiver_location, stencil=stencil, pml_width=pml_width,
                       source_component=source_component, receiver_component=receiver_component,
-                      model_gradient_sampling_interval=model_gradient_sampling_interval, nt=nt)
-    mode = stg.mode_code(storage_mode)
-    fmt = 1 if storage_compression in (True, "bf16") else 0
-    r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt)
+                      model_gradient_sampling_interval=model_gradient_sampling_interval, nt=nt_int,
+                      initial_state=init)
+    sm = str(storage_mode).lower()
+    fmt, sdtype = stg.compression_format(storage_compression, pb.dtype)
+    k = max(1, pb.grad_interval)
+    if sm == "checkpoint":
+        mode, seg = CHECKPOINT, checkpoint_steps(pb.nt, k, storage_chunk_steps)
+    else:
+        # 'auto': device history if it fits the device budget, else pinned host
+        mode = stg.resolve_mode(
+            sm, device=pb.device, n_store=(pb.nt + k - 1) // k, n_shots=pb.n_shots,
+            ny=pb.nz * pb.ny, nx=pb.nx, itemsize=torch.tensor([], dtype=sdtype).element_size(),
+            n_arrays=6, bytes_limit_device=storage_bytes_limit_device,
+            bytes_limit_host=storage_bytes_limit_host)
+        seg = 0
+    r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt, seg, bool(retain_history))
     s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
     outs = [t[s] for t in pb.fields]
     outs += [pb.layout.unpack(m, a)[s] for m, a in zip(pb.memories, MEM_AXES)]
+    if ratio > 1 and r.numel() > 0:
+        r = ph.downsample(r.movedim(0, -1), ratio).movedim(-1, 0)
     return (*outs, r)

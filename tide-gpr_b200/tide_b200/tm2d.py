@@ -352,8 +352,10 @@ class TMPropagate(torch.autograd.Function):
         else:
             g_ca, g_cb, g_f = _run_backward(pb, ca, cb, grad_r, ctx.snaps, need_ca, need_cb,
                                             need_f, ctx.opts)
-        ctx.snaps = None
-        ctx.ckpt = None
+        if not ctx.opts.get("retain_history"):
+            # release the history now (a linearization keeps it for more vjps)
+            ctx.snaps = None
+            ctx.ckpt = None
         return g_ca, g_cb, g_f, None, None
 
 
@@ -676,13 +678,17 @@ def maxwelltm(
     storage_bytes_limit_host: int | None = None,
     storage_chunk_steps: int = 0,
     dispersion: ph.DebyeDispersion | None = None,
+    retain_history: bool = False,
     **_unused: Any,
 ):
     """2-D TM solver with the reference's functional signature (src/tide/maxwell/tm2d.py:258).
 
     Returns (Ey, Hx, Hz, m_Ey_x, m_Ey_z, m_Hx_z, m_Hz_x, receiver_amplitudes);
     wavefields are cropped to the model plus CPML layer, receivers are
-    [nt, n_shots, n_receivers] at the user time step.
+    [nt, n_shots, n_receivers] at the user time step.  retain_history keeps
+    the snapshot history (or checkpoints) after a backward pass so that the
+    graph can be differentiated again (linearizations); by default it is
+    released by the first backward pass.
     """
     if callback_frequency <= 0:
         raise ValueError("callback_frequency must be positive")
@@ -699,7 +705,7 @@ def maxwelltm(
         storage_compression=storage_compression,
         storage_bytes_limit_device=storage_bytes_limit_device,
         storage_bytes_limit_host=storage_bytes_limit_host,
-        storage_chunk_steps=storage_chunk_steps,
+        storage_chunk_steps=storage_chunk_steps, retain_history=retain_history,
     )
     fields, r = propagate(pb, opts)
     if ratio > 1 and r.numel() > 0:
