@@ -325,9 +325,13 @@ def run_b200(args) -> None:
             "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
         }
 
-    serving = None
+    serving = em3d_leg = debye_leg = None
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         serving = serve_bench(args)
+    if rank == 0 and world == 1 and args.em3d_nt > 0:
+        em3d_leg = em3d_bench(args)
+    if rank == 0 and world == 1 and args.debye_nt > 0:
+        debye_leg = debye_bench(args)
     if rank == 0:
         cpu = cpu_baseline(args) if not args.no_cpu_baseline else None
         line = {
@@ -346,6 +350,7 @@ def run_b200(args) -> None:
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
+            "em3d": em3d_leg, "debye": debye_leg,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -426,6 +431,182 @@ def serve_bench(args) -> dict:
         "engine_launches": launches, "plain_launches": int(plain_launches), "plans": modes,
         "timing": "wall clock around host-to-host runs (models and sources in host memory, "
                   "results copied back), torch.cuda.synchronize at the end",
+    }
+
+
+# ---------------------------------------------------------------- 3-D and Debye legs
+
+
+def config4(seed: int = 4, shots: int = 4, nt: int = 1500, device="cpu"):
+    """Seeded config-4 model and acquisition (synthetic): 128^3, dx 0.02 m,
+    eps_r in 6 horizontal layers U[1, 16] with 8 ellipsoid inclusions (radii
+    5-20 cells, eps_r U[1, 30]), sigma U[0, 0.005] S/m per layer, dt at 0.9 x
+    the 3-axis CFL limit, Ez dipole Ricker 500 MHz, 64 receivers on the top
+    plane."""
+    n, dx = 128, 0.02
+    rng = np.random.default_rng(seed)
+    layer_eps = rng.uniform(1.0, 16.0, size=6)
+    layer_sig = rng.uniform(0.0, 0.005, size=6)
+    rows = np.minimum(np.arange(n) * 6 // n, 5)
+    eps = np.broadcast_to(layer_eps[rows][:, None, None], (n, n, n)).copy()
+    sig = np.broadcast_to(layer_sig[rows][:, None, None], (n, n, n)).copy()
+    z, y, x = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    for _ in range(8):
+        c = rng.uniform(0, n, size=3)
+        r = rng.uniform(5, 20, size=3)
+        e = rng.uniform(1.0, 30.0)
+        inside = ((z - c[0]) / r[0]) ** 2 + ((y - c[1]) / r[1]) ** 2 + ((x - c[2]) / r[2]) ** 2 <= 1
+        eps[inside] = e
+    vmax = tide.C0 / math.sqrt(float(eps.min()))
+    dt = 0.9 * dx / (math.sqrt(3.0) * vmax)
+    amp = tide.ricker(500e6, nt, dt, dtype=torch.float64).view(1, 1, nt).repeat(shots, 1, 1)
+    src = torch.tensor([[[12, 32 + 64 * (i // 2), 32 + 64 * (i % 2)]] for i in range(shots)])
+    rec = torch.tensor([[[0, 8 + 16 * (j // 8), 8 + 16 * (j % 8)] for j in range(64)]] * shots)
+    f32 = torch.float32
+    return dict(
+        eps=torch.from_numpy(eps).to(f32).to(device), sig=torch.from_numpy(sig).to(f32).to(device),
+        mu=torch.ones((n, n, n), dtype=f32, device=device), amp=amp.to(f32).to(device),
+        src=src.to(device), rec=rec.to(device), dx=dx, dt=dt, nt=nt, shots=shots, pml=12,
+    )
+
+
+PADDED3 = 153  # 128 + 2 x 12 CPML + 1 fd pad
+
+
+def _timed_gpu(fn, dev):
+    """Device time (CUDA events on the current stream) of fn(), ms."""
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1), out
+
+
+def em3d_bench(args) -> dict:
+    """Config-4 leg: 3-D fwd+adj with BF16 snapshots, (a) checkpoint segments
+    with recomputation at the full nt, (b) the history in pinned host memory
+    (host-link bound) on the first em3d_host_nt steps, with the checkpoint
+    gradient of the same steps compared to it; plus the box's H2D/D2H
+    bandwidth for a 1 GiB pinned copy."""
+    from tide_b200 import em3d
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.empty_cache()
+
+    def run(cfg, mode):
+        eps = cfg["eps"].detach().requires_grad_(True)
+        sig = cfg["sig"].detach().requires_grad_(True)
+        out = em3d.maxwell3d(eps, sig, cfg["mu"], cfg["dx"], cfg["dt"], cfg["amp"], cfg["src"],
+                             cfg["rec"], pml_width=cfg["pml"], source_component="ez",
+                             receiver_component="ez", storage_mode=mode, storage_compression=True)
+        r = out[-1]
+        (0.5 * (r * r).sum()).backward()
+        return eps.grad, sig.grad
+
+    full = config4(shots=4, nt=args.em3d_nt, device=dev)
+    run(dict(full, amp=full["amp"][..., :64]), "checkpoint")  # warm-up
+    ms_ck, _ = _timed_gpu(lambda: run(full, "checkpoint"), dev)
+    units = 2.0 * full["shots"] * PADDED3 ** 3 * args.em3d_nt
+    seg = em3d.checkpoint_steps(args.em3d_nt, 1, None)
+    torch.cuda.empty_cache()
+    short = dict(full, amp=full["amp"][..., : args.em3d_host_nt])
+    run(short, "cpu")  # warm-up: the pinned host history is allocated once and then cached
+    ms_host, g_host = _timed_gpu(lambda: run(short, "cpu"), dev)
+    _, g_ck = _timed_gpu(lambda: run(short, "checkpoint"), dev)
+    rel = lambda a, b: float((a - b).norm() / b.norm())  # noqa: E731
+    units_short = 2.0 * full["shots"] * PADDED3 ** 3 * args.em3d_host_nt
+    hist_step = 6 * full["shots"] * PADDED3 ** 3 * 2
+    # host link: 1 GiB pinned <-> device
+    h = torch.empty(1 << 28, dtype=torch.float32, pin_memory=True)
+    d = torch.empty(1 << 28, dtype=torch.float32, device=dev)
+    d.copy_(h, non_blocking=True)
+    ms_h2d, _ = _timed_gpu(lambda: d.copy_(h, non_blocking=True), dev)
+    ms_d2h, _ = _timed_gpu(lambda: h.copy_(d, non_blocking=True), dev)
+    del h, d
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"config4: 3-D Yee fwd+adj, 128^3 ({PADDED3}^3 padded), CPML 12, 4 shots, "
+                    "Ez dipole Ricker 500 MHz, 64 receivers on the top plane, BF16 snapshots",
+        "checkpoint_bf16": {"nt": args.em3d_nt, "segment_steps": seg, "ms_per_eval": ms_ck,
+                            "cell_updates_per_s": units / (ms_ck / 1e3),
+                            "note": "fwd + recomputed fwd with storage + adjoint; cell-updates "
+                                    "count fwd+adj only"},
+        "host_bf16": {"nt": args.em3d_host_nt, "ms_per_eval": ms_host,
+                      "cell_updates_per_s": units_short / (ms_host / 1e3),
+                      "history_bytes_per_step": hist_step,
+                      "history_gb_full_nt": hist_step * args.em3d_nt / 1e9},
+        "link": {"h2d_gbs": (1 << 30) / (ms_h2d / 1e3) / 1e9,
+                 "d2h_gbs": (1 << 30) / (ms_d2h / 1e3) / 1e9, "bytes": 1 << 30},
+        "grad_rel_l2_checkpoint_vs_host": {"eps": rel(g_ck[0], g_host[0]),
+                                            "sigma": rel(g_ck[1], g_host[1])},
+        "timing": "CUDA events around each whole evaluation (public API, device inputs)",
+    }
+
+
+def config5(seed: int = 5, shots: int = 128, nt: int = 8000, device="cpu"):
+    """Seeded config-5 Debye model (synthetic): 2048 x 4096, dx 0.02 m,
+    eps_inf U[3, 10], delta_eps U[0, 5], tau U[1e-10, 1e-9] s as Gaussian-
+    smoothed (8 cells) random fields, sigma 0, dt at 0.9 x the CFL limit of
+    eps_inf, sources on row 10 every 32 cells, 256 receivers on row 10,
+    Ricker 400 MHz."""
+    from scipy.ndimage import gaussian_filter
+
+    ny, nx, dx = 2048, 4096, 0.02
+    rng = np.random.default_rng(seed)
+
+    def field(lo, hi):
+        u = gaussian_filter(rng.uniform(0.0, 1.0, size=(ny, nx)), sigma=8)
+        u = (u - u.min()) / max(float(u.max() - u.min()), 1e-12)
+        return lo + (hi - lo) * u
+
+    eps_inf, deps, tau = field(3.0, 10.0), field(0.0, 5.0), field(1e-10, 1e-9)
+    vmax = tide.C0 / math.sqrt(float(eps_inf.min()))
+    dt = 0.9 / math.sqrt(2.0 / dx**2) / vmax
+    amp = tide.ricker(400e6, nt, dt, dtype=torch.float64).view(1, 1, nt).repeat(shots, 1, 1)
+    src = torch.tensor([[[10, 16 + 32 * i]] for i in range(shots)])
+    rec = torch.tensor([[[10, 8 + 16 * j] for j in range(256)]] * shots)
+    f32 = torch.float32
+    t = lambda a: torch.from_numpy(a).to(f32).to(device)  # noqa: E731
+    return dict(eps=t(eps_inf), sig=torch.zeros((ny, nx), dtype=f32, device=device),
+                mu=torch.ones((ny, nx), dtype=f32, device=device), deps=t(deps), tau=t(tau),
+                amp=amp.to(f32).to(device), src=src.to(device), rec=rec.to(device), dx=dx, dt=dt,
+                nt=nt, shots=shots, pml=30)
+
+
+def debye_bench(args) -> dict:
+    """Config-5 leg: Debye-medium fwd+adj (gradients in eps_inf, sigma,
+    delta_eps, tau) on the full 2109 x 4157 padded grid with checkpoint
+    segments, for the first debye_shots shots and debye_nt steps."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.empty_cache()
+    c = config5(shots=args.debye_shots, nt=args.debye_nt, device=dev)
+
+    def run(cfg):
+        eps = cfg["eps"].detach().requires_grad_(True)
+        sig = cfg["sig"].detach().requires_grad_(True)
+        deps = cfg["deps"].detach().requires_grad_(True)
+        tau = cfg["tau"].detach().requires_grad_(True)
+        out = tide.maxwelltm(eps, sig, cfg["mu"], cfg["dx"], cfg["dt"], cfg["amp"], cfg["src"],
+                             cfg["rec"], stencil=2, pml_width=cfg["pml"], storage_mode="checkpoint",
+                             dispersion=tide.DebyeDispersion(deps, tau))
+        r = out[-1]
+        (0.5 * (r * r).sum()).backward()
+        return eps.grad
+
+    run(dict(c, amp=c["amp"][..., :16]))  # warm-up
+    ms, _ = _timed_gpu(lambda: run(c), dev)
+    padded = (2048 + 61) * (4096 + 61)
+    units = 2.0 * args.debye_shots * padded * args.debye_nt
+    torch.cuda.empty_cache()
+    return {
+        "workload": "config5: 2-D TM 1-pole Debye fwd+adj, 2048x4096 (2109x4157 padded), CPML 30, "
+                    f"{args.debye_shots} of 128 shots, nt={args.debye_nt} of 8000, checkpoint "
+                    "segments, FP32 snapshots",
+        "ms_per_eval": ms, "cell_updates_per_s": units / (ms / 1e3),
+        "segment_steps": int(round(args.debye_nt ** 0.5)),
+        "timing": "CUDA events around one whole evaluation (public API, device inputs)",
     }
 
 
@@ -549,6 +730,13 @@ def main() -> None:
     ap.add_argument("--serve-plain-jobs", type=int, default=32)
     ap.add_argument("--serve-chunk", type=int, default=32)
     ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--em3d-nt", type=int, default=1500,
+                    help="steps of the 3-D (config 4) leg, checkpointed (0: skip)")
+    ap.add_argument("--em3d-host-nt", type=int, default=60,
+                    help="steps of the 3-D leg with the BF16 history in pinned host memory")
+    ap.add_argument("--debye-nt", type=int, default=256,
+                    help="steps of the Debye (config 5) leg (0: skip)")
+    ap.add_argument("--debye-shots", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
