@@ -14,8 +14,13 @@
 // Layout: fields [S, nz, ny, nx]; CPML memories compacted along their own
 // axis (cells c < c0 and c >= max(c0, c1 - 1) kept) as the reference's CUDA
 // callers allocate them.  Launch: blocks of 32 (x) x 8 (y) threads, each
-// thread walking kZRun consecutive z cells of one (y, x) column; grid z =
-// shot x z-run.
+// thread marching kZRun consecutive z cells of one (y, x) column; grid z =
+// shot x z-run.  Along the march the z neighbour of a cell (fields, and in
+// the adjoint the raw CPML terms) is carried in registers from the previous
+// cell; per-thread pointers start at the thread's shot, and the y / x strip
+// state and profile values of a column are read once.  CPML memories are
+// read and written only in their strips (the compact planes outside the
+// update domain stay zero).
 #include <algorithm>
 #include <utility>
 
@@ -27,7 +32,7 @@
 namespace tb {
 namespace {
 
-constexpr int kZRun = 4;
+constexpr int kZRun = 16;
 constexpr int kRing3 = 3;  // device ring slots of the cpu storage mode (NUM_BUFFERS)
 
 enum { PAZ, PBZ, PAZH, PBZH, PAY, PBY, PAYH, PBYH, PAX, PBX, PAXH, PBXH,
@@ -102,29 +107,113 @@ __device__ __forceinline__ void set_index(Cell &c, int ny, int nx, int64_t N) {
 }
 
 // ---------------------------------------------------------------- forward
+// Column of one thread: shot s, (y, x) and the z run [zb, ze) of cells with
+// z, y, x >= 1.
+struct Col {
+  int s, y, x, zb, ze;
+};
 template <typename T>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ bool column(const G3<T> &g, Col &c) {
+  const int zruns = (g.nz + kZRun - 1) / kZRun;
+  c.x = blockIdx.x * blockDim.x + threadIdx.x;
+  c.y = blockIdx.y * blockDim.y + threadIdx.y;
+  c.s = blockIdx.z / zruns;
+  c.zb = (blockIdx.z - c.s * zruns) * kZRun;
+  c.ze = min(c.zb + kZRun, g.nz);
+  if (c.x < 1 || c.x >= g.nx || c.y < 1 || c.y >= g.ny) return false;
+  if (c.zb < 1) c.zb = 1;
+  return c.zb < c.ze;
+}
+
+// Compact coordinate of a strip cell c along an axis whose memories keep
+// c < lo and c >= max(lo, hi - 1).
+__device__ __forceinline__ int ccoord(int c, int lo, int hi) {
+  const int hs = max(lo, hi - 1);
+  return c < lo ? c : lo + c - hs;
+}
+
+// Per-shot element counts of the compact memories along z, y, x.
+template <typename T> __device__ __forceinline__ int64_t msz0(const G3<T> &g) {
+  return (int64_t)g.ezc * g.ny * g.nx;
+}
+template <typename T> __device__ __forceinline__ int64_t msz1(const G3<T> &g) {
+  return (int64_t)g.nz * g.eyc * g.nx;
+}
+template <typename T> __device__ __forceinline__ int64_t msz2(const G3<T> &g) {
+  return (int64_t)g.nz * g.ny * g.exc;
+}
+
+// CPML profile triple (a, b, kappa) of one coordinate.
+template <typename T> struct Prof {
+  T a, b, k;
+};
+template <typename T>
+__device__ __forceinline__ Prof<T> prof_at(const G3<T> &g, int pa, int pk, int c, bool on) {
+  if (!on) return Prof<T>{(T)0, (T)0, (T)1};
+  return Prof<T>{ld(g.p[pa] + c), ld(g.p[pa + 1] + c), ld(g.p[pk] + c)};
+}
+
+// Operands of one forward-H cell, loaded one cell ahead of its arithmetic so
+// that two cells' loads are in flight per thread.
+template <typename T> struct OpsH {
+  T q, e_z, n_x, n_y, ez_y, ex_y, ez_x, ey_x, h_x, h_y, h_z;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256, 4)
 k3_fwd_h(G3<T> g, const T *__restrict__ cq, const T *__restrict__ ex, const T *__restrict__ ey,
          const T *__restrict__ ez, T *__restrict__ hx, T *__restrict__ hy, T *__restrict__ hz,
          T *__restrict__ m_ey_z, T *__restrict__ m_ez_y, T *__restrict__ m_ez_x,
          T *__restrict__ m_ex_z, T *__restrict__ m_ex_y, T *__restrict__ m_ey_x) {
-  Cell c;
-  if (!first_cell(g, c)) return;
-  const int64_t sz = (int64_t)g.ny * g.nx, sy = g.nx;
-  const bool py = c.y < g.y0 || c.y >= g.y1h, px = c.x < g.x0 || c.x >= g.x1h;
-  for (; c.z < c.zend; ++c.z) {
-    set_index(c, g.ny, g.nx, g.N);
-    const int64_t i = c.i;
-    const T q = ld(cq + (g.cq_b ? i : c.j));
-    const bool pz = c.z < g.z0 || c.z >= g.z1h;
-    const T e_x = ld(ex + i), e_y = ld(ey + i), e_z = ld(ez + i);
+  Col c;
+  if (!column(g, c)) return;
+  const int nz = g.nz, ny = g.ny, nx = g.nx, y = c.y, x = c.x;
+  const int64_t sz = (int64_t)ny * nx, sy = nx;
+  const int64_t base = (int64_t)c.s * g.N;
+  ex += base; ey += base; ez += base; hx += base; hy += base; hz += base;
+  if (g.cq_b) cq += base;
+  m_ey_z += c.s * msz0(g); m_ex_z += c.s * msz0(g);
+  m_ez_y += c.s * msz1(g); m_ex_y += c.s * msz1(g);
+  m_ez_x += c.s * msz2(g); m_ey_x += c.s * msz2(g);
+  const bool yok = y < ny - 1, xok = x < nx - 1;
+  const bool py = y < g.y0 || y >= g.y1h, px = x < g.x0 || x >= g.x1h;
+  const Prof<T> fy = prof_at(g, PAYH, PKYH, y, py && yok), fx = prof_at(g, PAXH, PKXH, x, px && xok);
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  auto load = [&](int z, int64_t jj) {
+    OpsH<T> o{};
+    o.q = ld(cq + jj);
+    o.e_z = ld(ez + jj);
+    if (z < nz - 1) {
+      o.n_y = ld(ey + jj + sz);
+      o.n_x = ld(ex + jj + sz);
+    }
+    if (yok) {
+      o.ez_y = ld(ez + jj + sy);
+      o.ex_y = ld(ex + jj + sy);
+    }
+    if (xok) {
+      o.ez_x = ld(ez + jj + 1);
+      o.ey_x = ld(ey + jj + 1);
+    }
+    o.h_x = hx[jj];
+    o.h_y = hy[jj];
+    o.h_z = hz[jj];
+    return o;
+  };
+  int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
+  T e_x = ld(ex + j), e_y = ld(ey + j);
+  OpsH<T> o = load(c.zb, j);
+  for (int z = c.zb; z < c.ze; ++z, j += sz) {
+    OpsH<T> on{};
+    if (z + 1 < c.ze) on = load(z + 1, j + sz);
     T dEy_dz = 0, dEz_dy = 0, dEz_dx = 0, dEx_dz = 0, dEx_dy = 0, dEy_dx = 0;
-    if (c.z < g.nz - 1) {
-      T d = (ld(ey + i + sz) - e_y) * g.rdz;
-      T d2 = (ld(ex + i + sz) - e_x) * g.rdz;
-      if (pz) {
-        const int64_t m = cidx<T, 0>(g, c.s, c.z, c.y, c.x);
-        const T b = ld(g.p[PBZH] + c.z), a = ld(g.p[PAZH] + c.z), k = ld(g.p[PKZH] + c.z);
+    if (z < nz - 1) {
+      T d = (o.n_y - e_y) * g.rdz;
+      T d2 = (o.n_x - e_x) * g.rdz;
+      if (z < g.z0 || z >= g.z1h) {
+        const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+        const T b = ld(g.p[PBZH] + z), a = ld(g.p[PAZH] + z), k = ld(g.p[PKZH] + z);
         const T m1 = b * m_ey_z[m] + a * d;
         m_ey_z[m] = m1;
         d = div_k(d, k) + m1;
@@ -135,46 +224,52 @@ k3_fwd_h(G3<T> g, const T *__restrict__ cq, const T *__restrict__ ex, const T *_
       dEy_dz = d;
       dEx_dz = d2;
     }
-    if (c.y < g.ny - 1) {
-      T d = (ld(ez + i + sy) - e_z) * g.rdy;
-      T d2 = (ld(ex + i + sy) - e_x) * g.rdy;
+    if (yok) {
+      T d = (o.ez_y - o.e_z) * g.rdy;
+      T d2 = (o.ex_y - e_x) * g.rdy;
       if (py) {
-        const int64_t m = cidx<T, 1>(g, c.s, c.z, c.y, c.x);
-        const T b = ld(g.p[PBYH] + c.y), a = ld(g.p[PAYH] + c.y), k = ld(g.p[PKYH] + c.y);
-        const T m1 = b * m_ez_y[m] + a * d;
+        const int64_t m = z * s1 + o1;
+        const T m1 = fy.b * m_ez_y[m] + fy.a * d;
         m_ez_y[m] = m1;
-        d = div_k(d, k) + m1;
-        const T m2 = b * m_ex_y[m] + a * d2;
+        d = div_k(d, fy.k) + m1;
+        const T m2 = fy.b * m_ex_y[m] + fy.a * d2;
         m_ex_y[m] = m2;
-        d2 = div_k(d2, k) + m2;
+        d2 = div_k(d2, fy.k) + m2;
       }
       dEz_dy = d;
       dEx_dy = d2;
     }
-    if (c.x < g.nx - 1) {
-      T d = (ld(ez + i + 1) - e_z) * g.rdx;
-      T d2 = (ld(ey + i + 1) - e_y) * g.rdx;
+    if (xok) {
+      T d = (o.ez_x - o.e_z) * g.rdx;
+      T d2 = (o.ey_x - e_y) * g.rdx;
       if (px) {
-        const int64_t m = cidx<T, 2>(g, c.s, c.z, c.y, c.x);
-        const T b = ld(g.p[PBXH] + c.x), a = ld(g.p[PAXH] + c.x), k = ld(g.p[PKXH] + c.x);
-        const T m1 = b * m_ez_x[m] + a * d;
+        const int64_t m = z * s2 + o2;
+        const T m1 = fx.b * m_ez_x[m] + fx.a * d;
         m_ez_x[m] = m1;
-        d = div_k(d, k) + m1;
-        const T m2 = b * m_ey_x[m] + a * d2;
+        d = div_k(d, fx.k) + m1;
+        const T m2 = fx.b * m_ey_x[m] + fx.a * d2;
         m_ey_x[m] = m2;
-        d2 = div_k(d2, k) + m2;
+        d2 = div_k(d2, fx.k) + m2;
       }
       dEz_dx = d;
       dEy_dx = d2;
     }
-    hx[i] = hx[i] - q * (dEy_dz - dEz_dy);
-    hy[i] = hy[i] - q * (dEz_dx - dEx_dz);
-    hz[i] = hz[i] - q * (dEx_dy - dEy_dx);
+    hx[j] = o.h_x - o.q * (dEy_dz - dEz_dy);
+    hy[j] = o.h_y - o.q * (dEz_dx - dEx_dz);
+    hz[j] = o.h_z - o.q * (dEx_dy - dEy_dx);
+    e_x = o.n_x;
+    e_y = o.n_y;
+    o = on;
   }
 }
 
+// Operands of one forward-E cell (loaded one cell ahead, as OpsH).
+template <typename T> struct OpsE {
+  T a, b, h_x, h_y, h_z, hz_y, hz_x, hx_y, hy_x, e_x, e_y, e_z;
+};
+
 template <typename T, typename S>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restrict__ ex,
          T *__restrict__ ey, T *__restrict__ ez, const T *__restrict__ hx,
          const T *__restrict__ hy, const T *__restrict__ hz, T *__restrict__ m_hz_y,
@@ -182,24 +277,55 @@ k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restr
          T *__restrict__ m_hy_x, T *__restrict__ m_hx_y, S *__restrict__ st_ex,
          S *__restrict__ st_ey, S *__restrict__ st_ez, S *__restrict__ st_cx,
          S *__restrict__ st_cy, S *__restrict__ st_cz) {
-  Cell c;
-  if (!first_cell(g, c)) return;
-  const int64_t sz = (int64_t)g.ny * g.nx, sy = g.nx;
-  const bool py = c.y < g.y0 || c.y >= g.y1, px = c.x < g.x0 || c.x >= g.x1;
-  for (; c.z < c.zend; ++c.z) {
-    set_index(c, g.ny, g.nx, g.N);
-    const int64_t i = c.i;
-    const T a = ld(ca + (g.ca_b ? i : c.j)), b = ld(cb + (g.cb_b ? i : c.j));
-    const T h_x = ld(hx + i), h_y = ld(hy + i), h_z = ld(hz + i);
-    T dHy_dz = (h_y - ld(hy + i - sz)) * g.rdz;
-    T dHz_dy = (h_z - ld(hz + i - sy)) * g.rdy;
-    T dHz_dx = (h_z - ld(hz + i - 1)) * g.rdx;
-    T dHx_dz = (h_x - ld(hx + i - sz)) * g.rdz;
-    T dHx_dy = (h_x - ld(hx + i - sy)) * g.rdy;
-    T dHy_dx = (h_y - ld(hy + i - 1)) * g.rdx;
-    if (c.z < g.z0 || c.z >= g.z1) {
-      const int64_t m = cidx<T, 0>(g, c.s, c.z, c.y, c.x);
-      const T bb = ld(g.p[PBZ] + c.z), aa = ld(g.p[PAZ] + c.z), k = ld(g.p[PKZ] + c.z);
+  Col c;
+  if (!column(g, c)) return;
+  const int ny = g.ny, nx = g.nx, y = c.y, x = c.x;
+  const int64_t sz = (int64_t)ny * nx, sy = nx;
+  const int64_t base = (int64_t)c.s * g.N;
+  ex += base; ey += base; ez += base; hx += base; hy += base; hz += base;
+  if (g.ca_b) ca += base;
+  if (g.cb_b) cb += base;
+  const bool se = st_ex != nullptr, sc = st_cx != nullptr;
+  if (se) { st_ex += base; st_ey += base; st_ez += base; }
+  if (sc) { st_cx += base; st_cy += base; st_cz += base; }
+  m_hy_z += c.s * msz0(g); m_hx_z += c.s * msz0(g);
+  m_hz_y += c.s * msz1(g); m_hx_y += c.s * msz1(g);
+  m_hz_x += c.s * msz2(g); m_hy_x += c.s * msz2(g);
+  const bool py = y < g.y0 || y >= g.y1, px = x < g.x0 || x >= g.x1;
+  const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  auto load = [&](int64_t jj) {
+    OpsE<T> o;
+    o.a = ld(ca + jj);
+    o.b = ld(cb + jj);
+    o.h_x = ld(hx + jj);
+    o.h_y = ld(hy + jj);
+    o.h_z = ld(hz + jj);
+    o.hz_y = ld(hz + jj - sy);
+    o.hz_x = ld(hz + jj - 1);
+    o.hx_y = ld(hx + jj - sy);
+    o.hy_x = ld(hy + jj - 1);
+    o.e_x = ex[jj];
+    o.e_y = ey[jj];
+    o.e_z = ez[jj];
+    return o;
+  };
+  int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
+  T p_x = ld(hx + j - sz), p_y = ld(hy + j - sz);  // Hx, Hy at z - 1
+  OpsE<T> o = load(j);
+  for (int z = c.zb; z < c.ze; ++z, j += sz) {
+    OpsE<T> on{};
+    if (z + 1 < c.ze) on = load(j + sz);
+    T dHy_dz = (o.h_y - p_y) * g.rdz;
+    T dHz_dy = (o.h_z - o.hz_y) * g.rdy;
+    T dHz_dx = (o.h_z - o.hz_x) * g.rdx;
+    T dHx_dz = (o.h_x - p_x) * g.rdz;
+    T dHx_dy = (o.h_x - o.hx_y) * g.rdy;
+    T dHy_dx = (o.h_y - o.hy_x) * g.rdx;
+    if (z < g.z0 || z >= g.z1) {
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const T bb = ld(g.p[PBZ] + z), aa = ld(g.p[PAZ] + z), k = ld(g.p[PKZ] + z);
       const T m1 = bb * m_hy_z[m] + aa * dHy_dz;
       m_hy_z[m] = m1;
       dHy_dz = div_k(dHy_dz, k) + m1;
@@ -208,40 +334,40 @@ k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restr
       dHx_dz = div_k(dHx_dz, k) + m2;
     }
     if (py) {
-      const int64_t m = cidx<T, 1>(g, c.s, c.z, c.y, c.x);
-      const T bb = ld(g.p[PBY] + c.y), aa = ld(g.p[PAY] + c.y), k = ld(g.p[PKY] + c.y);
-      const T m1 = bb * m_hz_y[m] + aa * dHz_dy;
+      const int64_t m = z * s1 + o1;
+      const T m1 = fy.b * m_hz_y[m] + fy.a * dHz_dy;
       m_hz_y[m] = m1;
-      dHz_dy = div_k(dHz_dy, k) + m1;
-      const T m2 = bb * m_hx_y[m] + aa * dHx_dy;
+      dHz_dy = div_k(dHz_dy, fy.k) + m1;
+      const T m2 = fy.b * m_hx_y[m] + fy.a * dHx_dy;
       m_hx_y[m] = m2;
-      dHx_dy = div_k(dHx_dy, k) + m2;
+      dHx_dy = div_k(dHx_dy, fy.k) + m2;
     }
     if (px) {
-      const int64_t m = cidx<T, 2>(g, c.s, c.z, c.y, c.x);
-      const T bb = ld(g.p[PBX] + c.x), aa = ld(g.p[PAX] + c.x), k = ld(g.p[PKX] + c.x);
-      const T m1 = bb * m_hz_x[m] + aa * dHz_dx;
+      const int64_t m = z * s2 + o2;
+      const T m1 = fx.b * m_hz_x[m] + fx.a * dHz_dx;
       m_hz_x[m] = m1;
-      dHz_dx = div_k(dHz_dx, k) + m1;
-      const T m2 = bb * m_hy_x[m] + aa * dHy_dx;
+      dHz_dx = div_k(dHz_dx, fx.k) + m1;
+      const T m2 = fx.b * m_hy_x[m] + fx.a * dHy_dx;
       m_hy_x[m] = m2;
-      dHy_dx = div_k(dHy_dx, k) + m2;
+      dHy_dx = div_k(dHy_dx, fx.k) + m2;
     }
     const T cx = dHy_dz - dHz_dy, cy = dHz_dx - dHx_dz, cz = dHx_dy - dHy_dx;
-    const T e_x = ex[i], e_y = ey[i], e_z = ez[i];
-    if (st_ex) {
-      st_ex[i] = Snap<S, T>::enc(e_x);
-      st_ey[i] = Snap<S, T>::enc(e_y);
-      st_ez[i] = Snap<S, T>::enc(e_z);
+    if (se) {
+      st_ex[j] = Snap<S, T>::enc(o.e_x);
+      st_ey[j] = Snap<S, T>::enc(o.e_y);
+      st_ez[j] = Snap<S, T>::enc(o.e_z);
     }
-    if (st_cx) {
-      st_cx[i] = Snap<S, T>::enc(cx);
-      st_cy[i] = Snap<S, T>::enc(cy);
-      st_cz[i] = Snap<S, T>::enc(cz);
+    if (sc) {
+      st_cx[j] = Snap<S, T>::enc(cx);
+      st_cy[j] = Snap<S, T>::enc(cy);
+      st_cz[j] = Snap<S, T>::enc(cz);
     }
-    ex[i] = a * e_x + b * cx;
-    ey[i] = a * e_y + b * cy;
-    ez[i] = a * e_z + b * cz;
+    ex[j] = o.a * o.e_x + o.b * cx;
+    ey[j] = o.a * o.e_y + o.b * cy;
+    ez[j] = o.a * o.e_z + o.b * cz;
+    p_x = o.h_x;
+    p_y = o.h_y;
+    o = on;
   }
 }
 
@@ -274,152 +400,344 @@ template <typename T> struct Mem12 {
   T *m[kNMem];
 };
 
-__device__ __forceinline__ bool active3(int z, int y, int x, int nz, int ny, int nx) {
-  return z >= 1 && z < nz && y >= 1 && y < ny && x >= 1 && x < nx;
-}
-
-// E-side raw adjoint at the cell (z, y, x) (maxwell_3d_cuda_inst.cu:1478-1520).
-template <typename T, int AXIS, bool NEG>
-__device__ __forceinline__ T raw_e(const G3<T> &g, const T *cb, const T *lam, const T *mem,
-                                   int s, int z, int y, int x) {
-  if (!active3(z, y, x, g.nz, g.ny, g.nx)) return (T)0;
-  const int64_t j = ((int64_t)z * g.ny + y) * g.nx + x, i = (int64_t)s * g.N + j;
-  T q = ld(cb + (g.cb_b ? i : j)) * ld(lam + i);
-  if (NEG) q = -q;
-  const int c = AXIS == 0 ? z : AXIS == 1 ? y : x;
-  const int lo = AXIS == 0 ? g.z0 : AXIS == 1 ? g.y0 : g.x0;
-  const int hi = AXIS == 0 ? g.z1 : AXIS == 1 ? g.y1 : g.x1;
-  if (!(c < lo || c >= hi)) return q;
-  const int pa = AXIS == 0 ? PAZ : AXIS == 1 ? PAY : PAX;
-  const T m_used = ld(g.p[pa + 1] + c) * ld(mem + cidx<T, AXIS>(g, s, z, y, x)) + q;
-  return ld(g.p[pa] + c) * m_used + q / ld(g.p[PKZ + 2 * AXIS] + c);
-}
-
-// H-side raw adjoint (maxwell_3d_cuda_inst.cu:1522-1575).
-template <typename T, int AXIS, bool NEG>
-__device__ __forceinline__ T raw_h(const G3<T> &g, const T *cq, const T *lam, const T *mem,
-                                   int s, int z, int y, int x) {
-  if (!active3(z, y, x, g.nz, g.ny, g.nx)) return (T)0;
-  const int c = AXIS == 0 ? z : AXIS == 1 ? y : x;
-  const int n = AXIS == 0 ? g.nz : AXIS == 1 ? g.ny : g.nx;
-  if (c >= n - 1) return (T)0;
-  const int64_t j = ((int64_t)z * g.ny + y) * g.nx + x, i = (int64_t)s * g.N + j;
-  T q = ld(cq + (g.cq_b ? i : j)) * ld(lam + i);
-  if (NEG) q = -q;
-  const int lo = AXIS == 0 ? g.z0 : AXIS == 1 ? g.y0 : g.x0;
-  const int hi = AXIS == 0 ? g.z1h : AXIS == 1 ? g.y1h : g.x1h;
-  if (!(c < lo || c >= hi)) return q;
-  const int pa = AXIS == 0 ? PAZH : AXIS == 1 ? PAYH : PAXH;
-  const T m_used = ld(g.p[pa + 1] + c) * ld(mem + cidx<T, AXIS>(g, s, z, y, x)) + q;
-  return ld(g.p[pa] + c) * m_used + q / ld(g.p[PKZH + 2 * AXIS] + c);
-}
-
-// Adjoint of the forward E update (maxwell_3d_cuda_inst.cu:1625-1695):
-// next E-phase memories at the own cell, lambda_H gathers from lambda_E.
+// Raw adjoint term of a cell (maxwell_3d_cuda_inst.cu:1478-1575): q (the
+// signed product of coefficient and adjoint field) outside the CPML strip of
+// its axis, a (b m + q) + q / kappa inside it, m the current memory adjoint.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ T raw_term(T q, bool strip, T m, const Prof<T> &f) {
+  if (!strip) return q;
+  const T m_used = f.b * m + q;
+  return f.a * m_used + q / f.k;
+}
+
+// Operands of one adjoint-E cell: its own coefficient and lambda_E, those of
+// its y + 1 and x + 1 neighbours, and its lambda_H; loaded one cell ahead of
+// the arithmetic.
+template <typename T> struct OpsAE {
+  T b, lx, ly, lz, by_, lzy, lxy, bx_, lzx, lyx, hx, hy, hz;
+};
+
+// Adjoint of the forward E update (maxwell_3d_cuda_inst.cu:1625-1695): next
+// E-phase memory adjoints at the own cell (in their strips), lambda_H
+// gathers raw terms of the own cell and of its z + 1, y + 1, x + 1
+// neighbours (zero outside the update domain).  The z + 1 terms come from
+// the prefetched operands of the next cell and become the own z terms of the
+// next step of the march.
+template <typename T>
+__global__ void __launch_bounds__(256, 3)
 k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
          const T *__restrict__ ley, const T *__restrict__ lez, T *__restrict__ lhx,
          T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt) {
-  Cell c;
-  if (!first_cell(g, c)) return;
-  const bool py = c.y < g.y0 || c.y >= g.y1, px = c.x < g.x0 || c.x >= g.x1;
-  for (; c.z < c.zend; ++c.z) {
-    set_index(c, g.ny, g.nx, g.N);
-    const int64_t i = c.i;
-    const int s = c.s, z = c.z, y = c.y, x = c.x;
-    const T b = ld(cb + (g.cb_b ? i : c.j));
-    const T qx = b * ld(lex + i), qy = b * ld(ley + i), qz = b * ld(lez + i);
+  Col c;
+  if (!column(g, c)) return;
+  const int nz = g.nz, ny = g.ny, nx = g.nx, y = c.y, x = c.x;
+  const int64_t sz = (int64_t)ny * nx, sy = nx;
+  const int64_t base = (int64_t)c.s * g.N;
+  lex += base; ley += base; lez += base; lhx += base; lhy += base; lhz += base;
+  if (g.cb_b) cb += base;
+  const int64_t k0 = c.s * msz0(g), k1 = c.s * msz1(g), k2 = c.s * msz2(g);
+  const T *c_hy_z = cur.m[LHY_Z] + k0, *c_hx_z = cur.m[LHX_Z] + k0;
+  const T *c_hz_y = cur.m[LHZ_Y] + k1, *c_hx_y = cur.m[LHX_Y] + k1;
+  const T *c_hz_x = cur.m[LHZ_X] + k2, *c_hy_x = cur.m[LHY_X] + k2;
+  T *n_hy_z = nxt.m[LHY_Z] + k0, *n_hx_z = nxt.m[LHX_Z] + k0;
+  T *n_hz_y = nxt.m[LHZ_Y] + k1, *n_hx_y = nxt.m[LHX_Y] + k1;
+  T *n_hz_x = nxt.m[LHZ_X] + k2, *n_hy_x = nxt.m[LHY_X] + k2;
+  // strip state and profiles of the column and of its y + 1 / x + 1 neighbours
+  auto in_y = [&](int v) { return v < g.y0 || v >= g.y1; };
+  auto in_x = [&](int v) { return v < g.x0 || v >= g.x1; };
+  const bool py = in_y(y), px = in_x(x);
+  const bool y1ok = y + 1 < ny, x1ok = x + 1 < nx;
+  const bool py1 = y1ok && in_y(y + 1), px1 = x1ok && in_x(x + 1);
+  const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
+  const Prof<T> fy1 = prof_at(g, PAY, PKY, y + 1, py1), fx1 = prof_at(g, PAX, PKX, x + 1, px1);
+  const int64_t s1 = (int64_t)g.eyc * nx, s2 = (int64_t)ny * g.exc;
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x;
+  const int64_t o1n = (int64_t)ccoord(y + 1, g.y0, g.y1) * nx + x;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1);
+  const int64_t o2n = (int64_t)y * g.exc + ccoord(x + 1, g.x0, g.x1);
+  auto load = [&](int64_t jj) {
+    OpsAE<T> o{};
+    o.b = ld(cb + jj);
+    o.lx = ld(lex + jj);
+    o.ly = ld(ley + jj);
+    o.lz = ld(lez + jj);
+    if (y1ok) {
+      o.by_ = ld(cb + jj + sy);
+      o.lzy = ld(lez + jj + sy);
+      o.lxy = ld(lex + jj + sy);
+    }
+    if (x1ok) {
+      o.bx_ = ld(cb + jj + 1);
+      o.lzx = ld(lez + jj + 1);
+      o.lyx = ld(ley + jj + 1);
+    }
+    o.hx = lhx[jj];
+    o.hy = lhy[jj];
+    o.hz = lhz[jj];
+    return o;
+  };
+  // z-axis raw terms of cell z from its coefficient and lambda_E: r_hx from
+  // -cb ley with m_hx_z, r_hy from cb lex with m_hy_z
+  auto raw_z = [&](int z, T b, T lx, T ly, T &r_hx, T &r_hy) {
+    const T q_hx = -(b * ly), q_hy = b * lx;
     const bool pz = z < g.z0 || z >= g.z1;
-    {
-      const int64_t m = cidx<T, 0>(g, s, z, y, x);
+    T m_hx = 0, m_hy = 0;
+    Prof<T> fz{(T)0, (T)0, (T)1};
+    if (pz) {
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      m_hx = ld(c_hx_z + m);
+      m_hy = ld(c_hy_z + m);
+      fz = prof_at(g, PAZ, PKZ, z, true);
+    }
+    r_hx = raw_term(q_hx, pz, m_hx, fz);
+    r_hy = raw_term(q_hy, pz, m_hy, fz);
+  };
+  int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
+  OpsAE<T> o = load(j);
+  T rz_hx, rz_hy;
+  raw_z(c.zb, o.b, o.lx, o.ly, rz_hx, rz_hy);
+  for (int z = c.zb; z < c.ze; ++z, j += sz) {
+    // next cell's operands (also the z + 1 neighbour's), zero past the last plane
+    OpsAE<T> on{};
+    if (z + 1 < nz) on = load(j + sz);
+    const T qx = o.b * o.lx, qy = o.b * o.ly, qz = o.b * o.lz;
+    if (z < g.z0 || z >= g.z1) {
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
       const T bz = ld(g.p[PBZ] + z);
-      nxt.m[LHY_Z][m] = pz ? bz * cur.m[LHY_Z][m] + qx : (T)0;
-      nxt.m[LHX_Z][m] = pz ? bz * cur.m[LHX_Z][m] - qy : (T)0;
+      n_hy_z[m] = bz * ld(c_hy_z + m) + qx;
+      n_hx_z[m] = bz * ld(c_hx_z + m) - qy;
     }
-    {
-      const int64_t m = cidx<T, 1>(g, s, z, y, x);
-      const T by = ld(g.p[PBY] + y);
-      nxt.m[LHZ_Y][m] = py ? by * cur.m[LHZ_Y][m] - qx : (T)0;
-      nxt.m[LHX_Y][m] = py ? by * cur.m[LHX_Y][m] + qz : (T)0;
+    T m_zy = 0, m_xy = 0, m_zx = 0, m_yx = 0;
+    if (py) {
+      const int64_t m = z * s1 + o1;
+      m_zy = ld(c_hz_y + m);
+      m_xy = ld(c_hx_y + m);
+      n_hz_y[m] = fy.b * m_zy - qx;
+      n_hx_y[m] = fy.b * m_xy + qz;
     }
-    {
-      const int64_t m = cidx<T, 2>(g, s, z, y, x);
-      const T bx = ld(g.p[PBX] + x);
-      nxt.m[LHZ_X][m] = px ? bx * cur.m[LHZ_X][m] + qy : (T)0;
-      nxt.m[LHY_X][m] = px ? bx * cur.m[LHY_X][m] - qz : (T)0;
+    if (px) {
+      const int64_t m = z * s2 + o2;
+      m_zx = ld(c_hz_x + m);
+      m_yx = ld(c_hy_x + m);
+      n_hz_x[m] = fx.b * m_zx + qy;
+      n_hy_x[m] = fx.b * m_yx - qz;
     }
-    const T a1 = (raw_e<T, 0, true>(g, cb, ley, cur.m[LHX_Z], s, z, y, x) * (T)1 -
-                  raw_e<T, 0, true>(g, cb, ley, cur.m[LHX_Z], s, z + 1, y, x) * (T)1) * g.rdz;
-    const T a2 = (raw_e<T, 1, false>(g, cb, lez, cur.m[LHX_Y], s, z, y, x) * (T)1 -
-                  raw_e<T, 1, false>(g, cb, lez, cur.m[LHX_Y], s, z, y + 1, x) * (T)1) * g.rdy;
-    lhx[i] = lhx[i] + (a1 + a2);
-    const T b1 = (raw_e<T, 0, false>(g, cb, lex, cur.m[LHY_Z], s, z, y, x) * (T)1 -
-                  raw_e<T, 0, false>(g, cb, lex, cur.m[LHY_Z], s, z + 1, y, x) * (T)1) * g.rdz;
-    const T b2 = (raw_e<T, 2, true>(g, cb, lez, cur.m[LHY_X], s, z, y, x) * (T)1 -
-                  raw_e<T, 2, true>(g, cb, lez, cur.m[LHY_X], s, z, y, x + 1) * (T)1) * g.rdx;
-    lhy[i] = lhy[i] + (b1 + b2);
-    const T c1 = (raw_e<T, 1, true>(g, cb, lex, cur.m[LHZ_Y], s, z, y, x) * (T)1 -
-                  raw_e<T, 1, true>(g, cb, lex, cur.m[LHZ_Y], s, z, y + 1, x) * (T)1) * g.rdy;
-    const T c2 = (raw_e<T, 2, false>(g, cb, ley, cur.m[LHZ_X], s, z, y, x) * (T)1 -
-                  raw_e<T, 2, false>(g, cb, ley, cur.m[LHZ_X], s, z, y, x + 1) * (T)1) * g.rdx;
-    lhz[i] = lhz[i] + (c1 + c2);
+    T rz1_hx = 0, rz1_hy = 0;
+    if (z + 1 < nz) raw_z(z + 1, on.b, on.lx, on.ly, rz1_hx, rz1_hy);
+    // own y / x terms
+    const T ry_hx = raw_term(qz, py, m_xy, fy);   // cb lez, m_hx_y
+    const T ry_hz = raw_term(-qx, py, m_zy, fy);  // -cb lex, m_hz_y
+    const T rx_hy = raw_term(-qz, px, m_yx, fx);  // -cb lez, m_hy_x
+    const T rx_hz = raw_term(qy, px, m_zx, fx);   // cb ley, m_hz_x
+    // y + 1 and x + 1 neighbours' terms
+    T ry1_hx = 0, ry1_hz = 0, rx1_hy = 0, rx1_hz = 0;
+    if (y1ok) {
+      T mxy = 0, mzy = 0;
+      if (py1) {
+        const int64_t m = z * s1 + o1n;
+        mxy = ld(c_hx_y + m);
+        mzy = ld(c_hz_y + m);
+      }
+      ry1_hx = raw_term(o.by_ * o.lzy, py1, mxy, fy1);
+      ry1_hz = raw_term(-(o.by_ * o.lxy), py1, mzy, fy1);
+    }
+    if (x1ok) {
+      T myx = 0, mzx = 0;
+      if (px1) {
+        const int64_t m = z * s2 + o2n;
+        myx = ld(c_hy_x + m);
+        mzx = ld(c_hz_x + m);
+      }
+      rx1_hy = raw_term(-(o.bx_ * o.lzx), px1, myx, fx1);
+      rx1_hz = raw_term(o.bx_ * o.lyx, px1, mzx, fx1);
+    }
+    const T a1 = (rz_hx * (T)1 - rz1_hx * (T)1) * g.rdz;
+    const T a2 = (ry_hx * (T)1 - ry1_hx * (T)1) * g.rdy;
+    lhx[j] = o.hx + (a1 + a2);
+    const T b1 = (rz_hy * (T)1 - rz1_hy * (T)1) * g.rdz;
+    const T b2 = (rx_hy * (T)1 - rx1_hy * (T)1) * g.rdx;
+    lhy[j] = o.hy + (b1 + b2);
+    const T c1 = (ry_hz * (T)1 - ry1_hz * (T)1) * g.rdy;
+    const T c2 = (rx_hz * (T)1 - rx1_hz * (T)1) * g.rdx;
+    lhz[j] = o.hz + (c1 + c2);
+    rz_hx = rz1_hx;
+    rz_hy = rz1_hy;
+    o = on;
   }
 }
 
-// Adjoint of the forward H update (maxwell_3d_cuda_inst.cu:1748-1829).
+// Operands of one adjoint-H cell: its coefficients, lambda_H and lambda_E,
+// and the coefficient and lambda_H of its y - 1 and x - 1 neighbours; loaded
+// one cell ahead of the arithmetic.
+template <typename T> struct OpsAH {
+  T q, hx, hy, hz, a, ex, ey, ez, qy_, hzy, hxy, qx_, hzx, hyx;
+};
+
+// Adjoint of the forward H update (maxwell_3d_cuda_inst.cu:1748-1829): next
+// H-phase memory adjoints at the own cell (in their strips), lambda_E gathers
+// raw terms of its z - 1, y - 1, x - 1 neighbours and of the own cell (zero
+// outside the update domain and on the last plane of their axis); the own
+// z terms of a cell are the z - 1 terms of the next cell of the march.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
          const T *__restrict__ lhx, const T *__restrict__ lhy, const T *__restrict__ lhz,
          T *__restrict__ lex, T *__restrict__ ley, T *__restrict__ lez, Mem12<T> cur,
          Mem12<T> nxt) {
-  Cell c;
-  if (!first_cell(g, c)) return;
-  const bool py = c.y < g.ny - 1 && (c.y < g.y0 || c.y >= g.y1h);
-  const bool px = c.x < g.nx - 1 && (c.x < g.x0 || c.x >= g.x1h);
-  for (; c.z < c.zend; ++c.z) {
-    set_index(c, g.ny, g.nx, g.N);
-    const int64_t i = c.i;
-    const int s = c.s, z = c.z, y = c.y, x = c.x;
-    const T q = ld(cq + (g.cq_b ? i : c.j));
-    const T l_hx = ld(lhx + i), l_hy = ld(lhy + i), l_hz = ld(lhz + i);
-    const bool pz = z < g.nz - 1 && (z < g.z0 || z >= g.z1h);
-    {
-      const int64_t m = cidx<T, 0>(g, s, z, y, x);
+  Col c;
+  if (!column(g, c)) return;
+  const int nz = g.nz, ny = g.ny, nx = g.nx, y = c.y, x = c.x;
+  const int64_t sz = (int64_t)ny * nx, sy = nx;
+  const int64_t base = (int64_t)c.s * g.N;
+  lhx += base; lhy += base; lhz += base; lex += base; ley += base; lez += base;
+  if (g.ca_b) ca += base;
+  if (g.cq_b) cq += base;
+  const int64_t k0 = c.s * msz0(g), k1 = c.s * msz1(g), k2 = c.s * msz2(g);
+  const T *c_ey_z = cur.m[LEY_Z] + k0, *c_ex_z = cur.m[LEX_Z] + k0;
+  const T *c_ez_y = cur.m[LEZ_Y] + k1, *c_ex_y = cur.m[LEX_Y] + k1;
+  const T *c_ez_x = cur.m[LEZ_X] + k2, *c_ey_x = cur.m[LEY_X] + k2;
+  T *n_ey_z = nxt.m[LEY_Z] + k0, *n_ex_z = nxt.m[LEX_Z] + k0;
+  T *n_ez_y = nxt.m[LEZ_Y] + k1, *n_ex_y = nxt.m[LEX_Y] + k1;
+  T *n_ez_x = nxt.m[LEZ_X] + k2, *n_ey_x = nxt.m[LEY_X] + k2;
+  // raw terms exist for coordinates in [1, n - 1); strips use the half-cell bounds
+  auto in_y = [&](int v) { return v < g.y0 || v >= g.y1h; };
+  auto in_x = [&](int v) { return v < g.x0 || v >= g.x1h; };
+  const bool yok = y < ny - 1, xok = x < nx - 1;
+  const bool py = yok && in_y(y), px = xok && in_x(x);
+  const bool ymok = y - 1 >= 1, xmok = x - 1 >= 1;
+  const bool pym = ymok && in_y(y - 1), pxm = xmok && in_x(x - 1);
+  const Prof<T> fy = prof_at(g, PAYH, PKYH, y, py), fx = prof_at(g, PAXH, PKXH, x, px);
+  const Prof<T> fym = prof_at(g, PAYH, PKYH, y - 1, pym);
+  const Prof<T> fxm = prof_at(g, PAXH, PKXH, x - 1, pxm);
+  const int64_t s1 = (int64_t)g.eyc * nx, s2 = (int64_t)ny * g.exc;
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x;
+  const int64_t o1m = (int64_t)ccoord(y - 1, g.y0, g.y1) * nx + x;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1);
+  const int64_t o2m = (int64_t)y * g.exc + ccoord(x - 1, g.x0, g.x1);
+  auto load = [&](int64_t jj) {
+    OpsAH<T> o{};
+    o.q = ld(cq + jj);
+    o.hx = ld(lhx + jj);
+    o.hy = ld(lhy + jj);
+    o.hz = ld(lhz + jj);
+    o.a = ld(ca + jj);
+    o.ex = lex[jj];
+    o.ey = ley[jj];
+    o.ez = lez[jj];
+    if (ymok) {
+      o.qy_ = ld(cq + jj - sy);
+      o.hzy = ld(lhz + jj - sy);
+      o.hxy = ld(lhx + jj - sy);
+    }
+    if (xmok) {
+      o.qx_ = ld(cq + jj - 1);
+      o.hzx = ld(lhz + jj - 1);
+      o.hyx = ld(lhy + jj - 1);
+    }
+    return o;
+  };
+  // z-axis raw terms of cell z >= 1: r_ey from -cq lhx with m_ey_z, r_ex
+  // from cq lhy with m_ex_z (zero on the last plane)
+  auto raw_z = [&](int z, T q, T hx_, T hy_, T &r_ey, T &r_ex) {
+    if (z >= nz - 1) {
+      r_ey = r_ex = (T)0;
+      return;
+    }
+    const T q_ey = -(q * hx_), q_ex = q * hy_;
+    const bool pz = z < g.z0 || z >= g.z1h;
+    T m_ey = 0, m_ex = 0;
+    Prof<T> fz{(T)0, (T)0, (T)1};
+    if (pz) {
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      m_ey = ld(c_ey_z + m);
+      m_ex = ld(c_ex_z + m);
+      fz = prof_at(g, PAZH, PKZH, z, true);
+    }
+    r_ey = raw_term(q_ey, pz, m_ey, fz);
+    r_ex = raw_term(q_ex, pz, m_ex, fz);
+  };
+  int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
+  T rzm_ey = 0, rzm_ex = 0;  // terms of z - 1 (zero at z - 1 = 0)
+  if (c.zb - 1 >= 1)
+    raw_z(c.zb - 1, ld(cq + j - sz), ld(lhx + j - sz), ld(lhy + j - sz), rzm_ey, rzm_ex);
+  OpsAH<T> o = load(j);
+  for (int z = c.zb; z < c.ze; ++z, j += sz) {
+    OpsAH<T> on{};
+    if (z + 1 < c.ze) on = load(j + sz);
+    const T q = o.q, l_hx = o.hx, l_hy = o.hy, l_hz = o.hz;
+    const bool zok = z < nz - 1;
+    const bool pz = zok && (z < g.z0 || z >= g.z1h);
+    T m_eyz = 0, m_exz = 0;
+    if (pz) {
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
       const T bz = ld(g.p[PBZH] + z);
-      nxt.m[LEY_Z][m] = pz ? bz * cur.m[LEY_Z][m] - q * l_hx : (T)0;
-      nxt.m[LEX_Z][m] = pz ? bz * cur.m[LEX_Z][m] + q * l_hy : (T)0;
+      m_eyz = ld(c_ey_z + m);
+      m_exz = ld(c_ex_z + m);
+      n_ey_z[m] = bz * m_eyz - q * l_hx;
+      n_ex_z[m] = bz * m_exz + q * l_hy;
     }
-    {
-      const int64_t m = cidx<T, 1>(g, s, z, y, x);
-      const T by = ld(g.p[PBYH] + y);
-      nxt.m[LEZ_Y][m] = py ? by * cur.m[LEZ_Y][m] + q * l_hx : (T)0;
-      nxt.m[LEX_Y][m] = py ? by * cur.m[LEX_Y][m] - q * l_hz : (T)0;
+    T m_ezy = 0, m_exy = 0, m_ezx = 0, m_eyx = 0;
+    if (py) {
+      const int64_t m = z * s1 + o1;
+      m_ezy = ld(c_ez_y + m);
+      m_exy = ld(c_ex_y + m);
+      n_ez_y[m] = fy.b * m_ezy + q * l_hx;
+      n_ex_y[m] = fy.b * m_exy - q * l_hz;
     }
-    {
-      const int64_t m = cidx<T, 2>(g, s, z, y, x);
-      const T bx = ld(g.p[PBXH] + x);
-      nxt.m[LEZ_X][m] = px ? bx * cur.m[LEZ_X][m] - q * l_hy : (T)0;
-      nxt.m[LEY_X][m] = px ? bx * cur.m[LEY_X][m] + q * l_hz : (T)0;
+    if (px) {
+      const int64_t m = z * s2 + o2;
+      m_ezx = ld(c_ez_x + m);
+      m_eyx = ld(c_ey_x + m);
+      n_ez_x[m] = fx.b * m_ezx - q * l_hy;
+      n_ey_x[m] = fx.b * m_eyx + q * l_hz;
     }
-    const T a = ld(ca + (g.ca_b ? i : c.j));
-    const T v_x = a * lex[i], v_y = a * ley[i], v_z = a * lez[i];
-    const T e1 = (raw_h<T, 0, true>(g, cq, lhx, cur.m[LEY_Z], s, z - 1, y, x) * (T)1 -
-                  raw_h<T, 0, true>(g, cq, lhx, cur.m[LEY_Z], s, z, y, x) * (T)1) * g.rdz;
-    const T e2 = (raw_h<T, 2, false>(g, cq, lhz, cur.m[LEY_X], s, z, y, x - 1) * (T)1 -
-                  raw_h<T, 2, false>(g, cq, lhz, cur.m[LEY_X], s, z, y, x) * (T)1) * g.rdx;
-    ley[i] = v_y + (e1 + e2);
-    const T f1 = (raw_h<T, 0, false>(g, cq, lhy, cur.m[LEX_Z], s, z - 1, y, x) * (T)1 -
-                  raw_h<T, 0, false>(g, cq, lhy, cur.m[LEX_Z], s, z, y, x) * (T)1) * g.rdz;
-    const T f2 = (raw_h<T, 1, true>(g, cq, lhz, cur.m[LEX_Y], s, z, y - 1, x) * (T)1 -
-                  raw_h<T, 1, true>(g, cq, lhz, cur.m[LEX_Y], s, z, y, x) * (T)1) * g.rdy;
-    lex[i] = v_x + (f1 + f2);
-    const T h1 = (raw_h<T, 1, false>(g, cq, lhx, cur.m[LEZ_Y], s, z, y - 1, x) * (T)1 -
-                  raw_h<T, 1, false>(g, cq, lhx, cur.m[LEZ_Y], s, z, y, x) * (T)1) * g.rdy;
-    const T h2 = (raw_h<T, 2, true>(g, cq, lhy, cur.m[LEZ_X], s, z, y, x - 1) * (T)1 -
-                  raw_h<T, 2, true>(g, cq, lhy, cur.m[LEZ_X], s, z, y, x) * (T)1) * g.rdx;
-    lez[i] = v_z + (h1 + h2);
+    const T v_x = o.a * o.ex, v_y = o.a * o.ey, v_z = o.a * o.ez;
+    // own terms
+    T rz_ey = 0, rz_ex = 0;
+    if (zok) {
+      Prof<T> fz{(T)0, (T)0, (T)1};
+      if (pz) fz = prof_at(g, PAZH, PKZH, z, true);
+      rz_ey = raw_term(-(q * l_hx), pz, m_eyz, fz);
+      rz_ex = raw_term(q * l_hy, pz, m_exz, fz);
+    }
+    const T rx_ey = xok ? raw_term(q * l_hz, px, m_eyx, fx) : (T)0;     // cq lhz, m_ey_x
+    const T rx_ez = xok ? raw_term(-(q * l_hy), px, m_ezx, fx) : (T)0;  // -cq lhy, m_ez_x
+    const T ry_ex = yok ? raw_term(-(q * l_hz), py, m_exy, fy) : (T)0;  // -cq lhz, m_ex_y
+    const T ry_ez = yok ? raw_term(q * l_hx, py, m_ezy, fy) : (T)0;     // cq lhx, m_ez_y
+    // y - 1 and x - 1 neighbours' terms
+    T rym_ex = 0, rym_ez = 0, rxm_ey = 0, rxm_ez = 0;
+    if (ymok) {
+      T mexy = 0, mezy = 0;
+      if (pym) {
+        const int64_t m = z * s1 + o1m;
+        mexy = ld(c_ex_y + m);
+        mezy = ld(c_ez_y + m);
+      }
+      rym_ex = raw_term(-(o.qy_ * o.hzy), pym, mexy, fym);
+      rym_ez = raw_term(o.qy_ * o.hxy, pym, mezy, fym);
+    }
+    if (xmok) {
+      T meyx = 0, mezx = 0;
+      if (pxm) {
+        const int64_t m = z * s2 + o2m;
+        meyx = ld(c_ey_x + m);
+        mezx = ld(c_ez_x + m);
+      }
+      rxm_ey = raw_term(o.qx_ * o.hzx, pxm, meyx, fxm);
+      rxm_ez = raw_term(-(o.qx_ * o.hyx), pxm, mezx, fxm);
+    }
+    const T e1 = (rzm_ey * (T)1 - rz_ey * (T)1) * g.rdz;
+    const T e2 = (rxm_ey * (T)1 - rx_ey * (T)1) * g.rdx;
+    ley[j] = v_y + (e1 + e2);
+    const T f1 = (rzm_ex * (T)1 - rz_ex * (T)1) * g.rdz;
+    const T f2 = (rym_ex * (T)1 - ry_ex * (T)1) * g.rdy;
+    lex[j] = v_x + (f1 + f2);
+    const T h1 = (rym_ez * (T)1 - ry_ez * (T)1) * g.rdy;
+    const T h2 = (rxm_ez * (T)1 - rx_ez * (T)1) * g.rdx;
+    lez[j] = v_z + (h1 + h2);
+    rzm_ey = rz_ey;
+    rzm_ex = rz_ex;
+    o = on;
   }
 }
 
