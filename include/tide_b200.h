@@ -113,6 +113,40 @@ TIDE_TM_DECLARE(4, double)
 TIDE_TM_DECLARE(6, double)
 TIDE_TM_DECLARE(8, double)
 
+/* Argument list of maxwell_tm_*_born_forward_cuda, the Born (tangent)
+ * propagation behind operator.linearize(...).jvp.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1611-1703 (argtypes
+ * src/tide/backend_utils.py:336-349).  Advances the background state (ey ..
+ * m_hz_x, sources f0) and the scattered state (dey .. dm_hz_x, sources df)
+ * together; the scattered E update adds dca Ey^n + dcb curl H^n of the
+ * background.  r records the scattered Ey, background_r (may be null) the
+ * background Ey, at the receivers.  dca/dcb follow ca_batched/cb_batched. */
+#define TIDE_TM_BORN_FORWARD_ARGS(T)                                           \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T *ey, T *hx, T *hz, T *m_ey_x, T *m_ey_z,     \
+      T *m_hx_z, T *m_hz_x, T *dey, T *dhx, T *dhz, T *dm_ey_x, T *dm_ey_z,    \
+      T *dm_hx_z, T *dm_hz_x, T *r, T *background_r, T const *ay,              \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *ky, T const *kyh, T const *kx,      \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, bool ca_batched, bool cb_batched, bool cq_batched,   \
+      int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,         \
+      int64_t pml_x1, int64_t n_threads, int64_t device, void *compute_stream
+
+#define TIDE_TM_BORN_DECLARE(S, T)                                             \
+  void maxwell_tm_##S##_##T##_born_forward_cuda(TIDE_TM_BORN_FORWARD_ARGS(T));
+
+TIDE_TM_BORN_DECLARE(2, float)
+TIDE_TM_BORN_DECLARE(4, float)
+TIDE_TM_BORN_DECLARE(6, float)
+TIDE_TM_BORN_DECLARE(8, float)
+TIDE_TM_BORN_DECLARE(2, double)
+TIDE_TM_BORN_DECLARE(4, double)
+TIDE_TM_BORN_DECLARE(6, double)
+TIDE_TM_BORN_DECLARE(8, double)
+
 /* Allocation-free variant of maxwell_tm_2_float_forward_cuda (same arguments,
  * same results).  It has no counterpart in the reference.  It is for callers
  * that must not allocate device memory during the call -- code running inside

@@ -3,7 +3,8 @@
  * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg load
  * it, as the checker.  The product path never calls into this library.
  *
- * Exported symbols: tide_oracle_tm_{forward,forward_with_storage,backward}_
+ * Exported symbols: tide_oracle_tm_{forward,forward_with_storage,backward,
+ *   born_forward}_
  * {float,double}.  Their arguments mirror the reference native ABI
  * (src/tide/backend_utils.py:256-308) minus the storage-mode, stream, file
  * and Debye arguments, with the stencil order as the first argument.

@@ -186,6 +186,55 @@ static void FN(step_e)(const FN(geom) * g, const REAL *ca, const REAL *cb,
   }
 }
 
+/* Born E half-step for one shot (maxwell_tm_core.cuh:601-690): background
+ * and scattered curls with their own CPML memories; the scattered update adds
+ * dca Ey^n + dcb curl H^n of the background. */
+static void FN(step_e_born)(const FN(geom) * g, const REAL *ca, const REAL *cb,
+                            const REAL *dca, const REAL *dcb, const REAL *hx,
+                            const REAL *hz, REAL *ey, REAL *m_hx_z,
+                            REAL *m_hz_x, const REAL *dhx, const REAL *dhz,
+                            REAL *dey, REAL *dm_hx_z, REAL *dm_hz_x,
+                            int64_t s) {
+  const int64_t ny = g->ny, nx = g->nx, N = ny * nx;
+  const int p = g->stencil / 2;
+  for (int64_t y = p; y < ny - p + 1; ++y) {
+    for (int64_t x = p; x < nx - p + 1; ++x) {
+      const int64_t j = y * nx + x, i = s * N + j;
+      const REAL cav = g->ca_b ? ca[i] : ca[j];
+      const REAL cbv = g->cb_b ? cb[i] : cb[j];
+      const REAL dcav = g->ca_b ? dca[i] : dca[j];
+      const REAL dcbv = g->cb_b ? dcb[i] : dcb[j];
+      const bool pml_x = x < g->pml_x0 || x >= g->pml_x1;
+      const bool pml_y = y < g->pml_y0 || y >= g->pml_y1;
+      REAL dhz_dx = FN(d_x1)(hz, i, g->stencil, g->rdx);
+      REAL dhx_dz = FN(d_y1)(hx, i, nx, g->stencil, g->rdy);
+      if (pml_x) {
+        m_hz_x[i] = g->bx[x] * m_hz_x[i] + g->ax[x] * dhz_dx;
+        dhz_dx = dhz_dx / g->kx[x] + m_hz_x[i];
+      }
+      if (pml_y) {
+        m_hx_z[i] = g->by[y] * m_hx_z[i] + g->ay[y] * dhx_dz;
+        dhx_dz = dhx_dz / g->ky[y] + m_hx_z[i];
+      }
+      const REAL curl = dhz_dx - dhx_dz;
+      REAL ddhz_dx = FN(d_x1)(dhz, i, g->stencil, g->rdx);
+      REAL ddhx_dz = FN(d_y1)(dhx, i, nx, g->stencil, g->rdy);
+      if (pml_x) {
+        dm_hz_x[i] = g->bx[x] * dm_hz_x[i] + g->ax[x] * ddhz_dx;
+        ddhz_dx = ddhz_dx / g->kx[x] + dm_hz_x[i];
+      }
+      if (pml_y) {
+        dm_hx_z[i] = g->by[y] * dm_hx_z[i] + g->ay[y] * ddhx_dz;
+        ddhx_dz = ddhx_dz / g->ky[y] + dm_hx_z[i];
+      }
+      const REAL dcurl = ddhz_dx - ddhx_dz;
+      const REAL ey_n = ey[i], dey_n = dey[i];
+      ey[i] = cav * ey_n + cbv * curl;
+      dey[i] = cav * dey_n + cbv * dcurl + dcav * ey_n + dcbv * curl;
+    }
+  }
+}
+
 /* ---------------- exact adjoint (maxwell_tm_cuda_inst.cu:954-1165) -------- */
 
 static inline REAL FN(raw_x)(const FN(geom) * g, const REAL *cb,
@@ -419,6 +468,45 @@ void FN(tide_oracle_tm_forward_with_storage)(
         FN(inject)(ey, f + t * n_shots * n_src, sources_i, n_src, N, s);
       if (n_rec > 0)
         FN(record)(r + t * n_shots * n_rec, ey, receivers_i, n_rec, N, s);
+    }
+  }
+}
+
+/* Born forward: argument meaning of the reference's
+ * maxwell_tm_{S}_{dtype}_born_forward (maxwell_tm_inst.cpp:962-1045). */
+void FN(tide_oracle_tm_born_forward)(
+    int stencil, const REAL *ca, const REAL *cb, const REAL *cq,
+    const REAL *dca, const REAL *dcb, const REAL *f0, const REAL *df,
+    REAL *ey, REAL *hx, REAL *hz, REAL *m_ey_x, REAL *m_ey_z, REAL *m_hx_z,
+    REAL *m_hz_x, REAL *dey, REAL *dhx, REAL *dhz, REAL *dm_ey_x,
+    REAL *dm_ey_z, REAL *dm_hx_z, REAL *dm_hz_x, REAL *r, REAL *background_r,
+    const REAL *ay, const REAL *by, const REAL *ayh, const REAL *byh,
+    const REAL *ax, const REAL *bx, const REAL *axh, const REAL *bxh,
+    const REAL *ky, const REAL *kyh, const REAL *kx, const REAL *kxh,
+    const int64_t *sources_i, const int64_t *receivers_i, REAL rdy, REAL rdx,
+    int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, int64_t n_src,
+    int64_t n_rec, bool ca_batched, bool cb_batched, bool cq_batched,
+    int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,
+    int64_t pml_x1) {
+  ORACLE_GEOM_INIT
+  const int64_t N = ny * nx;
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < n_shots; ++s) {
+    for (int64_t t = start_t; t < start_t + nt; ++t) {
+      FN(step_h)(&g, cq, ey, hx, hz, m_ey_x, m_ey_z, s);
+      FN(step_h)(&g, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z, s);
+      FN(step_e_born)(&g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx,
+                      dhz, dey, dm_hx_z, dm_hz_x, s);
+      if (n_src > 0) {
+        FN(inject)(ey, f0 + t * n_shots * n_src, sources_i, n_src, N, s);
+        FN(inject)(dey, df + t * n_shots * n_src, sources_i, n_src, N, s);
+      }
+      if (n_rec > 0) {
+        FN(record)(r + t * n_shots * n_rec, dey, receivers_i, n_rec, N, s);
+        if (background_r)
+          FN(record)(background_r + t * n_shots * n_rec, ey, receivers_i,
+                     n_rec, N, s);
+      }
     }
   }
 }

@@ -101,6 +101,21 @@ class Oracle:
         return gca, gcb, gf, lam
 
 
+    def born_forward(self, pb, dca, dcb, f0, df, tan, r, bg_r, start_t=0, nt=None):
+        """Born forward: advance pb.fields (background) and tan (the 7
+        scattered state tensors) in place."""
+        nt = pb.nt if nt is None else nt
+        prof = [_p(pb.profiles[n]) for n in PROFILES]
+        P, I, B = c_void_p, c_int64, c_bool
+        fn, F = self._fn("born_forward", pb.dtype, None)
+        fn.argtypes = ([c_int] + [P] * 7 + [P] * 14 + [P] * 2 + [P] * 12 + [P, P, F, F]
+                       + [I] * 6 + [B] * 3 + [I] * 5)
+        fn(pb.stencil, _p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(f0), _p(df),
+           *[_p(t) for t in pb.fields], *[_p(t) for t in tan], _p(r), _p(bg_r), *prof,
+           _p(pb.sources_i), _p(pb.receivers_i), pb.rdy, pb.rdx, nt, pb.n_shots, pb.ny, pb.nx,
+           pb.n_src, pb.n_rec, pb.batched, pb.batched, pb.batched, start_t, pb.pml_y0,
+           pb.pml_x0, pb.pml_y1, pb.pml_x1)
+
 class OracleTM(torch.autograd.Function):
     """Autograd node over (ca, cb, f) backed by the C oracle (CPU)."""
 
@@ -151,6 +166,24 @@ class RefCPU:
            _p(pb.sources_i), _p(pb.receivers_i), pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.ny,
            pb.nx, pb.n_src, pb.n_rec, 1, False, pb.batched, pb.batched, pb.batched, 0, pb.pml_y0,
            pb.pml_x0, pb.pml_y1, pb.pml_x1, n_threads, 0, 0)
+
+    def born_forward(self, pb, dca, dcb, f0, df, tan, r, bg_r, n_threads=0):
+        """The reference's maxwell_tm_{S}_{dtype}_born_forward_cpu."""
+        import sys
+
+        sys.path.insert(0, str(REPO / "tide-gpr_b200"))
+        from tide_b200 import _native as nat
+
+        sfx = "float" if pb.dtype == torch.float32 else "double"
+        fn = getattr(self.lib, f"maxwell_tm_{pb.stencil}_{sfx}_born_forward_cpu")
+        fn.argtypes = nat.argtypes("maxwell_tm_born_forward", sfx)
+        fn.restype = None
+        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(f0), _p(df),
+           *[_p(t) for t in pb.fields], *[_p(t) for t in tan], _p(r), _p(bg_r),
+           *[_p(pb.profiles[n]) for n in PROFILES], _p(pb.sources_i), _p(pb.receivers_i),
+           pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec, 1,
+           pb.batched, pb.batched, pb.batched, 0, pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1,
+           n_threads, 0, 0)
 
 
 def rel_l2(a: torch.Tensor, b: torch.Tensor) -> float:

@@ -1,0 +1,106 @@
+"""Pinning of the Born (tangent) oracle.
+
+Three pins of the C restatement's Born forward (oracle/tm2d_oracle_impl.h,
+tide_oracle_tm_born_forward_*):
+* the reference's Python Born path (golden fixture born_case.npz, FP64,
+  stencils 2 and 4, with and without source linearization): bit for bit,
+  background and scattered receivers and the final scattered Ey;
+* the reference's CPU backend (maxwell_tm_{S}_{dtype}_born_forward_cpu,
+  compiled from the reference sources into oracle/_ref): background receivers
+  bit for bit; the scattered field to rounding (relative L2 <= 1e-5 FP32,
+  <= 1e-14 FP64), because that build's -Ofast reassociates the four-term
+  scattered update ca dE + cb dcurl + dca E + dcb curl;
+* a central finite difference of the oracle forward in (ca, cb, f): O(h^2).
+"""
+
+from __future__ import annotations
+
+import pytest
+import torch
+
+from cases import clone_problem, random_problem
+from oracle_harness import REF_SO, Oracle, RefCPU, rel_l2
+
+
+def _perturbation(pb, seed):
+    g = torch.Generator().manual_seed(seed)
+    shape = (1, pb.ny, pb.nx)
+    dca = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype)
+    dcb = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype) * pb.cb
+    df = (torch.randn(pb.f.shape, generator=g, dtype=torch.float64).to(pb.dtype) * 0.1
+          * pb.f.abs().max())
+    return dca.contiguous(), dcb.contiguous(), df.contiguous()
+
+
+def _zeros_r(pb):
+    return torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+
+
+def _tangent_state(pb):
+    return [torch.zeros_like(t) for t in pb.fields]
+
+
+def _run(driver, pb, dca, dcb, df):
+    q = clone_problem(pb)
+    tan = _tangent_state(q)
+    r, bg = _zeros_r(q), _zeros_r(q)
+    driver.born_forward(q, dca, dcb, q.f, df, tan, r, bg)
+    return r, bg, q.fields, tan
+
+
+@pytest.mark.skipif(not REF_SO.exists(), reason="reference CPU backend not built here")
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_born_oracle_equals_reference_cpu(stencil, dtype):
+    pb = random_problem(610 + stencil, 33, 41, 2, 70, stencil=stencil, dtype=dtype, pml=6)
+    dca, dcb, df = _perturbation(pb, 3)
+    got = _run(Oracle(), pb, dca, dcb, df)
+    ref = _run(RefCPU(), pb, dca, dcb, df)
+    assert torch.equal(got[1], ref[1]), "background receivers"
+    for a, b in zip(got[2], ref[2]):
+        assert torch.equal(a, b), "background state"
+    tol = 1e-5 if dtype == torch.float32 else 1e-14
+    assert rel_l2(got[0], ref[0]) <= tol
+    for a, b in zip(got[3], ref[3]):
+        assert rel_l2(a, b) <= tol
+    assert float(got[0].abs().max()) > 0
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("lin", [True, False])
+def test_born_oracle_equals_reference_python_golden(stencil, lin):
+    import numpy as np
+    from conftest import GOLDEN
+    from cases import hetero_inputs
+    from tide_b200.born import prepare_born
+    from tide_b200.tm2d import prepare_tm2d
+
+    z = np.load(GOLDEN / "born_case.npz")
+    c = hetero_inputs(torch.float64)
+    pb = prepare_tm2d(c["eps"], c["sig"], c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
+                      stencil=stencil, pml_width=c["pml"])
+    dca, dcb, df = prepare_born(pb, 1, c["dx"], c["amp"], depsilon=torch.from_numpy(z["deps"]),
+                                dsigma=torch.from_numpy(z["dsig"]), linearize_source=lin)
+    r, bg, _, tan = _run(Oracle(), pb, dca, dcb, df)
+    tag = f"s{stencil}_{'lin' if lin else 'nolin'}"
+    assert torch.equal(bg, torch.from_numpy(z[f"bg_r_{tag}"]))
+    assert torch.equal(r, torch.from_numpy(z[f"r_{tag}"])), rel_l2(r, torch.from_numpy(z[f"r_{tag}"]))
+    assert torch.equal(pb.crop(tan[0]), torch.from_numpy(z[f"dey_{tag}"]))
+
+
+def test_born_oracle_matches_central_difference():
+    pb = random_problem(77, 30, 38, 2, 80, dtype=torch.float64, pml=5)
+    dca, dcb, df = _perturbation(pb, 5)
+    r_born, bg, _, _ = _run(Oracle(), pb, dca, dcb, df)
+    o = Oracle()
+
+    def receivers(h):
+        q = clone_problem(pb)
+        r = _zeros_r(q)
+        o.forward(q, q.ca + h * dca, q.cb + h * dcb, q.f + h * df, r)
+        return r
+
+    h = 1e-4
+    fd = (receivers(h) - receivers(-h)) / (2 * h)
+    assert rel_l2(r_born, fd) < 1e-6
+    assert torch.equal(bg, receivers(0.0))

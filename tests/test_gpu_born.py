@@ -1,0 +1,201 @@
+"""Born (tangent) propagation on the GPU: the CUDA Born forward against the CPU
+oracle, the public ``borntm`` against the reference's Born (golden fixture),
+and ``MaxwellTM.linearize(...).jvp`` against the vjp (adjoint dot-product
+test) and against central differences of ``maxwelltm``.  The public API is
+compared with the reference golden to relative L2 <= 1e-13 in FP64.
+
+The CUDA kernels keep the reference's operation order without FMA
+contraction, so background and scattered receivers and states are
+bit-identical to the oracle (pinned to the reference in test_born_oracle.py);
+the FP32 bar (relative L2 <= 1e-5) is asserted next to every equality.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import tide_b200 as tide
+from cases import clone_problem, hetero_inputs, random_problem
+from conftest import GOLDEN
+from oracle_harness import Oracle, rel_l2
+from tide_b200 import _native as nat
+from tide_b200.tm2d import _PROFILE_ORDER
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _same(a, b, what):
+    a, b = a.detach().cpu(), b.detach().cpu()
+    err = rel_l2(a, b)
+    assert err <= TOL, f"{what}: rel l2 {err}"
+    assert torch.equal(a, b), f"{what}: not bit-identical (rel l2 {err})"
+
+
+def _perturbation(pb, seed):
+    g = torch.Generator().manual_seed(seed)
+    shape = (1, pb.ny, pb.nx)
+    dca = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype)
+    dcb = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype) * pb.cb
+    df = (torch.randn(pb.f.shape, generator=g, dtype=torch.float64).to(pb.dtype) * 0.1
+          * pb.f.abs().max())
+    return dca.contiguous(), dcb.contiguous(), df.contiguous()
+
+
+def _cuda_born(pb, dca, dcb, df, dev):
+    q = clone_problem(pb, dev)
+    tan = [torch.zeros_like(t) for t in q.fields]
+    r = torch.zeros((q.nt, q.n_shots, q.n_rec), device=dev, dtype=q.dtype)
+    bg = torch.zeros_like(r)
+    fn = nat.get_backend_function("maxwell_tm", "born_forward", q.stencil, q.dtype, dev)
+    d = [x.to(dev) for x in (dca, dcb, df)]
+    fn(nat.ptr(q.ca), nat.ptr(q.cb), nat.ptr(q.cq), nat.ptr(d[0]), nat.ptr(d[1]), nat.ptr(q.f),
+       nat.ptr(d[2]), *[nat.ptr(t) for t in q.fields], *[nat.ptr(t) for t in tan], nat.ptr(r),
+       nat.ptr(bg), *[nat.ptr(q.profiles[n]) for n in _PROFILE_ORDER], nat.ptr(q.sources_i),
+       nat.ptr(q.receivers_i), q.rdy, q.rdx, q.dt, q.nt, q.n_shots, q.ny, q.nx, q.n_src, q.n_rec,
+       1, q.batched, q.batched, q.batched, 0, q.pml_y0, q.pml_x0, q.pml_y1, q.pml_x1, 0,
+       dev.index or 0, torch.cuda.current_stream(dev).cuda_stream)
+    nat.check("born_forward")
+    torch.cuda.synchronize()
+    return r, bg, q.fields, tan
+
+
+def _oracle_born(pb, dca, dcb, df):
+    q = clone_problem(pb)
+    tan = [torch.zeros_like(t) for t in q.fields]
+    r = torch.zeros((q.nt, q.n_shots, q.n_rec), dtype=q.dtype)
+    bg = torch.zeros_like(r)
+    Oracle().born_forward(q, dca, dcb, q.f, df, tan, r, bg)
+    return r, bg, q.fields, tan
+
+
+@pytest.mark.parametrize("stencil", [2, 4, 6, 8])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_born_forward_bitwise_vs_oracle(cuda_device, stencil, dtype):
+    pb = random_problem(700 + stencil, 37, 53, 3, 60, stencil=stencil, dtype=dtype, pml=7)
+    dca, dcb, df = _perturbation(pb, stencil)
+    got = _cuda_born(pb, dca, dcb, df, cuda_device)
+    ref = _oracle_born(pb, dca, dcb, df)
+    _same(got[0], ref[0], "scattered receivers")
+    _same(got[1], ref[1], "background receivers")
+    for i, (a, b) in enumerate(zip(got[2] + got[3], ref[2] + ref[3])):
+        _same(a, b, f"state tensor {i}")
+    assert nat.device_status(cuda_device) == 0
+
+
+def test_born_edge_case_points(cuda_device):
+    """Duplicate, negative and out-of-domain sources and receivers."""
+    pb = random_problem(71, 26, 34, 2, 40, n_rec=6)
+    N = pb.ny * pb.nx
+    pb.sources_i = torch.cat([pb.sources_i, pb.sources_i, torch.tensor([[-1], [pb.nx]])],
+                             dim=1).contiguous()
+    pb.n_src = 3
+    f = torch.randn((pb.nt, pb.n_shots, 3), generator=torch.Generator().manual_seed(9))
+    pb.f = f.reshape(-1).contiguous()
+    ri = pb.receivers_i.clone()
+    ri[0, 1] = ri[0, 0]
+    ri[1, 2] = -1
+    ri[1, 3] = N - 1
+    pb.receivers_i = ri.contiguous()
+    dca, dcb, df = _perturbation(pb, 4)
+    got = _cuda_born(pb, dca, dcb, df, cuda_device)
+    ref = _oracle_born(pb, dca, dcb, df)
+    _same(got[0], ref[0], "scattered receivers")
+    _same(got[1], ref[1], "background receivers")
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("lin", [True, False])
+def test_borntm_public_api_vs_reference_golden(cuda_device, stencil, lin):
+    z = np.load(GOLDEN / "born_case.npz")
+    c = hetero_inputs(torch.float64)
+    dev = cuda_device
+    out = tide.borntm(
+        c["eps"].to(dev), c["sig"].to(dev), c["mu"].to(dev), c["dx"], c["dt"], c["amp"].to(dev),
+        c["src"].to(dev), c["rec"].to(dev), c["rec"].to(dev),
+        depsilon=torch.from_numpy(z["deps"]).to(dev), dsigma=torch.from_numpy(z["dsig"]).to(dev),
+        stencil=stencil, pml_width=c["pml"], linearize_source=lin,
+    )
+    tag = f"s{stencil}_{'lin' if lin else 'nolin'}"
+    assert len(out) == 16
+    # the host preparation (padding, dca/dcb, source values) runs as torch ops
+    # on the GPU, whose scalar arithmetic may round differently from the
+    # reference's CPU torch: FP64 agreement to 1e-13 (the kernels themselves
+    # are bit-identical to the oracle, test_born_forward_bitwise_vs_oracle)
+    for got, key in ((out[-1], f"r_{tag}"), (out[-2], f"bg_r_{tag}"), (out[7], f"dey_{tag}")):
+        ref = torch.from_numpy(z[key])
+        assert rel_l2(got, ref) <= 1e-13, key
+
+
+def _operator(dev, dtype=torch.float64, seed=3, stencil=2):
+    g = torch.Generator().manual_seed(seed)
+    ny, nx, S, nt = 30, 44, 2, 70
+    eps = (2.0 + 4.0 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    sig = (0.005 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    mu = torch.ones((ny, nx), device=dev, dtype=dtype)
+    dx = 0.02
+    dt = 0.9 * dx / (tide.C0 / float(eps.min().sqrt()) * 2 ** 0.5)
+    amp = tide.ricker(500e6, nt, dt, dtype=dtype).view(1, 1, nt).repeat(S, 1, 1).to(dev)
+    src = torch.tensor([[[10, 12]], [[15, 30]]], device=dev)
+    rec = torch.tensor([[[5, 5 + 3 * j] for j in range(10)]] * S, device=dev)
+    op = tide.MaxwellTM(tide.Discretization(dx, dt, stencil=stencil, boundary=tide.CPML(8)),
+                        tide.Experiment(tide.Acquisition(src, rec), amp))
+    # The Born perturbation is zero-padded into the CPML region (as the
+    # reference's), the forward model replicate-padded: directions that vanish
+    # on the outer model cells make the two maps' derivatives agree exactly.
+    mask = torch.zeros((ny, nx), dtype=torch.float64)
+    mask[2:-2, 2:-2] = 1.0
+    d_eps = 0.3 * mask * torch.randn((ny, nx), generator=g, dtype=torch.float64)
+    d_sig = 1e-3 * mask * torch.randn((ny, nx), generator=g, dtype=torch.float64)
+    return (op, tide.EMModel(eps, sig, mu),
+            tide.EMDirection(d_eps.to(dtype).to(dev), d_sig.to(dtype).to(dev)))
+
+
+def test_jvp_adjoint_dot_product(cuda_device):
+    """<J v, w> = <v, J^T w>: the Born jvp against the exact adjoint vjp (FP64)."""
+    op, model, v = _operator(cuda_device)
+    lin = op.linearize(model)
+    jv = lin.jvp(v)
+    w = torch.randn(jv.receiver_data.shape, generator=torch.Generator().manual_seed(2),
+                    dtype=torch.float64).to(cuda_device)
+    g = lin.vjp(w)
+    lhs = float((jv.receiver_data * w).sum())
+    rhs = float((g.epsilon * v.epsilon).sum() + (g.sigma * v.sigma).sum())
+    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), abs(rhs))
+    assert abs(lhs) > 0
+    # linear in the direction
+    jv2 = lin.jvp(tide.EMDirection(2 * v.epsilon, 2 * v.sigma))
+    assert rel_l2(jv2.receiver_data, 2 * jv.receiver_data) <= 1e-12
+
+
+def test_jvp_matches_central_difference(cuda_device):
+    op, model, v = _operator(cuda_device, stencil=4)
+    lin = op.linearize(model)
+    jv = lin.jvp(v).receiver_data
+    h = 1e-4
+
+    def data(s):
+        m = tide.EMModel(model.epsilon + s * v.epsilon, model.sigma + s * v.sigma, model.mu)
+        return op(m).receiver_data
+
+    fd = (data(h) - data(-h)) / (2 * h)
+    assert rel_l2(jv, fd) < 1e-6
+
+
+def test_jvp_fp32_equals_fp64_within_tolerance(cuda_device):
+    op64, m64, v64 = _operator(cuda_device, torch.float64)
+    op32, m32, v32 = _operator(cuda_device, torch.float32)
+    j64 = op64.linearize(m64).jvp(v64).receiver_data
+    j32 = op32.linearize(m32).jvp(v32).receiver_data
+    assert rel_l2(j32, j64) < 1e-4
+
+
+def test_unbuilt_linearization_parts_raise(cuda_device):
+    op, model, v = _operator(cuda_device)
+    lin = op.linearize(model)
+    with pytest.raises(NotImplementedError):
+        lin.second_vjp(v, torch.zeros_like(lin.primal.receiver_data))
+    with pytest.raises(NotImplementedError):
+        lin.jvp(tide.EMDirection(mu=torch.ones_like(model.mu)))

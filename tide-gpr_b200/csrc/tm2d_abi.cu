@@ -893,3 +893,6 @@ extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(flo
 
 // Debye-medium forward with storage and adjoint (same launch helpers).
 #include "tm2d_debye.cuh"
+
+// Born (tangent) forward of the linearization (same launch helpers).
+#include "tm2d_born.cuh"

@@ -1,0 +1,143 @@
+// Born (tangent) propagation of the TM2D path: the background state and the
+// scattered state advance together (maxwell_tm_cuda_inst.cu:1611-1703,
+// maxwell_tm_core.cuh:601-690).  Included by tm2d_abi.cu: both H half-steps
+// are the forward H kernel on the two states; one E kernel updates both
+// states, the scattered one with the extra terms dca Ey^n + dcb curl H^n of
+// the background, then injects the background sources (f0) and the
+// scattered sources (df) and records both states at the receivers.  Every
+// expression keeps the reference's operation order, so with the same inputs
+// the results are bit-identical to its CPU backend.
+#pragma once
+
+namespace tb {
+namespace {
+
+// Born E half-step.  Full-grid tiles of 32 x 8R (as k_fwd_e) so point
+// entries outside the update domain are still served.
+template <typename T, int ST, int R>
+__global__ void __launch_bounds__(256)
+k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
+         const T *__restrict__ dca, const T *__restrict__ dcb, const T *__restrict__ hx,
+         const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
+         T *__restrict__ m_hz_x, const T *__restrict__ dhx, const T *__restrict__ dhz,
+         T *__restrict__ dey, T *__restrict__ dm_hx_z, T *__restrict__ dm_hz_x, PointCSR src,
+         PointCSR rec, const T *__restrict__ f0_t, const T *__restrict__ df_t,
+         T *__restrict__ r_t, T *__restrict__ bgr_t) {
+  constexpr int P = FD<ST>::P;
+  const int x = blockIdx.x * kTileX + threadIdx.x;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
+  const int s = blockIdx.z;
+  const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const bool pts = !point_tile_empty(src, rec, tile);
+  if (x >= g.nx || y0 >= g.ny) return;
+  const int64_t base = (int64_t)s * g.N;
+  const bool xdom = x >= P && x < g.nx - P + 1;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (y >= g.ny) break;
+    const bool dom = xdom && y >= P && y < g.ny - P + 1;
+    if (!dom && !pts) continue;
+    const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+    T e = ey[i], de = dey[i];
+    if (dom) {
+      const T cav = g.ca_b ? ldg(ca + i) : ldg(ca + j);
+      const T cbv = g.cb_b ? ldg(cb + i) : ldg(cb + j);
+      const T dcav = g.ca_b ? ldg(dca + i) : ldg(dca + j);
+      const T dcbv = g.cb_b ? ldg(dcb + i) : ldg(dcb + j);
+      T dz = d_x1<T, ST>(hz, i, g.rdx), dy = d_y1<T, ST>(hx, i, g.nx, g.rdy);
+      T ddz = d_x1<T, ST>(dhz, i, g.rdx), ddy = d_y1<T, ST>(dhx, i, g.nx, g.rdy);
+      if (px) {
+        const T bxv = ldg(g.bx + x), axv = ldg(g.ax + x), kxv = ldg(g.kx + x);
+        const T m = bxv * m_hz_x[i] + axv * dz;
+        m_hz_x[i] = m;
+        dz = dz / kxv + m;
+        const T dm = bxv * dm_hz_x[i] + axv * ddz;
+        dm_hz_x[i] = dm;
+        ddz = ddz / kxv + dm;
+      }
+      if (y < g.pml_y0 || y >= g.pml_y1) {
+        const T byv = ldg(g.by + y), ayv = ldg(g.ay + y), kyv = ldg(g.ky + y);
+        const T m = byv * m_hx_z[i] + ayv * dy;
+        m_hx_z[i] = m;
+        dy = dy / kyv + m;
+        const T dm = byv * dm_hx_z[i] + ayv * ddy;
+        dm_hx_z[i] = dm;
+        ddy = ddy / kyv + dm;
+      }
+      const T curl = dz - dy, dcurl = ddz - ddy;
+      const T e_n = e, de_n = de;
+      e = cav * e_n + cbv * curl;
+      de = cav * de_n + cbv * dcurl + dcav * e_n + dcbv * curl;
+    }
+    if (pts) {
+      e = point_accumulate(src, tile, (int)j, f0_t, e);
+      de = point_accumulate(src, tile, (int)j, df_t, de);
+    }
+    ey[i] = e;
+    dey[i] = de;
+    if (pts) {
+      point_record(rec, tile, (int)j, r_t, de);
+      point_record(rec, tile, (int)j, bgr_t, e);
+    }
+  }
+}
+
+template <typename T, int ST>
+void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
+  (void)dt; (void)step_ratio; (void)n_threads;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0, "TM2D born_forward: nt must be >= 0");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z &&
+                 m_hz_x && dey && dhx && dhz && dm_ey_x && dm_ey_z && dm_hx_z && dm_hz_x,
+             "TM2D born_forward: a field, memory or coefficient pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || (f0 && df),
+             "TM2D born_forward: sources without background or scattered amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D born_forward: receivers without output");
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = as_stream(compute_stream);
+  PointScratch ps;
+  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+                    sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
+    return;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    if (L.has_domain) {
+      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+    }
+    k_born_e<T, ST, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+        L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
+        ps.src, ps.rec, f0 ? f0 + t * fs : nullptr, df ? df + t * fs : nullptr,
+        r ? r + t * rs : nullptr, background_r ? background_r + t * rs : nullptr);
+  }
+  count_launches(nt * (L.has_domain ? 3 : 1));
+  TB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+}  // namespace tb
+
+#define TB_BORN_DEFINE(S, T)                                                           \
+  extern "C" void maxwell_tm_##S##_##T##_born_forward_cuda(TIDE_TM_BORN_FORWARD_ARGS(T)) { \
+    tb::tm_born_forward<T, S>(                                                         \
+        ca, cb, cq, dca, dcb, f0, df, ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x, dey, dhx,   \
+        dhz, dm_ey_x, dm_ey_z, dm_hx_z, dm_hz_x, r, background_r, ay, by, ayh, byh, ax, bx,   \
+        axh, bxh, ky, kyh, kx, kxh, sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, \
+        n_sources_per_shot, n_receivers_per_shot, step_ratio, ca_batched, cb_batched,         \
+        cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device,               \
+        compute_stream);                                                               \
+  }
+
+TB_BORN_DEFINE(2, float)
+TB_BORN_DEFINE(4, float)
+TB_BORN_DEFINE(6, float)
+TB_BORN_DEFINE(8, float)
+TB_BORN_DEFINE(2, double)
+TB_BORN_DEFINE(4, double)
+TB_BORN_DEFINE(6, double)
+TB_BORN_DEFINE(8, double)

@@ -13,6 +13,7 @@ from .api import (
     BackendPreference,
     Discretization,
     EM3DState,
+    EMDirection,
     EMGradient,
     EMModel,
     ExecutionOptions,
@@ -24,6 +25,7 @@ from .api import (
     Maxwell3D,
     MaxwellTM,
     Observers,
+    TangentResult,
     TMState,
 )
 from .physics import (
@@ -38,14 +40,15 @@ from .physics import (
     upsample,
 )
 from .storage import StorageMode, StorageOptions
+from .born import borntm
 from .em3d import maxwell3d
 from .tm2d import CallbackState, maxwelltm, prepare_tm2d, propagate
 
 __all__ = [
     "CPML", "Acquisition", "BackendPreference", "C0", "CallbackState", "DebyeDispersion",
-    "Discretization", "EM3DState", "EMGradient", "EMModel", "EP0", "ExecutionOptions",
+    "Discretization", "EM3DState", "EMDirection", "EMGradient", "EMModel", "EP0", "ExecutionOptions",
     "Experiment", "FallbackPolicy", "ForwardResult", "LinearizedMaxwell3D",
-    "LinearizedMaxwellTM", "MU0", "Maxwell3D", "MaxwellTM", "Observers",
-    "StorageMode", "StorageOptions", "TMState", "cfl_condition", "downsample", "maxwell3d", "maxwelltm",
+    "LinearizedMaxwellTM", "MU0", "Maxwell3D", "MaxwellTM", "Observers", "TangentResult",
+    "StorageMode", "StorageOptions", "TMState", "borntm", "cfl_condition", "downsample", "maxwell3d", "maxwelltm",
     "prepare_parameters", "prepare_tm2d", "propagate", "ricker", "upsample",
 ]

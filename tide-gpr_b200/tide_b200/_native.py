@@ -46,6 +46,11 @@ SPECS: dict[str, list] = {
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6),
         *_TM_PROFILES, *_TM_TAIL, *_TM_STORAGE, *_TM_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:336-349
+    "maxwell_tm_born_forward": [
+        (_P, 3), (_P, 2), (_P, 2), (_P, 3), (_P, 4), (_P, 3), (_P, 4), (_P, 2),
+        *_TM_PROFILES, *_TM_TAIL, *_TM_FLAGS, (_P, 1),
+    ],
     # src/tide/backend_utils.py:289-308
     "maxwell_tm_backward": [
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6), (_P, 1), (_P, 2), (_P, 2),
@@ -177,6 +182,10 @@ def exported_symbols() -> list[str]:
         for a in ACCURACIES
         for d in ("float", "double")
         for p in PASSES
+    ] + [
+        symbol_name("maxwell_tm", "born_forward", a, d)
+        for a in ACCURACIES
+        for d in ("float", "double")
     ] + [
         symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D

@@ -196,6 +196,39 @@ class ForwardResult:
 
 
 @dataclass(frozen=True, slots=True)
+class EMDirection:
+    """A direction in model space (contracts.py:143-166)."""
+
+    epsilon: torch.Tensor | None = None
+    sigma: torch.Tensor | None = None
+    mu: torch.Tensor | None = None
+
+    def validate_for(self, model: EMModel) -> None:
+        if self.epsilon is None and self.sigma is None and self.mu is None:
+            raise ValueError("At least one model direction must be provided.")
+        for name, direction, parameter in (
+            ("epsilon", self.epsilon, model.epsilon),
+            ("sigma", self.sigma, model.sigma),
+            ("mu", self.mu, model.mu),
+        ):
+            if direction is not None and (
+                direction.shape != parameter.shape
+                or direction.device != parameter.device
+                or direction.dtype != parameter.dtype
+            ):
+                raise ValueError(f"The {name} direction must match the corresponding model tensor.")
+
+
+@dataclass(frozen=True, slots=True)
+class TangentResult:
+    """Receiver data and final scattered state of one tangent propagation
+    (results.py:67-72)."""
+
+    receiver_data: torch.Tensor
+    final_state: TMState | EM3DState
+
+
+@dataclass(frozen=True, slots=True)
 class EMGradient:
     epsilon: torch.Tensor | None
     sigma: torch.Tensor | None
@@ -301,8 +334,34 @@ class LinearizedMaxwellTM:
         g = dict(zip(self.targets, grads))
         return EMGradient(epsilon=g.get("epsilon"), sigma=g.get("sigma"))
 
-    def jvp(self, direction):  # pragma: no cover - documented gap
-        raise NotImplementedError("Born (jvp) propagation is not built in tide_b200.")
+    def jvp(self, direction: EMDirection) -> TangentResult:
+        """Apply the Jacobian J(model) to a model direction: the Born scattered
+        receiver data and final scattered state (linearization.py:162-229).
+        The direction's epsilon / sigma parts are used; a mu part raises."""
+        direction.validate_for(self.model)
+        if direction.mu is not None:
+            raise NotImplementedError("TM2D tangent propagation for mu is not available.")
+        from .born import borntm
+
+        op = self.operator
+        d, e = op.discretization, op.experiment
+        res = borntm(
+            self.model.epsilon, self.model.sigma, self.model.mu, grid_spacing=d.spacing,
+            dt=d.dt, source_amplitude=e.source_amplitude,
+            source_location=e.acquisition.source_location,
+            receiver_location=e.acquisition.receiver_location,
+            bg_receiver_location=e.acquisition.receiver_location,
+            depsilon=direction.epsilon, dsigma=direction.sigma, stencil=d.stencil,
+            pml_width=d.boundary.width, max_vel=d.max_velocity, nt=e.nt,
+            model_gradient_sampling_interval=op.model_gradient_sampling_interval,
+        )
+        return TangentResult(res[-1], TMState.from_tensors(res[7:14]))
+
+    def second_vjp(self, direction: EMDirection, cotangent: torch.Tensor) -> EMGradient:
+        """Gradient of <cotangent, J(model) direction> with respect to the
+        model: needs the Born adjoint with background gradients, which this
+        build does not have."""
+        raise NotImplementedError("second_vjp (Born adjoint) is not built in tide_b200.")
 
 
 class Maxwell3D:
@@ -386,3 +445,6 @@ class LinearizedMaxwell3D(LinearizedMaxwellTM):
                        storage=storage,
                        model_gradient_sampling_interval=operator.model_gradient_sampling_interval)
         self._result = op(self.model, retain_history=True)
+
+    def jvp(self, direction: EMDirection) -> TangentResult:
+        raise NotImplementedError("3-D Born (jvp) propagation is not built in tide_b200.")
