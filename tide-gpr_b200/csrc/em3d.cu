@@ -797,17 +797,17 @@ k3_coeff_grad(G3<T> g, const T *__restrict__ lex, const T *__restrict__ ley,
   }
 }
 
-// grad[j] += sum over shots of grad_shot[s, j] (shot order), then clear.
+// grad[j] += sum over shots of grad_shot[s, j] (shot order), then clear.  The
+// shot loads come first and the clearing stores after them, so a thread's
+// loads are all in flight together.
 template <typename T>
 __global__ void k3_combine(T *__restrict__ grad, T *__restrict__ shot, int S, int64_t N) {
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < N;
        j += (int64_t)gridDim.x * blockDim.x) {
     T sum = 0;
-    for (int s = 0; s < S; ++s) {
-      sum = sum + shot[(int64_t)s * N + j];
-      shot[(int64_t)s * N + j] = (T)0;
-    }
+    for (int s = 0; s < S; ++s) sum = sum + shot[(int64_t)s * N + j];
     grad[j] = grad[j] + sum;
+    for (int s = 0; s < S; ++s) shot[(int64_t)s * N + j] = (T)0;
   }
 }
 
