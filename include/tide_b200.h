@@ -266,6 +266,38 @@ void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
 TIDE_3D_DECLARE(2, float)
 TIDE_3D_DECLARE(2, double)
 
+/* maxwell_3d_*_born_forward_cuda, the 3-D Born (tangent) propagation.
+ * Replaces maxwell_3d_{S}_{dtype}_born_forward_cuda (CPU counterpart
+ * src/tide/csrc/em3d/maxwell_3d_inst.cpp:1100-1527; argtypes
+ * src/tide/backend_utils.py:556-577).  Background state (ex .. m_ey_x,
+ * sources f0) and scattered state (dex .. dm_ey_x, sources df) advance
+ * together; the scattered E update adds dca E^n + dcb curl H^n of the
+ * background.  r records the scattered, background_r (may be null) the
+ * background receiver component.  CPML memories compacted as for forward. */
+#define TIDE_3D_BORN_FORWARD_ARGS(T)                                           \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T *ex, T *ey, T *ez, T *hx, T *hy, T *hz,      \
+      T *m_hz_y, T *m_hy_z, T *m_hx_z, T *m_hz_x, T *m_hy_x, T *m_hx_y,        \
+      T *m_ey_z, T *m_ez_y, T *m_ez_x, T *m_ex_z, T *m_ex_y, T *m_ey_x,        \
+      T *dex, T *dey, T *dez, T *dhx, T *dhy, T *dhz, T *dm_hz_y, T *dm_hy_z,  \
+      T *dm_hx_z, T *dm_hz_x, T *dm_hy_x, T *dm_hx_y, T *dm_ey_z, T *dm_ez_y,  \
+      T *dm_ez_x, T *dm_ex_z, T *dm_ex_y, T *dm_ey_x, T *r, T *background_r,   \
+      T const *az, T const *bz, T const *azh, T const *bzh, T const *ay,       \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *kz, T const *kzh, T const *ky,      \
+      T const *kyh, T const *kx, T const *kxh, int64_t const *sources_i,       \
+      int64_t const *receivers_i, T rdz, T rdy, T rdx, T dt, int64_t nt,       \
+      int64_t n_shots, int64_t nz, int64_t ny, int64_t nx,                     \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, bool ca_batched, bool cb_batched, bool cq_batched,   \
+      int64_t start_t, int64_t pml_z0, int64_t pml_y0, int64_t pml_x0,         \
+      int64_t pml_z1, int64_t pml_y1, int64_t pml_x1,                          \
+      int64_t source_component, int64_t receiver_component, int64_t n_threads, \
+      int64_t device, int64_t execution_backend, void *compute_stream
+
+void maxwell_3d_2_float_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(float));
+void maxwell_3d_2_double_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(double));
+
 /* Comma-separated CUDA architectures the library was built for ("100a").
  * Replaces tide_cuda_arches, src/tide/csrc/storage/storage_utils.cu:213. */
 const char *tide_cuda_arches(void);

@@ -202,6 +202,61 @@ static void FN(step_e)(const FN(g3) * g, const REAL *ca, const REAL *cb, REAL **
         }
 }
 
+/* Born E half-step (maxwell_3d_inst.cpp:1390-1475): background and scattered
+ * curls with their own CPML memories; the scattered update adds
+ * dca E^n + dcb curl H^n of the background. */
+static void FN(step_e_born)(const FN(g3) * g, const REAL *ca, const REAL *cb, const REAL *dca,
+                            const REAL *dcb, REAL **F, REAL **M, REAL **DF, REAL **DM) {
+  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = 1; z < g->nz; ++z)
+      for (int64_t y = 1; y < g->ny; ++y)
+        for (int64_t x = 1; x < g->nx; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL a = ca[g->ca_b ? i : j], b = cb[g->cb_b ? i : j];
+          const REAL da = dca[g->ca_b ? i : j], db = dcb[g->cb_b ? i : j];
+          const int pz = z < g->z0 || z >= g->z1, py = y < g->y0 || y >= g->y1,
+                    px = x < g->x0 || x >= g->x1;
+          REAL c[2][3];
+          for (int w = 0; w < 2; ++w) {
+            REAL **H = w ? DF : F, **Q = w ? DM : M;
+            const REAL *hx = H[3], *hy = H[4], *hz = H[5];
+            REAL dHy_dz = (hy[i] - hy[i - sz]) * g->rdz;
+            REAL dHz_dy = (hz[i] - hz[i - sy]) * g->rdy;
+            REAL dHz_dx = (hz[i] - hz[i - 1]) * g->rdx;
+            REAL dHx_dz = (hx[i] - hx[i - sz]) * g->rdz;
+            REAL dHx_dy = (hx[i] - hx[i - sy]) * g->rdy;
+            REAL dHy_dx = (hy[i] - hy[i - 1]) * g->rdx;
+            if (pz) {
+              Q[1][i] = g->p[BZ][z] * Q[1][i] + g->p[AZ][z] * dHy_dz;
+              dHy_dz = dHy_dz / g->p[KZ][z] + Q[1][i];
+              Q[2][i] = g->p[BZ][z] * Q[2][i] + g->p[AZ][z] * dHx_dz;
+              dHx_dz = dHx_dz / g->p[KZ][z] + Q[2][i];
+            }
+            if (py) {
+              Q[0][i] = g->p[BY][y] * Q[0][i] + g->p[AY][y] * dHz_dy;
+              dHz_dy = dHz_dy / g->p[KY][y] + Q[0][i];
+              Q[5][i] = g->p[BY][y] * Q[5][i] + g->p[AY][y] * dHx_dy;
+              dHx_dy = dHx_dy / g->p[KY][y] + Q[5][i];
+            }
+            if (px) {
+              Q[3][i] = g->p[BX][x] * Q[3][i] + g->p[AX][x] * dHz_dx;
+              dHz_dx = dHz_dx / g->p[KX][x] + Q[3][i];
+              Q[4][i] = g->p[BX][x] * Q[4][i] + g->p[AX][x] * dHy_dx;
+              dHy_dx = dHy_dx / g->p[KX][x] + Q[4][i];
+            }
+            c[w][0] = dHy_dz - dHz_dy;
+            c[w][1] = dHz_dx - dHx_dz;
+            c[w][2] = dHx_dy - dHy_dx;
+          }
+          for (int k = 0; k < 3; ++k) {
+            const REAL e_old = F[k][i];
+            DF[k][i] = a * DF[k][i] + b * c[1][k] + da * e_old + db * c[0][k];
+            F[k][i] = a * e_old + b * c[0][k];
+          }
+        }
+}
+
 static void FN(inject)(REAL *field, const REAL *vals, const int64_t *idx, int64_t S, int64_t n,
                        int64_t N) {
   for (int64_t s = 0; s < S; ++s)
@@ -266,6 +321,34 @@ void FN(tide_oracle_em3d_forward)(const REAL *ca, const REAL *cb, const REAL *cq
     FN(step_e)(&g, ca, cb, F, M, store ? st : 0, fmt);
     if (n_src > 0 && f && src_i) FN(inject)(F[src_comp], f + t * S * n_src, src_i, S, n_src, g.N);
     if (n_rec > 0 && r && rec_i) FN(record)(r + t * S * n_rec, F[rec_comp], rec_i, S, n_rec, g.N);
+  }
+}
+
+/* Born forward over steps [start_t, start_t + nt) (maxwell_3d_inst.cpp:
+ * 1100-1527): F/M background, DF/DM scattered state; r records the scattered
+ * and bg_r (may be NULL) the background receiver component. */
+void FN(tide_oracle_em3d_born_forward)(const REAL *ca, const REAL *cb, const REAL *cq,
+                                       const REAL *dca, const REAL *dcb, const REAL *f0,
+                                       const REAL *df, REAL **F, REAL **M, REAL **DF, REAL **DM,
+                                       REAL *r, REAL *bg_r, const REAL **prof,
+                                       const int64_t *src_i, const int64_t *rec_i, REAL rdz,
+                                       REAL rdy, REAL rdx, int64_t nt, int64_t S, int64_t nz,
+                                       int64_t ny, int64_t nx, int64_t n_src, int64_t n_rec,
+                                       int64_t start_t, const int64_t *pml, int ca_b, int cb_b,
+                                       int cq_b, int src_comp, int rec_comp) {
+  FN(g3) g;
+  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    FN(step_h)(&g, cq, F, M);
+    FN(step_h)(&g, cq, DF, DM);
+    FN(step_e_born)(&g, ca, cb, dca, dcb, F, M, DF, DM);
+    if (n_src > 0 && f0 && src_i) {
+      FN(inject)(F[src_comp], f0 + t * S * n_src, src_i, S, n_src, g.N);
+      FN(inject)(DF[src_comp], df + t * S * n_src, src_i, S, n_src, g.N);
+    }
+    if (n_rec > 0 && r && rec_i) FN(record)(r + t * S * n_rec, DF[rec_comp], rec_i, S, n_rec, g.N);
+    if (n_rec > 0 && bg_r && rec_i)
+      FN(record)(bg_r + t * S * n_rec, F[rec_comp], rec_i, S, n_rec, g.N);
   }
 }
 

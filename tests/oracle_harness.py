@@ -249,6 +249,19 @@ class Oracle3D:
            int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp,
            st if st is not None else None, k, fmt)
 
+    def born_forward(self, pb, dca, dcb, f0, df, fields, mem, dfields, dmem, r, bg_r):
+        """3-D Born forward on full-layout state lists (see full_state)."""
+        fn, F = self._fn("born_forward", pb.dtype)
+        P, I = c_void_p, c_int64
+        pml = (c_int64 * 6)(*pb.pml)
+        fn.argtypes = [P] * 7 + [P] * 4 + [P, P, P, P, P] + [F, F, F] + [I] * 8 + [P] + [c_int] * 5
+        prof = _ptr_array([pb.profiles[n].cpu() for n in PROFILES_3D])
+        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq.cpu()), _p(dca), _p(dcb), _p(f0), _p(df),
+           _ptr_array(fields), _ptr_array(mem), _ptr_array(dfields), _ptr_array(dmem), _p(r),
+           _p(bg_r), prof, _p(pb.sources_i.cpu()), _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy,
+           pb.rdx, pb.nt, pb.n_shots, pb.nz, pb.ny, pb.nx, pb.n_src, pb.n_rec, 0, pml,
+           int(pb.batched), int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp)
+
     def backward(self, pb, ca, cb, grad_r, store, *, k=1, fmt=0, need_ca=True, need_cb=True,
                  need_f=True, start_t=None, nt=None, lam=None, grads=None, eps_sigma=False):
         """Returns (grad_ca, grad_cb, grad_f, lam_fields, lam_mem[, grad_eps, grad_sigma])."""
@@ -333,6 +346,26 @@ class RefCPU3D:
            _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.nz,
            pb.ny, pb.nx, pb.n_src, pb.n_rec, 1, False, b, b, b, 0, *pb.pml, pb.src_comp,
            pb.rec_comp, n_threads, 0, 0, 0)
+
+    def born_forward(self, pb, dca, dcb, f0, df, fields, mem, dfields, dmem, r, bg_r,
+                     n_threads=0):
+        import sys
+
+        sys.path.insert(0, str(REPO / "tide-gpr_b200"))
+        from tide_b200 import _native as nat
+
+        sfx = "float" if pb.dtype == torch.float32 else "double"
+        fn = getattr(self.lib, f"maxwell_3d_2_{sfx}_born_forward_cpu")
+        fn.argtypes = nat.argtypes("maxwell_3d_born_forward", sfx)
+        fn.restype = None
+        b = pb.batched
+        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq.cpu()), _p(dca), _p(dcb), _p(f0), _p(df),
+           *[_p(t) for t in fields], *[_p(t) for t in mem], *[_p(t) for t in dfields],
+           *[_p(t) for t in dmem], _p(r), _p(bg_r),
+           *[_p(pb.profiles[n].cpu()) for n in PROFILES_3D], _p(pb.sources_i.cpu()),
+           _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, pb.n_shots, pb.nz,
+           pb.ny, pb.nx, pb.n_src, pb.n_rec, 1, b, b, b, 0, *pb.pml, pb.src_comp, pb.rec_comp,
+           n_threads, 0, 0, 0)
 
 
 class OracleDebye:

@@ -104,3 +104,84 @@ def test_born_oracle_matches_central_difference():
     fd = (receivers(h) - receivers(-h)) / (2 * h)
     assert rel_l2(r_born, fd) < 1e-6
     assert torch.equal(bg, receivers(0.0))
+
+
+# ---------------------------------------------------------------------- 3-D
+def _case3d(dtype, comps=("ey", "ey"), seed=5):
+    from tide_b200.em3d import prepare_em3d
+
+    g = torch.Generator().manual_seed(seed)
+    nz, ny, nx, S, nt = 9, 10, 11, 2, 40
+    eps = (1.5 + 6.0 * torch.rand((nz, ny, nx), generator=g, dtype=torch.float64)).to(dtype)
+    sig = (0.006 * torch.rand((nz, ny, nx), generator=g, dtype=torch.float64)).to(dtype)
+    mu = torch.ones((nz, ny, nx), dtype=dtype)
+    dx = 0.02
+    dt = 0.9 * dx / (299792458.0 / float(eps.min().double().sqrt()) * 3 ** 0.5)
+    t = torch.arange(nt, dtype=torch.float64) * dt
+    amp = (torch.sin(2 * 3.14159265 * 6e8 * t) * torch.exp(-((t - 3e-9) / 1e-9) ** 2))
+    amp = amp.view(1, 1, nt).repeat(S, 1, 1).to(dtype)
+    src = torch.stack([torch.randint(2, n - 2, (S, 1), generator=g) for n in (nz, ny, nx)], -1)
+    rec = torch.stack([torch.randint(0, n, (S, 4), generator=g) for n in (nz, ny, nx)], -1)
+    return prepare_em3d(eps, sig, mu, dx, dt, amp, src, rec, pml_width=3,
+                        source_component=comps[0], receiver_component=comps[1])
+
+
+def _perturbation3d(pb, seed):
+    g = torch.Generator().manual_seed(seed)
+    shape = (1, pb.nz, pb.ny, pb.nx)
+    dca = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype)
+    dcb = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype) * pb.cb
+    df = (torch.randn(pb.f.shape, generator=g, dtype=torch.float64).to(pb.dtype) * 0.1
+          * pb.f.abs().max())
+    return dca.contiguous(), dcb.contiguous(), df.contiguous()
+
+
+def _run3d(driver, pb, dca, dcb, df):
+    from oracle_harness import Oracle3D
+
+    F, M = Oracle3D.full_state(pb)
+    DF, DM = [torch.zeros_like(t) for t in F], [torch.zeros_like(t) for t in M]
+    r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+    bg = torch.zeros_like(r)
+    driver.born_forward(pb, dca, dcb, pb.f, df, F, M, DF, DM, r, bg)
+    return r, bg, F + M, DF + DM
+
+
+@pytest.mark.skipif(not REF_SO.exists(), reason="reference CPU backend not built here")
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("comps", [("ey", "ey"), ("ex", "ez")])
+def test_born3d_oracle_equals_reference_cpu(dtype, comps):
+    from oracle_harness import Oracle3D, RefCPU3D
+
+    pb = _case3d(dtype, comps)
+    dca, dcb, df = _perturbation3d(pb, 7)
+    got = _run3d(Oracle3D(), pb, dca, dcb, df)
+    ref = _run3d(RefCPU3D(), pb, dca, dcb, df)
+    assert torch.equal(got[1], ref[1]), "background receivers"
+    for a, b in zip(got[2], ref[2]):
+        assert torch.equal(a, b), "background state"
+    tol = 1e-5 if dtype == torch.float32 else 1e-14
+    assert rel_l2(got[0], ref[0]) <= tol
+    for a, b in zip(got[3], ref[3]):
+        assert rel_l2(a, b) <= tol
+    assert float(got[0].abs().max()) > 0
+
+
+def test_born3d_oracle_matches_central_difference():
+    from oracle_harness import Oracle3D
+
+    pb = _case3d(torch.float64)
+    dca, dcb, df = _perturbation3d(pb, 9)
+    r_born, bg, _, _ = _run3d(Oracle3D(), pb, dca, dcb, df)
+    o = Oracle3D()
+
+    def receivers(h):
+        F, M = Oracle3D.full_state(pb)
+        r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+        o.forward(pb, pb.ca + h * dca, pb.cb + h * dcb, pb.f + h * df, r, F, M)
+        return r
+
+    h = 1e-4
+    fd = (receivers(h) - receivers(-h)) / (2 * h)
+    assert rel_l2(r_born, fd) < 1e-6
+    assert torch.equal(bg, receivers(0.0))

@@ -199,3 +199,106 @@ def test_unbuilt_linearization_parts_raise(cuda_device):
         lin.second_vjp(v, torch.zeros_like(lin.primal.receiver_data))
     with pytest.raises(NotImplementedError):
         lin.jvp(tide.EMDirection(mu=torch.ones_like(model.mu)))
+
+
+# ---------------------------------------------------------------------- 3-D
+def _born3d_cuda(pb, dca, dcb, df, dev):
+    import copy
+
+    from tide_b200 import em3d
+
+    q = copy.copy(pb)
+    mv = lambda t: t.detach().to(dev).clone()  # noqa: E731
+    q.ca, q.cb, q.cq, q.f = mv(pb.ca), mv(pb.cb), mv(pb.cq), mv(pb.f)
+    q.profiles = {k: mv(v) for k, v in pb.profiles.items()}
+    q.sources_i, q.receivers_i = mv(pb.sources_i), mv(pb.receivers_i)
+    q.fields = [mv(t) for t in pb.fields]
+    q.memories = [mv(t) for t in pb.memories]
+    q.device = torch.device(dev)
+    dfields = [torch.zeros_like(t) for t in q.fields]
+    dmem = [torch.zeros_like(t) for t in q.memories]
+    r = torch.zeros((q.nt, q.n_shots, q.n_rec), device=dev, dtype=q.dtype)
+    bg = torch.zeros_like(r)
+    d = [x.to(dev) for x in (dca, dcb, df)]
+    fn = nat.get_backend_function("maxwell_3d", "born_forward", 2, q.dtype, dev)
+    p = nat.ptr
+    fn(p(q.ca), p(q.cb), p(q.cq), p(d[0]), p(d[1]), p(q.f), p(d[2]),
+       *[p(t) for t in q.fields], *[p(t) for t in q.memories], *[p(t) for t in dfields],
+       *[p(t) for t in dmem], p(r), p(bg), *em3d._profile_ptrs(q), p(q.sources_i),
+       p(q.receivers_i), q.rdz, q.rdy, q.rdx, q.dt, q.nt, q.n_shots, q.nz, q.ny, q.nx, q.n_src,
+       q.n_rec, 1, q.batched, q.batched, q.batched, 0, *q.pml, q.src_comp, q.rec_comp, 0,
+       dev.index or 0, 0, torch.cuda.current_stream(dev).cuda_stream)
+    nat.check("born_forward 3-D")
+    torch.cuda.synchronize()
+    full = lambda mems: [q.layout.unpack(m.cpu(), a) for m, a in zip(mems, em3d.MEM_AXES)]  # noqa: E731
+    return r, bg, q.fields + full(q.memories), dfields + full(dmem)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("comps", [("ey", "ey"), ("ex", "ez")])
+def test_born3d_forward_bitwise_vs_oracle(cuda_device, dtype, comps):
+    from oracle_harness import Oracle3D
+    from test_born_oracle import _case3d, _perturbation3d
+
+    pb = _case3d(dtype, comps)
+    dca, dcb, df = _perturbation3d(pb, 7)
+    got = _born3d_cuda(pb, dca, dcb, df, cuda_device)
+    F, M = Oracle3D.full_state(pb)
+    DF, DM = [torch.zeros_like(t) for t in F], [torch.zeros_like(t) for t in M]
+    r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+    bg = torch.zeros_like(r)
+    Oracle3D().born_forward(pb, dca, dcb, pb.f, df, F, M, DF, DM, r, bg)
+    _same(got[0], r, "scattered receivers")
+    _same(got[1], bg, "background receivers")
+    for i, (a, b) in enumerate(zip(got[2] + got[3], F + M + DF + DM)):
+        _same(a, b, f"state tensor {i}")
+    assert nat.device_status(cuda_device) == 0
+
+
+def _operator3d(dev, dtype=torch.float64, seed=5):
+    g = torch.Generator().manual_seed(seed)
+    nz, ny, nx, S, nt = 10, 12, 11, 2, 50
+    eps = (1.5 + 5.0 * torch.rand((nz, ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    sig = (0.004 * torch.rand((nz, ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    mu = torch.ones((nz, ny, nx), device=dev, dtype=dtype)
+    dx = 0.02
+    dt = 0.9 * dx / (tide.C0 / float(eps.min().sqrt()) * 3 ** 0.5)
+    amp = tide.ricker(600e6, nt, dt, dtype=dtype).view(1, 1, nt).repeat(S, 1, 1).to(dev)
+    src = torch.tensor([[[4, 5, 5]], [[6, 7, 4]]], device=dev)
+    rec = torch.tensor([[[1, 2 + j, 3] for j in range(6)]] * S, device=dev)
+    op = tide.Maxwell3D(tide.Discretization(dx, dt, boundary=tide.CPML(3)),
+                        tide.Experiment(tide.Acquisition(src, rec), amp, source_component="ez",
+                                        receiver_component="ez"))
+    mask = torch.zeros((nz, ny, nx), dtype=torch.float64)
+    mask[2:-2, 2:-2, 2:-2] = 1.0
+    d_eps = 0.3 * mask * torch.randn((nz, ny, nx), generator=g, dtype=torch.float64)
+    d_sig = 1e-3 * mask * torch.randn((nz, ny, nx), generator=g, dtype=torch.float64)
+    return (op, tide.EMModel(eps, sig, mu),
+            tide.EMDirection(d_eps.to(dtype).to(dev), d_sig.to(dtype).to(dev)))
+
+
+def test_maxwell3d_jvp_adjoint_dot_product(cuda_device):
+    op, model, v = _operator3d(cuda_device)
+    lin = op.linearize(model)
+    jv = lin.jvp(v)
+    assert len(jv.final_state.tensors()) == 18
+    w = torch.randn(jv.receiver_data.shape, generator=torch.Generator().manual_seed(2),
+                    dtype=torch.float64).to(cuda_device)
+    g = lin.vjp(w)
+    lhs = float((jv.receiver_data * w).sum())
+    rhs = float((g.epsilon * v.epsilon).sum() + (g.sigma * v.sigma).sum())
+    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), abs(rhs))
+    assert abs(lhs) > 0
+
+
+def test_maxwell3d_jvp_matches_central_difference(cuda_device):
+    op, model, v = _operator3d(cuda_device)
+    jv = op.linearize(model).jvp(v).receiver_data
+    h = 1e-4
+
+    def data(s):
+        m = tide.EMModel(model.epsilon + s * v.epsilon, model.sigma + s * v.sigma, model.mu)
+        return op(m).receiver_data
+
+    fd = (data(h) - data(-h)) / (2 * h)
+    assert rel_l2(jv, fd) < 1e-6

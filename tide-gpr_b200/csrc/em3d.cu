@@ -371,6 +371,108 @@ k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restr
   }
 }
 
+// Born E half-step (maxwell_3d_inst.cpp:1390-1475): background and scattered
+// curls with their own CPML memories, then the scattered update
+// ca dE + cb dcurl + dca E^n + dcb curl H^n and the background update.  The
+// same z-marching columns as k3_fwd_e; H at z - 1 of both states is carried
+// in registers.
+template <typename T>
+struct BornMem {
+  T *hz_y, *hy_z, *hx_z, *hz_x, *hy_x, *hx_y;  // E-phase memories of one state
+};
+template <typename T>
+__global__ void __launch_bounds__(256)
+k3_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
+          const T *__restrict__ dca, const T *__restrict__ dcb, T *__restrict__ ex,
+          T *__restrict__ ey, T *__restrict__ ez, const T *__restrict__ hx,
+          const T *__restrict__ hy, const T *__restrict__ hz, T *__restrict__ dex,
+          T *__restrict__ dey, T *__restrict__ dez, const T *__restrict__ dhx,
+          const T *__restrict__ dhy, const T *__restrict__ dhz, BornMem<T> mb, BornMem<T> ms) {
+  Col c;
+  if (!column(g, c)) return;
+  const int ny = g.ny, nx = g.nx, y = c.y, x = c.x;
+  const int64_t sz = (int64_t)ny * nx, sy = nx;
+  const int64_t base = (int64_t)c.s * g.N;
+  ex += base; ey += base; ez += base; hx += base; hy += base; hz += base;
+  dex += base; dey += base; dez += base; dhx += base; dhy += base; dhz += base;
+  if (g.ca_b) { ca += base; dca += base; }
+  if (g.cb_b) { cb += base; dcb += base; }
+  const int64_t k0 = c.s * msz0(g), k1 = c.s * msz1(g), k2 = c.s * msz2(g);
+  BornMem<T> m[2] = {mb, ms};
+  for (int w = 0; w < 2; ++w) {
+    m[w].hy_z += k0; m[w].hx_z += k0;
+    m[w].hz_y += k1; m[w].hx_y += k1;
+    m[w].hz_x += k2; m[w].hy_x += k2;
+  }
+  const bool py = y < g.y0 || y >= g.y1, px = x < g.x0 || x >= g.x1;
+  const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  const T *H[2][3] = {{hx, hy, hz}, {dhx, dhy, dhz}};
+  int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
+  T p_x[2], p_y[2];  // Hx, Hy at z - 1 of both states
+  for (int w = 0; w < 2; ++w) {
+    p_x[w] = ld(H[w][0] + j - sz);
+    p_y[w] = ld(H[w][1] + j - sz);
+  }
+  for (int z = c.zb; z < c.ze; ++z, j += sz) {
+    const T a = ld(ca + j), b = ld(cb + j), da = ld(dca + j), db = ld(dcb + j);
+    const bool pz = z < g.z0 || z >= g.z1;
+    Prof<T> fz{(T)0, (T)0, (T)1};
+    if (pz) fz = prof_at(g, PAZ, PKZ, z, true);
+    const int64_t m0 = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+    T cu[2][3];
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+      const T h_x = ld(H[w][0] + j), h_y = ld(H[w][1] + j), h_z = ld(H[w][2] + j);
+      T dHy_dz = (h_y - p_y[w]) * g.rdz;
+      T dHz_dy = (h_z - ld(H[w][2] + j - sy)) * g.rdy;
+      T dHz_dx = (h_z - ld(H[w][2] + j - 1)) * g.rdx;
+      T dHx_dz = (h_x - p_x[w]) * g.rdz;
+      T dHx_dy = (h_x - ld(H[w][0] + j - sy)) * g.rdy;
+      T dHy_dx = (h_y - ld(H[w][1] + j - 1)) * g.rdx;
+      if (pz) {
+        const T m1 = fz.b * m[w].hy_z[m0] + fz.a * dHy_dz;
+        m[w].hy_z[m0] = m1;
+        dHy_dz = div_k(dHy_dz, fz.k) + m1;
+        const T m2 = fz.b * m[w].hx_z[m0] + fz.a * dHx_dz;
+        m[w].hx_z[m0] = m2;
+        dHx_dz = div_k(dHx_dz, fz.k) + m2;
+      }
+      if (py) {
+        const int64_t mm = z * s1 + o1;
+        const T m1 = fy.b * m[w].hz_y[mm] + fy.a * dHz_dy;
+        m[w].hz_y[mm] = m1;
+        dHz_dy = div_k(dHz_dy, fy.k) + m1;
+        const T m2 = fy.b * m[w].hx_y[mm] + fy.a * dHx_dy;
+        m[w].hx_y[mm] = m2;
+        dHx_dy = div_k(dHx_dy, fy.k) + m2;
+      }
+      if (px) {
+        const int64_t mm = z * s2 + o2;
+        const T m1 = fx.b * m[w].hz_x[mm] + fx.a * dHz_dx;
+        m[w].hz_x[mm] = m1;
+        dHz_dx = div_k(dHz_dx, fx.k) + m1;
+        const T m2 = fx.b * m[w].hy_x[mm] + fx.a * dHy_dx;
+        m[w].hy_x[mm] = m2;
+        dHy_dx = div_k(dHy_dx, fx.k) + m2;
+      }
+      cu[w][0] = dHy_dz - dHz_dy;
+      cu[w][1] = dHz_dx - dHx_dz;
+      cu[w][2] = dHx_dy - dHy_dx;
+      p_x[w] = h_x;
+      p_y[w] = h_y;
+    }
+    T *E[3] = {ex, ey, ez}, *D[3] = {dex, dey, dez};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T e_old = E[k][j];
+      D[k][j] = a * D[k][j] + b * cu[1][k] + da * e_old + db * cu[0][k];
+      E[k][j] = a * e_old + b * cu[0][k];
+    }
+  }
+}
+
 // Sources then receivers of one step: one thread per (shot, point).
 template <typename T>
 __global__ void k3_points(T *__restrict__ field_src, const T *__restrict__ f_t,
@@ -1210,6 +1312,78 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   if ((need_ca || need_cb) && storage_mode == 1) TB_CUDA(cudaStreamSynchronize(st));
 }
 
+template <typename T>
+void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
+  (void)dt; (void)step_ratio; (void)n_threads;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0, "3-D born_forward: nt must be >= 0");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && ex && ey && ez && hx && hy && hz && dex && dey &&
+                 dez && dhx && dhy && dhz,
+             "3-D born_forward: a field or coefficient pointer is null");
+  T *M[12] = {m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y,
+              m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x};
+  T *DM[12] = {dm_hz_y, dm_hy_z, dm_hx_z, dm_hz_x, dm_hy_x, dm_hx_y,
+               dm_ey_z, dm_ez_y, dm_ez_x, dm_ex_z, dm_ex_y, dm_ey_x};
+  for (int k = 0; k < 12; ++k)
+    TB_REQUIRE(M[k] && DM[k], "3-D born_forward: a CPML memory pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || (f0 && df),
+             "3-D born_forward: sources without background or scattered amplitudes");
+  if (!common_checks("3-D born_forward", 0, (const T *)nullptr, n_receivers_per_shot, r,
+                     source_component, receiver_component, execution_backend))
+    return;
+  const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
+                           kz, kzh, ky, kyh, kx, kxh};
+  Launch3<T> L;
+  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = stream_of(compute_stream);
+  T *F[6] = {ex, ey, ez, hx, hy, hz}, *DF[6] = {dex, dey, dez, dhx, dhy, dhz};
+  const BornMem<T> mb{M[0], M[1], M[2], M[3], M[4], M[5]};
+  const BornMem<T> ms{DM[0], DM[1], DM[2], DM[3], DM[4], DM[5]};
+  const int S_ = (int)n_shots;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  int64_t launches = 0;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    T *const *fs2[2] = {F, DF};
+    T *const *ms2[2] = {M, DM};
+    for (int w = 0; w < 2; ++w) {
+      T *const *Fw = fs2[w], *const *Mw = ms2[w];
+      k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, Fw[0], Fw[1], Fw[2], Fw[3], Fw[4], Fw[5],
+                                              Mw[6], Mw[7], Mw[8], Mw[9], Mw[10], Mw[11]);
+    }
+    k3_born_e<T><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy, hz, dex,
+                                             dey, dez, dhx, dhy, dhz, mb, ms);
+    launches += 3;
+    if (n_sources_per_shot > 0 && sources_i) {
+      k3_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
+          field_of(ex, ey, ez, source_component), f0 + t * fs, sources_i,
+          (int)n_sources_per_shot, nullptr, nullptr, nullptr, 0, S_, L.g.N, 0);
+      k3_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
+          field_of(dex, dey, dez, source_component), df + t * fs, sources_i,
+          (int)n_sources_per_shot, nullptr, nullptr, nullptr, 0, S_, L.g.N, 0);
+      launches += 2;
+    }
+    if (n_receivers_per_shot > 0 && receivers_i) {
+      const int tot = S_ * (int)n_receivers_per_shot;
+      if (r) {
+        k3_points<T><<<(tot + 127) / 128, 128, 0, st>>>(
+            nullptr, nullptr, nullptr, 0, field_of(dex, dey, dez, receiver_component),
+            r + t * rs, receivers_i, (int)n_receivers_per_shot, S_, L.g.N, 1);
+        ++launches;
+      }
+      if (background_r) {
+        k3_points<T><<<(tot + 127) / 128, 128, 0, st>>>(
+            nullptr, nullptr, nullptr, 0, field_of(ex, ey, ez, receiver_component),
+            background_r + t * rs, receivers_i, (int)n_receivers_per_shot, S_, L.g.N, 1);
+        ++launches;
+      }
+    }
+  }
+  count_launches(launches);
+  TB_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 }  // namespace tb
 
@@ -1259,3 +1433,20 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
 
 TB3_DEFINE(2, float)
 TB3_DEFINE(2, double)
+
+#define TB3_BORN_DEFINE(S, T)                                                              \
+  extern "C" void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T)) { \
+    tb::em3d_born_forward<T>(                                                              \
+        ca, cb, cq, dca, dcb, f0, df, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z,      \
+        m_hz_x, m_hy_x, m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, dex, dey,  \
+        dez, dhx, dhy, dhz, dm_hz_y, dm_hy_z, dm_hx_z, dm_hz_x, dm_hy_x, dm_hx_y, dm_ey_z, \
+        dm_ez_y, dm_ez_x, dm_ex_z, dm_ex_y, dm_ey_x, r, background_r, az, bz, azh, bzh,   \
+        ay, by, ayh, byh, ax, bx, axh, bxh, kz, kzh, ky, kyh, kx, kxh, sources_i,          \
+        receivers_i, rdz, rdy, rdx, dt, nt, n_shots, nz, ny, nx, n_sources_per_shot,       \
+        n_receivers_per_shot, step_ratio, ca_batched, cb_batched, cq_batched, start_t,     \
+        pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1, source_component,                 \
+        receiver_component, n_threads, device, execution_backend, compute_stream);        \
+  }
+
+TB3_BORN_DEFINE(2, float)
+TB3_BORN_DEFINE(2, double)

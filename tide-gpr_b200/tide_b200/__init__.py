@@ -41,7 +41,7 @@ from .physics import (
 )
 from .storage import StorageMode, StorageOptions
 from .born import borntm
-from .em3d import maxwell3d
+from .em3d import born3d, maxwell3d
 from .tm2d import CallbackState, maxwelltm, prepare_tm2d, propagate
 
 __all__ = [
@@ -49,6 +49,6 @@ __all__ = [
     "Discretization", "EM3DState", "EMDirection", "EMGradient", "EMModel", "EP0", "ExecutionOptions",
     "Experiment", "FallbackPolicy", "ForwardResult", "LinearizedMaxwell3D",
     "LinearizedMaxwellTM", "MU0", "Maxwell3D", "MaxwellTM", "Observers", "TangentResult",
-    "StorageMode", "StorageOptions", "TMState", "borntm", "cfl_condition", "downsample", "maxwell3d", "maxwelltm",
+    "StorageMode", "StorageOptions", "TMState", "born3d", "borntm", "cfl_condition", "downsample", "maxwell3d", "maxwelltm",
     "prepare_parameters", "prepare_tm2d", "propagate", "ricker", "upsample",
 ]

@@ -74,6 +74,11 @@ SPECS.update({
         (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), *_3D_PROFILES, *_3D_TAIL,
         *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:556-577
+    "maxwell_3d_born_forward": [
+        (_P, 3), (_P, 2), (_P, 2), *_3D_FIELDS, (_P, 6), (_P, 12), (_P, 2), *_3D_PROFILES,
+        *_3D_TAIL, *_3D_FLAGS, (_P, 1),
+    ],
     # src/tide/backend_utils.py:537-556
     "maxwell_3d_backward": [
         (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 4), (_P, 2), (_B, 1),
@@ -185,6 +190,10 @@ def exported_symbols() -> list[str]:
     ] + [
         symbol_name("maxwell_tm", "born_forward", a, d)
         for a in ACCURACIES
+        for d in ("float", "double")
+    ] + [
+        symbol_name("maxwell_3d", "born_forward", a, d)
+        for a in ACCURACIES_3D
         for d in ("float", "double")
     ] + [
         symbol_name("maxwell_3d", p, a, d)

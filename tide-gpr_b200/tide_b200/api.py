@@ -447,4 +447,22 @@ class LinearizedMaxwell3D(LinearizedMaxwellTM):
         self._result = op(self.model, retain_history=True)
 
     def jvp(self, direction: EMDirection) -> TangentResult:
-        raise NotImplementedError("3-D Born (jvp) propagation is not built in tide_b200.")
+        """Born scattered receiver data and final scattered state for a model
+        direction (linearization.py:232-300); a mu part raises."""
+        direction.validate_for(self.model)
+        if direction.mu is not None:
+            raise NotImplementedError("3-D tangent propagation for mu is not available.")
+        op = self.operator
+        d, e = op.discretization, op.experiment
+        res = em3d.born3d(
+            self.model.epsilon, self.model.sigma, self.model.mu, grid_spacing=d.spacing,
+            dt=d.dt, source_amplitude=e.source_amplitude,
+            source_location=e.acquisition.source_location,
+            receiver_location=e.acquisition.receiver_location,
+            bg_receiver_location=e.acquisition.receiver_location,
+            depsilon=direction.epsilon, dsigma=direction.sigma, stencil=d.stencil,
+            pml_width=d.boundary.width, max_vel=d.max_velocity, nt=e.nt,
+            model_gradient_sampling_interval=op.model_gradient_sampling_interval,
+            source_component=e.source_component, receiver_component=e.receiver_component,
+        )
+        return TangentResult(res[-1], EM3DState.from_tensors(res[18:36]))

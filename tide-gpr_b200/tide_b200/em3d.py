@@ -127,6 +127,31 @@ def _spacing(h: float | Sequence[float]) -> list[float]:
     return v
 
 
+def initial_state_3d(initial_state, layout: CompactLayout, fd, device, dtype):
+    """Padded fields and compact CPML memories from an 18-tensor state (None
+    entries start at zero): zero fd padding as create_or_pad(...,
+    mode="constant"), memories packed to their strips."""
+    S = layout.shots
+    shape = (S, *layout.shape)
+    init = list(initial_state) if initial_state is not None else [None] * 18
+    if len(init) != 18:
+        raise ValueError("initial_state holds 6 fields and 12 CPML memories")
+
+    def padded(t):
+        if t.ndim == 3:
+            t = t[None].expand(S, -1, -1, -1)
+        t = t.to(device=device, dtype=dtype)
+        if tuple(t.shape) == shape:
+            return t.clone().contiguous()
+        return torch.nn.functional.pad(t, ph._torch_pad_order(fd)).contiguous()
+
+    fields = [padded(t) if t is not None and t.numel() else torch.zeros(shape, device=device, dtype=dtype)
+              for t in init[:6]]
+    memories = [layout.pack(padded(t), a) if t is not None and t.numel() else layout.zeros(a, device, dtype)
+                for t, a in zip(init[6:], MEM_AXES)]
+    return fields, memories
+
+
 def prepare_em3d(
     epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
     grid_spacing: float | Sequence[float], dt: float,
@@ -191,23 +216,7 @@ def prepare_em3d(
         f = torch.empty(0, device=device, dtype=dtype)
     prof = ph.set_pml_profiles_3d(widths, fd, dt, [dz, dy, dx], dtype, device, nz, ny, nx)
     layout = CompactLayout(S, (nz, ny, nx), ((pml[0], pml[3]), (pml[1], pml[4]), (pml[2], pml[5])))
-    shape = (S, nz, ny, nx)
-    init = list(initial_state) if initial_state is not None else [None] * 18
-    if len(init) != 18:
-        raise ValueError("initial_state holds 6 fields and 12 CPML memories")
-
-    def padded(t):  # zero fd padding, as create_or_pad(..., mode="constant")
-        if t.ndim == 3:
-            t = t[None].expand(S, -1, -1, -1)
-        t = t.to(device=device, dtype=dtype)
-        if tuple(t.shape) == shape:
-            return t.clone().contiguous()
-        return torch.nn.functional.pad(t, ph._torch_pad_order(fd)).contiguous()
-
-    fields = [padded(t) if t is not None and t.numel() else torch.zeros(shape, device=device, dtype=dtype)
-              for t in init[:6]]
-    memories = [layout.pack(padded(t), a) if t is not None and t.numel() else layout.zeros(a, device, dtype)
-                for t, a in zip(init[6:], MEM_AXES)]
+    fields, memories = initial_state_3d(initial_state, layout, fd, device, dtype)
     shp = (S, nz, ny, nx) if batched else (1, nz, ny, nx)
     return EM3DProblem(
         ca=ca.reshape(shp), cb=cb.reshape(shp), cq=cq.reshape(shp), f=f, profiles=prof,
@@ -523,3 +532,115 @@ def maxwell3d(
     if ratio > 1 and r.numel() > 0:
         r = ph.downsample(r.movedim(0, -1), ratio).movedim(-1, 0)
     return (*outs, r)
+
+
+@torch.no_grad()
+def born3d(
+    epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
+    grid_spacing: float | Sequence[float], dt: float,
+    source_amplitude: torch.Tensor | None, source_location: torch.Tensor | None,
+    receiver_location: torch.Tensor | None, bg_receiver_location: torch.Tensor | None = None,
+    *, depsilon: torch.Tensor | None = None, dsigma: torch.Tensor | None = None,
+    dca: torch.Tensor | None = None, dcb: torch.Tensor | None = None, stencil: int = 2,
+    pml_width: int | Sequence[int] = 20, max_vel: float | None = None, nt: int | None = None,
+    model_gradient_sampling_interval: int = 1, parameterization: str = "epsilon_sigma",
+    linearize_source: bool = True, source_component: str = "ey",
+    receiver_component: str = "ey", **state_and_unused,
+):
+    """3-D Born propagator (src/tide/maxwell/maxwell3d_born.py:27): the
+    background and the scattered (J(m) v) states advance together in
+    maxwell_3d_2_{dtype}_born_forward_cuda.  The perturbation is zero-padded;
+    (dca, dcb) from the closed-form coefficient derivative; with
+    linearize_source the scattered source is the source pre-scale taken with
+    dcb.  Initial states: Ex_0 .. m_ey_x_0 (background) and dEx_0 ..
+    dm_ey_x_0 (scattered).  Returns the background final state (18 tensors),
+    the scattered final state (18), the background receivers (recorded when
+    bg_receiver_location equals receiver_location, else empty) and the
+    scattered receivers.  Not differentiable in this build."""
+    from .born import linearize_material_coefficients
+
+    if epsilon.ndim != 3:
+        raise NotImplementedError("born3d supports a single 3-D model only.")
+    if parameterization not in ("epsilon_sigma", "ca_cb"):
+        raise ValueError("parameterization must be 'epsilon_sigma' or 'ca_cb'")
+    if epsilon.device.type != "cuda":
+        raise nat.NativeError("libtide_b200 runs on CUDA devices only; there is no CPU path.")
+    names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") + MEM_NAMES
+    bg_init = [state_and_unused.get(f"{n}_0") for n in names]
+    sc_init = [state_and_unused.get(f"d{n}_0") for n in names]
+    epsilon, sigma, mu = epsilon.detach(), sigma.detach(), mu.detach()
+    if max_vel is None:
+        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
+    spacing = _spacing(grid_spacing)
+    inner_dt, ratio = ph.cfl_condition(spacing, dt, max_vel)
+    amp = source_amplitude
+    if ratio > 1 and amp is not None and amp.numel() > 0:
+        amp = ph.upsample(amp, ratio)
+    nt_int = nt * ratio if nt is not None else None
+    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, inner_dt, amp, source_location,
+                      receiver_location, stencil=stencil, pml_width=pml_width,
+                      source_component=source_component, receiver_component=receiver_component,
+                      model_gradient_sampling_interval=model_gradient_sampling_interval,
+                      nt=nt_int, initial_state=bg_init)
+    dev, dtype = pb.device, pb.dtype
+    pad = [a + b for a, b in zip(pb.fd_pad, pb.pml_width)]
+    shape = (pb.nz, pb.ny, pb.nx)
+
+    def zpad(t):
+        if t is None or t.numel() == 0:
+            return torch.zeros(shape, device=dev, dtype=dtype)
+        return torch.nn.functional.pad(t.to(device=dev, dtype=dtype),
+                                       ph._torch_pad_order(pad)).contiguous()
+
+    if parameterization == "epsilon_sigma":
+        dca_p, dcb_p = linearize_material_coefficients(pb.ca[0], pb.cb[0], pb.dt, zpad(depsilon),
+                                                       zpad(dsigma))
+    else:
+        dca_p, dcb_p = zpad(dca), zpad(dcb)
+    dca_p = dca_p.reshape(1, *shape).contiguous()
+    dcb_p = dcb_p.reshape(1, *shape).contiguous()
+    S, N = pb.n_shots, pb.nz * pb.ny * pb.nx
+    n_src = pb.n_src if pb.f.numel() else 0
+    if n_src > 0:
+        if linearize_source:
+            dz, dy, dx = spacing
+            dcb_at = dcb_p.reshape(1, N).expand(S, -1).gather(1, pb.sources_i)
+            df = (amp.to(dev).permute(2, 0, 1) * dcb_at[None] * (-1.0 / (dx * dy * dz)))
+            df = df.reshape(-1).contiguous()
+        else:
+            df = torch.zeros_like(pb.f)
+    else:
+        df = torch.empty(0, device=dev, dtype=dtype)
+    sc_fields, sc_mem = initial_state_3d(sc_init, pb.layout, pb.fd_pad, dev, dtype)
+    same_rec = bg_receiver_location is not None and receiver_location is not None and (
+        bg_receiver_location.shape == receiver_location.shape
+        and bool(torch.equal(bg_receiver_location.to(dev), receiver_location.to(dev))))
+    r = torch.zeros((pb.nt, S, pb.n_rec), device=dev, dtype=dtype)
+    bg_r = torch.zeros_like(r) if same_rec else torch.empty(0, device=dev, dtype=dtype)
+    fn = nat.get_backend_function("maxwell_3d", "born_forward", 2, dtype, dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca_p), _p(dcb_p), _p(pb.f), _p(df),
+       *[_p(t) for t in pb.fields], *[_p(t) for t in pb.memories],
+       *[_p(t) for t in sc_fields], *[_p(t) for t in sc_mem], _p(r), _p(bg_r),
+       *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
+       pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, n_src, pb.n_rec, 1,
+       pb.batched, pb.batched, pb.batched, 0, *pb.pml, pb.src_comp, pb.rec_comp, 0,
+       dev.index or 0, 0, stream)
+    nat.check("maxwell_3d born_forward")
+    if not same_rec and bg_receiver_location is not None and bg_receiver_location.numel() > 0:
+        bg_r = maxwell3d(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
+                         bg_receiver_location, stencil=stencil, pml_width=pml_width,
+                         max_vel=max_vel, nt=nt, source_component=source_component,
+                         receiver_component=receiver_component, storage_mode="none",
+                         **{f"{n}_0" if n[0] in "EH" else n: t
+                            for n, t in zip(names, bg_init)})[-1]
+    elif same_rec and ratio > 1:
+        bg_r = ph.downsample(bg_r.movedim(0, -1), ratio).movedim(-1, 0)
+    if ratio > 1 and r.numel() > 0:
+        r = ph.downsample(r.movedim(0, -1), ratio).movedim(-1, 0)
+    s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
+
+    def outs(fields, mems):
+        return [t[s] for t in fields] + [pb.layout.unpack(m, a)[s] for m, a in zip(mems, MEM_AXES)]
+
+    return (*outs(pb.fields, pb.memories), *outs(sc_fields, sc_mem), bg_r, r)
