@@ -54,7 +54,11 @@ extern "C" {
  * (argtypes src/tide/backend_utils.py:271-287).  step_ratio is the gradient
  * sampling interval k: Ey^t and curl H^t are stored when t % k == 0.
  * storage_mode: 0 device, 1 cpu (pinned host history, 3-slot device ring),
- * 2 disk (rejected: not built), 3 none.  storage_format: 0 full, 1 bf16. */
+ * 2 disk (3-slot device ring, 3-slot pinned staging ring passed as
+ * *_store_3, the history in the file named by *_filenames[0]: stored step q
+ * at byte offset q * n_shots * shot_bytes_uncomp, written by a background
+ * thread; the call returns after its writes are on disk), 3 none.
+ * storage_format: 0 full, 1 bf16. */
 #define TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)                                   \
   T const *ca, T const *cb, T const *cq, T const *f, T *ey, T *hx, T *hz,      \
       T *m_ey_x, T *m_ey_z, T *m_hx_z, T *m_hz_x, T *r, void *ey_store_1,      \

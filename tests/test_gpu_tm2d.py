@@ -276,8 +276,14 @@ def test_bad_arguments_raise_not_exit(cuda_device):
     pb = random_problem(92, 20, 24, 1, 5)
     g = clone_problem(pb, cuda_device)
     fn = nat.get_backend_function("maxwell_tm", "forward_with_storage", 2, torch.float32, cuda_device)
-    with pytest.raises(nat.NativeError, match="disk"):
-        snaps = stg.SnapshotBuffers(2, 0, torch.float32, 5, g.ny * g.nx * 4, *(torch.empty(0),) * 4)
+    with pytest.raises(nat.NativeError, match="storage_mode"):
+        snaps = stg.SnapshotBuffers(7, 0, torch.float32, 5, g.ny * g.nx * 4, *(torch.empty(0),) * 4)
+        tm2d._run_forward_storage(g, g.ca, g.cb, g.f, _zeros_r(g, cuda_device), snaps, True, True,
+                                  None, 0)
+    with pytest.raises(nat.NativeError, match="file names"):
+        snaps = stg.allocate(stg.STORAGE_DISK, torch.float32, 0, 5, g.n_shots, g.ny, g.nx,
+                             cuda_device, True, True)
+        snaps.files = None  # no file names
         tm2d._run_forward_storage(g, g.ca, g.cb, g.f, _zeros_r(g, cuda_device), snaps, True, True,
                                   None, 0)
     del fn

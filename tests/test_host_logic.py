@@ -42,9 +42,9 @@ def test_storage_modes():
     assert stg.mode_code("cpu") == stg.STORAGE_CPU
     with pytest.raises(ValueError):
         stg.mode_code("tape")
-    with pytest.raises(NotImplementedError):
-        stg.resolve_mode("disk", device=torch.device("cpu"), n_store=1, n_shots=1, ny=4, nx=4,
-                         itemsize=4, n_arrays=2, bytes_limit_device=None, bytes_limit_host=None)
+    assert stg.resolve_mode("disk", device=torch.device("cpu"), n_store=1, n_shots=1, ny=4,
+                            nx=4, itemsize=4, n_arrays=2, bytes_limit_device=None,
+                            bytes_limit_host=None) == stg.STORAGE_DISK
     # auto: device when the history fits the device budget, else pinned host
     kw = dict(device=torch.device("cpu"), n_store=10, n_shots=2, ny=8, nx=8, itemsize=4, n_arrays=2)
     total = stg.history_bytes(10, 2, 8, 8, 4, 2)

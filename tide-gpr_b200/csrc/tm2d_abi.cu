@@ -5,10 +5,12 @@
 //
 // Every call works on the caller's stream (compute_stream; 0 = legacy
 // default) and returns as soon as its work is enqueued, except that the cpu
-// storage mode synchronises its side stream before returning, as the
-// reference does (maxwell_tm_cuda_inst.cu:1601-1604).
+// and disk storage modes synchronise their copies before returning, as the
+// reference does (maxwell_tm_cuda_inst.cu:1601-1604); the disk mode also
+// waits for its file writes.
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <type_traits>
 #include <utility>
@@ -19,6 +21,7 @@
 #include "tm2d_kernels.cuh"
 #include "tm2d_fused.cuh"
 #include "tm2d_s2.cuh"
+#include "tb_disk.cuh"
 
 namespace tb {
 namespace {
@@ -440,8 +443,6 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
              "TM2D forward_with_storage: a field or coefficient pointer is null");
   TB_REQUIRE(n_sources_per_shot == 0 || f, "TM2D forward_with_storage: sources without amplitudes");
   TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D forward_with_storage: receivers without output");
-  TB_REQUIRE(storage_mode != 2,
-             "TM2D forward_with_storage: disk storage mode is not built in this library");
   TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "TM2D: unknown storage_mode %lld",
              (long long)storage_mode);
   const bool bf16 = storage_format == 1;
@@ -454,9 +455,13 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
                (long long)shot_bytes_uncomp, (long long)(ny * nx * (int64_t)esz));
     TB_REQUIRE((!ca_requires_grad || ey_store_1) && (!cb_requires_grad || curl_store_1),
                "TM2D: snapshot buffers missing");
-    TB_REQUIRE(storage_mode != 1 ||
+    TB_REQUIRE((storage_mode != 1 && storage_mode != 2) ||
                    ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
-               "TM2D: cpu storage mode needs host snapshot buffers");
+               "TM2D: cpu / disk storage modes need host snapshot buffers");
+    TB_REQUIRE(storage_mode != 2 ||
+                   ((!ca_requires_grad || (ey_filenames && ey_filenames[0])) &&
+                    (!cb_requires_grad || (curl_filenames && curl_filenames[0]))),
+               "TM2D: disk storage mode needs snapshot file names");
   }
   Launch<T, ST> L;
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
@@ -464,7 +469,27 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     return;
   cudaStream_t st = as_stream(compute_stream);
   cudaStream_t ss = as_stream(storage_stream);
-  const bool pipeline = want_store && storage_mode == 1 && ss != nullptr && ss != st;
+  const bool host_side = want_store && (storage_mode == 1 || storage_mode == 2);
+  const bool pipeline = host_side && ss != nullptr && ss != st;
+  // disk mode: one writer per snapshot kind; host staging ring in *_store_3
+  std::unique_ptr<DiskHistory> disk[2];
+  EventRing staged;
+  if (want_store && storage_mode == 2) {
+    if (!staged.ok) {
+      set_error(kCudaError, "TM2D: event creation failed");
+      return;
+    }
+    const char *names[2] = {ca_requires_grad ? ey_filenames[0] : nullptr,
+                            cb_requires_grad ? curl_filenames[0] : nullptr};
+    for (int k = 0; k < 2; ++k)
+      if (names[k]) {
+        disk[k].reset(new DiskHistory(names[k], true, kRing));
+        if (!disk[k]->ok()) {
+          set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
+          return;
+        }
+      }
+  }
   // one launch per step (see fused_pays)
   const bool fused = is_float<T>() && ST == 2 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N);
   PitchedFwd pf;
@@ -530,20 +555,32 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
                                ps, ft, rt);
       if (smp) prof.end(kKFwdE);
     }
-    if (store_step && storage_mode == 1) {
+    if (store_step && host_side) {
       cudaStream_t cs = st;
       if (pipeline) {
         if (TB_CUDA(cudaEventRecord(compute_done.ev[slot], st))) return;
         if (TB_CUDA(cudaStreamWaitEvent(ss, compute_done.ev[slot], 0))) return;
         cs = ss;
       }
-      const size_t off3 = (size_t)q * step_bytes;
-      if (e1 && TB_CUDA(cudaMemcpyAsync((char *)ey_store_3 + off3, e1, step_bytes,
-                                        cudaMemcpyDeviceToHost, cs)))
-        return;
-      if (c1 && TB_CUDA(cudaMemcpyAsync((char *)curl_store_3 + off3, c1, step_bytes,
-                                        cudaMemcpyDeviceToHost, cs)))
-        return;
+      // cpu mode: straight into the host history; disk mode: into the staging
+      // slot, whose previous write must have finished, then queued for the file
+      const bool to_disk = storage_mode == 2;
+      const size_t off3 = to_disk ? (size_t)slot * step_bytes : (size_t)q * step_bytes;
+      char *h3[2] = {(char *)ey_store_3 + off3, (char *)curl_store_3 + off3};
+      const char *d1[2] = {e1, c1};
+      for (int k = 0; k < 2; ++k) {
+        if (!d1[k]) continue;
+        if (to_disk) disk[k]->wait_slot(slot);
+        if (TB_CUDA(cudaMemcpyAsync(h3[k], d1[k], step_bytes, cudaMemcpyDeviceToHost, cs)))
+          return;
+      }
+      if (to_disk) {
+        if (TB_CUDA(cudaEventRecord(staged.ev[slot], cs))) return;
+        for (int k = 0; k < 2; ++k)
+          if (d1[k])
+            disk[k]->enqueue_write(slot, h3[k], step_bytes, (int64_t)(q * step_bytes),
+                                   staged.ev[slot]);
+      }
       if (pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss))) return;
     }
   }
@@ -553,6 +590,11 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     if (fused && !pf.finish()) return;
   }
   if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
+  for (int k = 0; k < 2; ++k)
+    if (disk[k] && !disk[k]->finish()) {
+      set_error(kCudaError, "TM2D disk storage: %s", disk[k]->error().c_str());
+      return;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -575,7 +617,6 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
                  m_lambda_ey_z && m_lambda_hx_z && m_lambda_hz_x && adjoint_memory_scratch,
              "TM2D backward: a field or coefficient pointer is null");
   TB_REQUIRE(n_receivers_per_shot == 0 || grad_r, "TM2D backward: receivers without grad_r");
-  TB_REQUIRE(storage_mode != 2, "TM2D backward: disk storage mode is not built in this library");
   const bool bf16 = storage_format == 1;
   TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
   const bool grads = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
@@ -586,9 +627,13 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     TB_REQUIRE((!ca_requires_grad || (ey_store_1 && grad_ca)) &&
                    (!cb_requires_grad || (curl_store_1 && grad_cb)),
                "TM2D backward: gradient or snapshot buffers missing");
-    TB_REQUIRE(storage_mode != 1 ||
+    TB_REQUIRE((storage_mode != 1 && storage_mode != 2) ||
                    ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
-               "TM2D backward: cpu storage mode needs host snapshot buffers");
+               "TM2D backward: cpu / disk storage modes need host snapshot buffers");
+    TB_REQUIRE(storage_mode != 2 ||
+                   ((!ca_requires_grad || (ey_filenames && ey_filenames[0])) &&
+                    (!cb_requires_grad || (curl_filenames && curl_filenames[0]))),
+               "TM2D backward: disk storage mode needs snapshot file names");
   }
   Launch<T, ST> L;
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
@@ -597,8 +642,29 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
   cudaStream_t st = as_stream(compute_stream);
   cudaStream_t ss = as_stream(storage_stream);
-  const bool pipeline = grads && storage_mode == 1 && ss != nullptr && ss != st;
+  const bool host_side = grads && (storage_mode == 1 || storage_mode == 2);
+  const bool pipeline = host_side && ss != nullptr && ss != st;
   const size_t SN = (size_t)n_shots * (size_t)L.g.N;
+  // disk mode: readers per snapshot kind into the host staging ring (*_store_3)
+  std::unique_ptr<DiskHistory> disk[2];
+  EventRing staged;  // the staging slot's host-to-device copy has completed
+  if (grads && storage_mode == 2) {
+    if (!staged.ok) {
+      set_error(kCudaError, "TM2D: event creation failed");
+      return;
+    }
+    const char *names[2] = {ca_requires_grad ? ey_filenames[0] : nullptr,
+                            cb_requires_grad ? curl_filenames[0] : nullptr};
+    for (int k = 0; k < 2; ++k)
+      if (names[k]) {
+        disk[k].reset(new DiskHistory(names[k], false, kRing));
+        if (!disk[k]->ok()) {
+          set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
+          return;
+        }
+      }
+  }
+  bool staged_used[kRing] = {false, false, false};
   // Both ping-pong buffers of every CPML memory adjoint hold zeros outside
   // their strips for the whole call, so the kernels only write strip cells.
   if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, 4 * SN * sizeof(T), st))) return;
@@ -634,20 +700,32 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     const int slot = (int)(q % kRing);
     cudaStream_t ls = pipeline ? ss : st;
     if (pipeline && TB_CUDA(cudaStreamWaitEvent(ss, consumed.ev[slot], 0))) return false;
-    const size_t off1 = (size_t)slot * step_bytes, off3 = (size_t)q * step_bytes;
-    if (ca_requires_grad && TB_CUDA(cudaMemcpyAsync((char *)ey_store_1 + off1,
-                                                    (char *)ey_store_3 + off3, step_bytes,
-                                                    cudaMemcpyHostToDevice, ls)))
-      return false;
-    if (cb_requires_grad && TB_CUDA(cudaMemcpyAsync((char *)curl_store_1 + off1,
-                                                    (char *)curl_store_3 + off3, step_bytes,
-                                                    cudaMemcpyHostToDevice, ls)))
-      return false;
+    const bool from_disk = storage_mode == 2;
+    const size_t off1 = (size_t)slot * step_bytes;
+    const size_t off3 = from_disk ? (size_t)slot * step_bytes : (size_t)q * step_bytes;
+    if (from_disk && staged_used[slot] && TB_CUDA(cudaEventSynchronize(staged.ev[slot])))
+      return false;  // the staging slot's previous copy to the device has finished
+    void *d1[2] = {ca_requires_grad ? (char *)ey_store_1 + off1 : nullptr,
+                   cb_requires_grad ? (char *)curl_store_1 + off1 : nullptr};
+    char *h3[2] = {(char *)ey_store_3 + off3, (char *)curl_store_3 + off3};
+    for (int k = 0; k < 2; ++k) {
+      if (!d1[k]) continue;
+      if (from_disk && !disk[k]->read(h3[k], step_bytes, (int64_t)(q * step_bytes))) {
+        set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
+        return false;
+      }
+      if (TB_CUDA(cudaMemcpyAsync(d1[k], h3[k], step_bytes, cudaMemcpyHostToDevice, ls)))
+        return false;
+    }
+    if (from_disk) {
+      if (TB_CUDA(cudaEventRecord(staged.ev[slot], ls))) return false;
+      staged_used[slot] = true;
+    }
     if (pipeline && TB_CUDA(cudaEventRecord(loaded.ev[slot], ss))) return false;
     return true;
   };
   size_t next_q = 0;
-  if (storage_mode == 1 && grads)
+  if (host_side)
     for (size_t n = 0; n < std::min<size_t>(2, qs.size()); ++n)
       if (!load(n)) return;
 
@@ -695,7 +773,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (smp) prof.end(kKAdjH);
     std::swap(cur_ey_x, nxt_ey_x);
     std::swap(cur_ey_z, nxt_ey_z);
-    if (grad_step && storage_mode == 1) {
+    if (grad_step && host_side) {
       ++next_q;
       if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
       if (!load(next_q + 1)) return;
@@ -717,6 +795,9 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   count_launches(nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
   if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
+  // disk mode: the staging ring is the caller's and is refilled by the next
+  // call, so every copy out of it has finished before returning
+  else if (grads && storage_mode == 2) TB_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace

@@ -279,7 +279,8 @@ class MaxwellTM:
             model_gradient_sampling_interval=self.model_gradient_sampling_interval,
             forward_callback=observers.forward, backward_callback=observers.backward,
             callback_frequency=observers.frequency,
-            storage_mode=self.storage.mode.value, storage_compression=self.storage.compression,
+            storage_mode=self.storage.mode.value, storage_path=self.storage.path,
+            storage_compression=self.storage.compression,
             storage_bytes_limit_device=self.storage.bytes_limit_device,
             storage_bytes_limit_host=self.storage.bytes_limit_host,
             storage_chunk_steps=self.storage.chunk_steps,

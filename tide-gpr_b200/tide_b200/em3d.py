@@ -524,6 +524,9 @@ def maxwell3d(
             ny=pb.nz * pb.ny, nx=pb.nx, itemsize=torch.tensor([], dtype=sdtype).element_size(),
             n_arrays=6, bytes_limit_device=storage_bytes_limit_device,
             bytes_limit_host=storage_bytes_limit_host)
+        if mode == stg.STORAGE_DISK:
+            raise NotImplementedError("storage_mode='disk' is built for the 2-D TM path only; "
+                                      "use 'checkpoint' or 'cpu' for 3-D")
         seg = 0
     r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt, seg, bool(retain_history))
     s = (slice(None), slice(1, None), slice(1, None), slice(1, None))

@@ -23,6 +23,8 @@ Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
 
 from __future__ import annotations
 
+import os
+
 from dataclasses import dataclass, field
 from enum import StrEnum
 
@@ -107,6 +109,44 @@ class SnapshotBuffers:
     curl_dev: torch.Tensor
     curl_host: torch.Tensor
     keep: list = field(default_factory=list)
+    files: object = None  # DiskFiles of the disk mode
+
+
+class DiskFiles:
+    """Temporary snapshot files of one disk-mode history (one per snapshot
+    kind, under the storage path), removed when the history is released, and
+    the char* arrays the native calls take (ey_filenames / curl_filenames)."""
+
+    def __init__(self, directory: str, want_ey: bool, want_curl: bool):
+        import ctypes
+        import tempfile
+
+        self.paths: list[str | None] = []
+        self.arrays = []
+        for want, tag in ((want_ey, "ey"), (want_curl, "curl")):
+            if not want:
+                self.paths.append(None)
+                self.arrays.append(None)
+                continue
+            fd, path = tempfile.mkstemp(prefix=f"tide_b200_{tag}_", suffix=".bin",
+                                        dir=directory or ".")
+            os.close(fd)
+            self.paths.append(path)
+            self.arrays.append((ctypes.c_char_p * 1)(path.encode()))
+
+    def pointer(self, k: int) -> int:
+        import ctypes
+
+        a = self.arrays[k]
+        return 0 if a is None else ctypes.addressof(a)
+
+    def __del__(self):
+        for p in getattr(self, "paths", []):
+            if p:
+                try:
+                    os.remove(p)
+                except OSError:
+                    pass
 
 
 def history_bytes(n_store: int, n_shots: int, ny: int, nx: int, itemsize: int, n_arrays: int) -> int:
@@ -129,11 +169,6 @@ def resolve_mode(
     m = str(mode).lower()
     if m != "auto":
         code = mode_code(m)
-        if code == STORAGE_DISK:
-            raise NotImplementedError(
-                "storage_mode='disk' is not built in tide_b200; use 'device', 'cpu' "
-                "(pinned host offload) or 'checkpoint' (recompute segments)."
-            )
         return code
     total = history_bytes(n_store, n_shots, ny, nx, itemsize, n_arrays)
     limit_dev = bytes_limit_device
@@ -161,7 +196,12 @@ def allocate(
     device: torch.device,
     want_ey: bool,
     want_curl: bool,
+    path: str = ".",
 ) -> SnapshotBuffers:
+    """Buffers of a snapshot history: device mode the whole history on the
+    device; cpu mode a 3-slot device ring and the pinned host history; disk
+    mode a 3-slot device ring, a 3-slot pinned staging ring and one
+    temporary file per snapshot kind under `path`."""
     empty = torch.empty(0, device=device, dtype=fmt_dtype)
     empty_h = torch.empty(0, dtype=fmt_dtype)
     shot_bytes = ny * nx * fmt_dtype.itemsize
@@ -172,9 +212,13 @@ def allocate(
         if mode == STORAGE_DEVICE:
             return torch.empty((n_store, n_shots, ny, nx), device=device, dtype=fmt_dtype), empty_h
         ring = torch.empty((RING_SLOTS, n_shots, ny, nx), device=device, dtype=fmt_dtype)
-        host = torch.empty((n_store, n_shots, ny * nx), dtype=fmt_dtype, pin_memory=True)
+        n_host = RING_SLOTS if mode == STORAGE_DISK else n_store
+        host = torch.empty((n_host, n_shots, ny * nx), dtype=fmt_dtype, pin_memory=True)
         return ring, host
 
     ed, eh = one(want_ey)
     cd, ch = one(want_curl)
-    return SnapshotBuffers(mode, fmt, fmt_dtype, n_store, shot_bytes, ed, eh, cd, ch)
+    snaps = SnapshotBuffers(mode, fmt, fmt_dtype, n_store, shot_bytes, ed, eh, cd, ch)
+    if mode == STORAGE_DISK and (want_ey or want_curl):
+        snaps.files = DiskFiles(path, want_ey, want_curl)
+    return snaps

@@ -318,7 +318,8 @@ class TMPropagate(torch.autograd.Function):
             )
             if mode == stg.STORAGE_NONE:
                 raise ValueError("storage_mode='none' is incompatible with model gradients")
-            snaps = stg.allocate(mode, sdtype, fmt, n_store, S, pb.ny, pb.nx, device, need_ca, need_cb)
+            snaps = stg.allocate(mode, sdtype, fmt, n_store, S, pb.ny, pb.nx, device, need_ca,
+                                 need_cb, path=opts.get("storage_path") or ".")
             if pb.debye is not None:
                 raise NotImplementedError(
                     "Debye media: gradients run through tide_b200.debye (propagate routes "
@@ -388,7 +389,7 @@ def _storage_call(pb, ca, cb, f, r_ptr, ptrs, mode, fmt, shot_bytes, need_ca, ne
     fn(
         nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(f),
         nat.ptr(ey), nat.ptr(hx), nat.ptr(hz), nat.ptr(mex), nat.ptr(mez), nat.ptr(mhx),
-        nat.ptr(mhz), r_ptr, ptrs[0], ptrs[1], 0, ptrs[2], ptrs[3], 0,
+        nat.ptr(mhz), r_ptr, *ptrs,
         *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
         pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec,
         pb.grad_interval, mode, fmt, shot_bytes, need_ca, need_cb,
@@ -400,15 +401,20 @@ def _storage_call(pb, ca, cb, f, r_ptr, ptrs, mode, fmt, shot_bytes, need_ca, ne
 
 
 def _snap_ptrs(snaps, shift_bytes: int = 0):
-    """Raw addresses of a snapshot set; device pointers shifted back by
+    """Raw addresses of a snapshot set (ey device, ey host, ey file names,
+    curl device, curl host, curl file names); device pointers shifted back by
     shift_bytes so that a segment-sized buffer receives the slots of a later
     segment (the native call adds slot * step_bytes)."""
     d = lambda t: nat.ptr(t) - shift_bytes if t is not None and t.numel() else 0  # noqa: E731
-    return (d(snaps.ey_dev), nat.ptr(snaps.ey_host), d(snaps.curl_dev), nat.ptr(snaps.curl_host))
+    files = snaps.files
+    fp = (lambda k: files.pointer(k)) if files is not None else (lambda k: 0)  # noqa: E731
+    return (d(snaps.ey_dev), nat.ptr(snaps.ey_host), fp(0), d(snaps.curl_dev),
+            nat.ptr(snaps.curl_host), fp(1))
 
 
 def _run_forward_storage(pb, ca, cb, f, r, snaps, need_ca, need_cb, fwd_cb, freq):
-    side = torch.cuda.Stream(pb.device) if snaps.mode == stg.STORAGE_CPU else None
+    side = (torch.cuda.Stream(pb.device)
+            if snaps.mode in (stg.STORAGE_CPU, stg.STORAGE_DISK) else None)
     snaps.keep.append(side)
     nt = pb.nt
     chunk = nt if not fwd_cb else max(1, freq)
@@ -457,7 +463,7 @@ def _backward_call(pb, ca, cb, grad_r, st: _AdjointState, ptrs, mode, fmt, shot_
     fn(
         nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(grad_r),
         *[nat.ptr(t) for t in st.lam], nat.ptr(st.scratch),
-        ptrs[0], ptrs[1], 0, ptrs[2], ptrs[3], 0,
+        *ptrs,
         nat.ptr(st.grad_f), nat.ptr(st.grad_ca), nat.ptr(st.grad_cb), nat.ptr(st.shot_ca),
         nat.ptr(st.shot_cb), *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
         pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec, pb.grad_interval,
@@ -495,8 +501,8 @@ def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts):
     mode = snaps.mode if snaps is not None else stg.STORAGE_NONE
     fmt = snaps.fmt if snaps is not None else 0
     shot_bytes = snaps.shot_bytes if snaps is not None else 0
-    ptrs = _snap_ptrs(snaps) if snaps is not None else (0, 0, 0, 0)
-    side = torch.cuda.Stream(pb.device) if mode == stg.STORAGE_CPU else None
+    ptrs = _snap_ptrs(snaps) if snaps is not None else (0,) * 6
+    side = torch.cuda.Stream(pb.device) if mode in (stg.STORAGE_CPU, stg.STORAGE_DISK) else None
     bwd_cb: Callback | None = opts.get("backward_callback")
     freq = int(opts.get("callback_frequency", 1)) if bwd_cb else 0
     chunk = nt if not bwd_cb else max(1, freq)
@@ -673,6 +679,7 @@ def maxwelltm(
     backward_callback: Callback | None = None,
     callback_frequency: int = 1,
     storage_mode: str = "device",
+    storage_path: str = ".",
     storage_compression: bool | str = False,
     storage_bytes_limit_device: int | None = None,
     storage_bytes_limit_host: int | None = None,
@@ -702,7 +709,7 @@ def maxwelltm(
     opts = dict(
         forward_callback=forward_callback, backward_callback=backward_callback,
         callback_frequency=callback_frequency, storage_mode=storage_mode,
-        storage_compression=storage_compression,
+        storage_path=storage_path, storage_compression=storage_compression,
         storage_bytes_limit_device=storage_bytes_limit_device,
         storage_bytes_limit_host=storage_bytes_limit_host,
         storage_chunk_steps=storage_chunk_steps, retain_history=retain_history,
