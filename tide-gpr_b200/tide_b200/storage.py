@@ -8,6 +8,10 @@ Modes and formats share the reference's integer codes
   ``[n_store, S, ny*nx]``; the native library copies each stored step to the
   host on a side stream while the next steps compute, and streams it back in
   the adjoint (pinned-host offload);
+* ``disk`` (2): a 3-slot device ring, a 3-slot pinned staging ring and one
+  temporary file per snapshot kind under ``storage_path``; a writer thread in
+  the native library writes each staged step, the adjoint reads it back (2-D
+  path);
 * ``none`` (3): nothing stored (forward only);
 * ``auto``: ``device`` when the history fits the device budget, else ``cpu``;
 * ``checkpoint`` (this library's addition): no history; the forward keeps the
@@ -18,7 +22,7 @@ Modes and formats share the reference's integer codes
   ``device`` mode's.
 
 Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
-(float32 fields only).  Disk spilling (mode 2) is not built in this library.
+(float32 fields only).
 """
 
 from __future__ import annotations
