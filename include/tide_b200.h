@@ -139,8 +139,68 @@ TIDE_TM_DECLARE(8, double)
       int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,         \
       int64_t pml_x1, int64_t n_threads, int64_t device, void *compute_stream
 
+/* maxwell_tm_*_born_forward_with_storage_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1701-2086 (argtypes
+ * src/tide/backend_utils.py:351-370).  The Born
+ * forward that also stores the background history the adjoint needs: Ey^n
+ * (ca_requires_grad) and the CPML-corrected curl H^n (cb_requires_grad) at
+ * steps t % step_ratio == 0, in the storage modes and formats of
+ * forward_with_storage.  dey_store / dcurl_store (may be null) receive the
+ * scattered dEy^n and dcurl H^n of the same steps in a device history
+ * [n_store, n_shots, ny, nx] of the snapshot type. */
+#define TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)                              \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T *ey, T *hx, T *hz, T *m_ey_x, T *m_ey_z,     \
+      T *m_hx_z, T *m_hz_x, T *dey, T *dhx, T *dhz, T *dm_ey_x, T *dm_ey_z,    \
+      T *dm_hx_z, T *dm_hz_x, T *r, T *background_r, void *ey_store_1,         \
+      void *ey_store_3, char const *const *ey_filenames, void *curl_store_1,   \
+      void *curl_store_3, char const *const *curl_filenames, void *dey_store,  \
+      void *dcurl_store, T const *ay, T const *by, T const *ayh, T const *byh, \
+      T const *ax, T const *bx, T const *axh, T const *bxh, T const *ky,       \
+      T const *kyh, T const *kx, T const *kxh, int64_t const *sources_i,       \
+      int64_t const *receivers_i, T rdy, T rdx, T dt, int64_t nt,              \
+      int64_t n_shots, int64_t ny, int64_t nx, int64_t n_sources_per_shot,     \
+      int64_t n_receivers_per_shot, int64_t step_ratio, int64_t storage_mode,  \
+      int64_t storage_format, int64_t shot_bytes_uncomp,                       \
+      bool ca_requires_grad, bool cb_requires_grad, bool ca_batched,           \
+      bool cb_batched, bool cq_batched, int64_t start_t, int64_t pml_y0,       \
+      int64_t pml_x0, int64_t pml_y1, int64_t pml_x1, int64_t n_threads,       \
+      int64_t device, void *compute_stream, void *storage_stream
+
+/* maxwell_tm_*_born_backward_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:2088-2400 (argtypes
+ * src/tide/backend_utils.py:386-405).  The adjoint of the
+ * Born map for (dca, dcb, df): the scattered E update adds dca Ey^n + dcb
+ * curl H^n of the background, so grad_ca / grad_cb are the background
+ * history correlated with the adjoint Ey, exactly as in backward, and
+ * grad_f is the adjoint at the sources.  The arguments are backward's
+ * without adjoint_memory_scratch (the call allocates its CPML adjoint
+ * ping-pong buffers in stream order) and with work_x / work_z (unused, as
+ * in the reference). */
+#define TIDE_TM_BORN_BACKWARD_ARGS(T)                                          \
+  T const *ca, T const *cb, T const *cq, T const *grad_r, T *lambda_ey,        \
+      T *lambda_hx, T *lambda_hz, T *m_lambda_ey_x, T *m_lambda_ey_z,          \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, void *ey_store_1, void *ey_store_3,  \
+      char const *const *ey_filenames, void *curl_store_1, void *curl_store_3, \
+      char const *const *curl_filenames, T *grad_f, T *grad_ca, T *grad_cb,    \
+      T *grad_ca_shot, T *grad_cb_shot, T *work_x, T *work_z, T const *ay,     \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *ky, T const *kyh, T const *kx,      \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream,                 \
+      void *storage_stream
+
 #define TIDE_TM_BORN_DECLARE(S, T)                                             \
-  void maxwell_tm_##S##_##T##_born_forward_cuda(TIDE_TM_BORN_FORWARD_ARGS(T));
+  void maxwell_tm_##S##_##T##_born_forward_cuda(TIDE_TM_BORN_FORWARD_ARGS(T)); \
+  void maxwell_tm_##S##_##T##_born_forward_with_storage_cuda(                  \
+      TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T));                              \
+  void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T));
 
 TIDE_TM_BORN_DECLARE(2, float)
 TIDE_TM_BORN_DECLARE(4, float)

@@ -1,0 +1,236 @@
+"""Gradients through the Born pass on the GPU.
+
+* ``born_forward_with_storage`` advances both states exactly as
+  ``born_forward`` (receivers and states bit-identical), stores the same
+  background history as ``forward_with_storage`` (bit for bit, FULL and BF16,
+  sampling intervals 1 and 2), and its scattered history holds dEy^n and
+  dcurl H^n of the scattered state;
+* ``born_backward`` returns backward's gradients bit for bit on that
+  history (the scattered update is linear in (dca, dcb, df) with the
+  background factors of (ca, cb, f));
+* through ``borntm``: the adjoint dot-product test <J v, w> = <v, J^T w> in
+  (depsilon, dsigma) (FP64, 1e-12), the depsilon gradient against the
+  epsilon gradient of ``maxwelltm`` on interior cells (FP64, 1e-10), the
+  background-receiver gradient equal to ``maxwelltm``'s bit for bit, and
+  cpu / disk storage giving the device mode's gradients bit for bit;
+* the second-order term (scattered receivers in the background model) and
+  checkpoint storage raise.
+"""
+
+from __future__ import annotations
+
+import pytest
+import torch
+
+import tide_b200 as tide
+from cases import clone_problem, random_problem
+from oracle_harness import rel_l2
+from tide_b200 import born as bn
+from tide_b200 import storage as stg
+from tide_b200 import tm2d
+
+pytestmark = pytest.mark.gpu
+
+
+def _perturbation(pb, seed, dev):
+    g = torch.Generator().manual_seed(seed)
+    shape = (1, pb.ny, pb.nx)
+    dca = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype)
+    dcb = (1e-3 * torch.randn(shape, generator=g, dtype=torch.float64)).to(pb.dtype) * pb.cb
+    df = (torch.randn(pb.f.shape, generator=g, dtype=torch.float64).to(pb.dtype) * 0.1
+          * pb.f.abs().max())
+    return [t.contiguous().to(dev) for t in (dca, dcb, df)]
+
+
+def _born(q, d, snaps=None, direct=(0, 0)):
+    tan = [torch.zeros_like(t) for t in q.fields]
+    r = torch.zeros((q.nt, q.n_shots, q.n_rec), device=q.device, dtype=q.dtype)
+    bg = torch.zeros_like(r)
+    need = (snaps is not None and snaps.ey_dev.numel() > 0,
+            snaps is not None and snaps.curl_dev.numel() > 0)
+    bn._born_forward_call(q, d[0], d[1], d[2], q.f, tan, r, bg, snaps, need, None, direct)
+    torch.cuda.synchronize()
+    return r, bg, q.fields, tan
+
+
+def _history(q, fmt, sdtype, n_store, mode=stg.STORAGE_DEVICE, path="."):
+    """A history whose cells outside the update domain (never written) are 0."""
+    h = stg.allocate(mode, sdtype, fmt, n_store, q.n_shots, q.ny, q.nx, q.device, True, True,
+                     path=path)
+    h.ey_dev.zero_()
+    h.curl_dev.zero_()
+    return h
+
+
+@pytest.mark.parametrize("stencil,k,bf16", [(2, 1, False), (4, 2, False), (2, 1, True),
+                                            (8, 3, True)])
+def test_born_storage_forward_matches_born_and_storage_forward(cuda_device, stencil, k, bf16):
+    dev = cuda_device
+    pb = random_problem(810 + stencil, 33, 47, 3, 41, stencil=stencil, pml=6, k=k)
+    d = _perturbation(pb, 5, dev)
+    fmt, sdtype = (1, torch.bfloat16) if bf16 else (0, torch.float32)
+    n_store = (pb.nt + k - 1) // k
+    ref = _born(clone_problem(pb, dev), d)
+    q = clone_problem(pb, dev)
+    snaps = _history(q, fmt, sdtype, n_store)
+    got = _born(q, d, snaps)
+    for a, b in zip((ref[0], ref[1], *ref[2], *ref[3]), (got[0], got[1], *got[2], *got[3])):
+        assert torch.equal(a, b)
+    # the same history as the plain storing forward
+    p = clone_problem(pb, dev)
+    plain = _history(p, fmt, sdtype, n_store)
+    r = torch.zeros((p.nt, p.n_shots, p.n_rec), device=dev, dtype=p.dtype)
+    tm2d._storage_call(p, p.ca, p.cb, p.f, r.data_ptr(), tm2d._snap_ptrs(plain), 0, fmt,
+                       plain.shot_bytes, True, True, 0, p.nt)
+    torch.cuda.synchronize()
+    assert torch.equal(r, got[1])
+    assert torch.equal(plain.ey_dev, snaps.ey_dev)
+    assert torch.equal(plain.curl_dev, snaps.curl_dev)
+
+
+def test_born_storage_scattered_history(cuda_device):
+    """dey_store[q] is the scattered Ey after q*k steps; dcurl_store[q] is the
+    curl a plain storing step computes from that scattered state."""
+    dev = cuda_device
+    k = 2
+    pb = random_problem(833, 31, 45, 2, 30, pml=6, k=k)
+    d = _perturbation(pb, 7, dev)
+    n_store = (pb.nt + k - 1) // k
+    q = clone_problem(pb, dev)
+    snaps = _history(q, 0, torch.float32, n_store)
+    dey_h = torch.zeros((n_store, q.n_shots, q.ny, q.nx), device=dev, dtype=q.dtype)
+    dcurl_h = torch.zeros_like(dey_h)
+    _born(q, d, snaps, (dey_h.data_ptr(), dcurl_h.data_ptr()))
+    for qi in (3, n_store - 1):
+        t = qi * k
+        p = clone_problem(pb, dev)
+        p.nt = t
+        p.f = p.f[: t * p.n_shots * p.n_src].contiguous()
+        dp = [d[0], d[1], d[2][: t * p.n_shots * p.n_src].contiguous()]
+        _, _, _, tan = _born(p, dp)
+        assert torch.equal(tan[0], dey_h[qi])
+        # one plain storing step from the scattered state gives its curl
+        s = clone_problem(pb, dev)
+        for a, b in zip(s.fields, tan):
+            a.copy_(b)
+        one = _history(s, 0, torch.float32, 1)
+        r = torch.zeros((1, s.n_shots, s.n_rec), device=dev, dtype=s.dtype)
+        s.f = torch.zeros_like(s.f[: s.n_shots * s.n_src])
+        tm2d._storage_call(s, s.ca, s.cb, s.f, r.data_ptr(), tm2d._snap_ptrs(one), 0, 0,
+                           one.shot_bytes, True, True, 0, 1)
+        torch.cuda.synchronize()
+        assert torch.equal(one.curl_dev[0], dcurl_h[qi])
+
+
+@pytest.mark.parametrize("stencil,k", [(2, 1), (4, 2)])
+def test_born_backward_equals_backward(cuda_device, stencil, k):
+    dev = cuda_device
+    pb = random_problem(850 + stencil, 35, 49, 3, 44, stencil=stencil, pml=6, k=k)
+    d = _perturbation(pb, 9, dev)
+    q = clone_problem(pb, dev)
+    snaps = _history(q, 0, torch.float32, (pb.nt + k - 1) // k)
+    _born(q, d, snaps)
+    g = torch.Generator().manual_seed(4)
+    grad_r = torch.randn((pb.nt, pb.n_shots, pb.n_rec), generator=g).to(dev)
+    st = tm2d._AdjointState(q, True, True, scratch=False)
+    bn._born_backward_call(q, grad_r, st, snaps, True, True)
+    ref = tm2d._AdjointState(q, True, True)
+    tm2d._backward_call(q, q.ca, q.cb, grad_r, ref, tm2d._snap_ptrs(snaps), 0, 0,
+                        snaps.shot_bytes, True, True, pb.nt, pb.nt)
+    torch.cuda.synchronize()
+    for a, b in zip(st.result(q, True, True, True), ref.result(q, True, True, True)):
+        assert torch.equal(a, b)
+    assert float(st.grad_ca.abs().max()) > 0 and float(st.grad_cb.abs().max()) > 0
+
+
+def _case(dev, dtype=torch.float64, seed=3, stencil=2):
+    g = torch.Generator().manual_seed(seed)
+    ny, nx, S, nt = 30, 44, 2, 70
+    eps = (2.0 + 4.0 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    sig = (0.005 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    mu = torch.ones((ny, nx), device=dev, dtype=dtype)
+    dx = 0.02
+    dt = 0.9 * dx / (tide.C0 / float(eps.min().sqrt()) * 2 ** 0.5)
+    amp = tide.ricker(500e6, nt, dt, dtype=dtype).view(1, 1, nt).repeat(S, 1, 1).to(dev)
+    src = torch.tensor([[[10, 12]], [[15, 30]]], device=dev)
+    rec = torch.tensor([[[5, 5 + 3 * j] for j in range(10)]] * S, device=dev)
+    deps = (0.3 * torch.randn((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    dsig = (1e-3 * torch.randn((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    w = torch.randn((nt, S, 10), generator=g, dtype=torch.float64).to(dtype).to(dev)
+    return dict(eps=eps, sig=sig, mu=mu, dx=dx, dt=dt, amp=amp, src=src, rec=rec, deps=deps,
+                dsig=dsig, w=w, stencil=stencil)
+
+
+def _borntm(c, deps, dsig, eps=None, **kw):
+    return tide.borntm(c["eps"] if eps is None else eps, c["sig"], c["mu"], c["dx"], c["dt"],
+                       c["amp"], c["src"], c["rec"], c["rec"], depsilon=deps, dsigma=dsig,
+                       stencil=c["stencil"], pml_width=8, **kw)
+
+
+def _born_grads(c, **kw):
+    deps = c["deps"].clone().requires_grad_()
+    dsig = c["dsig"].clone().requires_grad_()
+    r = _borntm(c, deps, dsig, **kw)[-1]
+    (r * c["w"]).sum().backward()
+    return r.detach(), deps.grad, dsig.grad
+
+
+def test_borntm_adjoint_dot_product(cuda_device):
+    c = _case(cuda_device)
+    r, g_eps, g_sig = _born_grads(c)
+    lhs = float((r * c["w"]).sum())
+    rhs = float((g_eps * c["deps"]).sum() + (g_sig * c["dsig"]).sum())
+    assert abs(lhs) > 0
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_borntm_gradient_matches_maxwelltm_gradient(cuda_device, stencil):
+    """d<r_born(v), w>/dv = J^T w = d<r(eps), w>/d eps (interior cells: the
+    Born perturbation is zero-padded, the model replicate-padded)."""
+    c = _case(cuda_device, stencil=stencil)
+    _, g_eps, g_sig = _born_grads(c)
+    eps = c["eps"].clone().requires_grad_()
+    sig = c["sig"].clone().requires_grad_()
+    r = tide.maxwelltm(eps, sig, c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
+                       stencil=stencil, pml_width=8)[-1]
+    (r * c["w"]).sum().backward()
+    inner = (slice(1, -1), slice(1, -1))
+    assert rel_l2(g_eps[inner], eps.grad[inner]) <= 1e-10
+    assert rel_l2(g_sig[inner], sig.grad[inner]) <= 1e-10
+
+
+def test_borntm_background_receiver_gradient_equals_maxwelltm(cuda_device):
+    c = _case(cuda_device)
+    eps = c["eps"].clone().requires_grad_()
+    bg_r = _borntm(c, c["deps"], c["dsig"], eps=eps)[-2]
+    (bg_r * c["w"]).sum().backward()
+    eps2 = c["eps"].clone().requires_grad_()
+    r = tide.maxwelltm(eps2, c["sig"], c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
+                       pml_width=8)[-1]
+    assert torch.equal(bg_r.detach(), r.detach())
+    (r * c["w"]).sum().backward()
+    assert torch.equal(eps.grad, eps2.grad)
+
+
+@pytest.mark.parametrize("mode", ["cpu", "disk"])
+@pytest.mark.parametrize("compression", [False, "bf16"])
+def test_borntm_host_and_disk_storage_match_device(cuda_device, tmp_path, mode, compression):
+    c = _case(cuda_device, dtype=torch.float32)
+    ref = _born_grads(c, storage_compression=compression)
+    got = _born_grads(c, storage_mode=mode, storage_path=str(tmp_path),
+                      storage_compression=compression)
+    for a, b in zip(ref, got):
+        assert torch.equal(a, b)
+    assert list(tmp_path.iterdir()) == [] or mode == "cpu"
+
+
+def test_borntm_unbuilt_parts_raise(cuda_device):
+    c = _case(cuda_device)
+    eps = c["eps"].clone().requires_grad_()
+    deps = c["deps"].clone().requires_grad_()
+    r = _borntm(c, deps, c["dsig"], eps=eps)[-1]
+    with pytest.raises(NotImplementedError, match="second"):
+        (r * c["w"]).sum().backward()
+    with pytest.raises(NotImplementedError, match="checkpoint"):
+        _borntm(c, deps, c["dsig"], storage_mode="checkpoint")

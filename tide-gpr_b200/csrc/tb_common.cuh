@@ -70,3 +70,12 @@ class ProfileScope {
       return;                                                                 \
     }                                                                         \
   } while (0)
+
+// TB_REQUIRE for helpers that report failure by returning false.
+#define TB_REQUIRE_B(cond, ...)                                               \
+  do {                                                                        \
+    if (!(cond)) {                                                            \
+      tb::set_error(tb::kBadArgument, __VA_ARGS__);                           \
+      return false;                                                           \
+    }                                                                         \
+  } while (0)

@@ -434,62 +434,169 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Snapshot history of a storing forward pass, shared by the plain and the Born
+// storing forwards (cu_inst:1281-1609 and 1701-2086 run the same pipeline).
+// Storage modes: 0 device (the whole history in *_store_1), 1 cpu (3-slot
+// device ring in *_store_1, pinned host history in *_store_3), 2 disk (device
+// ring, 3-slot pinned staging ring in *_store_3, one file per snapshot kind
+// written by a DiskHistory thread), 3 none.  Store index q = t / step_ratio
+// sits at q * step_bytes of its history (device, host or file).
+struct StoreRun {
+  bool want = false, bf16 = false, host_side = false, pipeline = false, to_disk = false;
+  int64_t mode = 3, step_ratio = 1;
+  size_t step_bytes = 0;
+  char *e1 = nullptr, *c1 = nullptr, *e3 = nullptr, *c3 = nullptr;
+  cudaStream_t st = nullptr, ss = nullptr;
+  std::unique_ptr<DiskHistory> disk[2];
+  EventRing staged;                     // a staging slot's device-to-host copy is done
+  EventRing store_done, compute_done;   // cpu/disk pipeline on the storage stream
+
+  // Validates the storage arguments; false (with the error set) on bad ones.
+  bool init(bool store_ey, bool store_curl, int64_t storage_mode, int64_t storage_format,
+            size_t field_size, int64_t shot_bytes_uncomp, int64_t ny, int64_t nx,
+            int64_t n_shots, int64_t ratio, void *ey_store_1, void *ey_store_3,
+            char const *const *ey_filenames, void *curl_store_1, void *curl_store_3,
+            char const *const *curl_filenames, cudaStream_t compute, cudaStream_t storage) {
+    TB_REQUIRE_B(storage_mode >= 0 && storage_mode <= 3, "TM2D: unknown storage_mode %lld",
+                 (long long)storage_mode);
+    bf16 = storage_format == 1;
+    TB_REQUIRE_B(!bf16 || field_size == 4, "TM2D: bf16 snapshot storage requires float32 fields");
+    want = (store_ey || store_curl) && storage_mode != 3;
+    mode = storage_mode;
+    step_ratio = ratio;
+    st = compute;
+    ss = storage;
+    if (!want) return true;
+    const size_t esz = bf16 ? 2 : field_size;
+    TB_REQUIRE_B(shot_bytes_uncomp == ny * nx * (int64_t)esz,
+                 "TM2D: shot_bytes_uncomp=%lld does not match ny*nx*elem=%lld",
+                 (long long)shot_bytes_uncomp, (long long)(ny * nx * (int64_t)esz));
+    TB_REQUIRE_B((!store_ey || ey_store_1) && (!store_curl || curl_store_1),
+                 "TM2D: snapshot buffers missing");
+    host_side = mode == 1 || mode == 2;
+    to_disk = mode == 2;
+    TB_REQUIRE_B(!host_side || ((!store_ey || ey_store_3) && (!store_curl || curl_store_3)),
+                 "TM2D: cpu / disk storage modes need host snapshot buffers");
+    TB_REQUIRE_B(!to_disk || ((!store_ey || (ey_filenames && ey_filenames[0])) &&
+                              (!store_curl || (curl_filenames && curl_filenames[0]))),
+                 "TM2D: disk storage mode needs snapshot file names");
+    if (store_ey) {
+      e1 = (char *)ey_store_1;
+      e3 = (char *)ey_store_3;
+    }
+    if (store_curl) {
+      c1 = (char *)curl_store_1;
+      c3 = (char *)curl_store_3;
+    }
+    step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+    pipeline = host_side && ss != nullptr && ss != st;
+    if (to_disk) {
+      if (!staged.ok) {
+        set_error(kCudaError, "TM2D: event creation failed");
+        return false;
+      }
+      const char *names[2] = {store_ey ? ey_filenames[0] : nullptr,
+                              store_curl ? curl_filenames[0] : nullptr};
+      for (int k = 0; k < 2; ++k)
+        if (names[k]) {
+          disk[k].reset(new DiskHistory(names[k], true, kRing));
+          if (!disk[k]->ok()) {
+            set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
+            return false;
+          }
+        }
+    }
+    if (pipeline) {
+      if (!store_done.ok || !compute_done.ok) {
+        set_error(kCudaError, "TM2D: event creation failed");
+        return false;
+      }
+      for (int k = 0; k < kRing; ++k)
+        if (TB_CUDA(cudaEventRecord(store_done.ev[k], ss))) return false;
+    }
+    return true;
+  }
+
+  bool stores(int64_t t) const { return want && (t % step_ratio) == 0; }
+
+  // Device slots that step t writes (null when the step stores nothing); the
+  // compute stream waits until the slot's previous host copy has run.
+  bool begin(int64_t t, char **e, char **c) {
+    *e = *c = nullptr;
+    if (!stores(t)) return true;
+    const int64_t q = t / step_ratio;
+    const int slot = (int)(q % kRing);
+    const size_t off = mode == 0 ? (size_t)q * step_bytes : (size_t)slot * step_bytes;
+    if (e1) *e = e1 + off;
+    if (c1) *c = c1 + off;
+    return !(pipeline && TB_CUDA(cudaStreamWaitEvent(st, store_done.ev[slot], 0)));
+  }
+
+  // After step t's launches: cpu mode copies the slots into the host history;
+  // disk mode copies them into the staging slot (whose previous write must
+  // have finished) and queues the slot for the file.
+  bool end(int64_t t, const char *e, const char *c) {
+    if (!stores(t) || !host_side) return true;
+    const int64_t q = t / step_ratio;
+    const int slot = (int)(q % kRing);
+    cudaStream_t cs = st;
+    if (pipeline) {
+      if (TB_CUDA(cudaEventRecord(compute_done.ev[slot], st))) return false;
+      if (TB_CUDA(cudaStreamWaitEvent(ss, compute_done.ev[slot], 0))) return false;
+      cs = ss;
+    }
+    const size_t off3 = to_disk ? (size_t)slot * step_bytes : (size_t)q * step_bytes;
+    char *h3[2] = {e3 ? e3 + off3 : nullptr, c3 ? c3 + off3 : nullptr};
+    const char *d1[2] = {e, c};
+    for (int k = 0; k < 2; ++k) {
+      if (!d1[k]) continue;
+      if (to_disk) disk[k]->wait_slot(slot);
+      if (TB_CUDA(cudaMemcpyAsync(h3[k], d1[k], step_bytes, cudaMemcpyDeviceToHost, cs)))
+        return false;
+    }
+    if (to_disk) {
+      if (TB_CUDA(cudaEventRecord(staged.ev[slot], cs))) return false;
+      for (int k = 0; k < 2; ++k)
+        if (d1[k])
+          disk[k]->enqueue_write(slot, h3[k], step_bytes, (int64_t)(q * step_bytes),
+                                 staged.ev[slot]);
+    }
+    return !(pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss)));
+  }
+
+  // The call returns once the host history is complete and the files written.
+  bool finish() {
+    if (pipeline && TB_CUDA(cudaStreamSynchronize(ss))) return false;
+    for (int k = 0; k < 2; ++k)
+      if (disk[k] && !disk[k]->finish()) {
+        set_error(kCudaError, "TM2D disk storage: %s", disk[k]->error().c_str());
+        return false;
+      }
+    return true;
+  }
+};
+
 template <typename T, int ST>
 void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
-  (void)dt; (void)n_threads; (void)ey_filenames; (void)curl_filenames;
+  (void)dt; (void)n_threads;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
   TB_REQUIRE(nt >= 0 && step_ratio >= 1, "TM2D forward_with_storage: bad nt/step_ratio");
   TB_REQUIRE(ca && cb && cq && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z && m_hz_x,
              "TM2D forward_with_storage: a field or coefficient pointer is null");
   TB_REQUIRE(n_sources_per_shot == 0 || f, "TM2D forward_with_storage: sources without amplitudes");
   TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D forward_with_storage: receivers without output");
-  TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "TM2D: unknown storage_mode %lld",
-             (long long)storage_mode);
-  const bool bf16 = storage_format == 1;
-  TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
-  const bool want_store = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
-  const size_t esz = bf16 ? 2 : sizeof(T);
-  if (want_store) {
-    TB_REQUIRE(shot_bytes_uncomp == ny * nx * (int64_t)esz,
-               "TM2D: shot_bytes_uncomp=%lld does not match ny*nx*elem=%lld",
-               (long long)shot_bytes_uncomp, (long long)(ny * nx * (int64_t)esz));
-    TB_REQUIRE((!ca_requires_grad || ey_store_1) && (!cb_requires_grad || curl_store_1),
-               "TM2D: snapshot buffers missing");
-    TB_REQUIRE((storage_mode != 1 && storage_mode != 2) ||
-                   ((!ca_requires_grad || ey_store_3) && (!cb_requires_grad || curl_store_3)),
-               "TM2D: cpu / disk storage modes need host snapshot buffers");
-    TB_REQUIRE(storage_mode != 2 ||
-                   ((!ca_requires_grad || (ey_filenames && ey_filenames[0])) &&
-                    (!cb_requires_grad || (curl_filenames && curl_filenames[0]))),
-               "TM2D: disk storage mode needs snapshot file names");
-  }
+  cudaStream_t st = as_stream(compute_stream);
+  StoreRun sr;
+  if (!sr.init(ca_requires_grad, cb_requires_grad, storage_mode, storage_format, sizeof(T),
+               shot_bytes_uncomp, ny, nx, n_shots, step_ratio, ey_store_1, ey_store_3,
+               ey_filenames, curl_store_1, curl_store_3, curl_filenames, st,
+               as_stream(storage_stream)))
+    return;
   Launch<T, ST> L;
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
-  cudaStream_t st = as_stream(compute_stream);
-  cudaStream_t ss = as_stream(storage_stream);
-  const bool host_side = want_store && (storage_mode == 1 || storage_mode == 2);
-  const bool pipeline = host_side && ss != nullptr && ss != st;
-  // disk mode: one writer per snapshot kind; host staging ring in *_store_3
-  std::unique_ptr<DiskHistory> disk[2];
-  EventRing staged;
-  if (want_store && storage_mode == 2) {
-    if (!staged.ok) {
-      set_error(kCudaError, "TM2D: event creation failed");
-      return;
-    }
-    const char *names[2] = {ca_requires_grad ? ey_filenames[0] : nullptr,
-                            cb_requires_grad ? curl_filenames[0] : nullptr};
-    for (int k = 0; k < 2; ++k)
-      if (names[k]) {
-        disk[k].reset(new DiskHistory(names[k], true, kRing));
-        if (!disk[k]->ok()) {
-          set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
-          return;
-        }
-      }
-  }
   // one launch per step (see fused_pays)
   const bool fused = is_float<T>() && ST == 2 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N);
   PitchedFwd pf;
@@ -503,31 +610,15 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
               : build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0}, sources_i,
                              n_sources_per_shot, receivers_i, n_receivers_per_shot, st)))
     return;
-  EventRing store_done, compute_done;
-  if (pipeline) {
-    if (!store_done.ok || !compute_done.ok) {
-      set_error(kCudaError, "TM2D: event creation failed");
-      return;
-    }
-    for (int k = 0; k < kRing; ++k)
-      if (TB_CUDA(cudaEventRecord(store_done.ev[k], ss))) return;
-  }
-  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
+  const bool bf16 = sr.bf16;
   ProfileScope prof(st);
   for (int64_t t = start_t; t < start_t + nt; ++t) {
     const bool smp = prof.sample(t);
-    const bool store_step = want_store && (t % step_ratio) == 0;
-    const int64_t q = t / step_ratio;
-    const int slot = (int)(q % kRing);
-    char *e1 = nullptr, *c1 = nullptr;
-    if (store_step) {
-      const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes : (size_t)slot * step_bytes;
-      if (ca_requires_grad) e1 = (char *)ey_store_1 + off1;
-      if (cb_requires_grad) c1 = (char *)curl_store_1 + off1;
-      if (pipeline && TB_CUDA(cudaStreamWaitEvent(st, store_done.ev[slot], 0))) return;
-    }
+    const bool store_step = sr.stores(t);
+    char *e1, *c1;
+    if (!sr.begin(t, &e1, &c1)) return;
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
     if (fused) {
@@ -555,46 +646,14 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
                                ps, ft, rt);
       if (smp) prof.end(kKFwdE);
     }
-    if (store_step && host_side) {
-      cudaStream_t cs = st;
-      if (pipeline) {
-        if (TB_CUDA(cudaEventRecord(compute_done.ev[slot], st))) return;
-        if (TB_CUDA(cudaStreamWaitEvent(ss, compute_done.ev[slot], 0))) return;
-        cs = ss;
-      }
-      // cpu mode: straight into the host history; disk mode: into the staging
-      // slot, whose previous write must have finished, then queued for the file
-      const bool to_disk = storage_mode == 2;
-      const size_t off3 = to_disk ? (size_t)slot * step_bytes : (size_t)q * step_bytes;
-      char *h3[2] = {(char *)ey_store_3 + off3, (char *)curl_store_3 + off3};
-      const char *d1[2] = {e1, c1};
-      for (int k = 0; k < 2; ++k) {
-        if (!d1[k]) continue;
-        if (to_disk) disk[k]->wait_slot(slot);
-        if (TB_CUDA(cudaMemcpyAsync(h3[k], d1[k], step_bytes, cudaMemcpyDeviceToHost, cs)))
-          return;
-      }
-      if (to_disk) {
-        if (TB_CUDA(cudaEventRecord(staged.ev[slot], cs))) return;
-        for (int k = 0; k < 2; ++k)
-          if (d1[k])
-            disk[k]->enqueue_write(slot, h3[k], step_bytes, (int64_t)(q * step_bytes),
-                                   staged.ev[slot]);
-      }
-      if (pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss))) return;
-    }
+    if (!sr.end(t, e1, c1)) return;
   }
   count_launches(fused ? nt : nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
   if constexpr (is_float<T>()) {
     if (fused && !pf.finish()) return;
   }
-  if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
-  for (int k = 0; k < 2; ++k)
-    if (disk[k] && !disk[k]->finish()) {
-      set_error(kCudaError, "TM2D disk storage: %s", disk[k]->error().c_str());
-      return;
-    }
+  sr.finish();
 }
 
 // ---------------------------------------------------------------------------

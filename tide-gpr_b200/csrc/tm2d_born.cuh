@@ -7,14 +7,24 @@
 // scattered sources (df) and records both states at the receivers.  Every
 // expression keeps the reference's operation order, so with the same inputs
 // the results are bit-identical to its CPU backend.
+//
+// The storing Born forward (cu_inst:1701-2086) runs the same steps through the
+// snapshot pipeline of forward_with_storage (StoreRun), storing the
+// background Ey^n / curl H^n and, when asked, the scattered dEy^n / dcurl H^n.
+// The Born backward for (dca, dcb, df) (cu_inst:2088-2400) is the ordinary
+// adjoint over the background history: the scattered update is linear in
+// (dca, dcb, df) with factors Ey^n, curl H^n and the source weights, which
+// are the factors of (ca, cb, f) in the background update.
 #pragma once
 
 namespace tb {
 namespace {
 
 // Born E half-step.  Full-grid tiles of 32 x 8R (as k_fwd_e) so point
-// entries outside the update domain are still served.
-template <typename T, int ST, int R>
+// entries outside the update domain are still served.  Non-null store
+// pointers (this step's slots, type S) receive Ey^n, curl H^n, dEy^n and
+// dcurl H^n of the update domain.
+template <typename T, int ST, typename S, int R>
 __global__ void __launch_bounds__(256)
 k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
          const T *__restrict__ dca, const T *__restrict__ dcb, const T *__restrict__ hx,
@@ -22,7 +32,8 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
          T *__restrict__ m_hz_x, const T *__restrict__ dhx, const T *__restrict__ dhz,
          T *__restrict__ dey, T *__restrict__ dm_hx_z, T *__restrict__ dm_hz_x, PointCSR src,
          PointCSR rec, const T *__restrict__ f0_t, const T *__restrict__ df_t,
-         T *__restrict__ r_t, T *__restrict__ bgr_t) {
+         T *__restrict__ r_t, T *__restrict__ bgr_t, S *__restrict__ es,
+         S *__restrict__ cs, S *__restrict__ des, S *__restrict__ dcs) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
@@ -68,6 +79,10 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
       }
       const T curl = dz - dy, dcurl = ddz - ddy;
       const T e_n = e, de_n = de;
+      if (es) store_stream(es + i, Codec<S, T>::enc(e_n));
+      if (cs) store_stream(cs + i, Codec<S, T>::enc(curl));
+      if (des) store_stream(des + i, Codec<S, T>::enc(de_n));
+      if (dcs) store_stream(dcs + i, Codec<S, T>::enc(dcurl));
       e = cav * e_n + cbv * curl;
       de = cav * de_n + cbv * dcurl + dcav * e_n + dcbv * curl;
     }
@@ -110,13 +125,98 @@ void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
       launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
       launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
     }
-    k_born_e<T, ST, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+    k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
         L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
         ps.src, ps.rec, f0 ? f0 + t * fs : nullptr, df ? df + t * fs : nullptr,
-        r ? r + t * rs : nullptr, background_r ? background_r + t * rs : nullptr);
+        r ? r + t * rs : nullptr, background_r ? background_r + t * rs : nullptr, nullptr,
+        nullptr, nullptr, nullptr);
   }
   count_launches(nt * (L.has_domain ? 3 : 1));
   TB_CUDA(cudaGetLastError());
+}
+
+template <typename T, int ST>
+void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
+  (void)dt; (void)n_threads;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1, "TM2D born_forward_with_storage: bad nt/step_ratio");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && ey && hx && hz && m_ey_x && m_ey_z && m_hx_z &&
+                 m_hz_x && dey && dhx && dhz && dm_ey_x && dm_ey_z && dm_hx_z && dm_hz_x,
+             "TM2D born_forward_with_storage: a field, memory or coefficient pointer is null");
+  TB_REQUIRE(n_sources_per_shot == 0 || (f0 && df),
+             "TM2D born_forward_with_storage: sources without background or scattered amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r,
+             "TM2D born_forward_with_storage: receivers without output");
+  cudaStream_t st = as_stream(compute_stream);
+  StoreRun sr;
+  if (!sr.init(ca_requires_grad, cb_requires_grad, storage_mode, storage_format, sizeof(T),
+               shot_bytes_uncomp, ny, nx, n_shots, step_ratio, ey_store_1, ey_store_3,
+               ey_filenames, curl_store_1, curl_store_3, curl_filenames, st,
+               as_stream(storage_stream)))
+    return;
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  PointScratch ps;
+  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+                    sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
+    return;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    char *e1, *c1;
+    if (!sr.begin(t, &e1, &c1)) return;
+    // scattered history: device-resident, indexed by store index
+    char *de1 = nullptr, *dc1 = nullptr;
+    if (sr.stores(t)) {
+      const size_t off = (size_t)(t / step_ratio) * sr.step_bytes;
+      if (dey_store) de1 = (char *)dey_store + off;
+      if (dcurl_store) dc1 = (char *)dcurl_store + off;
+    }
+    if (L.has_domain) {
+      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+    }
+    const T *f0t = f0 ? f0 + t * fs : nullptr, *dft = df ? df + t * fs : nullptr;
+    T *rt = r ? r + t * rs : nullptr, *bgt = background_r ? background_r + t * rs : nullptr;
+    if (sr.stores(t) && sr.bf16) {
+      using B = __nv_bfloat16;
+      k_born_e<T, ST, B, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+          L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
+          ps.src, ps.rec, f0t, dft, rt, bgt, (B *)e1, (B *)c1, (B *)de1, (B *)dc1);
+    } else {
+      k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+          L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
+          ps.src, ps.rec, f0t, dft, rt, bgt, (T *)e1, (T *)c1, (T *)de1, (T *)dc1);
+    }
+    if (!sr.end(t, e1, c1)) return;
+  }
+  count_launches(nt * (L.has_domain ? 3 : 1));
+  if (TB_CUDA(cudaGetLastError())) return;
+  sr.finish();
+}
+
+// The CPML adjoint ping-pong buffers backward takes as adjoint_memory_scratch
+// are allocated here in stream order (4 x n_shots x ny x nx).
+template <typename T, int ST>
+void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
+  (void)work_x; (void)work_z;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(n_shots >= 0 && ny > 0 && nx > 0, "TM2D born_backward: bad shape");
+  cudaStream_t st = as_stream(compute_stream);
+  T *scratch = nullptr;
+  const size_t bytes = 4 * (size_t)n_shots * (size_t)ny * (size_t)nx * sizeof(T);
+  if (TB_CUDA(cudaMallocAsync((void **)&scratch, bytes > 0 ? bytes : sizeof(T), st))) return;
+  tm_backward<T, ST>(ca, cb, cq, grad_r, lambda_ey, lambda_hx, lambda_hz, m_lambda_ey_x,
+                     m_lambda_ey_z, m_lambda_hx_z, m_lambda_hz_x, scratch, ey_store_1,
+                     ey_store_3, ey_filenames, curl_store_1, curl_store_3, curl_filenames,
+                     grad_f, grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ay, by, ayh, byh, ax,
+                     bx, axh, bxh, ky, kyh, kx, kxh, sources_i, receivers_i, rdy, rdx, dt, nt,
+                     n_shots, ny, nx, n_sources_per_shot, n_receivers_per_shot, step_ratio,
+                     storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad,
+                     cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t, pml_y0,
+                     pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);
+  TB_CUDA(cudaFreeAsync(scratch, st));
 }
 
 }  // namespace
@@ -131,6 +231,29 @@ void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
         n_sources_per_shot, n_receivers_per_shot, step_ratio, ca_batched, cb_batched,         \
         cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device,               \
         compute_stream);                                                               \
+  }                                                                                    \
+  extern "C" void maxwell_tm_##S##_##T##_born_forward_with_storage_cuda(              \
+      TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {                                     \
+    tb::tm_born_forward_with_storage<T, S>(                                            \
+        ca, cb, cq, dca, dcb, f0, df, ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x, dey, dhx,   \
+        dhz, dm_ey_x, dm_ey_z, dm_hx_z, dm_hz_x, r, background_r, ey_store_1, ey_store_3,     \
+        ey_filenames, curl_store_1, curl_store_3, curl_filenames, dey_store, dcurl_store, ay, \
+        by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, sources_i, receivers_i, rdy, rdx,   \
+        dt, nt, n_shots, ny, nx, n_sources_per_shot, n_receivers_per_shot, step_ratio,        \
+        storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad, cb_requires_grad,  \
+        ca_batched, cb_batched, cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1,          \
+        n_threads, device, compute_stream, storage_stream);                            \
+  }                                                                                    \
+  extern "C" void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T)) { \
+    tb::tm_born_backward<T, S>(                                                        \
+        ca, cb, cq, grad_r, lambda_ey, lambda_hx, lambda_hz, m_lambda_ey_x, m_lambda_ey_z,    \
+        m_lambda_hx_z, m_lambda_hz_x, ey_store_1, ey_store_3, ey_filenames, curl_store_1,     \
+        curl_store_3, curl_filenames, grad_f, grad_ca, grad_cb, grad_ca_shot, grad_cb_shot,   \
+        work_x, work_z, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, sources_i,      \
+        receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,                   \
+        n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
+        ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,      \
+        pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);  \
   }
 
 TB_BORN_DEFINE(2, float)

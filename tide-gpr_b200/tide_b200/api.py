@@ -346,8 +346,11 @@ class LinearizedMaxwellTM:
 
         op = self.operator
         d, e = op.discretization, op.experiment
+        # the background enters as values (no history is kept for it); a
+        # direction that requires grad is differentiated through the Born pass
         res = borntm(
-            self.model.epsilon, self.model.sigma, self.model.mu, grid_spacing=d.spacing,
+            self.model.epsilon.detach(), self.model.sigma.detach(), self.model.mu.detach(),
+            grid_spacing=d.spacing,
             dt=d.dt, source_amplitude=e.source_amplitude,
             source_location=e.acquisition.source_location,
             receiver_location=e.acquisition.receiver_location,

@@ -430,13 +430,14 @@ class _AdjointState:
     """Adjoint fields, scratch and gradient accumulators of one backward pass
     (kept across the calls of a chunked or checkpointed backward)."""
 
-    def __init__(self, pb, need_ca, need_cb):
+    def __init__(self, pb, need_ca, need_cb, scratch=True):
         device, dtype = pb.device, pb.dtype
         S, ny, nx, nt = pb.n_shots, pb.ny, pb.nx, pb.nt
         shape = (S, ny, nx)
         z = lambda: torch.zeros(shape, device=device, dtype=dtype)  # noqa: E731
         self.lam = [z() for _ in range(7)]
-        self.scratch = torch.empty((4, S, ny, nx), device=device, dtype=dtype)
+        self.scratch = (torch.empty((4, S, ny, nx), device=device, dtype=dtype) if scratch
+                        else None)
         self.grad_f = (
             torch.zeros((nt, S, pb.n_src), device=device, dtype=dtype)
             if pb.n_src > 0
