@@ -196,10 +196,37 @@ TIDE_TM_DECLARE(8, double)
       int64_t n_threads, int64_t device, void *compute_stream,                 \
       void *storage_stream
 
+/* maxwell_tm_*_born_tangent_forward_with_storage_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1974-2086 (argtypes
+ * src/tide/backend_utils.py:372-384).  Advances only the scattered state,
+ * reading the background Ey^n / curl H^n of each step from a stored device
+ * history [nt, background_n_shots, ny, nx] (snapshot type of
+ * storage_format) instead of recomputing the background; scattered shot s
+ * uses background shot s % background_n_shots (direction batches).
+ * step_ratio must be 1.  r records the scattered Ey; dey_store /
+ * dcurl_store (may be null) receive the scattered history
+ * [nt, n_shots, ny, nx]. */
+#define TIDE_TM_BORN_TANGENT_ARGS(T)                                           \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *df, T *dey, T *dhx, T *dhz, T *dm_ey_x, T *dm_ey_z,             \
+      T *dm_hx_z, T *dm_hz_x, T *r, void const *ey_store,                      \
+      void const *curl_store, void *dey_store, void *dcurl_store, T const *ay, \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *ky, T const *kyh, T const *kx,      \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_format, int64_t background_n_shots,  \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream
+
 #define TIDE_TM_BORN_DECLARE(S, T)                                             \
   void maxwell_tm_##S##_##T##_born_forward_cuda(TIDE_TM_BORN_FORWARD_ARGS(T)); \
   void maxwell_tm_##S##_##T##_born_forward_with_storage_cuda(                  \
       TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T));                              \
+  void maxwell_tm_##S##_##T##_born_tangent_forward_with_storage_cuda(          \
+      TIDE_TM_BORN_TANGENT_ARGS(T));                                           \
   void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T));
 
 TIDE_TM_BORN_DECLARE(2, float)

@@ -234,3 +234,77 @@ def test_borntm_unbuilt_parts_raise(cuda_device):
         (r * c["w"]).sum().backward()
     with pytest.raises(NotImplementedError, match="checkpoint"):
         _borntm(c, deps, c["dsig"], storage_mode="checkpoint")
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_jvp_from_kept_history_equals_born_pass(cuda_device, dtype, stencil):
+    """MaxwellTM.linearize(...).jvp reads the primal's device history
+    (born_tangent_forward_with_storage) instead of recomputing the
+    background: bit-identical to the full Born pass."""
+    c = _case(cuda_device, dtype=dtype, stencil=stencil)
+    op = tide.MaxwellTM(tide.Discretization(c["dx"], c["dt"], stencil=stencil,
+                                            boundary=tide.CPML(8)),
+                        tide.Experiment(tide.Acquisition(c["src"], c["rec"]), c["amp"]))
+    lin = op.linearize(tide.EMModel(c["eps"], c["sig"], c["mu"]))
+    v = tide.EMDirection(c["deps"], c["dsig"])
+    fast = lin._jvp_from_history(v)
+    assert fast is not None
+    with torch.no_grad():
+        full = _borntm(c, c["deps"], c["dsig"])
+    assert torch.equal(fast.receiver_data, full[-1])
+    assert torch.equal(lin.jvp(v).receiver_data, full[-1])
+    st = fast.final_state
+    for a, b in zip((st.Ey, st.Hx, st.Hz, st.m_Ey_x, st.m_Ey_z, st.m_Hx_z, st.m_Hz_x),
+                    full[7:14]):
+        assert torch.equal(a, b)
+
+
+def test_tangent_pass_direction_batches(cuda_device):
+    """n_shots = directions x background shots: scattered shot s reads
+    background shot s % background_n_shots; each direction block equals a
+    separate tangent pass."""
+    from tide_b200 import _native as nat
+    from tide_b200.tm2d import _PROFILE_ORDER
+
+    dev = cuda_device
+    pb = random_problem(871, 29, 41, 2, 36, pml=6, dtype=torch.float64)
+    q = clone_problem(pb, dev)
+    snaps = _history(q, 0, torch.float64, pb.nt)
+    d = _perturbation(pb, 11, dev)
+    _born(q, d, snaps)
+    S, n_dir = pb.n_shots, 3
+    g = torch.Generator().manual_seed(12)
+    dirs = [(1e-3 * torch.randn((1, pb.ny, pb.nx), generator=g, dtype=torch.float64)).to(dev)
+            for _ in range(n_dir)]
+
+    def tangent(dca, dcb, shots, bg_shots, src_i, rec_i, df):
+        tan = [torch.zeros((shots, pb.ny, pb.nx), device=dev, dtype=pb.dtype) for _ in range(7)]
+        r = torch.zeros((pb.nt, shots, pb.n_rec), device=dev, dtype=pb.dtype)
+        batched = dca.shape[0] > 1
+        ca = q.ca.expand(shots, -1, -1).contiguous() if batched else q.ca
+        cb = q.cb.expand(shots, -1, -1).contiguous() if batched else q.cb
+        cq = q.cq.expand(shots, -1, -1).contiguous() if batched else q.cq
+        fn = nat.get_backend_function("maxwell_tm", "born_tangent_forward_with_storage", 2,
+                                      pb.dtype, dev)
+        fn(nat.ptr(ca), nat.ptr(cb), nat.ptr(cq), nat.ptr(dca), nat.ptr(dcb), nat.ptr(df),
+           *[nat.ptr(t) for t in tan], nat.ptr(r), nat.ptr(snaps.ey_dev), nat.ptr(snaps.curl_dev),
+           0, 0, *[nat.ptr(q.profiles[n]) for n in _PROFILE_ORDER], nat.ptr(src_i),
+           nat.ptr(rec_i), q.rdy, q.rdx, q.dt, pb.nt, shots, q.ny, q.nx, q.n_src, q.n_rec, 1, 0,
+           bg_shots, batched, batched, batched, 0, q.pml_y0, q.pml_x0, q.pml_y1, q.pml_x1, 0,
+           dev.index or 0, torch.cuda.current_stream(dev).cuda_stream)
+        nat.check("born_tangent_forward_with_storage")
+        torch.cuda.synchronize()
+        return r, tan
+
+    df0 = torch.zeros(pb.nt * S * pb.n_src, device=dev, dtype=pb.dtype)
+    singles = [tangent(dv, 0.5 * dv, S, S, q.sources_i, q.receivers_i, df0) for dv in dirs]
+    dca = torch.cat([dv.expand(S, -1, -1) for dv in dirs]).contiguous()
+    src_i = q.sources_i.repeat(n_dir, 1).contiguous()
+    rec_i = q.receivers_i.repeat(n_dir, 1).contiguous()
+    dfb = torch.zeros(pb.nt * S * n_dir * pb.n_src, device=dev, dtype=pb.dtype)
+    rb, tb = tangent(dca, (0.5 * dca).contiguous(), S * n_dir, S, src_i, rec_i, dfb)
+    for k, (r1, t1) in enumerate(singles):
+        assert torch.equal(rb[:, k * S:(k + 1) * S], r1)
+        assert torch.equal(tb[0][k * S:(k + 1) * S], t1[0])
+    assert float(rb.abs().max()) > 0

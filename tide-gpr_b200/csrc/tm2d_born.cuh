@@ -99,6 +99,67 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
   }
 }
 
+// Scattered E half-step from a stored background history
+// (maxwell_tm_core.cuh:691-743): Ey^n and curl H^n of background shot
+// s % bg_shots are read from this step's slots e_bg / c_bg (type S) instead
+// of being recomputed; then the scattered sources and receivers.
+template <typename T, int ST, typename S, int R>
+__global__ void __launch_bounds__(256)
+k_born_tangent_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
+                 const T *__restrict__ dca, const T *__restrict__ dcb,
+                 const T *__restrict__ dhx, const T *__restrict__ dhz, T *__restrict__ dey,
+                 T *__restrict__ dm_hx_z, T *__restrict__ dm_hz_x, const S *__restrict__ e_bg,
+                 const S *__restrict__ c_bg, int bg_shots, PointCSR src, PointCSR rec,
+                 const T *__restrict__ df_t, T *__restrict__ r_t, S *__restrict__ des,
+                 S *__restrict__ dcs) {
+  constexpr int P = FD<ST>::P;
+  const int x = blockIdx.x * kTileX + threadIdx.x;
+  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
+  const int s = blockIdx.z;
+  const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const bool pts = !point_tile_empty(src, rec, tile);
+  if (x >= g.nx || y0 >= g.ny) return;
+  const int64_t base = (int64_t)s * g.N, bg_base = (int64_t)(s % bg_shots) * g.N;
+  const bool xdom = x >= P && x < g.nx - P + 1;
+  const bool px = x < g.pml_x0 || x >= g.pml_x1;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = y0 + r;
+    if (y >= g.ny) break;
+    const bool dom = xdom && y >= P && y < g.ny - P + 1;
+    if (!dom && !pts) continue;
+    const int64_t j = (int64_t)y * g.nx + x, i = base + j;
+    T de = dey[i];
+    if (dom) {
+      const T cav = g.ca_b ? ldg(ca + i) : ldg(ca + j);
+      const T cbv = g.cb_b ? ldg(cb + i) : ldg(cb + j);
+      const T dcav = g.ca_b ? ldg(dca + i) : ldg(dca + j);
+      const T dcbv = g.cb_b ? ldg(dcb + i) : ldg(dcb + j);
+      T ddz = d_x1<T, ST>(dhz, i, g.rdx), ddy = d_y1<T, ST>(dhx, i, g.nx, g.rdy);
+      if (px) {
+        const T dm = ldg(g.bx + x) * dm_hz_x[i] + ldg(g.ax + x) * ddz;
+        dm_hz_x[i] = dm;
+        ddz = ddz / ldg(g.kx + x) + dm;
+      }
+      if (y < g.pml_y0 || y >= g.pml_y1) {
+        const T dm = ldg(g.by + y) * dm_hx_z[i] + ldg(g.ay + y) * ddy;
+        dm_hx_z[i] = dm;
+        ddy = ddy / ldg(g.ky + y) + dm;
+      }
+      const T dcurl = ddz - ddy;
+      const T de_n = de;
+      const T e_n = Codec<S, T>::dec(e_bg[bg_base + j]);
+      const T curl = Codec<S, T>::dec(c_bg[bg_base + j]);
+      if (des) store_stream(des + i, Codec<S, T>::enc(de_n));
+      if (dcs) store_stream(dcs + i, Codec<S, T>::enc(dcurl));
+      de = cav * de_n + cbv * dcurl + dcav * e_n + dcbv * curl;
+    }
+    if (pts) de = point_accumulate(src, tile, (int)j, df_t, de);
+    dey[i] = de;
+    if (pts) point_record(rec, tile, (int)j, r_t, de);
+  }
+}
+
 template <typename T, int ST>
 void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads;
@@ -196,6 +257,65 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
   sr.finish();
 }
 
+// Tangent (scattered-only) propagation from a stored device background
+// history (cu_inst:1974-2086): step ratio 1, the history slot of step t at
+// t * background_n_shots * ny * nx elements, scattered shot s reading
+// background shot s % background_n_shots (direction batches).
+template <typename T, int ST>
+void tm_born_tangent_forward_with_storage(TIDE_TM_BORN_TANGENT_ARGS(T)) {
+  (void)dt; (void)n_threads;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(step_ratio == 1,
+             "TM2D born_tangent_forward_with_storage requires step_ratio=1, got %lld",
+             (long long)step_ratio);
+  TB_REQUIRE(nt >= 0 && start_t >= 0, "TM2D born_tangent_forward_with_storage: bad nt/start_t");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && dey && dhx && dhz && dm_ey_x && dm_ey_z &&
+                 dm_hx_z && dm_hz_x && ey_store && curl_store,
+             "TM2D born_tangent_forward_with_storage: a field, history or coefficient pointer "
+             "is null");
+  TB_REQUIRE(background_n_shots >= 1 && n_shots % background_n_shots == 0,
+             "TM2D born_tangent_forward_with_storage: n_shots=%lld is not a multiple of "
+             "background_n_shots=%lld", (long long)n_shots, (long long)background_n_shots);
+  TB_REQUIRE(n_sources_per_shot == 0 || df,
+             "TM2D born_tangent_forward_with_storage: sources without amplitudes");
+  TB_REQUIRE(n_receivers_per_shot == 0 || r,
+             "TM2D born_tangent_forward_with_storage: receivers without output");
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  cudaStream_t st = as_stream(compute_stream);
+  PointScratch ps;
+  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+                    sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
+    return;
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  const int64_t bg_step = background_n_shots * ny * nx, sc_step = n_shots * ny * nx;
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    if (L.has_domain) launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+    const T *dft = df ? df + t * fs : nullptr;
+    T *rt = r ? r + t * rs : nullptr;
+    if (bf16) {
+      using B = __nv_bfloat16;
+      k_born_tangent_e<T, ST, B, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x, (const B *)ey_store + t * bg_step,
+          (const B *)curl_store + t * bg_step, (int)background_n_shots, ps.src, ps.rec, dft, rt,
+          dey_store ? (B *)dey_store + t * sc_step : nullptr,
+          dcurl_store ? (B *)dcurl_store + t * sc_step : nullptr);
+    } else {
+      k_born_tangent_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x, (const T *)ey_store + t * bg_step,
+          (const T *)curl_store + t * bg_step, (int)background_n_shots, ps.src, ps.rec, dft, rt,
+          dey_store ? (T *)dey_store + t * sc_step : nullptr,
+          dcurl_store ? (T *)dcurl_store + t * sc_step : nullptr);
+    }
+  }
+  count_launches(nt * (L.has_domain ? 2 : 1));
+  TB_CUDA(cudaGetLastError());
+}
+
 // The CPML adjoint ping-pong buffers backward takes as adjoint_memory_scratch
 // are allocated here in stream order (4 x n_shots x ny x nx).
 template <typename T, int ST>
@@ -243,6 +363,16 @@ void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
         storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad, cb_requires_grad,  \
         ca_batched, cb_batched, cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1,          \
         n_threads, device, compute_stream, storage_stream);                            \
+  }                                                                                    \
+  extern "C" void maxwell_tm_##S##_##T##_born_tangent_forward_with_storage_cuda(      \
+      TIDE_TM_BORN_TANGENT_ARGS(T)) {                                                  \
+    tb::tm_born_tangent_forward_with_storage<T, S>(                                    \
+        ca, cb, cq, dca, dcb, df, dey, dhx, dhz, dm_ey_x, dm_ey_z, dm_hx_z, dm_hz_x, r,       \
+        ey_store, curl_store, dey_store, dcurl_store, ay, by, ayh, byh, ax, bx, axh, bxh, ky, \
+        kyh, kx, kxh, sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx,              \
+        n_sources_per_shot, n_receivers_per_shot, step_ratio, storage_format,                 \
+        background_n_shots, ca_batched, cb_batched, cq_batched, start_t, pml_y0, pml_x0,      \
+        pml_y1, pml_x1, n_threads, device, compute_stream);                            \
   }                                                                                    \
   extern "C" void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T)) { \
     tb::tm_born_backward<T, S>(                                                        \

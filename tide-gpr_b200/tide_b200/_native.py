@@ -56,6 +56,11 @@ SPECS: dict[str, list] = {
         (_P, 3), (_P, 2), (_P, 2), (_P, 3), (_P, 4), (_P, 3), (_P, 4), (_P, 2), (_P, 8),
         *_TM_PROFILES, *_TM_TAIL, *_TM_STORAGE, *_TM_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:372-384
+    "maxwell_tm_born_tangent_forward_with_storage": [
+        (_P, 3), (_P, 2), (_P, 1), (_P, 7), (_P, 5), *_TM_PROFILES, *_TM_TAIL, (_I, 1), (_I, 1),
+        *_TM_FLAGS, (_P, 1),
+    ],
     # src/tide/backend_utils.py:386-405
     "maxwell_tm_born_backward": [
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 6), (_P, 1), (_P, 2), (_P, 2), (_P, 2),
@@ -201,7 +206,8 @@ def exported_symbols() -> list[str]:
         symbol_name("maxwell_tm", p, a, d)
         for a in ACCURACIES
         for d in ("float", "double")
-        for p in ("born_forward", "born_forward_with_storage", "born_backward")
+        for p in ("born_forward", "born_forward_with_storage",
+                  "born_tangent_forward_with_storage", "born_backward")
     ] + [
         symbol_name("maxwell_3d", "born_forward", a, d)
         for a in ACCURACIES_3D

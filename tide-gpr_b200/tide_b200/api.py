@@ -15,6 +15,7 @@ from typing import Literal
 
 import torch
 
+from . import _native as nat
 from . import physics as ph
 from .storage import StorageOptions
 from .tm2d import Callback, maxwelltm
@@ -342,6 +343,9 @@ class LinearizedMaxwellTM:
         direction.validate_for(self.model)
         if direction.mu is not None:
             raise NotImplementedError("TM2D tangent propagation for mu is not available.")
+        fast = self._jvp_from_history(direction)
+        if fast is not None:
+            return fast
         from .born import borntm
 
         op = self.operator
@@ -360,6 +364,50 @@ class LinearizedMaxwellTM:
             model_gradient_sampling_interval=op.model_gradient_sampling_interval,
         )
         return TangentResult(res[-1], TMState.from_tensors(res[7:14]))
+
+    def _jvp_from_history(self, direction: EMDirection) -> TangentResult | None:
+        """The jvp from the primal's kept background history (the reference's
+        reusable linearization background, tm2d_born_autograd.py:134-259):
+        only the scattered state advances, reading Ey^n and curl H^n of each
+        step from the history (born_tangent_forward_with_storage).  Applies
+        when that history is a FULL-format device history at sampling
+        interval 1 without sub-stepping and the direction needs no gradient;
+        the result is then bit-identical to the full Born pass.  None
+        otherwise."""
+        from . import storage as stg
+        from .born import prepare_born
+        from .tm2d import _PROFILE_ORDER, _stream_handle
+
+        node = self._result.receiver_data.grad_fn
+        if type(node).__name__ != "TMPropagateBackward":
+            return None
+        snaps, pb = getattr(node, "snaps", None), getattr(node, "pb", None)
+        if (snaps is None or pb is None or snaps.mode != stg.STORAGE_DEVICE or snaps.fmt != 0
+                or pb.grad_interval != 1 or pb.batched or pb.debye is not None
+                or snaps.ey_dev.numel() == 0 or snaps.curl_dev.numel() == 0):
+            return None
+        if torch.is_grad_enabled() and any(
+                t is not None and t.requires_grad for t in (direction.epsilon, direction.sigma)):
+            return None
+        d, e = self.operator.discretization, self.operator.experiment
+        with torch.no_grad():
+            dca, dcb, df = prepare_born(pb, 1, d.spacing, e.source_amplitude,
+                                        depsilon=direction.epsilon, dsigma=direction.sigma)
+            S = pb.n_shots
+            tan = [torch.zeros((S, pb.ny, pb.nx), device=pb.device, dtype=pb.dtype)
+                   for _ in range(7)]
+            r = torch.zeros((pb.nt, S, pb.n_rec), device=pb.device, dtype=pb.dtype)
+            fn = nat.get_backend_function("maxwell_tm", "born_tangent_forward_with_storage",
+                                          pb.stencil, pb.dtype, pb.device)
+            fn(nat.ptr(pb.ca), nat.ptr(pb.cb), nat.ptr(pb.cq), nat.ptr(dca), nat.ptr(dcb),
+               nat.ptr(df), *[nat.ptr(t) for t in tan], nat.ptr(r), nat.ptr(snaps.ey_dev),
+               nat.ptr(snaps.curl_dev), 0, 0, *[nat.ptr(pb.profiles[n]) for n in _PROFILE_ORDER],
+               nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i), pb.rdy, pb.rdx, pb.dt, pb.nt, S,
+               pb.ny, pb.nx, pb.n_src if df.numel() else 0, pb.n_rec, 1, 0, S, False, False,
+               False, 0, pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, pb.device.index or 0,
+               _stream_handle(pb.device))
+            nat.check("maxwell_tm born_tangent_forward_with_storage")
+        return TangentResult(r, TMState.from_tensors([pb.crop(t) for t in tan]))
 
     def second_vjp(self, direction: EMDirection, cotangent: torch.Tensor) -> EMGradient:
         """Gradient of <cotangent, J(model) direction> with respect to the
