@@ -288,7 +288,7 @@ void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
  * src/tide/backend_utils.py:506-524).  Stores E^t (3 components) and the
  * CPML-corrected curl H (3 components) at steps t % step_ratio == 0; each
  * component has a device buffer (s1), a pinned host history (s3, cpu mode)
- * and a file-name list (fn, disk mode: rejected on the 3-D path). */
+ * and a file-name list (fn, disk mode: one file name, char **). */
 #define TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)                                   \
   T const *ca, T const *cb, T const *cq, T const *f, T *ex, T *ey, T *ez,      \
       T *hx, T *hy, T *hz, T *m_hz_y, T *m_hy_z, T *m_hx_z, T *m_hz_x,         \

@@ -200,5 +200,24 @@ def test_unbuilt_options_raise(cuda_device):
     c = _case(3, 6, 6, 6, 1, 5)
     with pytest.raises(NotImplementedError):
         _run(c, cuda_device, grads=False, forward_callback=lambda s: None)
-    with pytest.raises(NotImplementedError):
-        _run(c, cuda_device, grads=True, storage_mode="disk")
+
+
+@pytest.mark.parametrize("mode", ["cpu", "disk"])
+@pytest.mark.parametrize("dtype,shots,k,compression", [
+    (torch.float64, 2, 1, False), (torch.float32, 3, 2, False), (torch.float32, 1, 1, "bf16"),
+])
+def test_3d_host_and_disk_storage_equal_device(cuda_device, tmp_path, mode, dtype, shots, k,
+                                               compression):
+    """cpu (pinned host history, copies on a storage stream) and disk (one
+    file per snapshot kind through a pinned staging ring) give the device
+    mode's receivers and gradients bit for bit; the files are removed."""
+    c = _case(21 + shots, 9, 10, 11, shots, 37, dtype=dtype)
+    kw = dict(model_gradient_sampling_interval=k, storage_compression=compression)
+    ref = _run(c, cuda_device, storage_mode="device", **kw)
+    got = _run(c, cuda_device, storage_mode=mode, storage_path=str(tmp_path), **kw)
+    assert torch.equal(ref[0], got[0])
+    assert torch.equal(ref[2], got[2]) and torch.equal(ref[3], got[3])
+    import gc
+
+    gc.collect()
+    assert list(tmp_path.iterdir()) == []

@@ -28,12 +28,12 @@
 
 #include "../../include/tide_b200.h"
 #include "tb_common.cuh"
+#include "tb_store.cuh"
 
 namespace tb {
 namespace {
 
 constexpr int kZRun = 16;
-constexpr int kRing3 = 3;  // device ring slots of the cpu storage mode (NUM_BUFFERS)
 
 enum { PAZ, PBZ, PAZH, PBZH, PAY, PBY, PAYH, PBYH, PAX, PBX, PAXH, PBXH,
        PKZ, PKZH, PKY, PKYH, PKX, PKXH, kNProf };
@@ -1074,59 +1074,43 @@ void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
 
 template <typename T>
 void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
-  (void)dt; (void)n_threads; (void)ex_fn; (void)ey_fn; (void)ez_fn; (void)cx_fn; (void)cy_fn;
-  (void)cz_fn;
+  (void)dt; (void)n_threads;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
   TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D forward_with_storage: bad nt/step_ratio");
   TB_REQUIRE(ca && cb && cq && ex && ey && ez && hx && hy && hz,
              "3-D forward_with_storage: a field or coefficient pointer is null");
-  TB_REQUIRE(storage_mode != 2,
-             "3-D forward_with_storage: disk storage mode is not built in this library");
-  TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "3-D: unknown storage_mode %lld",
-             (long long)storage_mode);
   T *M[12] = {m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x, m_hx_y,
               m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x};
   for (T *m : M) TB_REQUIRE(m != nullptr, "3-D forward_with_storage: a CPML memory is null");
   if (!common_checks("3-D forward_with_storage", n_sources_per_shot, f, n_receivers_per_shot,
                      r, source_component, receiver_component, execution_backend))
     return;
-  const bool bf16 = storage_format == 1;
-  TB_REQUIRE(!bf16 || sizeof(T) == 4, "3-D: bf16 snapshot storage requires float32 fields");
-  const size_t esz = bf16 ? 2 : sizeof(T);
-  const bool want = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
-  void *s1[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};
-  void *s3[6] = {ex_s3, ey_s3, ez_s3, cx_s3, cy_s3, cz_s3};
-  const bool need[6] = {ca_requires_grad, ca_requires_grad, ca_requires_grad,
-                        cb_requires_grad, cb_requires_grad, cb_requires_grad};
-  if (want) {
-    TB_REQUIRE(shot_bytes_uncomp == nz * ny * nx * (int64_t)esz,
-               "3-D: shot_bytes_uncomp=%lld does not match nz*ny*nx*elem=%lld",
-               (long long)shot_bytes_uncomp, (long long)(nz * ny * nx * (int64_t)esz));
-    for (int c = 0; c < 6; ++c) {
-      TB_REQUIRE(!need[c] || s1[c], "3-D: snapshot buffer %d missing", c);
-      TB_REQUIRE(!need[c] || storage_mode != 1 || s3[c],
-                 "3-D: cpu storage mode needs host snapshot buffer %d", c);
-    }
+  cudaStream_t st = stream_of(compute_stream);
+  StoreRun<6> sr;
+  {
+    void *const s1[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};
+    void *const s3[6] = {ex_s3, ey_s3, ez_s3, cx_s3, cy_s3, cz_s3};
+    char const *const *const fn[6] = {
+        (char const *const *)ex_fn, (char const *const *)ey_fn, (char const *const *)ez_fn,
+        (char const *const *)cx_fn, (char const *const *)cy_fn, (char const *const *)cz_fn};
+    const bool need[6] = {ca_requires_grad, ca_requires_grad, ca_requires_grad,
+                          cb_requires_grad, cb_requires_grad, cb_requires_grad};
+    if (!sr.init("3-D", need, storage_mode, storage_format, sizeof(T), shot_bytes_uncomp,
+                 nz * ny * nx, n_shots, step_ratio, s1, s3, fn, st, stream_of(storage_stream)))
+      return;
   }
+  const bool bf16 = sr.bf16;
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
   if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
              pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
-  cudaStream_t st = stream_of(compute_stream);
   T *F[6] = {ex, ey, ez, hx, hy, hz};
-  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   for (int64_t t = start_t; t < start_t + nt; ++t) {
-    const bool store = want && (t % step_ratio) == 0;
-    const int64_t q = t / step_ratio;
-    char *dst[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    if (store)
-      for (int c = 0; c < 6; ++c)
-        if (need[c])
-          dst[c] = (char *)s1[c] +
-                   (storage_mode == 0 ? (size_t)q : (size_t)(q % kRing3)) * step_bytes;
+    char *dst[6];
+    if (!sr.begin(t, dst)) return;
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
     if (bf16) {
@@ -1143,20 +1127,15 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
                             source_component, rt, receivers_i, n_receivers_per_shot,
                             receiver_component);
     }
-    if (store && storage_mode == 1)  // ordered on the compute stream: the ring slot is reused
-      for (int c = 0; c < 6; ++c)
-        if (dst[c] && TB_CUDA(cudaMemcpyAsync((char *)s3[c] + (size_t)q * step_bytes, dst[c],
-                                              step_bytes, cudaMemcpyDeviceToHost, st)))
-          return;
+    if (!sr.end(t, dst)) return;
   }
-  (void)storage_stream;
   if (TB_CUDA(cudaGetLastError())) return;
-  if (want && storage_mode == 1) TB_CUDA(cudaStreamSynchronize(st));
+  sr.finish();
 }
 
 template <typename T>
 void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
-  (void)n_threads; (void)ex_fn; (void)ey_fn; (void)ez_fn; (void)cx_fn; (void)cy_fn; (void)cz_fn;
+  (void)n_threads;
   (void)storage_stream;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
   TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D backward: bad nt/step_ratio");
@@ -1164,7 +1143,6 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   TB_REQUIRE(ca && cb && cq && lambda_ex && lambda_ey && lambda_ez && lambda_hx && lambda_hy &&
                  lambda_hz && adjoint_memory_scratch,
              "3-D backward: a field, coefficient or scratch pointer is null");
-  TB_REQUIRE(storage_mode != 2, "3-D backward: disk storage mode is not built in this library");
   TB_REQUIRE(storage_mode >= 0 && storage_mode <= 3, "3-D: unknown storage_mode %lld",
              (long long)storage_mode);
   T *lm[12] = {m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,
@@ -1186,11 +1164,34 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
     TB_REQUIRE(shot_bytes_uncomp == nz * ny * nx * (int64_t)esz,
                "3-D: shot_bytes_uncomp=%lld does not match nz*ny*nx*elem=%lld",
                (long long)shot_bytes_uncomp, (long long)(nz * ny * nx * (int64_t)esz));
+    void *const fnp[6] = {ex_fn, ey_fn, ez_fn, cx_fn, cy_fn, cz_fn};
     for (int c = 0; c < 6; ++c) {
       TB_REQUIRE(!need[c] || s1[c], "3-D backward: snapshot buffer %d missing", c);
-      TB_REQUIRE(!need[c] || storage_mode != 1 || s3[c],
-                 "3-D backward: cpu storage mode needs host snapshot buffer %d", c);
+      TB_REQUIRE(!need[c] || (storage_mode != 1 && storage_mode != 2) || s3[c],
+                 "3-D backward: cpu / disk storage modes need host snapshot buffer %d", c);
+      TB_REQUIRE(!need[c] || storage_mode != 2 ||
+                     (fnp[c] && ((char const *const *)fnp[c])[0]),
+                 "3-D backward: disk storage mode needs snapshot file names");
     }
+  }
+  // disk mode: one reader per snapshot kind into the pinned staging ring (s3)
+  std::unique_ptr<DiskHistory> disk[6];
+  EventRing staged;  // the staging slot's host-to-device copy has completed
+  bool staged_used[kStoreRing] = {false, false, false};
+  if ((need_ca || need_cb) && storage_mode == 2) {
+    if (!staged.ok) {
+      set_error(kCudaError, "3-D: event creation failed");
+      return;
+    }
+    void *const fnp[6] = {ex_fn, ey_fn, ez_fn, cx_fn, cy_fn, cz_fn};
+    for (int c = 0; c < 6; ++c)
+      if (need[c]) {
+        disk[c].reset(new DiskHistory(((char const *const *)fnp[c])[0], false, kStoreRing));
+        if (!disk[c]->ok()) {
+          set_error(kBadArgument, "3-D disk storage: %s", disk[c]->error().c_str());
+          return;
+        }
+      }
   }
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
@@ -1255,19 +1256,38 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
     }
     if ((need_ca || need_cb) && (t % step_ratio) == 0) {
       const int64_t q = t / step_ratio;
+      const int ring = (int)(q % kStoreRing);
       const char *src[6];
+      if (storage_mode == 2 && staged_used[ring]) {
+        // the staging slot is rewritten below: its previous copy must be done
+        if (TB_CUDA(cudaEventSynchronize(staged.ev[ring]))) return;
+      }
       for (int c = 0; c < 6; ++c) {
         src[c] = nullptr;
         if (!need[c]) continue;
-        if (storage_mode == 1) {  // bring the host history back through a ring slot
-          char *slot = (char *)s1[c] + (size_t)(q % kRing3) * step_bytes;
-          if (TB_CUDA(cudaMemcpyAsync(slot, (const char *)s3[c] + (size_t)q * step_bytes,
-                                      step_bytes, cudaMemcpyHostToDevice, st)))
+        if (storage_mode == 1 || storage_mode == 2) {
+          // bring the host (cpu) or file (disk, through a staging slot)
+          // history back through a device ring slot
+          char *slot = (char *)s1[c] + (size_t)ring * step_bytes;
+          const char *host = (const char *)s3[c] + (size_t)q * step_bytes;
+          if (storage_mode == 2) {
+            char *stage = (char *)s3[c] + (size_t)ring * step_bytes;
+            if (!disk[c]->read(stage, step_bytes, (int64_t)(q * step_bytes))) {
+              set_error(kCudaError, "3-D disk storage: %s", disk[c]->error().c_str());
+              return;
+            }
+            host = stage;
+          }
+          if (TB_CUDA(cudaMemcpyAsync(slot, host, step_bytes, cudaMemcpyHostToDevice, st)))
             return;
           src[c] = slot;
         } else {
           src[c] = (const char *)s1[c] + (size_t)q * step_bytes;
         }
+      }
+      if (storage_mode == 2) {
+        if (TB_CUDA(cudaEventRecord(staged.ev[ring], st))) return;
+        staged_used[ring] = true;
       }
       const T ks = (T)step_ratio;
       if (bf16)
@@ -1309,7 +1329,8 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   }
   count_launches(launches);
   if (TB_CUDA(cudaGetLastError())) return;
-  if ((need_ca || need_cb) && storage_mode == 1) TB_CUDA(cudaStreamSynchronize(st));
+  if ((need_ca || need_cb) && (storage_mode == 1 || storage_mode == 2))
+    TB_CUDA(cudaStreamSynchronize(st));
 }
 
 template <typename T>

@@ -21,13 +21,12 @@
 #include "tm2d_kernels.cuh"
 #include "tm2d_fused.cuh"
 #include "tm2d_s2.cuh"
-#include "tb_disk.cuh"
+#include "tb_store.cuh"
 
 namespace tb {
 namespace {
 
-constexpr int kRing = 3;  // device ring slots of the cpu storage mode
-                          // (NUM_BUFFERS, maxwell.cu:45-47)
+constexpr int kRing = kStoreRing;  // device ring slots of the cpu / disk storage modes
 
 inline cudaStream_t as_stream(void *h) { return reinterpret_cast<cudaStream_t>(h); }
 
@@ -196,18 +195,6 @@ bool build_points(PointScratch &ps, const Launch<T, ST> &L, const PointTiles &pt
   return !TB_CUDA(cudaGetLastError());
 }
 
-struct EventRing {
-  cudaEvent_t ev[kRing]{};
-  bool ok = true;
-  EventRing() {
-    for (auto &e : ev)
-      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) ok = false;
-  }
-  ~EventRing() {
-    for (auto e : ev)
-      if (e) cudaEventDestroy(e);
-  }
-};
 
 // ---------------------------------------------------------------------------
 // Stencil order 2 runs the single-path kernels of tm2d_s2.cuh (Debye media use
@@ -434,149 +421,6 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
 }
 
 // ---------------------------------------------------------------------------
-// ---------------------------------------------------------------------------
-// Snapshot history of a storing forward pass, shared by the plain and the Born
-// storing forwards (cu_inst:1281-1609 and 1701-2086 run the same pipeline).
-// Storage modes: 0 device (the whole history in *_store_1), 1 cpu (3-slot
-// device ring in *_store_1, pinned host history in *_store_3), 2 disk (device
-// ring, 3-slot pinned staging ring in *_store_3, one file per snapshot kind
-// written by a DiskHistory thread), 3 none.  Store index q = t / step_ratio
-// sits at q * step_bytes of its history (device, host or file).
-struct StoreRun {
-  bool want = false, bf16 = false, host_side = false, pipeline = false, to_disk = false;
-  int64_t mode = 3, step_ratio = 1;
-  size_t step_bytes = 0;
-  char *e1 = nullptr, *c1 = nullptr, *e3 = nullptr, *c3 = nullptr;
-  cudaStream_t st = nullptr, ss = nullptr;
-  std::unique_ptr<DiskHistory> disk[2];
-  EventRing staged;                     // a staging slot's device-to-host copy is done
-  EventRing store_done, compute_done;   // cpu/disk pipeline on the storage stream
-
-  // Validates the storage arguments; false (with the error set) on bad ones.
-  bool init(bool store_ey, bool store_curl, int64_t storage_mode, int64_t storage_format,
-            size_t field_size, int64_t shot_bytes_uncomp, int64_t ny, int64_t nx,
-            int64_t n_shots, int64_t ratio, void *ey_store_1, void *ey_store_3,
-            char const *const *ey_filenames, void *curl_store_1, void *curl_store_3,
-            char const *const *curl_filenames, cudaStream_t compute, cudaStream_t storage) {
-    TB_REQUIRE_B(storage_mode >= 0 && storage_mode <= 3, "TM2D: unknown storage_mode %lld",
-                 (long long)storage_mode);
-    bf16 = storage_format == 1;
-    TB_REQUIRE_B(!bf16 || field_size == 4, "TM2D: bf16 snapshot storage requires float32 fields");
-    want = (store_ey || store_curl) && storage_mode != 3;
-    mode = storage_mode;
-    step_ratio = ratio;
-    st = compute;
-    ss = storage;
-    if (!want) return true;
-    const size_t esz = bf16 ? 2 : field_size;
-    TB_REQUIRE_B(shot_bytes_uncomp == ny * nx * (int64_t)esz,
-                 "TM2D: shot_bytes_uncomp=%lld does not match ny*nx*elem=%lld",
-                 (long long)shot_bytes_uncomp, (long long)(ny * nx * (int64_t)esz));
-    TB_REQUIRE_B((!store_ey || ey_store_1) && (!store_curl || curl_store_1),
-                 "TM2D: snapshot buffers missing");
-    host_side = mode == 1 || mode == 2;
-    to_disk = mode == 2;
-    TB_REQUIRE_B(!host_side || ((!store_ey || ey_store_3) && (!store_curl || curl_store_3)),
-                 "TM2D: cpu / disk storage modes need host snapshot buffers");
-    TB_REQUIRE_B(!to_disk || ((!store_ey || (ey_filenames && ey_filenames[0])) &&
-                              (!store_curl || (curl_filenames && curl_filenames[0]))),
-                 "TM2D: disk storage mode needs snapshot file names");
-    if (store_ey) {
-      e1 = (char *)ey_store_1;
-      e3 = (char *)ey_store_3;
-    }
-    if (store_curl) {
-      c1 = (char *)curl_store_1;
-      c3 = (char *)curl_store_3;
-    }
-    step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
-    pipeline = host_side && ss != nullptr && ss != st;
-    if (to_disk) {
-      if (!staged.ok) {
-        set_error(kCudaError, "TM2D: event creation failed");
-        return false;
-      }
-      const char *names[2] = {store_ey ? ey_filenames[0] : nullptr,
-                              store_curl ? curl_filenames[0] : nullptr};
-      for (int k = 0; k < 2; ++k)
-        if (names[k]) {
-          disk[k].reset(new DiskHistory(names[k], true, kRing));
-          if (!disk[k]->ok()) {
-            set_error(kBadArgument, "TM2D disk storage: %s", disk[k]->error().c_str());
-            return false;
-          }
-        }
-    }
-    if (pipeline) {
-      if (!store_done.ok || !compute_done.ok) {
-        set_error(kCudaError, "TM2D: event creation failed");
-        return false;
-      }
-      for (int k = 0; k < kRing; ++k)
-        if (TB_CUDA(cudaEventRecord(store_done.ev[k], ss))) return false;
-    }
-    return true;
-  }
-
-  bool stores(int64_t t) const { return want && (t % step_ratio) == 0; }
-
-  // Device slots that step t writes (null when the step stores nothing); the
-  // compute stream waits until the slot's previous host copy has run.
-  bool begin(int64_t t, char **e, char **c) {
-    *e = *c = nullptr;
-    if (!stores(t)) return true;
-    const int64_t q = t / step_ratio;
-    const int slot = (int)(q % kRing);
-    const size_t off = mode == 0 ? (size_t)q * step_bytes : (size_t)slot * step_bytes;
-    if (e1) *e = e1 + off;
-    if (c1) *c = c1 + off;
-    return !(pipeline && TB_CUDA(cudaStreamWaitEvent(st, store_done.ev[slot], 0)));
-  }
-
-  // After step t's launches: cpu mode copies the slots into the host history;
-  // disk mode copies them into the staging slot (whose previous write must
-  // have finished) and queues the slot for the file.
-  bool end(int64_t t, const char *e, const char *c) {
-    if (!stores(t) || !host_side) return true;
-    const int64_t q = t / step_ratio;
-    const int slot = (int)(q % kRing);
-    cudaStream_t cs = st;
-    if (pipeline) {
-      if (TB_CUDA(cudaEventRecord(compute_done.ev[slot], st))) return false;
-      if (TB_CUDA(cudaStreamWaitEvent(ss, compute_done.ev[slot], 0))) return false;
-      cs = ss;
-    }
-    const size_t off3 = to_disk ? (size_t)slot * step_bytes : (size_t)q * step_bytes;
-    char *h3[2] = {e3 ? e3 + off3 : nullptr, c3 ? c3 + off3 : nullptr};
-    const char *d1[2] = {e, c};
-    for (int k = 0; k < 2; ++k) {
-      if (!d1[k]) continue;
-      if (to_disk) disk[k]->wait_slot(slot);
-      if (TB_CUDA(cudaMemcpyAsync(h3[k], d1[k], step_bytes, cudaMemcpyDeviceToHost, cs)))
-        return false;
-    }
-    if (to_disk) {
-      if (TB_CUDA(cudaEventRecord(staged.ev[slot], cs))) return false;
-      for (int k = 0; k < 2; ++k)
-        if (d1[k])
-          disk[k]->enqueue_write(slot, h3[k], step_bytes, (int64_t)(q * step_bytes),
-                                 staged.ev[slot]);
-    }
-    return !(pipeline && TB_CUDA(cudaEventRecord(store_done.ev[slot], ss)));
-  }
-
-  // The call returns once the host history is complete and the files written.
-  bool finish() {
-    if (pipeline && TB_CUDA(cudaStreamSynchronize(ss))) return false;
-    for (int k = 0; k < 2; ++k)
-      if (disk[k] && !disk[k]->finish()) {
-        set_error(kCudaError, "TM2D disk storage: %s", disk[k]->error().c_str());
-        return false;
-      }
-    return true;
-  }
-};
-
 template <typename T, int ST>
 void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   (void)dt; (void)n_threads;
@@ -587,12 +431,15 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   TB_REQUIRE(n_sources_per_shot == 0 || f, "TM2D forward_with_storage: sources without amplitudes");
   TB_REQUIRE(n_receivers_per_shot == 0 || r, "TM2D forward_with_storage: receivers without output");
   cudaStream_t st = as_stream(compute_stream);
-  StoreRun sr;
-  if (!sr.init(ca_requires_grad, cb_requires_grad, storage_mode, storage_format, sizeof(T),
-               shot_bytes_uncomp, ny, nx, n_shots, step_ratio, ey_store_1, ey_store_3,
-               ey_filenames, curl_store_1, curl_store_3, curl_filenames, st,
-               as_stream(storage_stream)))
-    return;
+  StoreRun<2> sr;
+  {
+    const bool need[2] = {ca_requires_grad, cb_requires_grad};
+    void *const dev[2] = {ey_store_1, curl_store_1}, *const host[2] = {ey_store_3, curl_store_3};
+    char const *const *const files[2] = {ey_filenames, curl_filenames};
+    if (!sr.init("TM2D", need, storage_mode, storage_format, sizeof(T), shot_bytes_uncomp,
+                 ny * nx, n_shots, step_ratio, dev, host, files, st, as_stream(storage_stream)))
+      return;
+  }
   Launch<T, ST> L;
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
@@ -617,8 +464,9 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   for (int64_t t = start_t; t < start_t + nt; ++t) {
     const bool smp = prof.sample(t);
     const bool store_step = sr.stores(t);
-    char *e1, *c1;
-    if (!sr.begin(t, &e1, &c1)) return;
+    char *dst[2];
+    if (!sr.begin(t, dst)) return;
+    char *const e1 = dst[0], *const c1 = dst[1];
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
     if (fused) {
@@ -646,7 +494,7 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
                                ps, ft, rt);
       if (smp) prof.end(kKFwdE);
     }
-    if (!sr.end(t, e1, c1)) return;
+    if (!sr.end(t, dst)) return;
   }
   count_launches(fused ? nt : nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;

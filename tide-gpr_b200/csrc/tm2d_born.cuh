@@ -209,12 +209,15 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
   TB_REQUIRE(n_receivers_per_shot == 0 || r,
              "TM2D born_forward_with_storage: receivers without output");
   cudaStream_t st = as_stream(compute_stream);
-  StoreRun sr;
-  if (!sr.init(ca_requires_grad, cb_requires_grad, storage_mode, storage_format, sizeof(T),
-               shot_bytes_uncomp, ny, nx, n_shots, step_ratio, ey_store_1, ey_store_3,
-               ey_filenames, curl_store_1, curl_store_3, curl_filenames, st,
-               as_stream(storage_stream)))
-    return;
+  StoreRun<2> sr;
+  {
+    const bool need[2] = {ca_requires_grad, cb_requires_grad};
+    void *const dev[2] = {ey_store_1, curl_store_1}, *const host[2] = {ey_store_3, curl_store_3};
+    char const *const *const files[2] = {ey_filenames, curl_filenames};
+    if (!sr.init("TM2D", need, storage_mode, storage_format, sizeof(T), shot_bytes_uncomp,
+                 ny * nx, n_shots, step_ratio, dev, host, files, st, as_stream(storage_stream)))
+      return;
+  }
   Launch<T, ST> L;
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
@@ -225,8 +228,9 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   for (int64_t t = start_t; t < start_t + nt; ++t) {
-    char *e1, *c1;
-    if (!sr.begin(t, &e1, &c1)) return;
+    char *dst[2];
+    if (!sr.begin(t, dst)) return;
+    char *const e1 = dst[0], *const c1 = dst[1];
     // scattered history: device-resident, indexed by store index
     char *de1 = nullptr, *dc1 = nullptr;
     if (sr.stores(t)) {
@@ -250,7 +254,7 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
           L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
           ps.src, ps.rec, f0t, dft, rt, bgt, (T *)e1, (T *)c1, (T *)de1, (T *)dc1);
     }
-    if (!sr.end(t, e1, c1)) return;
+    if (!sr.end(t, dst)) return;
   }
   count_launches(nt * (L.has_domain ? 3 : 1));
   if (TB_CUDA(cudaGetLastError())) return;

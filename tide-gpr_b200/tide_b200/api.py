@@ -460,7 +460,8 @@ class Maxwell3D:
             source_component=e.source_component, receiver_component=e.receiver_component,
             forward_callback=observers.forward, backward_callback=observers.backward,
             callback_frequency=observers.frequency,
-            storage_mode=self.storage.mode.value, storage_compression=self.storage.compression,
+            storage_mode=self.storage.mode.value, storage_path=self.storage.path,
+            storage_compression=self.storage.compression,
             storage_chunk_steps=self.storage.chunk_steps, dispersion=model.dispersion,
             retain_history=retain_history, **init,
         )

@@ -267,12 +267,18 @@ class Snapshots3D:
     n_store: int
     shot_bytes: int
     dev: list  # 6 device buffers (or empty)
-    host: list  # 6 pinned host histories (cpu mode)
+    host: list  # 6 pinned host histories (cpu mode) or staging rings (disk mode)
     q0: int = 0  # first store slot held by the device buffers (checkpoint segments)
+    files: object = None  # storage.DiskFiles of the disk mode
+    side: object = None  # storage stream of the cpu / disk modes
 
 
 def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need_cb: bool,
-                       n_store: int | None = None) -> Snapshots3D:
+                       n_store: int | None = None, path: str = ".") -> Snapshots3D:
+    """Buffers of the six snapshot kinds: device mode the whole history on
+    the device; cpu mode a 3-slot device ring and the pinned host history;
+    disk mode a 3-slot device ring, a 3-slot pinned staging ring and one
+    temporary file per kind under path."""
     k = max(1, pb.grad_interval)
     n_store = (pb.nt + k - 1) // k if n_store is None else int(n_store)
     sdt = torch.bfloat16 if fmt == 1 else pb.dtype
@@ -290,9 +296,15 @@ def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need
             host.append(torch.empty(0, dtype=sdt))
         else:
             dev.append(torch.empty((3, pb.n_shots, pb.nz, pb.ny, pb.nx), device=pb.device, dtype=sdt))
-            host.append(torch.empty((n_store, pb.n_shots, pb.nz * pb.ny * pb.nx), dtype=sdt,
+            n_host = 3 if mode == stg.STORAGE_DISK else n_store
+            host.append(torch.empty((n_host, pb.n_shots, pb.nz * pb.ny * pb.nx), dtype=sdt,
                                     pin_memory=True))
-    return Snapshots3D(mode, fmt, n_store, shot_bytes, dev, host)
+    sn = Snapshots3D(mode, fmt, n_store, shot_bytes, dev, host)
+    if mode == stg.STORAGE_DISK and any(need):
+        sn.files = stg.DiskFiles(path, *need, tags=("ex", "ey", "ez", "cx", "cy", "cz"))
+    if mode in (stg.STORAGE_CPU, stg.STORAGE_DISK) and any(need):
+        sn.side = torch.cuda.Stream(pb.device)
+    return sn
 
 
 def _store_ptrs(sn: Snapshots3D) -> list[int]:
@@ -303,7 +315,8 @@ def _store_ptrs(sn: Snapshots3D) -> list[int]:
     for c in range(6):
         d = sn.dev[c]
         step = d[0].numel() * d.element_size() if d.numel() else 0
-        out += [_p(d) - sn.q0 * step if d.numel() else 0, _p(sn.host[c]), 0]
+        out += [_p(d) - sn.q0 * step if d.numel() else 0, _p(sn.host[c]),
+                sn.files.pointer(c) if sn.files is not None else 0]
     return out
 
 
@@ -315,7 +328,8 @@ def native_forward_storage(pb: EM3DProblem, ca, cb, f, r, sn: Snapshots3D, need_
     fn(_p(ca), _p(cb), _p(pb.cq), _p(f), *[_p(t) for t in pb.fields],
        *[_p(t) for t in pb.memories], _p(r), *_store_ptrs(sn), *_profile_ptrs(pb),
        _p(pb.sources_i), _p(pb.receivers_i), *_tail(pb, nt, max(1, pb.grad_interval)),
-       sn.mode, sn.fmt, sn.shot_bytes, need_ca, need_cb, *_flags(pb, start_t), stream, stream)
+       sn.mode, sn.fmt, sn.shot_bytes, need_ca, need_cb, *_flags(pb, start_t), stream,
+       sn.side.cuda_stream if sn.side is not None else stream)
     nat.check("maxwell_3d forward_with_storage")
 
 
@@ -419,7 +433,8 @@ class EM3DPropagate(torch.autograd.Function):
     with recomputation (mode CHECKPOINT)."""
 
     @staticmethod
-    def forward(ctx, ca, cb, f, pb: EM3DProblem, mode: int, fmt: int, seg: int, retain: bool):
+    def forward(ctx, ca, cb, f, pb: EM3DProblem, mode: int, fmt: int, seg: int, retain: bool,
+                path: str = "."):
         need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
         ctx.pb, ctx.mode, ctx.fmt, ctx.seg, ctx.retain = pb, mode, fmt, seg, retain
@@ -428,7 +443,7 @@ class EM3DPropagate(torch.autograd.Function):
             ctx.ckpts = forward_checkpointed(pb, ca, cb, f, r, seg)
             ctx.save_for_backward(ca, cb, f)
         elif need_ca or need_cb or ctx.needs_input_grad[2]:
-            sn = allocate_snapshots(pb, mode, fmt, need_ca, need_cb)
+            sn = allocate_snapshots(pb, mode, fmt, need_ca, need_cb, path=path)
             native_forward_storage(pb, ca, cb, f, r, sn, need_ca, need_cb)
             ctx.sn = sn
             ctx.save_for_backward(ca, cb, f)
@@ -449,7 +464,7 @@ class EM3DPropagate(torch.autograd.Function):
         if not ctx.retain:  # release the history (a linearization keeps it)
             ctx.ckpts = ctx.sn = None
         return (gca if need_ca else None, gcb if need_cb else None,
-                gf if need_f else None, None, None, None, None, None)
+                gf if need_f else None, None, None, None, None, None, None)
 
 
 STATE_NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") + MEM_NAMES
@@ -472,7 +487,7 @@ def maxwell3d(
     m_ex_y: torch.Tensor | None = None, m_ey_x: torch.Tensor | None = None,
     nt: int | None = None,
     model_gradient_sampling_interval: int = 1, source_component: str = "ey",
-    receiver_component: str = "ey", storage_mode: str = "device",
+    receiver_component: str = "ey", storage_mode: str = "device", storage_path: str = ".",
     storage_compression: bool | str = False, storage_bytes_limit_device: int | None = None,
     storage_bytes_limit_host: int | None = None, storage_chunk_steps: int | None = None,
     forward_callback=None, backward_callback=None, callback_frequency: int = 1,
@@ -483,7 +498,8 @@ def maxwell3d(
     region (outer fd_pad cells removed), then the receiver data [nt, S, n_rec].
     Differentiable in epsilon, sigma and source_amplitude.  The initial state
     (Ex_0 .. m_ey_x) takes the same shapes.  storage_mode: 'device', 'cpu'
-    (pinned host history), 'none', or 'checkpoint' (segments of
+    (pinned host history), 'disk' (one temporary file per snapshot kind under
+    storage_path), 'none', 'auto', or 'checkpoint' (segments of
     storage_chunk_steps steps, default about sqrt(nt), recomputed in the
     backward pass).  As in the reference (maxwell3d.py:418-440), a dt above
     the CFL bound for max_vel (default: the model's largest wave speed) runs
@@ -524,11 +540,9 @@ def maxwell3d(
             ny=pb.nz * pb.ny, nx=pb.nx, itemsize=torch.tensor([], dtype=sdtype).element_size(),
             n_arrays=6, bytes_limit_device=storage_bytes_limit_device,
             bytes_limit_host=storage_bytes_limit_host)
-        if mode == stg.STORAGE_DISK:
-            raise NotImplementedError("storage_mode='disk' is built for the 2-D TM path only; "
-                                      "use 'checkpoint' or 'cpu' for 3-D")
         seg = 0
-    r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt, seg, bool(retain_history))
+    r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt, seg, bool(retain_history),
+                            storage_path or ".")
     s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
     outs = [t[s] for t in pb.fields]
     outs += [pb.layout.unpack(m, a)[s] for m, a in zip(pb.memories, MEM_AXES)]

@@ -119,16 +119,17 @@ class SnapshotBuffers:
 class DiskFiles:
     """Temporary snapshot files of one disk-mode history (one per snapshot
     kind, under the storage path), removed when the history is released, and
-    the char* arrays the native calls take (ey_filenames / curl_filenames)."""
+    the char* arrays the native calls take (ey_filenames / curl_filenames;
+    the six *_fn of the 3-D path)."""
 
-    def __init__(self, directory: str, want_ey: bool, want_curl: bool):
+    def __init__(self, directory: str, *want: bool, tags: tuple[str, ...] = ("ey", "curl")):
         import ctypes
         import tempfile
 
         self.paths: list[str | None] = []
         self.arrays = []
-        for want, tag in ((want_ey, "ey"), (want_curl, "curl")):
-            if not want:
+        for want_k, tag in zip(want, tags, strict=True):
+            if not want_k:
                 self.paths.append(None)
                 self.arrays.append(None)
                 continue
