@@ -10,8 +10,8 @@ Modes and formats share the reference's integer codes
   the adjoint (pinned-host offload);
 * ``disk`` (2): a 3-slot device ring, a 3-slot pinned staging ring and one
   temporary file per snapshot kind under ``storage_path``; a writer thread in
-  the native library writes each staged step, the adjoint reads it back (2-D
-  path);
+  the native library writes each staged step, the adjoint reads it back
+  (2-D and 3-D paths);
 * ``none`` (3): nothing stored (forward only);
 * ``auto``: ``device`` when the history fits the device budget, else ``cpu``;
 * ``checkpoint`` (this library's addition): no history; the forward keeps the
