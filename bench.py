@@ -49,6 +49,7 @@ sys.path.insert(0, str(ROOT / "tide-gpr_b200"))
 
 import tide_b200 as tide  # noqa: E402
 from tide_b200 import _native as nat  # noqa: E402
+from tide_b200 import storage as stg  # noqa: E402
 
 METRIC = "2D TM cell-updates/s fwd+adj (% of HBM roofline); served p50/p99 latency"
 UNIT = "cell-updates/s"
@@ -326,6 +327,7 @@ def run_b200(args) -> None:
         }
 
     serving = em3d_leg = debye_leg = None
+    stg.release_history_pool()  # the other legs budget device memory themselves
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         serving = serve_bench(args)
     if rank == 0 and world == 1 and args.em3d_nt > 0:

@@ -52,3 +52,25 @@ def test_storage_modes():
     assert stg.resolve_mode("auto", bytes_limit_device=total - 1, bytes_limit_host=None, **kw) == stg.STORAGE_CPU
     with pytest.raises(MemoryError, match="checkpoint"):
         stg.resolve_mode("auto", bytes_limit_device=0, bytes_limit_host=0, **kw)
+
+
+def test_history_pool_reuses_released_device_history():
+    """A released device history is handed to the next request of the same
+    shape (both snapshot kinds); another shape releases it."""
+    import gc
+
+    from tide_b200 import storage as stg
+
+    stg.release_history_pool()
+    dev = torch.device("cpu")  # the pool logic is device-agnostic
+    a = stg.allocate(stg.STORAGE_DEVICE, torch.float32, 0, 3, 2, 4, 5, dev, True, True)
+    ptrs = {a.ey_dev.data_ptr(), a.curl_dev.data_ptr()}
+    del a
+    gc.collect()
+    b = stg.allocate(stg.STORAGE_DEVICE, torch.float32, 0, 3, 2, 4, 5, dev, True, True)
+    assert {b.ey_dev.data_ptr(), b.curl_dev.data_ptr()} == ptrs
+    c = stg.allocate(stg.STORAGE_DEVICE, torch.float32, 0, 4, 2, 4, 5, dev, True, False)
+    assert c.ey_dev.data_ptr() not in ptrs
+    del b, c
+    gc.collect()
+    stg.release_history_pool()

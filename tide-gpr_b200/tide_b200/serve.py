@@ -369,6 +369,9 @@ class TMServer:
             raise nat.NativeError("TMServer runs on a CUDA device only")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
+        # the server budgets device memory itself: a history kept for reuse by
+        # earlier gradient calls goes back to torch first
+        stg.release_history_pool()
         self.fmt, self.sdtype = stg.compression_format(storage_compression, torch.float32)
         self.item = self.sdtype.itemsize
         if memory_budget is None:

@@ -28,6 +28,7 @@ Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
 from __future__ import annotations
 
 import os
+import weakref
 
 from dataclasses import dataclass, field
 from enum import StrEnum
@@ -99,7 +100,7 @@ def mode_code(mode: str) -> int:
     return codes[m]
 
 
-@dataclass(slots=True)
+@dataclass(slots=True, weakref_slot=True)
 class SnapshotBuffers:
     """Device (and host) buffers for the Ey and curl-H histories."""
 
@@ -154,6 +155,53 @@ class DiskFiles:
                     pass
 
 
+class _HistoryPool:
+    """Keeps the most recently released device history of each (shape, dtype,
+    device) for the next request of the same shape.
+
+    A shot-batched gradient allocates and releases a device history of
+    100+ GB per batch.  Returned to torch's caching allocator, that block can
+    be split by the next batch's small allocations, after which the next
+    history no longer fits and the allocator frees its cache and calls
+    cudaMalloc again (a device synchronisation and a large mapping per
+    batch).  Reuse is stream-ordered: a history is written and read only on
+    the compute stream, so the next user's kernels run after the previous
+    user's.  ``release_history_pool()`` hands the kept buffers back to torch."""
+
+    def __init__(self) -> None:
+        self._free: dict = {}
+
+    def take(self, shape, dtype, device) -> torch.Tensor:
+        key = (tuple(shape), dtype, torch.device(device))
+        kept = self._free.get(key)
+        if kept:
+            return kept.pop()
+        self._free.clear()  # other shapes go back to torch before a new block
+        return torch.empty(shape, device=device, dtype=dtype)
+
+    def give(self, t: torch.Tensor) -> None:
+        key = (tuple(t.shape), t.dtype, t.device)
+        if key not in self._free:
+            self._free = {key: []}  # keep the latest shape only
+        self._free[key].append(t)
+
+    def clear(self) -> None:
+        self._free.clear()
+
+    def nbytes(self, device) -> int:
+        dev = torch.device(device)
+        return sum(t.numel() * t.element_size() for k, ts in self._free.items() if k[2] == dev
+                   for t in ts)
+
+
+_POOL = _HistoryPool()
+
+
+def release_history_pool() -> None:
+    """Return the kept device snapshot history to torch's allocator."""
+    _POOL.clear()
+
+
 def history_bytes(n_store: int, n_shots: int, ny: int, nx: int, itemsize: int, n_arrays: int) -> int:
     return n_store * n_shots * ny * nx * itemsize * n_arrays
 
@@ -179,7 +227,7 @@ def resolve_mode(
     limit_dev = bytes_limit_device
     if limit_dev is None:
         free, _ = torch.cuda.mem_get_info(device)
-        limit_dev = int(0.8 * free)
+        limit_dev = int(0.8 * (free + _POOL.nbytes(device)))  # the pool's buffers are free to it
     if total <= limit_dev:
         return STORAGE_DEVICE
     if bytes_limit_host is not None and total > bytes_limit_host:
@@ -215,7 +263,7 @@ def allocate(
         if not want or mode == STORAGE_NONE:
             return empty, empty_h
         if mode == STORAGE_DEVICE:
-            return torch.empty((n_store, n_shots, ny, nx), device=device, dtype=fmt_dtype), empty_h
+            return _POOL.take((n_store, n_shots, ny, nx), fmt_dtype, device), empty_h
         ring = torch.empty((RING_SLOTS, n_shots, ny, nx), device=device, dtype=fmt_dtype)
         n_host = RING_SLOTS if mode == STORAGE_DISK else n_store
         host = torch.empty((n_host, n_shots, ny * nx), dtype=fmt_dtype, pin_memory=True)
@@ -224,6 +272,11 @@ def allocate(
     ed, eh = one(want_ey)
     cd, ch = one(want_curl)
     snaps = SnapshotBuffers(mode, fmt, fmt_dtype, n_store, shot_bytes, ed, eh, cd, ch)
+    if mode == STORAGE_DEVICE:
+        # released histories go back to the pool (see _HistoryPool)
+        for t in (ed, cd):
+            if t.numel():
+                weakref.finalize(snaps, _POOL.give, t)
     if mode == STORAGE_DISK and (want_ey or want_curl):
         snaps.files = DiskFiles(path, want_ey, want_curl)
     return snaps
