@@ -286,6 +286,8 @@ def allocate_snapshots(pb: EM3DProblem, mode: int, fmt: int, need_ca: bool, need
     shot_bytes = pb.nz * pb.ny * pb.nx * esz
     empty = torch.empty(0, device=pb.device, dtype=sdt)
     need = [need_ca] * 3 + [need_cb] * 3
+    if mode != stg.STORAGE_NONE and any(need):
+        stg.release_history_pool()  # a kept 2-D history would hold the device memory
     dev, host = [], []
     for c in range(6):
         if not need[c] or mode == stg.STORAGE_NONE:
