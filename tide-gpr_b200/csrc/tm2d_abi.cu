@@ -1,7 +1,10 @@
 // extern "C" entry points of the TM2D path: forward, forward_with_storage and
 // backward for stencil orders 2/4/6/8 in float and double, under the
 // reference's symbol names (see include/tide_b200.h for the interface each
-// one replaces).
+// one replaces).  The serving engine (tm2d_serve.cuh), the Debye gradient
+// (tm2d_debye.cuh) and the Born passes (tm2d_born.cuh) are compiled into this
+// translation unit from the includes at its end; the snapshot pipeline of the
+// storing forwards is StoreRun (tb_store.cuh).
 //
 // Every call works on the caller's stream (compute_stream; 0 = legacy
 // default) and returns as soon as its work is enqueued, except that the cpu
