@@ -10,7 +10,9 @@ tide_oracle_tm_born_forward_*):
   bit for bit; the scattered field to rounding (relative L2 <= 1e-5 FP32,
   <= 1e-14 FP64), because that build's -Ofast reassociates the four-term
   scattered update ca dE + cb dcurl + dca E + dcb curl;
-* a central finite difference of the oracle forward in (ca, cb, f): O(h^2).
+* a central finite difference of the oracle forward in (ca, cb, f): O(h^2);
+* the adjoint dot product against the oracle's exact adjoint over the stored
+  background history (the Born adjoint in the perturbation).
 """
 
 from __future__ import annotations
@@ -104,6 +106,28 @@ def test_born_oracle_matches_central_difference():
     fd = (receivers(h) - receivers(-h)) / (2 * h)
     assert rel_l2(r_born, fd) < 1e-6
     assert torch.equal(bg, receivers(0.0))
+
+
+def test_born_adjoint_is_the_adjoint_over_the_background_history():
+    """<J v, w> = <v, J^T w> with J v the oracle Born forward in (dca, dcb, df)
+    and J^T w the oracle's exact adjoint over the stored background history
+    (Ey^n, curl H^n): the scattered update is linear in (dca, dcb, df) with
+    the background factors of (ca, cb, f), so the Born adjoint in the
+    perturbation (born_backward) is that adjoint (FP64)."""
+    pb = random_problem(91, 28, 36, 2, 50, dtype=torch.float64, pml=5)
+    dca, dcb, df = _perturbation(pb, 13)
+    r, _, _, _ = _run(Oracle(), pb, dca, dcb, df)
+    o = Oracle()
+    q = clone_problem(pb)
+    shape = (q.nt, q.n_shots, q.ny, q.nx)
+    store = (torch.zeros(shape, dtype=q.dtype), torch.zeros(shape, dtype=q.dtype))
+    o.forward(q, q.ca, q.cb, q.f, _zeros_r(q), store=store, need_ca=True, need_cb=True)
+    w = torch.randn(r.shape, generator=torch.Generator().manual_seed(8), dtype=torch.float64)
+    gca, gcb, gf, _ = o.backward(q, q.ca, q.cb, w, store)
+    lhs = float((r * w).sum())
+    rhs = float((dca[0] * gca).sum() + (dcb[0] * gcb).sum() + (df.reshape(gf.shape) * gf).sum())
+    assert abs(lhs) > 0
+    assert abs(lhs - rhs) <= 1e-11 * abs(lhs)
 
 
 # ---------------------------------------------------------------------- 3-D
