@@ -74,3 +74,25 @@ def test_history_pool_reuses_released_device_history():
     del b, c
     gc.collect()
     stg.release_history_pool()
+
+
+def test_disk_files_per_kind(tmp_path):
+    """One temporary file per wanted snapshot kind (the 2-D pair or the six
+    3-D components), a char** array per file for the native calls, and the
+    files removed with the history."""
+    import ctypes
+    import gc
+
+    from tide_b200 import storage as stg
+
+    f = stg.DiskFiles(str(tmp_path), True, False, True, tags=("ex", "ey", "ez"))
+    assert f.pointer(1) == 0 and f.pointer(0) != 0 and f.pointer(2) != 0
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert len(names) == 2 and names[0].startswith("tide_b200_ex_")
+    first = ctypes.cast(f.pointer(0), ctypes.POINTER(ctypes.c_char_p))[0].decode()
+    assert first == f.paths[0]
+    two = stg.DiskFiles(str(tmp_path), True, True)  # the 2-D default kinds
+    assert two.paths[0].split("/")[-1].startswith("tide_b200_ey_")
+    del f, two
+    gc.collect()
+    assert list(tmp_path.iterdir()) == []
