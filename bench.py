@@ -23,8 +23,11 @@ Arms:
                    with OpenMP) on the host cores, on a bounded sample of the
                    same workload.
 
-Run with torchrun for N > 1 GPUs (weak scaling: every rank evaluates the full
-64-shot gradient; ranks then all-reduce the model gradients over NCCL).
+Run with torchrun for N > 1 GPUs: the 64 shots of the evaluation are split
+over the ranks (strided, as the reference's workflow/distributed.py does),
+each rank back-propagates its shots in batches, and the partial eps/sigma
+gradients are summed with one NCCL all-reduce (strong scaling: the job is
+fixed, `value` counts its cell-updates once).
 """
 
 from __future__ import annotations
@@ -202,9 +205,10 @@ def kernel_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho_x: float, rho_
 # ---------------------------------------------------------------- B200 arm
 
 
-# DRAM bytes per cell moved by each kernel in one ncu capture on the config-2
-# grid (profiles/k2_adj_h_config2_ncu_full.md); None where not captured.
-TRAFFIC_B_PER_CELL = {"adj_h": 24.6}
+# DRAM bytes per cell (one shot, one step) moved by each kernel in an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) on the config-2 grid
+# with 8-shot launches; None where not captured.
+TRAFFIC_B_PER_CELL = {"adj_h": 23.7}
 
 
 def shot_batches(shots: int, snap_bytes: int, device) -> int:
@@ -217,6 +221,42 @@ def shot_batches(shots: int, snap_bytes: int, device) -> int:
     return b
 
 
+def _shot_take(t: torch.Tensor, ids: torch.Tensor) -> torch.Tensor:
+    """Rows `ids` (CPU int64, ascending) of a per-shot tensor: a view for a
+    contiguous range, a gathered copy otherwise."""
+    lo, n = int(ids[0]), int(ids.numel())
+    if int(ids[-1]) - lo + 1 == n:
+        return t[lo:lo + n]
+    return t.index_select(0, ids.to(t.device))
+
+
+def sharded_gradient(eps, sig, n_shots: int, batch: int, batch_fn, ctx):
+    """One gradient evaluation of an n_shots acquisition across the ranks of
+    `ctx` (shot-parallel, as the reference's workflow/distributed.py:151,260-274):
+    each rank takes its strided share of the shots (rank_shot_indices), runs
+    them in batches of `batch` through batch_fn(eps, sig, ids) -- which
+    back-propagates into eps.grad / sig.grad and returns the batch loss --
+    and the partial gradients and losses are then summed over the ranks (the
+    path's one exchange).  Every rank returns the full gradient [2, ny, nx]
+    and the full loss, equal to a single-rank evaluation of all shots up to
+    the order of the shot sum."""
+    from tide_b200 import distributed as tdist
+
+    e = eps.detach().requires_grad_(True)
+    s = sig.detach().requires_grad_(True)
+    ids = tdist.rank_shot_indices(n_shots, ctx=ctx, device="cpu")
+    loss = torch.zeros((), dtype=eps.dtype, device=eps.device)
+    for b in ids.split(max(1, int(batch))):
+        loss = loss + batch_fn(e, s, b)
+    tdist.all_reduce_gradients([e, s], ctx=ctx)
+    loss = tdist.all_reduce_tensor(loss, ctx=ctx)
+    if e.grad is None:
+        e.grad = torch.zeros_like(e)
+    if s.grad is None:
+        s.grad = torch.zeros_like(s)
+    return torch.stack([e.grad, s.grad]), loss
+
+
 def run_b200(args) -> None:
     from tide_b200 import distributed as tdist
 
@@ -226,7 +266,8 @@ def run_b200(args) -> None:
     snap_bytes = 2 if args.storage == "bf16" else 4
     cfg = config2(shots=args.shots, nt=args.nt)
     S_total = args.shots
-    batch = args.batch or shot_batches(S_total, snap_bytes, dev)
+    S_rank = int(tdist.rank_shot_indices(S_total, ctx=ctx, device="cpu").numel())
+    batch = args.batch or shot_batches(S_rank, snap_bytes, dev)
     compression = args.storage == "bf16"
 
     # host (pinned) copies for the end-to-end leg, device copies for `value`
@@ -238,23 +279,20 @@ def run_b200(args) -> None:
             d = {k: (v.to(dev, non_blocking=True) if torch.is_tensor(v) else v) for k, v in inp.items()}
         else:
             d = inp
-        eps = d["eps"].detach().requires_grad_(True)
-        sig = d["sig"].detach().requires_grad_(True)
-        loss_total = torch.zeros((), device=dev)
-        for b0 in range(0, S_total, batch):
-            sl = slice(b0, b0 + batch)
+
+        def batch_fn(eps, sig, ids):
             out = tide.maxwelltm(
-                eps, sig, d["mu"], d["dx"], d["dt"], d["amp"][sl], d["src"][sl], d["rec"][sl],
+                eps, sig, d["mu"], d["dx"], d["dt"], _shot_take(d["amp"], ids),
+                _shot_take(d["src"], ids), _shot_take(d["rec"], ids),
                 stencil=2, pml_width=d["pml"], storage_mode="device",
                 storage_compression=compression,
             )
             r = out[-1]
             loss = 0.5 * (r * r).sum()
             loss.backward()
-            loss_total = loss_total + loss.detach()
-        tdist.all_reduce_gradients([eps, sig], ctx=ctx)  # the one exchange per gradient
-        g = torch.stack([eps.grad, sig.grad])
-        return g, loss_total
+            return loss.detach()
+
+        return sharded_gradient(d["eps"], d["sig"], S_total, batch, batch_fn, ctx)
 
     def timed(n_steps, copy_in):
         if world > 1:
@@ -301,7 +339,7 @@ def run_b200(args) -> None:
     clk = clocks.stop()
     e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)
 
-    units = cell_updates(S_total, args.nt) * world
+    units = cell_updates(S_total, args.nt)  # the whole job; its shots are split over the ranks
     value = units * args.steps / (ms / 1e3)
     e2e_value = units * max(1, args.e2e_steps) / (e2e_ms / 1e3)
 
@@ -336,22 +374,25 @@ def run_b200(args) -> None:
         debye_leg = debye_bench(args)
     if rank == 0:
         cpu = cpu_baseline(args) if not args.no_cpu_baseline else None
+        parity = parity_report(args, dev) if not args.no_cpu_baseline and args.parity_nt > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded config-2 model and acquisition)",
             "config": {
                 "workload": "config2: 2D TM fwd+adj, 512x1024 (553x1065 padded), CPML 20, "
                             f"stencil 2, nt={args.nt}, {S_total} shots, snapshots {args.storage} on device",
                 "shots": S_total, "shot_batch": batch, "nt": args.nt,
                 "cell_updates_per_step": units, "l2": "per-step working set (snapshot history) >> L2",
-                "parallelism": f"shots-weak-dp{world}",
+                "parallelism": f"shot-parallel dp{world}: {S_rank} shots per rank in batches "
+                               f"of {batch}, one all-reduce of the eps/sigma gradient",
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clk, "serving": serving,
+            "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
+            "serving": serving,
             "em3d": em3d_leg, "debye": debye_leg,
         }
         print(json.dumps(line), flush=True)
@@ -678,6 +719,35 @@ def cpu_baseline(args) -> dict:
     }
 
 
+def parity_report(args, dev) -> dict:
+    """Accuracy beside the speed (part of the CPU-baseline leg: the CPU
+    checkers run here only to check the GPU results): config-1 receivers
+    against the reference CPU backend's FP32 and FP64 runs, and the eps /
+    sigma gradient of a config-2 sample (full grid, the first
+    --parity-shots shots, --parity-nt steps) against the C oracle's exact
+    adjoint in FP32 and FP64, plus the BF16-snapshot gradient error."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    try:
+        import parity_config2 as pc2
+
+        t0 = time.perf_counter()
+        c1 = pc2.config1_errors(dev)
+        c2 = pc2.config2_sample_errors(config2(shots=args.parity_shots, nt=args.parity_nt), dev)
+        sec = time.perf_counter() - t0
+    except Exception as exc:  # noqa: BLE001
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+    return {
+        "config1_receivers": c1,
+        "config2_sample": dict(c2, sample=f"config-2 model and acquisition, 553x1065 padded, "
+                                          f"first {args.parity_shots} shots, nt={args.parity_nt}, "
+                                          "loss 0.5|r|^2, FP32 public API vs C oracle exact "
+                                          "adjoint (reference summation order)"),
+        "bar": "FP32 relative L2 <= 1e-5 against the FP32 checkers; FP64 figures are the "
+               "FP32 error statement; BF16 snapshots: gradient error reported",
+        "seconds": round(sec, 1),
+    }
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -723,7 +793,11 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-shots", type=int, default=4)
     ap.add_argument("--cpu-nt", type=int, default=64)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline and the accuracy checks")
+    ap.add_argument("--parity-shots", type=int, default=2)
+    ap.add_argument("--parity-nt", type=int, default=250,
+                    help="steps of the config-2 accuracy sample (0: skip)")
     ap.add_argument("--profile-every", type=int, default=32,
                     help="time every n-th step's kernels with events in the timed region "
                          "(0: off; the roofline needs it)")

@@ -248,8 +248,10 @@ TIDE_TM_BORN_DECLARE(8, double)
  * than the array holds (2 (tiles + 1) + 2 entries words per point list,
  * tiles = n_shots * ceil(nx/32) * ceil(ny/16)) are rejected with a status
  * message.  All calls on a device share the array, so calls whose GPU work
- * overlaps race and must be serialised; the first call on each device looks
- * up the array's address and should come before any stream capture.  Debye
+ * overlaps race and must be serialised.  Every call looks the array's
+ * address up on the current device (nothing is cached, so a device reset is
+ * harmless); the first call on a device may load the library's device code
+ * and should come before any stream capture.  Debye
  * media are not supported by this variant. */
 void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
 Run in a container where the reference tree is mounted (read-only) at
-$TIDE_REFERENCE (default /root/reference) and after `make -C oracle ref`
+$TIDE_REFERENCE (default: a directory `reference` beside the repository) and after `make -C oracle ref`
 has compiled the reference CPU backend into oracle/_ref/:
 
     python tests/golden/make_golden.py
@@ -37,7 +37,7 @@ import torch
 
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", "/root/reference"))
+REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", pathlib.Path(__file__).resolve().parents[3] / "reference"))
 sys.path.insert(0, str(REF / "src"))
 
 import tide  # noqa: E402

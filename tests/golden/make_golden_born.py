@@ -1,7 +1,7 @@
 """Generate tests/golden/born_case.npz from the reference's Born propagator.
 
 Run where the reference tree is mounted (read-only) at $TIDE_REFERENCE
-(default /root/reference):
+(default: a directory `reference` beside the repository):
 
     python tests/golden/make_golden_born.py
 
@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 HERE = pathlib.Path(__file__).resolve().parent
-REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", "/root/reference"))
+REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", pathlib.Path(__file__).resolve().parents[3] / "reference"))
 sys.path.insert(0, str(REF / "src"))
 
 from tide.maxwell.tm2d_born import borntm  # noqa: E402

@@ -1,7 +1,7 @@
 """Generate the Debye golden fixture (debye_case.npz) from the reference.
 
-Run where the reference tree is mounted at $TIDE_REFERENCE (default
-/root/reference) and after `make -C oracle ref` built oracle/_ref/:
+Run where the reference tree is mounted at $TIDE_REFERENCE (default: a directory
+`reference` beside the repository) and after `make -C oracle ref` built oracle/_ref/:
 
     python tests/golden/make_golden_debye.py
 
@@ -30,7 +30,7 @@ import torch
 
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", "/root/reference"))
+REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", pathlib.Path(__file__).resolve().parents[3] / "reference"))
 sys.path.insert(0, str(REF / "src"))
 
 import tide  # noqa: E402

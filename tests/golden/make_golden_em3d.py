@@ -1,7 +1,7 @@
 """Generate the 3-D golden fixture from the reference itself.
 
 Run where the reference tree is mounted (read-only) at $TIDE_REFERENCE
-(default /root/reference), after `make -C oracle ref`:
+(default: a directory `reference` beside the repository), after `make -C oracle ref`:
 
     python tests/golden/make_golden_em3d.py
 
@@ -27,7 +27,7 @@ import torch
 
 HERE = pathlib.Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", "/root/reference"))
+REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", pathlib.Path(__file__).resolve().parents[3] / "reference"))
 sys.path.insert(0, str(REF / "src"))
 
 import tide  # noqa: E402

@@ -125,3 +125,85 @@ def test_rank_leaving_before_collective_is_an_error_not_a_hang(tmp_path):
     assert procs[1].exitcode == 3
     out = torch.load(tmp_path / "rank0.pt")
     assert "error" in out
+
+
+# ---------------------------------------------------------------- bench step
+
+
+def _bench_case(dtype):
+    from tide_b200 import physics as ph
+
+    g = torch.Generator().manual_seed(7)
+    ny, nx, S, nt = 16, 20, 5, 30
+    eps = (2.0 + 4.0 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype)
+    sig = (0.004 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype)
+    mu = torch.ones((ny, nx), dtype=dtype)
+    dt = 3e-11
+    amp = ph.ricker(900e6, nt, dt, dtype=dtype).view(1, 1, nt).repeat(S, 1, 1)
+    amp = amp * (1.0 + torch.arange(S, dtype=dtype)).view(S, 1, 1)
+    src = torch.tensor([[[4, 3 + 3 * i]] for i in range(S)])
+    rec = torch.tensor([[[5, 2 + 4 * j] for j in range(4)]] * S)
+    return dict(eps=eps, sig=sig, mu=mu, dx=0.02, dt=dt, amp=amp, src=src, rec=rec, S=S)
+
+
+def _bench_batch_fn(c):
+    """bench.py's per-batch step with the C oracle (CPU) in place of the GPU
+    propagator: forward, loss 0.5 |r|^2, backward into eps/sigma."""
+    from oracle_harness import Oracle, OracleTM
+    from tide_b200.tm2d import prepare_tm2d
+
+    oracle = Oracle()
+
+    def fn(eps, sig, ids):
+        pb = prepare_tm2d(eps, sig, c["mu"], c["dx"], c["dt"], c["amp"][ids], c["src"][ids],
+                          c["rec"][ids], stencil=2, pml_width=4)
+        r = OracleTM.apply(pb.ca, pb.cb, pb.f, pb, oracle, 1, 0)
+        loss = 0.5 * (r * r).sum()
+        loss.backward()
+        return loss.detach()
+
+    return fn
+
+
+def _bench_worker(rank, world, port, out_dir, dtype):
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, here)
+    sys.path.insert(0, os.path.dirname(here))
+    sys.path.insert(0, os.path.join(os.path.dirname(here), "tide-gpr_b200"))
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import bench
+
+    ctx = tdist.init_distributed(device="cpu", timeout_s=30.0)
+    try:
+        c = _bench_case(dtype)
+        g, loss = bench.sharded_gradient(c["eps"], c["sig"], c["S"], 2, _bench_batch_fn(c), ctx)
+        torch.save({"g": g, "loss": loss}, os.path.join(out_dir, f"bench{rank}.pt"))
+    finally:
+        tdist.destroy_distributed(ctx)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 1e-5)])
+def test_bench_step_sharded_equals_single_rank(tmp_path, dtype, tol):
+    """bench.py's multi-GPU step: the ranks split the shots, each
+    back-propagates its shard in batches and the eps/sigma gradients are
+    summed once.  The two-rank gradient and loss equal the single-rank ones
+    (only the order of the shot sum changes: FP64 1e-12, FP32 1e-5 relative
+    L2)."""
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+
+    port = _free_port()
+    mp.spawn(_bench_worker, args=(2, port, str(tmp_path), dtype), nprocs=2, join=True)
+    c = _bench_case(dtype)
+    g1, loss1 = bench.sharded_gradient(c["eps"], c["sig"], c["S"], 2, _bench_batch_fn(c), None)
+    assert float(g1.norm()) > 0
+    for rank in range(2):
+        res = torch.load(tmp_path / f"bench{rank}.pt")
+        err = float((res["g"] - g1).norm() / g1.norm())
+        assert err <= tol, (rank, err)
+        assert abs(float(res["loss"]) - float(loss1)) <= tol * abs(float(loss1))

@@ -68,25 +68,72 @@ def test_noalloc_forward_matches_regular_on_two_calls(cuda_device):
 
 
 def test_noalloc_forward_rejects_oversize(cuda_device):
+    """A problem needing more scratch than the fixed array is refused.  The
+    buffers match the arguments (one shot, a small grid, 2.2 M source entries
+    per shot, all with index -1, one step), so even if the size check ever
+    stopped refusing the call every access would stay in bounds."""
     fn = _noalloc_fn()
     lib = nat.load()
     lib.tide_b200_clear_error()
-    pb = random_problem(303, 20, 24, 1, 4)
+    pb = random_problem(303, 20, 24, 1, 1)
     g = clone_problem(pb, cuda_device)
-    # Claim a huge shot count: the size check refuses the call before any GPU
-    # work touches the (much smaller) buffers.
+    n_src = 2_200_000  # 2 (tiles + 1) + 2 n_src words > 4 Mi words
+    src_i = torch.full((1, n_src), -1, dtype=torch.int64, device=cuda_device)
+    f = torch.zeros((1, 1, n_src), device=cuda_device)
     ey, hx, hz, mex, mez, mhx, mhz = g.fields
     prof = [nat.ptr(g.profiles[n]) for n in tm2d._PROFILE_ORDER]
-    r = torch.zeros((g.nt, 1, g.n_rec), device=cuda_device)
+    r = torch.zeros((1, 1, g.n_rec), device=cuda_device)
     fn(
-        nat.ptr(g.ca), nat.ptr(g.cb), nat.ptr(g.cq), nat.ptr(g.f),
+        nat.ptr(g.ca), nat.ptr(g.cb), nat.ptr(g.cq), nat.ptr(f),
         nat.ptr(ey), nat.ptr(hx), nat.ptr(hz), nat.ptr(mex), nat.ptr(mez), nat.ptr(mhx), nat.ptr(mhz),
-        0, 0, 0, 0, 0, nat.ptr(r), 0, *prof, nat.ptr(g.sources_i), nat.ptr(g.receivers_i),
-        g.rdy, g.rdx, g.dt, g.nt, 60000, 4096, 4096, g.n_src, g.n_rec, 1, False,
+        0, 0, 0, 0, 0, nat.ptr(r), 0, *prof, nat.ptr(src_i), nat.ptr(g.receivers_i),
+        g.rdy, g.rdx, g.dt, 1, 1, g.ny, g.nx, n_src, g.n_rec, 1, False,
         False, False, False, 0, g.pml_y0, g.pml_x0, g.pml_y1, g.pml_x1,
-        0, 0, int(torch.cuda.current_stream(cuda_device).cuda_stream),
+        0, cuda_device.index or 0, int(torch.cuda.current_stream(cuda_device).cuda_stream),
     )
     assert lib.tide_b200_last_status() != 0
     assert b"scratch words" in lib.tide_b200_last_error()
     lib.tide_b200_clear_error()
     torch.cuda.synchronize()
+
+
+def _driver():
+    import ctypes
+
+    cu = ctypes.CDLL("libcuda.so.1")
+    cu.cuDeviceGetDefaultMemPool.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+    cu.cuMemPoolGetAttribute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    cu.cuMemPoolSetAttribute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    return cu
+
+
+def test_noalloc_forward_allocates_nothing(cuda_device):
+    """The call's promise: no allocation of any kind.  The regular forward
+    takes its point lists from the device's default stream-ordered pool, so
+    the pool's high-water mark of used memory (reset just before the call)
+    would grow with it; here it must not, and the device's free memory must
+    not change either."""
+    import ctypes
+
+    used_current, used_high = 7, 8  # CU_MEMPOOL_ATTR_USED_MEM_CURRENT / _HIGH
+    fn = _noalloc_fn()
+    pb = random_problem(304, 90, 130, 4, 60, n_rec=25)
+    g = clone_problem(pb, cuda_device)
+    r = torch.zeros((g.nt, g.n_shots, g.n_rec), device=cuda_device)
+    _call(fn, g, r, 0, g.nt)  # first call on the device: may load the module
+    torch.cuda.synchronize()
+    cu = _driver()
+    pool = ctypes.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(ctypes.byref(pool), cuda_device.index or 0) == 0
+    zero = ctypes.c_uint64(0)
+    assert cu.cuMemPoolSetAttribute(pool, used_high, ctypes.byref(zero)) == 0
+    cur = ctypes.c_uint64(0)
+    assert cu.cuMemPoolGetAttribute(pool, used_current, ctypes.byref(cur)) == 0
+    free0, _ = torch.cuda.mem_get_info(cuda_device)
+    _call(fn, g, r, 0, g.nt)
+    torch.cuda.synchronize()
+    high = ctypes.c_uint64(0)
+    assert cu.cuMemPoolGetAttribute(pool, used_high, ctypes.byref(high)) == 0
+    free1, _ = torch.cuda.mem_get_info(cuda_device)
+    assert high.value <= cur.value, (high.value, cur.value)
+    assert free1 == free0

@@ -789,31 +789,22 @@ extern "C" int tide_b200_device_status(int64_t device) {
 //    behind; each call clears the counters it needs first.  Calls whose GPU
 //    work overlaps (for example on two streams at once) race on the array and
 //    must be serialised by the caller;
-//  - the first call on each device looks the array's device address up (with
-//    that device current) and caches it; make that first call before any
-//    stream capture.
+//  - every call looks the array's device address up with cudaGetSymbolAddress
+//    (the device selected by `device` current), so the address stays valid
+//    after a device reset reloads the module; the first call on a device may
+//    load the library's device code, so make it before any stream capture.
 namespace tb {
 namespace {
 
 constexpr size_t kNoAllocScratchWords = size_t(1) << 22;
 static __device__ __align__(256) int g_noalloc_scratch[kNoAllocScratchWords];
 
-std::mutex g_noalloc_mu;
-int *g_noalloc_ptr[128] = {};
-
-// Device address of the scratch array on the current device (set up once).
-int *noalloc_scratch(int device) {
-  if (device < 0 || device >= 128) {
-    set_error(kBadArgument, "noalloc forward: device index %d out of range", device);
-    return nullptr;
-  }
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (g_noalloc_ptr[device] == nullptr) {
-    void *p = nullptr;
-    if (TB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch))) return nullptr;
-    g_noalloc_ptr[device] = static_cast<int *>(p);
-  }
-  return g_noalloc_ptr[device];
+// Device address of the scratch array on the current device.  Looked up on
+// every call: cheap, allocates nothing, and never stale after a device reset.
+int *noalloc_scratch() {
+  void *p = nullptr;
+  if (TB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch))) return nullptr;
+  return static_cast<int *>(p);
 }
 
 }  // namespace
@@ -846,7 +837,7 @@ extern "C" void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(flo
              "noalloc forward: problem needs %zu scratch words, the fixed array holds %zu "
              "(reduce n_shots per call or use maxwell_tm_2_float_forward_cuda)",
              words, kNoAllocScratchWords);
-  int *scratch = noalloc_scratch((int)device);
+  int *scratch = noalloc_scratch();
   if (scratch == nullptr) return;
   cudaStream_t st = as_stream(compute_stream);
   PointScratch ps;  // ps.mem stays null: nothing is freed at scope exit

@@ -28,6 +28,7 @@ Formats: ``FULL`` (0) stores the field dtype, ``BF16`` (1) stores bfloat16
 from __future__ import annotations
 
 import os
+import threading
 import weakref
 
 from dataclasses import dataclass, field
@@ -164,34 +165,66 @@ class _HistoryPool:
     be split by the next batch's small allocations, after which the next
     history no longer fits and the allocator frees its cache and calls
     cudaMalloc again (a device synchronisation and a large mapping per
-    batch).  Reuse is stream-ordered: a history is written and read only on
-    the compute stream, so the next user's kernels run after the previous
-    user's.  ``release_history_pool()`` hands the kept buffers back to torch."""
+    batch).
+
+    Stream order.  A history is written by the storing forward and read by
+    the adjoint on the stream that allocated it (autograd runs a backward
+    node on its forward's stream), and it is released by a finalizer as soon
+    as the host drops it -- possibly while that adjoint is still queued.  So
+    ``give`` records an event on the allocating stream (and on the stream
+    current at release) and ``take`` makes the requesting stream wait for
+    those events before the buffer is handed out; a history is never
+    overwritten by a later batch on another stream before its reader ran.
+    ``give`` may run on any thread (garbage collection), so every method
+    holds a lock.  ``release_history_pool()`` hands the kept buffers back to
+    torch."""
 
     def __init__(self) -> None:
         self._free: dict = {}
+        self._lock = threading.Lock()
 
     def take(self, shape, dtype, device) -> torch.Tensor:
         key = (tuple(shape), dtype, torch.device(device))
-        kept = self._free.get(key)
-        if kept:
-            return kept.pop()
-        self._free.clear()  # other shapes go back to torch before a new block
-        return torch.empty(shape, device=device, dtype=dtype)
+        with self._lock:
+            kept = self._free.get(key)
+            if kept:
+                t, events = kept.pop()
+            else:
+                self._free.clear()  # other shapes go back to torch before a new block
+                t, events = None, ()
+        if t is None:
+            return torch.empty(shape, device=device, dtype=dtype)
+        if events:
+            cur = torch.cuda.current_stream(t.device)
+            for ev in events:
+                cur.wait_event(ev)
+        return t
 
-    def give(self, t: torch.Tensor) -> None:
+    def give(self, t: torch.Tensor, stream=None) -> None:
+        events = []
+        if t.device.type == "cuda":
+            streams = [torch.cuda.current_stream(t.device)]
+            if stream is not None and stream != streams[0]:
+                streams.append(stream)
+            for s in streams:
+                ev = torch.cuda.Event()
+                ev.record(s)
+                events.append(ev)
         key = (tuple(t.shape), t.dtype, t.device)
-        if key not in self._free:
-            self._free = {key: []}  # keep the latest shape only
-        self._free[key].append(t)
+        with self._lock:
+            if key not in self._free:
+                self._free = {key: []}  # keep the latest shape only
+            self._free[key].append((t, tuple(events)))
 
     def clear(self) -> None:
-        self._free.clear()
+        with self._lock:
+            self._free.clear()
 
     def nbytes(self, device) -> int:
         dev = torch.device(device)
-        return sum(t.numel() * t.element_size() for k, ts in self._free.items() if k[2] == dev
-                   for t in ts)
+        with self._lock:
+            return sum(t.numel() * t.element_size() for k, ts in self._free.items()
+                       if k[2] == dev for t, _ in ts)
 
 
 _POOL = _HistoryPool()
@@ -274,9 +307,11 @@ def allocate(
     snaps = SnapshotBuffers(mode, fmt, fmt_dtype, n_store, shot_bytes, ed, eh, cd, ch)
     if mode == STORAGE_DEVICE:
         # released histories go back to the pool (see _HistoryPool)
+        dev_t = torch.device(device)
+        alloc_stream = torch.cuda.current_stream(dev_t) if dev_t.type == "cuda" else None
         for t in (ed, cd):
             if t.numel():
-                weakref.finalize(snaps, _POOL.give, t)
+                weakref.finalize(snaps, _POOL.give, t, alloc_stream)
     if mode == STORAGE_DISK and (want_ey or want_curl):
         snaps.files = DiskFiles(path, want_ey, want_curl)
     return snaps
