@@ -100,11 +100,40 @@ extern "C" {
       int64_t n_threads, int64_t device, void *compute_stream,                 \
       void *storage_stream
 
+/* Argument list of maxwell_tm_*_background_vjp_reuse_cuda: the backward's,
+ * with background_n_shots after shot_bytes_uncomp.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:2405-2460 (argtypes
+ * src/tide/backend_utils.py:310-334; called by the Born autograd,
+ * src/tide/maxwell/tm2d_born_autograd.py:886-960): the snapshot history holds
+ * background_n_shots shots (n_shots must be a multiple of it) and adjoint
+ * shot s images against snapshot shot s % background_n_shots. */
+#define TIDE_TM_BACKGROUND_VJP_REUSE_ARGS(T)                                   \
+  T const *ca, T const *cb, T const *cq, T const *grad_r, T *lambda_ey,        \
+      T *lambda_hx, T *lambda_hz, T *m_lambda_ey_x, T *m_lambda_ey_z,          \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, T *adjoint_memory_scratch,           \
+      void *ey_store_1, void *ey_store_3, char const *const *ey_filenames,     \
+      void *curl_store_1, void *curl_store_3,                                  \
+      char const *const *curl_filenames, T *grad_f, T *grad_ca, T *grad_cb,    \
+      T *grad_ca_shot, T *grad_cb_shot, T const *ay, T const *by,              \
+      T const *ayh, T const *byh, T const *ax, T const *bx, T const *axh,      \
+      T const *bxh, T const *ky, T const *kyh, T const *kx, T const *kxh,      \
+      int64_t const *sources_i, int64_t const *receivers_i, T rdy, T rdx,      \
+      T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx,               \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, int64_t background_n_shots,                   \
+      bool ca_requires_grad, bool cb_requires_grad, bool ca_batched,           \
+      bool cb_batched, bool cq_batched, int64_t start_t, int64_t pml_y0,       \
+      int64_t pml_x0, int64_t pml_y1, int64_t pml_x1, int64_t n_threads,       \
+      int64_t device, void *compute_stream, void *storage_stream
+
 #define TIDE_TM_DECLARE(S, T)                                                  \
   void maxwell_tm_##S##_##T##_forward_cuda(TIDE_TM_FORWARD_ARGS(T));           \
   void maxwell_tm_##S##_##T##_forward_with_storage_cuda(                       \
       TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T));                                   \
-  void maxwell_tm_##S##_##T##_backward_cuda(TIDE_TM_BACKWARD_ARGS(T));
+  void maxwell_tm_##S##_##T##_backward_cuda(TIDE_TM_BACKWARD_ARGS(T));         \
+  void maxwell_tm_##S##_##T##_background_vjp_reuse_cuda(                       \
+      TIDE_TM_BACKGROUND_VJP_REUSE_ARGS(T));
 
 /* Stencil orders 2/4/6/8 in float and double, as the reference exports
  * (src/tide/csrc/tm2d/maxwell_tm_cuda_instantiations.inc). */
@@ -412,7 +441,8 @@ int tide_b200_device_status(int64_t device);
  * kernels with CUDA events on the launching stream; durations accumulate per
  * kernel kind until read (reading waits for the recorded events; profiled
  * calls themselves never block).  Kinds: 0 fwd_h, 1 fwd_e, 2 adj_e, 3 adj_h,
- * 4 fwd_step (fused forward), 5 adj_step (fused adjoint). */
+ * 4 fwd_step (one-sweep forward), 5 adj_step (one-sweep adjoint), 6 em3d_fwd_h,
+ * 7 em3d_fwd_e, 8 em3d_adj_e, 9 em3d_adj_h, 10 em3d_grad (3-D path). */
 void tide_b200_profile_enable(int on, int sample_every);
 int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds);
 const char *tide_b200_profile_kind_name(int kind);
@@ -427,6 +457,21 @@ int64_t tide_b200_launch_count(void);
  * fused, negative = never.  Default 64 MiB.  Returns the previous setting;
  * process-wide, takes effect at the next call. */
 int64_t tide_b200_set_fused_threshold(int64_t bytes);
+
+/* Selection of the one-sweep TMA time steps (new; no reference counterpart):
+ * FP32 stencil-2 forward, forward_with_storage and backward with model
+ * coefficients shared by the shots and no Debye poles run one launch per time
+ * step on TMA-staged tiles (both half steps fused) on persistent CTAs.
+ * 0 = never, 1 = when the grid has at least 64 tiles of 32 x 64 cells
+ * (default), 2 = whenever eligible.  Results are bit-identical in every mode.
+ * Returns the previous mode; process-wide, takes effect at the next call. */
+int tide_b200_set_tma_mode(int mode);
+
+/* Upper bound on the persistent CTAs of the TMA time steps (new; no reference
+ * counterpart): 0 = one per SM (default).  Smaller bounds give each CTA more
+ * tiles and split more tiles between neighbouring CTAs; results are
+ * bit-identical for every bound.  Returns the previous bound. */
+int tide_b200_set_tma_ctas(int max_ctas);
 
 #ifdef __cplusplus
 }

@@ -131,8 +131,16 @@ def abi_specs():
     import json
 
     specs = {}
-    for prop in ("maxwell_tm", "maxwell_3d"):
-        for pass_name in ("forward", "forward_with_storage", "backward"):
+    passes = {
+        "maxwell_tm": ("forward", "forward_with_storage", "backward", "background_vjp_reuse",
+                       "born_forward", "born_forward_with_storage",
+                       "born_tangent_forward_with_storage", "born_backward",
+                       "born_backward_bggrad"),
+        "maxwell_3d": ("forward", "forward_with_storage", "backward", "born_forward",
+                       "born_forward_with_storage", "born_backward", "born_backward_bggrad"),
+    }
+    for prop, names in passes.items():
+        for pass_name in names:
             for dt in ("float", "double"):
                 ats = bu._template_argtypes(f"{prop}_{pass_name}", dt)
                 specs[f"{prop}_{pass_name}_{dt}"] = [a.__name__ for a in ats]
@@ -141,6 +149,9 @@ def abi_specs():
 
 
 def main():
+    if sys.argv[1:] == ["specs"]:  # only the loader's argtypes
+        abi_specs()
+        return
     abi_specs()
     out = {}
     n32 = config1(torch.float32, False)

@@ -1015,12 +1015,17 @@ template <typename T, typename S>
 void launch_fwd_step(const Launch3<T> &L, cudaStream_t st, const T *ca, const T *cb,
                      const T *cq, T *F[6], T *M[12], S *const snap[6], const T *f_t,
                      const int64_t *src_i, int64_t n_src, int64_t src_c, T *r_t,
-                     const int64_t *rec_i, int64_t n_rec, int64_t rec_c) {
+                     const int64_t *rec_i, int64_t n_rec, int64_t rec_c,
+                     ProfileScope *prof = nullptr, bool smp = false) {
+  if (smp) prof->begin(kK3FwdH);
   k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, F[0], F[1], F[2], F[3], F[4], F[5], M[6],
                                           M[7], M[8], M[9], M[10], M[11]);
+  if (smp) prof->end(kK3FwdH);
+  if (smp) prof->begin(kK3FwdE);
   k3_fwd_e<T, S><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, F[0], F[1], F[2], F[3], F[4], F[5],
                                              M[0], M[1], M[2], M[3], M[4], M[5], snap[0],
                                              snap[1], snap[2], snap[3], snap[4], snap[5]);
+  if (smp) prof->end(kK3FwdE);
   int n = 2;
   const int S_ = L.g.S;
   if (n_src > 0 && f_t && src_i) {
@@ -1065,10 +1070,12 @@ void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
   T *F[6] = {ex, ey, ez, hx, hy, hz};
   T *const none[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  ProfileScope ps(st);
   for (int64_t t = start_t; t < start_t + nt; ++t)
     launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, none, f ? f + t * fs : nullptr, sources_i,
                           n_sources_per_shot, source_component, r ? r + t * rs : nullptr,
-                          receivers_i, n_receivers_per_shot, receiver_component);
+                          receivers_i, n_receivers_per_shot, receiver_component, &ps,
+                          ps.sample(t));
   TB_CUDA(cudaGetLastError());
 }
 
@@ -1108,7 +1115,9 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
     return;
   T *F[6] = {ex, ey, ez, hx, hy, hz};
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  ProfileScope ps(st);
   for (int64_t t = start_t; t < start_t + nt; ++t) {
+    const bool smp = ps.sample(t);
     char *dst[6];
     if (!sr.begin(t, dst)) return;
     const T *ft = f ? f + t * fs : nullptr;
@@ -1119,13 +1128,13 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
                                     (__nv_bfloat16 *)dst[4], (__nv_bfloat16 *)dst[5]};
       launch_fwd_step<T, __nv_bfloat16>(L, st, ca, cb, cq, F, M, sp, ft, sources_i,
                                         n_sources_per_shot, source_component, rt, receivers_i,
-                                        n_receivers_per_shot, receiver_component);
+                                        n_receivers_per_shot, receiver_component, &ps, smp);
     } else {
       T *const sp[6] = {(T *)dst[0], (T *)dst[1], (T *)dst[2],
                         (T *)dst[3], (T *)dst[4], (T *)dst[5]};
       launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, sp, ft, sources_i, n_sources_per_shot,
                             source_component, rt, receivers_i, n_receivers_per_shot,
-                            receiver_component);
+                            receiver_component, &ps, smp);
     }
     if (!sr.end(t, dst)) return;
   }
@@ -1235,11 +1244,17 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
   const int S_ = (int)n_shots;
   int64_t launches = 0;
+  ProfileScope ps(st);
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    const bool smp = ps.sample(t);
+    if (smp) ps.begin(kK3AdjE);
     k3_adj_e<T><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez, lambda_hx,
                                             lambda_hy, lambda_hz, cur, nxt);
+    if (smp) ps.end(kK3AdjE);
+    if (smp) ps.begin(kK3AdjH);
     k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
                                             lambda_ex, lambda_ey, lambda_ez, cur, nxt);
+    if (smp) ps.end(kK3AdjH);
     launches += 2;
     if (n_receivers_per_shot > 0 && grad_r && receivers_i) {
       k3_adj_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
@@ -1290,6 +1305,7 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
         staged_used[ring] = true;
       }
       const T ks = (T)step_ratio;
+      if (smp) ps.begin(kK3Grad);
       if (bf16)
         k3_coeff_grad<T, __nv_bfloat16><<<L.grid, L.block, 0, st>>>(
             g, lambda_ex, lambda_ey, lambda_ez, (const __nv_bfloat16 *)src[0],
@@ -1301,6 +1317,7 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
             g, lambda_ex, lambda_ey, lambda_ez, (const T *)src[0], (const T *)src[1],
             (const T *)src[2], (const T *)src[3], (const T *)src[4], (const T *)src[5],
             grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
+      if (smp) ps.end(kK3Grad);
       ++launches;
     }
     std::swap(cur, nxt);

@@ -9,6 +9,9 @@
 
 #include "../../include/tide_b200.h"
 #include "tb_common.cuh"
+#include "tb_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 namespace tb {
 
@@ -141,6 +144,49 @@ void resolve_pending() {
   }
 }
 
+// Driver entry point of the tensor-map encoder, looked up once through the
+// runtime (no link-time dependence on libcuda).
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+}  // namespace
+
+bool encode_map_3d(CUtensorMap *map, const float *base, int64_t nx, int64_t ny, int64_t nz,
+                   int64_t pitch, int bx, int by) {
+  auto fn = encoder();
+  if (!fn) {
+    set_error(kCudaError, "cuTensorMapEncodeTiled is not available from the driver");
+    return false;
+  }
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)(pitch * ny) * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error(kCudaError,
+              "cuTensorMapEncodeTiled failed (%d): dims %lld x %lld x %lld, pitch %lld, box %d x %d",
+              (int)r, (long long)nx, (long long)ny, (long long)nz, (long long)pitch, bx, by);
+    return false;
+  }
+  return true;
+}
+
 }  // namespace tb
 
 extern "C" {
@@ -166,8 +212,9 @@ int tide_b200_profile_read(double *ms_out, int64_t *launches_out, int max_kinds)
 }
 
 const char *tide_b200_profile_kind_name(int kind) {
-  static const char *names[] = {"fwd_h", "fwd_e", "adj_e", "adj_h", "fwd_step",
-                                "adj_step"};
+  static const char *names[] = {"fwd_h",      "fwd_e",      "adj_e",      "adj_h",
+                                "fwd_step",   "adj_step",   "em3d_fwd_h", "em3d_fwd_e",
+                                "em3d_adj_e", "em3d_adj_h", "em3d_grad"};
   return (kind >= 0 && kind < tb::kKindCount) ? names[kind] : "";
 }
 

@@ -34,7 +34,12 @@ enum KernelKind : int {
   kKAdjH = 3,     // adjoint H-phase (+ points, gradient)
   kKFwdStep = 4,  // fused forward step (stencil 2)
   kKAdjStep = 5,  // fused adjoint step (stencil 2)
-  kKindCount = 6
+  kK3FwdH = 6,    // 3-D forward H half step
+  kK3FwdE = 7,    // 3-D forward E half step (+ snapshots)
+  kK3AdjE = 8,    // 3-D adjoint E-phase
+  kK3AdjH = 9,    // 3-D adjoint H-phase
+  kK3Grad = 10,   // 3-D coefficient gradient of an imaged step
+  kKindCount = 11
 };
 void count_launches(int64_t n);
 

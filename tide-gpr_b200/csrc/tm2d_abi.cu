@@ -24,6 +24,7 @@
 #include "tm2d_kernels.cuh"
 #include "tm2d_fused.cuh"
 #include "tm2d_s2.cuh"
+#include "tm2d_tma.cuh"
 #include "tb_store.cuh"
 
 namespace tb {
@@ -344,6 +345,216 @@ struct PitchedFwd {
 
 template <typename T> constexpr bool is_float() { return std::is_same<T, float>::value; }
 
+// ---------------------------------------------------------------------------
+// One-sweep TMA path (tm2d_tma.cuh): FP32, stencil 2, model coefficients
+// shared by the shots, no Debye poles.  A call copies its fields into two
+// pitched copies (ping-pong) and its coefficients into a pitched copy,
+// encodes the tensor maps of both copies once, runs one launch per time
+// step on P = min(SMs, tiles) persistent CTAs and copies the final state
+// back.  Mode (tide_b200_set_tma_mode): 0 off, 1 when the grid has at least
+// kQMinTiles tiles (default), 2 whenever eligible.
+std::atomic<int> g_tma_mode{1};
+std::atomic<int> g_tma_max_ctas{0};  // 0: one CTA per SM (tide_b200_set_tma_ctas)
+constexpr int kQTY = 32;        // tile height of the TMA kernels
+constexpr int kQMinTiles = 64;  // auto mode: below this the per-call kernels win
+
+template <bool ADJ> struct QRun {
+  using B = QBox<kQTY>;
+  cudaStream_t st = nullptr;
+  void *mem = nullptr;
+  int64_t pitch = 0, pshot = 0;
+  int nx = 0, ny = 0, S = 0, tiles_x = 0, tiles_y = 0, P = 0;
+  float *f[2][3] = {};  // pitched copies [set][Ey, Hx, Hz]
+  float *coef[3] = {};  // adjoint: ca, cb, cq; forward: cq, ca, cb
+  float *user[3] = {};  // caller's field arrays
+  QMaps maps[2];
+  int cur = 0;
+  // forward: H-phase memories ping-pong (caller's array and a copy)
+  float *mex[2] = {}, *mez[2] = {};
+  float *user_mex = nullptr, *user_mez = nullptr;
+  // adjoint: hand-off sums and flags
+  float *hand = nullptr;
+  int *flags = nullptr;
+  int epoch = 0;
+  ~QRun() {
+    if (mem) cudaFreeAsync(mem, st);
+  }
+
+  static bool eligible(const TMGeom<float> &g, int64_t nt) {
+    const int mode = g_tma_mode.load();
+    if (mode == 0 || nt <= 0 || g.ca_b || g.cb_b || g.cq_b) return false;
+    if (g.nx < 2 || g.ny < 2) return false;
+    const int64_t tiles = (int64_t)((g.nx + kQX - 1) / kQX) * ((g.ny + kQTY - 1) / kQTY);
+    if ((int64_t)g.n_shots * tiles > ((int64_t)1 << 30)) return false;
+    return mode == 2 || tiles >= kQMinTiles;
+  }
+
+  bool copy2d(float *dst, int64_t dpitch, const float *src, int64_t spitch, int64_t rows) {
+    return !TB_CUDA(cudaMemcpy2DAsync(dst, (size_t)dpitch * 4, src, (size_t)spitch * 4,
+                                      (size_t)nx * 4, (size_t)rows, cudaMemcpyDeviceToDevice, st));
+  }
+
+  // fields: caller's Ey, Hx, Hz (or lambda_*); c3: adjoint ca, cb, cq /
+  // forward cq, ca, cb; mex / mez: forward H-phase memories (null for the
+  // adjoint).
+  bool init(const TMGeom<float> &g, float *const fields[3], const float *const c3[3],
+            float *m_ey_x, float *m_ey_z, cudaStream_t s) {
+    st = s;
+    nx = g.nx; ny = g.ny; S = g.n_shots;
+    pitch = ((int64_t)nx + 31) / 32 * 32;
+    pshot = (int64_t)ny * pitch;
+    tiles_x = (nx + kQX - 1) / kQX;
+    tiles_y = (ny + kQTY - 1) / kQTY;
+    int dev = 0, n_sm = 0;
+    if (TB_CUDA(cudaGetDevice(&dev)) ||
+        TB_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev)))
+      return false;
+    const int cap = g_tma_max_ctas.load();
+    P = std::max(1, std::min(cap > 0 ? std::min(cap, n_sm) : n_sm, tiles_x * tiles_y));
+    const size_t state = (size_t)S * (size_t)pshot;
+    const size_t N = (size_t)ny * nx;
+    size_t total = 6 * state + 3 * (size_t)pshot;
+    if (ADJ) total += (size_t)P * 2 * kQTY * kQX + (size_t)P;
+    else total += 2 * (size_t)S * N;
+    if (TB_CUDA(cudaMallocAsync(&mem, total * sizeof(float), st))) return false;
+    float *p = static_cast<float *>(mem);
+    for (int k = 0; k < 2; ++k)
+      for (int i = 0; i < 3; ++i) {
+        f[k][i] = p;
+        p += state;
+      }
+    for (int i = 0; i < 3; ++i) {
+      coef[i] = p;
+      p += pshot;
+    }
+    for (int i = 0; i < 3; ++i) {
+      user[i] = fields[i];
+      if (!copy2d(f[0][i], pitch, fields[i], nx, (int64_t)S * ny)) return false;
+      if (!copy2d(coef[i], pitch, c3[i], nx, ny)) return false;
+    }
+    if (ADJ) {
+      hand = p;
+      p += (size_t)P * 2 * kQTY * kQX;
+      flags = reinterpret_cast<int *>(p);
+      if (TB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * (size_t)P, st))) return false;
+    } else {
+      user_mex = m_ey_x; user_mez = m_ey_z;
+      mex[0] = m_ey_x; mez[0] = m_ey_z;
+      mex[1] = p; p += (size_t)S * N;
+      mez[1] = p; p += (size_t)S * N;
+      // the copies start equal, so cells outside the strips (never written)
+      // agree in both
+      if (TB_CUDA(cudaMemcpyAsync(mex[1], m_ey_x, S * N * 4, cudaMemcpyDeviceToDevice, st)) ||
+          TB_CUDA(cudaMemcpyAsync(mez[1], m_ey_z, S * N * 4, cudaMemcpyDeviceToDevice, st)))
+        return false;
+    }
+    for (int k = 0; k < 2; ++k) {
+      QMaps &m = maps[k];
+      if (!encode_map_3d(&m.e, f[k][0], nx, ny, S, pitch, B::EW, B::EH) ||
+          !encode_map_3d(&m.x, f[k][1], nx, ny, S, pitch, B::XW, B::XH) ||
+          !encode_map_3d(&m.z, f[k][2], nx, ny, S, pitch, B::ZW, B::ZH))
+        return false;
+      if (ADJ) {
+        if (!encode_map_3d(&m.c0, coef[0], nx, ny, 1, pitch, B::OW, B::OH) ||
+            !encode_map_3d(&m.c1, coef[1], nx, ny, 1, pitch, B::EW, B::EH) ||
+            !encode_map_3d(&m.c2, coef[2], nx, ny, 1, pitch, B::QW, B::QH))
+          return false;
+      } else {
+        if (!encode_map_3d(&m.c0, coef[0], nx, ny, 1, pitch, B::QW, B::QH) ||
+            !encode_map_3d(&m.c1, coef[1], nx, ny, 1, pitch, B::OW, B::OH) ||
+            !encode_map_3d(&m.c2, coef[2], nx, ny, 1, pitch, B::OW, B::OH))
+          return false;
+      }
+    }
+    return true;
+  }
+
+  QCommon common(const TMGeom<float> &g, const PointScratch &ps, const float *v0,
+                 float *v1) const {
+    QCommon c{};
+    c.g = g;
+    c.tiles_x = tiles_x; c.tiles_y = tiles_y; c.P = P;
+    c.pitch = pitch; c.pshot = pshot;
+    c.ey_n = f[cur ^ 1][0]; c.hx_n = f[cur ^ 1][1]; c.hz_n = f[cur ^ 1][2];
+    c.p0 = ADJ ? ps.rec : ps.src;
+    c.p1 = ADJ ? ps.src : ps.rec;
+    c.v0 = v0; c.v1 = v1;
+    return c;
+  }
+
+  // Opt the kernel into its dynamic shared memory once per device.
+  template <typename SN> bool prepare() const {
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    if (TB_CUDA(cudaGetDevice(&dev))) return false;
+    const uint64_t bit = uint64_t(1) << (dev & 63);
+    if (done.load() & bit) return true;
+    const cudaError_t e =
+        ADJ ? cudaFuncSetAttribute(kq_adj_step<kQTY, SN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   B::smem_bytes(true))
+            : cudaFuncSetAttribute(kq_fwd_step<kQTY, SN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   B::smem_bytes(false));
+    if (TB_CUDA(e)) return false;
+    done.fetch_or(bit);
+    return true;
+  }
+
+  // One forward step: E-phase memories m_hx_z / m_hz_x in place.
+  template <typename SN>
+  bool fwd_step(const TMGeom<float> &g, const PointScratch &ps, const float *ft, float *rt,
+                float *mhx, float *mhz, SN *e_st, SN *c_st) {
+    if (!prepare<SN>()) return false;
+    QFwdArgs a{};
+    a.c = common(g, ps, ft, rt);
+    a.mex_c = mex[cur]; a.mez_c = mez[cur];
+    a.mex_n = mex[cur ^ 1]; a.mez_n = mez[cur ^ 1];
+    a.mhx = mhx; a.mhz = mhz;
+    a.ey_st = e_st; a.cu_st = c_st;
+    kq_fwd_step<kQTY, SN><<<P, kQThreads, B::smem_bytes(false), st>>>(maps[cur], a);
+    cur ^= 1;
+    return true;
+  }
+
+  // One adjoint step; mem_c / mem_n: the l-memories (hz_x, hx_z, ey_x, ey_z)
+  // read / written.
+  template <typename SN>
+  bool adj_step(const TMGeom<float> &g, const PointScratch &ps, const float *grt, float *gft,
+                const float *const mem_c[4], float *const mem_n[4], const SN *e_st,
+                const SN *c_st, int bg_shots, float *grad_ca, float *grad_cb, float kscale) {
+    if (!prepare<SN>()) return false;
+    QAdjArgs a{};
+    a.c = common(g, ps, grt, gft);
+    a.mhz_c = mem_c[0]; a.mhx_c = mem_c[1]; a.mex_c = mem_c[2]; a.mez_c = mem_c[3];
+    a.mhz_n = mem_n[0]; a.mhx_n = mem_n[1]; a.mex_n = mem_n[2]; a.mez_n = mem_n[3];
+    a.ey_st = e_st; a.cu_st = c_st;
+    a.bg_shots = bg_shots;
+    a.grad_ca = grad_ca; a.grad_cb = grad_cb;
+    a.kscale = kscale;
+    a.hand = hand; a.flags = flags;
+    a.epoch = ++epoch;
+    kq_adj_step<kQTY, SN><<<P, kQThreads, B::smem_bytes(true), st>>>(maps[cur], a);
+    cur ^= 1;
+    return true;
+  }
+
+  // Copy the final state back into the caller's arrays.
+  bool finish() {
+    for (int i = 0; i < 3; ++i)
+      if (!copy2d(user[i], nx, f[cur][i], pitch, (int64_t)S * ny)) return false;
+    if (!ADJ && mex[cur] != user_mex) {
+      const size_t nb = (size_t)S * ny * nx * 4;
+      if (TB_CUDA(cudaMemcpyAsync(user_mex, mex[cur], nb, cudaMemcpyDeviceToDevice, st)) ||
+          TB_CUDA(cudaMemcpyAsync(user_mez, mez[cur], nb, cudaMemcpyDeviceToDevice, st)))
+        return false;
+    }
+    return true;
+  }
+  PointTiles point_tiles() const { return PointTiles{tiles_x, tiles_y, kQX, kQTY, 0}; }
+};
+
+
 // The two-kernel forward re-reads H and Ey between its half steps; while the
 // three fields of a call fit in about half of the 126 MB L2 those re-reads
 // are L2 hits and the two-kernel path is the faster one (measured on the
@@ -379,6 +590,31 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
   cudaStream_t st = as_stream(compute_stream);
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   if constexpr (is_float<T>() && ST == 2) {
+    if (db.n_poles == 0 && L.has_domain && QRun<false>::eligible(L.g, nt)) {
+      // One-sweep TMA path.
+      QRun<false> qr;
+      float *const fl[3] = {ey, hx, hz};
+      const float *const c3[3] = {cq, ca, cb};
+      if (!qr.init(L.g, fl, c3, m_ey_x, m_ey_z, st)) return;
+      PointScratch ps;
+      if (!build_points(ps, L, qr.point_tiles(), sources_i, n_sources_per_shot, receivers_i,
+                        n_receivers_per_shot, st))
+        return;
+      ProfileScope prof(st);
+      for (int64_t t = start_t; t < start_t + nt; ++t) {
+        const bool smp = prof.sample(t);
+        if (smp) prof.begin(kKFwdStep);
+        if (!qr.template fwd_step<float>(L.g, ps, f ? f + t * fs : nullptr,
+                                         r ? r + t * rs : nullptr, m_hx_z, m_hz_x, nullptr,
+                                         nullptr))
+          return;
+        if (smp) prof.end(kKFwdStep);
+      }
+      count_launches(nt);
+      if (TB_CUDA(cudaGetLastError())) return;
+      qr.finish();
+      return;
+    }
     if (db.n_poles == 0 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N)) {
       // Fused one-launch-per-step path.
       PitchedFwd pf;
@@ -447,18 +683,28 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
-  // one launch per step (see fused_pays)
-  const bool fused = is_float<T>() && ST == 2 && L.has_domain && nt > 0 && fused_pays(n_shots, L.g.N);
+  // one launch per step: the TMA path, else the pitched fused path (see fused_pays)
+  bool qpath = false;
+  if constexpr (is_float<T>() && ST == 2) qpath = L.has_domain && QRun<false>::eligible(L.g, nt);
+  const bool fused = !qpath && is_float<T>() && ST == 2 && L.has_domain && nt > 0 &&
+                     fused_pays(n_shots, L.g.N);
   PitchedFwd pf;
+  QRun<false> qr;
   if constexpr (is_float<T>()) {
     float *const fields[7] = {ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x};
     if (fused && !pf.init(L.g, fields, ca, cb, cq, st)) return;
+    float *const fl[3] = {ey, hx, hz};
+    const float *const c3[3] = {cq, ca, cb};
+    if (qpath && !qr.init(L.g, fl, c3, m_ey_x, m_ey_z, st)) return;
   }
   PointScratch ps;
-  if (!(fused ? build_points(ps, L, pf.q.pt, sources_i, n_sources_per_shot, receivers_i,
-                             n_receivers_per_shot, st)
-              : build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0}, sources_i,
-                             n_sources_per_shot, receivers_i, n_receivers_per_shot, st)))
+  if (!(qpath   ? build_points(ps, L, qr.point_tiles(), sources_i, n_sources_per_shot,
+                               receivers_i, n_receivers_per_shot, st)
+        : fused ? build_points(ps, L, pf.q.pt, sources_i, n_sources_per_shot, receivers_i,
+                               n_receivers_per_shot, st)
+                : build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+                               sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot,
+                               st)))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
@@ -472,7 +718,19 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     char *const e1 = dst[0], *const c1 = dst[1];
     const T *ft = f ? f + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
-    if (fused) {
+    if (qpath) {
+      if (smp) prof.begin(kKFwdStep);
+      if constexpr (is_float<T>()) {
+        const bool ok =
+            (store_step && bf16)
+                ? qr.template fwd_step<__nv_bfloat16>(L.g, ps, ft, rt, m_hx_z, m_hz_x,
+                                                      (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1)
+                : qr.template fwd_step<float>(L.g, ps, ft, rt, m_hx_z, m_hz_x, (float *)e1,
+                                              (float *)c1);
+        if (!ok) return;
+      }
+      if (smp) prof.end(kKFwdStep);
+    } else if (fused) {
       if (smp) prof.begin(kKFwdStep);
       if constexpr (is_float<T>()) {
         if (store_step && bf16)
@@ -499,10 +757,11 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     }
     if (!sr.end(t, dst)) return;
   }
-  count_launches(fused ? nt : nt * (L.has_domain ? 2 : 1));
+  count_launches((fused || qpath) ? nt : nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
   if constexpr (is_float<T>()) {
     if (fused && !pf.finish()) return;
+    if (qpath && !qr.finish()) return;
   }
   sr.finish();
 }
@@ -516,8 +775,12 @@ bool zero_band(T *m, const TMGeom<T> &g, int axis, int lo, int hi, cudaStream_t 
   return !TB_CUDA(cudaGetLastError());
 }
 
+// Exact adjoint (backward) and its background-reuse form: with
+// background_n_shots < n_shots the snapshot history holds background_n_shots
+// shots and adjoint shot s images against snapshot shot s %
+// background_n_shots (maxwell_tm_cuda_inst.cu:2405-2460, 651-660).
 template <typename T, int ST>
-void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
+void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
   (void)dt; (void)n_threads; (void)ey_filenames; (void)curl_filenames;
   (void)grad_ca_shot; (void)grad_cb_shot;  // gradients are reduced in-kernel (see k_adj_h)
   if (TB_CUDA(cudaSetDevice((int)device))) return;
@@ -527,6 +790,10 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
                  m_lambda_ey_z && m_lambda_hx_z && m_lambda_hz_x && adjoint_memory_scratch,
              "TM2D backward: a field or coefficient pointer is null");
   TB_REQUIRE(n_receivers_per_shot == 0 || grad_r, "TM2D backward: receivers without grad_r");
+  TB_REQUIRE(background_n_shots >= 1 && n_shots % background_n_shots == 0,
+             "TM2D backward: n_shots (%lld) must be a multiple of background_n_shots (%lld)",
+             (long long)n_shots, (long long)background_n_shots);
+  const int bg_shots = (int)background_n_shots;
   const bool bf16 = storage_format == 1;
   TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
   const bool grads = (ca_requires_grad || cb_requires_grad) && storage_mode != 3;
@@ -551,6 +818,15 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     return;
   if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
   cudaStream_t st = as_stream(compute_stream);
+  // one launch per step on the TMA path (float, stencil 2, unbatched)
+  bool qpath = false;
+  if constexpr (is_float<T>() && ST == 2) qpath = L.has_domain && QRun<true>::eligible(L.g, nt);
+  QRun<true> qr;
+  if constexpr (is_float<T>()) {
+    float *const fl[3] = {lambda_ey, lambda_hx, lambda_hz};
+    const float *const c3[3] = {ca, cb, cq};
+    if (qpath && !qr.init(L.g, fl, c3, nullptr, nullptr, st)) return;
+  }
   cudaStream_t ss = as_stream(storage_stream);
   const bool host_side = grads && (storage_mode == 1 || storage_mode == 2);
   const bool pipeline = host_side && ss != nullptr && ss != st;
@@ -584,8 +860,8 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
       !zero_band(m_lambda_ey_z, L.g, 0, L.g.pml_y0, L.g.pml_y1h, st))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, L.ah_tiles(), sources_i, n_sources_per_shot, receivers_i,
-                    n_receivers_per_shot, st))
+  if (!build_points(ps, L, qpath ? qr.point_tiles() : L.ah_tiles(), sources_i,
+                    n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
 
   // Store indices consumed by this call, latest first.
@@ -593,7 +869,7 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   if (grads)
     for (int64_t t = start_t - 1; t >= start_t - nt; --t)
       if (t % step_ratio == 0) qs.push_back(t / step_ratio);
-  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)bg_shots;
   EventRing loaded, consumed;
   if (pipeline && (!loaded.ok || !consumed.ok)) {
     set_error(kCudaError, "TM2D: event creation failed");
@@ -648,6 +924,43 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
   ProfileScope prof(st);
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
     const bool smp = prof.sample(t);
+    if constexpr (is_float<T>()) {
+      if (qpath) {
+        const bool grad_step = grads && t % step_ratio == 0;
+        const int64_t q = t / step_ratio;
+        const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
+                                              : (size_t)(q % kRing) * step_bytes;
+        if (grad_step && pipeline &&
+            TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0)))
+          return;
+        const char *es = grad_step && ca_requires_grad ? (const char *)ey_store_1 + off1 : nullptr;
+        const char *cs = grad_step && cb_requires_grad ? (const char *)curl_store_1 + off1 : nullptr;
+        const float *const mc[4] = {cur_hz_x, cur_hx_z, cur_ey_x, cur_ey_z};
+        float *const mn[4] = {nxt_hz_x, nxt_hx_z, nxt_ey_x, nxt_ey_z};
+        const float *grt = grad_r ? grad_r + t * rs : nullptr;
+        float *gft = grad_f ? grad_f + t * fs : nullptr;
+        if (smp) prof.begin(kKAdjStep);
+        const bool ok =
+            bf16 ? qr.template adj_step<__nv_bfloat16>(
+                       L.g, ps, grt, gft, mc, mn, (const __nv_bfloat16 *)es,
+                       (const __nv_bfloat16 *)cs, bg_shots, grad_ca, grad_cb, (float)step_ratio)
+                 : qr.template adj_step<float>(L.g, ps, grt, gft, mc, mn, (const float *)es,
+                                               (const float *)cs, bg_shots, grad_ca, grad_cb,
+                                               (float)step_ratio);
+        if (!ok) return;
+        if (smp) prof.end(kKAdjStep);
+        std::swap(cur_hx_z, nxt_hx_z);
+        std::swap(cur_hz_x, nxt_hz_x);
+        std::swap(cur_ey_x, nxt_ey_x);
+        std::swap(cur_ey_z, nxt_ey_z);
+        if (grad_step && host_side) {
+          ++next_q;
+          if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
+          if (!load(next_q + 1)) return;
+        }
+        continue;
+      }
+    }
     if (L.has_domain) {
       if (smp) prof.begin(kKAdjE);
       launch_adj_e<T, ST>(L, st, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x,
@@ -670,13 +983,14 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (smp) prof.begin(kKAdjH);
     if (bf16) {
       GradArgs<T, __nv_bfloat16> ga{(const __nv_bfloat16 *)es, (const __nv_bfloat16 *)cs,
-                                    grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched};
+                                    grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched,
+                                    bg_shots};
       launch_adj_h<T, ST, __nv_bfloat16>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey,
                                          cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft,
                                          ga);
     } else {
       GradArgs<T, T> ga{(const T *)es, (const T *)cs, grad_ca, grad_cb, (T)step_ratio,
-                        ca_batched, cb_batched};
+                        ca_batched, cb_batched, bg_shots};
       launch_adj_h<T, ST, T>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x,
                              cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft, ga);
     }
@@ -702,8 +1016,11 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
     if (TB_CUDA(cudaMemcpyAsync(m_lambda_hz_x, cur_hz_x, nbytes, cudaMemcpyDeviceToDevice, st)))
       return;
   }
-  count_launches(nt * (L.has_domain ? 2 : 1));
+  count_launches(qpath ? nt : nt * (L.has_domain ? 2 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
+  if constexpr (is_float<T>()) {
+    if (qpath && !qr.finish()) return;
+  }
   if (pipeline) TB_CUDA(cudaStreamSynchronize(ss));
   // disk mode: the staging ring is the caller's and is refilled by the next
   // call, so every copy out of it has finished before returning
@@ -742,7 +1059,21 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T)) {
         sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,        \
         n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
         ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,      \
-        pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);   \
+        pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream,    \
+        n_shots);                                                              \
+  }                                                                            \
+  extern "C" void maxwell_tm_##S##_##T##_background_vjp_reuse_cuda(            \
+      TIDE_TM_BACKGROUND_VJP_REUSE_ARGS(T)) {                                  \
+    tb::tm_backward<T, S>(                                                     \
+        ca, cb, cq, grad_r, lambda_ey, lambda_hx, lambda_hz, m_lambda_ey_x, m_lambda_ey_z,    \
+        m_lambda_hx_z, m_lambda_hz_x, adjoint_memory_scratch, ey_store_1, ey_store_3,         \
+        ey_filenames, curl_store_1, curl_store_3, curl_filenames, grad_f, grad_ca, grad_cb,   \
+        grad_ca_shot, grad_cb_shot, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh,     \
+        sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,        \
+        n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
+        ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,      \
+        pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream,    \
+        background_n_shots);                                                   \
   }
 
 TB_DEFINE(2, float)
@@ -753,6 +1084,14 @@ TB_DEFINE(2, double)
 TB_DEFINE(4, double)
 TB_DEFINE(6, double)
 TB_DEFINE(8, double)
+
+extern "C" int tide_b200_set_tma_ctas(int max_ctas) {
+  return tb::g_tma_max_ctas.exchange(max_ctas < 0 ? 0 : max_ctas);
+}
+
+extern "C" int tide_b200_set_tma_mode(int mode) {
+  return tb::g_tma_mode.exchange(mode < 0 ? 0 : (mode > 2 ? 2 : mode));
+}
 
 extern "C" int64_t tide_b200_set_fused_threshold(int64_t bytes) {
   return tb::g_fused_min_bytes.exchange(bytes < 0 ? -1 : bytes);

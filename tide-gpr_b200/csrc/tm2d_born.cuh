@@ -339,7 +339,8 @@ void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
                      n_shots, ny, nx, n_sources_per_shot, n_receivers_per_shot, step_ratio,
                      storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad,
                      cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t, pml_y0,
-                     pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);
+                     pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream,
+                     n_shots);
   TB_CUDA(cudaFreeAsync(scratch, st));
 }
 

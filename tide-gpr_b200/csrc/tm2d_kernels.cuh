@@ -582,6 +582,12 @@ template <typename T, typename S> struct GradArgs {
   T *grad_cb;
   T kscale;        // gradient sampling interval as T
   bool batched_ca, batched_cb;
+  // Shots of the snapshot history: adjoint shot s images against snapshot
+  // shot s % bg_shots (background_vjp_reuse); 0 = one snapshot per shot.
+  int bg_shots = 0;
+  __device__ __forceinline__ int64_t snap_base(int s, int64_t N) const {
+    return (int64_t)(bg_shots > 0 ? s % bg_shots : s) * N;
+  }
 };
 
 // Adjoint H-phase update of one cell (general path: strips, domain edges).
@@ -683,6 +689,7 @@ k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
   const int j0 = y0 * g.nx + x;
   for (int s = 0; s < g.n_shots; ++s) {
     const int64_t base = (int64_t)s * g.N;
+    const int64_t sbase = ga.snap_base(s, g.N);
     const int tile = s * tiles_per_shot + tile_xy;
     const bool pts = !point_tile_empty(src, rec, tile);
     T lam[R];
@@ -715,12 +722,12 @@ k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
       if (pts) point_record(src, tile, j, gf_t, v);
       if (imaging && dom[r]) {
         if (ga.ey_st) {
-          const T t = v * Codec<S, T>::dec(load_stream(ga.ey_st + i)) * ga.kscale;
+          const T t = v * Codec<S, T>::dec(load_stream(ga.ey_st + sbase + j)) * ga.kscale;
           if (ga.batched_ca) ga.grad_ca[i] = ga.grad_ca[i] + t;
           else sum_ca[r] = sum_ca[r] + t;
         }
         if (ga.cu_st) {
-          const T t = v * Codec<S, T>::dec(load_stream(ga.cu_st + i)) * ga.kscale;
+          const T t = v * Codec<S, T>::dec(load_stream(ga.cu_st + sbase + j)) * ga.kscale;
           if (ga.batched_cb) ga.grad_cb[i] = ga.grad_cb[i] + t;
           else sum_cb[r] = sum_cb[r] + t;
         }

@@ -431,13 +431,14 @@ __device__ __forceinline__ void adj_h_interior_group(
 #pragma unroll
     for (int r = 0; r <= R; ++r) hxz[u][r] = ldg(lam_hx + base + j0 + (r - 1) * nx);
 #pragma unroll
+    const int64_t sbase = ga.snap_base(s0 + u, g.N);
     for (int r = 0; r < R; ++r) {
       const int64_t i = base + j0 + r * nx;
       lam[u][r] = lam_ey[i];
       hzx[u][r] = ldg(lam_hz + i);
       hzl[u][r] = ldg(lam_hz + i - 1);
-      ev[u][r] = ga.ey_st ? load_stream(ga.ey_st + i) : S(0.f);
-      cv[u][r] = ga.cu_st ? load_stream(ga.cu_st + i) : S(0.f);
+      ev[u][r] = ga.ey_st ? load_stream(ga.ey_st + sbase + j0 + r * nx) : S(0.f);
+      cv[u][r] = ga.cu_st ? load_stream(ga.cu_st + sbase + j0 + r * nx) : S(0.f);
     }
   }
 #pragma unroll
@@ -585,8 +586,9 @@ __device__ __forceinline__ void adj_h_tile(
     const T *lhx = lam_hx + base, *lhz = lam_hz + base, *mex = m_ey_x + base;
     const T *mez = m_ey_z + base;
     T *ley = lam_ey + base;
-    const S *est = ga.ey_st ? ga.ey_st + base : nullptr;
-    const S *cst = ga.cu_st ? ga.cu_st + base : nullptr;
+    const int64_t sbase = ga.snap_base(s, g.N);
+    const S *est = ga.ey_st ? ga.ey_st + sbase : nullptr;
+    const S *cst = ga.cu_st ? ga.cu_st + sbase : nullptr;
     // ---- loads for this shot
     T hxz[R + 1], mz[R + 1], cz[R + 1], hzx[R], hzl[R], mx[R], ml[R], lam[R], as[R];
     T cx[R], cl[R];

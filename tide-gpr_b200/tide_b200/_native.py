@@ -71,6 +71,11 @@ SPECS: dict[str, list] = {
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6), (_P, 1), (_P, 2), (_P, 2),
         *_TM_PROFILES, *_TM_TAIL, *_TM_STORAGE, *_TM_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:310-334 (backward + background_n_shots)
+    "maxwell_tm_background_vjp_reuse": [
+        (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6), (_P, 1), (_P, 2), (_P, 2),
+        *_TM_PROFILES, *_TM_TAIL, (_I, 4), (_B, 2), *_TM_FLAGS, (_P, 2),
+    ],
 }
 
 _3D_TAIL = [(_FLOAT, 3), (_FLOAT, 1), (_I, 1), (_I, 1), (_I, 3), (_I, 2), (_I, 1)]
@@ -189,6 +194,23 @@ def set_fused_threshold(nbytes: int) -> int:
     return int(lib.tide_b200_set_fused_threshold(int(nbytes)))
 
 
+def set_tma_mode(mode: int) -> int:
+    """One-sweep TMA time steps: 0 never, 1 on grids of at least 64 tiles
+    (default), 2 whenever eligible; returns the previous mode."""
+    lib = load()
+    lib.tide_b200_set_tma_mode.argtypes = [ctypes.c_int]
+    lib.tide_b200_set_tma_mode.restype = ctypes.c_int
+    return int(lib.tide_b200_set_tma_mode(int(mode)))
+
+
+def set_tma_ctas(max_ctas: int) -> int:
+    """Upper bound on the TMA path's persistent CTAs (0: one per SM)."""
+    lib = load()
+    lib.tide_b200_set_tma_ctas.argtypes = [ctypes.c_int]
+    lib.tide_b200_set_tma_ctas.restype = ctypes.c_int
+    return int(lib.tide_b200_set_tma_ctas(int(max_ctas)))
+
+
 def ptr(t: torch.Tensor | None) -> int:
     if t is None or t.numel() == 0:
         return 0
@@ -206,7 +228,7 @@ def exported_symbols() -> list[str]:
         symbol_name("maxwell_tm", p, a, d)
         for a in ACCURACIES
         for d in ("float", "double")
-        for p in ("born_forward", "born_forward_with_storage",
+        for p in ("background_vjp_reuse", "born_forward", "born_forward_with_storage",
                   "born_tangent_forward_with_storage", "born_backward")
     ] + [
         symbol_name("maxwell_3d", "born_forward", a, d)
@@ -225,6 +247,8 @@ def exported_symbols() -> list[str]:
         "tide_b200_clear_error",
         "tide_b200_device_status",
         "tide_b200_set_fused_threshold",
+        "tide_b200_set_tma_mode",
+        "tide_b200_set_tma_ctas",
         "tide_b200_launch_count",
         "tide_b200_profile_enable",
         "tide_b200_profile_read",

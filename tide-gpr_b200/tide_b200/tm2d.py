@@ -458,9 +458,15 @@ class _AdjointState:
 
 
 def _backward_call(pb, ca, cb, grad_r, st: _AdjointState, ptrs, mode, fmt, shot_bytes, need_ca,
-                   need_cb, start_t, n, side=None):
-    """One backward call over t = start_t-1 down to start_t-n."""
-    fn = nat.get_backend_function("maxwell_tm", "backward", pb.stencil, pb.dtype, pb.device)
+                   need_cb, start_t, n, side=None, bg_shots=None):
+    """One backward call over t = start_t-1 down to start_t-n.  With
+    bg_shots (< n_shots) the snapshot history holds bg_shots shots and shot s
+    images against snapshot shot s % bg_shots (the background_vjp_reuse
+    entry point)."""
+    reuse = bg_shots is not None and bg_shots != pb.n_shots
+    fn = nat.get_backend_function("maxwell_tm", "background_vjp_reuse" if reuse else "backward",
+                                  pb.stencil, pb.dtype, pb.device)
+    storage = (mode, fmt, shot_bytes, bg_shots) if reuse else (mode, fmt, shot_bytes)
     fn(
         nat.ptr(ca), nat.ptr(cb), nat.ptr(pb.cq), nat.ptr(grad_r),
         *[nat.ptr(t) for t in st.lam], nat.ptr(st.scratch),
@@ -468,7 +474,7 @@ def _backward_call(pb, ca, cb, grad_r, st: _AdjointState, ptrs, mode, fmt, shot_
         nat.ptr(st.grad_f), nat.ptr(st.grad_ca), nat.ptr(st.grad_cb), nat.ptr(st.shot_ca),
         nat.ptr(st.shot_cb), *_profile_ptrs(pb), nat.ptr(pb.sources_i), nat.ptr(pb.receivers_i),
         pb.rdy, pb.rdx, pb.dt, n, pb.n_shots, pb.ny, pb.nx, pb.n_src, pb.n_rec, pb.grad_interval,
-        mode, fmt, shot_bytes, need_ca, need_cb, pb.batched, pb.batched, pb.batched, start_t,
+        *storage, need_ca, need_cb, pb.batched, pb.batched, pb.batched, start_t,
         pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0, pb.device.index or 0,
         _stream_handle(pb.device), int(side.cuda_stream) if side is not None else 0,
     )
@@ -495,7 +501,7 @@ def _adjoint_callback(pb, st: _AdjointState, bwd_cb, step, need_ca, need_cb):
     ))
 
 
-def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts):
+def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts, bg_shots=None):
     grad_r = _grad_r(pb, grad_r)
     nt = pb.nt
     st = _AdjointState(pb, need_ca, need_cb)
@@ -511,7 +517,7 @@ def _run_backward(pb, ca, cb, grad_r, snaps, need_ca, need_cb, need_f, opts):
         n = min(chunk, start_t)
         _backward_call(pb, ca, cb, grad_r, st, ptrs, mode, fmt, shot_bytes,
                        need_ca and snaps is not None, need_cb and snaps is not None, start_t, n,
-                       side)
+                       side, bg_shots)
         if bwd_cb:
             _adjoint_callback(pb, st, bwd_cb, start_t - n, need_ca, need_cb)
     return st.result(pb, need_ca, need_cb, need_f)
