@@ -385,8 +385,17 @@ void maxwell_tm_2_float_forward_noalloc_cuda(TIDE_TM_FORWARD_ARGS(float));
       TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T));                                   \
   void maxwell_3d_##S##_##T##_backward_cuda(TIDE_3D_BACKWARD_ARGS(T));
 
+/* Stencil orders 2, 4, 6, 8 (S): the update domain is [S/2, n - S/2 + 1)
+ * per axis, with the model padded by S/2 cells before and S/2 - 1 after it
+ * (maxwell3d_cuda.py:314-326). */
 TIDE_3D_DECLARE(2, float)
 TIDE_3D_DECLARE(2, double)
+TIDE_3D_DECLARE(4, float)
+TIDE_3D_DECLARE(4, double)
+TIDE_3D_DECLARE(6, float)
+TIDE_3D_DECLARE(6, double)
+TIDE_3D_DECLARE(8, float)
+TIDE_3D_DECLARE(8, double)
 
 /* maxwell_3d_*_born_forward_cuda, the 3-D Born (tangent) propagation.
  * Replaces maxwell_3d_{S}_{dtype}_born_forward_cuda (CPU counterpart
@@ -417,8 +426,16 @@ TIDE_3D_DECLARE(2, double)
       int64_t source_component, int64_t receiver_component, int64_t n_threads, \
       int64_t device, int64_t execution_backend, void *compute_stream
 
-void maxwell_3d_2_float_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(float));
-void maxwell_3d_2_double_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(double));
+#define TIDE_3D_BORN_DECLARE(S, T) \
+  void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T));
+TIDE_3D_BORN_DECLARE(2, float)
+TIDE_3D_BORN_DECLARE(2, double)
+TIDE_3D_BORN_DECLARE(4, float)
+TIDE_3D_BORN_DECLARE(4, double)
+TIDE_3D_BORN_DECLARE(6, float)
+TIDE_3D_BORN_DECLARE(6, double)
+TIDE_3D_BORN_DECLARE(8, float)
+TIDE_3D_BORN_DECLARE(8, double)
 
 /* Comma-separated CUDA architectures the library was built for ("100a").
  * Replaces tide_cuda_arches, src/tide/csrc/storage/storage_utils.cu:213. */

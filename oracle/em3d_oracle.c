@@ -9,6 +9,12 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Stencil order of every following call (2, 4, 6 or 8). */
+static int g_em3d_stencil = 2;
+void tide_oracle_em3d_set_stencil(int st) {
+  g_em3d_stencil = (st == 4 || st == 6 || st == 8) ? st : 2;
+}
+
 #define REAL float
 #define SFX float
 #include "em3d_oracle_impl.h"

@@ -3,7 +3,10 @@
  *
  * Included twice by em3d_oracle.c (REAL = float / double, SFX names the
  * instantiation).  Plain sequential C restating the reference's arithmetic
- * for stencil order 2:
+ * for stencil orders 2, 4, 6 and 8 (set by tide_oracle_em3d_set_stencil;
+ * staggered differences and their transposes as
+ * src/tide/csrc/common/staggered_grid.h:7-230, update domain
+ * [FD_PAD, n - FD_PAD + 1) per axis with FD_PAD = order / 2):
  *
  *   forward H update        src/tide/csrc/em3d/maxwell_3d_inst.cpp:560-632
  *   forward E update        src/tide/csrc/em3d/maxwell_3d_inst.cpp:646-702
@@ -42,6 +45,7 @@ typedef struct {
   int64_t z1h, y1h, x1h;           /* half-grid strips:    c < c0 || c >= c1h */
   const REAL *p[18];
   int ca_b, cb_b, cq_b;
+  int st, P;  /* stencil order, FD_PAD */
 } FN(g3);
 
 #ifndef EM3D_ORACLE_ENUMS
@@ -52,68 +56,110 @@ enum { L_EY_Z, L_EZ_Y, L_EZ_X, L_EX_Z, L_EX_Y, L_EY_X, L_HZ_Y, L_HY_Z, L_HX_Z, L
 #endif
 
 static inline int FN(active)(const FN(g3) * g, int64_t z, int64_t y, int64_t x) {
-  return z >= 1 && z < g->nz && y >= 1 && y < g->ny && x >= 1 && x < g->nx;
+  const int64_t P = g->P;
+  return z >= P && z < g->nz - P + 1 && y >= P && y < g->ny - P + 1 && x >= P &&
+         x < g->nx - P + 1;
 }
 static inline int64_t FN(mi)(const FN(g3) * g, int64_t s, int64_t z, int64_t y, int64_t x) {
   return ((s * g->nz + z) * g->ny + y) * g->nx + x;
+}
+
+/* Staggered-grid coefficient m of an order-st difference. */
+static inline REAL FN(cf)(int st, int m) {
+  switch (st) {
+    case 4: return m == 0 ? (REAL)(9.0 / 8.0) : (REAL)(-1.0 / 24.0);
+    case 6: return m == 0 ? (REAL)(75.0 / 64.0) : m == 1 ? (REAL)(-25.0 / 384.0) : (REAL)(3.0 / 640.0);
+    case 8:
+      return m == 0 ? (REAL)(1225.0 / 1024.0)
+             : m == 1 ? (REAL)(-245.0 / 3072.0)
+             : m == 2 ? (REAL)(49.0 / 5120.0)
+                      : (REAL)(-5.0 / 7168.0);
+    default: return (REAL)1;
+  }
+}
+/* Integer-grid difference (DIFF?1) of f at flat index i along stride sd. */
+static inline REAL FN(d1)(const FN(g3) * g, const REAL *f, int64_t i, int64_t sd, REAL rd) {
+  if (g->st == 2) return (f[i] - f[i - sd]) * rd;
+  REAL acc = FN(cf)(g->st, 0) * (f[i] - f[i - sd]);
+  for (int m = 1; m < g->P; ++m) acc = acc + FN(cf)(g->st, m) * (f[i + m * sd] - f[i - (m + 1) * sd]);
+  return acc * rd;
+}
+/* Half-grid difference (DIFF?H1). */
+static inline REAL FN(dh)(const FN(g3) * g, const REAL *f, int64_t i, int64_t sd, REAL rd) {
+  if (g->st == 2) return (f[i + sd] - f[i]) * rd;
+  REAL acc = FN(cf)(g->st, 0) * (f[i + sd] - f[i]);
+  for (int m = 1; m < g->P; ++m) acc = acc + FN(cf)(g->st, m) * (f[i + (m + 1) * sd] - f[i - m * sd]);
+  return acc * rd;
+}
+/* Transpose of a difference over raw terms (DIFF?1_ADJ(C, 1) and
+ * DIFF?H1_ADJ(C, 1)): r[P - 1 - m] and r[P + m] are the raw terms paired by
+ * coefficient m (offsets -m and m + 1 for the integer grid, -m - 1 and m for
+ * the half grid; r holds offsets from -P + 1, resp. -P). */
+static inline REAL FN(tadj)(const FN(g3) * g, const REAL *r, REAL rd) {
+  const int P = g->P;
+  if (g->st == 2) return (r[P - 1] * (REAL)1 - r[P] * (REAL)1) * rd;
+  REAL acc = FN(cf)(g->st, 0) * (r[P - 1] * (REAL)1 - r[P] * (REAL)1);
+  for (int m = 1; m < P; ++m)
+    acc = acc + FN(cf)(g->st, m) * (r[P - 1 - m] * (REAL)1 - r[P + m] * (REAL)1);
+  return acc * rd;
 }
 
 static void FN(step_h)(const FN(g3) * g, const REAL *cq, REAL **F, REAL **M) {
   REAL *ex = F[0], *ey = F[1], *ez = F[2], *hx = F[3], *hy = F[4], *hz = F[5];
   REAL *m_ey_z = M[6], *m_ez_y = M[7], *m_ez_x = M[8], *m_ex_z = M[9], *m_ex_y = M[10],
        *m_ey_x = M[11];
-  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  const int64_t sz = g->ny * g->nx, sy = g->nx, P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
-    for (int64_t z = 1; z < g->nz; ++z)
-      for (int64_t y = 1; y < g->ny; ++y)
-        for (int64_t x = 1; x < g->nx; ++x) {
+    for (int64_t z = P; z < g->nz - P + 1; ++z)
+      for (int64_t y = P; y < g->ny - P + 1; ++y)
+        for (int64_t x = P; x < g->nx - P + 1; ++x) {
           const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
           const REAL c = cq[g->cq_b ? i : j];
           const int pz = z < g->z0 || z >= g->z1h, py = y < g->y0 || y >= g->y1h,
                     px = x < g->x0 || x >= g->x1h;
           REAL dEy_dz = 0, dEz_dy = 0, dEz_dx = 0, dEx_dz = 0, dEx_dy = 0, dEy_dx = 0;
-          if (z < g->nz - 1) {
-            REAL d = (ey[i + sz] - ey[i]) * g->rdz;
+          if (z < g->nz - P) {
+            REAL d = FN(dh)(g, ey, i, sz, g->rdz);
             if (pz) {
               m_ey_z[i] = g->p[BZH][z] * m_ey_z[i] + g->p[AZH][z] * d;
               d = d / g->p[KZH][z] + m_ey_z[i];
             }
             dEy_dz = d;
           }
-          if (y < g->ny - 1) {
-            REAL d = (ez[i + sy] - ez[i]) * g->rdy;
+          if (y < g->ny - P) {
+            REAL d = FN(dh)(g, ez, i, sy, g->rdy);
             if (py) {
               m_ez_y[i] = g->p[BYH][y] * m_ez_y[i] + g->p[AYH][y] * d;
               d = d / g->p[KYH][y] + m_ez_y[i];
             }
             dEz_dy = d;
           }
-          if (x < g->nx - 1) {
-            REAL d = (ez[i + 1] - ez[i]) * g->rdx;
+          if (x < g->nx - P) {
+            REAL d = FN(dh)(g, ez, i, 1, g->rdx);
             if (px) {
               m_ez_x[i] = g->p[BXH][x] * m_ez_x[i] + g->p[AXH][x] * d;
               d = d / g->p[KXH][x] + m_ez_x[i];
             }
             dEz_dx = d;
           }
-          if (z < g->nz - 1) {
-            REAL d = (ex[i + sz] - ex[i]) * g->rdz;
+          if (z < g->nz - P) {
+            REAL d = FN(dh)(g, ex, i, sz, g->rdz);
             if (pz) {
               m_ex_z[i] = g->p[BZH][z] * m_ex_z[i] + g->p[AZH][z] * d;
               d = d / g->p[KZH][z] + m_ex_z[i];
             }
             dEx_dz = d;
           }
-          if (y < g->ny - 1) {
-            REAL d = (ex[i + sy] - ex[i]) * g->rdy;
+          if (y < g->ny - P) {
+            REAL d = FN(dh)(g, ex, i, sy, g->rdy);
             if (py) {
               m_ex_y[i] = g->p[BYH][y] * m_ex_y[i] + g->p[AYH][y] * d;
               d = d / g->p[KYH][y] + m_ex_y[i];
             }
             dEx_dy = d;
           }
-          if (x < g->nx - 1) {
-            REAL d = (ey[i + 1] - ey[i]) * g->rdx;
+          if (x < g->nx - P) {
+            REAL d = FN(dh)(g, ey, i, 1, g->rdx);
             if (px) {
               m_ey_x[i] = g->p[BXH][x] * m_ey_x[i] + g->p[AXH][x] * d;
               d = d / g->p[KXH][x] + m_ey_x[i];
@@ -154,19 +200,19 @@ static void FN(step_e)(const FN(g3) * g, const REAL *ca, const REAL *cb, REAL **
   REAL *ex = F[0], *ey = F[1], *ez = F[2], *hx = F[3], *hy = F[4], *hz = F[5];
   REAL *m_hz_y = M[0], *m_hy_z = M[1], *m_hx_z = M[2], *m_hz_x = M[3], *m_hy_x = M[4],
        *m_hx_y = M[5];
-  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  const int64_t sz = g->ny * g->nx, sy = g->nx, P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
-    for (int64_t z = 1; z < g->nz; ++z)
-      for (int64_t y = 1; y < g->ny; ++y)
-        for (int64_t x = 1; x < g->nx; ++x) {
+    for (int64_t z = P; z < g->nz - P + 1; ++z)
+      for (int64_t y = P; y < g->ny - P + 1; ++y)
+        for (int64_t x = P; x < g->nx - P + 1; ++x) {
           const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
           const REAL a = ca[g->ca_b ? i : j], b = cb[g->cb_b ? i : j];
-          REAL dHy_dz = (hy[i] - hy[i - sz]) * g->rdz;
-          REAL dHz_dy = (hz[i] - hz[i - sy]) * g->rdy;
-          REAL dHz_dx = (hz[i] - hz[i - 1]) * g->rdx;
-          REAL dHx_dz = (hx[i] - hx[i - sz]) * g->rdz;
-          REAL dHx_dy = (hx[i] - hx[i - sy]) * g->rdy;
-          REAL dHy_dx = (hy[i] - hy[i - 1]) * g->rdx;
+          REAL dHy_dz = FN(d1)(g, hy, i, sz, g->rdz);
+          REAL dHz_dy = FN(d1)(g, hz, i, sy, g->rdy);
+          REAL dHz_dx = FN(d1)(g, hz, i, 1, g->rdx);
+          REAL dHx_dz = FN(d1)(g, hx, i, sz, g->rdz);
+          REAL dHx_dy = FN(d1)(g, hx, i, sy, g->rdy);
+          REAL dHy_dx = FN(d1)(g, hy, i, 1, g->rdx);
           if (z < g->z0 || z >= g->z1) {
             m_hy_z[i] = g->p[BZ][z] * m_hy_z[i] + g->p[AZ][z] * dHy_dz;
             dHy_dz = dHy_dz / g->p[KZ][z] + m_hy_z[i];
@@ -207,11 +253,11 @@ static void FN(step_e)(const FN(g3) * g, const REAL *ca, const REAL *cb, REAL **
  * dca E^n + dcb curl H^n of the background. */
 static void FN(step_e_born)(const FN(g3) * g, const REAL *ca, const REAL *cb, const REAL *dca,
                             const REAL *dcb, REAL **F, REAL **M, REAL **DF, REAL **DM) {
-  const int64_t sz = g->ny * g->nx, sy = g->nx;
+  const int64_t sz = g->ny * g->nx, sy = g->nx, P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
-    for (int64_t z = 1; z < g->nz; ++z)
-      for (int64_t y = 1; y < g->ny; ++y)
-        for (int64_t x = 1; x < g->nx; ++x) {
+    for (int64_t z = P; z < g->nz - P + 1; ++z)
+      for (int64_t y = P; y < g->ny - P + 1; ++y)
+        for (int64_t x = P; x < g->nx - P + 1; ++x) {
           const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
           const REAL a = ca[g->ca_b ? i : j], b = cb[g->cb_b ? i : j];
           const REAL da = dca[g->ca_b ? i : j], db = dcb[g->cb_b ? i : j];
@@ -221,12 +267,12 @@ static void FN(step_e_born)(const FN(g3) * g, const REAL *ca, const REAL *cb, co
           for (int w = 0; w < 2; ++w) {
             REAL **H = w ? DF : F, **Q = w ? DM : M;
             const REAL *hx = H[3], *hy = H[4], *hz = H[5];
-            REAL dHy_dz = (hy[i] - hy[i - sz]) * g->rdz;
-            REAL dHz_dy = (hz[i] - hz[i - sy]) * g->rdy;
-            REAL dHz_dx = (hz[i] - hz[i - 1]) * g->rdx;
-            REAL dHx_dz = (hx[i] - hx[i - sz]) * g->rdz;
-            REAL dHx_dy = (hx[i] - hx[i - sy]) * g->rdy;
-            REAL dHy_dx = (hy[i] - hy[i - 1]) * g->rdx;
+            REAL dHy_dz = FN(d1)(g, hy, i, sz, g->rdz);
+            REAL dHz_dy = FN(d1)(g, hz, i, sy, g->rdy);
+            REAL dHz_dx = FN(d1)(g, hz, i, 1, g->rdx);
+            REAL dHx_dz = FN(d1)(g, hx, i, sz, g->rdz);
+            REAL dHx_dy = FN(d1)(g, hx, i, sy, g->rdy);
+            REAL dHy_dx = FN(d1)(g, hy, i, 1, g->rdx);
             if (pz) {
               Q[1][i] = g->p[BZ][z] * Q[1][i] + g->p[AZ][z] * dHy_dz;
               dHy_dz = dHy_dz / g->p[KZ][z] + Q[1][i];
@@ -298,6 +344,8 @@ static void FN(setup)(FN(g3) * g, const REAL **prof, REAL rdz, REAL rdy, REAL rd
   g->ca_b = ca_b;
   g->cb_b = cb_b;
   g->cq_b = cq_b;
+  g->st = g_em3d_stencil;
+  g->P = g_em3d_stencil / 2;
 }
 
 /* Forward over steps [start_t, start_t + nt).  store: 6 snapshot histories
@@ -375,7 +423,7 @@ static inline REAL FN(raw_h)(const FN(g3) * g, const REAL *coef, int cq_batched,
   if (!FN(active)(g, z, y, x)) return 0;
   const int64_t c = axis == 0 ? z : axis == 1 ? y : x;
   const int64_t n = axis == 0 ? g->nz : axis == 1 ? g->ny : g->nx;
-  if (c >= n - 1) return 0;
+  if (c >= n - g->P) return 0;
   const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
   REAL q = coef[cq_batched ? i : j] * lam[i];
   if (neg) q = -q;
@@ -390,10 +438,11 @@ static inline REAL FN(raw_h)(const FN(g3) * g, const REAL *coef, int cq_batched,
 
 static void FN(adj_e)(const FN(g3) * g, const REAL *cb, REAL **L, REAL **cur, REAL **nxt) {
   REAL *lex = L[0], *ley = L[1], *lez = L[2], *lhx = L[3], *lhy = L[4], *lhz = L[5];
+  const int64_t P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
-    for (int64_t z = 1; z < g->nz; ++z)
-      for (int64_t y = 1; y < g->ny; ++y)
-        for (int64_t x = 1; x < g->nx; ++x) {
+    for (int64_t z = P; z < g->nz - P + 1; ++z)
+      for (int64_t y = P; y < g->ny - P + 1; ++y)
+        for (int64_t x = P; x < g->nx - P + 1; ++x) {
           const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
           const REAL c = cb[g->cb_b ? i : j];
           const REAL qx = c * lex[i], qy = c * ley[i], qz = c * lez[i];
@@ -406,23 +455,21 @@ static void FN(adj_e)(const FN(g3) * g, const REAL *cb, REAL **L, REAL **cur, RE
           nxt[L_HZ_X][i] = px ? g->p[BX][x] * cur[L_HZ_X][i] + qy : (REAL)0;
           nxt[L_HY_X][i] = px ? g->p[BX][x] * cur[L_HY_X][i] - qz : (REAL)0;
           const int cb_b = g->cb_b;
-#define RE(lam, mem, ax, ng, dz, dy, dx) \
-  FN(raw_e)(g, cb, cb_b, lam, cur[mem], ax, ng, s, z + (dz), y + (dy), x + (dx))
-          const REAL a1 = (RE(ley, L_HX_Z, 0, 1, 0, 0, 0) * (REAL)1 -
-                           RE(ley, L_HX_Z, 0, 1, 1, 0, 0) * (REAL)1) * g->rdz;
-          const REAL a2 = (RE(lez, L_HX_Y, 1, 0, 0, 0, 0) * (REAL)1 -
-                           RE(lez, L_HX_Y, 1, 0, 0, 1, 0) * (REAL)1) * g->rdy;
-          lhx[i] = lhx[i] + (a1 + a2);
-          const REAL b1 = (RE(lex, L_HY_Z, 0, 0, 0, 0, 0) * (REAL)1 -
-                           RE(lex, L_HY_Z, 0, 0, 1, 0, 0) * (REAL)1) * g->rdz;
-          const REAL b2 = (RE(lez, L_HY_X, 2, 1, 0, 0, 0) * (REAL)1 -
-                           RE(lez, L_HY_X, 2, 1, 0, 0, 1) * (REAL)1) * g->rdx;
-          lhy[i] = lhy[i] + (b1 + b2);
-          const REAL c1 = (RE(lex, L_HZ_Y, 1, 1, 0, 0, 0) * (REAL)1 -
-                           RE(lex, L_HZ_Y, 1, 1, 0, 1, 0) * (REAL)1) * g->rdy;
-          const REAL c2 = (RE(ley, L_HZ_X, 2, 0, 0, 0, 0) * (REAL)1 -
-                           RE(ley, L_HZ_X, 2, 0, 0, 0, 1) * (REAL)1) * g->rdx;
-          lhz[i] = lhz[i] + (c1 + c2);
+          /* raw terms at offsets -P+1 .. P along one axis (DIFF?1_ADJ) */
+#define RE(dst, lam, mem, ax, ng)                                                         \
+  for (int o = 1 - (int)P; o <= (int)P; ++o)                                                \
+    dst[o + P - 1] = FN(raw_e)(g, cb, cb_b, lam, cur[mem], ax, ng, s, z + (ax == 0 ? o : 0), \
+                               y + (ax == 1 ? o : 0), x + (ax == 2 ? o : 0));
+          REAL r1[8], r2[8];
+          RE(r1, ley, L_HX_Z, 0, 1)
+          RE(r2, lez, L_HX_Y, 1, 0)
+          lhx[i] = lhx[i] + (FN(tadj)(g, r1, g->rdz) + FN(tadj)(g, r2, g->rdy));
+          RE(r1, lex, L_HY_Z, 0, 0)
+          RE(r2, lez, L_HY_X, 2, 1)
+          lhy[i] = lhy[i] + (FN(tadj)(g, r1, g->rdz) + FN(tadj)(g, r2, g->rdx));
+          RE(r1, lex, L_HZ_Y, 1, 1)
+          RE(r2, ley, L_HZ_X, 2, 0)
+          lhz[i] = lhz[i] + (FN(tadj)(g, r1, g->rdy) + FN(tadj)(g, r2, g->rdx));
 #undef RE
         }
 }
@@ -430,15 +477,16 @@ static void FN(adj_e)(const FN(g3) * g, const REAL *cb, REAL **L, REAL **cur, RE
 static void FN(adj_h)(const FN(g3) * g, const REAL *ca, const REAL *cq, REAL **L, REAL **cur,
                       REAL **nxt) {
   REAL *lex = L[0], *ley = L[1], *lez = L[2], *lhx = L[3], *lhy = L[4], *lhz = L[5];
+  const int64_t P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
-    for (int64_t z = 1; z < g->nz; ++z)
-      for (int64_t y = 1; y < g->ny; ++y)
-        for (int64_t x = 1; x < g->nx; ++x) {
+    for (int64_t z = P; z < g->nz - P + 1; ++z)
+      for (int64_t y = P; y < g->ny - P + 1; ++y)
+        for (int64_t x = P; x < g->nx - P + 1; ++x) {
           const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
           const REAL c = cq[g->cq_b ? i : j];
-          const int pz = z < g->nz - 1 && (z < g->z0 || z >= g->z1h);
-          const int py = y < g->ny - 1 && (y < g->y0 || y >= g->y1h);
-          const int px = x < g->nx - 1 && (x < g->x0 || x >= g->x1h);
+          const int pz = z < g->nz - P && (z < g->z0 || z >= g->z1h);
+          const int py = y < g->ny - P && (y < g->y0 || y >= g->y1h);
+          const int px = x < g->nx - P && (x < g->x0 || x >= g->x1h);
           nxt[L_EY_Z][i] = pz ? g->p[BZH][z] * cur[L_EY_Z][i] - c * lhx[i] : (REAL)0;
           nxt[L_EX_Z][i] = pz ? g->p[BZH][z] * cur[L_EX_Z][i] + c * lhy[i] : (REAL)0;
           nxt[L_EZ_Y][i] = py ? g->p[BYH][y] * cur[L_EZ_Y][i] + c * lhx[i] : (REAL)0;
@@ -450,23 +498,21 @@ static void FN(adj_h)(const FN(g3) * g, const REAL *ca, const REAL *cq, REAL **L
           ley[i] = a * ley[i];
           lez[i] = a * lez[i];
           const int cq_b = g->cq_b;
-#define RH(lam, mem, ax, ng, dz, dy, dx) \
-  FN(raw_h)(g, cq, cq_b, lam, cur[mem], ax, ng, s, z + (dz), y + (dy), x + (dx))
-          const REAL e1 = (RH(lhx, L_EY_Z, 0, 1, -1, 0, 0) * (REAL)1 -
-                           RH(lhx, L_EY_Z, 0, 1, 0, 0, 0) * (REAL)1) * g->rdz;
-          const REAL e2 = (RH(lhz, L_EY_X, 2, 0, 0, 0, -1) * (REAL)1 -
-                           RH(lhz, L_EY_X, 2, 0, 0, 0, 0) * (REAL)1) * g->rdx;
-          ley[i] = ley[i] + (e1 + e2);
-          const REAL f1 = (RH(lhy, L_EX_Z, 0, 0, -1, 0, 0) * (REAL)1 -
-                           RH(lhy, L_EX_Z, 0, 0, 0, 0, 0) * (REAL)1) * g->rdz;
-          const REAL f2 = (RH(lhz, L_EX_Y, 1, 1, 0, -1, 0) * (REAL)1 -
-                           RH(lhz, L_EX_Y, 1, 1, 0, 0, 0) * (REAL)1) * g->rdy;
-          lex[i] = lex[i] + (f1 + f2);
-          const REAL h1 = (RH(lhx, L_EZ_Y, 1, 0, 0, -1, 0) * (REAL)1 -
-                           RH(lhx, L_EZ_Y, 1, 0, 0, 0, 0) * (REAL)1) * g->rdy;
-          const REAL h2 = (RH(lhy, L_EZ_X, 2, 1, 0, 0, -1) * (REAL)1 -
-                           RH(lhy, L_EZ_X, 2, 1, 0, 0, 0) * (REAL)1) * g->rdx;
-          lez[i] = lez[i] + (h1 + h2);
+          /* raw terms at offsets -P .. P-1 along one axis (DIFF?H1_ADJ) */
+#define RH(dst, lam, mem, ax, ng)                                                         \
+  for (int o = -(int)P; o < (int)P; ++o)                                                    \
+    dst[o + P] = FN(raw_h)(g, cq, cq_b, lam, cur[mem], ax, ng, s, z + (ax == 0 ? o : 0),     \
+                           y + (ax == 1 ? o : 0), x + (ax == 2 ? o : 0));
+          REAL r1[8], r2[8];
+          RH(r1, lhx, L_EY_Z, 0, 1)
+          RH(r2, lhz, L_EY_X, 2, 0)
+          ley[i] = ley[i] + (FN(tadj)(g, r1, g->rdz) + FN(tadj)(g, r2, g->rdx));
+          RH(r1, lhy, L_EX_Z, 0, 0)
+          RH(r2, lhz, L_EX_Y, 1, 1)
+          lex[i] = lex[i] + (FN(tadj)(g, r1, g->rdz) + FN(tadj)(g, r2, g->rdy));
+          RH(r1, lhx, L_EZ_Y, 1, 0)
+          RH(r2, lhy, L_EZ_X, 2, 1)
+          lez[i] = lez[i] + (FN(tadj)(g, r1, g->rdy) + FN(tadj)(g, r2, g->rdx));
 #undef RH
         }
 }
@@ -509,9 +555,9 @@ void FN(tide_oracle_em3d_backward)(const REAL *ca, const REAL *cb, const REAL *c
     if (k > 0 && t % k == 0 && store) {
       const size_t off = (size_t)(t / k) * (size_t)tot * esz;
       for (int64_t s = 0; s < S; ++s)
-        for (int64_t z = 1; z < nz; ++z)
-          for (int64_t y = 1; y < ny; ++y)
-            for (int64_t x = 1; x < nx; ++x) {
+        for (int64_t z = g.P; z < nz - g.P + 1; ++z)
+          for (int64_t y = g.P; y < ny - g.P + 1; ++y)
+            for (int64_t x = g.P; x < nx - g.P + 1; ++x) {
               const int64_t i = FN(mi)(&g, s, z, y, x), j = i - s * g.N;
               const REAL lx = L[0][i], ly = L[1][i], lz = L[2][i];
               if (need_ca && store[0]) {

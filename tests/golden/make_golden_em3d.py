@@ -13,6 +13,11 @@ seeded heterogeneous case with two shots, in FP64:
     respect to epsilon and sigma, from the Python path (torch autograd);
   - the inputs, so the tests rebuild the identical problem.
 Output: em3d_case.npz.
+
+The same runs at stencil orders 4, 6 and 8 (the time step halved, inside the
+stability limit of every order) give em3d_hi_case.npz: receivers from the
+reference CPU backend and the Python path, and Python-path gradients, keyed
+by order (r_native_s4, r_python_s4, geps_s4, gsig_s4, ...).
 """
 
 from __future__ import annotations
@@ -55,11 +60,11 @@ def case(seed: int = 11):
     return dict(eps=eps, sig=sig, mu=mu, dx=dx, dt=dt, amp=amp, src=src, rec=rec, nt=nt, pml=3)
 
 
-def run(c, python_backend, grads):
+def run(c, python_backend, grads, stencil=2):
     eps = c["eps"].clone().requires_grad_(grads)
     sig = c["sig"].clone().requires_grad_(grads)
     out = kapi.maxwell3d(eps, sig, c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
-                         stencil=2, pml_width=c["pml"], python_backend=python_backend,
+                         stencil=stencil, pml_width=c["pml"], python_backend=python_backend,
                          source_component="ey", receiver_component="ey")
     r = out[-1]
     if not grads:
@@ -79,6 +84,20 @@ def main():
         rec=c["rec"].numpy(), nt=c["nt"], pml=c["pml"], r_native_f64=r_native,
         r_python_f64=r_py, geps_python_f64=geps, gsig_python_f64=gsig)
     print("rel(native, python) receivers:", np.linalg.norm(r_native - r_py) / np.linalg.norm(r_py))
+
+    c = case()
+    c["dt"] = 0.5 * c["dt"]
+    c["amp"] = tide.ricker(700e6, c["nt"], c["dt"], dtype=torch.float64).view(1, 1, -1).repeat(2, 1, 1)
+    c["amp"] = c["amp"] * torch.tensor([1.0, 0.7], dtype=torch.float64).view(2, 1, 1)
+    hi = dict(dt=c["dt"], amp=c["amp"].numpy())
+    for st in (4, 6, 8):
+        r_native, _, _ = run(c, False, False, st)
+        r_py, geps, gsig = run(c, True, True, st)
+        hi.update({f"r_native_s{st}": r_native, f"r_python_s{st}": r_py, f"geps_s{st}": geps,
+                   f"gsig_s{st}": gsig})
+        print(f"stencil {st}: rel(native, python) receivers:",
+              np.linalg.norm(r_native - r_py) / np.linalg.norm(r_py))
+    np.savez_compressed(HERE / "em3d_hi_case.npz", **hi)
 
 
 if __name__ == "__main__":

@@ -217,7 +217,8 @@ class Oracle3D:
             build_oracle()
         self.lib = ctypes.CDLL(str(ORACLE_SO))
 
-    def _fn(self, name, dtype):
+    def _fn(self, name, dtype, stencil=2):
+        self.lib.tide_oracle_em3d_set_stencil(c_int(stencil))
         sfx = "float" if dtype == torch.float32 else "double"
         fn = getattr(self.lib, f"tide_oracle_em3d_{name}_{sfx}")
         fn.restype = None
@@ -236,7 +237,7 @@ class Oracle3D:
     def forward(self, pb, ca, cb, f, r, fields, mem, *, store=None, k=1, fmt=0, start_t=0,
                 nt=None):
         nt = pb.nt if nt is None else nt
-        fn, F = self._fn("forward", pb.dtype)
+        fn, F = self._fn("forward", pb.dtype, pb.stencil)
         P, I = c_void_p, c_int64
         pml = (c_int64 * 6)(*pb.pml)
         fn.argtypes = [P, P, P, P, P, P, P, P, P, P, F, F, F, I, I, I, I, I, I, I, I, P, c_int,
@@ -251,7 +252,7 @@ class Oracle3D:
 
     def born_forward(self, pb, dca, dcb, f0, df, fields, mem, dfields, dmem, r, bg_r):
         """3-D Born forward on full-layout state lists (see full_state)."""
-        fn, F = self._fn("born_forward", pb.dtype)
+        fn, F = self._fn("born_forward", pb.dtype, pb.stencil)
         P, I = c_void_p, c_int64
         pml = (c_int64 * 6)(*pb.pml)
         fn.argtypes = [P] * 7 + [P] * 4 + [P, P, P, P, P] + [F, F, F] + [I] * 8 + [P] + [c_int] * 5
@@ -280,7 +281,7 @@ class Oracle3D:
         gca, gcb, gf = grads
         geps = torch.zeros(mshape, dtype=dt) if eps_sigma else None
         gsig = torch.zeros(mshape, dtype=dt) if eps_sigma else None
-        fn, F = self._fn("backward", dt)
+        fn, F = self._fn("backward", dt, pb.stencil)
         P, I = c_void_p, c_int64
         fn.argtypes = [P, P, P, P, P, P, P, P, P, P, P, P, F, P, P, P, F, F, F, I, I, I, I, I,
                        I, I, I, c_int, I, P, c_int, c_int, c_int, c_int, c_int, c_int, c_int]
@@ -336,7 +337,7 @@ class RefCPU3D:
         from tide_b200 import _native as nat
 
         sfx = "float" if pb.dtype == torch.float32 else "double"
-        fn = getattr(self.lib, f"maxwell_3d_2_{sfx}_forward_cpu")
+        fn = getattr(self.lib, f"maxwell_3d_{pb.stencil}_{sfx}_forward_cpu")
         fn.argtypes = nat.argtypes("maxwell_3d_forward", sfx)
         fn.restype = None
         b = pb.batched
@@ -355,7 +356,7 @@ class RefCPU3D:
         from tide_b200 import _native as nat
 
         sfx = "float" if pb.dtype == torch.float32 else "double"
-        fn = getattr(self.lib, f"maxwell_3d_2_{sfx}_born_forward_cpu")
+        fn = getattr(self.lib, f"maxwell_3d_{pb.stencil}_{sfx}_born_forward_cpu")
         fn.argtypes = nat.argtypes("maxwell_3d_born_forward", sfx)
         fn.restype = None
         b = pb.batched

@@ -131,7 +131,7 @@ def test_born_adjoint_is_the_adjoint_over_the_background_history():
 
 
 # ---------------------------------------------------------------------- 3-D
-def _case3d(dtype, comps=("ey", "ey"), seed=5):
+def _case3d(dtype, comps=("ey", "ey"), seed=5, stencil=2):
     from tide_b200.em3d import prepare_em3d
 
     g = torch.Generator().manual_seed(seed)
@@ -141,12 +141,13 @@ def _case3d(dtype, comps=("ey", "ey"), seed=5):
     mu = torch.ones((nz, ny, nx), dtype=dtype)
     dx = 0.02
     dt = 0.9 * dx / (299792458.0 / float(eps.min().double().sqrt()) * 3 ** 0.5)
+    dt = dt if stencil == 2 else 0.5 * dt
     t = torch.arange(nt, dtype=torch.float64) * dt
     amp = (torch.sin(2 * 3.14159265 * 6e8 * t) * torch.exp(-((t - 3e-9) / 1e-9) ** 2))
     amp = amp.view(1, 1, nt).repeat(S, 1, 1).to(dtype)
     src = torch.stack([torch.randint(2, n - 2, (S, 1), generator=g) for n in (nz, ny, nx)], -1)
     rec = torch.stack([torch.randint(0, n, (S, 4), generator=g) for n in (nz, ny, nx)], -1)
-    return prepare_em3d(eps, sig, mu, dx, dt, amp, src, rec, pml_width=3,
+    return prepare_em3d(eps, sig, mu, dx, dt, amp, src, rec, pml_width=3, stencil=stencil,
                         source_component=comps[0], receiver_component=comps[1])
 
 
@@ -174,17 +175,26 @@ def _run3d(driver, pb, dca, dcb, df):
 @pytest.mark.skipif(not REF_SO.exists(), reason="reference CPU backend not built here")
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("comps", [("ey", "ey"), ("ex", "ez")])
-def test_born3d_oracle_equals_reference_cpu(dtype, comps):
+@pytest.mark.parametrize("stencil", [2, 4, 8])
+def test_born3d_oracle_equals_reference_cpu(dtype, comps, stencil):
+    """Background bit-identical at order 2; at orders 4 to 8 the reference
+    CPU build (-Ofast) may reassociate the multi-term differences, so every
+    output is held to rounding there."""
     from oracle_harness import Oracle3D, RefCPU3D
 
-    pb = _case3d(dtype, comps)
+    pb = _case3d(dtype, comps, stencil=stencil)
     dca, dcb, df = _perturbation3d(pb, 7)
     got = _run3d(Oracle3D(), pb, dca, dcb, df)
     ref = _run3d(RefCPU3D(), pb, dca, dcb, df)
-    assert torch.equal(got[1], ref[1]), "background receivers"
-    for a, b in zip(got[2], ref[2]):
-        assert torch.equal(a, b), "background state"
-    tol = 1e-5 if dtype == torch.float32 else 1e-14
+    tol = 1e-5 if dtype == torch.float32 else (1e-14 if stencil == 2 else 1e-12)
+    if stencil == 2:
+        assert torch.equal(got[1], ref[1]), "background receivers"
+        for a, b in zip(got[2], ref[2]):
+            assert torch.equal(a, b), "background state"
+    else:
+        assert rel_l2(got[1], ref[1]) <= tol
+        for a, b in zip(got[2], ref[2]):
+            assert rel_l2(a, b) <= tol
     assert rel_l2(got[0], ref[0]) <= tol
     for a, b in zip(got[3], ref[3]):
         assert rel_l2(a, b) <= tol

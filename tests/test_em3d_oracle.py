@@ -110,3 +110,58 @@ def test_oracle_gradient_matches_finite_difference():
         fm = float(_functional(c["eps"] - h * d_eps, sig, c, w))
     fd = (fp - fm) / (2 * h)
     assert abs(analytic - fd) <= 1e-6 * abs(fd), (analytic, fd)
+
+
+# ------------------------------------------------------- stencil orders 4, 6, 8
+def _hi_case(dtype=torch.float64, batched=False):
+    c = _case(dtype, batched)
+    hi = np.load(GOLDEN / "em3d_hi_case.npz")
+    c["dt"], c["amp"] = float(hi["dt"]), torch.from_numpy(hi["amp"]).to(dtype)
+    return c, hi
+
+
+@pytest.mark.parametrize("stencil", [4, 6, 8])
+def test_oracle_high_order_forward_matches_public_api_golden(stencil):
+    c, hi = _hi_case()
+    pb = _prep(c, stencil=stencil)
+    r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+    fields, mem = Oracle3D.full_state(pb)
+    Oracle3D().forward(pb, pb.ca, pb.cb, pb.f, r, fields, mem)
+    assert rel_l2(r, torch.from_numpy(hi[f"r_python_s{stencil}"])) < 1e-13
+    assert rel_l2(r, torch.from_numpy(hi[f"r_native_s{stencil}"])) < 1e-13
+
+
+@pytest.mark.skipif(not REF_SO.exists(), reason="reference CPU backend not built here")
+@pytest.mark.parametrize("stencil", [4, 6, 8])
+@pytest.mark.parametrize("dtype,tol", [(torch.float32, 1e-5), (torch.float64, 1e-13)])
+@pytest.mark.parametrize("batched", [False, True])
+def test_oracle_high_order_forward_vs_reference_cpu(stencil, dtype, tol, batched):
+    """The reference CPU backend is built with -Ofast (its CMake flags), which
+    lets the compiler reassociate the multi-term differences; the strict
+    restatement agrees to rounding, state arrays included."""
+    c, _ = _hi_case(dtype, batched)
+    pb = _prep(c, stencil=stencil, source_component="ex", receiver_component="ez")
+    r_o = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=dtype)
+    f_o, m_o = Oracle3D.full_state(pb)
+    Oracle3D().forward(pb, pb.ca, pb.cb, pb.f, r_o, f_o, m_o)
+    r_r = torch.zeros_like(r_o)
+    f_r, m_r = Oracle3D.full_state(pb)
+    RefCPU3D().forward(pb, pb.ca, pb.cb, pb.f, r_r, f_r, m_r, n_threads=1)
+    assert rel_l2(r_o, r_r) < tol
+    for a, b in zip(f_o, f_r):
+        assert rel_l2(a, b) < tol
+
+
+@pytest.mark.parametrize("stencil", [4, 6, 8])
+def test_oracle_high_order_gradient_matches_reference_autograd(stencil):
+    c, hi = _hi_case()
+    eps = c["eps"].clone().requires_grad_(True)
+    sig = c["sig"].clone().requires_grad_(True)
+    w = torch.randn((int(_golden()["nt"]), 2, 3), generator=torch.Generator().manual_seed(5),
+                    dtype=torch.float64)
+    pb = prepare_em3d(eps, sig, c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
+                      pml_width=c["pml"], stencil=stencil)
+    r = OracleEM3D.apply(pb.ca, pb.cb, pb.f, pb, Oracle3D())
+    (r * w).sum().backward()
+    assert rel_l2(eps.grad, torch.from_numpy(hi[f"geps_s{stencil}"])) < 1e-9
+    assert rel_l2(sig.grad, torch.from_numpy(hi[f"gsig_s{stencil}"])) < 1e-9

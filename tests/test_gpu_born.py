@@ -220,7 +220,7 @@ def _born3d_cuda(pb, dca, dcb, df, dev):
     r = torch.zeros((q.nt, q.n_shots, q.n_rec), device=dev, dtype=q.dtype)
     bg = torch.zeros_like(r)
     d = [x.to(dev) for x in (dca, dcb, df)]
-    fn = nat.get_backend_function("maxwell_3d", "born_forward", 2, q.dtype, dev)
+    fn = nat.get_backend_function("maxwell_3d", "born_forward", q.stencil, q.dtype, dev)
     p = nat.ptr
     fn(p(q.ca), p(q.cb), p(q.cq), p(d[0]), p(d[1]), p(q.f), p(d[2]),
        *[p(t) for t in q.fields], *[p(t) for t in q.memories], *[p(t) for t in dfields],
@@ -236,11 +236,12 @@ def _born3d_cuda(pb, dca, dcb, df, dev):
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("comps", [("ey", "ey"), ("ex", "ez")])
-def test_born3d_forward_bitwise_vs_oracle(cuda_device, dtype, comps):
+@pytest.mark.parametrize("stencil", [2, 4, 6, 8])
+def test_born3d_forward_bitwise_vs_oracle(cuda_device, dtype, comps, stencil):
     from oracle_harness import Oracle3D
     from test_born_oracle import _case3d, _perturbation3d
 
-    pb = _case3d(dtype, comps)
+    pb = _case3d(dtype, comps, stencil=stencil)
     dca, dcb, df = _perturbation3d(pb, 7)
     got = _born3d_cuda(pb, dca, dcb, df, cuda_device)
     F, M = Oracle3D.full_state(pb)

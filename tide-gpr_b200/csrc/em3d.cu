@@ -1,7 +1,9 @@
-// 3-D Maxwell (Yee) path, stencil order 2: forward, forward with snapshot
-// storage and exact adjoint with coefficient gradients, behind the
-// reference's maxwell_3d_2_{float,double}_{forward,forward_with_storage,
-// backward}_cuda symbols (declared in include/tide_b200.h).
+// 3-D Maxwell (Yee) path, stencil orders 2, 4, 6 and 8: forward, forward
+// with snapshot storage, Born forward and exact adjoint with coefficient
+// gradients, behind the reference's maxwell_3d_{S}_{float,double}_{forward,
+// forward_with_storage,born_forward,backward}_cuda symbols (declared in
+// include/tide_b200.h).  Order 2 has the register-marching kernels below;
+// orders 4 to 8 the generic kernels of em3d_hi.cuh.
 //
 // Arithmetic follows the reference's 3-D update and adjoint (forward H/E
 // src/tide/csrc/em3d/maxwell_3d_inst.cpp:560-702; snapshots
@@ -45,6 +47,7 @@ template <typename T> struct G3 {
   int64_t N;
   int z0, y0, x0, z1, y1, x1, z1h, y1h, x1h;
   int ezc, eyc, exc;  // compact extents along z, y, x
+  int P;              // half stencil width: update domain [P, n - P + 1) per axis
   bool ca_b, cb_b, cq_b;
 };
 
@@ -96,9 +99,9 @@ __device__ __forceinline__ bool first_cell(const G3<T> &g, Cell &c) {
   c.y = blockIdx.y * blockDim.y + threadIdx.y;
   c.s = blockIdx.z / zruns;
   c.z = (blockIdx.z - c.s * zruns) * kZRun;
-  c.zend = min(c.z + kZRun, g.nz);
-  if (c.x < 1 || c.x >= g.nx || c.y < 1 || c.y >= g.ny) return false;
-  if (c.z < 1) c.z = 1;
+  c.zend = min(c.z + kZRun, g.nz - g.P + 1);
+  if (c.x < g.P || c.x >= g.nx - g.P + 1 || c.y < g.P || c.y >= g.ny - g.P + 1) return false;
+  if (c.z < g.P) c.z = g.P;
   return c.z < c.zend;
 }
 __device__ __forceinline__ void set_index(Cell &c, int ny, int nx, int64_t N) {
@@ -107,8 +110,8 @@ __device__ __forceinline__ void set_index(Cell &c, int ny, int nx, int64_t N) {
 }
 
 // ---------------------------------------------------------------- forward
-// Column of one thread: shot s, (y, x) and the z run [zb, ze) of cells with
-// z, y, x >= 1.
+// Column of one thread: shot s, (y, x) and the z run [zb, ze) of cells in
+// the update domain (z, y, x in [P, n - P + 1)).
 struct Col {
   int s, y, x, zb, ze;
 };
@@ -119,9 +122,9 @@ __device__ __forceinline__ bool column(const G3<T> &g, Col &c) {
   c.y = blockIdx.y * blockDim.y + threadIdx.y;
   c.s = blockIdx.z / zruns;
   c.zb = (blockIdx.z - c.s * zruns) * kZRun;
-  c.ze = min(c.zb + kZRun, g.nz);
-  if (c.x < 1 || c.x >= g.nx || c.y < 1 || c.y >= g.ny) return false;
-  if (c.zb < 1) c.zb = 1;
+  c.ze = min(c.zb + kZRun, g.nz - g.P + 1);
+  if (c.x < g.P || c.x >= g.nx - g.P + 1 || c.y < g.P || c.y >= g.ny - g.P + 1) return false;
+  if (c.zb < g.P) c.zb = g.P;
   return c.zb < c.ze;
 }
 
@@ -843,6 +846,8 @@ k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
   }
 }
 
+#include "em3d_hi.cuh"
+
 // Adjoint sources (receivers inject grad_r) then adjoint receivers (sources
 // record grad_f), one step.
 template <typename T>
@@ -942,10 +947,11 @@ template <typename T> struct Launch3 {
 };
 
 template <typename T>
-bool make3(Launch3<T> &L, const T *const prof[kNProf], T rdz, T rdy, T rdx, int64_t S,
+bool make3(Launch3<T> &L, int stencil, const T *const prof[kNProf], T rdz, T rdy, T rdx, int64_t S,
            int64_t nz, int64_t ny, int64_t nx, int64_t pz0, int64_t py0, int64_t px0,
            int64_t pz1, int64_t py1, int64_t px1, bool ca_b, bool cb_b, bool cq_b) {
-  if (S < 1 || nz < 2 || ny < 2 || nx < 2 || nz > (1 << 20) || ny > (1 << 20) ||
+  const int P = stencil / 2;
+  if (S < 1 || nz < 2 * P || ny < 2 * P || nx < 2 * P || nz > (1 << 20) || ny > (1 << 20) ||
       nx > (1 << 20) || nz * ny * nx > ((int64_t)1 << 40) ||
       S * ((nz + kZRun - 1) / kZRun) > 65535) {
     set_error(kBadArgument, "3-D: unsupported shape n_shots=%lld nz=%lld ny=%lld nx=%lld",
@@ -975,6 +981,7 @@ bool make3(Launch3<T> &L, const T *const prof[kNProf], T rdz, T rdy, T rdx, int6
   g.ezc = (int)(pz0 + nz - std::max(pz0, pz1 - 1));
   g.eyc = (int)(py0 + ny - std::max(py0, py1 - 1));
   g.exc = (int)(px0 + nx - std::max(px0, px1 - 1));
+  g.P = P;
   g.ca_b = ca_b; g.cb_b = cb_b; g.cq_b = cq_b;
   L.grid = dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8),
                 (unsigned)(S * ((nz + kZRun - 1) / kZRun)));
@@ -1011,20 +1018,30 @@ bool common_checks(const char *what, int64_t n_src, const T *f, int64_t n_rec, c
   return true;
 }
 
-template <typename T, typename S>
+template <typename T, typename S, int ST>
 void launch_fwd_step(const Launch3<T> &L, cudaStream_t st, const T *ca, const T *cb,
                      const T *cq, T *F[6], T *M[12], S *const snap[6], const T *f_t,
                      const int64_t *src_i, int64_t n_src, int64_t src_c, T *r_t,
                      const int64_t *rec_i, int64_t n_rec, int64_t rec_c,
                      ProfileScope *prof = nullptr, bool smp = false) {
   if (smp) prof->begin(kK3FwdH);
-  k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, F[0], F[1], F[2], F[3], F[4], F[5], M[6],
-                                          M[7], M[8], M[9], M[10], M[11]);
+  if constexpr (ST == 2)
+    k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, F[0], F[1], F[2], F[3], F[4], F[5], M[6],
+                                            M[7], M[8], M[9], M[10], M[11]);
+  else
+    k3p_fwd_h<T, ST / 2><<<L.grid, L.block, 0, st>>>(L.g, cq, F[0], F[1], F[2], F[3], F[4], F[5],
+                                                     M[6], M[7], M[8], M[9], M[10], M[11]);
   if (smp) prof->end(kK3FwdH);
   if (smp) prof->begin(kK3FwdE);
-  k3_fwd_e<T, S><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, F[0], F[1], F[2], F[3], F[4], F[5],
-                                             M[0], M[1], M[2], M[3], M[4], M[5], snap[0],
-                                             snap[1], snap[2], snap[3], snap[4], snap[5]);
+  if constexpr (ST == 2)
+    k3_fwd_e<T, S><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, F[0], F[1], F[2], F[3], F[4], F[5],
+                                               M[0], M[1], M[2], M[3], M[4], M[5], snap[0],
+                                               snap[1], snap[2], snap[3], snap[4], snap[5]);
+  else
+    k3p_fwd_e<T, S, ST / 2><<<L.grid, L.block, 0, st>>>(
+        L.g, ca, cb, F[0], F[1], F[2], F[3], F[4], F[5],
+        BornMem<T>{M[0], M[1], M[2], M[3], M[4], M[5]}, snap[0], snap[1], snap[2], snap[3],
+        snap[4], snap[5]);
   if (smp) prof->end(kK3FwdE);
   int n = 2;
   const int S_ = L.g.S;
@@ -1044,7 +1061,7 @@ void launch_fwd_step(const Launch3<T> &L, cudaStream_t st, const T *ca, const T 
   count_launches(n);
 }
 
-template <typename T>
+template <typename T, int ST>
 void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads; (void)n_poles;
   (void)debye_a; (void)debye_b; (void)debye_cp; (void)pol_ex; (void)pol_ey; (void)pol_ez;
@@ -1063,7 +1080,7 @@ void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
-  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+  if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
              pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   cudaStream_t st = stream_of(compute_stream);
@@ -1072,14 +1089,14 @@ void em3d_forward(TIDE_3D_FORWARD_ARGS(T)) {
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   ProfileScope ps(st);
   for (int64_t t = start_t; t < start_t + nt; ++t)
-    launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, none, f ? f + t * fs : nullptr, sources_i,
+    launch_fwd_step<T, T, ST>(L, st, ca, cb, cq, F, M, none, f ? f + t * fs : nullptr, sources_i,
                           n_sources_per_shot, source_component, r ? r + t * rs : nullptr,
                           receivers_i, n_receivers_per_shot, receiver_component, &ps,
                           ps.sample(t));
   TB_CUDA(cudaGetLastError());
 }
 
-template <typename T>
+template <typename T, int ST>
 void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
   (void)dt; (void)n_threads;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
@@ -1110,7 +1127,7 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
-  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+  if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
              pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   T *F[6] = {ex, ey, ez, hx, hy, hz};
@@ -1126,13 +1143,13 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
       __nv_bfloat16 *const sp[6] = {(__nv_bfloat16 *)dst[0], (__nv_bfloat16 *)dst[1],
                                     (__nv_bfloat16 *)dst[2], (__nv_bfloat16 *)dst[3],
                                     (__nv_bfloat16 *)dst[4], (__nv_bfloat16 *)dst[5]};
-      launch_fwd_step<T, __nv_bfloat16>(L, st, ca, cb, cq, F, M, sp, ft, sources_i,
+      launch_fwd_step<T, __nv_bfloat16, ST>(L, st, ca, cb, cq, F, M, sp, ft, sources_i,
                                         n_sources_per_shot, source_component, rt, receivers_i,
                                         n_receivers_per_shot, receiver_component, &ps, smp);
     } else {
       T *const sp[6] = {(T *)dst[0], (T *)dst[1], (T *)dst[2],
                         (T *)dst[3], (T *)dst[4], (T *)dst[5]};
-      launch_fwd_step<T, T>(L, st, ca, cb, cq, F, M, sp, ft, sources_i, n_sources_per_shot,
+      launch_fwd_step<T, T, ST>(L, st, ca, cb, cq, F, M, sp, ft, sources_i, n_sources_per_shot,
                             source_component, rt, receivers_i, n_receivers_per_shot,
                             receiver_component, &ps, smp);
     }
@@ -1142,7 +1159,7 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
   sr.finish();
 }
 
-template <typename T>
+template <typename T, int ST>
 void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   (void)n_threads;
   (void)storage_stream;
@@ -1205,7 +1222,7 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
-  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+  if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
              pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   const G3<T> &g = L.g;
@@ -1248,12 +1265,20 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
     const bool smp = ps.sample(t);
     if (smp) ps.begin(kK3AdjE);
-    k3_adj_e<T><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez, lambda_hx,
-                                            lambda_hy, lambda_hz, cur, nxt);
+    if constexpr (ST == 2)
+      k3_adj_e<T><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez, lambda_hx,
+                                              lambda_hy, lambda_hz, cur, nxt);
+    else
+      k3p_adj_e<T, ST / 2><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez,
+                                                       lambda_hx, lambda_hy, lambda_hz, cur, nxt);
     if (smp) ps.end(kK3AdjE);
     if (smp) ps.begin(kK3AdjH);
-    k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
-                                            lambda_ex, lambda_ey, lambda_ez, cur, nxt);
+    if constexpr (ST == 2)
+      k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
+                                              lambda_ex, lambda_ey, lambda_ez, cur, nxt);
+    else
+      k3p_adj_h<T, ST / 2><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
+                                                       lambda_ex, lambda_ey, lambda_ez, cur, nxt);
     if (smp) ps.end(kK3AdjH);
     launches += 2;
     if (n_receivers_per_shot > 0 && grad_r && receivers_i) {
@@ -1350,7 +1375,7 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
     TB_CUDA(cudaStreamSynchronize(st));
 }
 
-template <typename T>
+template <typename T, int ST>
 void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
@@ -1372,7 +1397,7 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
-  if (!make3(L, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+  if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
              pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   cudaStream_t st = stream_of(compute_stream);
@@ -1387,11 +1412,20 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
     T *const *ms2[2] = {M, DM};
     for (int w = 0; w < 2; ++w) {
       T *const *Fw = fs2[w], *const *Mw = ms2[w];
-      k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, Fw[0], Fw[1], Fw[2], Fw[3], Fw[4], Fw[5],
-                                              Mw[6], Mw[7], Mw[8], Mw[9], Mw[10], Mw[11]);
+      if constexpr (ST == 2)
+        k3_fwd_h<T><<<L.grid, L.block, 0, st>>>(L.g, cq, Fw[0], Fw[1], Fw[2], Fw[3], Fw[4],
+                                                Fw[5], Mw[6], Mw[7], Mw[8], Mw[9], Mw[10], Mw[11]);
+      else
+        k3p_fwd_h<T, ST / 2><<<L.grid, L.block, 0, st>>>(L.g, cq, Fw[0], Fw[1], Fw[2], Fw[3],
+                                                         Fw[4], Fw[5], Mw[6], Mw[7], Mw[8], Mw[9],
+                                                         Mw[10], Mw[11]);
     }
-    k3_born_e<T><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy, hz, dex,
-                                             dey, dez, dhx, dhy, dhz, mb, ms);
+    if constexpr (ST == 2)
+      k3_born_e<T><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy, hz, dex,
+                                               dey, dez, dhx, dhy, dhz, mb, ms);
+    else
+      k3p_born_e<T, ST / 2><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy,
+                                                        hz, dex, dey, dez, dhx, dhy, dhz, mb, ms);
     launches += 3;
     if (n_sources_per_shot > 0 && sources_i) {
       k3_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
@@ -1427,7 +1461,7 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
 
 #define TB3_DEFINE(S, T)                                                                   \
   extern "C" void maxwell_3d_##S##_##T##_forward_cuda(TIDE_3D_FORWARD_ARGS(T)) {           \
-    tb::em3d_forward<T>(                                                                   \
+    tb::em3d_forward<T, S>(                                                                   \
         ca, cb, cq, f, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x,     \
         m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, debye_a, debye_b,          \
         debye_cp, pol_ex, pol_ey, pol_ez, ex_prev, ey_prev, ez_prev, r, n_poles, az, bz,   \
@@ -1440,7 +1474,7 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
   }                                                                                        \
   extern "C" void maxwell_3d_##S##_##T##_forward_with_storage_cuda(                        \
       TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {                                              \
-    tb::em3d_forward_with_storage<T>(                                                      \
+    tb::em3d_forward_with_storage<T, S>(                                                      \
         ca, cb, cq, f, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z, m_hz_x, m_hy_x,     \
         m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, r, ex_s1, ex_s3, ex_fn,    \
         ey_s1, ey_s3, ey_fn, ez_s1, ez_s3, ez_fn, cx_s1, cx_s3, cx_fn, cy_s1, cy_s3,       \
@@ -1453,7 +1487,7 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
         compute_stream, storage_stream);                                                   \
   }                                                                                        \
   extern "C" void maxwell_3d_##S##_##T##_backward_cuda(TIDE_3D_BACKWARD_ARGS(T)) {         \
-    tb::em3d_backward<T>(                                                                  \
+    tb::em3d_backward<T, S>(                                                                  \
         ca, cb, cq, grad_r, lambda_ex, lambda_ey, lambda_ez, lambda_hx, lambda_hy,         \
         lambda_hz, m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,             \
         m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z, m_lambda_hx_z,         \
@@ -1471,10 +1505,16 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
 
 TB3_DEFINE(2, float)
 TB3_DEFINE(2, double)
+TB3_DEFINE(4, float)
+TB3_DEFINE(4, double)
+TB3_DEFINE(6, float)
+TB3_DEFINE(6, double)
+TB3_DEFINE(8, float)
+TB3_DEFINE(8, double)
 
 #define TB3_BORN_DEFINE(S, T)                                                              \
   extern "C" void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T)) { \
-    tb::em3d_born_forward<T>(                                                              \
+    tb::em3d_born_forward<T, S>(                                                              \
         ca, cb, cq, dca, dcb, f0, df, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z,      \
         m_hz_x, m_hy_x, m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, dex, dey,  \
         dez, dhx, dhy, dhz, dm_hz_y, dm_hy_z, dm_hx_z, dm_hz_x, dm_hy_x, dm_hx_y, dm_ey_z, \
@@ -1488,3 +1528,9 @@ TB3_DEFINE(2, double)
 
 TB3_BORN_DEFINE(2, float)
 TB3_BORN_DEFINE(2, double)
+TB3_BORN_DEFINE(4, float)
+TB3_BORN_DEFINE(4, double)
+TB3_BORN_DEFINE(6, float)
+TB3_BORN_DEFINE(6, double)
+TB3_BORN_DEFINE(8, float)
+TB3_BORN_DEFINE(8, double)

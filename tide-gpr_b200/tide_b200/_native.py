@@ -107,7 +107,7 @@ SPECS.update({
 })
 
 ACCURACIES = (2, 4, 6, 8)
-ACCURACIES_3D = (2,)
+ACCURACIES_3D = (2, 4, 6, 8)
 DTYPES = {torch.float32: "float", torch.float64: "double"}
 PASSES = ("forward", "forward_with_storage", "backward")
 

@@ -1,4 +1,4 @@
-"""3-D Maxwell (Yee) propagation on libtide_b200.so (stencil order 2).
+"""3-D Maxwell (Yee) propagation on libtide_b200.so (stencil orders 2, 4, 6, 8).
 
 Mirrors the reference's 3-D operator path (src/tide/maxwell/maxwell3d.py:
 200-951 and maxwell3d_cuda.py:27-921): coordinate order [z, y, x]; models
@@ -105,6 +105,7 @@ class EM3DProblem:
     dtype: torch.dtype
     device: torch.device
     models: dict = field(default_factory=dict)
+    stencil: int = 2
 
 
 def _widths(pml_width: int | Sequence[int]) -> list[int]:
@@ -166,8 +167,8 @@ def prepare_em3d(
     Hy, Hz and the 12 CPML memories in MEM_NAMES order, each [nz', ny', nx']
     or [S, nz', ny', nx'] on the model + CPML region (the shape this module
     returns) or on the full padded grid; None entries start at zero."""
-    if stencil != 2:
-        raise ValueError("the 3-D path is built for stencil order 2")
+    if stencil not in (2, 4, 6, 8):
+        raise ValueError("stencil must be 2, 4, 6 or 8")
     if epsilon.ndim not in (3, 4) or sigma.shape != epsilon.shape or mu.shape != epsilon.shape:
         raise ValueError("epsilon, sigma, mu must share a [nz, ny, nx] or [S, nz, ny, nx] shape")
     if source_component not in COMPONENTS or receiver_component not in COMPONENTS:
@@ -176,7 +177,8 @@ def prepare_em3d(
     batched = epsilon.ndim == 4
     dz, dy, dx = _spacing(grid_spacing)
     widths = _widths(pml_width)
-    fd = [1, 0, 1, 0, 1, 0]
+    hp = stencil // 2
+    fd = [hp, hp - 1, hp, hp - 1, hp, hp - 1]
     pad = [a + b for a, b in zip(fd, widths)]
     mz, my, mx = epsilon.shape[-3:]
     nz, ny, nx = mz + pad[0] + pad[1], my + pad[2] + pad[3], mx + pad[4] + pad[5]
@@ -227,6 +229,7 @@ def prepare_em3d(
         rec_comp=COMPONENTS[receiver_component],
         grad_interval=int(model_gradient_sampling_interval), fd_pad=fd, pml_width=widths,
         dtype=dtype, device=device, models={"epsilon": eps_p, "sigma": sig_p, "mu": mu_p},
+        stencil=int(stencil),
     )
 
 
@@ -251,7 +254,7 @@ def _flags(pb: EM3DProblem, start_t: int) -> list:
 
 
 def native_forward(pb: EM3DProblem, ca, cb, f, r, start_t: int, nt: int) -> None:
-    fn = nat.get_backend_function("maxwell_3d", "forward", 2, pb.dtype, pb.device)
+    fn = nat.get_backend_function("maxwell_3d", "forward", pb.stencil, pb.dtype, pb.device)
     stream = torch.cuda.current_stream(pb.device).cuda_stream
     fn(_p(ca), _p(cb), _p(pb.cq), _p(f), *[_p(t) for t in pb.fields],
        *[_p(t) for t in pb.memories], *([0] * 9), _p(r), 0, *_profile_ptrs(pb),
@@ -325,7 +328,7 @@ def _store_ptrs(sn: Snapshots3D) -> list[int]:
 def native_forward_storage(pb: EM3DProblem, ca, cb, f, r, sn: Snapshots3D, need_ca: bool,
                            need_cb: bool, start_t: int = 0, nt: int | None = None) -> None:
     nt = pb.nt if nt is None else nt
-    fn = nat.get_backend_function("maxwell_3d", "forward_with_storage", 2, pb.dtype, pb.device)
+    fn = nat.get_backend_function("maxwell_3d", "forward_with_storage", pb.stencil, pb.dtype, pb.device)
     stream = torch.cuda.current_stream(pb.device).cuda_stream
     fn(_p(ca), _p(cb), _p(pb.cq), _p(f), *[_p(t) for t in pb.fields],
        *[_p(t) for t in pb.memories], _p(r), *_store_ptrs(sn), *_profile_ptrs(pb),
@@ -362,7 +365,7 @@ def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: b
                   if need_f and pb.n_src > 0 else empty)
     shot_ca = torch.empty(shape, device=dev, dtype=dt_) if need_ca and not pb.batched and S > 1 else empty
     shot_cb = torch.empty(shape, device=dev, dtype=dt_) if need_cb and not pb.batched and S > 1 else empty
-    fn = nat.get_backend_function("maxwell_3d", "backward", 2, dt_, dev)
+    fn = nat.get_backend_function("maxwell_3d", "backward", pb.stencil, dt_, dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     fn(_p(ca), _p(cb), _p(pb.cq), _p(grad_r), *[_p(t) for t in lam["fields"]],
        *[_p(t) for t in lam["mem"]], _p(scratch), *_store_ptrs(sn), _p(grad_f), _p(grad_ca),
@@ -472,6 +475,15 @@ class EM3DPropagate(torch.autograd.Function):
 STATE_NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") + MEM_NAMES
 
 
+def _crop(pb: EM3DProblem) -> tuple:
+    """Index of the model + CPML region of a padded [S, nz, ny, nx] array:
+    fd_pad[before] cells off the start and fd_pad[after] off the end of each
+    axis (maxwell3d_cuda.py:864-876)."""
+    fd, n = pb.fd_pad, (pb.nz, pb.ny, pb.nx)
+    return (slice(None),) + tuple(
+        slice(fd[2 * a], n[a] - fd[2 * a + 1] if fd[2 * a + 1] > 0 else None) for a in range(3))
+
+
 def maxwell3d(
     epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
     grid_spacing: float | Sequence[float], dt: float,
@@ -545,7 +557,7 @@ def maxwell3d(
         seg = 0
     r = EM3DPropagate.apply(pb.ca, pb.cb, pb.f, pb, mode, fmt, seg, bool(retain_history),
                             storage_path or ".")
-    s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
+    s = _crop(pb)
     outs = [t[s] for t in pb.fields]
     outs += [pb.layout.unpack(m, a)[s] for m, a in zip(pb.memories, MEM_AXES)]
     if ratio > 1 and r.numel() > 0:
@@ -636,7 +648,7 @@ def born3d(
         and bool(torch.equal(bg_receiver_location.to(dev), receiver_location.to(dev))))
     r = torch.zeros((pb.nt, S, pb.n_rec), device=dev, dtype=dtype)
     bg_r = torch.zeros_like(r) if same_rec else torch.empty(0, device=dev, dtype=dtype)
-    fn = nat.get_backend_function("maxwell_3d", "born_forward", 2, dtype, dev)
+    fn = nat.get_backend_function("maxwell_3d", "born_forward", pb.stencil, dtype, dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca_p), _p(dcb_p), _p(pb.f), _p(df),
        *[_p(t) for t in pb.fields], *[_p(t) for t in pb.memories],
@@ -657,7 +669,7 @@ def born3d(
         bg_r = ph.downsample(bg_r.movedim(0, -1), ratio).movedim(-1, 0)
     if ratio > 1 and r.numel() > 0:
         r = ph.downsample(r.movedim(0, -1), ratio).movedim(-1, 0)
-    s = (slice(None), slice(1, None), slice(1, None), slice(1, None))
+    s = _crop(pb)
 
     def outs(fields, mems):
         return [t[s] for t in fields] + [pb.layout.unpack(m, a)[s] for m, a in zip(mems, MEM_AXES)]
