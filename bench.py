@@ -516,6 +516,29 @@ def config4(seed: int = 4, shots: int = 4, nt: int = 1500, device="cpu"):
 PADDED3 = 153  # 128 + 2 x 12 CPML + 1 fd pad
 
 
+# Algorithmic bytes per cell (one shot, one step) of each 3-D kernel, FP32
+# fields: six field components each read or read-modify-written once, the
+# model coefficients once per launch of S shots, the two CPML memories of
+# each axis read + written in that axis's strips (strip fraction rho per
+# axis), snapshots (six components of snap_bytes) where stored or read, and
+# the per-shot coefficient-gradient buffers read-modify-written by the
+# gradient pass.
+def em3d_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho: float) -> float:
+    f = 4.0
+    strips = 2 * 2 * f * 3 * rho  # 2 memories per axis, read + write, 3 axes
+    if kind == "em3d_fwd_h":  # read Ex, Ey, Ez; RMW Hx, Hy, Hz; cq
+        return 9 * f + f / S + strips
+    if kind == "em3d_fwd_e":  # read H; RMW E; ca, cb; store E^t and curl H^t
+        return 9 * f + 2 * f / S + strips + 6 * snap_bytes
+    if kind == "em3d_adj_e":  # read lambda_E; RMW lambda_H; cb; adjoint memories
+        return 9 * f + f / S + strips
+    if kind == "em3d_adj_h":  # read lambda_H; RMW lambda_E; ca, cq; adjoint memories
+        return 9 * f + 2 * f / S + strips
+    if kind == "em3d_grad":  # read lambda_E, six snapshots; RMW two per-shot gradients
+        return 3 * f + 6 * snap_bytes + 2 * 2 * f
+    raise KeyError(kind)
+
+
 def _timed_gpu(fn, dev):
     """Device time (CUDA events on the current stream) of fn(), ms."""
     torch.cuda.synchronize(dev)
@@ -553,6 +576,38 @@ def em3d_bench(args) -> dict:
     ms_ck, _ = _timed_gpu(lambda: run(full, "checkpoint"), dev)
     units = 2.0 * full["shots"] * PADDED3 ** 3 * args.em3d_nt
     seg = em3d.checkpoint_steps(args.em3d_nt, 1, None)
+    # per-kernel device times: CUDA events around every 10th step's launches
+    # (on the launching stream, inside the library) during one more evaluation
+    L = lib()
+    L.tide_b200_profile_enable(1, 10)
+    read_profile(L)
+    run(full, "checkpoint")
+    torch.cuda.synchronize(dev)
+    L.tide_b200_profile_enable(0, 1)
+    prof = {k: v for k, v in read_profile(L).items() if k.startswith("em3d_") and v[1] > 0}
+    peak, peak_kind = hbm_peak()
+    rho = 27 / PADDED3  # 13 + 14 compact strip cells per axis
+    cells = full["shots"] * PADDED3 ** 3
+    kernels = {}
+    for k, (tot, n) in prof.items():
+        bpc = em3d_bytes_per_cell(k, full["shots"], 2, rho)
+        if k == "em3d_fwd_e":  # checkpoint mode: half the sampled launches store snapshots
+            bpc -= 0.5 * 6 * 2
+        avg = tot / n
+        ach = bpc * cells / (avg / 1e3) / 1e9
+        kernels[k] = {"avg_launch_ms": avg, "launches_sampled": n, "bytes_per_cell": round(bpc, 2),
+                      "achieved_gbs": round(ach, 1), "frac": round(ach / peak, 4)}
+    share = {k: v[0] for k, v in prof.items()}
+    dom = max(share, key=share.get) if share else None
+    roof3 = None
+    if dom:
+        roof3 = {"kernel": dom, "bound": "hbm", "achieved": kernels[dom]["achieved_gbs"],
+                 "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                 "frac": kernels[dom]["frac"], "traffic": None,
+                 "algorithmic_bytes_per_launch": kernels[dom]["bytes_per_cell"] * cells,
+                 "avg_launch_ms": kernels[dom]["avg_launch_ms"],
+                 "kernel_ms_share": {k: round(v / sum(share.values()), 4) for k, v in share.items()},
+                 "kernels": kernels}
     torch.cuda.empty_cache()
     short = dict(full, amp=full["amp"][..., : args.em3d_host_nt])
     run(short, "cpu")  # warm-up: the pinned host history is allocated once and then cached
@@ -584,6 +639,7 @@ def em3d_bench(args) -> dict:
                  "d2h_gbs": (1 << 30) / (ms_d2h / 1e3) / 1e9, "bytes": 1 << 30},
         "grad_rel_l2_checkpoint_vs_host": {"eps": rel(g_ck[0], g_host[0]),
                                             "sigma": rel(g_ck[1], g_host[1])},
+        "roofline": roof3,
         "timing": "CUDA events around each whole evaluation (public API, device inputs)",
     }
 

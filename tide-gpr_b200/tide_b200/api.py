@@ -33,6 +33,16 @@ class FallbackPolicy(StrEnum):
     REFERENCE = "reference"
 
 
+def _check(ok: bool, message: str) -> None:
+    """Raise ValueError(message) unless ok (value-object invariants)."""
+    if not ok:
+        raise ValueError(message)
+
+
+def _as_tuple(v) -> tuple:
+    return (v,) if isinstance(v, (int, float)) else tuple(v)
+
+
 @dataclass(frozen=True, slots=True)
 class CPML:
     """Convolutional PML boundary configuration."""
@@ -40,9 +50,8 @@ class CPML:
     width: int | tuple[int, ...] = 20
 
     def __post_init__(self) -> None:
-        widths = (self.width,) if isinstance(self.width, int) else self.width
-        if not widths or any(w < 0 for w in widths):
-            raise ValueError("CPML widths must be non-negative.")
+        w = _as_tuple(self.width)
+        _check(len(w) > 0 and min(w) >= 0, "CPML width(s) must be given and be >= 0.")
 
 
 @dataclass(frozen=True, slots=True)
@@ -54,15 +63,12 @@ class Discretization:
     max_velocity: float | None = None
 
     def __post_init__(self) -> None:
-        sp = (self.spacing,) if isinstance(self.spacing, (int, float)) else self.spacing
-        if not sp or any(v <= 0 for v in sp):
-            raise ValueError("Grid spacing must be positive.")
-        if self.dt <= 0:
-            raise ValueError("dt must be positive.")
-        if self.stencil not in {2, 4, 6, 8}:
-            raise ValueError("stencil must be one of 2, 4, 6, or 8.")
-        if self.max_velocity is not None and self.max_velocity <= 0:
-            raise ValueError("max_velocity must be positive when provided.")
+        h = _as_tuple(self.spacing)
+        _check(len(h) > 0 and min(h) > 0, "Grid spacing must be > 0 along every axis.")
+        _check(self.dt > 0, "dt must be > 0.")
+        _check(self.stencil in (2, 4, 6, 8), f"stencil {self.stencil} is not 2, 4, 6 or 8.")
+        _check(self.max_velocity is None or self.max_velocity > 0,
+               "max_velocity, when given, must be > 0.")
 
 
 @dataclass(frozen=True, slots=True)
@@ -98,10 +104,9 @@ class Experiment:
     receiver_component: str = "ey"
 
     def __post_init__(self) -> None:
-        if self.nt is not None and self.nt <= 0:
-            raise ValueError("nt must be positive when provided.")
-        if self.source_amplitude is None and self.nt is None:
-            raise ValueError("nt is required when source_amplitude is absent.")
+        _check(self.nt is None or self.nt > 0, "nt, when given, must be > 0.")
+        _check(self.nt is not None or self.source_amplitude is not None,
+               "Without source amplitudes the number of steps nt must be given.")
 
 
 @dataclass(frozen=True, slots=True)
@@ -112,12 +117,10 @@ class EMModel:
     dispersion: ph.DebyeDispersion | None = None
 
     def __post_init__(self) -> None:
-        if self.sigma.shape != self.epsilon.shape or self.mu.shape != self.epsilon.shape:
-            raise ValueError("epsilon, sigma, and mu must have the same shape.")
-        if self.sigma.device != self.epsilon.device or self.mu.device != self.epsilon.device:
-            raise ValueError("epsilon, sigma, and mu must be on the same device.")
-        if self.sigma.dtype != self.epsilon.dtype or self.mu.dtype != self.epsilon.dtype:
-            raise ValueError("epsilon, sigma, and mu must have the same dtype.")
+        ts = (self.epsilon, self.sigma, self.mu)
+        for what in ("shape", "device", "dtype"):
+            _check(len({getattr(t, what) for t in ts}) == 1,
+                   f"The epsilon, sigma and mu tensors differ in {what}.")
 
 
 @dataclass(frozen=True, slots=True)
@@ -127,8 +130,7 @@ class Observers:
     frequency: int = 1
 
     def __post_init__(self) -> None:
-        if self.frequency <= 0:
-            raise ValueError("Observer frequency must be positive.")
+        _check(self.frequency > 0, "Observer frequency must be >= 1.")
 
 
 @dataclass(frozen=True, slots=True)
@@ -151,8 +153,8 @@ class TMState:
 
     @classmethod
     def from_tensors(cls, tensors) -> TMState:
-        if len(tensors) != 7:
-            raise ValueError(f"TM state requires 7 tensors, got {len(tensors)}.")
+        _check(len(tensors) == 7, f"A TM state has 7 tensors (Ey, Hx, Hz and four CPML "
+                                  f"memories); {len(tensors)} were given.")
         return cls(*tensors)
 
 
@@ -182,8 +184,8 @@ class EM3DState:
 
     @classmethod
     def from_tensors(cls, tensors) -> EM3DState:
-        if len(tensors) != 18:
-            raise ValueError(f"EM3D state requires 18 tensors, got {len(tensors)}.")
+        _check(len(tensors) == 18, f"A 3-D state has 18 tensors (six fields, twelve CPML "
+                                   f"memories); {len(tensors)} were given.")
         return cls(*tensors)
 
     def tensors(self) -> tuple:
@@ -205,19 +207,13 @@ class EMDirection:
     mu: torch.Tensor | None = None
 
     def validate_for(self, model: EMModel) -> None:
-        if self.epsilon is None and self.sigma is None and self.mu is None:
-            raise ValueError("At least one model direction must be provided.")
-        for name, direction, parameter in (
-            ("epsilon", self.epsilon, model.epsilon),
-            ("sigma", self.sigma, model.sigma),
-            ("mu", self.mu, model.mu),
-        ):
-            if direction is not None and (
-                direction.shape != parameter.shape
-                or direction.device != parameter.device
-                or direction.dtype != parameter.dtype
-            ):
-                raise ValueError(f"The {name} direction must match the corresponding model tensor.")
+        given = {n: getattr(self, n) for n in ("epsilon", "sigma", "mu")
+                 if getattr(self, n) is not None}
+        _check(bool(given), "The direction is empty: give epsilon, sigma and/or mu.")
+        for n, d in given.items():
+            m = getattr(model, n)
+            _check((d.shape, d.device, d.dtype) == (m.shape, m.device, m.dtype),
+                   f"The {n} direction differs from the model's {n} in shape, device or dtype.")
 
 
 @dataclass(frozen=True, slots=True)
