@@ -404,7 +404,9 @@ TIDE_3D_DECLARE(8, double)
  * sources f0) and scattered state (dex .. dm_ey_x, sources df) advance
  * together; the scattered E update adds dca E^n + dcb curl H^n of the
  * background.  r records the scattered, background_r (may be null) the
- * background receiver component.  CPML memories compacted as for forward. */
+ * background receiver component.  CPML memories are full [S, nz, ny, nx]
+ * arrays on the Born entry points (the reference's Born callers allocate
+ * them so; its forward / backward entry points use the compact layout). */
 #define TIDE_3D_BORN_FORWARD_ARGS(T)                                           \
   T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
       T const *f0, T const *df, T *ex, T *ey, T *ez, T *hx, T *hy, T *hz,      \

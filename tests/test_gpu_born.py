@@ -213,7 +213,8 @@ def _born3d_cuda(pb, dca, dcb, df, dev):
     q.profiles = {k: mv(v) for k, v in pb.profiles.items()}
     q.sources_i, q.receivers_i = mv(pb.sources_i), mv(pb.receivers_i)
     q.fields = [mv(t) for t in pb.fields]
-    q.memories = [mv(t) for t in pb.memories]
+    # full-layout CPML memories on the Born entry point
+    q.memories = [mv(pb.layout.unpack(t, a)) for t, a in zip(pb.memories, em3d.MEM_AXES)]
     q.device = torch.device(dev)
     dfields = [torch.zeros_like(t) for t in q.fields]
     dmem = [torch.zeros_like(t) for t in q.memories]
@@ -230,7 +231,7 @@ def _born3d_cuda(pb, dca, dcb, df, dev):
        dev.index or 0, 0, torch.cuda.current_stream(dev).cuda_stream)
     nat.check("born_forward 3-D")
     torch.cuda.synchronize()
-    full = lambda mems: [q.layout.unpack(m.cpu(), a) for m, a in zip(mems, em3d.MEM_AXES)]  # noqa: E731
+    full = lambda mems: [m.cpu() for m in mems]  # noqa: E731
     return r, bg, q.fields + full(q.memories), dfields + full(dmem)
 
 

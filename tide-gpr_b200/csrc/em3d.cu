@@ -46,30 +46,13 @@ template <typename T> struct G3 {
   int nz, ny, nx, S;
   int64_t N;
   int z0, y0, x0, z1, y1, x1, z1h, y1h, x1h;
-  int ezc, eyc, exc;  // compact extents along z, y, x
+  int zhs, yhs, xhs;  // first kept cell of each axis's upper strip (compact layout)
+  int ezc, eyc, exc;  // memory extents along z, y, x
   int P;              // half stencil width: update domain [P, n - P + 1) per axis
   bool ca_b, cb_b, cq_b;
 };
 
 template <typename T> __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
-
-// Compact memory index of cell (s, z, y, x) for a memory of `axis`.
-template <typename T, int AXIS>
-__device__ __forceinline__ int64_t cidx(const G3<T> &g, int s, int z, int y, int x) {
-  if (AXIS == 0) {
-    const int hs = max(g.z0, g.z1 - 1);
-    const int c = z < g.z0 ? z : (z >= hs ? g.z0 + z - hs : 0);
-    return (((int64_t)s * g.ezc + c) * g.ny + y) * g.nx + x;
-  } else if (AXIS == 1) {
-    const int hs = max(g.y0, g.y1 - 1);
-    const int c = y < g.y0 ? y : (y >= hs ? g.y0 + y - hs : 0);
-    return (((int64_t)s * g.nz + z) * g.eyc + c) * g.nx + x;
-  } else {
-    const int hs = max(g.x0, g.x1 - 1);
-    const int c = x < g.x0 ? x : (x >= hs ? g.x0 + x - hs : 0);
-    return (((int64_t)s * g.nz + z) * g.ny + y) * g.exc + c;
-  }
-}
 
 // d / k for a CPML kappa k > 0; a zero numerator (a field the wave has not
 // reached) divides 1 instead so the division stays on its fast path, and d
@@ -128,10 +111,11 @@ __device__ __forceinline__ bool column(const G3<T> &g, Col &c) {
   return c.zb < c.ze;
 }
 
-// Compact coordinate of a strip cell c along an axis whose memories keep
-// c < lo and c >= max(lo, hi - 1).
-__device__ __forceinline__ int ccoord(int c, int lo, int hi) {
-  const int hs = max(lo, hi - 1);
+// Memory coordinate of a strip cell c along an axis whose memories keep the
+// cells c < lo and c >= hs: the compact layout of the forward and adjoint
+// entry points has hs = max(lo, hi - 1), the full layout of the Born entry
+// points hs = lo (identity).
+__device__ __forceinline__ int ccoord(int c, int lo, int hs) {
   return c < lo ? c : lo + c - hs;
 }
 
@@ -181,8 +165,8 @@ k3_fwd_h(G3<T> g, const T *__restrict__ cq, const T *__restrict__ ex, const T *_
   const bool yok = y < ny - 1, xok = x < nx - 1;
   const bool py = y < g.y0 || y >= g.y1h, px = x < g.x0 || x >= g.x1h;
   const Prof<T> fy = prof_at(g, PAYH, PKYH, y, py && yok), fx = prof_at(g, PAXH, PKXH, x, px && xok);
-  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
-  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.yhs) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.xhs), s2 = (int64_t)ny * g.exc;
   auto load = [&](int z, int64_t jj) {
     OpsH<T> o{};
     o.q = ld(cq + jj);
@@ -215,7 +199,7 @@ k3_fwd_h(G3<T> g, const T *__restrict__ cq, const T *__restrict__ ex, const T *_
       T d = (o.n_y - e_y) * g.rdz;
       T d2 = (o.n_x - e_x) * g.rdz;
       if (z < g.z0 || z >= g.z1h) {
-        const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+        const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
         const T b = ld(g.p[PBZH] + z), a = ld(g.p[PAZH] + z), k = ld(g.p[PKZH] + z);
         const T m1 = b * m_ey_z[m] + a * d;
         m_ey_z[m] = m1;
@@ -296,8 +280,8 @@ k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restr
   m_hz_x += c.s * msz2(g); m_hy_x += c.s * msz2(g);
   const bool py = y < g.y0 || y >= g.y1, px = x < g.x0 || x >= g.x1;
   const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
-  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
-  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.yhs) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.xhs), s2 = (int64_t)ny * g.exc;
   auto load = [&](int64_t jj) {
     OpsE<T> o;
     o.a = ld(ca + jj);
@@ -327,7 +311,7 @@ k3_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__restr
     T dHx_dy = (o.h_x - o.hx_y) * g.rdy;
     T dHy_dx = (o.h_y - o.hy_x) * g.rdx;
     if (z < g.z0 || z >= g.z1) {
-      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       const T bb = ld(g.p[PBZ] + z), aa = ld(g.p[PAZ] + z), k = ld(g.p[PKZ] + z);
       const T m1 = bb * m_hy_z[m] + aa * dHy_dz;
       m_hy_z[m] = m1;
@@ -409,8 +393,8 @@ k3_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
   }
   const bool py = y < g.y0 || y >= g.y1, px = x < g.x0 || x >= g.x1;
   const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
-  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x, s1 = (int64_t)g.eyc * nx;
-  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1), s2 = (int64_t)ny * g.exc;
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.yhs) * nx + x, s1 = (int64_t)g.eyc * nx;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.xhs), s2 = (int64_t)ny * g.exc;
   const T *H[2][3] = {{hx, hy, hz}, {dhx, dhy, dhz}};
   int64_t j = ((int64_t)c.zb * ny + y) * nx + x;
   T p_x[2], p_y[2];  // Hx, Hy at z - 1 of both states
@@ -423,7 +407,7 @@ k3_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
     const bool pz = z < g.z0 || z >= g.z1;
     Prof<T> fz{(T)0, (T)0, (T)1};
     if (pz) fz = prof_at(g, PAZ, PKZ, z, true);
-    const int64_t m0 = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+    const int64_t m0 = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
     T cu[2][3];
 #pragma unroll
     for (int w = 0; w < 2; ++w) {
@@ -556,10 +540,10 @@ k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
   const Prof<T> fy = prof_at(g, PAY, PKY, y, py), fx = prof_at(g, PAX, PKX, x, px);
   const Prof<T> fy1 = prof_at(g, PAY, PKY, y + 1, py1), fx1 = prof_at(g, PAX, PKX, x + 1, px1);
   const int64_t s1 = (int64_t)g.eyc * nx, s2 = (int64_t)ny * g.exc;
-  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x;
-  const int64_t o1n = (int64_t)ccoord(y + 1, g.y0, g.y1) * nx + x;
-  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1);
-  const int64_t o2n = (int64_t)y * g.exc + ccoord(x + 1, g.x0, g.x1);
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.yhs) * nx + x;
+  const int64_t o1n = (int64_t)ccoord(y + 1, g.y0, g.yhs) * nx + x;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.xhs);
+  const int64_t o2n = (int64_t)y * g.exc + ccoord(x + 1, g.x0, g.xhs);
   auto load = [&](int64_t jj) {
     OpsAE<T> o{};
     o.b = ld(cb + jj);
@@ -589,7 +573,7 @@ k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
     T m_hx = 0, m_hy = 0;
     Prof<T> fz{(T)0, (T)0, (T)1};
     if (pz) {
-      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       m_hx = ld(c_hx_z + m);
       m_hy = ld(c_hy_z + m);
       fz = prof_at(g, PAZ, PKZ, z, true);
@@ -607,7 +591,7 @@ k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
     if (z + 1 < nz) on = load(j + sz);
     const T qx = o.b * o.lx, qy = o.b * o.ly, qz = o.b * o.lz;
     if (z < g.z0 || z >= g.z1) {
-      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       const T bz = ld(g.p[PBZ] + z);
       n_hy_z[m] = bz * ld(c_hy_z + m) + qx;
       n_hx_z[m] = bz * ld(c_hx_z + m) - qy;
@@ -715,10 +699,10 @@ k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
   const Prof<T> fym = prof_at(g, PAYH, PKYH, y - 1, pym);
   const Prof<T> fxm = prof_at(g, PAXH, PKXH, x - 1, pxm);
   const int64_t s1 = (int64_t)g.eyc * nx, s2 = (int64_t)ny * g.exc;
-  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.y1) * nx + x;
-  const int64_t o1m = (int64_t)ccoord(y - 1, g.y0, g.y1) * nx + x;
-  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.x1);
-  const int64_t o2m = (int64_t)y * g.exc + ccoord(x - 1, g.x0, g.x1);
+  const int64_t o1 = (int64_t)ccoord(y, g.y0, g.yhs) * nx + x;
+  const int64_t o1m = (int64_t)ccoord(y - 1, g.y0, g.yhs) * nx + x;
+  const int64_t o2 = (int64_t)y * g.exc + ccoord(x, g.x0, g.xhs);
+  const int64_t o2m = (int64_t)y * g.exc + ccoord(x - 1, g.x0, g.xhs);
   auto load = [&](int64_t jj) {
     OpsAH<T> o{};
     o.q = ld(cq + jj);
@@ -753,7 +737,7 @@ k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
     T m_ey = 0, m_ex = 0;
     Prof<T> fz{(T)0, (T)0, (T)1};
     if (pz) {
-      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       m_ey = ld(c_ey_z + m);
       m_ex = ld(c_ex_z + m);
       fz = prof_at(g, PAZH, PKZH, z, true);
@@ -774,7 +758,7 @@ k3_adj_h(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
     const bool pz = zok && (z < g.z0 || z >= g.z1h);
     T m_eyz = 0, m_exz = 0;
     if (pz) {
-      const int64_t m = ((int64_t)ccoord(z, g.z0, g.z1) * ny + y) * nx + x;
+      const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       const T bz = ld(g.p[PBZH] + z);
       m_eyz = ld(c_ey_z + m);
       m_exz = ld(c_ex_z + m);
@@ -949,7 +933,8 @@ template <typename T> struct Launch3 {
 template <typename T>
 bool make3(Launch3<T> &L, int stencil, const T *const prof[kNProf], T rdz, T rdy, T rdx, int64_t S,
            int64_t nz, int64_t ny, int64_t nx, int64_t pz0, int64_t py0, int64_t px0,
-           int64_t pz1, int64_t py1, int64_t px1, bool ca_b, bool cb_b, bool cq_b) {
+           int64_t pz1, int64_t py1, int64_t px1, bool ca_b, bool cb_b, bool cq_b,
+           bool compact = true) {
   const int P = stencil / 2;
   if (S < 1 || nz < 2 * P || ny < 2 * P || nx < 2 * P || nz > (1 << 20) || ny > (1 << 20) ||
       nx > (1 << 20) || nz * ny * nx > ((int64_t)1 << 40) ||
@@ -978,9 +963,12 @@ bool make3(Launch3<T> &L, int stencil, const T *const prof[kNProf], T rdz, T rdy
   g.z1h = pz1 > pz0 ? (int)pz1 - 1 : (int)pz0;
   g.y1h = py1 > py0 ? (int)py1 - 1 : (int)py0;
   g.x1h = px1 > px0 ? (int)px1 - 1 : (int)px0;
-  g.ezc = (int)(pz0 + nz - std::max(pz0, pz1 - 1));
-  g.eyc = (int)(py0 + ny - std::max(py0, py1 - 1));
-  g.exc = (int)(px0 + nx - std::max(px0, px1 - 1));
+  g.zhs = (int)(compact ? std::max(pz0, pz1 - 1) : pz0);
+  g.yhs = (int)(compact ? std::max(py0, py1 - 1) : py0);
+  g.xhs = (int)(compact ? std::max(px0, px1 - 1) : px0);
+  g.ezc = (int)pz0 + g.nz - g.zhs;
+  g.eyc = (int)py0 + g.ny - g.yhs;
+  g.exc = (int)px0 + g.nx - g.xhs;
   g.P = P;
   g.ca_b = ca_b; g.cb_b = cb_b; g.cq_b = cq_b;
   L.grid = dim3((unsigned)((nx + 31) / 32), (unsigned)((ny + 7) / 8),
@@ -1396,9 +1384,11 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
     return;
   const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
                            kz, kzh, ky, kyh, kx, kxh};
+  // The Born entry points take full [S, nz, ny, nx] CPML memories
+  // (maxwell_3d_cuda_inst.cu:3871-3890 sets the compact flag off there).
   Launch3<T> L;
   if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
-             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched, /*compact=*/false))
     return;
   cudaStream_t st = stream_of(compute_stream);
   T *F[6] = {ex, ey, ez, hx, hy, hz}, *DF[6] = {dex, dey, dez, dhx, dhy, dhz};

@@ -68,9 +68,9 @@ __device__ __forceinline__ T cpml(T d, T *__restrict__ mem, int64_t m, const Pro
 // Compact in-shot index of (z, y, x) in a memory of `AXIS`.
 template <typename T, int AXIS>
 __device__ __forceinline__ int64_t pmi(const G3<T> &g, int z, int y, int x) {
-  if (AXIS == 0) return ((int64_t)ccoord(z, g.z0, g.z1) * g.ny + y) * g.nx + x;
-  if (AXIS == 1) return ((int64_t)z * g.eyc + ccoord(y, g.y0, g.y1)) * g.nx + x;
-  return ((int64_t)z * g.ny + y) * g.exc + ccoord(x, g.x0, g.x1);
+  if (AXIS == 0) return ((int64_t)ccoord(z, g.z0, g.zhs) * g.ny + y) * g.nx + x;
+  if (AXIS == 1) return ((int64_t)z * g.eyc + ccoord(y, g.y0, g.yhs)) * g.nx + x;
+  return ((int64_t)z * g.ny + y) * g.exc + ccoord(x, g.x0, g.xhs);
 }
 
 // --------------------------------------------------------------- forward H

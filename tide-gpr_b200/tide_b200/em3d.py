@@ -648,10 +648,13 @@ def born3d(
         and bool(torch.equal(bg_receiver_location.to(dev), receiver_location.to(dev))))
     r = torch.zeros((pb.nt, S, pb.n_rec), device=dev, dtype=dtype)
     bg_r = torch.zeros_like(r) if same_rec else torch.empty(0, device=dev, dtype=dtype)
+    # the Born entry points keep full [S, nz, ny, nx] CPML memories
+    bg_mem = [pb.layout.unpack(m, a).contiguous() for m, a in zip(pb.memories, MEM_AXES)]
+    sc_mem = [pb.layout.unpack(m, a).contiguous() for m, a in zip(sc_mem, MEM_AXES)]
     fn = nat.get_backend_function("maxwell_3d", "born_forward", pb.stencil, dtype, dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
     fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca_p), _p(dcb_p), _p(pb.f), _p(df),
-       *[_p(t) for t in pb.fields], *[_p(t) for t in pb.memories],
+       *[_p(t) for t in pb.fields], *[_p(t) for t in bg_mem],
        *[_p(t) for t in sc_fields], *[_p(t) for t in sc_mem], _p(r), _p(bg_r),
        *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
        pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, n_src, pb.n_rec, 1,
@@ -672,6 +675,6 @@ def born3d(
     s = _crop(pb)
 
     def outs(fields, mems):
-        return [t[s] for t in fields] + [pb.layout.unpack(m, a)[s] for m, a in zip(mems, MEM_AXES)]
+        return [t[s] for t in fields] + [m[s] for m in mems]
 
-    return (*outs(pb.fields, pb.memories), *outs(sc_fields, sc_mem), bg_r, r)
+    return (*outs(pb.fields, bg_mem), *outs(sc_fields, sc_mem), bg_r, r)
