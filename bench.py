@@ -364,6 +364,9 @@ def run_b200(args) -> None:
             "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
         }
 
+    tma_leg = None
+    if rank == 0 and world == 1 and args.tma_nt > 0:
+        tma_leg = tma_bench(args, dev, batch, snap_bytes)
     serving = em3d_leg = debye_leg = None
     stg.release_history_pool()  # the other legs budget device memory themselves
     if rank == 0 and world == 1 and args.serve_jobs > 0:
@@ -392,6 +395,7 @@ def run_b200(args) -> None:
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
+            "tma_path": tma_leg,
             "serving": serving,
             "em3d": em3d_leg, "debye": debye_leg,
         }
@@ -401,6 +405,61 @@ def run_b200(args) -> None:
 
         dist.barrier()
         dist.destroy_process_group()
+
+
+def tma_bench(args, dev, batch: int, snap_bytes: int) -> dict:
+    """The one-sweep TMA time steps (opt-in, tide_b200_set_tma_mode) against
+    the default per-call kernels on one batch of the same workload: first
+    `batch` shots, tma_nt steps, fwd + adj through the public API, CUDA-event
+    device time of the whole evaluation and per-kernel event samples."""
+    cfg = config2(shots=batch, nt=args.tma_nt, device=dev)
+    L = lib()
+    peak, peak_kind = hbm_peak()
+    rho_x, rho_y = 41 / PADDED[1], 41 / PADDED[0]
+
+    def once():
+        eps = cfg["eps"].detach().requires_grad_(True)
+        sig = cfg["sig"].detach().requires_grad_(True)
+        out = tide.maxwelltm(eps, sig, cfg["mu"], cfg["dx"], cfg["dt"], cfg["amp"], cfg["src"],
+                             cfg["rec"], stencil=2, pml_width=cfg["pml"], storage_mode="device",
+                             storage_compression=args.storage == "bf16")
+        (0.5 * (out[-1] * out[-1]).sum()).backward()
+        return torch.stack([eps.grad, sig.grad])
+
+    res = {}
+    grads = {}
+    for name, mode in (("default", 0), ("tma", 2)):
+        prev = nat.set_tma_mode(mode)
+        try:
+            once()
+            once()  # warm-up (pool, tensor maps)
+            ms, g = _timed_gpu(once, dev)
+            L.tide_b200_profile_enable(1, 10)
+            read_profile(L)
+            once()
+            torch.cuda.synchronize(dev)
+            L.tide_b200_profile_enable(0, 1)
+            prof = {k: v for k, v in read_profile(L).items() if v[1] > 0}
+        finally:
+            nat.set_tma_mode(prev)
+        grads[name] = g
+        kern = {}
+        for k, (tot, n) in prof.items():
+            avg = tot / n
+            bpc = kernel_bytes_per_cell(k, batch, snap_bytes, rho_x, rho_y)
+            ach = bpc * batch * PADDED[0] * PADDED[1] / (avg / 1e3) / 1e9
+            kern[k] = {"avg_launch_ms": round(avg, 5), "achieved_gbs": round(ach, 1),
+                       "frac": round(ach / peak, 4)}
+        res[name] = {"ms_per_eval": ms,
+                     "cell_updates_per_s": 2.0 * batch * PADDED[0] * PADDED[1] * args.tma_nt / (ms / 1e3),
+                     "kernels": kern}
+    d = grads["tma"] - grads["default"]
+    res["grad_bitwise_equal"] = bool(torch.equal(grads["tma"], grads["default"]))
+    res["grad_max_abs_diff"] = float(d.abs().max())
+    res["workload"] = (f"config2 grid, {batch} shots, nt={args.tma_nt}, snapshots {args.storage} "
+                       "on device; fwd+adj through the public API")
+    res["peak"] = {"hbm_gbs": peak, "source": peak_kind}
+    return res
 
 
 # ---------------------------------------------------------------- serving
@@ -862,6 +921,8 @@ def main() -> None:
     ap.add_argument("--serve-plain-jobs", type=int, default=32)
     ap.add_argument("--serve-chunk", type=int, default=32)
     ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--tma-nt", type=int, default=400,
+                    help="steps of the TMA-path comparison leg (0: skip)")
     ap.add_argument("--em3d-nt", type=int, default=1500,
                     help="steps of the 3-D (config 4) leg, checkpointed (0: skip)")
     ap.add_argument("--em3d-host-nt", type=int, default=60,

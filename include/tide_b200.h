@@ -481,8 +481,8 @@ int64_t tide_b200_set_fused_threshold(int64_t bytes);
  * FP32 stencil-2 forward, forward_with_storage and backward with model
  * coefficients shared by the shots and no Debye poles run one launch per time
  * step on TMA-staged tiles (both half steps fused) on persistent CTAs.
- * 0 = never, 1 = when the grid has at least 64 tiles of 32 x 64 cells
- * (default), 2 = whenever eligible.  Results are bit-identical in every mode.
+ * 0 = never (default), 1 = when the grid has at least 64 tiles of 32 x 64
+ * cells, 2 = whenever eligible.  Results are bit-identical in every mode.
  * Returns the previous mode; process-wide, takes effect at the next call. */
 int tide_b200_set_tma_mode(int mode);
 

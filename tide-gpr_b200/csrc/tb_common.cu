@@ -71,6 +71,22 @@ void give_event(cudaEvent_t e) {
 
 void count_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st) {
+  static std::atomic<uint64_t> kept{0};  // bit d: device d's pool configured
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 64 && !(kept.load() & (1ull << dev))) {
+    cudaMemPool_t pool;
+    uint64_t keep = UINT64_MAX;
+    e = cudaDeviceGetDefaultMemPool(&pool, dev);
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    kept.fetch_or(1ull << dev);
+  }
+  return cudaMallocAsync(p, bytes, st);
+}
+
 ProfileScope::ProfileScope(cudaStream_t st)
     : st_(st), on_(g_prof_on.load() != 0), every_(std::max(1, g_prof_every.load())) {}
 

@@ -43,6 +43,11 @@ enum KernelKind : int {
 };
 void count_launches(int64_t n);
 
+// cudaMallocAsync on the current device's default pool, with the pool told
+// (once per device) to keep freed memory instead of releasing it at every
+// synchronisation, so per-call scratch is a pool hit after the first call.
+cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st);
+
 // Brackets sampled launches with events on one stream; accumulates into the
 // process-wide profile when the scope closes (after waiting for its events).
 class ProfileScope {

@@ -176,7 +176,9 @@ bool build_points(PointScratch &ps, const Launch<T, ST> &L, const PointTiles &pt
   const size_t ns = want_s ? (size_t)(n_src * S) : 0, nr = want_r ? (size_t)(n_rec * S) : 0;
   const size_t words = (want_s ? 2 * nt1 + 2 * ns : 0) + (want_r ? 2 * nt1 + 2 * nr : 0);
   const int n_rows = pt.tiles_y * (int)S;
-  if (TB_CUDA(cudaMallocAsync(&ps.mem, words * sizeof(int) + (size_t)n_rows, st))) return false;
+  if (TB_CUDA(pool_malloc(reinterpret_cast<void **>(&ps.mem),
+                          words * sizeof(int) + (size_t)n_rows, st)))
+    return false;
   int *w = static_cast<int *>(ps.mem);
   if (want_s) {
     int *count = w, *start = w + nt1, *cell = w + 2 * nt1, *ent = w + 2 * nt1 + ns;
@@ -294,7 +296,7 @@ struct PitchedFwd {
     const size_t state = (size_t)(rows + 2) * q.pitch;
     size_t total = 12 * state;
     for (int i = 0; i < 3; ++i) total += (size_t)(rc[i] + 2) * q.pitch;
-    if (TB_CUDA(cudaMallocAsync(&mem, total * sizeof(float), st))) return false;
+    if (TB_CUDA(pool_malloc(&mem, total * sizeof(float), st))) return false;
     if (TB_CUDA(cudaMemsetAsync(mem, 0, total * sizeof(float), st))) return false;
     float *p = static_cast<float *>(mem);
     auto take = [&](size_t n) {
@@ -351,15 +353,17 @@ template <typename T> constexpr bool is_float() { return std::is_same<T, float>:
 // pitched copies (ping-pong) and its coefficients into a pitched copy,
 // encodes the tensor maps of both copies once, runs one launch per time
 // step on P = min(SMs, tiles) persistent CTAs and copies the final state
-// back.  Mode (tide_b200_set_tma_mode): 0 off, 1 when the grid has at least
-// kQMinTiles tiles (default), 2 whenever eligible.
-std::atomic<int> g_tma_mode{1};
+// back.  Mode (tide_b200_set_tma_mode): 0 off (default: on the 553 x 1065,
+// 8-shot gradient workload these kernels issue about 270 instructions per
+// cell and run slower than the per-call pair kernels), 1 when the grid has
+// at least kQMinTiles tiles, 2 whenever eligible.
+std::atomic<int> g_tma_mode{0};
 std::atomic<int> g_tma_max_ctas{0};  // 0: one CTA per SM (tide_b200_set_tma_ctas)
 constexpr int kQTY = 32;        // tile height of the TMA kernels
 constexpr int kQMinTiles = 64;  // auto mode: below this the per-call kernels win
 
 template <bool ADJ> struct QRun {
-  using B = QBox<kQTY>;
+  using B = QBox;
   cudaStream_t st = nullptr;
   void *mem = nullptr;
   int64_t pitch = 0, pshot = 0;
@@ -375,6 +379,7 @@ template <bool ADJ> struct QRun {
   // adjoint: hand-off sums and flags
   float *hand = nullptr;
   int *flags = nullptr;
+  int *order = nullptr;  // grid tile at each position of the tile sequence
   int epoch = 0;
   ~QRun() {
     if (mem) cudaFreeAsync(mem, st);
@@ -413,10 +418,11 @@ template <bool ADJ> struct QRun {
     P = std::max(1, std::min(cap > 0 ? std::min(cap, n_sm) : n_sm, tiles_x * tiles_y));
     const size_t state = (size_t)S * (size_t)pshot;
     const size_t N = (size_t)ny * nx;
-    size_t total = 6 * state + 3 * (size_t)pshot;
+    const int tiles = tiles_x * tiles_y;
+    size_t total = 6 * state + 3 * (size_t)pshot + (size_t)tiles;
     if (ADJ) total += (size_t)P * 2 * kQTY * kQX + (size_t)P;
     else total += 2 * (size_t)S * N;
-    if (TB_CUDA(cudaMallocAsync(&mem, total * sizeof(float), st))) return false;
+    if (TB_CUDA(pool_malloc(&mem, total * sizeof(float), st))) return false;
     float *p = static_cast<float *>(mem);
     for (int k = 0; k < 2; ++k)
       for (int i = 0; i < 3; ++i) {
@@ -427,6 +433,9 @@ template <bool ADJ> struct QRun {
       coef[i] = p;
       p += pshot;
     }
+    order = reinterpret_cast<int *>(p);
+    p += tiles;
+    if (!upload_order(g)) return false;
     for (int i = 0; i < 3; ++i) {
       user[i] = fields[i];
       if (!copy2d(f[0][i], pitch, fields[i], nx, (int64_t)S * ny)) return false;
@@ -469,16 +478,46 @@ template <bool ADJ> struct QRun {
     return true;
   }
 
-  QCommon common(const TMGeom<float> &g, const PointScratch &ps, const float *v0,
-                 float *v1) const {
+  // Tile sequence: tiles that take the CPML / edge path are spread evenly
+  // between the interior ones (tile k of a class of n goes to key (k+0.5)/n),
+  // so every CTA's contiguous range of units holds the same mix.
+  bool upload_order(const TMGeom<float> &g) {
+    const int tiles = tiles_x * tiles_y;
+    std::vector<std::pair<double, int>> key;
+    key.reserve(tiles);
+    int n_cls[2] = {0, 0};
+    std::vector<int> cls(tiles);
+    for (int t = 0; t < tiles; ++t) {
+      const int y0 = (t / tiles_x) * kQTY, x0 = (t % tiles_x) * kQX;
+      const bool in = y0 - 1 >= std::max(1, g.pml_y0) && y0 + kQTY < std::min(g.ny, g.pml_y1) &&
+                      x0 - 1 >= std::max(1, g.pml_x0) && x0 + kQX < std::min(g.nx, g.pml_x1);
+      cls[t] = in ? 0 : 1;
+      ++n_cls[cls[t]];
+    }
+    int seen[2] = {0, 0};
+    for (int t = 0; t < tiles; ++t) {
+      const int c = cls[t];
+      key.emplace_back((seen[c]++ + 0.5) / n_cls[c] + 1e-9 * c, t);
+    }
+    std::stable_sort(key.begin(), key.end());
+    std::vector<int> h(tiles);
+    for (int t = 0; t < tiles; ++t) h[t] = key[t].second;
+    return !TB_CUDA(cudaMemcpyAsync(order, h.data(), sizeof(int) * tiles,
+                                    cudaMemcpyHostToDevice, st)) &&
+           !TB_CUDA(cudaStreamSynchronize(st));
+  }
+
+  QCommon common(const TMGeom<float> &g, const PointScratch &ps, const float *va,
+                 float *vb) const {
     QCommon c{};
     c.g = g;
     c.tiles_x = tiles_x; c.tiles_y = tiles_y; c.P = P;
+    c.order = order;
     c.pitch = pitch; c.pshot = pshot;
     c.ey_n = f[cur ^ 1][0]; c.hx_n = f[cur ^ 1][1]; c.hz_n = f[cur ^ 1][2];
-    c.p0 = ADJ ? ps.rec : ps.src;
-    c.p1 = ADJ ? ps.src : ps.rec;
-    c.v0 = v0; c.v1 = v1;
+    c.pa = ADJ ? ps.rec : ps.src;
+    c.pb = ADJ ? ps.src : ps.rec;
+    c.va = va; c.vb = vb;
     return c;
   }
 
@@ -490,10 +529,10 @@ template <bool ADJ> struct QRun {
     const uint64_t bit = uint64_t(1) << (dev & 63);
     if (done.load() & bit) return true;
     const cudaError_t e =
-        ADJ ? cudaFuncSetAttribute(kq_adj_step<kQTY, SN>,
+        ADJ ? cudaFuncSetAttribute(kq_adj_step<SN>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    B::smem_bytes(true))
-            : cudaFuncSetAttribute(kq_fwd_step<kQTY, SN>,
+            : cudaFuncSetAttribute(kq_fwd_step<SN>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    B::smem_bytes(false));
     if (TB_CUDA(e)) return false;
@@ -512,7 +551,7 @@ template <bool ADJ> struct QRun {
     a.mex_n = mex[cur ^ 1]; a.mez_n = mez[cur ^ 1];
     a.mhx = mhx; a.mhz = mhz;
     a.ey_st = e_st; a.cu_st = c_st;
-    kq_fwd_step<kQTY, SN><<<P, kQThreads, B::smem_bytes(false), st>>>(maps[cur], a);
+    kq_fwd_step<SN><<<P, kQThreads, B::smem_bytes(false), st>>>(maps[cur], a);
     cur ^= 1;
     return true;
   }
@@ -534,7 +573,7 @@ template <bool ADJ> struct QRun {
     a.kscale = kscale;
     a.hand = hand; a.flags = flags;
     a.epoch = ++epoch;
-    kq_adj_step<kQTY, SN><<<P, kQThreads, B::smem_bytes(true), st>>>(maps[cur], a);
+    kq_adj_step<SN><<<P, kQThreads, B::smem_bytes(true), st>>>(maps[cur], a);
     cur ^= 1;
     return true;
   }

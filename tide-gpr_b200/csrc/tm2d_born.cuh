@@ -330,7 +330,7 @@ void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
   cudaStream_t st = as_stream(compute_stream);
   T *scratch = nullptr;
   const size_t bytes = 4 * (size_t)n_shots * (size_t)ny * (size_t)nx * sizeof(T);
-  if (TB_CUDA(cudaMallocAsync((void **)&scratch, bytes > 0 ? bytes : sizeof(T), st))) return;
+  if (TB_CUDA(pool_malloc((void **)&scratch, bytes > 0 ? bytes : sizeof(T), st))) return;
   tm_backward<T, ST>(ca, cb, cq, grad_r, lambda_ey, lambda_hx, lambda_hz, m_lambda_ey_x,
                      m_lambda_ey_z, m_lambda_hx_z, m_lambda_hz_x, scratch, ey_store_1,
                      ey_store_3, ey_filenames, curl_store_1, curl_store_3, curl_filenames,

@@ -428,10 +428,10 @@ __device__ __forceinline__ void adj_h_interior_group(
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     const int64_t base = (int64_t)(s0 + u) * g.N;
+    const int64_t sbase = ga.snap_base(s0 + u, g.N);
 #pragma unroll
     for (int r = 0; r <= R; ++r) hxz[u][r] = ldg(lam_hx + base + j0 + (r - 1) * nx);
 #pragma unroll
-    const int64_t sbase = ga.snap_base(s0 + u, g.N);
     for (int r = 0; r < R; ++r) {
       const int64_t i = base + j0 + r * nx;
       lam[u][r] = lam_ey[i];

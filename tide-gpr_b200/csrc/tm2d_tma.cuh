@@ -14,26 +14,37 @@
 // the adjoint all four (the caller's arrays and adjoint_memory_scratch, as
 // the reference's backward lays them out).
 //
-// Data movement.  A tile is TY rows x 64 columns.  Its three fields (with
-// the halo) arrive in shared memory by 3-D tiled TMA loads (tensor maps over
-// this GPU's pitched buffers; elements outside the grid read as zero), one
-// mbarrier per pipeline stage; the model coefficients of a tile arrive the
-// same way once per tile.  Results go back with coalesced 8-byte stores;
-// snapshots (caller layout, rows of nx cells at any alignment) with
-// streaming scalar stores / loads.
+// Warp roles.  A CTA has 16 compute warps and one producer warp.  The
+// producer walks the CTA's units kQStages ahead of the compute warps: for
+// each it waits until the stage is empty (an mbarrier the compute warps
+// arrive on), stages the tile's point entries (cell, value) and -- on a new
+// tile -- its CPML profile values into shared memory, then issues 3-D tiled
+// TMA loads of the three fields (with the halo) and, on a new tile, of the
+// model coefficients, all completing on the stage's full mbarrier.  The
+// compute warps therefore never issue a transfer and never wait on a
+// dependent global load for profile values or point lists; elements outside
+// the grid read as zero.  Results go back with coalesced stores; snapshots
+// (caller layout, rows of nx cells at any alignment) with streaming scalar
+// stores / loads, the adjoint's loaded one unit ahead.
+//
+// Layout of the work.  A tile is 32 rows x 64 columns; compute warp w owns
+// rows 2w and 2w+1 of it, lane l the columns l and l + 32, so every shared
+// memory access of a warp is 32 consecutive words (no bank conflict) and
+// every store 128 contiguous bytes.
 //
 // Schedule.  The grid is persistent: P CTAs (one per SM; P <= tiles), CTA c
 // owns the units [c U / P, (c+1) U / P) of the tile-major sequence of
-// U = tiles x shots (tile, shot) units, so every CTA gets the same work to
-// within one unit, and a TMA pipeline of kQStages units runs across tile
-// boundaries.  A tile's shots are processed in ascending order, so the
-// adjoint's coefficient gradient is the kernels' step-major shot sum
-// (grad += ((0 + t_0) + t_1) + ...), bit-identical to the other stencil-2
-// kernels and to the oracle in that order.  A tile whose shots are split
-// between CTA c-1 (shots [0, k), processed first) and CTA c (shots [k, S),
-// processed last) hands the running sums over through global memory: CTA
-// c-1 stores them and releases a flag, CTA c acquires it (a bounded wait,
-// normally long satisfied) and continues the sums.
+// U = tiles x shots (tile, shot) units, so every CTA gets the same number of
+// units to within one.  The tile sequence is a host-chosen permutation that
+// spreads the tiles with CPML strips or grid edges (the slower ones) evenly
+// over it, so every CTA gets the same mix.  A tile's shots are processed in
+// ascending order, so the adjoint's coefficient gradient is the kernels'
+// step-major shot sum (grad += ((0 + t_0) + t_1) + ...), bit-identical to
+// the other stencil-2 kernels and to the oracle in that order.  A tile whose
+// shots are split between CTA c-1 (shots [0, k), processed first) and CTA c
+// (shots [k, S), processed last) hands the running sums over through global
+// memory: CTA c-1 stores them and releases a flag, CTA c acquires it (a
+// bounded wait, normally long satisfied) and continues the sums.
 //
 // Numerics.  Every cell value is computed with the same operations in the
 // same order as tm2d_s2.cuh (--fmad=false), so fields, snapshots, receivers,
@@ -45,29 +56,42 @@
 
 namespace tb {
 
-constexpr int kQX = 64;            // tile width (cells)
-constexpr int kQThreads = 512;     // 16 warps per CTA
-constexpr int kQWarps = kQThreads / 32;
-constexpr int kQStages = 3;        // TMA pipeline depth (units in flight)
-constexpr uint32_t kQWaitLimit = 1u << 24;  // bounded waits (polls)
+constexpr int kQX = 64;                          // tile width (cells)
+constexpr int kQTY_ = 32;                        // tile height (cells)
+constexpr int kQCWarps = 16;                     // compute warps
+constexpr int kQCompute = 32 * kQCWarps;         // compute threads
+constexpr int kQThreads = kQCompute + 32;        // + the producer warp
+constexpr int kQStages = 3;                      // units in flight
+constexpr int kQPtCap = 64;                      // point entries staged per list
+constexpr uint32_t kQWaitLimit = 1u << 24;       // bounded waits (polls)
+constexpr int kQPW = kQX + 2;                    // profile columns x0-1 .. x0+64
+constexpr int kQPH = kQTY_ + 2;                  // profile rows y0-1 .. y0+32
 
-// Shared-memory extents (floats) of the staged boxes for a tile of TY rows.
-template <int TY> struct QBox {
+// Bytes rounded up to the 128-byte alignment of every shared-memory buffer.
+constexpr int q_rb(int bytes) { return (bytes + 127) / 128 * 128; }
+
+// Shared-memory extents (floats) of the staged boxes.
+struct QBox {
+  static constexpr int TY = kQTY_;
   static constexpr int EW = kQX + 8, EH = TY + 2;  // rows y0-1..y0+TY,   cols x0-4..x0+67
   static constexpr int XW = kQX, XH = TY + 1;      // rows y0-1..y0+TY-1, cols x0..x0+63
   static constexpr int ZW = kQX + 4, ZH = TY;      // rows y0..y0+TY-1,   cols x0-4..x0+63
   static constexpr int OW = kQX, OH = TY;          // own cells
   static constexpr int QW = kQX + 4, QH = TY + 1;  // rows y0-1..y0+TY-1, cols x0-4..x0+63
-  static constexpr int rb(int n) { return (n * 4 + 127) / 128 * 128; }
-  static constexpr int E_B = rb(EW * EH), X_B = rb(XW * XH), Z_B = rb(ZW * ZH),
-                       O_B = rb(OW * OH), Q_B = rb(QW * QH);
-  static constexpr int STAGE_B = E_B + X_B + Z_B;  // one unit's fields
-  // coefficient slot: adjoint (ca own, cb E-box, cq Q-box); forward (cq, ca, cb own)
-  static constexpr int COEF_ADJ_B = O_B + E_B + Q_B;
-  static constexpr int COEF_FWD_B = Q_B + O_B + O_B;
-  static constexpr int EXTRA_B = X_B + Z_B + O_B;  // new Hx, new Hz, point pass
+  static constexpr int E_B = q_rb(4 * EW * EH), X_B = q_rb(4 * XW * XH),
+                       Z_B = q_rb(4 * ZW * ZH), O_B = q_rb(4 * OW * OH), Q_B = q_rb(4 * QW * QH);
+  // staged point lists: counts (2 ints) then list A (index, value) and list B
+  // (index, entry), kQPtCap each
+  static constexpr int PT_B = q_rb(4 * (2 + 4 * kQPtCap));
+  // CPML profiles of a tile: x (bx ax kx bxh axh kxh) x kQPW, y (by ay ky byh ayh kyh) x kQPH
+  static constexpr int PR_B = q_rb(4 * 6 * (kQPW + kQPH));
+  static constexpr int STAGE_B = E_B + X_B + Z_B + PT_B;
+  static constexpr int COEF_ADJ_B = O_B + E_B + Q_B + PR_B;  // ca, cb (E box), cq (Q box)
+  static constexpr int COEF_FWD_B = Q_B + O_B + O_B + PR_B;  // cq (Q box), ca, cb
+  static constexpr int EXTRA_B = X_B + Z_B;                   // new Hx, new Hz
   static constexpr int smem_bytes(bool adj) {
-    return kQStages * (STAGE_B + (adj ? COEF_ADJ_B : COEF_FWD_B)) + EXTRA_B + 8 * kQStages;
+    return kQStages * (STAGE_B + (adj ? COEF_ADJ_B : COEF_FWD_B)) + EXTRA_B +
+           16 * kQStages;
   }
   // transaction bytes of the boxes
   static constexpr uint32_t FIELD_TX = 4u * (EW * EH + XW * XH + ZW * ZH);
@@ -80,13 +104,13 @@ template <int TY> struct QBox {
 // segment B = whole tiles, segment C = the last shots [cC0, S) of the tile
 // its range starts in (processed last; continues CTA c-1's sums).  Requires
 // P <= tiles, so that a range spans at least S units and a tile is split
-// between at most two CTAs.
+// between at most two CTAs.  Tiles are positions in the tile sequence.
 struct QSched {
   int S;
   int nA, nB, nC;
   int tA, tB0, tC, cC0;
   __device__ __forceinline__ int n() const { return nA + nB + nC; }
-  // (tile, shot, ordinal of the tile in this CTA's sequence, segment 0/1/2)
+  // (sequence tile, shot, ordinal of the tile in this CTA's sequence, segment 0/1/2)
   __device__ __forceinline__ void unit(int i, int &tile, int &shot, int &ord, int &seg) const {
     const int oA = nA > 0 ? 1 : 0;
     if (i < nA) {
@@ -123,44 +147,49 @@ __device__ __forceinline__ QSched q_sched(int c, int P, int tiles, int S) {
   return q;
 }
 
-// Shared memory carve-up: kQStages field stages, kQStages coefficient
-// slots, the new-H tiles, the point-pass tile and the stage barriers.  Stage
-// addresses are computed, not tabulated, so nothing is indexed dynamically
-// in local memory.
-template <int TY, bool ADJ> struct QSmem {
-  using B = QBox<TY>;
+// Shared memory carve-up: kQStages stages (fields + point lists),
+// kQStages coefficient slots (coefficients + profiles), the new-H tiles and
+// the full / empty barriers of the stages.  Addresses are computed, not
+// tabulated, so nothing is indexed dynamically in local memory.
+template <bool ADJ> struct QSmem {
+  using B = QBox;
   static constexpr int COEF_B = ADJ ? B::COEF_ADJ_B : B::COEF_FWD_B;
   static constexpr int COEF0 = kQStages * B::STAGE_B;
   static constexpr int EXTRA0 = COEF0 + kQStages * COEF_B;
   unsigned char *base;
-  float *hxn, *hzn, *ve;
-  uint64_t *full;
+  float *hxn, *hzn;
+  uint64_t *full, *empty;
   __device__ __forceinline__ explicit QSmem(unsigned char *b) : base(b) {
     hxn = reinterpret_cast<float *>(b + EXTRA0);
     hzn = reinterpret_cast<float *>(b + EXTRA0 + B::X_B);
-    ve = reinterpret_cast<float *>(b + EXTRA0 + B::X_B + B::Z_B);
     full = reinterpret_cast<uint64_t *>(b + EXTRA0 + B::EXTRA_B);
+    empty = full + kQStages;
   }
-  __device__ __forceinline__ float *e(int k) const {
-    return reinterpret_cast<float *>(base + k * B::STAGE_B);
-  }
+  __device__ __forceinline__ unsigned char *st(int k) const { return base + k * B::STAGE_B; }
+  __device__ __forceinline__ float *e(int k) const { return reinterpret_cast<float *>(st(k)); }
   __device__ __forceinline__ float *x(int k) const {
-    return reinterpret_cast<float *>(base + k * B::STAGE_B + B::E_B);
+    return reinterpret_cast<float *>(st(k) + B::E_B);
   }
   __device__ __forceinline__ float *z(int k) const {
-    return reinterpret_cast<float *>(base + k * B::STAGE_B + B::E_B + B::X_B);
+    return reinterpret_cast<float *>(st(k) + B::E_B + B::X_B);
+  }
+  __device__ __forceinline__ int *pt(int k) const {
+    return reinterpret_cast<int *>(st(k) + B::E_B + B::X_B + B::Z_B);
+  }
+  __device__ __forceinline__ unsigned char *cs(int k) const {
+    return base + COEF0 + k * COEF_B;
   }
   // adjoint: c0 = ca (own box), c1 = cb (E box), c2 = cq (Q box);
   // forward: c0 = cq (Q box), c1 = ca (own box), c2 = cb (own box)
-  __device__ __forceinline__ float *c0(int k) const {
-    return reinterpret_cast<float *>(base + COEF0 + k * COEF_B);
-  }
+  __device__ __forceinline__ float *c0(int k) const { return reinterpret_cast<float *>(cs(k)); }
   __device__ __forceinline__ float *c1(int k) const {
-    return reinterpret_cast<float *>(base + COEF0 + k * COEF_B + (ADJ ? B::O_B : B::Q_B));
+    return reinterpret_cast<float *>(cs(k) + (ADJ ? B::O_B : B::Q_B));
   }
   __device__ __forceinline__ float *c2(int k) const {
-    return reinterpret_cast<float *>(base + COEF0 + k * COEF_B +
-                                     (ADJ ? B::O_B + B::E_B : B::Q_B + B::O_B));
+    return reinterpret_cast<float *>(cs(k) + (ADJ ? B::O_B + B::E_B : B::Q_B + B::O_B));
+  }
+  __device__ __forceinline__ float *pr(int k) const {
+    return reinterpret_cast<float *>(cs(k) + COEF_B - B::PR_B);
   }
 };
 
@@ -174,11 +203,13 @@ struct QMaps {
 struct QCommon {
   TMGeom<float> g;
   int tiles_x, tiles_y, P;
-  int64_t pitch, pshot;  // floats per pitched row / per pitched shot
+  const int *order;           // grid tile at each position of the tile sequence
+  int64_t pitch, pshot;       // floats per pitched row / per pitched shot
   float *ey_n, *hx_n, *hz_n;  // next copy (pitched)
-  PointCSR p0, p1;            // forward: sources, receivers; adjoint: receivers, sources
-  const float *v0;            // forward: f_t; adjoint: grad_r_t
-  float *v1;                  // forward: r_t; adjoint: grad_f_t
+  PointCSR pa, pb;            // list A (values added) / list B (values recorded):
+                              // forward sources / receivers, adjoint receivers / sources
+  const float *va;            // forward: f_t; adjoint: grad_r_t
+  float *vb;                  // forward: r_t; adjoint: grad_f_t
 };
 
 struct QFwdArgs {
@@ -197,124 +228,230 @@ struct QAdjArgs {
   int bg_shots;                                // shots of the snapshot history
   float *grad_ca, *grad_cb;                    // [ny, nx]
   float kscale;
-  float *hand;  // [P][2][TY * 64] running sums handed from CTA c-1 to c
+  float *hand;  // [P][2][32 * 64] running sums handed from CTA c-1 to c
   int *flags;   // [P]
   int epoch;    // distinct per launch within a call (flags start at 0)
 };
 
-// Issue the TMA loads of unit (tile, shot) into stage k (thread 0 only).
-template <int TY, bool ADJ>
-__device__ __forceinline__ void q_issue(const QSmem<TY, ADJ> &sm, const QMaps &m, int k, int tile,
-                                        int shot, bool coef, int cslot, int tiles_x) {
-  using B = QBox<TY>;
-  const int y0 = (tile / tiles_x) * TY, x0 = (tile % tiles_x) * kQX;
-  uint64_t *bar = sm.full + k;
-  fence_proxy_async_smem();
-  mbar_arrive_expect_tx(bar, B::FIELD_TX + (coef ? (ADJ ? B::COEF_ADJ_TX : B::COEF_FWD_TX) : 0u));
-  tma_load_3d(sm.e(k), &m.e, bar, x0 - 4, y0 - 1, shot);
-  tma_load_3d(sm.x(k), &m.x, bar, x0, y0 - 1, shot);
-  tma_load_3d(sm.z(k), &m.z, bar, x0 - 4, y0, shot);
-  if (coef) {
-    if (ADJ) {
-      tma_load_3d(sm.c0(cslot), &m.c0, bar, x0, y0, 0);
-      tma_load_3d(sm.c1(cslot), &m.c1, bar, x0 - 4, y0 - 1, 0);
-      tma_load_3d(sm.c2(cslot), &m.c2, bar, x0 - 4, y0 - 1, 0);
-    } else {
-      tma_load_3d(sm.c0(cslot), &m.c0, bar, x0 - 4, y0 - 1, 0);
-      tma_load_3d(sm.c1(cslot), &m.c1, bar, x0, y0, 0);
-      tma_load_3d(sm.c2(cslot), &m.c2, bar, x0, y0, 0);
-    }
-  }
+// Compute-warp barrier (the producer warp does not take part).
+__device__ __forceinline__ void q_csync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kQCompute) : "memory");
 }
 
-// Does (tile, shot) have point entries in either list?
-__device__ __forceinline__ bool q_pts(const PointCSR &a, const PointCSR &b, int id) {
-  return !point_tile_empty(a, b, id);
-}
-
-// Point passes over the own cells of a tile (values v, RPT rows x 2 columns
-// per thread).  The tile's list is staged in shared memory in chunks (cell
-// as a tile-local index, and the entry's value or index); every thread then
-// scans the chunk for entries at its own cells, so entries at one cell are
-// applied in entry order and the lists are read with parallel loads.
-constexpr int kQPtChunk = 512;
-__device__ __forceinline__ int q_local(int cell, int ybase, int nx, int ty) {
+// Tile-local index (oy * 64 + ox) of a flat cell, or -1 outside the tile.
+__device__ __forceinline__ int q_local(int cell, int ybase, int nx) {
   const int d = cell - ybase;
   if (d < 0) return -1;
   const int oy = d / nx, ox = d - oy * nx;
-  return (oy < ty && ox < kQX) ? oy * kQX + ox : -1;
+  return (oy < kQTY_ && ox < kQX) ? oy * kQX + ox : -1;
 }
-// v[c] = v[c] + vals[e] for each entry e at cell c, in entry order.
-template <int TY, int RPT>
-__device__ __forceinline__ void q_points_add(const PointCSR &pl, const float *vals, int pid,
-                                             int ybase, int nx, float (&v)[RPT][2], int *s_cell,
-                                             float *s_val) {
-  if (pl.start == nullptr || vals == nullptr) return;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int b = __ldg(pl.start + pid), e = __ldg(pl.start + pid + 1);
-  for (int c0 = b; c0 < e; c0 += kQPtChunk) {
-    const int n = min(kQPtChunk, e - c0);
-    __syncthreads();
-    for (int i = tid; i < n; i += kQThreads) {
-      s_cell[i] = q_local(__ldg(pl.cell + c0 + i), ybase, nx, TY);
-      s_val[i] = __ldg(vals + __ldg(pl.ent + c0 + i));
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < RPT; ++r)
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int me = (warp + r * kQWarps) * kQX + 2 * lane + q;
-        for (int i = 0; i < n; ++i)
-          if (s_cell[i] == me) v[r][q] = v[r][q] + s_val[i];
+
+// ------------------------------------------------------------ producer
+
+// Stage one point list of unit pid into dst: count (or -1 when it holds
+// more than kQPtCap entries), then (local index, value / entry) pairs in
+// entry order.  Executed by the 32 lanes of the producer warp.
+__device__ __forceinline__ void q_stage_list(const PointCSR &pl, const float *vals, bool by_value,
+                                             int pid, int ybase, int nx, int *cnt, int *dst) {
+  const int lane = threadIdx.x & 31;
+  int n = 0;
+  if (pl.start != nullptr && vals != nullptr) {
+    const int b = __ldg(pl.start + pid), e = __ldg(pl.start + pid + 1);
+    n = e - b;
+    if (n > kQPtCap) {
+      n = -1;
+    } else {
+      for (int i = lane; i < n; i += 32) {
+        const int ent = __ldg(pl.ent + b + i);
+        dst[2 * i] = q_local(__ldg(pl.cell + b + i), ybase, nx);
+        dst[2 * i + 1] = by_value ? __float_as_int(__ldg(vals + ent)) : ent;
       }
+    }
+  }
+  if (lane == 0) *cnt = n;
+}
+
+// Profiles of a new tile: x profiles at columns x0-1 .. x0+64 and y profiles
+// at rows y0-1 .. y0+32 (zero, kappa one, outside the grid).
+__device__ __forceinline__ void q_stage_profiles(const TMGeom<float> &g, int y0, int x0,
+                                                 float *pr) {
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < 6 * kQPW; i += 32) {
+    const int a = i / kQPW, c = i - a * kQPW, x = x0 - 1 + c;
+    const float *p = a == 0 ? g.bx : a == 1 ? g.ax : a == 2 ? g.kx
+                   : a == 3 ? g.bxh : a == 4 ? g.axh : g.kxh;
+    pr[i] = (x >= 0 && x < g.nx) ? __ldg(p + x) : ((a == 2 || a == 5) ? 1.f : 0.f);
+  }
+  for (int i = lane; i < 6 * kQPH; i += 32) {
+    const int a = i / kQPH, r = i - a * kQPH, y = y0 - 1 + r;
+    const float *p = a == 0 ? g.by : a == 1 ? g.ay : a == 2 ? g.ky
+                   : a == 3 ? g.byh : a == 4 ? g.ayh : g.kyh;
+    pr[6 * kQPW + i] = (y >= 0 && y < g.ny) ? __ldg(p + y) : ((a == 2 || a == 5) ? 1.f : 0.f);
   }
 }
-// out[e] = v[c] for each entry e at cell c.
-template <int TY, int RPT>
-__device__ __forceinline__ void q_points_record(const PointCSR &pl, float *out, int pid,
-                                                int ybase, int nx, const float (&v)[RPT][2],
-                                                int *s_cell, int *s_ent) {
-  if (pl.start == nullptr || out == nullptr) return;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int b = __ldg(pl.start + pid), e = __ldg(pl.start + pid + 1);
-  for (int c0 = b; c0 < e; c0 += kQPtChunk) {
-    const int n = min(kQPtChunk, e - c0);
-    __syncthreads();
-    for (int i = tid; i < n; i += kQThreads) {
-      s_cell[i] = q_local(__ldg(pl.cell + c0 + i), ybase, nx, TY);
-      s_ent[i] = __ldg(pl.ent + c0 + i);
+
+// The producer warp: for every unit of the CTA (kQStages ahead of the
+// compute warps) wait for the stage to be empty, stage point lists and, on a
+// new tile, profiles, then lane 0 issues the TMA loads on the full barrier.
+template <bool ADJ>
+__device__ __forceinline__ void q_producer(const QSmem<ADJ> &sm, const QMaps &m,
+                                           const QCommon &cm, const QSched &sc) {
+  using B = QBox;
+  const int lane = threadIdx.x & 31;
+  const TMGeom<float> &g = cm.g;
+  const int n_units = sc.n();
+  int prev_ord = -1;
+  for (int j = 0; j < n_units; ++j) {
+    const int k = j % kQStages;
+    if (j >= kQStages &&
+        !mbar_wait(sm.empty + k, (uint32_t)((j / kQStages - 1) & 1), kQWaitLimit) &&
+        lane == 0)
+      atomicOr(&g_tide_dev_err, 16);
+    int stile, shot, ord, seg;
+    sc.unit(j, stile, shot, ord, seg);
+    const int tile = __ldg(cm.order + stile);
+    const int ty = tile / cm.tiles_x, tx = tile - ty * cm.tiles_x;
+    const int y0 = ty * B::TY, x0 = tx * kQX;
+    const bool new_tile = ord != prev_ord;
+    prev_ord = ord;
+    const int cs = ord % kQStages;
+    // point lists of (tile, shot)
+    const int pid = (shot * cm.tiles_y + ty) * cm.tiles_x + tx;
+    int *pt = sm.pt(k);
+    q_stage_list(cm.pa, cm.va, true, pid, y0 * g.nx + x0, g.nx, pt, pt + 2);
+    q_stage_list(cm.pb, cm.vb, false, pid, y0 * g.nx + x0, g.nx, pt + 1, pt + 2 + 2 * kQPtCap);
+    if (new_tile) q_stage_profiles(g, y0, x0, sm.pr(cs));
+    __syncwarp();
+    if (lane == 0) {
+      uint64_t *bar = sm.full + k;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(
+          bar, B::FIELD_TX + (new_tile ? (ADJ ? B::COEF_ADJ_TX : B::COEF_FWD_TX) : 0u));
+      tma_load_3d(sm.e(k), &m.e, bar, x0 - 4, y0 - 1, shot);
+      tma_load_3d(sm.x(k), &m.x, bar, x0, y0 - 1, shot);
+      tma_load_3d(sm.z(k), &m.z, bar, x0 - 4, y0, shot);
+      if (new_tile) {
+        if (ADJ) {
+          tma_load_3d(sm.c0(cs), &m.c0, bar, x0, y0, 0);
+          tma_load_3d(sm.c1(cs), &m.c1, bar, x0 - 4, y0 - 1, 0);
+          tma_load_3d(sm.c2(cs), &m.c2, bar, x0 - 4, y0 - 1, 0);
+        } else {
+          tma_load_3d(sm.c0(cs), &m.c0, bar, x0 - 4, y0 - 1, 0);
+          tma_load_3d(sm.c1(cs), &m.c1, bar, x0, y0, 0);
+          tma_load_3d(sm.c2(cs), &m.c2, bar, x0, y0, 0);
+        }
+      }
     }
-    __syncthreads();
+  }
+}
+
+// Barrier set-up and tensor-map prefetch (thread 0), then a block barrier.
+template <bool ADJ>
+__device__ __forceinline__ void q_setup(const QSmem<ADJ> &sm, const QMaps &m) {
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kQStages; ++k) {
+      mbar_init(sm.full + k, 1);
+      mbar_init(sm.empty + k, kQCWarps);
+    }
+    mbar_init_fence();
+    tma_prefetch_map(&m.e);
+    tma_prefetch_map(&m.x);
+    tma_prefetch_map(&m.z);
+    tma_prefetch_map(&m.c0);
+    tma_prefetch_map(&m.c1);
+    tma_prefetch_map(&m.c2);
+  }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------ compute helpers
+
+// Profile lookups in a tile's staged profiles.
+struct QProf {
+  const float *p;
+  int x0, y0;
+  // a: 0 b, 1 a, 2 kappa (integer grid), 3 bh, 4 ah, 5 kappah (half grid)
+  __device__ __forceinline__ float x(int a, int xx) const { return p[a * kQPW + xx - x0 + 1]; }
+  __device__ __forceinline__ float y(int a, int yy) const {
+    return p[6 * kQPW + a * kQPH + yy - y0 + 1];
+  }
+};
+
+// Point passes over the own cells (values v[r][q] at rows 2w + r, columns
+// l + 32 q) from the staged lists; a list that did not fit the stage is read
+// from global memory instead.  Entries at one cell are applied in entry order.
+__device__ __forceinline__ void q_points(const int *pt, const QCommon &cm, int pid, int ybase,
+                                         float (&v)[2][2]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int na = pt[0], nb = pt[1];
+  const int *la = pt + 2, *lb = pt + 2 + 2 * kQPtCap;
+  if (na != 0) {
+    int b = 0, e = 0;
+    if (na < 0) {
+      b = __ldg(cm.pa.start + pid);
+      e = __ldg(cm.pa.start + pid + 1);
+    }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r)
+    for (int r = 0; r < 2; ++r)
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int me = (warp + r * kQWarps) * kQX + 2 * lane + q;
-        for (int i = 0; i < n; ++i)
-          if (s_cell[i] == me) out[s_ent[i]] = v[r][q];
+        const int me = (2 * warp + r) * kQX + lane + 32 * q;
+        if (na > 0) {
+          for (int i = 0; i < na; ++i)
+            if (la[2 * i] == me) v[r][q] = v[r][q] + __int_as_float(la[2 * i + 1]);
+        } else {
+          for (int i = b; i < e; ++i)
+            if (q_local(__ldg(cm.pa.cell + i), ybase, cm.g.nx) == me)
+              v[r][q] = v[r][q] + __ldg(cm.va + __ldg(cm.pa.ent + i));
+        }
+      }
+  }
+  if (nb != 0) {
+    int b = 0, e = 0;
+    if (nb < 0) {
+      b = __ldg(cm.pb.start + pid);
+      e = __ldg(cm.pb.start + pid + 1);
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int me = (2 * warp + r) * kQX + lane + 32 * q;
+        if (nb > 0) {
+          for (int i = 0; i < nb; ++i)
+            if (lb[2 * i] == me) cm.vb[lb[2 * i + 1]] = v[r][q];
+        } else {
+          for (int i = b; i < e; ++i)
+            if (q_local(__ldg(cm.pb.cell + i), ybase, cm.g.nx) == me)
+              cm.vb[__ldg(cm.pb.ent + i)] = v[r][q];
+        }
       }
   }
 }
 
-// ============================================================== adjoint
-//
-// Per unit: phase 1 = adjoint E-phase (cb lEy -> lHx, lHz and the x / y
-// memories of the E-phase) on the own cells plus the halo row y0-1 (lHx) and
-// column x0-1 (lHz), into shared memory; phase 2 = adjoint H-phase (lEy from
-// the new lHx / lHz, the H-phase memories), receivers injected, sources
-// recorded, image terms summed over the tile's shots.  Formulas: tm2d_s2.cuh
-// adj_e_tile / adj_h_tile.
-// CPML memory values one cell reads (prefetched before its arithmetic, so a
+// CPML memory values one cell reads (loaded before its arithmetic, so a
 // strip tile waits for memory once per phase, not once per cell).
 struct QM4 {
   float a, b, c, d;
 };
 
-template <int TY>
+// Interior tile: no cell it updates or recomputes is in a CPML strip or on
+// the grid edge.
+__device__ __forceinline__ bool q_interior(const TMGeom<float> &g, int y0, int x0) {
+  return y0 - 1 >= max(1, g.pml_y0) && y0 + kQTY_ < min(g.ny, g.pml_y1) &&
+         x0 - 1 >= max(1, g.pml_x0) && x0 + kQX < min(g.nx, g.pml_x1);
+}
+
+// ============================================================== adjoint
+//
+// Per unit: phase 1 = adjoint E-phase (cb lEy -> lHx, lHz and the E-phase
+// memories) on the own cells plus the halo row y0-1 (lHx) and column x0-1
+// (lHz), into shared memory; phase 2 = adjoint H-phase (lEy from the new
+// lHx / lHz, the H-phase memories), receivers injected, sources recorded,
+// image terms summed over the tile's shots.  Formulas: tm2d_s2.cuh
+// adj_e_tile / adj_h_tile.
 struct QAdjCell {
-  using B = QBox<TY>;
-  // Strip tests of the E-phase (integer grid) and H-phase (half grid).
+  using B = QBox;
   static __device__ __forceinline__ bool xs(const TMGeom<float> &g, int x) {
     return !(x >= g.pml_x0 && x < g.pml_x1);
   }
@@ -342,10 +479,11 @@ struct QAdjCell {
   // phase 1 at cell (y, x): new lHx and lHz; own cells also write the next
   // E-phase memories.
   template <bool IN>
-  static __device__ __forceinline__ void e_phase(const QAdjArgs &a, const float *E,
-                                                 const float *CB, float lhx, float lhz, int y,
-                                                 int x, int y0, int x0, int64_t sb, bool own,
-                                                 const QM4 &m, float &hx_new, float &hz_new) {
+  static __device__ __forceinline__ void e_phase(const QAdjArgs &a, const QProf &pf,
+                                                 const float *E, const float *CB, float lhx,
+                                                 float lhz, int y, int x, int y0, int x0,
+                                                 int64_t sb, bool own, const QM4 &m,
+                                                 float &hx_new, float &hz_new) {
     const TMGeom<float> &g = a.c.g;
     const int ly = y - y0 + 1, lx = x - x0 + 4;  // E-box coordinates
     const float q = CB[ly * B::EW + lx] * E[ly * B::EW + lx];
@@ -364,8 +502,8 @@ struct QAdjCell {
     if (!xs(g, x)) {
       rx = q;
     } else {
-      const float mn = __ldg(g.bx + x) * m.a + q;
-      rx = __ldg(g.ax + x) * mn + q / __ldg(g.kx + x);
+      const float mn = pf.x(0, x) * m.a + q;
+      rx = pf.x(1, x) * mn + q / pf.x(2, x);
       if (own) a.mhz_n[j] = mn;
     }
     if (x + 1 >= g.nx) {
@@ -373,14 +511,14 @@ struct QAdjCell {
     } else if (!xs(g, x + 1)) {
       rxr = qr;
     } else {
-      const float mn = __ldg(g.bx + x + 1) * m.b + qr;
-      rxr = __ldg(g.ax + x + 1) * mn + qr / __ldg(g.kx + x + 1);
+      const float mn = pf.x(0, x + 1) * m.b + qr;
+      rxr = pf.x(1, x + 1) * mn + qr / pf.x(2, x + 1);
     }
     if (!ys(g, y)) {
       ry0 = -q;
     } else {
-      const float mn = __ldg(g.by + y) * m.c - q;
-      ry0 = __ldg(g.ay + y) * mn - q / __ldg(g.ky + y);
+      const float mn = pf.y(0, y) * m.c - q;
+      ry0 = pf.y(1, y) * mn - q / pf.y(2, y);
       if (own) a.mhx_n[j] = mn;
     }
     if (y + 1 >= g.ny) {
@@ -388,8 +526,8 @@ struct QAdjCell {
     } else if (!ys(g, y + 1)) {
       ry1 = -q1;
     } else {
-      const float mn = __ldg(g.by + y + 1) * m.d - q1;
-      ry1 = __ldg(g.ay + y + 1) * mn - q1 / __ldg(g.ky + y + 1);
+      const float mn = pf.y(0, y + 1) * m.d - q1;
+      ry1 = pf.y(1, y + 1) * mn - q1 / pf.y(2, y + 1);
     }
     hz_new = lhz + ((float)1 * (rx - rxr)) * g.rdx;
     hx_new = lhx + ((float)1 * (ry0 - ry1)) * g.rdy;
@@ -409,21 +547,22 @@ struct QAdjCell {
   }
   // phase 2 at own cell (y, x): the new lEy before points.
   template <bool IN>
-  static __device__ __forceinline__ float h_phase(const QAdjArgs &a, const float *E,
-                                                  const float *CA, const float *CQ,
-                                                  const float *HXN, const float *HZN, int y, int x,
-                                                  int y0, int x0, int64_t sb, const QM4 &m) {
+  static __device__ __forceinline__ float h_phase(const QAdjArgs &a, const QProf &pf,
+                                                  const float *E, const float *CA,
+                                                  const float *CQ, const float *HXN,
+                                                  const float *HZN, int y, int x, int y0, int x0,
+                                                  int64_t sb, const QM4 &m) {
     const TMGeom<float> &g = a.c.g;
     const int oy = y - y0, ox = x - x0;
     const float lam = E[(oy + 1) * B::EW + ox + 4];
     const float ca = CA[oy * B::OW + ox];
     const float cz0 = CQ[oy * B::QW + ox + 4], cz1 = CQ[(oy + 1) * B::QW + ox + 4];
-    const float cx = CQ[(oy + 1) * B::QW + ox + 4], cl = CQ[(oy + 1) * B::QW + ox + 3];
+    const float cl = CQ[(oy + 1) * B::QW + ox + 3];
     const float h0 = HXN[oy * B::XW + ox], h1 = HXN[(oy + 1) * B::XW + ox];
     const float zx = HZN[oy * B::ZW + ox + 4], zl = HZN[oy * B::ZW + ox + 3];
     if (IN) {
       const float rz0 = -cz0 * h0, rz1 = -cz1 * h1;
-      const float rx = cx * zx, rxl = cl * zl;
+      const float rx = cz1 * zx, rxl = cl * zl;
       float v = ca * lam;
       v = v + (((float)1 * (rz0 - rz1)) * g.rdy + ((float)1 * (rxl - rx)) * g.rdx);
       return v;
@@ -438,8 +577,8 @@ struct QAdjCell {
         if (!ysh(g, yy)) {
           rz0 = adj;
         } else {
-          const float mn = __ldg(g.byh + yy) * m.a + adj;
-          rz0 = __ldg(g.ayh + yy) * mn + adj / __ldg(g.kyh + yy);
+          const float mn = pf.y(3, yy) * m.a + adj;
+          rz0 = pf.y(4, yy) * mn + adj / pf.y(5, yy);
         }
       }
     }
@@ -448,18 +587,18 @@ struct QAdjCell {
       if (!ysh(g, y)) {
         rz1 = adj;
       } else {
-        const float mn = __ldg(g.byh + y) * m.b + adj;
-        rz1 = __ldg(g.ayh + y) * mn + adj / __ldg(g.kyh + y);
+        const float mn = pf.y(3, y) * m.b + adj;
+        rz1 = pf.y(4, y) * mn + adj / pf.y(5, y);
         a.mez_n[j] = mn;
       }
     }
     if (x < g.nx - 1) {  // column x (x >= 1 here)
-      const float adj = cx * zx;
+      const float adj = cz1 * zx;
       if (!xsh(g, x)) {
         rx = adj;
       } else {
-        const float mn = __ldg(g.bxh + x) * m.c + adj;
-        rx = __ldg(g.axh + x) * mn + adj / __ldg(g.kxh + x);
+        const float mn = pf.x(3, x) * m.c + adj;
+        rx = pf.x(4, x) * mn + adj / pf.x(5, x);
         a.mex_n[j] = mn;
       }
     }
@@ -470,8 +609,8 @@ struct QAdjCell {
         if (!xsh(g, xl)) {
           rxl = adj;
         } else {
-          const float mn = __ldg(g.bxh + xl) * m.d + adj;
-          rxl = __ldg(g.axh + xl) * mn + adj / __ldg(g.kxh + xl);
+          const float mn = pf.x(3, xl) * m.d + adj;
+          rxl = pf.x(4, xl) * mn + adj / pf.x(5, xl);
         }
       }
     }
@@ -483,20 +622,22 @@ struct QAdjCell {
 
 template <typename SN> __device__ __forceinline__ float q_dec(SN v) { return Codec<SN, float>::dec(v); }
 
-// Snapshots of the own cells of unit (tile, shot): shot s images against
-// snapshot shot s % bg_shots; cells outside the update domain read nothing.
-template <int TY, int RPT, typename SN>
+// Snapshots of the own cells of unit (grid tile, shot): shot s images
+// against snapshot shot s % bg_shots; cells outside the update domain read
+// nothing.
+template <typename SN>
 __device__ __forceinline__ void q_snap_load(const QAdjArgs &a, int tile, int shot,
-                                            SN (&ev)[RPT][2], SN (&cv)[RPT][2]) {
+                                            SN (&ev)[2][2], SN (&cv)[2][2]) {
   const TMGeom<float> &g = a.c.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int y0 = (tile / a.c.tiles_x) * TY, x0 = (tile % a.c.tiles_x) * kQX;
+  const int ty = tile / a.c.tiles_x;
+  const int y0 = ty * kQTY_, x0 = (tile - ty * a.c.tiles_x) * kQX;
   const int64_t snb = (int64_t)(shot % a.bg_shots) * g.N;
 #pragma unroll
-  for (int r = 0; r < RPT; ++r)
+  for (int r = 0; r < 2; ++r)
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      const int y = y0 + warp + r * kQWarps, x = x0 + 2 * lane + q;
+      const int y = y0 + 2 * warp + r, x = x0 + lane + 32 * q;
       const bool ok = y >= 1 && x >= 1 && y < g.ny && x < g.nx;
       const int64_t j = snb + (int64_t)y * g.nx + x;
       ev[r][q] = (ok && a.ey_st) ? load_stream(static_cast<const SN *>(a.ey_st) + j) : SN(0.f);
@@ -504,14 +645,13 @@ __device__ __forceinline__ void q_snap_load(const QAdjArgs &a, int tile, int sho
     }
 }
 
-template <int TY, typename SN>
+template <typename SN>
 __global__ void __launch_bounds__(kQThreads, 1)
 kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
-  using B = QBox<TY>;
-  using C = QAdjCell<TY>;
-  constexpr int RPT = TY / kQWarps;  // own rows per thread (x 2 columns)
+  using B = QBox;
+  using C = QAdjCell;
   extern __shared__ __align__(128) unsigned char q_smem[];
-  const QSmem<TY, true> sm(q_smem);
+  const QSmem<true> sm(q_smem);
   const QCommon &cm = a.c;
   const TMGeom<float> &g = cm.g;
   const int S = g.n_shots, nx = g.nx, ny = g.ny;
@@ -521,36 +661,30 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
   const int n_units = sc.n();
   const bool imaging = a.ey_st != nullptr || a.cu_st != nullptr;
 
-  if (tid == 0) {
-    for (int k = 0; k < kQStages; ++k) mbar_init(sm.full + k, 1);
-    mbar_init_fence();
+  q_setup<true>(sm, m);
+  if (warp == kQCWarps) {
+    q_producer<true>(sm, m, cm, sc);
+    return;
   }
-  __syncthreads();
-  // prologue: the first kQStages units
-  if (tid == 0) {
-    int prev_ord = -1;
-    for (int i = 0; i < n_units && i < kQStages; ++i) {
-      int tile, shot, ord, seg;
-      sc.unit(i, tile, shot, ord, seg);
-      q_issue<TY, true>(sm, m, i, tile, shot, ord != prev_ord, ord % kQStages, cm.tiles_x);
-      prev_ord = ord;
-    }
-  }
-  float sum_a[RPT][2], sum_b[RPT][2];
+
+  float sum_a[2][2], sum_b[2][2];
   // snapshots are loaded one unit ahead (their latency overlaps a whole unit)
-  SN ev[RPT][2], cv[RPT][2];
+  SN ev[2][2], cv[2][2];
   if (imaging && n_units > 0) {
     int t0, s0, o0, g0;
     sc.unit(0, t0, s0, o0, g0);
-    q_snap_load<TY, RPT, SN>(a, t0, s0, ev, cv);
+    q_snap_load<SN>(a, __ldg(cm.order + t0), s0, ev, cv);
   }
+  const QM4 z4{0.f, 0.f, 0.f, 0.f};
   int prev_ord = -1;
   for (int i = 0; i < n_units; ++i) {
-    int tile, shot, ord, seg;
-    sc.unit(i, tile, shot, ord, seg);
+    int stile, shot, ord, seg;
+    sc.unit(i, stile, shot, ord, seg);
+    const int tile = __ldg(cm.order + stile);
     const int k = i % kQStages;
     const int cs = ord % kQStages;
-    const int y0 = (tile / cm.tiles_x) * TY, x0 = (tile % cm.tiles_x) * kQX;
+    const int ty = tile / cm.tiles_x, tx = tile - ty * cm.tiles_x;
+    const int y0 = ty * B::TY, x0 = tx * kQX;
     const int64_t sb = (int64_t)shot * g.N;  // shot base, caller layout
     const int64_t pb = (int64_t)shot * cm.pshot;
     const bool first_of_tile = ord != prev_ord;
@@ -569,26 +703,26 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
             __nanosleep(64);
           }
         }
-        __syncthreads();
-        const float *h = a.hand + (size_t)(cta - 1) * 2 * TY * kQX;
+        q_csync();
+        const float *h = a.hand + (size_t)(cta - 1) * 2 * B::TY * kQX;
 #pragma unroll
-        for (int r = 0; r < RPT; ++r)
+        for (int r = 0; r < 2; ++r)
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
-            const int o = (warp + r * kQWarps) * kQX + 2 * lane + q;
+            const int o = (2 * warp + r) * kQX + lane + 32 * q;
             sum_a[r][q] = __ldcg(h + o);
-            sum_b[r][q] = __ldcg(h + TY * kQX + o);
+            sum_b[r][q] = __ldcg(h + B::TY * kQX + o);
           }
       } else {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) sum_a[r][0] = sum_a[r][1] = sum_b[r][0] = sum_b[r][1] = 0.f;
+        for (int r = 0; r < 2; ++r) sum_a[r][0] = sum_a[r][1] = sum_b[r][0] = sum_b[r][1] = 0.f;
       }
     }
-    SN evn[RPT][2], cvn[RPT][2];
+    SN evn[2][2], cvn[2][2];
     if (imaging && i + 1 < n_units) {
       int t1, s1, o1, g1;
       sc.unit(i + 1, t1, s1, o1, g1);
-      q_snap_load<TY, RPT, SN>(a, t1, s1, evn, cvn);
+      q_snap_load<SN>(a, __ldg(cm.order + t1), s1, evn, cvn);
     }
     // A transfer that never lands ends the wait with the error word set; the
     // CTA still runs every barrier so the launch finishes.
@@ -596,38 +730,36 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
       atomicOr(&g_tide_dev_err, 8);
     const float *E = sm.e(k), *LX = sm.x(k), *LZ = sm.z(k);
     const float *CA = sm.c0(cs), *CB = sm.c1(cs), *CQ = sm.c2(cs);
-    const bool in = y0 - 1 >= max(1, g.pml_y0) && y0 + TY < min(ny, g.pml_y1) &&
-                    x0 - 1 >= max(1, g.pml_x0) && x0 + kQX < min(nx, g.pml_x1);
+    const QProf pf{sm.pr(cs), x0, y0};
+    const bool in = q_interior(g, y0, x0);
     // ---------------- phase 1: adjoint E-phase
     // (strip tiles: every memory value the thread's cells read is loaded first)
-    QM4 mm[RPT][2], mh[2];
-    const QM4 z4{0.f, 0.f, 0.f, 0.f};
+    QM4 mm[2][2], mh[2];
     if (!in) {
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          mm[r][q] = C::e_loads(a, y0 + warp + r * kQWarps, x0 + 2 * lane + q, sb);
+          mm[r][q] = C::e_loads(a, y0 + 2 * warp + r, x0 + lane + 32 * q, sb);
       if (warp == 0) {
-        mh[0] = C::e_loads(a, y0 - 1, x0 + 2 * lane, sb);
-        mh[1] = C::e_loads(a, y0 - 1, x0 + 2 * lane + 1, sb);
-      } else if (warp == 1 && lane < TY) {
+        mh[0] = C::e_loads(a, y0 - 1, x0 + lane, sb);
+        mh[1] = C::e_loads(a, y0 - 1, x0 + lane + 32, sb);
+      } else if (warp == 1) {
         mh[0] = C::e_loads(a, y0 + lane, x0 - 1, sb);
       }
     }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int oy = warp + r * kQWarps, y = y0 + oy;
+    for (int r = 0; r < 2; ++r) {
+      const int oy = 2 * warp + r, y = y0 + oy;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int ox = 2 * lane + q, x = x0 + ox;
+        const int ox = lane + 32 * q, x = x0 + ox;
         const float lhx = LX[(oy + 1) * B::XW + ox], lhz = LZ[oy * B::ZW + ox + 4];
         float hxn, hzn;
         if (in)
-          C::template e_phase<true>(a, E, CB, lhx, lhz, y, x, y0, x0, sb, true, z4, hxn, hzn);
+          C::e_phase<true>(a, pf, E, CB, lhx, lhz, y, x, y0, x0, sb, true, z4, hxn, hzn);
         else
-          C::template e_phase<false>(a, E, CB, lhx, lhz, y, x, y0, x0, sb, true, mm[r][q], hxn,
-                                     hzn);
+          C::e_phase<false>(a, pf, E, CB, lhx, lhz, y, x, y0, x0, sb, true, mm[r][q], hxn, hzn);
         sm.hxn[(oy + 1) * B::XW + ox] = hxn;
         sm.hzn[oy * B::ZW + ox + 4] = hzn;
         if (y < ny && x < nx) {
@@ -640,68 +772,61 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
     if (warp == 0) {  // halo row y0 - 1 (new lHx only)
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int ox = 2 * lane + q, y = y0 - 1, x = x0 + ox;
-        const float lhx = LX[ox];
+        const int ox = lane + 32 * q, y = y0 - 1, x = x0 + ox;
         float hxn, hzn;
         if (in)
-          C::template e_phase<true>(a, E, CB, lhx, 0.f, y, x, y0, x0, sb, false, z4, hxn, hzn);
+          C::e_phase<true>(a, pf, E, CB, LX[ox], 0.f, y, x, y0, x0, sb, false, z4, hxn, hzn);
         else
-          C::template e_phase<false>(a, E, CB, lhx, 0.f, y, x, y0, x0, sb, false, mh[q], hxn,
-                                     hzn);
+          C::e_phase<false>(a, pf, E, CB, LX[ox], 0.f, y, x, y0, x0, sb, false, mh[q], hxn,
+                            hzn);
         sm.hxn[ox] = hxn;
       }
-    } else if (warp == 1 && lane < TY) {  // halo column x0 - 1 (new lHz only)
+    } else if (warp == 1) {  // halo column x0 - 1 (new lHz only)
       const int oy = lane, y = y0 + oy, x = x0 - 1;
       const float lhz = LZ[oy * B::ZW + 3];
       float hxn, hzn;
       if (in)
-        C::template e_phase<true>(a, E, CB, 0.f, lhz, y, x, y0, x0, sb, false, z4, hxn, hzn);
+        C::e_phase<true>(a, pf, E, CB, 0.f, lhz, y, x, y0, x0, sb, false, z4, hxn, hzn);
       else
-        C::template e_phase<false>(a, E, CB, 0.f, lhz, y, x, y0, x0, sb, false, mh[0], hxn, hzn);
+        C::e_phase<false>(a, pf, E, CB, 0.f, lhz, y, x, y0, x0, sb, false, mh[0], hxn, hzn);
       sm.hzn[oy * B::ZW + 3] = hzn;
     }
-    __syncthreads();
+    q_csync();
     // ---------------- phase 2: adjoint H-phase
-    const int pid = (shot * cm.tiles_y + tile / cm.tiles_x) * cm.tiles_x + tile % cm.tiles_x;
-    const bool pts = q_pts(cm.p0, cm.p1, pid);
-    float v[RPT][2];
+    float v[2][2];
     if (in) {
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          v[r][q] = C::template h_phase<true>(a, E, CA, CQ, sm.hxn, sm.hzn, y0 + warp + r * kQWarps,
-                                              x0 + 2 * lane + q, y0, x0, sb, z4);
+          v[r][q] = C::h_phase<true>(a, pf, E, CA, CQ, sm.hxn, sm.hzn, y0 + 2 * warp + r,
+                                     x0 + lane + 32 * q, y0, x0, sb, z4);
     } else {
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          mm[r][q] = C::h_loads(a, y0 + warp + r * kQWarps, x0 + 2 * lane + q, sb);
+          mm[r][q] = C::h_loads(a, y0 + 2 * warp + r, x0 + lane + 32 * q, sb);
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          v[r][q] = C::template h_phase<false>(a, E, CA, CQ, sm.hxn, sm.hzn,
-                                               y0 + warp + r * kQWarps, x0 + 2 * lane + q, y0,
-                                               x0, sb, mm[r][q]);
+          v[r][q] = C::h_phase<false>(a, pf, E, CA, CQ, sm.hxn, sm.hzn, y0 + 2 * warp + r,
+                                      x0 + lane + 32 * q, y0, x0, sb, mm[r][q]);
     }
-    if (pts) {
-      // receivers (lEy += grad_r, entry order), then sources (grad_f = lEy)
-      int *s_cell = reinterpret_cast<int *>(sm.ve);
-      float *s_val = sm.ve + kQPtChunk;
-      const int ybase = y0 * nx + x0;
-      q_points_add<TY, RPT>(cm.p0, cm.v0, pid, ybase, nx, v, s_cell, s_val);
-      q_points_record<TY, RPT>(cm.p1, cm.v1, pid, ybase, nx, v, s_cell,
-                               reinterpret_cast<int *>(s_val));
-    }
+    // receivers (lEy += grad_r, entry order), then sources (grad_f = lEy)
+    const int pid = (shot * cm.tiles_y + ty) * cm.tiles_x + tx;
+    q_points(sm.pt(k), cm, pid, y0 * nx + x0, v);
+    // the stage (fields, point lists) is no longer read by this warp
+    __syncwarp();
+    if (lane == 0) mbar_arrive(sm.empty + k);
     // store lEy, image terms
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int y = y0 + warp + r * kQWarps;
+    for (int r = 0; r < 2; ++r) {
+      const int y = y0 + 2 * warp + r;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int x = x0 + 2 * lane + q;
+        const int x = x0 + lane + 32 * q;
         if (y < ny && x < nx) {
           cm.ey_n[pb + (int64_t)y * cm.pitch + x] = v[r][q];
           if (imaging && y >= 1 && x >= 1) {
@@ -715,25 +840,25 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
     const bool last_of_tile = (seg == 0) ? (shot == sc.nA - 1) : (shot == S - 1);
     if (imaging && last_of_tile) {
       if (seg == 0) {
-        float *h = a.hand + (size_t)cta * 2 * TY * kQX;
+        float *h = a.hand + (size_t)cta * 2 * B::TY * kQX;
 #pragma unroll
-        for (int r = 0; r < RPT; ++r)
+        for (int r = 0; r < 2; ++r)
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
-            const int o = (warp + r * kQWarps) * kQX + 2 * lane + q;
+            const int o = (2 * warp + r) * kQX + lane + 32 * q;
             __stcg(h + o, sum_a[r][q]);
-            __stcg(h + TY * kQX + o, sum_b[r][q]);
+            __stcg(h + B::TY * kQX + o, sum_b[r][q]);
           }
         __threadfence();
-        __syncthreads();
+        q_csync();
         if (tid == 0) st_release_gpu(a.flags + cta, a.epoch);
       } else {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-          const int y = y0 + warp + r * kQWarps;
+        for (int r = 0; r < 2; ++r) {
+          const int y = y0 + 2 * warp + r;
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
-            const int x = x0 + 2 * lane + q;
+            const int x = x0 + lane + 32 * q;
             if (y >= 1 && x >= 1 && y < ny && x < nx) {
               const int64_t j = (int64_t)y * nx + x;
               if (a.ey_st) a.grad_ca[j] = a.grad_ca[j] + sum_a[r][q];
@@ -744,36 +869,25 @@ kq_adj_step(const __grid_constant__ QMaps m, const QAdjArgs a) {
       }
     }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r)
+    for (int r = 0; r < 2; ++r)
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         ev[r][q] = evn[r][q];
         cv[r][q] = cvn[r][q];
       }
-    __syncthreads();  // stage k and the new-H tiles are free
-    if (tid == 0 && i + kQStages < n_units) {
-      int t2, s2, o2, g2;
-      sc.unit(i + kQStages, t2, s2, o2, g2);
-      int op;
-      {
-        int t1, s1, g1;
-        sc.unit(i + kQStages - 1, t1, s1, op, g1);
-      }
-      q_issue<TY, true>(sm, m, k, t2, s2, o2 != op, o2 % kQStages, cm.tiles_x);
-    }
+    q_csync();  // the new-H tiles are free for the next unit
   }
 }
 
 // ============================================================== forward
 //
-// Per unit: phase 1 = H half step (new Hx on rows y0-1..y0+TY-1, new Hz on
+// Per unit: phase 1 = H half step (new Hx on rows y0-1..y0+31, new Hz on
 // columns x0-1..x0+63; own cells write the next H-phase memories), phase 2 =
 // E half step on the own cells (E-phase memories in place), snapshots of
 // Ey^n and curl H, sources added, receivers recorded.  Formulas:
 // tm2d_s2.cuh fwd_h_tile / fwd_e_tile.
-template <int TY>
 struct QFwdCell {
-  using B = QBox<TY>;
+  using B = QBox;
   // H-phase memories of cell (y, x): m_ey_z (a) and m_ey_x (b) where the cell
   // is in their strips
   static __device__ __forceinline__ QM4 h_loads(const QFwdArgs &a, int y, int x, int64_t sb) {
@@ -796,10 +910,11 @@ struct QFwdCell {
     return m;
   }
   template <bool IN>
-  static __device__ __forceinline__ void h_phase(const QFwdArgs &a, const float *E,
-                                                 const float *CQ, float hx, float hz, int y,
-                                                 int x, int y0, int x0, int64_t sb, bool own,
-                                                 const QM4 &m, float &hx_new, float &hz_new) {
+  static __device__ __forceinline__ void h_phase(const QFwdArgs &a, const QProf &pf,
+                                                 const float *E, const float *CQ, float hx,
+                                                 float hz, int y, int x, int y0, int x0,
+                                                 int64_t sb, bool own, const QM4 &m,
+                                                 float &hx_new, float &hz_new) {
     const TMGeom<float> &g = a.c.g;
     const int ly = y - y0 + 1, lx = x - x0 + 4;
     const float e0 = E[ly * B::EW + lx], e1 = E[(ly + 1) * B::EW + lx], er = E[ly * B::EW + lx + 1];
@@ -816,99 +931,88 @@ struct QFwdCell {
     if (y < g.ny - 1) {
       float d = (e1 - e0) * g.rdy;
       if (y < g.pml_y0 || y >= g.pml_y1h) {
-        const float mm = __ldg(g.byh + y) * m.a + __ldg(g.ayh + y) * d;
+        const float mm = pf.y(3, y) * m.a + pf.y(4, y) * d;
         if (own) a.mez_n[j] = mm;
-        d = d / __ldg(g.kyh + y) + mm;
+        d = d / pf.y(5, y) + mm;
       }
       hx_new = hx - c * d;
     }
     if (x < g.nx - 1) {
       float d = (er - e0) * g.rdx;
       if (x < g.pml_x0 || x >= g.pml_x1h) {
-        const float mm = __ldg(g.bxh + x) * m.b + __ldg(g.axh + x) * d;
+        const float mm = pf.x(3, x) * m.b + pf.x(4, x) * d;
         if (own) a.mex_n[j] = mm;
-        d = d / __ldg(g.kxh + x) + mm;
+        d = d / pf.x(5, x) + mm;
       }
       hz_new = hz + c * d;
     }
   }
 };
 
-template <int TY, typename SN>
+template <typename SN>
 __global__ void __launch_bounds__(kQThreads, 1)
 kq_fwd_step(const __grid_constant__ QMaps m, const QFwdArgs a) {
-  using B = QBox<TY>;
-  using C = QFwdCell<TY>;
-  constexpr int RPT = TY / kQWarps;
+  using B = QBox;
+  using C = QFwdCell;
   extern __shared__ __align__(128) unsigned char q_smem[];
-  const QSmem<TY, false> sm(q_smem);
+  const QSmem<false> sm(q_smem);
   const QCommon &cm = a.c;
   const TMGeom<float> &g = cm.g;
-  const int S = g.n_shots, nx = g.nx, ny = g.ny;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const QSched sc = q_sched(blockIdx.x, cm.P, cm.tiles_x * cm.tiles_y, S);
+  const int nx = g.nx, ny = g.ny;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const QSched sc = q_sched(blockIdx.x, cm.P, cm.tiles_x * cm.tiles_y, g.n_shots);
   const int n_units = sc.n();
 
-  if (tid == 0) {
-    for (int k = 0; k < kQStages; ++k) mbar_init(sm.full + k, 1);
-    mbar_init_fence();
+  q_setup<false>(sm, m);
+  if (warp == kQCWarps) {
+    q_producer<false>(sm, m, cm, sc);
+    return;
   }
-  __syncthreads();
-  if (tid == 0) {
-    int prev_ord = -1;
-    for (int i = 0; i < n_units && i < kQStages; ++i) {
-      int tile, shot, ord, seg;
-      sc.unit(i, tile, shot, ord, seg);
-      q_issue<TY, false>(sm, m, i, tile, shot, ord != prev_ord, ord % kQStages, cm.tiles_x);
-      prev_ord = ord;
-    }
-  }
+  const QM4 z4{0.f, 0.f, 0.f, 0.f};
   for (int i = 0; i < n_units; ++i) {
-    int tile, shot, ord, seg;
-    sc.unit(i, tile, shot, ord, seg);
+    int stile, shot, ord, seg;
+    sc.unit(i, stile, shot, ord, seg);
+    const int tile = __ldg(cm.order + stile);
     const int k = i % kQStages;
     const int cs = ord % kQStages;
-    const int y0 = (tile / cm.tiles_x) * TY, x0 = (tile % cm.tiles_x) * kQX;
+    const int ty = tile / cm.tiles_x, tx = tile - ty * cm.tiles_x;
+    const int y0 = ty * B::TY, x0 = tx * kQX;
     const int64_t sb = (int64_t)shot * g.N;
     const int64_t pb = (int64_t)shot * cm.pshot;
-    // A transfer that never lands ends the wait with the error word set; the
-    // CTA still runs every barrier so the launch finishes.
     if (!mbar_wait(sm.full + k, (uint32_t)((i / kQStages) & 1), kQWaitLimit))
       atomicOr(&g_tide_dev_err, 8);
     const float *E = sm.e(k), *HX = sm.x(k), *HZ = sm.z(k);
     const float *CQ = sm.c0(cs), *CA = sm.c1(cs), *CB = sm.c2(cs);
-    const bool in = y0 - 1 >= max(1, g.pml_y0) && y0 + TY < min(ny, g.pml_y1) &&
-                    x0 - 1 >= max(1, g.pml_x0) && x0 + kQX < min(nx, g.pml_x1);
+    const QProf pf{sm.pr(cs), x0, y0};
+    const bool in = q_interior(g, y0, x0);
     // ---------------- phase 1: H half step
     // (strip tiles: the memories of the thread's cells are loaded first)
-    QM4 mm[RPT][2], mh[2];
-    const QM4 z4{0.f, 0.f, 0.f, 0.f};
+    QM4 mm[2][2], mh[2];
     if (!in) {
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          mm[r][q] = C::h_loads(a, y0 + warp + r * kQWarps, x0 + 2 * lane + q, sb);
+          mm[r][q] = C::h_loads(a, y0 + 2 * warp + r, x0 + lane + 32 * q, sb);
       if (warp == 0) {
-        mh[0] = C::h_loads(a, y0 - 1, x0 + 2 * lane, sb);
-        mh[1] = C::h_loads(a, y0 - 1, x0 + 2 * lane + 1, sb);
-      } else if (warp == 1 && lane < TY) {
+        mh[0] = C::h_loads(a, y0 - 1, x0 + lane, sb);
+        mh[1] = C::h_loads(a, y0 - 1, x0 + lane + 32, sb);
+      } else if (warp == 1) {
         mh[0] = C::h_loads(a, y0 + lane, x0 - 1, sb);
       }
     }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int oy = warp + r * kQWarps, y = y0 + oy;
+    for (int r = 0; r < 2; ++r) {
+      const int oy = 2 * warp + r, y = y0 + oy;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int ox = 2 * lane + q, x = x0 + ox;
+        const int ox = lane + 32 * q, x = x0 + ox;
         const float hx = HX[(oy + 1) * B::XW + ox], hz = HZ[oy * B::ZW + ox + 4];
         float hxn, hzn;
         if (in)
-          C::template h_phase<true>(a, E, CQ, hx, hz, y, x, y0, x0, sb, true, z4, hxn, hzn);
+          C::h_phase<true>(a, pf, E, CQ, hx, hz, y, x, y0, x0, sb, true, z4, hxn, hzn);
         else
-          C::template h_phase<false>(a, E, CQ, hx, hz, y, x, y0, x0, sb, true, mm[r][q], hxn,
-                                     hzn);
+          C::h_phase<false>(a, pf, E, CQ, hx, hz, y, x, y0, x0, sb, true, mm[r][q], hxn, hzn);
         sm.hxn[(oy + 1) * B::XW + ox] = hxn;
         sm.hzn[oy * B::ZW + ox + 4] = hzn;
         if (y < ny && x < nx) {
@@ -921,45 +1025,43 @@ kq_fwd_step(const __grid_constant__ QMaps m, const QFwdArgs a) {
     if (warp == 0) {  // halo row y0 - 1 (new Hx only)
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int ox = 2 * lane + q;
+        const int ox = lane + 32 * q;
         float hxn, hzn;
         if (in)
-          C::template h_phase<true>(a, E, CQ, HX[ox], 0.f, y0 - 1, x0 + ox, y0, x0, sb, false,
-                                    z4, hxn, hzn);
+          C::h_phase<true>(a, pf, E, CQ, HX[ox], 0.f, y0 - 1, x0 + ox, y0, x0, sb, false, z4,
+                           hxn, hzn);
         else
-          C::template h_phase<false>(a, E, CQ, HX[ox], 0.f, y0 - 1, x0 + ox, y0, x0, sb, false,
-                                     mh[q], hxn, hzn);
+          C::h_phase<false>(a, pf, E, CQ, HX[ox], 0.f, y0 - 1, x0 + ox, y0, x0, sb, false, mh[q],
+                            hxn, hzn);
         sm.hxn[ox] = hxn;
       }
-    } else if (warp == 1 && lane < TY) {  // halo column x0 - 1 (new Hz only)
+    } else if (warp == 1) {  // halo column x0 - 1 (new Hz only)
       const int oy = lane;
       float hxn, hzn;
       if (in)
-        C::template h_phase<true>(a, E, CQ, 0.f, HZ[oy * B::ZW + 3], y0 + oy, x0 - 1, y0, x0, sb,
-                                  false, z4, hxn, hzn);
+        C::h_phase<true>(a, pf, E, CQ, 0.f, HZ[oy * B::ZW + 3], y0 + oy, x0 - 1, y0, x0, sb,
+                         false, z4, hxn, hzn);
       else
-        C::template h_phase<false>(a, E, CQ, 0.f, HZ[oy * B::ZW + 3], y0 + oy, x0 - 1, y0, x0,
-                                   sb, false, mh[0], hxn, hzn);
+        C::h_phase<false>(a, pf, E, CQ, 0.f, HZ[oy * B::ZW + 3], y0 + oy, x0 - 1, y0, x0, sb,
+                          false, mh[0], hxn, hzn);
       sm.hzn[oy * B::ZW + 3] = hzn;
     }
-    __syncthreads();
+    q_csync();
     // ---------------- phase 2: E half step
-    const int pid = (shot * cm.tiles_y + tile / cm.tiles_x) * cm.tiles_x + tile % cm.tiles_x;
-    const bool pts = q_pts(cm.p0, cm.p1, pid);
-    float v[RPT][2];
+    float v[2][2];
     if (!in) {
 #pragma unroll
-      for (int r = 0; r < RPT; ++r)
+      for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-          mm[r][q] = C::e_loads(a, y0 + warp + r * kQWarps, x0 + 2 * lane + q, sb);
+          mm[r][q] = C::e_loads(a, y0 + 2 * warp + r, x0 + lane + 32 * q, sb);
     }
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int oy = warp + r * kQWarps, y = y0 + oy;
+    for (int r = 0; r < 2; ++r) {
+      const int oy = 2 * warp + r, y = y0 + oy;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int ox = 2 * lane + q, x = x0 + ox;
+        const int ox = lane + 32 * q, x = x0 + ox;
         const float eo = E[(oy + 1) * B::EW + ox + 4];
         const float vz = sm.hzn[oy * B::ZW + ox + 4], vzl = sm.hzn[oy * B::ZW + ox + 3];
         const float vx1 = sm.hxn[(oy + 1) * B::XW + ox], vx0 = sm.hxn[oy * B::XW + ox];
@@ -977,14 +1079,14 @@ kq_fwd_step(const __grid_constant__ QMaps m, const QFwdArgs a) {
           float dz = (vz - vzl) * g.rdx;
           float dy = (vx1 - vx0) * g.rdy;
           if (x < g.pml_x0 || x >= g.pml_x1) {
-            const float m1 = __ldg(g.bx + x) * mm[r][q].a + __ldg(g.ax + x) * dz;
+            const float m1 = pf.x(0, x) * mm[r][q].a + pf.x(1, x) * dz;
             a.mhz[j] = m1;
-            dz = dz / __ldg(g.kx + x) + m1;
+            dz = dz / pf.x(2, x) + m1;
           }
           if (y < g.pml_y0 || y >= g.pml_y1) {
-            const float m1 = __ldg(g.by + y) * mm[r][q].b + __ldg(g.ay + y) * dy;
+            const float m1 = pf.y(0, y) * mm[r][q].b + pf.y(1, y) * dy;
             a.mhx[j] = m1;
-            dy = dy / __ldg(g.ky + y) + m1;
+            dy = dy / pf.y(2, y) + m1;
           }
           const float curl = dz - dy;
           if (a.ey_st) store_stream(static_cast<SN *>(a.ey_st) + j, Codec<SN, float>::enc(eo));
@@ -994,31 +1096,21 @@ kq_fwd_step(const __grid_constant__ QMaps m, const QFwdArgs a) {
         v[r][q] = e;
       }
     }
-    if (pts) {
-      // sources (Ey += f, entry order), then receivers (r = Ey)
-      int *s_cell = reinterpret_cast<int *>(sm.ve);
-      float *s_val = sm.ve + kQPtChunk;
-      const int ybase = y0 * nx + x0;
-      q_points_add<TY, RPT>(cm.p0, cm.v0, pid, ybase, nx, v, s_cell, s_val);
-      q_points_record<TY, RPT>(cm.p1, cm.v1, pid, ybase, nx, v, s_cell,
-                               reinterpret_cast<int *>(s_val));
-    }
+    // sources (Ey += f, entry order), then receivers (r = Ey)
+    const int pid = (shot * cm.tiles_y + ty) * cm.tiles_x + tx;
+    q_points(sm.pt(k), cm, pid, y0 * nx + x0, v);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(sm.empty + k);
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-      const int y = y0 + warp + r * kQWarps;
+    for (int r = 0; r < 2; ++r) {
+      const int y = y0 + 2 * warp + r;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int x = x0 + 2 * lane + q;
+        const int x = x0 + lane + 32 * q;
         if (y < ny && x < nx) cm.ey_n[pb + (int64_t)y * cm.pitch + x] = v[r][q];
       }
     }
-    __syncthreads();  // stage k and the new-H tiles are free
-    if (tid == 0 && i + kQStages < n_units) {
-      int t2, s2, o2, g2, t1, s1, o1, g1;
-      sc.unit(i + kQStages, t2, s2, o2, g2);
-      sc.unit(i + kQStages - 1, t1, s1, o1, g1);
-      q_issue<TY, false>(sm, m, k, t2, s2, o2 != o1, o2 % kQStages, cm.tiles_x);
-    }
+    q_csync();  // the new-H tiles are free for the next unit
   }
 }
 

@@ -195,8 +195,8 @@ def set_fused_threshold(nbytes: int) -> int:
 
 
 def set_tma_mode(mode: int) -> int:
-    """One-sweep TMA time steps: 0 never, 1 on grids of at least 64 tiles
-    (default), 2 whenever eligible; returns the previous mode."""
+    """One-sweep TMA time steps: 0 never (default), 1 on grids of at least 64
+    tiles, 2 whenever eligible; returns the previous mode."""
     lib = load()
     lib.tide_b200_set_tma_mode.argtypes = [ctypes.c_int]
     lib.tide_b200_set_tma_mode.restype = ctypes.c_int
