@@ -428,8 +428,85 @@ TIDE_3D_DECLARE(8, double)
       int64_t source_component, int64_t receiver_component, int64_t n_threads, \
       int64_t device, int64_t execution_backend, void *compute_stream
 
-#define TIDE_3D_BORN_DECLARE(S, T) \
-  void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T));
+/* maxwell_3d_*_born_forward_with_storage_cuda.  Replaces
+ * maxwell_3d_{S}_{dtype}_born_forward_with_storage_cuda,
+ * src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:4045-4540 (argtypes
+ * src/tide/backend_utils.py:579-612).  born_forward plus, at steps
+ * t % step_ratio == 0 in device storage mode, the background E^n (when
+ * ca_requires_grad) and CPML-corrected curl H^n (when cb_requires_grad) into
+ * the s1 buffers, and the scattered E^n and curl into the dex_store ..
+ * dcurl_z_store buffers that are not null; snapshot t sits at byte offset
+ * (t / step_ratio) * n_shots * shot_bytes_uncomp.  Other storage modes store
+ * nothing, as in the reference.  CPML memories are full arrays. */
+#define TIDE_3D_BORN_FORWARD_WITH_STORAGE_ARGS(T)                              \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T *ex, T *ey, T *ez, T *hx, T *hy, T *hz,      \
+      T *m_hz_y, T *m_hy_z, T *m_hx_z, T *m_hz_x, T *m_hy_x, T *m_hx_y,        \
+      T *m_ey_z, T *m_ez_y, T *m_ez_x, T *m_ex_z, T *m_ex_y, T *m_ey_x,        \
+      T *dex, T *dey, T *dez, T *dhx, T *dhy, T *dhz, T *dm_hz_y, T *dm_hy_z,  \
+      T *dm_hx_z, T *dm_hz_x, T *dm_hy_x, T *dm_hx_y, T *dm_ey_z, T *dm_ez_y,  \
+      T *dm_ez_x, T *dm_ex_z, T *dm_ex_y, T *dm_ey_x, T *r, T *background_r,   \
+      void *ex_s1, void *ex_s3, void *ex_fn, void *ey_s1, void *ey_s3,         \
+      void *ey_fn, void *ez_s1, void *ez_s3, void *ez_fn, void *cx_s1,         \
+      void *cx_s3, void *cx_fn, void *cy_s1, void *cy_s3, void *cy_fn,         \
+      void *cz_s1, void *cz_s3, void *cz_fn, void *dex_store, void *dey_store, \
+      void *dez_store, void *dcurl_x_store, void *dcurl_y_store,               \
+      void *dcurl_z_store, T const *az, T const *bz, T const *azh,             \
+      T const *bzh, T const *ay, T const *by, T const *ayh, T const *byh,      \
+      T const *ax, T const *bx, T const *axh, T const *bxh, T const *kz,       \
+      T const *kzh, T const *ky, T const *kyh, T const *kx, T const *kxh,      \
+      int64_t const *sources_i, int64_t const *receivers_i, T rdz, T rdy,      \
+      T rdx, T dt, int64_t nt, int64_t n_shots, int64_t nz, int64_t ny,        \
+      int64_t nx, int64_t n_sources_per_shot, int64_t n_receivers_per_shot,    \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream, void *storage_stream
+
+/* maxwell_3d_*_born_backward_cuda.  Replaces
+ * maxwell_3d_{S}_{dtype}_born_backward_cuda,
+ * src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:5901-6290 (argtypes
+ * src/tide/backend_utils.py:614-633).  The adjoint of the Born map with
+ * respect to dca, dcb and the scattered sources: the exact adjoint of the
+ * background operator driven by grad_r, imaging against the stored
+ * background E^n / curl H^n into grad_ca / grad_cb (the gradients of dca /
+ * dcb) and recording grad_f at the sources.  grad_f, grad_ca, grad_cb and
+ * grad_*_shot are zeroed on entry; CPML memories and adjoint_memory_scratch
+ * are full [S, nz, ny, nx] arrays (12 of them in the scratch). */
+#define TIDE_3D_BORN_BACKWARD_ARGS(T)                                          \
+  T const *ca, T const *cb, T const *cq, T const *grad_r, T *lambda_ex,        \
+      T *lambda_ey, T *lambda_ez, T *lambda_hx, T *lambda_hy, T *lambda_hz,    \
+      T *m_lambda_ey_z, T *m_lambda_ez_y, T *m_lambda_ez_x, T *m_lambda_ex_z,  \
+      T *m_lambda_ex_y, T *m_lambda_ey_x, T *m_lambda_hz_y, T *m_lambda_hy_z,  \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, T *m_lambda_hy_x, T *m_lambda_hx_y,  \
+      T *adjoint_memory_scratch, void *ex_s1, void *ex_s3, void *ex_fn,        \
+      void *ey_s1, void *ey_s3, void *ey_fn, void *ez_s1, void *ez_s3,         \
+      void *ez_fn, void *cx_s1, void *cx_s3, void *cx_fn, void *cy_s1,         \
+      void *cy_s3, void *cy_fn, void *cz_s1, void *cz_s3, void *cz_fn,         \
+      T *grad_f, T *grad_ca, T *grad_cb, T *grad_ca_shot, T *grad_cb_shot,     \
+      T const *az, T const *bz, T const *azh, T const *bzh, T const *ay,       \
+      T const *by, T const *ayh, T const *byh, T const *ax, T const *bx,       \
+      T const *axh, T const *bxh, T const *kz, T const *kzh, T const *ky,      \
+      T const *kyh, T const *kx, T const *kxh, int64_t const *sources_i,       \
+      int64_t const *receivers_i, T rdz, T rdy, T rdx, T dt, int64_t nt,       \
+      int64_t n_shots, int64_t nz, int64_t ny, int64_t nx,                     \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream, void *storage_stream
+
+#define TIDE_3D_BORN_DECLARE(S, T)                                              \
+  void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T)); \
+  void maxwell_3d_##S##_##T##_born_forward_with_storage_cuda(                   \
+      TIDE_3D_BORN_FORWARD_WITH_STORAGE_ARGS(T));                               \
+  void maxwell_3d_##S##_##T##_born_backward_cuda(TIDE_3D_BORN_BACKWARD_ARGS(T));
 TIDE_3D_BORN_DECLARE(2, float)
 TIDE_3D_BORN_DECLARE(2, double)
 TIDE_3D_BORN_DECLARE(4, float)

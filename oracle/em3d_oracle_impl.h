@@ -252,7 +252,8 @@ static void FN(step_e)(const FN(g3) * g, const REAL *ca, const REAL *cb, REAL **
  * curls with their own CPML memories; the scattered update adds
  * dca E^n + dcb curl H^n of the background. */
 static void FN(step_e_born)(const FN(g3) * g, const REAL *ca, const REAL *cb, const REAL *dca,
-                            const REAL *dcb, REAL **F, REAL **M, REAL **DF, REAL **DM) {
+                            const REAL *dcb, REAL **F, REAL **M, REAL **DF, REAL **DM,
+                            void **st, int fmt) {
   const int64_t sz = g->ny * g->nx, sy = g->nx, P = g->P;
   for (int64_t s = 0; s < g->S; ++s)
     for (int64_t z = P; z < g->nz - P + 1; ++z)
@@ -294,6 +295,14 @@ static void FN(step_e_born)(const FN(g3) * g, const REAL *ca, const REAL *cb, co
             c[w][0] = dHy_dz - dHz_dy;
             c[w][1] = dHz_dx - dHx_dz;
             c[w][2] = dHx_dy - dHy_dx;
+          }
+          /* snapshots before the update (maxwell_3d_cuda_inst.cu:1291-1340):
+           * background E^n, curl H^n, scattered E^n, scattered curl */
+          for (int k = 0; k < 3; ++k) {
+            if (st && st[k]) FN(put)(st[k], fmt, i, F[k][i]);
+            if (st && st[3 + k]) FN(put)(st[3 + k], fmt, i, c[0][k]);
+            if (st && st[6 + k]) FN(put)(st[6 + k], fmt, i, DF[k][i]);
+            if (st && st[9 + k]) FN(put)(st[9 + k], fmt, i, c[1][k]);
           }
           for (int k = 0; k < 3; ++k) {
             const REAL e_old = F[k][i];
@@ -374,7 +383,37 @@ void FN(tide_oracle_em3d_forward)(const REAL *ca, const REAL *cb, const REAL *cq
 
 /* Born forward over steps [start_t, start_t + nt) (maxwell_3d_inst.cpp:
  * 1100-1527): F/M background, DF/DM scattered state; r records the scattered
- * and bg_r (may be NULL) the background receiver component. */
+ * and bg_r (may be NULL) the background receiver component.  store: 12
+ * snapshot histories (background E, curl H, scattered E, scattered curl; any
+ * may be NULL) written at steps t % k == 0 into slot t / k, or NULL. */
+void FN(tide_oracle_em3d_born_forward_store)(
+    const REAL *ca, const REAL *cb, const REAL *cq, const REAL *dca, const REAL *dcb,
+    const REAL *f0, const REAL *df, REAL **F, REAL **M, REAL **DF, REAL **DM, REAL *r,
+    REAL *bg_r, const REAL **prof, const int64_t *src_i, const int64_t *rec_i, REAL rdz,
+    REAL rdy, REAL rdx, int64_t nt, int64_t S, int64_t nz, int64_t ny, int64_t nx,
+    int64_t n_src, int64_t n_rec, int64_t start_t, const int64_t *pml, int ca_b, int cb_b,
+    int cq_b, int src_comp, int rec_comp, void **store, int64_t k, int fmt) {
+  FN(g3) g;
+  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
+  const size_t esz = fmt ? 2 : sizeof(REAL);
+  for (int64_t t = start_t; t < start_t + nt; ++t) {
+    FN(step_h)(&g, cq, F, M);
+    FN(step_h)(&g, cq, DF, DM);
+    void *st[12] = {0};
+    if (store && k > 0 && t % k == 0)
+      for (int c = 0; c < 12; ++c)
+        if (store[c]) st[c] = (char *)store[c] + (size_t)(t / k) * (size_t)(S * g.N) * esz;
+    FN(step_e_born)(&g, ca, cb, dca, dcb, F, M, DF, DM, store ? st : 0, fmt);
+    if (n_src > 0 && f0 && src_i) {
+      FN(inject)(F[src_comp], f0 + t * S * n_src, src_i, S, n_src, g.N);
+      FN(inject)(DF[src_comp], df + t * S * n_src, src_i, S, n_src, g.N);
+    }
+    if (n_rec > 0 && r && rec_i) FN(record)(r + t * S * n_rec, DF[rec_comp], rec_i, S, n_rec, g.N);
+    if (n_rec > 0 && bg_r && rec_i)
+      FN(record)(bg_r + t * S * n_rec, F[rec_comp], rec_i, S, n_rec, g.N);
+  }
+}
+
 void FN(tide_oracle_em3d_born_forward)(const REAL *ca, const REAL *cb, const REAL *cq,
                                        const REAL *dca, const REAL *dcb, const REAL *f0,
                                        const REAL *df, REAL **F, REAL **M, REAL **DF, REAL **DM,
@@ -384,20 +423,10 @@ void FN(tide_oracle_em3d_born_forward)(const REAL *ca, const REAL *cb, const REA
                                        int64_t ny, int64_t nx, int64_t n_src, int64_t n_rec,
                                        int64_t start_t, const int64_t *pml, int ca_b, int cb_b,
                                        int cq_b, int src_comp, int rec_comp) {
-  FN(g3) g;
-  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
-  for (int64_t t = start_t; t < start_t + nt; ++t) {
-    FN(step_h)(&g, cq, F, M);
-    FN(step_h)(&g, cq, DF, DM);
-    FN(step_e_born)(&g, ca, cb, dca, dcb, F, M, DF, DM);
-    if (n_src > 0 && f0 && src_i) {
-      FN(inject)(F[src_comp], f0 + t * S * n_src, src_i, S, n_src, g.N);
-      FN(inject)(DF[src_comp], df + t * S * n_src, src_i, S, n_src, g.N);
-    }
-    if (n_rec > 0 && r && rec_i) FN(record)(r + t * S * n_rec, DF[rec_comp], rec_i, S, n_rec, g.N);
-    if (n_rec > 0 && bg_r && rec_i)
-      FN(record)(bg_r + t * S * n_rec, F[rec_comp], rec_i, S, n_rec, g.N);
-  }
+  FN(tide_oracle_em3d_born_forward_store)(ca, cb, cq, dca, dcb, f0, df, F, M, DF, DM, r, bg_r,
+                                          prof, src_i, rec_i, rdz, rdy, rdx, nt, S, nz, ny, nx,
+                                          n_src, n_rec, start_t, pml, ca_b, cb_b, cq_b, src_comp,
+                                          rec_comp, 0, 0, 0);
 }
 
 /* Raw adjoint terms at the offset cell o (reference raw_e_side / raw_h_side). */

@@ -1,0 +1,72 @@
+"""Generate tests/golden/born3d_grad.npz from the reference's 3-D Born path.
+
+Run where the reference tree is mounted (read-only) at $TIDE_REFERENCE
+(default: a directory `reference` beside the repository):
+
+    python tests/golden/make_golden_born3d.py
+
+Imports the reference package and runs its public ``born3d`` on the Python
+(torch) path in FP64 (python_backend=True) for the two-shot case of
+em3d_case.npz and a seeded smooth (depsilon, dsigma) direction, stencils 2
+and 4; then back-propagates a seeded linear functional of the scattered
+receivers to depsilon and dsigma with torch autograd.  Stored: the
+direction, the functional's weights, the scattered receivers and the two
+gradients per stencil.
+"""
+
+from __future__ import annotations
+
+import os
+import pathlib
+import sys
+
+import numpy as np
+import torch
+
+HERE = pathlib.Path(__file__).resolve().parent
+REF = pathlib.Path(os.environ.get("TIDE_REFERENCE", pathlib.Path(__file__).resolve().parents[3] / "reference"))
+sys.path.insert(0, str(REF / "src"))
+
+from tide.maxwell.maxwell3d_born import born3d  # noqa: E402
+
+
+def direction(shape, seed=13):
+    g = torch.Generator().manual_seed(seed)
+    k = torch.ones((1, 1, 3, 3, 3), dtype=torch.float64) / 27
+
+    def smooth(scale):
+        u = torch.randn((1, 1) + shape, generator=g, dtype=torch.float64)
+        u = torch.nn.functional.conv3d(torch.nn.functional.pad(u, (1,) * 6, mode="replicate"), k)
+        return scale * u[0, 0]
+
+    return smooth(0.5), smooth(2e-3)
+
+
+def main():
+    z = np.load(HERE / "em3d_case.npz")
+    eps, sig, mu = (torch.from_numpy(z[n]) for n in ("eps", "sig", "mu"))
+    amp, src, rec = (torch.from_numpy(z[n]) for n in ("amp", "src", "rec"))
+    deps, dsig = direction(tuple(eps.shape))
+    out = {"deps": deps.numpy(), "dsig": dsig.numpy()}
+    for stencil in (2, 4):
+        dt = float(z["dt"]) * (1.0 if stencil == 2 else 0.5)
+        a = amp if stencil == 2 else torch.from_numpy(np.load(HERE / "em3d_hi_case.npz")["amp"])
+        de = deps.clone().requires_grad_(True)
+        ds = dsig.clone().requires_grad_(True)
+        res = born3d(eps, sig, mu, float(z["dx"]), dt, a, src, rec, depsilon=de, dsigma=ds,
+                     stencil=stencil, pml_width=int(z["pml"]), python_backend=True,
+                     fallback="error")
+        r = res[-1]
+        w = torch.randn(r.shape, generator=torch.Generator().manual_seed(17), dtype=r.dtype)
+        (r * w).sum().backward()
+        out[f"w_s{stencil}"] = w.numpy()
+        out[f"r_s{stencil}"] = r.detach().numpy()
+        out[f"geps_s{stencil}"] = de.grad.numpy()
+        out[f"gsig_s{stencil}"] = ds.grad.numpy()
+        out[f"dt_s{stencil}"] = dt
+        print(stencil, float(r.abs().max()), float(de.grad.abs().max()), float(ds.grad.abs().max()))
+    np.savez_compressed(HERE / "born3d_grad.npz", **out)
+
+
+if __name__ == "__main__":
+    main()

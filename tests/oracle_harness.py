@@ -250,18 +250,24 @@ class Oracle3D:
            int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp,
            st if st is not None else None, k, fmt)
 
-    def born_forward(self, pb, dca, dcb, f0, df, fields, mem, dfields, dmem, r, bg_r):
-        """3-D Born forward on full-layout state lists (see full_state)."""
-        fn, F = self._fn("born_forward", pb.dtype, pb.stencil)
+    def born_forward(self, pb, dca, dcb, f0, df, fields, mem, dfields, dmem, r, bg_r, *,
+                     store=None, k=1, fmt=0):
+        """3-D Born forward on full-layout state lists (see full_state).
+        store: 12 snapshot histories (background E x3, curl H x3, scattered
+        E x3, scattered curl x3; None entries are not stored) or None."""
+        fn, F = self._fn("born_forward_store", pb.dtype, pb.stencil)
         P, I = c_void_p, c_int64
         pml = (c_int64 * 6)(*pb.pml)
-        fn.argtypes = [P] * 7 + [P] * 4 + [P, P, P, P, P] + [F, F, F] + [I] * 8 + [P] + [c_int] * 5
+        fn.argtypes = ([P] * 7 + [P] * 4 + [P, P, P, P, P] + [F, F, F] + [I] * 8 + [P] +
+                       [c_int] * 5 + [P, I, c_int])
         prof = _ptr_array([pb.profiles[n].cpu() for n in PROFILES_3D])
+        st = (c_void_p * 12)(*[_p(t) if t is not None else None for t in store]) if store else None
         fn(_p(pb.ca), _p(pb.cb), _p(pb.cq.cpu()), _p(dca), _p(dcb), _p(f0), _p(df),
            _ptr_array(fields), _ptr_array(mem), _ptr_array(dfields), _ptr_array(dmem), _p(r),
            _p(bg_r), prof, _p(pb.sources_i.cpu()), _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy,
            pb.rdx, pb.nt, pb.n_shots, pb.nz, pb.ny, pb.nx, pb.n_src, pb.n_rec, 0, pml,
-           int(pb.batched), int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp)
+           int(pb.batched), int(pb.batched), int(pb.batched), pb.src_comp, pb.rec_comp, st, k,
+           fmt)
 
     def backward(self, pb, ca, cb, grad_r, store, *, k=1, fmt=0, need_ca=True, need_cb=True,
                  need_f=True, start_t=None, nt=None, lam=None, grads=None, eps_sigma=False):

@@ -13,14 +13,20 @@ tide_oracle_tm_born_forward_*):
 * a central finite difference of the oracle forward in (ca, cb, f): O(h^2);
 * the adjoint dot product against the oracle's exact adjoint over the stored
   background history (the Born adjoint in the perturbation).
+The 3-D Born forward is pinned to the reference CPU backend (stencils 2, 4,
+8), and its adjoint in the perturbation (Born forward with background
+histories, then the exact background adjoint) to the reference Python path's
+autograd gradient in depsilon / dsigma (golden born3d_grad.npz, FP64).
 """
 
 from __future__ import annotations
 
+import numpy as np
 import pytest
 import torch
 
 from cases import clone_problem, random_problem
+from conftest import GOLDEN
 from oracle_harness import REF_SO, Oracle, RefCPU, rel_l2
 
 
@@ -219,3 +225,73 @@ def test_born3d_oracle_matches_central_difference():
     fd = (receivers(h) - receivers(-h)) / (2 * h)
     assert rel_l2(r_born, fd) < 1e-6
     assert torch.equal(bg, receivers(0.0))
+
+
+# ------------------------------------------- 3-D Born adjoint (perturbation)
+class _OracleBorn3D(torch.autograd.Function):
+    """(dca, dcb, df) -> scattered receivers on the oracle: Born forward with
+    background E / curl H histories, backward = the exact background adjoint
+    imaging against them (the restatement of maxwell_3d_*_born_backward)."""
+
+    @staticmethod
+    def forward(ctx, dca, dcb, df, pb):
+        from oracle_harness import Oracle3D
+
+        F, M = Oracle3D.full_state(pb)
+        DF, DM = [torch.zeros_like(t) for t in F], [torch.zeros_like(t) for t in M]
+        r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+        bg = torch.zeros_like(r)
+        st = [torch.zeros((pb.nt, pb.n_shots, pb.nz, pb.ny, pb.nx), dtype=pb.dtype)
+              for _ in range(6)] + [None] * 6
+        Oracle3D().born_forward(pb, dca.detach(), dcb.detach(), pb.f, df.detach(), F, M, DF,
+                                DM, r, bg, store=st)
+        ctx.pb, ctx.st = pb, st[:6]
+        return r
+
+    @staticmethod
+    def backward(ctx, grad_r):
+        from oracle_harness import Oracle3D
+
+        pb = ctx.pb
+        gca, gcb, gf, _, _ = Oracle3D().backward(pb, pb.ca, pb.cb, grad_r.contiguous(), ctx.st)
+        return gca.unsqueeze(0), gcb.unsqueeze(0), gf.reshape(-1), None
+
+
+def born3d_oracle(eps, sig, mu, dx, dt, amp, src, rec, pml, stencil, deps, dsig):
+    """The Born receivers of born3d(depsilon, dsigma) on the oracle, CPU,
+    differentiable in deps / dsig (the born3d preparation restated)."""
+    from tide_b200.born import linearize_material_coefficients
+    from tide_b200 import physics as ph
+    from tide_b200.em3d import prepare_em3d
+
+    pb = prepare_em3d(eps, sig, mu, dx, dt, amp, src, rec, pml_width=pml, stencil=stencil)
+    pad = [a + b for a, b in zip(pb.fd_pad, pb.pml_width)]
+    shape = (pb.nz, pb.ny, pb.nx)
+    zp = lambda t: torch.nn.functional.pad(t, ph._torch_pad_order(pad))  # noqa: E731
+    dca, dcb = linearize_material_coefficients(pb.ca[0], pb.cb[0], pb.dt, zp(deps), zp(dsig))
+    dca, dcb = dca.reshape(1, *shape), dcb.reshape(1, *shape)
+    S, N = pb.n_shots, pb.nz * pb.ny * pb.nx
+    dcb_at = dcb.reshape(1, N).expand(S, -1).gather(1, pb.sources_i)
+    df = (amp.permute(2, 0, 1) * dcb_at[None] * (-1.0 / (dx * dx * dx))).reshape(-1)
+    return _OracleBorn3D.apply(dca, dcb, df, pb)
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_born3d_oracle_adjoint_matches_reference_autograd(stencil):
+    """The perturbation gradient of the Born receivers through the oracle's
+    Born forward + background adjoint equals the reference Python path's
+    autograd gradient (tests/golden/born3d_grad.npz, make_golden_born3d.py),
+    FP64, relative L2 < 1e-9; the receivers to 1e-13."""
+    z = np.load(GOLDEN / "em3d_case.npz")
+    g = np.load(GOLDEN / "born3d_grad.npz")
+    eps, sig, mu = (torch.from_numpy(z[n]) for n in ("eps", "sig", "mu"))
+    amp = torch.from_numpy(z["amp"] if stencil == 2 else np.load(GOLDEN / "em3d_hi_case.npz")["amp"])
+    deps = torch.from_numpy(g["deps"]).requires_grad_(True)
+    dsig = torch.from_numpy(g["dsig"]).requires_grad_(True)
+    r = born3d_oracle(eps, sig, mu, float(z["dx"]), float(g[f"dt_s{stencil}"]), amp,
+                      torch.from_numpy(z["src"]), torch.from_numpy(z["rec"]), int(z["pml"]),
+                      stencil, deps, dsig)
+    assert rel_l2(r.detach(), torch.from_numpy(g[f"r_s{stencil}"])) < 1e-13
+    (r * torch.from_numpy(g[f"w_s{stencil}"])).sum().backward()
+    assert rel_l2(deps.grad, torch.from_numpy(g[f"geps_s{stencil}"])) < 1e-9
+    assert rel_l2(dsig.grad, torch.from_numpy(g[f"gsig_s{stencil}"])) < 1e-9

@@ -304,3 +304,163 @@ def test_maxwell3d_jvp_matches_central_difference(cuda_device):
 
     fd = (data(h) - data(-h)) / (2 * h)
     assert rel_l2(jv, fd) < 1e-6
+
+
+# ------------------------------------------------- 3-D Born storage / backward
+def _born3d_store_cuda(pb, dca, dcb, df, dev, k, fmt, scattered=True):
+    """maxwell_3d_*_born_forward_with_storage in device mode: background E /
+    curl H and (optionally) scattered E / curl snapshots, full memories."""
+    import copy
+
+    from tide_b200 import em3d
+
+    q = copy.copy(pb)
+    mv = lambda t: t.detach().to(dev).clone()  # noqa: E731
+    q.ca, q.cb, q.cq, q.f = mv(pb.ca), mv(pb.cb), mv(pb.cq), mv(pb.f)
+    q.profiles = {kk: mv(v) for kk, v in pb.profiles.items()}
+    q.sources_i, q.receivers_i = mv(pb.sources_i), mv(pb.receivers_i)
+    q.fields = [mv(t) for t in pb.fields]
+    q.memories = [mv(pb.layout.unpack(t, a)) for t, a in zip(pb.memories, em3d.MEM_AXES)]
+    dfields = [torch.zeros_like(t) for t in q.fields]
+    dmem = [torch.zeros_like(t) for t in q.memories]
+    n_store = (pb.nt + k - 1) // k
+    sdt = torch.bfloat16 if fmt else q.dtype
+    shape = (n_store, q.n_shots, q.nz, q.ny, q.nx)
+    st = [torch.zeros(shape, device=dev, dtype=sdt) for _ in range(12 if scattered else 6)]
+    r = torch.zeros((q.nt, q.n_shots, q.n_rec), device=dev, dtype=q.dtype)
+    bg = torch.zeros_like(r)
+    d = [x.to(dev) for x in (dca, dcb, df)]
+    fn = nat.get_backend_function("maxwell_3d", "born_forward_with_storage", q.stencil, q.dtype,
+                                  dev)
+    p = nat.ptr
+    s18 = []
+    for c in range(6):
+        s18 += [p(st[c]), 0, 0]
+    s6 = [p(st[6 + c]) for c in range(6)] if scattered else [0] * 6
+    shot_bytes = q.nz * q.ny * q.nx * (2 if fmt else q.ca.element_size())
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    fn(p(q.ca), p(q.cb), p(q.cq), p(d[0]), p(d[1]), p(q.f), p(d[2]),
+       *[p(t) for t in q.fields], *[p(t) for t in q.memories], *[p(t) for t in dfields],
+       *[p(t) for t in dmem], p(r), p(bg), *s18, *s6, *em3d._profile_ptrs(q), p(q.sources_i),
+       p(q.receivers_i), q.rdz, q.rdy, q.rdx, q.dt, q.nt, q.n_shots, q.nz, q.ny, q.nx, q.n_src,
+       q.n_rec, k, 0, fmt, shot_bytes, True, True, q.batched, q.batched, q.batched, 0, *q.pml,
+       q.src_comp, q.rec_comp, 0, dev.index or 0, 0, stream, stream)
+    nat.check("born_forward_with_storage 3-D")
+    torch.cuda.synchronize()
+    return q, r, bg, st, shot_bytes
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("dtype,fmt", [(torch.float32, 0), (torch.float32, 1), (torch.float64, 0)])
+@pytest.mark.parametrize("k", [1, 2])
+def test_born3d_storage_bitwise_vs_oracle(cuda_device, stencil, dtype, fmt, k):
+    from oracle_harness import Oracle3D
+    from test_born_oracle import _case3d, _perturbation3d
+
+    pb = _case3d(dtype, ("ex", "ez"), stencil=stencil)
+    dca, dcb, df = _perturbation3d(pb, 7)
+    _, r, bg, st, _ = _born3d_store_cuda(pb, dca, dcb, df, cuda_device, k, fmt)
+    F, M = Oracle3D.full_state(pb)
+    DF, DM = [torch.zeros_like(t) for t in F], [torch.zeros_like(t) for t in M]
+    r_o = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype)
+    bg_o = torch.zeros_like(r_o)
+    st_o = [torch.zeros(t.shape, dtype=t.dtype) for t in st]
+    Oracle3D().born_forward(pb, dca, dcb, pb.f, df, F, M, DF, DM, r_o, bg_o, store=st_o, k=k,
+                            fmt=fmt)
+    _same(r, r_o, "scattered receivers")
+    _same(bg, bg_o, "background receivers")
+    for c in range(12):
+        assert torch.equal(st[c].cpu(), st_o[c]), f"snapshot kind {c}"
+    assert float(st_o[9].float().abs().max()) > 0
+    assert nat.device_status(cuda_device) == 0
+
+
+@pytest.mark.parametrize("stencil", [2, 6])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("k", [1, 3])
+def test_born3d_backward_bitwise_vs_oracle(cuda_device, stencil, dtype, k):
+    """maxwell_3d_*_born_backward: the background adjoint imaging against
+    the background snapshots of born_forward_with_storage (full memories)
+    equals the oracle's exact adjoint with the oracle's background
+    snapshots: grad dca, grad dcb, grad f and the adjoint state."""
+    from oracle_harness import Oracle3D
+    from test_born_oracle import _case3d, _perturbation3d
+
+    from tide_b200 import em3d
+
+    pb = _case3d(dtype, ("ey", "ex"), stencil=stencil)
+    dca, dcb, df = _perturbation3d(pb, 11)
+    q, r, _, st, shot_bytes = _born3d_store_cuda(pb, dca, dcb, df, cuda_device, k, 0,
+                                                 scattered=False)
+    dev = cuda_device
+    S, shape = q.n_shots, (q.n_shots, q.nz, q.ny, q.nx)
+    grad_r = torch.randn((pb.nt, S, pb.n_rec), generator=torch.Generator().manual_seed(4),
+                         dtype=dtype)
+    lam = [torch.zeros(shape, device=dev, dtype=dtype) for _ in range(6)]
+    lmem = [torch.zeros(shape, device=dev, dtype=dtype) for _ in range(12)]
+    scratch = torch.empty((12, *shape), device=dev, dtype=dtype)
+    mshape = (q.nz, q.ny, q.nx)
+    gca = torch.full(mshape, 7.0, device=dev, dtype=dtype)  # zeroed on entry
+    gcb = torch.full(mshape, 7.0, device=dev, dtype=dtype)
+    gca_s = torch.empty(shape, device=dev, dtype=dtype)
+    gcb_s = torch.empty(shape, device=dev, dtype=dtype)
+    gf = torch.full((pb.nt * S * q.n_src,), 7.0, device=dev, dtype=dtype)
+    fn = nat.get_backend_function("maxwell_3d", "born_backward", q.stencil, dtype, dev)
+    p = nat.ptr
+    s18 = []
+    for c in range(6):
+        s18 += [p(st[c]), 0, 0]
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    fn(p(q.ca), p(q.cb), p(q.cq), p(grad_r.to(dev)), *[p(t) for t in lam],
+       *[p(t) for t in lmem], p(scratch), *s18, p(gf), p(gca), p(gcb), p(gca_s), p(gcb_s),
+       *em3d._profile_ptrs(q), p(q.sources_i), p(q.receivers_i), q.rdz, q.rdy, q.rdx, q.dt,
+       q.nt, S, q.nz, q.ny, q.nx, q.n_src, q.n_rec, k, 0, 0, shot_bytes, True, True, q.batched,
+       q.batched, q.batched, q.nt, *q.pml, q.src_comp, q.rec_comp, 0, dev.index or 0, 0, stream,
+       stream)
+    nat.check("born_backward 3-D")
+    torch.cuda.synchronize()
+    # oracle: background snapshots from the oracle's own forward, then the adjoint
+    n_store = (pb.nt + k - 1) // k
+    st_o = [torch.zeros((n_store, S, pb.nz, pb.ny, pb.nx), dtype=dtype) for _ in range(6)]
+    r_o = torch.zeros((pb.nt, S, pb.n_rec), dtype=dtype)
+    f_o, m_o = Oracle3D.full_state(pb)
+    o = Oracle3D()
+    o.forward(pb, pb.ca, pb.cb, pb.f, r_o, f_o, m_o, store=st_o, k=k)
+    for c in range(6):
+        assert torch.equal(st[c].cpu(), st_o[c]), f"background snapshot kind {c}"
+    oca, ocb, ogf, ol, olm = o.backward(pb, pb.ca, pb.cb, grad_r, st_o, k=k)
+    _same(gca.reshape(oca.shape), oca, "grad dca")
+    _same(gcb.reshape(ocb.shape), ocb, "grad dcb")
+    _same(gf.reshape(ogf.shape), ogf, "grad f")
+    for name, a, b in zip("lEx lEy lEz lHx lHy lHz".split(), lam, ol):
+        _same(a, b, name)
+    for i, (a, b) in enumerate(zip(lmem, olm)):
+        _same(a, b, f"adjoint memory {i}")
+    assert float(oca.abs().max()) > 0
+    assert nat.device_status(dev) == 0
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_born3d_public_api_gradient_vs_reference_golden(cuda_device, stencil):
+    """tide_b200.em3d.born3d in FP64 with depsilon / dsigma requiring grad:
+    scattered receivers and the perturbation gradient of a seeded functional
+    against the reference Python path's autograd (born3d_grad.npz)."""
+    from tide_b200 import em3d
+
+    z = np.load(GOLDEN / "em3d_case.npz")
+    g = np.load(GOLDEN / "born3d_grad.npz")
+    dev = cuda_device
+    amp = z["amp"] if stencil == 2 else np.load(GOLDEN / "em3d_hi_case.npz")["amp"]
+    deps = torch.from_numpy(g["deps"]).to(dev).requires_grad_(True)
+    dsig = torch.from_numpy(g["dsig"]).to(dev).requires_grad_(True)
+    out = em3d.born3d(torch.from_numpy(z["eps"]).to(dev), torch.from_numpy(z["sig"]).to(dev),
+                      torch.from_numpy(z["mu"]).to(dev), float(z["dx"]), float(g[f"dt_s{stencil}"]),
+                      torch.from_numpy(amp).to(dev), torch.from_numpy(z["src"]).to(dev),
+                      torch.from_numpy(z["rec"]).to(dev), depsilon=deps, dsigma=dsig,
+                      stencil=stencil, pml_width=int(z["pml"]))
+    r = out[-1]
+    assert rel_l2(r.detach().cpu(), torch.from_numpy(g[f"r_s{stencil}"])) < 1e-13
+    (r * torch.from_numpy(g[f"w_s{stencil}"]).to(dev)).sum().backward()
+    assert rel_l2(deps.grad.cpu(), torch.from_numpy(g[f"geps_s{stencil}"])) < 1e-9
+    assert rel_l2(dsig.grad.cpu(), torch.from_numpy(g[f"gsig_s{stencil}"])) < 1e-9
+    assert nat.device_status(dev) == 0

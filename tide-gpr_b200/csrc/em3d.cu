@@ -367,14 +367,32 @@ template <typename T>
 struct BornMem {
   T *hz_y, *hy_z, *hx_z, *hz_x, *hy_x, *hx_y;  // E-phase memories of one state
 };
-template <typename T>
+// Snapshots one Born E half step stores (maxwell_3d_cuda_inst.cu:1291-1340),
+// each [S, nz, ny, nx] of the step or null: background E^n and curl H^n, then
+// scattered E^n and curl.
+template <typename S> struct BornSnap {
+  S *e[3], *c[3], *de[3], *dc[3];
+};
+template <typename S, typename T>
+__device__ __forceinline__ void born_store(const BornSnap<S> &sn, int64_t i, T *const E[3],
+                                           T *const D[3], const T (&cu)[2][3], int64_t j) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (sn.e[0]) sn.e[k][i] = Snap<S, T>::enc(E[k][j]);
+    if (sn.c[0]) sn.c[k][i] = Snap<S, T>::enc(cu[0][k]);
+    if (sn.de[0]) sn.de[k][i] = Snap<S, T>::enc(D[k][j]);
+    if (sn.dc[0]) sn.dc[k][i] = Snap<S, T>::enc(cu[1][k]);
+  }
+}
+template <typename T, typename S>
 __global__ void __launch_bounds__(256)
 k3_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
           const T *__restrict__ dca, const T *__restrict__ dcb, T *__restrict__ ex,
           T *__restrict__ ey, T *__restrict__ ez, const T *__restrict__ hx,
           const T *__restrict__ hy, const T *__restrict__ hz, T *__restrict__ dex,
           T *__restrict__ dey, T *__restrict__ dez, const T *__restrict__ dhx,
-          const T *__restrict__ dhy, const T *__restrict__ dhz, BornMem<T> mb, BornMem<T> ms) {
+          const T *__restrict__ dhy, const T *__restrict__ dhz, BornMem<T> mb, BornMem<T> ms,
+          BornSnap<S> sn) {
   Col c;
   if (!column(g, c)) return;
   const int ny = g.ny, nx = g.nx, y = c.y, x = c.x;
@@ -451,6 +469,7 @@ k3_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
       p_y[w] = h_y;
     }
     T *E[3] = {ex, ey, ez}, *D[3] = {dex, dey, dez};
+    born_store(sn, base + j, E, D, cu, j);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const T e_old = E[k][j];
@@ -1148,7 +1167,7 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
 }
 
 template <typename T, int ST>
-void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
+void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   (void)n_threads;
   (void)storage_stream;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
@@ -1211,7 +1230,7 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
                            kz, kzh, ky, kyh, kx, kxh};
   Launch3<T> L;
   if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
-             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched, compact))
     return;
   const G3<T> &g = L.g;
   const bool shot_ca = need_ca && !ca_batched && n_shots > 1;
@@ -1363,11 +1382,50 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T)) {
     TB_CUDA(cudaStreamSynchronize(st));
 }
 
+// Snapshot plan of born_forward_with_storage: device base pointers of the
+// six background kinds (s1) and of the six scattered kinds (ds), the byte
+// size of one stored step and the storage precision.
+struct BornStore {
+  void *s1[6];
+  void *ds[6];
+  size_t step_bytes;
+  bool bf16;
+};
+
+template <typename S, typename T>
+BornSnap<S> born_snap(const BornStore *bs, int64_t q) {
+  BornSnap<S> sn{};
+  if (!bs) return sn;
+  const size_t off = (size_t)q * bs->step_bytes;
+  auto at = [&](void *b) { return b ? reinterpret_cast<S *>(static_cast<char *>(b) + off) : nullptr; };
+  for (int k = 0; k < 3; ++k) {
+    sn.e[k] = at(bs->s1[k]);
+    sn.c[k] = at(bs->s1[3 + k]);
+    sn.de[k] = at(bs->ds[k]);
+    sn.dc[k] = at(bs->ds[3 + k]);
+  }
+  return sn;
+}
+
+template <typename T, int ST, typename S>
+void launch_born_e(const Launch3<T> &L, cudaStream_t st, const T *ca, const T *cb, const T *dca,
+                   const T *dcb, T *const F[6], T *const DF[6], const BornMem<T> &mb,
+                   const BornMem<T> &ms, const BornSnap<S> &sn) {
+  if constexpr (ST == 2)
+    k3_born_e<T, S><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, F[0], F[1], F[2], F[3],
+                                                F[4], F[5], DF[0], DF[1], DF[2], DF[3], DF[4],
+                                                DF[5], mb, ms, sn);
+  else
+    k3p_born_e<T, S, ST / 2><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, F[0], F[1], F[2],
+                                                         F[3], F[4], F[5], DF[0], DF[1], DF[2],
+                                                         DF[3], DF[4], DF[5], mb, ms, sn);
+}
+
 template <typename T, int ST>
-void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
-  (void)dt; (void)step_ratio; (void)n_threads;
+void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T), const BornStore *bs = nullptr) {
+  (void)dt; (void)n_threads;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
-  TB_REQUIRE(nt >= 0, "3-D born_forward: nt must be >= 0");
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D born_forward: bad nt / step_ratio");
   TB_REQUIRE(ca && cb && cq && dca && dcb && ex && ey && ez && hx && hy && hz && dex && dey &&
                  dez && dhx && dhy && dhz,
              "3-D born_forward: a field or coefficient pointer is null");
@@ -1410,12 +1468,13 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T)) {
                                                          Fw[4], Fw[5], Mw[6], Mw[7], Mw[8], Mw[9],
                                                          Mw[10], Mw[11]);
     }
-    if constexpr (ST == 2)
-      k3_born_e<T><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy, hz, dex,
-                                               dey, dez, dhx, dhy, dhz, mb, ms);
+    const bool store = bs && t % step_ratio == 0;
+    if (store && bs->bf16)
+      launch_born_e<T, ST>(L, st, ca, cb, dca, dcb, F, DF, mb, ms,
+                           born_snap<__nv_bfloat16, T>(bs, t / step_ratio));
     else
-      k3p_born_e<T, ST / 2><<<L.grid, L.block, 0, st>>>(L.g, ca, cb, dca, dcb, ex, ey, ez, hx, hy,
-                                                        hz, dex, dey, dez, dhx, dhy, dhz, mb, ms);
+      launch_born_e<T, ST>(L, st, ca, cb, dca, dcb, F, DF, mb, ms,
+                           born_snap<T, T>(store ? bs : nullptr, t / step_ratio));
     launches += 3;
     if (n_sources_per_shot > 0 && sources_i) {
       k3_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
@@ -1516,11 +1575,81 @@ TB3_DEFINE(8, double)
         receiver_component, n_threads, device, execution_backend, compute_stream);        \
   }
 
+#define TB3_BORN_STORE_DEFINE(S, T)                                                          \
+  extern "C" void maxwell_3d_##S##_##T##_born_forward_with_storage_cuda(                   \
+      TIDE_3D_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {                                         \
+    (void)ex_s3; (void)ex_fn; (void)ey_s3; (void)ey_fn; (void)ez_s3; (void)ez_fn;          \
+    (void)cx_s3; (void)cx_fn; (void)cy_s3; (void)cy_fn; (void)cz_s3; (void)cz_fn;          \
+    (void)storage_stream;                                                                  \
+    tb::BornStore bs{};                                                                    \
+    const size_t esz = storage_format == 1 ? 2 : sizeof(T);                                \
+    /* the reference stores in device mode only, at one snapshot per shot */               \
+    const bool direct = storage_mode == 0 && shot_bytes_uncomp == nz * ny * nx * (int64_t)esz; \
+    if (storage_format == 1 && sizeof(T) != 4) {                                           \
+      tb::set_error(tb::kBadArgument, "3-D born: bf16 snapshots need float32 fields");    \
+      return;                                                                              \
+    }                                                                                      \
+    if (direct) {                                                                          \
+      void *s1[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};                            \
+      void *ds[6] = {dex_store, dey_store, dez_store, dcurl_x_store, dcurl_y_store,        \
+                     dcurl_z_store};                                                       \
+      for (int k = 0; k < 6; ++k) {                                                        \
+        const bool need = k < 3 ? ca_requires_grad : cb_requires_grad;                    \
+        bs.s1[k] = need ? s1[k] : nullptr;                                                 \
+        bs.ds[k] = ds[k];                                                                  \
+      }                                                                                    \
+      for (int k = 0; k < 6; k += 3) {                                                     \
+        if (!bs.s1[k] || !bs.s1[k + 1] || !bs.s1[k + 2]) bs.s1[k] = bs.s1[k + 1] =        \
+            bs.s1[k + 2] = nullptr;                                                        \
+        if (!bs.ds[k] || !bs.ds[k + 1] || !bs.ds[k + 2]) bs.ds[k] = bs.ds[k + 1] =        \
+            bs.ds[k + 2] = nullptr;                                                        \
+      }                                                                                    \
+      bs.step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;                         \
+      bs.bf16 = storage_format == 1;                                                       \
+    }                                                                                      \
+    tb::em3d_born_forward<T, S>(                                                           \
+        ca, cb, cq, dca, dcb, f0, df, ex, ey, ez, hx, hy, hz, m_hz_y, m_hy_z, m_hx_z,      \
+        m_hz_x, m_hy_x, m_hx_y, m_ey_z, m_ez_y, m_ez_x, m_ex_z, m_ex_y, m_ey_x, dex, dey,  \
+        dez, dhx, dhy, dhz, dm_hz_y, dm_hy_z, dm_hx_z, dm_hz_x, dm_hy_x, dm_hx_y, dm_ey_z, \
+        dm_ez_y, dm_ez_x, dm_ex_z, dm_ex_y, dm_ey_x, r, background_r, az, bz, azh, bzh,   \
+        ay, by, ayh, byh, ax, bx, axh, bxh, kz, kzh, ky, kyh, kx, kxh, sources_i,          \
+        receivers_i, rdz, rdy, rdx, dt, nt, n_shots, nz, ny, nx, n_sources_per_shot,       \
+        n_receivers_per_shot, step_ratio, ca_batched, cb_batched, cq_batched, start_t,     \
+        pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1, source_component,                 \
+        receiver_component, n_threads, device, execution_backend, compute_stream,         \
+        direct ? &bs : nullptr);                                                           \
+  }                                                                                        \
+  extern "C" void maxwell_3d_##S##_##T##_born_backward_cuda(TIDE_3D_BORN_BACKWARD_ARGS(T)) { \
+    tb::em3d_backward<T, S>(                                                               \
+        ca, cb, cq, grad_r, lambda_ex, lambda_ey, lambda_ez, lambda_hx, lambda_hy,         \
+        lambda_hz, m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,             \
+        m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z, m_lambda_hx_z,         \
+        m_lambda_hz_x, m_lambda_hy_x, m_lambda_hx_y, adjoint_memory_scratch, ex_s1, ex_s3, \
+        ex_fn, ey_s1, ey_s3, ey_fn, ez_s1, ez_s3, ez_fn, cx_s1, cx_s3, cx_fn, cy_s1,       \
+        cy_s3, cy_fn, cz_s1, cz_s3, cz_fn, grad_f, grad_ca, grad_cb, nullptr, nullptr,     \
+        grad_ca_shot, grad_cb_shot, /*zero_grad_on_entry=*/true, az, bz, azh, bzh, ay, by, \
+        ayh, byh, ax, bx, axh, bxh, kz, kzh, ky, kyh, kx, kxh, sources_i, receivers_i,     \
+        rdz, rdy, rdx, dt, nt, n_shots, nz, ny, nx, n_sources_per_shot,                    \
+        n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp, \
+        ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,   \
+        pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1, source_component,                 \
+        receiver_component, n_threads, device, execution_backend, compute_stream,         \
+        storage_stream, /*compact=*/false);                                               \
+  }
+
 TB3_BORN_DEFINE(2, float)
+TB3_BORN_STORE_DEFINE(2, float)
 TB3_BORN_DEFINE(2, double)
+TB3_BORN_STORE_DEFINE(2, double)
 TB3_BORN_DEFINE(4, float)
+TB3_BORN_STORE_DEFINE(4, float)
 TB3_BORN_DEFINE(4, double)
+TB3_BORN_STORE_DEFINE(4, double)
 TB3_BORN_DEFINE(6, float)
+TB3_BORN_STORE_DEFINE(6, float)
 TB3_BORN_DEFINE(6, double)
+TB3_BORN_STORE_DEFINE(6, double)
 TB3_BORN_DEFINE(8, float)
+TB3_BORN_STORE_DEFINE(8, float)
 TB3_BORN_DEFINE(8, double)
+TB3_BORN_STORE_DEFINE(8, double)

@@ -220,14 +220,15 @@ k3p_fwd_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb, T *__rest
 }
 
 // Born E half step (maxwell_3d_inst.cpp:1390-1475) at orders 4 to 8.
-template <typename T, int P>
+template <typename T, typename S, int P>
 __global__ void __launch_bounds__(256)
 k3p_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
            const T *__restrict__ dca, const T *__restrict__ dcb, T *__restrict__ ex,
            T *__restrict__ ey, T *__restrict__ ez, const T *__restrict__ hx,
            const T *__restrict__ hy, const T *__restrict__ hz, T *__restrict__ dex,
            T *__restrict__ dey, T *__restrict__ dez, const T *__restrict__ dhx,
-           const T *__restrict__ dhy, const T *__restrict__ dhz, BornMem<T> mb, BornMem<T> ms) {
+           const T *__restrict__ dhy, const T *__restrict__ dhz, BornMem<T> mb, BornMem<T> ms,
+           BornSnap<S> sn) {
   Col c;
   if (!column(g, c)) return;
   const int ny = g.ny, nx = g.nx, y = c.y, x = c.x;
@@ -244,16 +245,17 @@ k3p_born_e(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
     const int64_t j = ((int64_t)z * ny + y) * nx + x;
     const bool pz = z < g.z0 || z >= g.z1;
     const Prof<T> fz = prof_at(g, PAZ, PKZ, z, pz);
-    T c0[3], c1[3];
-    pcurl_h<T, P>(g, hx, hy, hz, j, z, y, x, pz, py, px, fz, fy, fx, mb, c0);
-    pcurl_h<T, P>(g, dhx, dhy, dhz, j, z, y, x, pz, py, px, fz, fy, fx, ms, c1);
+    T cu[2][3];
+    pcurl_h<T, P>(g, hx, hy, hz, j, z, y, x, pz, py, px, fz, fy, fx, mb, cu[0]);
+    pcurl_h<T, P>(g, dhx, dhy, dhz, j, z, y, x, pz, py, px, fz, fy, fx, ms, cu[1]);
     const T a = ld(ca + j), b = ld(cb + j), da = ld(dca + j), db = ld(dcb + j);
     T *E[3] = {ex, ey, ez}, *D[3] = {dex, dey, dez};
+    born_store(sn, base + j, E, D, cu, j);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const T e_old = E[k][j];
-      D[k][j] = a * D[k][j] + b * c1[k] + da * e_old + db * c0[k];
-      E[k][j] = a * e_old + b * c0[k];
+      D[k][j] = a * D[k][j] + b * cu[1][k] + da * e_old + db * cu[0][k];
+      E[k][j] = a * e_old + b * cu[0][k];
     }
   }
 }

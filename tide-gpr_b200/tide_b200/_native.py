@@ -99,6 +99,16 @@ SPECS.update({
         (_P, 3), (_P, 2), (_P, 2), *_3D_FIELDS, (_P, 6), (_P, 12), (_P, 2), *_3D_PROFILES,
         *_3D_TAIL, *_3D_FLAGS, (_P, 1),
     ],
+    # src/tide/backend_utils.py:579-612
+    "maxwell_3d_born_forward_with_storage": [
+        (_P, 3), (_P, 2), (_P, 2), *_3D_FIELDS, (_P, 6), (_P, 12), (_P, 2), (_P, 18), (_P, 6),
+        *_3D_PROFILES, *_3D_TAIL, *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
+    ],
+    # src/tide/backend_utils.py:614-633
+    "maxwell_3d_born_backward": [
+        (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 2), (_P, 2),
+        *_3D_PROFILES, *_3D_TAIL, *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
+    ],
     # src/tide/backend_utils.py:537-556
     "maxwell_3d_backward": [
         (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 4), (_P, 2), (_B, 1),
@@ -231,9 +241,10 @@ def exported_symbols() -> list[str]:
         for p in ("background_vjp_reuse", "born_forward", "born_forward_with_storage",
                   "born_tangent_forward_with_storage", "born_backward")
     ] + [
-        symbol_name("maxwell_3d", "born_forward", a, d)
+        symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D
         for d in ("float", "double")
+        for p in ("born_forward", "born_forward_with_storage", "born_backward")
     ] + [
         symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D

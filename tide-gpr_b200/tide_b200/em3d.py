@@ -565,7 +565,98 @@ def maxwell3d(
     return (*outs, r)
 
 
-@torch.no_grad()
+class Born3DPropagate(torch.autograd.Function):
+    """The Born map (dca, dcb, df) -> scattered receivers on the native 3-D
+    Born entry points: forward maxwell_3d_*_born_forward_with_storage (device
+    history of the background E^n / curl H^n, full CPML memories), backward
+    maxwell_3d_*_born_backward (the background adjoint imaging against that
+    history), as the reference's Born3DForwardFunc
+    (src/tide/maxwell/maxwell3d_born_autograd.py:17-1276) for the
+    perturbation.  The background and scattered states advance in place in
+    the call's tensors (call = the arguments of the native born_forward)."""
+
+    @staticmethod
+    def forward(ctx, dca_p, dcb_p, df, call):
+        pb, k = call["pb"], max(1, call["pb"].grad_interval)
+        need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        n_store = (pb.nt + k - 1) // k
+        shape = (n_store, pb.n_shots, pb.nz, pb.ny, pb.nx)
+        empty = torch.empty(0, device=pb.device, dtype=pb.dtype)
+        st = [torch.empty(shape, device=pb.device, dtype=pb.dtype)
+              if (need_ca if c < 3 else need_cb) else empty for c in range(6)]
+        s18 = []
+        for t in st:
+            s18 += [_p(t), 0, 0]
+        shot_bytes = pb.nz * pb.ny * pb.nx * pb.ca.element_size()
+        fn = nat.get_backend_function("maxwell_3d", "born_forward_with_storage", pb.stencil,
+                                      pb.dtype, pb.device)
+        stream = torch.cuda.current_stream(pb.device).cuda_stream
+        r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
+        fn(*call["head"](dca_p, dcb_p, df, r), *s18, *[0] * 6, *_profile_ptrs(pb),
+           _p(pb.sources_i), _p(pb.receivers_i), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt,
+           pb.n_shots, pb.nz, pb.ny, pb.nx, call["n_src"], pb.n_rec, k, 0, 0, shot_bytes,
+           need_ca, need_cb, pb.batched, pb.batched, pb.batched, 0, *pb.pml, pb.src_comp,
+           pb.rec_comp, 0, pb.device.index or 0, 0, stream, stream)
+        nat.check("maxwell_3d born_forward_with_storage")
+        ctx.pb, ctx.st, ctx.k, ctx.shot_bytes = pb, st, k, shot_bytes
+        ctx.n_src, ctx.need_f = call["n_src"], ctx.needs_input_grad[2]
+        return r
+
+    @staticmethod
+    def backward(ctx, grad_r):
+        pb, dev, dt = ctx.pb, ctx.pb.device, ctx.pb.dtype
+        S = pb.n_shots
+        full = (S, pb.nz, pb.ny, pb.nx)
+        empty = torch.empty(0, device=dev, dtype=dt)
+        need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        lam = [torch.zeros(full, device=dev, dtype=dt) for _ in range(6)]
+        lmem = [torch.zeros(full, device=dev, dtype=dt) for _ in range(12)]
+        scratch = torch.empty((12, *full), device=dev, dtype=dt)
+        mshape = (1, pb.nz, pb.ny, pb.nx)
+        gca = torch.empty(mshape, device=dev, dtype=dt) if need_ca else empty
+        gcb = torch.empty(mshape, device=dev, dtype=dt) if need_cb else empty
+        gca_s = torch.empty(full, device=dev, dtype=dt) if need_ca and S > 1 else empty
+        gcb_s = torch.empty(full, device=dev, dtype=dt) if need_cb and S > 1 else empty
+        gf = (torch.empty(pb.nt * S * ctx.n_src, device=dev, dtype=dt)
+              if ctx.need_f and ctx.n_src > 0 else empty)
+        s18 = []
+        for t in ctx.st:
+            s18 += [_p(t), 0, 0]
+        fn = nat.get_backend_function("maxwell_3d", "born_backward", pb.stencil, dt, dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(grad_r.contiguous()), *[_p(t) for t in lam],
+           *[_p(t) for t in lmem], _p(scratch), *s18, _p(gf), _p(gca), _p(gcb), _p(gca_s),
+           _p(gcb_s), *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i), pb.rdz, pb.rdy,
+           pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, ctx.n_src, pb.n_rec, ctx.k, 0, 0,
+           ctx.shot_bytes, need_ca, need_cb, pb.batched, pb.batched, pb.batched, pb.nt, *pb.pml,
+           pb.src_comp, pb.rec_comp, 0, dev.index or 0, 0, stream, stream)
+        nat.check("maxwell_3d born_backward")
+        ctx.st = None
+        return (gca if need_ca else None, gcb if need_cb else None,
+                gf if ctx.need_f and ctx.n_src > 0 else None, None)
+
+
+def _born3d_prep(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
+                 receiver_location, stencil, pml_width, max_vel, nt, grad_interval,
+                 source_component, receiver_component, bg_init):
+    """Background problem of a Born run at the CFL-resampled internal step:
+    (problem, internal source amplitudes, step ratio, spacing)."""
+    if max_vel is None:
+        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
+    spacing = _spacing(grid_spacing)
+    inner_dt, ratio = ph.cfl_condition(spacing, dt, max_vel)
+    amp = source_amplitude
+    if ratio > 1 and amp is not None and amp.numel() > 0:
+        amp = ph.upsample(amp, ratio)
+    nt_int = nt * ratio if nt is not None else None
+    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, inner_dt, amp, source_location,
+                      receiver_location, stencil=stencil, pml_width=pml_width,
+                      source_component=source_component, receiver_component=receiver_component,
+                      model_gradient_sampling_interval=grad_interval, nt=nt_int,
+                      initial_state=bg_init)
+    return pb, amp, ratio, spacing
+
+
 def born3d(
     epsilon: torch.Tensor, sigma: torch.Tensor, mu: torch.Tensor,
     grid_spacing: float | Sequence[float], dt: float,
@@ -587,7 +678,12 @@ def born3d(
     dm_ey_x_0 (scattered).  Returns the background final state (18 tensors),
     the scattered final state (18), the background receivers (recorded when
     bg_receiver_location equals receiver_location, else empty) and the
-    scattered receivers.  Not differentiable in this build."""
+    scattered receivers.  The scattered receivers are differentiable in the
+    perturbation (depsilon / dsigma or dca / dcb, and the linearised source),
+    through the native Born backward against a device history of the
+    background; the background model enters as a constant (its second-order
+    terms are not built).  storage_mode is 'device' when a gradient is
+    needed."""
     from .born import linearize_material_coefficients
 
     if epsilon.ndim != 3:
@@ -600,19 +696,15 @@ def born3d(
     bg_init = [state_and_unused.get(f"{n}_0") for n in names]
     sc_init = [state_and_unused.get(f"d{n}_0") for n in names]
     epsilon, sigma, mu = epsilon.detach(), sigma.detach(), mu.detach()
-    if max_vel is None:
-        max_vel = float((1.0 / torch.sqrt(epsilon * mu)).max().item()) * ph.C0
-    spacing = _spacing(grid_spacing)
-    inner_dt, ratio = ph.cfl_condition(spacing, dt, max_vel)
-    amp = source_amplitude
-    if ratio > 1 and amp is not None and amp.numel() > 0:
-        amp = ph.upsample(amp, ratio)
-    nt_int = nt * ratio if nt is not None else None
-    pb = prepare_em3d(epsilon, sigma, mu, grid_spacing, inner_dt, amp, source_location,
-                      receiver_location, stencil=stencil, pml_width=pml_width,
-                      source_component=source_component, receiver_component=receiver_component,
-                      model_gradient_sampling_interval=model_gradient_sampling_interval,
-                      nt=nt_int, initial_state=bg_init)
+    pert = (depsilon, dsigma) if parameterization == "epsilon_sigma" else (dca, dcb)
+    grad_on = torch.is_grad_enabled() and any(
+        t is not None and t.requires_grad for t in pert)
+    with torch.no_grad():
+        prep = _born3d_prep(epsilon, sigma, mu, grid_spacing, dt, source_amplitude,
+                            source_location, receiver_location, stencil, pml_width, max_vel,
+                            nt, model_gradient_sampling_interval, source_component,
+                            receiver_component, bg_init)
+    pb, amp, ratio, spacing = prep
     dev, dtype = pb.device, pb.dtype
     pad = [a + b for a, b in zip(pb.fd_pad, pb.pml_width)]
     shape = (pb.nz, pb.ny, pb.nx)
@@ -651,23 +743,32 @@ def born3d(
     # the Born entry points keep full [S, nz, ny, nx] CPML memories
     bg_mem = [pb.layout.unpack(m, a).contiguous() for m, a in zip(pb.memories, MEM_AXES)]
     sc_mem = [pb.layout.unpack(m, a).contiguous() for m, a in zip(sc_mem, MEM_AXES)]
-    fn = nat.get_backend_function("maxwell_3d", "born_forward", pb.stencil, dtype, dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca_p), _p(dcb_p), _p(pb.f), _p(df),
-       *[_p(t) for t in pb.fields], *[_p(t) for t in bg_mem],
-       *[_p(t) for t in sc_fields], *[_p(t) for t in sc_mem], _p(r), _p(bg_r),
-       *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
-       pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, n_src, pb.n_rec, 1,
-       pb.batched, pb.batched, pb.batched, 0, *pb.pml, pb.src_comp, pb.rec_comp, 0,
-       dev.index or 0, 0, stream)
-    nat.check("maxwell_3d born_forward")
+
+    def head(a, b, f, rr):
+        return (_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(a), _p(b), _p(pb.f), _p(f),
+                *[_p(t) for t in pb.fields], *[_p(t) for t in bg_mem],
+                *[_p(t) for t in sc_fields], *[_p(t) for t in sc_mem], _p(rr), _p(bg_r))
+
+    if grad_on:
+        r = Born3DPropagate.apply(dca_p, dcb_p, df, {"pb": pb, "head": head, "n_src": n_src})
+    else:
+        fn = nat.get_backend_function("maxwell_3d", "born_forward", pb.stencil, dtype, dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        fn(*head(dca_p.detach(), dcb_p.detach(), df.detach(), r),
+           *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
+           pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, n_src, pb.n_rec, 1,
+           pb.batched, pb.batched, pb.batched, 0, *pb.pml, pb.src_comp, pb.rec_comp, 0,
+           dev.index or 0, 0, stream)
+        nat.check("maxwell_3d born_forward")
     if not same_rec and bg_receiver_location is not None and bg_receiver_location.numel() > 0:
-        bg_r = maxwell3d(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
-                         bg_receiver_location, stencil=stencil, pml_width=pml_width,
-                         max_vel=max_vel, nt=nt, source_component=source_component,
-                         receiver_component=receiver_component, storage_mode="none",
-                         **{f"{n}_0" if n[0] in "EH" else n: t
-                            for n, t in zip(names, bg_init)})[-1]
+        with torch.no_grad():
+            bg_r = maxwell3d(epsilon, sigma, mu, grid_spacing, dt, source_amplitude,
+                             source_location, bg_receiver_location, stencil=stencil,
+                             pml_width=pml_width, max_vel=max_vel, nt=nt,
+                             source_component=source_component,
+                             receiver_component=receiver_component, storage_mode="none",
+                             **{f"{n}_0" if n[0] in "EH" else n: t
+                                for n, t in zip(names, bg_init)})[-1]
     elif same_rec and ratio > 1:
         bg_r = ph.downsample(bg_r.movedim(0, -1), ratio).movedim(-1, 0)
     if ratio > 1 and r.numel() > 0:
