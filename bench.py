@@ -371,6 +371,9 @@ def run_b200(args) -> None:
     stg.release_history_pool()  # the other legs budget device memory themselves
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         serving = serve_bench(args)
+    sweep = None
+    if rank == 0 and world == 1 and args.serve_sweep_jobs > 0:
+        sweep = serve_sweep(args)
     if rank == 0 and world == 1 and args.em3d_nt > 0:
         em3d_leg = em3d_bench(args)
     if rank == 0 and world == 1 and args.debye_nt > 0:
@@ -396,7 +399,7 @@ def run_b200(args) -> None:
             "gpu_launches": int(launches),
             "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
             "tma_path": tma_leg,
-            "serving": serving,
+            "serving": serving, "serving_sweep": sweep,
             "em3d": em3d_leg, "debye": debye_leg,
         }
         print(json.dumps(line), flush=True)
@@ -533,6 +536,63 @@ def serve_bench(args) -> dict:
         "engine_launches": launches, "plain_launches": int(plain_launches), "plans": modes,
         "timing": "wall clock around host-to-host runs (models and sources in host memory, "
                   "results copied back), torch.cuda.synchronize at the end",
+    }
+
+
+def serve_sweep(args) -> dict:
+    """Load sweep of the served stream on a bounded sample: the first
+    `serve_sweep_jobs` jobs of the seeded 2000-job stream with every nt
+    scaled by `serve_sweep_nt_scale` (sizes, shots and the forward/gradient
+    mix unchanged).  Capacity (all jobs at t = 0) through the server, the
+    same jobs one after another through the per-job path (plain), then
+    Poisson arrivals at each load of `serve_sweep_loads` x the served
+    capacity with p50 / p99 latency per load."""
+    from tide_b200 import serve as sv
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    torch.cuda.empty_cache()
+    n, scale = args.serve_sweep_jobs, args.serve_sweep_nt_scale
+    jobs = sv.mixed_stream(n, seed=3, nt_scale=scale)
+    cells = sum(j.cell_updates() for j in jobs)
+    with sv.TMServer(dev, chunk_steps=args.serve_chunk) as srv:
+        srv.serve([sv.mixed_stream(1, seed=11, nt_scale=0.02)[0]], realtime=False)  # capture
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        srv.serve(jobs, realtime=False)
+        torch.cuda.synchronize(dev)
+        t_served = time.perf_counter() - t0
+        plans = {j.job_id: srv.plan(j) for j in jobs}
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    for j in jobs:
+        sv.run_plain(j, plans[j.job_id], dev)
+    torch.cuda.synchronize(dev)
+    t_plain = time.perf_counter() - t0
+    loads = {}
+    for load in [float(v) for v in args.serve_sweep_loads.split(",") if v]:
+        rate = load * n / t_served
+        stream = sv.mixed_stream(n, seed=3, rate=rate, nt_scale=scale)
+        torch.cuda.empty_cache()
+        with sv.TMServer(dev, chunk_steps=args.serve_chunk) as srv:
+            srv.serve([sv.mixed_stream(1, seed=11, nt_scale=0.02)[0]], realtime=False)
+            t0 = time.perf_counter()
+            res = srv.serve(stream, realtime=True)
+            t_stream = time.perf_counter() - t0
+        lat = [r.latency for r in res]
+        loads[str(load)] = {"rate_jobs_per_s": rate, "latency_p50_s": sv.percentile(lat, 50),
+                            "latency_p99_s": sv.percentile(lat, 99), "latency_max_s": max(lat),
+                            "stream_cell_updates_per_s": cells / t_stream}
+    sizes = [j.cell_updates() for j in jobs]
+    return {
+        "workload": f"served 2D TM stream, seed 3, first {n} of 2000 jobs, nt x {scale} "
+                    "(nz 128-1024, nx 256-2048 log-uniform, shots 1-32, 30 % forward+gradient), "
+                    "CPML 20, stencil 2, FP32",
+        "jobs": n, "cell_updates": cells,
+        "cell_updates_per_job_p10_p50_p90": [sv.percentile(sizes, q) for q in (10, 50, 90)],
+        "served_cell_updates_per_s": cells / t_served, "served_s": t_served,
+        "plain_cell_updates_per_s": cells / t_plain, "plain_s": t_plain,
+        "served_over_plain": t_plain / t_served, "loads": loads,
+        "timing": "wall clock around host-to-host runs, torch.cuda.synchronize at the end",
     }
 
 
@@ -921,6 +981,10 @@ def main() -> None:
     ap.add_argument("--serve-plain-jobs", type=int, default=32)
     ap.add_argument("--serve-chunk", type=int, default=32)
     ap.add_argument("--serve-load", type=float, default=0.8)
+    ap.add_argument("--serve-sweep-jobs", type=int, default=200,
+                    help="jobs of the bounded serving load sweep (0: skip)")
+    ap.add_argument("--serve-sweep-nt-scale", type=float, default=0.05)
+    ap.add_argument("--serve-sweep-loads", default="0.5,0.8,1.0")
     ap.add_argument("--tma-nt", type=int, default=400,
                     help="steps of the TMA-path comparison leg (0: skip)")
     ap.add_argument("--em3d-nt", type=int, default=1500,
