@@ -649,11 +649,12 @@ def em3d_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho: float) -> float
         return 9 * f + f / S + strips
     if kind == "em3d_fwd_e":  # read H; RMW E; ca, cb; store E^t and curl H^t
         return 9 * f + 2 * f / S + strips + 6 * snap_bytes
-    if kind == "em3d_adj_e":  # read lambda_E; RMW lambda_H; cb; adjoint memories
-        return 9 * f + f / S + strips
+    if kind == "em3d_adj_e":  # read lambda_E; RMW lambda_H; cb; adjoint memories; and the
+        # previous stored step's gradient term: six snapshots, two per-shot gradients RMW
+        return 9 * f + f / S + strips + 6 * snap_bytes + 2 * 2 * f
     if kind == "em3d_adj_h":  # read lambda_H; RMW lambda_E; ca, cq; adjoint memories
         return 9 * f + 2 * f / S + strips
-    if kind == "em3d_grad":  # read lambda_E, six snapshots; RMW two per-shot gradients
+    if kind == "em3d_grad":  # last step's term: lambda_E, six snapshots, two gradients RMW
         return 3 * f + 6 * snap_bytes + 2 * 2 * f
     raise KeyError(kind)
 

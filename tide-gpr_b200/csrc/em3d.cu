@@ -525,17 +525,52 @@ template <typename T> struct OpsAE {
   T b, lx, ly, lz, by_, lzy, lxy, bx_, lzx, lyx, hx, hy, hz;
 };
 
+// Coefficient-gradient term of one stored step (maxwell_3d_cuda_inst.cu:
+// 2301-2368), taken by the adjoint E launch of the next (earlier) step, which
+// reads the same lambda_E: grad_ca += (lEx Ex^t + lEy Ey^t + lEz Ez^t) k and
+// grad_cb likewise with curl H^t, into the per-shot buffers when several
+// unbatched shots share the model.  Snapshot pointers are those of the step
+// (null: that half off); `on` false: no term.
+template <typename T, typename S> struct GradFold {
+  const S *e[3], *c[3];
+  T *gca, *gcb, *gca_shot, *gcb_shot;
+  T kscale;
+  bool on;
+};
+template <typename T, typename S>
+__device__ __forceinline__ void fold_grad(const G3<T> &g, const GradFold<T, S> &gf, int64_t i,
+                                          int64_t j, T lx, T ly, T lz) {
+  if (!gf.on) return;
+  if (gf.e[0]) {
+    const T acc = lx * Snap<S, T>::dec(gf.e[0][i]) + ly * Snap<S, T>::dec(gf.e[1][i]) +
+                  lz * Snap<S, T>::dec(gf.e[2][i]);
+    const T v = acc * gf.kscale;
+    if (g.ca_b) gf.gca[i] = gf.gca[i] + v;
+    else if (g.S == 1) gf.gca[j] = gf.gca[j] + v;
+    else gf.gca_shot[i] = gf.gca_shot[i] + v;
+  }
+  if (gf.c[0]) {
+    const T acc = lx * Snap<S, T>::dec(gf.c[0][i]) + ly * Snap<S, T>::dec(gf.c[1][i]) +
+                  lz * Snap<S, T>::dec(gf.c[2][i]);
+    const T v = acc * gf.kscale;
+    if (g.cb_b) gf.gcb[i] = gf.gcb[i] + v;
+    else if (g.S == 1) gf.gcb[j] = gf.gcb[j] + v;
+    else gf.gcb_shot[i] = gf.gcb_shot[i] + v;
+  }
+}
+
 // Adjoint of the forward E update (maxwell_3d_cuda_inst.cu:1625-1695): next
 // E-phase memory adjoints at the own cell (in their strips), lambda_H
 // gathers raw terms of the own cell and of its z + 1, y + 1, x + 1
 // neighbours (zero outside the update domain).  The z + 1 terms come from
 // the prefetched operands of the next cell and become the own z terms of the
 // next step of the march.
-template <typename T>
+template <typename T, typename S>
 __global__ void __launch_bounds__(256, 3)
 k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
          const T *__restrict__ ley, const T *__restrict__ lez, T *__restrict__ lhx,
-         T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt) {
+         T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt,
+         GradFold<T, S> gf) {
   Col c;
   if (!column(g, c)) return;
   const int nz = g.nz, ny = g.ny, nx = g.nx, y = c.y, x = c.x;
@@ -609,6 +644,7 @@ k3_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
     OpsAE<T> on{};
     if (z + 1 < nz) on = load(j + sz);
     const T qx = o.b * o.lx, qy = o.b * o.ly, qz = o.b * o.lz;
+    fold_grad(g, gf, base + j, j, o.lx, o.ly, o.lz);
     if (z < g.z0 || z >= g.z1) {
       const int64_t m = ((int64_t)ccoord(z, g.z0, g.zhs) * ny + y) * nx + x;
       const T bz = ld(g.p[PBZ] + z);
@@ -1269,15 +1305,42 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   const int S_ = (int)n_shots;
   int64_t launches = 0;
   ProfileScope ps(st);
+  // The coefficient-gradient term of a stored step t reads lambda_E as it
+  // stands after step t's receivers, which is what the adjoint E launch of
+  // step t - 1 reads: that launch takes it (`pending`), and a standalone
+  // pass takes the last step's.  Same additions in the same order as a
+  // separate pass.
+  const char *pending[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool has_pending = false;
+  auto fold_of = [&](auto tag) {
+    using S = decltype(tag);
+    GradFold<T, S> f{};
+    f.on = has_pending;
+    for (int k = 0; k < 3; ++k) {
+      f.e[k] = reinterpret_cast<const S *>(pending[k]);
+      f.c[k] = reinterpret_cast<const S *>(pending[3 + k]);
+    }
+    f.gca = grad_ca; f.gcb = grad_cb; f.gca_shot = grad_ca_shot; f.gcb_shot = grad_cb_shot;
+    f.kscale = (T)step_ratio;
+    return f;
+  };
+  auto launch_adj_e = [&](auto tag) {
+    using S = decltype(tag);
+    const GradFold<T, S> f = fold_of(tag);
+    if constexpr (ST == 2)
+      k3_adj_e<T, S><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez,
+                                                 lambda_hx, lambda_hy, lambda_hz, cur, nxt, f);
+    else
+      k3p_adj_e<T, S, ST / 2><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez,
+                                                          lambda_hx, lambda_hy, lambda_hz, cur,
+                                                          nxt, f);
+  };
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
     const bool smp = ps.sample(t);
     if (smp) ps.begin(kK3AdjE);
-    if constexpr (ST == 2)
-      k3_adj_e<T><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez, lambda_hx,
-                                              lambda_hy, lambda_hz, cur, nxt);
-    else
-      k3p_adj_e<T, ST / 2><<<L.grid, L.block, 0, st>>>(g, cb, lambda_ex, lambda_ey, lambda_ez,
-                                                       lambda_hx, lambda_hy, lambda_hz, cur, nxt);
+    if (has_pending && bf16) launch_adj_e(__nv_bfloat16(0.f));
+    else launch_adj_e(T(0));
+    has_pending = false;
     if (smp) ps.end(kK3AdjE);
     if (smp) ps.begin(kK3AdjH);
     if constexpr (ST == 2)
@@ -1336,23 +1399,28 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
         if (TB_CUDA(cudaEventRecord(staged.ev[ring], st))) return;
         staged_used[ring] = true;
       }
-      const T ks = (T)step_ratio;
-      if (smp) ps.begin(kK3Grad);
-      if (bf16)
-        k3_coeff_grad<T, __nv_bfloat16><<<L.grid, L.block, 0, st>>>(
-            g, lambda_ex, lambda_ey, lambda_ez, (const __nv_bfloat16 *)src[0],
-            (const __nv_bfloat16 *)src[1], (const __nv_bfloat16 *)src[2],
-            (const __nv_bfloat16 *)src[3], (const __nv_bfloat16 *)src[4],
-            (const __nv_bfloat16 *)src[5], grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
-      else
-        k3_coeff_grad<T, T><<<L.grid, L.block, 0, st>>>(
-            g, lambda_ex, lambda_ey, lambda_ez, (const T *)src[0], (const T *)src[1],
-            (const T *)src[2], (const T *)src[3], (const T *)src[4], (const T *)src[5],
-            grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
-      if (smp) ps.end(kK3Grad);
-      ++launches;
+      for (int c = 0; c < 6; ++c) pending[c] = src[c];
+      has_pending = true;
     }
     std::swap(cur, nxt);
+  }
+  if (has_pending) {  // the last step's term: a pass of its own
+    const T ks = (T)step_ratio;
+    const char *const *src = pending;
+    ps.begin(kK3Grad);
+    if (bf16)
+      k3_coeff_grad<T, __nv_bfloat16><<<L.grid, L.block, 0, st>>>(
+          g, lambda_ex, lambda_ey, lambda_ez, (const __nv_bfloat16 *)src[0],
+          (const __nv_bfloat16 *)src[1], (const __nv_bfloat16 *)src[2],
+          (const __nv_bfloat16 *)src[3], (const __nv_bfloat16 *)src[4],
+          (const __nv_bfloat16 *)src[5], grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
+    else
+      k3_coeff_grad<T, T><<<L.grid, L.block, 0, st>>>(
+          g, lambda_ex, lambda_ey, lambda_ez, (const T *)src[0], (const T *)src[1],
+          (const T *)src[2], (const T *)src[3], (const T *)src[4], (const T *)src[5],
+          grad_ca, grad_cb, grad_ca_shot, grad_cb_shot, ks);
+    ps.end(kK3Grad);
+    ++launches;
   }
   for (int m = 0; m < 12; ++m)
     if (cur.m[m] != lm[m]) {

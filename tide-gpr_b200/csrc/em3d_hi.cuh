@@ -308,11 +308,12 @@ __device__ __forceinline__ T pgather(const G3<T> &g, const T *__restrict__ coef,
 // Adjoint of the forward E update: next E-phase memory adjoints at the own
 // cell (in their strips) and lambda_H += transposed differences of the raw
 // terms of lambda_E's neighbourhood.
-template <typename T, int P>
+template <typename T, typename S, int P>
 __global__ void __launch_bounds__(256)
 k3p_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
           const T *__restrict__ ley, const T *__restrict__ lez, T *__restrict__ lhx,
-          T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt) {
+          T *__restrict__ lhy, T *__restrict__ lhz, Mem12<T> cur, Mem12<T> nxt,
+          GradFold<T, S> gf) {
   Col c;
   if (!column(g, c)) return;
   const int ny = g.ny, nx = g.nx, y = c.y, x = c.x;
@@ -328,7 +329,9 @@ k3p_adj_e(G3<T> g, const T *__restrict__ cb, const T *__restrict__ lex,
   for (int z = c.zb; z < c.ze; ++z) {
     const int64_t j = ((int64_t)z * ny + y) * nx + x;
     const T b = ld(cb + j);
-    const T qx = b * ld(lex + j), qy = b * ld(ley + j), qz = b * ld(lez + j);
+    const T lx = ld(lex + j), ly = ld(ley + j), lz = ld(lez + j);
+    const T qx = b * lx, qy = b * ly, qz = b * lz;
+    fold_grad(g, gf, base + j, j, lx, ly, lz);
     if (z < g.z0 || z >= g.z1) {
       const int64_t m = pmi<T, 0>(g, z, y, x);
       const T bz = ld(g.p[PBZ] + z);
