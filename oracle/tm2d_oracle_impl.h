@@ -194,7 +194,7 @@ static void FN(step_e_born)(const FN(geom) * g, const REAL *ca, const REAL *cb,
                             const REAL *hz, REAL *ey, REAL *m_hx_z,
                             REAL *m_hz_x, const REAL *dhx, const REAL *dhz,
                             REAL *dey, REAL *dm_hx_z, REAL *dm_hz_x,
-                            int64_t s) {
+                            void *const st[4], bool bf16, int64_t s) {
   const int64_t ny = g->ny, nx = g->nx, N = ny * nx;
   const int p = g->stencil / 2;
   for (int64_t y = p; y < ny - p + 1; ++y) {
@@ -229,6 +229,15 @@ static void FN(step_e_born)(const FN(geom) * g, const REAL *ca, const REAL *cb,
       }
       const REAL dcurl = ddhz_dx - ddhx_dz;
       const REAL ey_n = ey[i], dey_n = dey[i];
+      /* snapshots before the update: Ey^n, curl H^n, dEy^n, dcurl */
+      const REAL vals[4] = {ey_n, curl, dey_n, dcurl};
+      for (int k = 0; k < 4; ++k)
+        if (st && st[k]) {
+          if (bf16)
+            ((uint16_t *)st[k])[i] = FN(to_bf16)(vals[k]);
+          else
+            ((REAL *)st[k])[i] = vals[k];
+        }
       ey[i] = cav * ey_n + cbv * curl;
       dey[i] = cav * dey_n + cbv * dcurl + dcav * ey_n + dcbv * curl;
     }
@@ -473,7 +482,54 @@ void FN(tide_oracle_tm_forward_with_storage)(
 }
 
 /* Born forward: argument meaning of the reference's
- * maxwell_tm_{S}_{dtype}_born_forward (maxwell_tm_inst.cpp:962-1045). */
+ * maxwell_tm_{S}_{dtype}_born_forward (maxwell_tm_inst.cpp:962-1045); with
+ * store (4 histories [n_store, S, ny, nx]: background Ey^n, curl H^n,
+ * scattered dEy^n, dcurl; NULL entries are skipped) the snapshots of steps
+ * t % step_ratio == 0 into slot t / step_ratio. */
+void FN(tide_oracle_tm_born_forward_store)(
+    int stencil, const REAL *ca, const REAL *cb, const REAL *cq,
+    const REAL *dca, const REAL *dcb, const REAL *f0, const REAL *df,
+    REAL *ey, REAL *hx, REAL *hz, REAL *m_ey_x, REAL *m_ey_z, REAL *m_hx_z,
+    REAL *m_hz_x, REAL *dey, REAL *dhx, REAL *dhz, REAL *dm_ey_x,
+    REAL *dm_ey_z, REAL *dm_hx_z, REAL *dm_hz_x, REAL *r, REAL *background_r,
+    const REAL *ay, const REAL *by, const REAL *ayh, const REAL *byh,
+    const REAL *ax, const REAL *bx, const REAL *axh, const REAL *bxh,
+    const REAL *ky, const REAL *kyh, const REAL *kx, const REAL *kxh,
+    const int64_t *sources_i, const int64_t *receivers_i, REAL rdy, REAL rdx,
+    int64_t nt, int64_t n_shots, int64_t ny, int64_t nx, int64_t n_src,
+    int64_t n_rec, bool ca_batched, bool cb_batched, bool cq_batched,
+    int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,
+    int64_t pml_x1, void **store, int64_t step_ratio, int64_t storage_format) {
+  ORACLE_GEOM_INIT
+  const int64_t N = ny * nx;
+  const bool bf16 = storage_format == 1;
+  const size_t esz = bf16 ? 2 : sizeof(REAL);
+#pragma omp parallel for schedule(static)
+  for (int64_t s = 0; s < n_shots; ++s) {
+    for (int64_t t = start_t; t < start_t + nt; ++t) {
+      FN(step_h)(&g, cq, ey, hx, hz, m_ey_x, m_ey_z, s);
+      FN(step_h)(&g, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z, s);
+      void *st[4] = {NULL, NULL, NULL, NULL};
+      if (store && step_ratio > 0 && t % step_ratio == 0)
+        for (int k = 0; k < 4; ++k)
+          if (store[k])
+            st[k] = (char *)store[k] + (size_t)((t / step_ratio) * n_shots * N) * esz;
+      FN(step_e_born)(&g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx,
+                      dhz, dey, dm_hx_z, dm_hz_x, st, bf16, s);
+      if (n_src > 0) {
+        FN(inject)(ey, f0 + t * n_shots * n_src, sources_i, n_src, N, s);
+        FN(inject)(dey, df + t * n_shots * n_src, sources_i, n_src, N, s);
+      }
+      if (n_rec > 0) {
+        FN(record)(r + t * n_shots * n_rec, dey, receivers_i, n_rec, N, s);
+        if (background_r)
+          FN(record)(background_r + t * n_shots * n_rec, ey, receivers_i,
+                     n_rec, N, s);
+      }
+    }
+  }
+}
+
 void FN(tide_oracle_tm_born_forward)(
     int stencil, const REAL *ca, const REAL *cb, const REAL *cq,
     const REAL *dca, const REAL *dcb, const REAL *f0, const REAL *df,
@@ -488,27 +544,12 @@ void FN(tide_oracle_tm_born_forward)(
     int64_t n_rec, bool ca_batched, bool cb_batched, bool cq_batched,
     int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,
     int64_t pml_x1) {
-  ORACLE_GEOM_INIT
-  const int64_t N = ny * nx;
-#pragma omp parallel for schedule(static)
-  for (int64_t s = 0; s < n_shots; ++s) {
-    for (int64_t t = start_t; t < start_t + nt; ++t) {
-      FN(step_h)(&g, cq, ey, hx, hz, m_ey_x, m_ey_z, s);
-      FN(step_h)(&g, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z, s);
-      FN(step_e_born)(&g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx,
-                      dhz, dey, dm_hx_z, dm_hz_x, s);
-      if (n_src > 0) {
-        FN(inject)(ey, f0 + t * n_shots * n_src, sources_i, n_src, N, s);
-        FN(inject)(dey, df + t * n_shots * n_src, sources_i, n_src, N, s);
-      }
-      if (n_rec > 0) {
-        FN(record)(r + t * n_shots * n_rec, dey, receivers_i, n_rec, N, s);
-        if (background_r)
-          FN(record)(background_r + t * n_shots * n_rec, ey, receivers_i,
-                     n_rec, N, s);
-      }
-    }
-  }
+  FN(tide_oracle_tm_born_forward_store)(
+      stencil, ca, cb, cq, dca, dcb, f0, df, ey, hx, hz, m_ey_x, m_ey_z, m_hx_z, m_hz_x, dey,
+      dhx, dhz, dm_ey_x, dm_ey_z, dm_hx_z, dm_hz_x, r, background_r, ay, by, ayh, byh, ax, bx,
+      axh, bxh, ky, kyh, kx, kxh, sources_i, receivers_i, rdy, rdx, nt, n_shots, ny, nx, n_src,
+      n_rec, ca_batched, cb_batched, cq_batched, start_t, pml_y0, pml_x0, pml_y1, pml_x1, NULL,
+      0, 0);
 }
 
 /* Exact adjoint with fused coefficient gradient, device storage mode.
@@ -639,6 +680,132 @@ void FN(tide_oracle_tm_backward)(
       }
     }
   }
+}
+
+/* Step-major image of one stored step: grad[j] += sum over shots, in shot
+ * order, of lam[s, j] * store[s, j] * k (cells of the update domain). */
+static void FN(image_step)(const FN(geom) * g, const REAL *lam, const void *store, int64_t off,
+                           int bf16, REAL kscale, REAL *grad, int batched) {
+  const int64_t N = g->ny * g->nx;
+  const int p = g->stencil / 2;
+  for (int64_t y = p; y < g->ny - p + 1; ++y)
+    for (int64_t x = p; x < g->nx - p + 1; ++x) {
+      const int64_t j = y * g->nx + x;
+      REAL sum = (REAL)0;
+      for (int64_t s = 0; s < g->n_shots; ++s) {
+        const int64_t i = s * N + j;
+        const REAL v = bf16 ? FN(from_bf16)(((const uint16_t *)store)[off + i])
+                            : ((const REAL *)store)[off + i];
+        const REAL term = lam[i] * v * kscale;
+        if (batched)
+          grad[i] = grad[i] + term;
+        else
+          sum = sum + term;
+      }
+      if (!batched) grad[j] = grad[j] + sum;
+    }
+}
+
+/* Derivative of the Born receivers (and of the background receivers) in the
+ * background model, the perturbation and both source terms: the exact adjoint
+ * of the joint background + scattered recurrence (the reference's
+ * born_backward_bggrad, maxwell_tm_cuda_inst.cu:2785-3200, in its own
+ * formulation).  lam is the scattered state's adjoint (driven by grad_r),
+ * eta the background's (driven by grad_bg_r and by the scattered update's
+ * dependence on the background, dE' += dca E + dcb curlH):
+ *   per step, with lam and eta at t+1:  W = cb eta + dcb lam (the curl-H
+ *   adjoint's source of the background), eta_Ey <- ca eta + dca lam; the E-
+ *   and H-phase adjoints of lam (cb, ca) and of eta (with W in place of
+ *   cb eta and unit ca); receivers grad_r -> lam, grad_bg_r -> eta; sources
+ *   grad_df <- lam, grad_f0 <- eta; at stored steps, step-major:
+ *   grad_ca += eta E + lam dE,  grad_cb += eta curlH + lam dcurl,
+ *   grad_dca += lam E,  grad_dcb += lam curlH  (each times k, in that order).
+ * Stores: [n_store, S, ny, nx] background Ey / curl H and scattered dEy /
+ * dcurl.  scratch: 8 S ny nx (next-step memories of lam then eta). */
+void FN(tide_oracle_tm_born_bggrad)(
+    int stencil, const REAL *ca, const REAL *cb, const REAL *cq, const REAL *dca,
+    const REAL *dcb, const REAL *grad_r, const REAL *grad_bg_r, REAL *lam_ey, REAL *lam_hx,
+    REAL *lam_hz, REAL **m_lam, REAL *eta_ey, REAL *eta_hx, REAL *eta_hz, REAL **m_eta,
+    REAL *scratch, const void *ey_store, const void *curl_store, const void *dey_store,
+    const void *dcurl_store, REAL *grad_df, REAL *grad_f0, REAL *grad_ca, REAL *grad_cb,
+    REAL *grad_dca, REAL *grad_dcb, const REAL *ay, const REAL *by, const REAL *ayh,
+    const REAL *byh, const REAL *ax, const REAL *bx, const REAL *axh, const REAL *bxh,
+    const REAL *ky, const REAL *kyh, const REAL *kx, const REAL *kxh,
+    const int64_t *sources_i, const int64_t *receivers_i, REAL rdy, REAL rdx, int64_t nt,
+    int64_t n_shots, int64_t ny, int64_t nx, int64_t n_src, int64_t n_rec,
+    int64_t step_ratio, int64_t storage_format, bool ca_batched, bool cb_batched,
+    bool cq_batched, int64_t start_t, int64_t pml_y0, int64_t pml_x0, int64_t pml_y1,
+    int64_t pml_x1) {
+  ORACLE_GEOM_INIT
+  const int64_t N = ny * nx, SN = n_shots * N;
+  const int p = stencil / 2;
+  const int bf16 = storage_format == 1;
+  const REAL kscale = (REAL)step_ratio;
+  REAL *ones = (REAL *)malloc((size_t)SN * sizeof(REAL));
+  REAL *w = (REAL *)calloc((size_t)SN, sizeof(REAL));
+  for (int64_t i = 0; i < SN; ++i) ones[i] = (REAL)1;
+  memset(scratch, 0, (size_t)8 * SN * sizeof(REAL));
+  /* memories: 0 ey_x, 1 ey_z, 2 hx_z, 3 hz_x; cur / next per state */
+  REAL *cl[4], *nl[4], *ce[4], *ne[4];
+  for (int m = 0; m < 4; ++m) {
+    cl[m] = m_lam[m];
+    nl[m] = scratch + m * SN;
+    ce[m] = m_eta[m];
+    ne[m] = scratch + (4 + m) * SN;
+  }
+  int64_t swaps = 0;
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    REAL *tmp;
+    for (int64_t s = 0; s < n_shots; ++s)
+      for (int64_t y = p; y < ny - p + 1; ++y)
+        for (int64_t x = p; x < nx - p + 1; ++x) {
+          const int64_t j = y * nx + x, i = s * N + j;
+          const REAL cbv = cb_batched ? cb[i] : cb[j], dcbv = cb_batched ? dcb[i] : dcb[j];
+          const REAL cav = ca_batched ? ca[i] : ca[j], dcav = ca_batched ? dca[i] : dca[j];
+          w[i] = cbv * eta_ey[i] + dcbv * lam_ey[i];
+          eta_ey[i] = cav * eta_ey[i] + dcav * lam_ey[i];
+        }
+    for (int64_t s = 0; s < n_shots; ++s) {
+      FN(adj_e)(&g, cb, lam_ey, lam_hx, lam_hz, cl[2], cl[3], nl[2], nl[3], s);
+      FN(adj_e)(&g, ones, w, eta_hx, eta_hz, ce[2], ce[3], ne[2], ne[3], s);
+    }
+    for (int m = 2; m < 4; ++m) {
+      tmp = cl[m]; cl[m] = nl[m]; nl[m] = tmp;
+      tmp = ce[m]; ce[m] = ne[m]; ne[m] = tmp;
+    }
+    for (int64_t s = 0; s < n_shots; ++s) {
+      FN(adj_h)(&g, ones, cq, eta_hx, eta_hz, eta_ey, ce[0], ce[1], ne[0], ne[1], s);
+      if (n_rec > 0 && grad_bg_r)
+        FN(inject)(eta_ey, grad_bg_r + t * n_shots * n_rec, receivers_i, n_rec, N, s);
+      if (n_src > 0 && grad_f0)
+        FN(record)(grad_f0 + t * n_shots * n_src, eta_ey, sources_i, n_src, N, s);
+      FN(adj_h)(&g, ca, cq, lam_hx, lam_hz, lam_ey, cl[0], cl[1], nl[0], nl[1], s);
+      if (n_rec > 0 && grad_r)
+        FN(inject)(lam_ey, grad_r + t * n_shots * n_rec, receivers_i, n_rec, N, s);
+      if (n_src > 0 && grad_df)
+        FN(record)(grad_df + t * n_shots * n_src, lam_ey, sources_i, n_src, N, s);
+    }
+    for (int m = 0; m < 2; ++m) {
+      tmp = cl[m]; cl[m] = nl[m]; nl[m] = tmp;
+      tmp = ce[m]; ce[m] = ne[m]; ne[m] = tmp;
+    }
+    ++swaps;
+    if (t % step_ratio != 0) continue;
+    const int64_t off = (t / step_ratio) * SN;
+    FN(image_step)(&g, eta_ey, ey_store, off, bf16, kscale, grad_ca, ca_batched);
+    FN(image_step)(&g, eta_ey, curl_store, off, bf16, kscale, grad_cb, cb_batched);
+    FN(image_step)(&g, lam_ey, dey_store, off, bf16, kscale, grad_ca, ca_batched);
+    FN(image_step)(&g, lam_ey, dcurl_store, off, bf16, kscale, grad_cb, cb_batched);
+    FN(image_step)(&g, lam_ey, ey_store, off, bf16, kscale, grad_dca, ca_batched);
+    FN(image_step)(&g, lam_ey, curl_store, off, bf16, kscale, grad_dcb, cb_batched);
+  }
+  if (swaps % 2 == 1)
+    for (int m = 0; m < 4; ++m) {
+      memcpy(m_lam[m], cl[m], (size_t)SN * sizeof(REAL));
+      memcpy(m_eta[m], ce[m], (size_t)SN * sizeof(REAL));
+    }
+  free(ones);
+  free(w);
 }
 
 #undef ORACLE_GEOM_INIT

@@ -101,20 +101,49 @@ class Oracle:
         return gca, gcb, gf, lam
 
 
-    def born_forward(self, pb, dca, dcb, f0, df, tan, r, bg_r, start_t=0, nt=None):
+    def born_forward(self, pb, dca, dcb, f0, df, tan, r, bg_r, start_t=0, nt=None, *,
+                     store=None, k=1, fmt=0):
         """Born forward: advance pb.fields (background) and tan (the 7
-        scattered state tensors) in place."""
+        scattered state tensors) in place.  store: 4 histories (background
+        Ey^n, curl H^n, scattered dEy^n, dcurl; None entries skipped) or None."""
         nt = pb.nt if nt is None else nt
         prof = [_p(pb.profiles[n]) for n in PROFILES]
         P, I, B = c_void_p, c_int64, c_bool
-        fn, F = self._fn("born_forward", pb.dtype, None)
+        fn, F = self._fn("born_forward_store", pb.dtype, None)
         fn.argtypes = ([c_int] + [P] * 7 + [P] * 14 + [P] * 2 + [P] * 12 + [P, P, F, F]
-                       + [I] * 6 + [B] * 3 + [I] * 5)
+                       + [I] * 6 + [B] * 3 + [I] * 5 + [P, I, I])
+        st = (c_void_p * 4)(*[_p(t) if t is not None else None for t in store]) if store else None
         fn(pb.stencil, _p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(f0), _p(df),
            *[_p(t) for t in pb.fields], *[_p(t) for t in tan], _p(r), _p(bg_r), *prof,
            _p(pb.sources_i), _p(pb.receivers_i), pb.rdy, pb.rdx, nt, pb.n_shots, pb.ny, pb.nx,
            pb.n_src, pb.n_rec, pb.batched, pb.batched, pb.batched, start_t, pb.pml_y0,
-           pb.pml_x0, pb.pml_y1, pb.pml_x1)
+           pb.pml_x0, pb.pml_y1, pb.pml_x1, st, k, fmt)
+
+    def born_bggrad(self, pb, dca, dcb, grad_r, grad_bg_r, store, *, k=1, fmt=0):
+        """Second-order Born adjoint (joint background + scattered state) over
+        the 4 histories of born_forward(store=...); returns grad_ca,
+        grad_cb, grad_dca, grad_dcb (model-shaped), grad_f0, grad_df
+        ([nt, S, n_src]), lam (7) and eta (7)."""
+        S, ny, nx, dt = pb.n_shots, pb.ny, pb.nx, pb.dtype
+        z = lambda *s: torch.zeros(s, dtype=dt)  # noqa: E731
+        lam = [z(S, ny, nx) for _ in range(7)]
+        eta = [z(S, ny, nx) for _ in range(7)]
+        scratch = z(8, S, ny, nx)
+        mshape = (S, ny, nx) if pb.batched else (ny, nx)
+        g = [z(*mshape) for _ in range(4)]
+        gf0, gdf = z(pb.nt, S, max(pb.n_src, 1)), z(pb.nt, S, max(pb.n_src, 1))
+        fn, F = self._fn("born_bggrad", dt, None)
+        P, I, B = c_void_p, c_int64, c_bool
+        fn.argtypes = ([c_int] + [P] * 7 + [P] * 3 + [P] + [P] * 3 + [P] + [P] + [P] * 4 + [P] * 6
+                       + [P] * 12 + [P, P, F, F] + [I] * 8 + [B] * 3 + [I] * 5)
+        arr = lambda ts: (c_void_p * len(ts))(*[_p(t) for t in ts])  # noqa: E731
+        fn(pb.stencil, _p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(grad_r),
+           _p(grad_bg_r), *[_p(t) for t in lam[:3]], arr(lam[3:]), *[_p(t) for t in eta[:3]],
+           arr(eta[3:]), _p(scratch), *[_p(t) for t in store], _p(gdf), _p(gf0), *[_p(t) for t in g],
+           *[_p(pb.profiles[n]) for n in PROFILES], _p(pb.sources_i), _p(pb.receivers_i), pb.rdy,
+           pb.rdx, pb.nt, S, ny, nx, pb.n_src, pb.n_rec, k, fmt, pb.batched, pb.batched,
+           pb.batched, pb.nt, pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1)
+        return (*g, gf0, gdf, lam, eta)
 
 class OracleTM(torch.autograd.Function):
     """Autograd node over (ca, cb, f) backed by the C oracle (CPU)."""

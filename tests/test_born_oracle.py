@@ -295,3 +295,64 @@ def test_born3d_oracle_adjoint_matches_reference_autograd(stencil):
     (r * torch.from_numpy(g[f"w_s{stencil}"])).sum().backward()
     assert rel_l2(deps.grad, torch.from_numpy(g[f"geps_s{stencil}"])) < 1e-9
     assert rel_l2(dsig.grad, torch.from_numpy(g[f"gsig_s{stencil}"])) < 1e-9
+
+
+# ------------------------------------ second-order Born (background gradient)
+class _OracleBornFull(torch.autograd.Function):
+    """(dca, dcb, df, ca, cb, f0) -> (background receivers, scattered
+    receivers) on the oracle; backward = the joint adjoint of the background
+    and scattered recurrences (the restatement of born_backward_bggrad)."""
+
+    @staticmethod
+    def forward(ctx, dca, dcb, df, ca, cb, f0, pb):
+        q = clone_problem(pb)
+        q.ca, q.cb = ca.detach(), cb.detach()
+        tan = _tangent_state(q)
+        r, bg = _zeros_r(q), _zeros_r(q)
+        shape = (q.nt, q.n_shots, q.ny, q.nx)
+        st = [torch.zeros(shape, dtype=q.dtype) for _ in range(4)]
+        Oracle().born_forward(q, dca.detach(), dcb.detach(), f0.detach(), df.detach(), tan, r, bg,
+                              store=st)
+        ctx.q, ctx.st = q, st
+        ctx.save_for_backward(dca, dcb)
+        return bg, r
+
+    @staticmethod
+    def backward(ctx, g_bg, g_r):
+        dca, dcb = ctx.saved_tensors
+        q = ctx.q
+        gca, gcb, gdca, gdcb, gf0, gdf, _, _ = Oracle().born_bggrad(
+            q, dca.detach(), dcb.detach(), g_r.contiguous(), g_bg.contiguous(), ctx.st)
+        n = q.nt * q.n_shots * q.n_src
+        return (gdca.unsqueeze(0), gdcb.unsqueeze(0), gdf.reshape(-1)[:n], gca.unsqueeze(0),
+                gcb.unsqueeze(0), gf0.reshape(-1)[:n], None)
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_born_second_order_oracle_matches_reference_autograd(stencil):
+    """Gradient of <w, scattered> + <wb, background> receivers in the
+    background epsilon / sigma and the direction depsilon / dsigma, through
+    the oracle's joint adjoint chained by torch autograd, equals the
+    reference Python Born path's autograd (born_bggrad.npz, FP64) to 1e-9."""
+    from cases import hetero_inputs
+    from tide_b200.born import prepare_born
+    from tide_b200.tm2d import prepare_tm2d
+
+    z = np.load(GOLDEN / "born_bggrad.npz")
+    c = hetero_inputs(torch.float64)
+    eps = c["eps"].clone().requires_grad_(True)
+    sig = c["sig"].clone().requires_grad_(True)
+    deps = torch.from_numpy(z["deps"]).requires_grad_(True)
+    dsig = torch.from_numpy(z["dsig"]).requires_grad_(True)
+    pb = prepare_tm2d(eps, sig, c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"],
+                      stencil=stencil, pml_width=c["pml"])
+    dca, dcb, df = prepare_born(pb, 1, c["dx"], c["amp"], depsilon=deps, dsigma=dsig)
+    bg, r = _OracleBornFull.apply(dca, dcb, df, pb.ca, pb.cb, pb.f, pb)
+    tag = f"s{stencil}"
+    assert rel_l2(r.detach(), torch.from_numpy(z[f"r_{tag}"])) < 1e-13
+    assert rel_l2(bg.detach(), torch.from_numpy(z[f"bg_r_{tag}"])) < 1e-13
+    ((r * torch.from_numpy(z[f"w_{tag}"])).sum() + (bg * torch.from_numpy(z[f"wb_{tag}"])).sum()
+     ).backward()
+    for name, t in (("geps", eps), ("gsig", sig), ("gdeps", deps), ("gdsig", dsig)):
+        err = rel_l2(t.grad, torch.from_numpy(z[f"{name}_{tag}"]))
+        assert err < 1e-9, (name, err)

@@ -78,7 +78,7 @@ cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   if (dev < 64 && !(kept.load() & (1ull << dev))) {
     cudaMemPool_t pool;
-    uint64_t keep = UINT64_MAX;
+    uint64_t keep = (uint64_t)4 << 30;  // up to 4 GiB stays mapped between calls
     e = cudaDeviceGetDefaultMemPool(&pool, dev);
     if (e == cudaSuccess) e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     if (e != cudaSuccess) return e;

@@ -44,8 +44,9 @@ enum KernelKind : int {
 void count_launches(int64_t n);
 
 // cudaMallocAsync on the current device's default pool, with the pool told
-// (once per device) to keep freed memory instead of releasing it at every
-// synchronisation, so per-call scratch is a pool hit after the first call.
+// (once per device) to keep up to 4 GiB of freed memory instead of releasing
+// it at every synchronisation, so per-call scratch is a pool hit after the
+// first call while larger transient use still goes back to the driver.
 cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st);
 
 // Brackets sampled launches with events on one stream; accumulates into the
