@@ -225,6 +225,48 @@ TIDE_TM_DECLARE(8, double)
       int64_t n_threads, int64_t device, void *compute_stream,                 \
       void *storage_stream
 
+/* maxwell_tm_*_born_backward_bggrad_cuda.  Replaces
+ * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:2785-3200 (argtypes
+ * src/tide/backend_utils.py:407-440): the derivative of grad_r . (scattered
+ * receivers) + grad_background_r . (background receivers) in the background
+ * coefficients (grad_ca, grad_cb), the perturbation (grad_dca, grad_dcb) and
+ * the background and scattered sources (grad_f0, grad_df), by the exact
+ * adjoint of the joint background + scattered recurrence over the background
+ * history (ey_store_1 / curl_store_1, [n_store, background_n_shots, ny, nx])
+ * and the scattered history (dey_store / dcurl_store, [n_store, n_shots,
+ * ny, nx]) of born_forward_with_storage, device storage mode.  ey / hx / hz
+ * receive the scattered state's adjoint, dey / dhx / dhz the background's,
+ * the eight memories theirs (all zeroed on entry); adjoint_memory_scratch
+ * holds 8 n_shots ny nx values and work_eta_x n_shots ny nx; the gradients
+ * accumulate, shot sums in-kernel (grad_*_shot, eta_source_old, work_eta_z
+ * and lambda_store are not used).  capture_background_adjoint /
+ * reuse_background_adjoint are rejected with a status message. */
+#define TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)                                   \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T const *grad_r, T const *grad_background_r,   \
+      void *ey_store_1, void *ey_store_3, char const *const *ey_filenames,     \
+      void *curl_store_1, void *curl_store_3, char const *const *curl_filenames, \
+      void const *dey_store, void const *dcurl_store, void *lambda_store,      \
+      int64_t background_n_shots, T *ey, T *hx, T *hz, T *dey, T *dhx, T *dhz, \
+      T *grad_f0, T *grad_df, T *grad_ca, T *grad_cb, T *grad_dca, T *grad_dcb, \
+      T *m_lambda_ey_x, T *m_lambda_ey_z, T *m_lambda_hx_z, T *m_lambda_hz_x,  \
+      T *m_eta_ey_x, T *m_eta_ey_z, T *m_eta_hx_z, T *m_eta_hz_x,              \
+      T *eta_source_old, T *work_eta_x, T *work_eta_z, T *grad_ca_shot,        \
+      T *grad_cb_shot, T *grad_dca_shot, T *grad_dcb_shot,                     \
+      T *adjoint_memory_scratch, T const *ay, T const *by, T const *ayh,       \
+      T const *byh, T const *ax, T const *bx, T const *axh, T const *bxh,      \
+      T const *ky, T const *kyh, T const *kx, T const *kxh,                    \
+      int64_t const *sources_i, int64_t const *receivers_i, T rdy, T rdx,      \
+      T dt, int64_t nt, int64_t n_shots, int64_t ny, int64_t nx,               \
+      int64_t n_sources_per_shot, int64_t n_receivers_per_shot,                \
+      int64_t step_ratio, int64_t storage_mode, int64_t storage_format,        \
+      int64_t shot_bytes_uncomp, bool ca_requires_grad, bool cb_requires_grad, \
+      bool capture_background_adjoint, bool reuse_background_adjoint,          \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_y0, int64_t pml_x0, int64_t pml_y1, int64_t pml_x1,          \
+      int64_t n_threads, int64_t device, void *compute_stream,                 \
+      void *storage_stream
+
 /* maxwell_tm_*_born_tangent_forward_with_storage_cuda.  Replaces
  * src/tide/csrc/tm2d/maxwell_tm_cuda_inst.cu:1974-2086 (argtypes
  * src/tide/backend_utils.py:372-384).  Advances only the scattered state,
@@ -256,7 +298,9 @@ TIDE_TM_DECLARE(8, double)
       TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T));                              \
   void maxwell_tm_##S##_##T##_born_tangent_forward_with_storage_cuda(          \
       TIDE_TM_BORN_TANGENT_ARGS(T));                                           \
-  void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T));
+  void maxwell_tm_##S##_##T##_born_backward_cuda(TIDE_TM_BORN_BACKWARD_ARGS(T));        \
+  void maxwell_tm_##S##_##T##_born_backward_bggrad_cuda(                       \
+      TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T));
 
 TIDE_TM_BORN_DECLARE(2, float)
 TIDE_TM_BORN_DECLARE(4, float)

@@ -13,8 +13,13 @@
   epsilon gradient of ``maxwelltm`` on interior cells (FP64, 1e-10), the
   background-receiver gradient equal to ``maxwelltm``'s bit for bit, and
   cpu / disk storage giving the device mode's gradients bit for bit;
-* the second-order term (scattered receivers in the background model) and
-  checkpoint storage raise.
+* the second-order term (scattered receivers in the background model):
+  ``born_backward_bggrad`` bit-identical to the oracle's joint adjoint
+  (gradients in ca, cb, dca, dcb, f0, df; stencils 2, 4, 6; FP32 and FP64;
+  sampling intervals 1 and 2), and ``borntm``'s gradients in epsilon, sigma,
+  depsilon, dsigma equal the reference Python path's autograd (FP64, 1e-9,
+  golden born_bggrad.npz);
+* the second-order term in cpu storage mode and checkpoint storage raise.
 """
 
 from __future__ import annotations
@@ -229,7 +234,7 @@ def test_borntm_unbuilt_parts_raise(cuda_device):
     c = _case(cuda_device)
     eps = c["eps"].clone().requires_grad_()
     deps = c["deps"].clone().requires_grad_()
-    r = _borntm(c, deps, c["dsig"], eps=eps)[-1]
+    r = _borntm(c, deps, c["dsig"], eps=eps, storage_mode="cpu")[-1]
     with pytest.raises(NotImplementedError, match="second"):
         (r * c["w"]).sum().backward()
     with pytest.raises(NotImplementedError, match="checkpoint"):
@@ -308,3 +313,79 @@ def test_tangent_pass_direction_batches(cuda_device):
         assert torch.equal(rb[:, k * S:(k + 1) * S], r1)
         assert torch.equal(tb[0][k * S:(k + 1) * S], t1[0])
     assert float(rb.abs().max()) > 0
+
+
+# ------------------------------------------------------------ second order
+@pytest.mark.parametrize("stencil", [2, 4, 6])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("k", [1, 2])
+def test_born_bggrad_bitwise_vs_oracle(cuda_device, stencil, dtype, k):
+    from oracle_harness import Oracle
+
+    dev = cuda_device
+    pb = random_problem(900 + stencil + k, 31, 43, 3, 36, stencil=stencil, pml=6, k=k,
+                        dtype=dtype)
+    d = _perturbation(pb, 19, dev)
+    n_store = (pb.nt + k - 1) // k
+    q = clone_problem(pb, dev)
+    snaps = _history(q, 0, dtype, n_store)
+    shape = (n_store, q.n_shots, q.ny, q.nx)
+    scat = [torch.zeros(shape, device=dev, dtype=dtype) for _ in range(2)]
+    _born(q, d, snaps, direct=tuple(t.data_ptr() for t in scat))
+    g = torch.Generator().manual_seed(29)
+    grad_r = torch.randn((pb.nt, pb.n_shots, pb.n_rec), generator=g, dtype=torch.float64).to(dtype)
+    grad_bg = torch.randn((pb.nt, pb.n_shots, pb.n_rec), generator=g, dtype=torch.float64).to(dtype)
+    got = bn._born_bggrad_call(q, tuple(d), grad_r.to(dev), grad_bg.to(dev), snaps, scat)
+    torch.cuda.synchronize()
+    # oracle: the same Born forward with the four histories, then the joint adjoint
+    op = clone_problem(pb)
+    tan = [torch.zeros_like(t) for t in op.fields]
+    r = torch.zeros((op.nt, op.n_shots, op.n_rec), dtype=dtype)
+    bg = torch.zeros_like(r)
+    st = [torch.zeros(shape, dtype=dtype) for _ in range(4)]
+    dc = [t.cpu() for t in d]
+    o = Oracle()
+    o.born_forward(op, dc[0], dc[1], op.f, dc[2], tan, r, bg, store=st, k=k)
+    for a, b in zip((snaps.ey_dev, snaps.curl_dev, *scat), st):
+        assert torch.equal(a.cpu(), b)
+    gca, gcb, gdca, gdcb, gf0, gdf, _, _ = o.born_bggrad(op, dc[0], dc[1], grad_r, grad_bg, st, k=k)
+    n = pb.nt * pb.n_shots * pb.n_src
+    pairs = (("dca", got[0], gdca), ("dcb", got[1], gdcb), ("df", got[2], gdf.reshape(-1)[:n]),
+             ("ca", got[3], gca), ("cb", got[4], gcb), ("f0", got[5], gf0.reshape(-1)[:n]))
+    for name, a, b in pairs:
+        a = a.cpu().reshape(b.shape)
+        assert float(b.abs().max()) > 0, name
+        assert rel_l2(a, b) <= 1e-5, (name, rel_l2(a, b))
+        assert torch.equal(a, b), (name, rel_l2(a, b))
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+def test_borntm_second_order_gradient_vs_reference_golden(cuda_device, stencil):
+    """borntm with the background and the direction all requiring gradients
+    (FP64): the gradients of <w, scattered> + <wb, background> receivers in
+    epsilon, sigma, depsilon and dsigma against the reference Python path's
+    autograd (golden born_bggrad.npz) to 1e-9."""
+    import numpy as np
+
+    from cases import hetero_inputs
+    from conftest import GOLDEN
+
+    z = np.load(GOLDEN / "born_bggrad.npz")
+    dev = cuda_device
+    c = hetero_inputs(torch.float64)
+    eps = c["eps"].to(dev).requires_grad_(True)
+    sig = c["sig"].to(dev).requires_grad_(True)
+    deps = torch.from_numpy(z["deps"]).to(dev).requires_grad_(True)
+    dsig = torch.from_numpy(z["dsig"]).to(dev).requires_grad_(True)
+    rec = c["rec"].to(dev)
+    out = tide.borntm(eps, sig, c["mu"].to(dev), c["dx"], c["dt"], c["amp"].to(dev),
+                      c["src"].to(dev), rec, rec, depsilon=deps, dsigma=dsig, stencil=stencil,
+                      pml_width=c["pml"])
+    bg, r = out[-2], out[-1]
+    tag = f"s{stencil}"
+    assert rel_l2(r.detach().cpu(), torch.from_numpy(z[f"r_{tag}"])) < 1e-13
+    w, wb = torch.from_numpy(z[f"w_{tag}"]).to(dev), torch.from_numpy(z[f"wb_{tag}"]).to(dev)
+    ((r * w).sum() + (bg * wb).sum()).backward()
+    for name, t in (("geps", eps), ("gsig", sig), ("gdeps", deps), ("gdsig", dsig)):
+        err = rel_l2(t.grad.cpu(), torch.from_numpy(z[f"{name}_{tag}"]))
+        assert err < 1e-9, (name, err)

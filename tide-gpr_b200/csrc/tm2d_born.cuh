@@ -344,6 +344,194 @@ void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
   TB_CUDA(cudaFreeAsync(scratch, st));
 }
 
+// ------------------------------------------- second-order Born adjoint
+// Derivative of the scattered (and background) receivers in the background
+// model, the perturbation and both source terms: the exact adjoint of the
+// joint recurrence.  lam is the scattered state's adjoint (driven by grad_r),
+// eta the background's (driven by grad_background_r and by the scattered
+// update's dependence on the background, dEy' += dca Ey + dcb curlH).  Per
+// step, with lam and eta at t+1: W = cb eta + dcb lam (the curl-H adjoint's
+// source of the background) and eta_Ey <- ca eta + dca lam (k_bg_prep); the
+// E- and H-phase adjoints of lam (cb, ca) and of eta (W in place of cb eta,
+// unit ca); receivers and sources as two ordinary adjoints; at stored steps,
+// step-major in this order: grad_ca += eta Ey + lam dEy, grad_cb += eta curl
+// + lam dcurl, grad_dca += lam Ey, grad_dcb += lam curl (times k).
+
+template <typename T>
+__global__ void k_fill(T *__restrict__ p, int64_t n, T v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// W and the ca / dca part of eta_Ey on the update domain of every shot.
+template <typename T>
+__global__ void k_bg_prep(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
+                          const T *__restrict__ dca, const T *__restrict__ dcb,
+                          const T *__restrict__ lam, T *__restrict__ eta, T *__restrict__ w,
+                          int p) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int s = blockIdx.z;
+  if (x < p || x >= g.nx - p + 1 || y < p || y >= g.ny - p + 1) return;
+  const int64_t j = (int64_t)y * g.nx + x, i = (int64_t)s * g.N + j;
+  const T cav = g.ca_b ? ca[i] : ca[j], dcav = g.ca_b ? dca[i] : dca[j];
+  const T cbv = g.cb_b ? cb[i] : cb[j], dcbv = g.cb_b ? dcb[i] : dcb[j];
+  const T l = lam[i], e = eta[i];
+  w[i] = cbv * e + dcbv * l;
+  eta[i] = cav * e + dcav * l;
+}
+
+// Step-major image of lam against the background history into the gradients
+// of the perturbation: grad_dca[j] += sum_s lam Ey^t k, grad_dcb likewise
+// with curl H^t (per shot when batched); snapshot shot s % bg_shots.
+template <typename T, typename S>
+__global__ void k_image_bg(TMGeom<T> g, const T *__restrict__ lam, const S *__restrict__ e_st,
+                           const S *__restrict__ c_st, T *__restrict__ gdca,
+                           T *__restrict__ gdcb, T kscale, int bg_shots, int p) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x < p || x >= g.nx - p + 1 || y < p || y >= g.ny - p + 1) return;
+  const int64_t j = (int64_t)y * g.nx + x;
+  T sa = 0, sb = 0;
+  for (int s = 0; s < g.n_shots; ++s) {
+    const int64_t i = (int64_t)s * g.N + j, k = (int64_t)(s % bg_shots) * g.N + j;
+    const T v = lam[i];
+    const T ta = v * Codec<S, T>::dec(e_st[k]) * kscale;
+    const T tb = v * Codec<S, T>::dec(c_st[k]) * kscale;
+    if (g.ca_b) gdca[i] = gdca[i] + ta;
+    else sa = sa + ta;
+    if (g.cb_b) gdcb[i] = gdcb[i] + tb;
+    else sb = sb + tb;
+  }
+  if (!g.ca_b) gdca[j] = gdca[j] + sa;
+  if (!g.cb_b) gdcb[j] = gdcb[j] + sb;
+}
+
+template <typename T, int ST>
+void tm_born_backward_bggrad(TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {
+  (void)f0; (void)df; (void)ey_store_3; (void)ey_filenames; (void)curl_store_3;
+  (void)curl_filenames; (void)lambda_store; (void)eta_source_old; (void)work_eta_z;
+  (void)grad_ca_shot; (void)grad_cb_shot; (void)grad_dca_shot; (void)grad_dcb_shot; (void)dt;
+  (void)n_threads; (void)storage_stream;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1 && start_t - nt >= 0,
+             "TM2D born_backward_bggrad: bad nt/step_ratio/start_t");
+  TB_REQUIRE(storage_mode == 0, "TM2D born_backward_bggrad: device storage mode only");
+  TB_REQUIRE(ca_requires_grad && cb_requires_grad,
+             "TM2D born_backward_bggrad: needs both the Ey and the curl H history");
+  TB_REQUIRE(!capture_background_adjoint && !reuse_background_adjoint,
+             "TM2D born_backward_bggrad: capturing or reusing the background adjoint is not "
+             "built");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && ey && hx && hz && dey && dhx && dhz &&
+                 m_lambda_ey_x && m_lambda_ey_z && m_lambda_hx_z && m_lambda_hz_x &&
+                 m_eta_ey_x && m_eta_ey_z && m_eta_hx_z && m_eta_hz_x && work_eta_x &&
+                 adjoint_memory_scratch && grad_ca && grad_cb && grad_dca && grad_dcb,
+             "TM2D born_backward_bggrad: a field, memory, gradient or scratch pointer is null");
+  TB_REQUIRE(ey_store_1 && curl_store_1 && dey_store && dcurl_store,
+             "TM2D born_backward_bggrad: background and scattered histories are required");
+  TB_REQUIRE(background_n_shots >= 1 && n_shots % background_n_shots == 0,
+             "TM2D born_backward_bggrad: n_shots must be a multiple of background_n_shots");
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "TM2D: bf16 snapshot storage requires float32 fields");
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  TB_REQUIRE(shot_bytes_uncomp == ny * nx * (int64_t)esz,
+             "TM2D born_backward_bggrad: shot_bytes_uncomp does not match ny*nx*elem");
+  Launch<T, ST> L;
+  if (!make_launch(L, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh, rdy, rdx, n_shots,
+                   ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
+    return;
+  if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
+  cudaStream_t st = as_stream(compute_stream);
+  const size_t SN = (size_t)n_shots * (size_t)L.g.N;
+  const int bg = (int)background_n_shots;
+  // the caller's adjoint state starts at zero (maxwell_tm_cuda_inst.cu:2963-2987)
+  for (T *p : {ey, hx, hz, dey, dhx, dhz, m_lambda_ey_x, m_lambda_ey_z, m_lambda_hx_z,
+               m_lambda_hz_x, m_eta_ey_x, m_eta_ey_z, m_eta_hx_z, m_eta_hz_x, work_eta_x})
+    if (TB_CUDA(cudaMemsetAsync(p, 0, SN * sizeof(T), st))) return;
+  if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, 8 * SN * sizeof(T), st))) return;
+  // unit coefficients standing for ca / cb in eta's phases (the kernels form
+  // 1 * value exactly); per shot when the coefficients are batched
+  T *ones = nullptr;
+  const size_t n_ones = (ca_batched || cb_batched) ? SN : (size_t)L.g.N;
+  if (TB_CUDA(pool_malloc((void **)&ones, n_ones * sizeof(T), st))) return;
+  k_fill<T><<<592, 256, 0, st>>>(ones, (int64_t)n_ones, (T)1);
+  PointScratch ps;
+  if (!build_points(ps, L, L.ah_tiles(), sources_i, n_sources_per_shot, receivers_i,
+                    n_receivers_per_shot, st))
+    return;
+  T *lc[4] = {m_lambda_ey_x, m_lambda_ey_z, m_lambda_hx_z, m_lambda_hz_x};
+  T *ln[4], *ec[4] = {m_eta_ey_x, m_eta_ey_z, m_eta_hx_z, m_eta_hz_x}, *en[4];
+  for (int m = 0; m < 4; ++m) {
+    ln[m] = adjoint_memory_scratch + m * SN;
+    en[m] = adjoint_memory_scratch + (4 + m) * SN;
+  }
+  T *w = work_eta_x;
+  const int p = FD<ST>::P;
+  const dim3 pblk(128, 1, 1), pgrid((unsigned)((nx + 127) / 128), (unsigned)ny, (unsigned)n_shots);
+  const dim3 igrid((unsigned)((nx + 127) / 128), (unsigned)ny, 1);
+  const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
+  const size_t bstep = (size_t)shot_bytes_uncomp * (size_t)bg;       // background history step
+  const size_t sstep = (size_t)shot_bytes_uncomp * (size_t)n_shots;  // scattered history step
+  int64_t launches = 1;
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    k_bg_prep<T><<<pgrid, pblk, 0, st>>>(L.g, ca, cb, dca, dcb, ey, dey, w, p);
+    if (L.has_domain) {
+      launch_adj_e<T, ST>(L, st, cb, ey, hx, hz, lc[2], lc[3], ln[2], ln[3]);
+      launch_adj_e<T, ST>(L, st, ones, w, dhx, dhz, ec[2], ec[3], en[2], en[3]);
+    }
+    for (int m = 2; m < 4; ++m) {
+      std::swap(lc[m], ln[m]);
+      std::swap(ec[m], en[m]);
+    }
+    const bool grad_step = t % step_ratio == 0;
+    const int64_t q = t / step_ratio;
+    const char *es = grad_step ? (const char *)ey_store_1 + (size_t)q * bstep : nullptr;
+    const char *cs = grad_step ? (const char *)curl_store_1 + (size_t)q * bstep : nullptr;
+    const char *des = grad_step ? (const char *)dey_store + (size_t)q * sstep : nullptr;
+    const char *dcs = grad_step ? (const char *)dcurl_store + (size_t)q * sstep : nullptr;
+    const T *gbr = grad_background_r ? grad_background_r + t * rs : nullptr;
+    const T *grt = grad_r ? grad_r + t * rs : nullptr;
+    T *gf0 = grad_f0 ? grad_f0 + t * fs : nullptr;
+    T *gdf = grad_df ? grad_df + t * fs : nullptr;
+    auto both_h = [&](auto tag) {
+      using SN_T = decltype(tag);
+      GradArgs<T, SN_T> ge{(const SN_T *)es, (const SN_T *)cs, grad_ca, grad_cb,
+                           (T)step_ratio, ca_batched, cb_batched, bg};
+      launch_adj_h<T, ST, SN_T>(L, st, ones, cq, dhx, dhz, dey, ec[0], ec[1], en[0], en[1], ps,
+                                gbr, gf0, ge);
+      GradArgs<T, SN_T> gl{(const SN_T *)des, (const SN_T *)dcs, grad_ca, grad_cb,
+                           (T)step_ratio, ca_batched, cb_batched, 0};
+      launch_adj_h<T, ST, SN_T>(L, st, ca, cq, hx, hz, ey, lc[0], lc[1], ln[0], ln[1], ps, grt,
+                                gdf, gl);
+      if (grad_step)
+        k_image_bg<T, SN_T><<<igrid, pblk, 0, st>>>(L.g, ey, (const SN_T *)es, (const SN_T *)cs,
+                                                    grad_dca, grad_dcb, (T)step_ratio, bg, p);
+    };
+    if (bf16) both_h(__nv_bfloat16(0.f));
+    else both_h(T(0));
+    for (int m = 0; m < 2; ++m) {
+      std::swap(lc[m], ln[m]);
+      std::swap(ec[m], en[m]);
+    }
+    launches += 3 + (L.has_domain ? 2 : 0) + (grad_step ? 1 : 0);
+  }
+  // leave the final memories in the caller's arrays
+  const size_t nb = SN * sizeof(T);
+  if (lc[0] != m_lambda_ey_x)
+    for (int m = 0; m < 4; ++m) {
+      T *dst[2] = {m == 0 ? m_lambda_ey_x : m == 1 ? m_lambda_ey_z : m == 2 ? m_lambda_hx_z
+                                                                            : m_lambda_hz_x,
+                   m == 0 ? m_eta_ey_x : m == 1 ? m_eta_ey_z : m == 2 ? m_eta_hx_z : m_eta_hz_x};
+      if (TB_CUDA(cudaMemcpyAsync(dst[0], lc[m], nb, cudaMemcpyDeviceToDevice, st)) ||
+          TB_CUDA(cudaMemcpyAsync(dst[1], ec[m], nb, cudaMemcpyDeviceToDevice, st)))
+        return;
+    }
+  count_launches(launches);
+  TB_CUDA(cudaFreeAsync(ones, st));
+  TB_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 }  // namespace tb
 
@@ -389,6 +577,22 @@ void tm_born_backward(TIDE_TM_BORN_BACKWARD_ARGS(T)) {
         n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
         ca_requires_grad, cb_requires_grad, ca_batched, cb_batched, cq_batched, start_t,      \
         pml_y0, pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);  \
+  }                                                                                    \
+  extern "C" void maxwell_tm_##S##_##T##_born_backward_bggrad_cuda(                   \
+      TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {                                          \
+    tb::tm_born_backward_bggrad<T, S>(                                                 \
+        ca, cb, cq, dca, dcb, f0, df, grad_r, grad_background_r, ey_store_1, ey_store_3,     \
+        ey_filenames, curl_store_1, curl_store_3, curl_filenames, dey_store, dcurl_store,     \
+        lambda_store, background_n_shots, ey, hx, hz, dey, dhx, dhz, grad_f0, grad_df,        \
+        grad_ca, grad_cb, grad_dca, grad_dcb, m_lambda_ey_x, m_lambda_ey_z, m_lambda_hx_z,    \
+        m_lambda_hz_x, m_eta_ey_x, m_eta_ey_z, m_eta_hx_z, m_eta_hz_x, eta_source_old,        \
+        work_eta_x, work_eta_z, grad_ca_shot, grad_cb_shot, grad_dca_shot, grad_dcb_shot,     \
+        adjoint_memory_scratch, ay, by, ayh, byh, ax, bx, axh, bxh, ky, kyh, kx, kxh,         \
+        sources_i, receivers_i, rdy, rdx, dt, nt, n_shots, ny, nx, n_sources_per_shot,        \
+        n_receivers_per_shot, step_ratio, storage_mode, storage_format, shot_bytes_uncomp,    \
+        ca_requires_grad, cb_requires_grad, capture_background_adjoint,                       \
+        reuse_background_adjoint, ca_batched, cb_batched, cq_batched, start_t, pml_y0,        \
+        pml_x0, pml_y1, pml_x1, n_threads, device, compute_stream, storage_stream);           \
   }
 
 TB_BORN_DEFINE(2, float)

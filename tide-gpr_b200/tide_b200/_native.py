@@ -71,6 +71,12 @@ SPECS: dict[str, list] = {
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6), (_P, 1), (_P, 2), (_P, 2),
         *_TM_PROFILES, *_TM_TAIL, *_TM_STORAGE, *_TM_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:407-440
+    "maxwell_tm_born_backward_bggrad": [
+        (_P, 3), (_P, 2), (_P, 2), (_P, 2), (_P, 6), (_P, 2), (_P, 1), (_I, 1), (_P, 3), (_P, 3),
+        (_P, 2), (_P, 2), (_P, 2), (_P, 15), (_P, 1), *_TM_PROFILES, *_TM_TAIL, *_TM_STORAGE,
+        (_B, 2), *_TM_FLAGS, (_P, 2),
+    ],
     # src/tide/backend_utils.py:310-334 (backward + background_n_shots)
     "maxwell_tm_background_vjp_reuse": [
         (_P, 3), (_P, 1), (_P, 3), (_P, 4), (_P, 1), (_P, 6), (_P, 1), (_P, 2), (_P, 2),
@@ -239,7 +245,7 @@ def exported_symbols() -> list[str]:
         for a in ACCURACIES
         for d in ("float", "double")
         for p in ("background_vjp_reuse", "born_forward", "born_forward_with_storage",
-                  "born_tangent_forward_with_storage", "born_backward")
+                  "born_tangent_forward_with_storage", "born_backward", "born_backward_bggrad")
     ] + [
         symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D

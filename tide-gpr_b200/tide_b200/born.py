@@ -146,6 +146,41 @@ def _born_backward_call(pb, grad_r, st, snaps, need_dca, need_dcb, side=None):
     nat.check("maxwell_tm born_backward")
 
 
+def _born_bggrad_call(pb, pert, grad_r, grad_bg_r, snaps, scattered):
+    """born_backward_bggrad over all nt steps: the gradients of
+    grad_r . scattered + grad_bg_r . background receivers in (dca, dcb, df,
+    ca, cb, f0), shaped like those inputs."""
+    dev, dt = pb.device, pb.dtype
+    S, ny, nx = pb.n_shots, pb.ny, pb.nx
+    dca, dcb, df = pert
+    full = lambda: torch.zeros((S, ny, nx), device=dev, dtype=dt)  # noqa: E731
+    lam, eta = [full() for _ in range(3)], [full() for _ in range(3)]
+    mem = [full() for _ in range(8)]
+    work = torch.empty((S, ny, nx), device=dev, dtype=dt)
+    scratch = torch.empty((8, S, ny, nx), device=dev, dtype=dt)
+    mshape = pb.ca.shape
+    g_ca, g_cb, g_dca, g_dcb = (torch.zeros(mshape, device=dev, dtype=dt) for _ in range(4))
+    n_src = pb.n_src if pb.f.numel() else 0
+    g_f0 = torch.zeros(pb.nt * S * n_src, device=dev, dtype=dt)
+    g_df = torch.zeros_like(g_f0)
+    empty_r = torch.zeros((pb.nt, S, pb.n_rec), device=dev, dtype=dt)
+    gr = grad_r.contiguous() if grad_r is not None and grad_r.numel() else empty_r
+    gb = grad_bg_r.contiguous() if grad_bg_r is not None and grad_bg_r.numel() else empty_r
+    fn = nat.get_backend_function("maxwell_tm", "born_backward_bggrad", pb.stencil, dt, dev)
+    fn(nat.ptr(pb.ca), nat.ptr(pb.cb), nat.ptr(pb.cq), nat.ptr(dca), nat.ptr(dcb),
+       nat.ptr(pb.f), nat.ptr(df), nat.ptr(gr), nat.ptr(gb), *_tm._snap_ptrs(snaps),
+       nat.ptr(scattered[0]), nat.ptr(scattered[1]), 0, S, *[nat.ptr(t) for t in lam],
+       *[nat.ptr(t) for t in eta], nat.ptr(g_f0), nat.ptr(g_df), nat.ptr(g_ca), nat.ptr(g_cb),
+       nat.ptr(g_dca), nat.ptr(g_dcb), *[nat.ptr(t) for t in mem], 0, nat.ptr(work), 0, 0, 0, 0,
+       0, nat.ptr(scratch), *_tm._profile_ptrs(pb), nat.ptr(pb.sources_i),
+       nat.ptr(pb.receivers_i), pb.rdy, pb.rdx, pb.dt, pb.nt, S, ny, nx, n_src, pb.n_rec,
+       pb.grad_interval, snaps.mode, snaps.fmt, snaps.shot_bytes, True, True, False, False,
+       pb.batched, pb.batched, pb.batched, pb.nt, pb.pml_y0, pb.pml_x0, pb.pml_y1, pb.pml_x1, 0,
+       dev.index or 0, _stream_handle(dev), 0)
+    nat.check("maxwell_tm born_backward_bggrad")
+    return g_dca, g_dcb, g_df, g_ca, g_cb, g_f0, None, None, None, None
+
+
 class BornPropagate(torch.autograd.Function):
     """Autograd node of the Born pass over the perturbation (dca, dcb, df) and
     the background (ca, cb, f0) (tm2d_born_autograd.py:38-1210).
@@ -161,6 +196,12 @@ class BornPropagate(torch.autograd.Function):
         dev, dtype = pb.device, pb.dtype
         need = tuple(t.requires_grad for t in (dca, dcb, df, ca, cb, f0))
         store_ey, store_curl = need[0] or need[3], need[1] or need[4]
+        # the background enters the scattered receivers too: with a background
+        # gradient wanted, both histories and the scattered ones are kept for
+        # the second-order adjoint (born_backward_bggrad, device mode)
+        second = need[3] or need[4] or need[5]
+        if second:
+            store_ey = store_curl = True
         r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=dev, dtype=dtype)
         bg_r = torch.zeros_like(r) if same_rec else torch.empty(0, device=dev, dtype=dtype)
         snaps = side = None
@@ -185,9 +226,16 @@ class BornPropagate(torch.autograd.Function):
             if mode in (stg.STORAGE_CPU, stg.STORAGE_DISK):
                 side = torch.cuda.Stream(dev)
                 snaps.keep.append(side)
+        direct, ctx.scattered = (0, 0), None
+        if second and snaps is not None and snaps.mode == stg.STORAGE_DEVICE:
+            shape = (snaps.ey_dev.shape[0], pb.n_shots, pb.ny, pb.nx)
+            ctx.scattered = [torch.empty(shape, device=dev, dtype=snaps.ey_dev.dtype)
+                             for _ in range(2)]
+            direct = tuple(nat.ptr(t) for t in ctx.scattered)
         _born_forward_call(pb, dca.detach(), dcb.detach(), df.detach(), f0.detach(), tan, r,
-                           bg_r, snaps, (store_ey, store_curl), side)
+                           bg_r, snaps, (store_ey, store_curl), side, direct)
         ctx.pb, ctx.snaps, ctx.side, ctx.need, ctx.opts = pb, snaps, side, need, opts
+        ctx.pert = (dca.detach(), dcb.detach(), df.detach())
         ctx.f0 = f0.detach()
         outs = (*pb.fields, *tan)
         for t in outs:
@@ -201,12 +249,16 @@ class BornPropagate(torch.autograd.Function):
         grad_bg_r, grad_r = grads[14], grads[15]
         nonzero = lambda g: g is not None and g.numel() > 0 and bool(g.count_nonzero())  # noqa: E731
         out = [None] * 10
-        if nonzero(grad_r):
-            if need_ca or need_cb or need_f0:
+        if nonzero(grad_r) and (need_ca or need_cb or need_f0):
+            if ctx.scattered is None:
                 raise NotImplementedError(
                     "the derivative of the Born receivers in the background model (second "
-                    "order, the reference's born_backward_bggrad) is not built; detach the "
-                    "background model or differentiate the background receivers")
+                    "order, born_backward_bggrad) needs the histories in device storage mode")
+            out = list(_born_bggrad_call(pb, ctx.pert, grad_r, grad_bg_r, snaps, ctx.scattered))
+            if not ctx.opts.get("retain_history"):
+                ctx.snaps = ctx.scattered = None
+            return tuple(out)
+        if nonzero(grad_r):
             if need_dca or need_dcb or need_df:
                 st = _tm._AdjointState(pb, need_dca, need_dcb, scratch=False)
                 _born_backward_call(pb, _tm._grad_r(pb, grad_r), st, snaps, need_dca, need_dcb,
