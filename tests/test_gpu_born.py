@@ -196,9 +196,35 @@ def test_unbuilt_linearization_parts_raise(cuda_device):
     op, model, v = _operator(cuda_device)
     lin = op.linearize(model)
     with pytest.raises(NotImplementedError):
-        lin.second_vjp(v, torch.zeros_like(lin.primal.receiver_data))
-    with pytest.raises(NotImplementedError):
         lin.jvp(tide.EMDirection(mu=torch.ones_like(model.mu)))
+    with pytest.raises(NotImplementedError):
+        lin.second_vjp(tide.EMDirection(mu=torch.ones_like(model.mu)),
+                       torch.zeros_like(lin.primal.receiver_data))
+
+
+def test_second_vjp_matches_central_difference_of_jvp(cuda_device):
+    """<second_vjp(v, w), u> = d/ds <w, J(m + s u) v> at s = 0: the
+    second-order Born adjoint against a central difference of the Born jvp
+    (FP64)."""
+    op, model, v = _operator(cuda_device, stencil=2)
+    lin = op.linearize(model)
+    w = torch.randn(lin.primal.receiver_data.shape, generator=torch.Generator().manual_seed(4),
+                    dtype=torch.float64).to(cuda_device)
+    g = lin.second_vjp(v, w)
+    gu = torch.Generator().manual_seed(6)
+    u_eps = 0.2 * torch.randn(model.epsilon.shape, generator=gu, dtype=torch.float64)
+    u_sig = 1e-3 * torch.randn(model.sigma.shape, generator=gu, dtype=torch.float64)
+    u_eps, u_sig = u_eps.to(cuda_device), u_sig.to(cuda_device)
+    analytic = float((g.epsilon * u_eps).sum() + (g.sigma * u_sig).sum())
+    h = 1e-4
+
+    def jw(s):
+        m = tide.EMModel(model.epsilon + s * u_eps, model.sigma + s * u_sig, model.mu)
+        return float((op.linearize(m).jvp(v).receiver_data * w).sum())
+
+    fd = (jw(h) - jw(-h)) / (2 * h)
+    assert abs(fd) > 0
+    assert abs(analytic - fd) <= 1e-6 * abs(fd), (analytic, fd)
 
 
 # ---------------------------------------------------------------------- 3-D

@@ -407,9 +407,32 @@ class LinearizedMaxwellTM:
 
     def second_vjp(self, direction: EMDirection, cotangent: torch.Tensor) -> EMGradient:
         """Gradient of <cotangent, J(model) direction> with respect to the
-        model: needs the Born adjoint with background gradients, which this
-        build does not have."""
-        raise NotImplementedError("second_vjp (Born adjoint) is not built in tide_b200.")
+        linearization targets (linearization.py:125-146): a Born pass at the
+        differentiable background, back-propagated through the second-order
+        Born adjoint (born_backward_bggrad; device storage)."""
+        direction.validate_for(self.model)
+        if direction.mu is not None:
+            raise NotImplementedError("TM2D tangent propagation for mu is not available.")
+        from .born import borntm
+
+        op = self.operator
+        d, e = op.discretization, op.experiment
+        res = borntm(
+            self._inputs["epsilon"], self._inputs["sigma"], self.model.mu.detach(),
+            grid_spacing=d.spacing, dt=d.dt, source_amplitude=e.source_amplitude,
+            source_location=e.acquisition.source_location,
+            receiver_location=e.acquisition.receiver_location,
+            depsilon=direction.epsilon, dsigma=direction.sigma, stencil=d.stencil,
+            pml_width=d.boundary.width, max_vel=d.max_velocity, nt=e.nt,
+            model_gradient_sampling_interval=op.model_gradient_sampling_interval,
+        )
+        r = res[-1]
+        if cotangent.shape != r.shape:
+            raise ValueError("The cotangent's shape differs from the tangent receiver data's.")
+        ins = [self._inputs[t] for t in self.targets]
+        grads = torch.autograd.grad(r, ins, grad_outputs=cotangent, allow_unused=True)
+        g = dict(zip(self.targets, grads))
+        return EMGradient(epsilon=g.get("epsilon"), sigma=g.get("sigma"))
 
 
 class Maxwell3D:
