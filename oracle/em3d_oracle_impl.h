@@ -647,6 +647,119 @@ void FN(tide_oracle_em3d_backward)(const REAL *ca, const REAL *cb, const REAL *c
   free(gcb_s);
 }
 
+/* One stored step's coefficient-gradient term of the fields F[0..2] against
+ * the three snapshot histories st[0..2] (slot byte offset off), into grad
+ * (batched), grad[j] (one shot) or the per-shot buffer shot (several shots). */
+static void FN(image3)(const FN(g3) * g, REAL *const F[3], void *const st[3], size_t off,
+                       int fmt, REAL kscale, REAL *grad, REAL *shot, int batched) {
+  for (int64_t s = 0; s < g->S; ++s)
+    for (int64_t z = g->P; z < g->nz - g->P + 1; ++z)
+      for (int64_t y = g->P; y < g->ny - g->P + 1; ++y)
+        for (int64_t x = g->P; x < g->nx - g->P + 1; ++x) {
+          const int64_t i = FN(mi)(g, s, z, y, x), j = i - s * g->N;
+          const REAL acc = F[0][i] * FN(get)((const char *)st[0] + off, fmt, i) +
+                           F[1][i] * FN(get)((const char *)st[1] + off, fmt, i) +
+                           F[2][i] * FN(get)((const char *)st[2] + off, fmt, i);
+          const REAL sc = acc * kscale;
+          if (batched) grad[i] = grad[i] + sc;
+          else if (g->S == 1) grad[j] = grad[j] + sc;
+          else shot[i] = shot[i] + sc;
+        }
+}
+
+/* Second-order Born adjoint, 3-D (the reference's born_backward_bggrad,
+ * maxwell_3d_cuda_inst.cu:5262-5900, in the formulation of the TM2D oracle):
+ * lam (L, 6 fields + 12 memories) is the scattered state's adjoint driven by
+ * grad_r, eta (E) the background's, driven by the scattered update's
+ * dependence on the background: per step W = cb eta_E + dcb lam_E and
+ * eta_E <- ca eta_E + dca lam_E on the update domain, the adjoint phases of
+ * lam (cb, ca) and of eta (W for the E-phase input, unit ca), receivers
+ * grad_r -> lam, sources grad_df <- lam and grad_f0 <- eta, then at stored
+ * steps grad_ca += eta.E + lam.dE, grad_cb += eta.curl + lam.dcurl,
+ * grad_dca += lam.E, grad_dcb += lam.curl (times k; per-shot buffers summed
+ * over shots at the end).  store: background E x3, curl x3; dstore: the
+ * scattered ones; full-layout memories. */
+void FN(tide_oracle_em3d_born_bggrad)(
+    const REAL *ca, const REAL *cb, const REAL *cq, const REAL *dca, const REAL *dcb,
+    const REAL *grad_r, REAL **L, REAL **lmem, REAL **E, REAL **emem, void **store,
+    void **dstore, REAL *grad_f0, REAL *grad_df, REAL *grad_ca, REAL *grad_cb, REAL *grad_dca,
+    REAL *grad_dcb, const REAL **prof, const int64_t *src_i, const int64_t *rec_i, REAL rdz,
+    REAL rdy, REAL rdx, int64_t nt, int64_t S, int64_t nz, int64_t ny, int64_t nx, int64_t n_src,
+    int64_t n_rec, int64_t k, int fmt, int64_t start_t, const int64_t *pml, int ca_b, int cb_b,
+    int cq_b, int src_comp, int rec_comp) {
+  FN(g3) g;
+  FN(setup)(&g, prof, rdz, rdy, rdx, S, nz, ny, nx, pml, ca_b, cb_b, cq_b);
+  const int64_t tot = S * g.N;
+  REAL *scratch = (REAL *)calloc((size_t)(24 * tot), sizeof(REAL));
+  REAL *ones = (REAL *)malloc((size_t)tot * sizeof(REAL));
+  REAL *w = (REAL *)calloc((size_t)(3 * tot), sizeof(REAL));
+  for (int64_t i = 0; i < tot; ++i) ones[i] = (REAL)1;
+  REAL *lc[12], *ln[12], *ec[12], *en[12];
+  for (int m = 0; m < 12; ++m) {
+    lc[m] = lmem[m];
+    ln[m] = scratch + m * tot;
+    ec[m] = emem[m];
+    en[m] = scratch + (12 + m) * tot;
+  }
+  REAL *WE[6] = {w, w + tot, w + 2 * tot, E[3], E[4], E[5]};
+  const int sh_a = !ca_b && S > 1, sh_b = !cb_b && S > 1;
+  REAL *shot[4];
+  for (int q = 0; q < 4; ++q)
+    shot[q] = ((q % 2 == 0) ? sh_a : sh_b) ? (REAL *)calloc((size_t)tot, sizeof(REAL)) : 0;
+  const size_t esz = fmt ? 2 : sizeof(REAL);
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    for (int64_t s = 0; s < S; ++s)
+      for (int64_t z = g.P; z < nz - g.P + 1; ++z)
+        for (int64_t y = g.P; y < ny - g.P + 1; ++y)
+          for (int64_t x = g.P; x < nx - g.P + 1; ++x) {
+            const int64_t i = FN(mi)(&g, s, z, y, x), j = i - s * g.N;
+            const REAL a = ca[ca_b ? i : j], da = dca[ca_b ? i : j];
+            const REAL b = cb[cb_b ? i : j], db = dcb[cb_b ? i : j];
+            for (int c = 0; c < 3; ++c) {
+              WE[c][i] = b * E[c][i] + db * L[c][i];
+              E[c][i] = a * E[c][i] + da * L[c][i];
+            }
+          }
+    FN(adj_e)(&g, cb, L, lc, ln);
+    FN(adj_e)(&g, ones, WE, ec, en);
+    FN(adj_h)(&g, ones, cq, E, ec, en);
+    if (n_src > 0 && grad_f0 && src_i) FN(record)(grad_f0 + t * S * n_src, E[src_comp], src_i, S, n_src, g.N);
+    FN(adj_h)(&g, ca, cq, L, lc, ln);
+    if (n_rec > 0 && grad_r && rec_i) FN(inject)(L[rec_comp], grad_r + t * S * n_rec, rec_i, S, n_rec, g.N);
+    if (n_src > 0 && grad_df && src_i) FN(record)(grad_df + t * S * n_src, L[src_comp], src_i, S, n_src, g.N);
+    for (int m = 0; m < 12; ++m) {
+      REAL *tmp = lc[m]; lc[m] = ln[m]; ln[m] = tmp;
+      tmp = ec[m]; ec[m] = en[m]; en[m] = tmp;
+    }
+    if (k > 0 && t % k == 0) {
+      const size_t off = (size_t)(t / k) * (size_t)tot * esz;
+      FN(image3)(&g, E, store, off, fmt, (REAL)k, grad_ca, shot[0], ca_b);
+      FN(image3)(&g, E, store + 3, off, fmt, (REAL)k, grad_cb, shot[1], cb_b);
+      FN(image3)(&g, L, dstore, off, fmt, (REAL)k, grad_ca, shot[0], ca_b);
+      FN(image3)(&g, L, dstore + 3, off, fmt, (REAL)k, grad_cb, shot[1], cb_b);
+      FN(image3)(&g, L, store, off, fmt, (REAL)k, grad_dca, shot[2], ca_b);
+      FN(image3)(&g, L, store + 3, off, fmt, (REAL)k, grad_dcb, shot[3], cb_b);
+    }
+  }
+  for (int m = 0; m < 12; ++m) {
+    if (lc[m] != lmem[m]) memcpy(lmem[m], lc[m], (size_t)tot * sizeof(REAL));
+    if (ec[m] != emem[m]) memcpy(emem[m], ec[m], (size_t)tot * sizeof(REAL));
+  }
+  REAL *outs[4] = {grad_ca, grad_cb, grad_dca, grad_dcb};
+  for (int q = 0; q < 4; ++q) {
+    if (!shot[q]) continue;
+    for (int64_t j = 0; j < g.N; ++j) {
+      REAL sum = 0;
+      for (int64_t s = 0; s < S; ++s) sum = sum + shot[q][s * g.N + j];
+      outs[q][j] = outs[q][j] + sum;
+    }
+    free(shot[q]);
+  }
+  free(scratch);
+  free(ones);
+  free(w);
+}
+
 #undef FN
 #undef CAT2
 #undef CAT2_

@@ -11,7 +11,9 @@ em3d_case.npz and a seeded smooth (depsilon, dsigma) direction, stencils 2
 and 4; then back-propagates a seeded linear functional of the scattered
 receivers to depsilon and dsigma with torch autograd.  Stored: the
 direction, the functional's weights, the scattered receivers and the two
-gradients per stencil.
+gradients per stencil (born3d_grad.npz); and, with the background epsilon /
+sigma requiring gradients as well, the four gradients of a second seeded
+functional at stencil 2 (born3d_bggrad.npz, the second-order Born pin).
 """
 
 from __future__ import annotations
@@ -66,6 +68,27 @@ def main():
         out[f"dt_s{stencil}"] = dt
         print(stencil, float(r.abs().max()), float(de.grad.abs().max()), float(ds.grad.abs().max()))
     np.savez_compressed(HERE / "born3d_grad.npz", **out)
+
+    # second order: the background epsilon / sigma require gradients too
+    sec = {}
+    for stencil in (2,):
+        dt = float(z["dt"])
+        e_ = eps.clone().requires_grad_(True)
+        s_ = sig.clone().requires_grad_(True)
+        de = deps.clone().requires_grad_(True)
+        ds = dsig.clone().requires_grad_(True)
+        res = born3d(e_, s_, mu, float(z["dx"]), dt, amp, src, rec, depsilon=de, dsigma=ds,
+                     stencil=stencil, pml_width=int(z["pml"]), python_backend=True,
+                     fallback="error")
+        r = res[-1]
+        w = torch.randn(r.shape, generator=torch.Generator().manual_seed(31), dtype=r.dtype)
+        (r * w).sum().backward()
+        tag = f"s{stencil}"
+        sec.update({f"w_{tag}": w.numpy(), f"r_{tag}": r.detach().numpy(),
+                    f"geps_{tag}": e_.grad.numpy(), f"gsig_{tag}": s_.grad.numpy(),
+                    f"gdeps_{tag}": de.grad.numpy(), f"gdsig_{tag}": ds.grad.numpy()})
+        print("second order", stencil, {k: float(np.abs(v).max()) for k, v in sec.items()})
+    np.savez_compressed(HERE / "born3d_bggrad.npz", **sec)
 
 
 if __name__ == "__main__":

@@ -333,6 +333,34 @@ class Oracle3D:
         return out + ((geps, gsig) if eps_sigma else ())
 
 
+def _oracle3d_born_bggrad(o, pb, dca, dcb, grad_r, store, dstore, k=1, fmt=0):
+    """3-D second-order Born adjoint on the oracle (full-layout state);
+    returns grad_ca, grad_cb, grad_dca, grad_dcb (model-shaped), grad_f0 and
+    grad_df ([nt, S, n_src])."""
+    S, nz, ny, nx, dt = pb.n_shots, pb.nz, pb.ny, pb.nx, pb.dtype
+    z = lambda *s: torch.zeros(s, dtype=dt)  # noqa: E731
+    L = [z(S, nz, ny, nx) for _ in range(6)]
+    lm = [z(S, nz, ny, nx) for _ in range(12)]
+    E = [z(S, nz, ny, nx) for _ in range(6)]
+    em = [z(S, nz, ny, nx) for _ in range(12)]
+    mshape = (S, nz, ny, nx) if pb.batched else (nz, ny, nx)
+    g = [z(*mshape) for _ in range(4)]
+    gf0, gdf = z(pb.nt, S, max(pb.n_src, 1)), z(pb.nt, S, max(pb.n_src, 1))
+    fn, F = o._fn("born_bggrad", dt, pb.stencil)
+    P, I = c_void_p, c_int64
+    fn.argtypes = ([P] * 6 + [P] * 4 + [P, P] + [P] * 6 + [P, P, P] + [F, F, F] + [I] * 8
+                   + [c_int, I, P] + [c_int] * 5)
+    prof = _ptr_array([pb.profiles[n].cpu() for n in PROFILES_3D])
+    pml = (c_int64 * 6)(*pb.pml)
+    fn(_p(pb.ca), _p(pb.cb), _p(pb.cq.cpu()), _p(dca), _p(dcb), _p(grad_r), _ptr_array(L),
+       _ptr_array(lm), _ptr_array(E), _ptr_array(em), _ptr_array(list(store)),
+       _ptr_array(list(dstore)), _p(gf0), _p(gdf), *[_p(t) for t in g], prof,
+       _p(pb.sources_i.cpu()), _p(pb.receivers_i.cpu()), pb.rdz, pb.rdy, pb.rdx, pb.nt, S, nz,
+       ny, nx, pb.n_src, pb.n_rec, k, fmt, pb.nt, pml, int(pb.batched), int(pb.batched),
+       int(pb.batched), pb.src_comp, pb.rec_comp)
+    return (*g, gf0, gdf)
+
+
 class OracleEM3D(torch.autograd.Function):
     """Autograd node over (ca, cb, f) backed by the 3-D C oracle (CPU)."""
 
