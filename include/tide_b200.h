@@ -546,11 +546,62 @@ TIDE_3D_DECLARE(8, double)
       int64_t receiver_component, int64_t n_threads, int64_t device,           \
       int64_t execution_backend, void *compute_stream, void *storage_stream
 
+/* maxwell_3d_*_born_backward_bggrad_cuda.  Replaces
+ * maxwell_3d_{S}_{dtype}_born_backward_bggrad_cuda,
+ * src/tide/csrc/em3d/maxwell_3d_cuda_inst.cu:5262-5900 (argtypes
+ * src/tide/backend_utils.py:635-671): the derivative of grad_r . (scattered
+ * receivers) in the background coefficients (grad_ca, grad_cb), the
+ * perturbation (grad_dca, grad_dcb) and both sources (grad_f0, grad_df), by
+ * the exact adjoint of the joint background + scattered recurrence over the
+ * background (s1) and scattered (dex_store ..) histories of
+ * born_forward_with_storage, device storage mode.  lambda_* receive the
+ * scattered state's adjoint, eta_* the background's (fields and full-size
+ * memories, zeroed on entry); adjoint_memory_scratch holds 24 and
+ * eta_source_e* one n_shots nz ny nx array each; gradients accumulate, per
+ * shot into grad_*_shot (zeroed here) when several unbatched shots share the
+ * model, then summed in shot order. */
+#define TIDE_3D_BORN_BACKWARD_BGGRAD_ARGS(T)                                   \
+  T const *ca, T const *cb, T const *cq, T const *dca, T const *dcb,           \
+      T const *f0, T const *df, T const *grad_r, T *lambda_ex, T *lambda_ey,   \
+      T *lambda_ez, T *lambda_hx, T *lambda_hy, T *lambda_hz,                  \
+      T *m_lambda_ey_z, T *m_lambda_ez_y, T *m_lambda_ez_x, T *m_lambda_ex_z,  \
+      T *m_lambda_ex_y, T *m_lambda_ey_x, T *m_lambda_hz_y, T *m_lambda_hy_z,  \
+      T *m_lambda_hx_z, T *m_lambda_hz_x, T *m_lambda_hy_x, T *m_lambda_hx_y,  \
+      T *eta_ex, T *eta_ey, T *eta_ez, T *eta_hx, T *eta_hy, T *eta_hz,        \
+      T *m_eta_ey_z, T *m_eta_ez_y, T *m_eta_ez_x, T *m_eta_ex_z,              \
+      T *m_eta_ex_y, T *m_eta_ey_x, T *m_eta_hz_y, T *m_eta_hy_z,              \
+      T *m_eta_hx_z, T *m_eta_hz_x, T *m_eta_hy_x, T *m_eta_hx_y,              \
+      T *adjoint_memory_scratch, void *ex_s1, void *ex_s3, void *ex_fn,        \
+      void *ey_s1, void *ey_s3, void *ey_fn, void *ez_s1, void *ez_s3,         \
+      void *ez_fn, void *cx_s1, void *cx_s3, void *cx_fn, void *cy_s1,         \
+      void *cy_s3, void *cy_fn, void *cz_s1, void *cz_s3, void *cz_fn,         \
+      void *dex_store, void *dey_store, void *dez_store, void *dcurl_x_store,  \
+      void *dcurl_y_store, void *dcurl_z_store, T *grad_f0, T *grad_df,        \
+      T *grad_ca, T *grad_cb, T *grad_dca, T *grad_dcb, T *grad_ca_shot,       \
+      T *grad_cb_shot, T *grad_dca_shot, T *grad_dcb_shot, T *eta_source_ex,   \
+      T *eta_source_ey, T *eta_source_ez, T const *az, T const *bz,            \
+      T const *azh, T const *bzh, T const *ay, T const *by, T const *ayh,      \
+      T const *byh, T const *ax, T const *bx, T const *axh, T const *bxh,      \
+      T const *kz, T const *kzh, T const *ky, T const *kyh, T const *kx,       \
+      T const *kxh, int64_t const *sources_i, int64_t const *receivers_i,      \
+      T rdz, T rdy, T rdx, T dt, int64_t nt, int64_t n_shots, int64_t nz,      \
+      int64_t ny, int64_t nx, int64_t n_sources_per_shot,                      \
+      int64_t n_receivers_per_shot, int64_t step_ratio, int64_t storage_mode,  \
+      int64_t storage_format, int64_t shot_bytes_uncomp, bool ca_requires_grad, \
+      bool cb_requires_grad, bool dca_requires_grad, bool dcb_requires_grad,   \
+      bool ca_batched, bool cb_batched, bool cq_batched, int64_t start_t,      \
+      int64_t pml_z0, int64_t pml_y0, int64_t pml_x0, int64_t pml_z1,          \
+      int64_t pml_y1, int64_t pml_x1, int64_t source_component,                \
+      int64_t receiver_component, int64_t n_threads, int64_t device,           \
+      int64_t execution_backend, void *compute_stream, void *storage_stream
+
 #define TIDE_3D_BORN_DECLARE(S, T)                                              \
   void maxwell_3d_##S##_##T##_born_forward_cuda(TIDE_3D_BORN_FORWARD_ARGS(T)); \
   void maxwell_3d_##S##_##T##_born_forward_with_storage_cuda(                   \
       TIDE_3D_BORN_FORWARD_WITH_STORAGE_ARGS(T));                               \
-  void maxwell_3d_##S##_##T##_born_backward_cuda(TIDE_3D_BORN_BACKWARD_ARGS(T));
+  void maxwell_3d_##S##_##T##_born_backward_cuda(TIDE_3D_BORN_BACKWARD_ARGS(T));  \
+  void maxwell_3d_##S##_##T##_born_backward_bggrad_cuda(                        \
+      TIDE_3D_BORN_BACKWARD_BGGRAD_ARGS(T));
 TIDE_3D_BORN_DECLARE(2, float)
 TIDE_3D_BORN_DECLARE(2, double)
 TIDE_3D_BORN_DECLARE(4, float)

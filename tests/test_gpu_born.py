@@ -490,3 +490,98 @@ def test_born3d_public_api_gradient_vs_reference_golden(cuda_device, stencil):
     assert rel_l2(deps.grad.cpu(), torch.from_numpy(g[f"geps_s{stencil}"])) < 1e-9
     assert rel_l2(dsig.grad.cpu(), torch.from_numpy(g[f"gsig_s{stencil}"])) < 1e-9
     assert nat.device_status(dev) == 0
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("k", [1, 2])
+def test_born3d_bggrad_bitwise_vs_oracle(cuda_device, stencil, dtype, k):
+    """maxwell_3d_*_born_backward_bggrad over born_forward_with_storage's
+    background and scattered histories equals the oracle's 3-D joint adjoint:
+    gradients in ca, cb, dca, dcb and both sources, and the adjoint state."""
+    from oracle_harness import Oracle3D, _oracle3d_born_bggrad
+    from test_born_oracle import _case3d, _perturbation3d
+
+    from tide_b200 import em3d
+
+    dev = cuda_device
+    pb = _case3d(dtype, ("ez", "ey"), stencil=stencil)
+    pb.grad_interval = k
+    dca, dcb, df = _perturbation3d(pb, 23)
+    q, r, _, st, shot_bytes = _born3d_store_cuda(pb, dca, dcb, df, dev, k, 0)
+    S, shape = q.n_shots, (q.n_shots, q.nz, q.ny, q.nx)
+    grad_r = torch.randn((pb.nt, S, pb.n_rec), generator=torch.Generator().manual_seed(7),
+                         dtype=dtype)
+    z = lambda: torch.zeros(shape, device=dev, dtype=dtype)  # noqa: E731
+    lam, lmem, eta, emem = [z() for _ in range(6)], [z() for _ in range(12)], \
+        [z() for _ in range(6)], [z() for _ in range(12)]
+    scratch = torch.empty((24, *shape), device=dev, dtype=dtype)
+    work = [z() for _ in range(3)]
+    mshape = (q.nz, q.ny, q.nx)
+    g = [torch.zeros(mshape, device=dev, dtype=dtype) for _ in range(4)]
+    gs = [torch.empty(shape, device=dev, dtype=dtype) for _ in range(4)]
+    gf0 = torch.zeros(pb.nt * S * q.n_src, device=dev, dtype=dtype)
+    gdf = torch.zeros_like(gf0)
+    fn = nat.get_backend_function("maxwell_3d", "born_backward_bggrad", q.stencil, dtype, dev)
+    p = nat.ptr
+    s18 = []
+    for c in range(6):
+        s18 += [p(st[c]), 0, 0]
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    d = [t.to(dev) for t in (dca, dcb, df)]
+    fn(p(q.ca), p(q.cb), p(q.cq), p(d[0]), p(d[1]), p(q.f), p(d[2]), p(grad_r.to(dev)),
+       *[p(t) for t in lam], *[p(t) for t in lmem], *[p(t) for t in eta], *[p(t) for t in emem],
+       p(scratch), *s18, *[p(st[6 + c]) for c in range(6)], p(gf0), p(gdf), *[p(t) for t in g],
+       *[p(t) for t in gs], *[p(t) for t in work], *em3d._profile_ptrs(q), p(q.sources_i),
+       p(q.receivers_i), q.rdz, q.rdy, q.rdx, q.dt, q.nt, S, q.nz, q.ny, q.nx, q.n_src, q.n_rec,
+       k, 0, 0, shot_bytes, True, True, True, True, q.batched, q.batched, q.batched, q.nt,
+       *q.pml, q.src_comp, q.rec_comp, 0, dev.index or 0, 0, stream, stream)
+    nat.check("born_backward_bggrad 3-D")
+    torch.cuda.synchronize()
+    # oracle: Born forward with the 12 histories, then the joint adjoint
+    F, M = Oracle3D.full_state(pb)
+    DF, DM = [torch.zeros_like(t) for t in F], [torch.zeros_like(t) for t in M]
+    r_o = torch.zeros((pb.nt, S, pb.n_rec), dtype=dtype)
+    bg_o = torch.zeros_like(r_o)
+    st_o = [torch.zeros(t.shape, dtype=t.dtype) for t in st]
+    o = Oracle3D()
+    o.born_forward(pb, dca, dcb, pb.f, df, F, M, DF, DM, r_o, bg_o, store=st_o, k=k)
+    for c in range(12):
+        assert torch.equal(st[c].cpu(), st_o[c]), f"history {c}"
+    gca, gcb, gdca, gdcb, of0, odf = _oracle3d_born_bggrad(o, pb, dca, dcb, grad_r, st_o[:6],
+                                                           st_o[6:], k=k)
+    n = pb.nt * S * pb.n_src
+    for name, a, b in (("ca", g[0], gca), ("cb", g[1], gcb), ("dca", g[2], gdca),
+                       ("dcb", g[3], gdcb), ("f0", gf0, of0.reshape(-1)[:n]),
+                       ("df", gdf, odf.reshape(-1)[:n])):
+        assert float(b.abs().max()) > 0, name
+        _same(a.reshape(b.shape), b, f"grad {name}")
+    assert nat.device_status(dev) == 0
+
+
+def test_born3d_second_order_gradient_vs_reference_golden(cuda_device):
+    """born3d with the background and the direction all requiring gradients
+    (FP64, stencil 2): the gradients of <w, scattered receivers> in epsilon,
+    sigma, depsilon and dsigma against the reference Python path's autograd
+    (born3d_bggrad.npz) to 1e-9."""
+    from tide_b200 import em3d
+
+    z = np.load(GOLDEN / "em3d_case.npz")
+    g = np.load(GOLDEN / "born3d_grad.npz")
+    h = np.load(GOLDEN / "born3d_bggrad.npz")
+    dev = cuda_device
+    eps = torch.from_numpy(z["eps"]).to(dev).requires_grad_(True)
+    sig = torch.from_numpy(z["sig"]).to(dev).requires_grad_(True)
+    deps = torch.from_numpy(g["deps"]).to(dev).requires_grad_(True)
+    dsig = torch.from_numpy(g["dsig"]).to(dev).requires_grad_(True)
+    out = em3d.born3d(eps, sig, torch.from_numpy(z["mu"]).to(dev), float(z["dx"]), float(z["dt"]),
+                      torch.from_numpy(z["amp"]).to(dev), torch.from_numpy(z["src"]).to(dev),
+                      torch.from_numpy(z["rec"]).to(dev), depsilon=deps, dsigma=dsig,
+                      stencil=2, pml_width=int(z["pml"]))
+    r = out[-1]
+    assert rel_l2(r.detach().cpu(), torch.from_numpy(h["r_s2"])) < 1e-13
+    (r * torch.from_numpy(h["w_s2"]).to(dev)).sum().backward()
+    for name, t in (("geps", eps), ("gsig", sig), ("gdeps", deps), ("gdsig", dsig)):
+        err = rel_l2(t.grad.cpu(), torch.from_numpy(h[f"{name}_s2"]))
+        assert err < 1e-9, (name, err)
+    assert nat.device_status(dev) == 0

@@ -957,6 +957,13 @@ __global__ void k3_combine(T *__restrict__ grad, T *__restrict__ shot, int S, in
   }
 }
 
+template <typename T>
+__global__ void k3_fill(T *__restrict__ p, int64_t n, T v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
 // d/d(eps_r), d/d(sigma) from d/d(ca), d/d(cb) (maxwell_3d_inst.cpp:376-445).
 template <typename T>
 __global__ void k3_convert(const T *__restrict__ ca, const T *__restrict__ cb,
@@ -1573,6 +1580,218 @@ void em3d_born_forward(TIDE_3D_BORN_FORWARD_ARGS(T), const BornStore *bs = nullp
   TB_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------- second-order Born adjoint
+// The 3-D joint adjoint of the background and scattered recurrences (see the
+// 2-D version in tm2d_born.cuh): lam = the scattered state's adjoint (driven
+// by grad_r), eta = the background's.  Per step, with both at t+1:
+// W = cb eta_E + dcb lam_E and eta_E <- ca eta_E + dca lam_E (k3_bg_prep),
+// the adjoint phases of lam (cb, ca) and of eta (W as the E-phase input,
+// unit ca), sources grad_f0 <- eta and grad_df <- lam, receivers grad_r ->
+// lam; at stored steps grad_ca += eta.E + lam.dE, grad_cb += eta.curl +
+// lam.dcurl, grad_dca += lam.E, grad_dcb += lam.curl (times k), per shot
+// when several unbatched shots share the model, summed at the end.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k3_bg_prep(G3<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
+           const T *__restrict__ dca, const T *__restrict__ dcb, const T *__restrict__ lex,
+           const T *__restrict__ ley, const T *__restrict__ lez, T *__restrict__ eex,
+           T *__restrict__ eey, T *__restrict__ eez, T *__restrict__ w0, T *__restrict__ w1,
+           T *__restrict__ w2) {
+  Col c;
+  if (!column(g, c)) return;
+  const int64_t base = (int64_t)c.s * g.N;
+  const T *L[3] = {lex + base, ley + base, lez + base};
+  T *E[3] = {eex + base, eey + base, eez + base}, *W[3] = {w0 + base, w1 + base, w2 + base};
+  if (g.ca_b) { ca += base; dca += base; }
+  if (g.cb_b) { cb += base; dcb += base; }
+  for (int z = c.zb; z < c.ze; ++z) {
+    const int64_t j = ((int64_t)z * g.ny + c.y) * g.nx + c.x;
+    const T a = ld(ca + j), da = ld(dca + j), b = ld(cb + j), db = ld(dcb + j);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const T l = L[k][j], e = E[k][j];
+      W[k][j] = b * e + db * l;
+      E[k][j] = a * e + da * l;
+    }
+  }
+}
+
+template <typename T, int ST>
+void em3d_born_backward_bggrad(TIDE_3D_BORN_BACKWARD_BGGRAD_ARGS(T)) {
+  (void)f0; (void)df; (void)n_threads; (void)storage_stream; (void)dt;
+  (void)ex_s3; (void)ex_fn; (void)ey_s3; (void)ey_fn; (void)ez_s3; (void)ez_fn;
+  (void)cx_s3; (void)cx_fn; (void)cy_s3; (void)cy_fn; (void)cz_s3; (void)cz_fn;
+  if (TB_CUDA(cudaSetDevice((int)device))) return;
+  TB_REQUIRE(nt >= 0 && step_ratio >= 1 && start_t - nt >= 0,
+             "3-D born_backward_bggrad: bad nt/step_ratio/start_t");
+  TB_REQUIRE(storage_mode == 0, "3-D born_backward_bggrad: device storage mode only");
+  T *lam[6] = {lambda_ex, lambda_ey, lambda_ez, lambda_hx, lambda_hy, lambda_hz};
+  T *eta[6] = {eta_ex, eta_ey, eta_ez, eta_hx, eta_hy, eta_hz};
+  T *lm[12] = {m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,
+               m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z,
+               m_lambda_hx_z, m_lambda_hz_x, m_lambda_hy_x, m_lambda_hx_y};
+  T *em[12] = {m_eta_ey_z, m_eta_ez_y, m_eta_ez_x, m_eta_ex_z, m_eta_ex_y, m_eta_ey_x,
+               m_eta_hz_y, m_eta_hy_z, m_eta_hx_z, m_eta_hz_x, m_eta_hy_x, m_eta_hx_y};
+  for (int k = 0; k < 6; ++k)
+    TB_REQUIRE(lam[k] && eta[k], "3-D born_backward_bggrad: an adjoint field is null");
+  for (int k = 0; k < 12; ++k)
+    TB_REQUIRE(lm[k] && em[k], "3-D born_backward_bggrad: an adjoint memory is null");
+  TB_REQUIRE(ca && cb && cq && dca && dcb && adjoint_memory_scratch && eta_source_ex &&
+                 eta_source_ey && eta_source_ez,
+             "3-D born_backward_bggrad: a coefficient, scratch or work pointer is null");
+  if (!common_checks<T>("3-D born_backward_bggrad", 0, nullptr, 0, nullptr, source_component,
+                        receiver_component, execution_backend))
+    return;
+  const bool bf16 = storage_format == 1;
+  TB_REQUIRE(!bf16 || sizeof(T) == 4, "3-D: bf16 snapshot storage requires float32 fields");
+  const size_t esz = bf16 ? 2 : sizeof(T);
+  TB_REQUIRE(shot_bytes_uncomp == nz * ny * nx * (int64_t)esz,
+             "3-D born_backward_bggrad: shot_bytes_uncomp does not match nz*ny*nx*elem");
+  const bool need[4] = {ca_requires_grad && grad_ca, cb_requires_grad && grad_cb,
+                        dca_requires_grad && grad_dca, dcb_requires_grad && grad_dcb};
+  void *bg_st[6] = {ex_s1, ey_s1, ez_s1, cx_s1, cy_s1, cz_s1};
+  void *sc_st[6] = {dex_store, dey_store, dez_store, dcurl_x_store, dcurl_y_store,
+                    dcurl_z_store};
+  for (int k = 0; k < 6; ++k) {
+    const bool e = k < 3;
+    TB_REQUIRE(!((e ? need[0] || need[2] : need[1] || need[3]) && !bg_st[k]),
+               "3-D born_backward_bggrad: background history %d missing", k);
+    TB_REQUIRE(!((e ? need[0] : need[1]) && !sc_st[k]),
+               "3-D born_backward_bggrad: scattered history %d missing", k);
+  }
+  const T *prof[kNProf] = {az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh, bxh,
+                           kz, kzh, ky, kyh, kx, kxh};
+  Launch3<T> L;
+  if (!make3(L, ST, prof, rdz, rdy, rdx, n_shots, nz, ny, nx, pml_z0, pml_y0, pml_x0, pml_z1,
+             pml_y1, pml_x1, ca_batched, cb_batched, cq_batched, /*compact=*/false))
+    return;
+  const G3<T> &g = L.g;
+  cudaStream_t st = stream_of(compute_stream);
+  const int64_t tot = n_shots * g.N;
+  const size_t tb = sizeof(T) * (size_t)tot;
+  for (int k = 0; k < 6; ++k)
+    if (TB_CUDA(cudaMemsetAsync(lam[k], 0, tb, st)) || TB_CUDA(cudaMemsetAsync(eta[k], 0, tb, st)))
+      return;
+  for (int k = 0; k < 12; ++k)
+    if (TB_CUDA(cudaMemsetAsync(lm[k], 0, tb, st)) || TB_CUDA(cudaMemsetAsync(em[k], 0, tb, st)))
+      return;
+  if (TB_CUDA(cudaMemsetAsync(adjoint_memory_scratch, 0, 24 * tb, st))) return;
+  T *wf[3] = {eta_source_ex, eta_source_ey, eta_source_ez};
+  for (int k = 0; k < 3; ++k)
+    if (TB_CUDA(cudaMemsetAsync(wf[k], 0, tb, st))) return;
+  const bool shots = n_shots > 1;
+  T *gout[4] = {grad_ca, grad_cb, grad_dca, grad_dcb};
+  T *gshot[4] = {grad_ca_shot, grad_cb_shot, grad_dca_shot, grad_dcb_shot};
+  const bool batched_of[4] = {ca_batched, cb_batched, ca_batched, cb_batched};
+  for (int q = 0; q < 4; ++q)
+    if (need[q] && shots && !batched_of[q]) {
+      TB_REQUIRE(gshot[q], "3-D born_backward_bggrad: per-shot gradient buffer %d missing", q);
+      if (TB_CUDA(cudaMemsetAsync(gshot[q], 0, tb, st))) return;
+    }
+  T *ones = nullptr;
+  if (TB_CUDA(pool_malloc((void **)&ones, tb, st))) return;
+  k3_fill<T><<<592, 256, 0, st>>>(ones, tot, (T)1);
+  Mem12<T> lc, ln, ec, en;
+  for (int m = 0; m < 12; ++m) {
+    lc.m[m] = lm[m];
+    ln.m[m] = adjoint_memory_scratch + m * tot;
+    ec.m[m] = em[m];
+    en.m[m] = adjoint_memory_scratch + (12 + m) * tot;
+  }
+  const GradFold<T, T> off{};
+  auto adj_e = [&](const T *b, T *const F[6], Mem12<T> c, Mem12<T> n) {
+    if constexpr (ST == 2)
+      k3_adj_e<T, T><<<L.grid, L.block, 0, st>>>(g, b, F[0], F[1], F[2], F[3], F[4], F[5], c, n,
+                                                 off);
+    else
+      k3p_adj_e<T, T, ST / 2><<<L.grid, L.block, 0, st>>>(g, b, F[0], F[1], F[2], F[3], F[4],
+                                                          F[5], c, n, off);
+  };
+  auto adj_h = [&](const T *a, T *const F[6], Mem12<T> c, Mem12<T> n) {
+    if constexpr (ST == 2)
+      k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, a, cq, F[3], F[4], F[5], F[0], F[1], F[2], c, n);
+    else
+      k3p_adj_h<T, ST / 2><<<L.grid, L.block, 0, st>>>(g, a, cq, F[3], F[4], F[5], F[0], F[1],
+                                                       F[2], c, n);
+  };
+  auto image = [&](T *const F[6], void *const s6[6], size_t off_b, T *ga, T *gb, T *gas,
+                   T *gbs, bool na, bool nb) {
+    if (!na && !nb) return;
+    const char *p[6];
+    for (int k = 0; k < 6; ++k) p[k] = (k < 3 ? na : nb) ? (const char *)s6[k] + off_b : nullptr;
+    if (bf16)
+      k3_coeff_grad<T, __nv_bfloat16><<<L.grid, L.block, 0, st>>>(
+          g, F[0], F[1], F[2], (const __nv_bfloat16 *)p[0], (const __nv_bfloat16 *)p[1],
+          (const __nv_bfloat16 *)p[2], (const __nv_bfloat16 *)p[3], (const __nv_bfloat16 *)p[4],
+          (const __nv_bfloat16 *)p[5], ga, gb, gas, gbs, (T)step_ratio);
+    else
+      k3_coeff_grad<T, T><<<L.grid, L.block, 0, st>>>(
+          g, F[0], F[1], F[2], (const T *)p[0], (const T *)p[1], (const T *)p[2],
+          (const T *)p[3], (const T *)p[4], (const T *)p[5], ga, gb, gas, gbs, (T)step_ratio);
+  };
+  T *W6[6] = {wf[0], wf[1], wf[2], eta[3], eta[4], eta[5]};
+  const int S_ = (int)n_shots;
+  const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
+  int64_t launches = 1;
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
+    k3_bg_prep<T><<<L.grid, L.block, 0, st>>>(g, ca, cb, dca, dcb, lam[0], lam[1], lam[2], eta[0],
+                                              eta[1], eta[2], wf[0], wf[1], wf[2]);
+    adj_e(cb, lam, lc, ln);
+    adj_e(ones, W6, ec, en);
+    adj_h(ones, eta, ec, en);
+    if (n_sources_per_shot > 0 && grad_f0 && sources_i) {
+      const int n = S_ * (int)n_sources_per_shot;
+      k3_adj_points<T><<<(n + 127) / 128, 128, 0, st>>>(
+          nullptr, nullptr, nullptr, 0, field_of(eta[0], eta[1], eta[2], source_component),
+          grad_f0 + t * n_shots * n_sources_per_shot, sources_i, (int)n_sources_per_shot, S_,
+          g.N, 1);
+      ++launches;
+    }
+    adj_h(ca, lam, lc, ln);
+    if (n_receivers_per_shot > 0 && grad_r && receivers_i) {
+      k3_adj_points<T><<<(S_ + 127) / 128, 128, 0, st>>>(
+          field_of(lam[0], lam[1], lam[2], receiver_component),
+          grad_r + t * n_shots * n_receivers_per_shot, receivers_i, (int)n_receivers_per_shot,
+          nullptr, nullptr, nullptr, 0, S_, g.N, 0);
+      ++launches;
+    }
+    if (n_sources_per_shot > 0 && grad_df && sources_i) {
+      const int n = S_ * (int)n_sources_per_shot;
+      k3_adj_points<T><<<(n + 127) / 128, 128, 0, st>>>(
+          nullptr, nullptr, nullptr, 0, field_of(lam[0], lam[1], lam[2], source_component),
+          grad_df + t * n_shots * n_sources_per_shot, sources_i, (int)n_sources_per_shot, S_,
+          g.N, 1);
+      ++launches;
+    }
+    std::swap(lc, ln);
+    std::swap(ec, en);
+    launches += 5;
+    if (t % step_ratio == 0) {
+      const size_t ob = (size_t)(t / step_ratio) * step_bytes;
+      image(eta, bg_st, ob, gout[0], gout[1], gshot[0], gshot[1], need[0], need[1]);
+      image(lam, sc_st, ob, gout[0], gout[1], gshot[0], gshot[1], need[0], need[1]);
+      image(lam, bg_st, ob, gout[2], gout[3], gshot[2], gshot[3], need[2], need[3]);
+      launches += 3;
+    }
+  }
+  for (int m = 0; m < 12; ++m) {
+    if (lc.m[m] != lm[m] && TB_CUDA(cudaMemcpyAsync(lm[m], lc.m[m], tb, cudaMemcpyDeviceToDevice,
+                                                    st)))
+      return;
+    if (ec.m[m] != em[m] && TB_CUDA(cudaMemcpyAsync(em[m], ec.m[m], tb, cudaMemcpyDeviceToDevice,
+                                                    st)))
+      return;
+  }
+  for (int q = 0; q < 4; ++q)
+    if (need[q] && shots && !batched_of[q]) {
+      k3_combine<T><<<592, 256, 0, st>>>(gout[q], gshot[q], S_, g.N);
+      ++launches;
+    }
+  count_launches(launches);
+  TB_CUDA(cudaFreeAsync(ones, st));
+  TB_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 }  // namespace tb
 
@@ -1705,19 +1924,52 @@ TB3_DEFINE(8, double)
         storage_stream, /*compact=*/false);                                               \
   }
 
+#define TB3_BGGRAD_DEFINE(S, T)                                                            \
+  extern "C" void maxwell_3d_##S##_##T##_born_backward_bggrad_cuda(                        \
+      TIDE_3D_BORN_BACKWARD_BGGRAD_ARGS(T)) {                                              \
+    tb::em3d_born_backward_bggrad<T, S>(                                                   \
+        ca, cb, cq, dca, dcb, f0, df, grad_r, lambda_ex, lambda_ey, lambda_ez, lambda_hx,  \
+        lambda_hy, lambda_hz, m_lambda_ey_z, m_lambda_ez_y, m_lambda_ez_x, m_lambda_ex_z,  \
+        m_lambda_ex_y, m_lambda_ey_x, m_lambda_hz_y, m_lambda_hy_z, m_lambda_hx_z,         \
+        m_lambda_hz_x, m_lambda_hy_x, m_lambda_hx_y, eta_ex, eta_ey, eta_ez, eta_hx,       \
+        eta_hy, eta_hz, m_eta_ey_z, m_eta_ez_y, m_eta_ez_x, m_eta_ex_z, m_eta_ex_y,        \
+        m_eta_ey_x, m_eta_hz_y, m_eta_hy_z, m_eta_hx_z, m_eta_hz_x, m_eta_hy_x,            \
+        m_eta_hx_y, adjoint_memory_scratch, ex_s1, ex_s3, ex_fn, ey_s1, ey_s3, ey_fn,      \
+        ez_s1, ez_s3, ez_fn, cx_s1, cx_s3, cx_fn, cy_s1, cy_s3, cy_fn, cz_s1, cz_s3,       \
+        cz_fn, dex_store, dey_store, dez_store, dcurl_x_store, dcurl_y_store,              \
+        dcurl_z_store, grad_f0, grad_df, grad_ca, grad_cb, grad_dca, grad_dcb,             \
+        grad_ca_shot, grad_cb_shot, grad_dca_shot, grad_dcb_shot, eta_source_ex,           \
+        eta_source_ey, eta_source_ez, az, bz, azh, bzh, ay, by, ayh, byh, ax, bx, axh,     \
+        bxh, kz, kzh, ky, kyh, kx, kxh, sources_i, receivers_i, rdz, rdy, rdx, dt, nt,     \
+        n_shots, nz, ny, nx, n_sources_per_shot, n_receivers_per_shot, step_ratio,         \
+        storage_mode, storage_format, shot_bytes_uncomp, ca_requires_grad,                 \
+        cb_requires_grad, dca_requires_grad, dcb_requires_grad, ca_batched, cb_batched,    \
+        cq_batched, start_t, pml_z0, pml_y0, pml_x0, pml_z1, pml_y1, pml_x1,               \
+        source_component, receiver_component, n_threads, device, execution_backend,        \
+        compute_stream, storage_stream);                                                   \
+  }
+
 TB3_BORN_DEFINE(2, float)
 TB3_BORN_STORE_DEFINE(2, float)
+TB3_BGGRAD_DEFINE(2, float)
 TB3_BORN_DEFINE(2, double)
 TB3_BORN_STORE_DEFINE(2, double)
+TB3_BGGRAD_DEFINE(2, double)
 TB3_BORN_DEFINE(4, float)
 TB3_BORN_STORE_DEFINE(4, float)
+TB3_BGGRAD_DEFINE(4, float)
 TB3_BORN_DEFINE(4, double)
 TB3_BORN_STORE_DEFINE(4, double)
+TB3_BGGRAD_DEFINE(4, double)
 TB3_BORN_DEFINE(6, float)
 TB3_BORN_STORE_DEFINE(6, float)
+TB3_BGGRAD_DEFINE(6, float)
 TB3_BORN_DEFINE(6, double)
 TB3_BORN_STORE_DEFINE(6, double)
+TB3_BGGRAD_DEFINE(6, double)
 TB3_BORN_DEFINE(8, float)
 TB3_BORN_STORE_DEFINE(8, float)
+TB3_BGGRAD_DEFINE(8, float)
 TB3_BORN_DEFINE(8, double)
 TB3_BORN_STORE_DEFINE(8, double)
+TB3_BGGRAD_DEFINE(8, double)

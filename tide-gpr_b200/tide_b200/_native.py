@@ -115,6 +115,12 @@ SPECS.update({
         (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 2), (_P, 2),
         *_3D_PROFILES, *_3D_TAIL, *_3D_STORAGE, *_3D_FLAGS, (_P, 2),
     ],
+    # src/tide/backend_utils.py:635-671
+    "maxwell_3d_born_backward_bggrad": [
+        (_P, 3), (_P, 2), (_P, 2), (_P, 1), *_3D_FIELDS, (_P, 6), (_P, 12), (_P, 1), (_P, 18),
+        (_P, 6), (_P, 2), (_P, 4), (_P, 4), (_P, 3), *_3D_PROFILES, *_3D_TAIL, (_I, 3), (_B, 4),
+        *_3D_FLAGS, (_P, 2),
+    ],
     # src/tide/backend_utils.py:537-556
     "maxwell_3d_backward": [
         (_P, 3), (_P, 1), *_3D_FIELDS, (_P, 1), (_P, 18), (_P, 1), (_P, 4), (_P, 2), (_B, 1),
@@ -250,7 +256,8 @@ def exported_symbols() -> list[str]:
         symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D
         for d in ("float", "double")
-        for p in ("born_forward", "born_forward_with_storage", "born_backward")
+        for p in ("born_forward", "born_forward_with_storage", "born_backward",
+                  "born_backward_bggrad")
     ] + [
         symbol_name("maxwell_3d", p, a, d)
         for a in ACCURACIES_3D

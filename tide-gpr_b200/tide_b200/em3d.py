@@ -566,24 +566,32 @@ def maxwell3d(
 
 
 class Born3DPropagate(torch.autograd.Function):
-    """The Born map (dca, dcb, df) -> scattered receivers on the native 3-D
-    Born entry points: forward maxwell_3d_*_born_forward_with_storage (device
-    history of the background E^n / curl H^n, full CPML memories), backward
-    maxwell_3d_*_born_backward (the background adjoint imaging against that
-    history), as the reference's Born3DForwardFunc
-    (src/tide/maxwell/maxwell3d_born_autograd.py:17-1276) for the
-    perturbation.  The background and scattered states advance in place in
-    the call's tensors (call = the arguments of the native born_forward)."""
+    """The Born map (dca, dcb, df; ca, cb, f0) -> scattered receivers on the
+    native 3-D Born entry points, as the reference's Born3DForwardFunc
+    (src/tide/maxwell/maxwell3d_born_autograd.py:17-1276).  Forward:
+    maxwell_3d_*_born_forward_with_storage (device history of the background
+    E^n / curl H^n and, when the background needs a gradient, of the
+    scattered E^n / curl; full CPML memories).  Backward:
+    maxwell_3d_*_born_backward (the background adjoint imaging against the
+    background history) for the perturbation alone, or
+    maxwell_3d_*_born_backward_bggrad (the joint background + scattered
+    adjoint) when the background (ca, cb, f0) needs a gradient.  The
+    background and scattered states advance in place in the call's tensors
+    (call = the arguments of the native born_forward)."""
 
     @staticmethod
-    def forward(ctx, dca_p, dcb_p, df, call):
+    def forward(ctx, dca_p, dcb_p, df, ca, cb, f0, call):
         pb, k = call["pb"], max(1, call["pb"].grad_interval)
-        need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        need = ctx.needs_input_grad
+        second = need[3] or need[4] or need[5]
+        need_ca, need_cb = need[0] or second, need[1] or second
         n_store = (pb.nt + k - 1) // k
         shape = (n_store, pb.n_shots, pb.nz, pb.ny, pb.nx)
         empty = torch.empty(0, device=pb.device, dtype=pb.dtype)
         st = [torch.empty(shape, device=pb.device, dtype=pb.dtype)
               if (need_ca if c < 3 else need_cb) else empty for c in range(6)]
+        sc = [torch.empty(shape, device=pb.device, dtype=pb.dtype) for _ in range(6)] if second \
+            else [empty] * 6
         s18 = []
         for t in st:
             s18 += [_p(t), 0, 0]
@@ -592,14 +600,15 @@ class Born3DPropagate(torch.autograd.Function):
                                       pb.dtype, pb.device)
         stream = torch.cuda.current_stream(pb.device).cuda_stream
         r = torch.zeros((pb.nt, pb.n_shots, pb.n_rec), device=pb.device, dtype=pb.dtype)
-        fn(*call["head"](dca_p, dcb_p, df, r), *s18, *[0] * 6, *_profile_ptrs(pb),
+        fn(*call["head"](dca_p, dcb_p, df, r), *s18, *[_p(t) for t in sc], *_profile_ptrs(pb),
            _p(pb.sources_i), _p(pb.receivers_i), pb.rdz, pb.rdy, pb.rdx, pb.dt, pb.nt,
            pb.n_shots, pb.nz, pb.ny, pb.nx, call["n_src"], pb.n_rec, k, 0, 0, shot_bytes,
            need_ca, need_cb, pb.batched, pb.batched, pb.batched, 0, *pb.pml, pb.src_comp,
            pb.rec_comp, 0, pb.device.index or 0, 0, stream, stream)
         nat.check("maxwell_3d born_forward_with_storage")
-        ctx.pb, ctx.st, ctx.k, ctx.shot_bytes = pb, st, k, shot_bytes
-        ctx.n_src, ctx.need_f = call["n_src"], ctx.needs_input_grad[2]
+        ctx.pb, ctx.st, ctx.sc, ctx.k, ctx.shot_bytes = pb, st, sc, k, shot_bytes
+        ctx.n_src, ctx.second = call["n_src"], second
+        ctx.pert = (dca_p.detach(), dcb_p.detach(), df.detach())
         return r
 
     @staticmethod
@@ -608,32 +617,54 @@ class Born3DPropagate(torch.autograd.Function):
         S = pb.n_shots
         full = (S, pb.nz, pb.ny, pb.nx)
         empty = torch.empty(0, device=dev, dtype=dt)
-        need_ca, need_cb = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
-        lam = [torch.zeros(full, device=dev, dtype=dt) for _ in range(6)]
-        lmem = [torch.zeros(full, device=dev, dtype=dt) for _ in range(12)]
-        scratch = torch.empty((12, *full), device=dev, dtype=dt)
+        need = ctx.needs_input_grad
+        z = lambda: torch.zeros(full, device=dev, dtype=dt)  # noqa: E731
         mshape = (1, pb.nz, pb.ny, pb.nx)
+        s18 = []
+        for t in ctx.st:
+            s18 += [_p(t), 0, 0]
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        nf = pb.nt * S * ctx.n_src
+        tail = [*_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i), pb.rdz, pb.rdy,
+                pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, ctx.n_src, pb.n_rec, ctx.k, 0, 0,
+                ctx.shot_bytes]
+        flags = [pb.batched, pb.batched, pb.batched, pb.nt, *pb.pml, pb.src_comp, pb.rec_comp, 0,
+                 dev.index or 0, 0, stream, stream]
+        if ctx.second:
+            g = [torch.zeros(mshape, device=dev, dtype=dt) for _ in range(4)]
+            gs = [torch.empty(full, device=dev, dtype=dt) if S > 1 else empty for _ in range(4)]
+            gf0 = torch.zeros(nf, device=dev, dtype=dt) if ctx.n_src > 0 else empty
+            gdf = torch.zeros(nf, device=dev, dtype=dt) if ctx.n_src > 0 else empty
+            dca, dcb, df = ctx.pert
+            fn = nat.get_backend_function("maxwell_3d", "born_backward_bggrad", pb.stencil, dt,
+                                          dev)
+            fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(pb.f), _p(df),
+               _p(grad_r.contiguous()), *[_p(z()) for _ in range(18)],
+               *[_p(z()) for _ in range(18)], _p(torch.empty((24, *full), device=dev, dtype=dt)),
+               *s18, *[_p(t) for t in ctx.sc], _p(gf0), _p(gdf), _p(g[2]), _p(g[3]), _p(g[0]),
+               _p(g[1]), *[_p(t) for t in gs], *[_p(z()) for _ in range(3)], *tail, True, True,
+               True, True, *flags)
+            nat.check("maxwell_3d born_backward_bggrad")
+            ctx.st = ctx.sc = None
+            return (g[0], g[1], gdf if ctx.n_src > 0 else None, g[2], g[3],
+                    gf0 if ctx.n_src > 0 else None, None)
+        need_ca, need_cb = need[0], need[1]
+        lam = [z() for _ in range(6)]
+        lmem = [z() for _ in range(12)]
+        scratch = torch.empty((12, *full), device=dev, dtype=dt)
         gca = torch.empty(mshape, device=dev, dtype=dt) if need_ca else empty
         gcb = torch.empty(mshape, device=dev, dtype=dt) if need_cb else empty
         gca_s = torch.empty(full, device=dev, dtype=dt) if need_ca and S > 1 else empty
         gcb_s = torch.empty(full, device=dev, dtype=dt) if need_cb and S > 1 else empty
-        gf = (torch.empty(pb.nt * S * ctx.n_src, device=dev, dtype=dt)
-              if ctx.need_f and ctx.n_src > 0 else empty)
-        s18 = []
-        for t in ctx.st:
-            s18 += [_p(t), 0, 0]
+        gf = torch.empty(nf, device=dev, dtype=dt) if need[2] and ctx.n_src > 0 else empty
         fn = nat.get_backend_function("maxwell_3d", "born_backward", pb.stencil, dt, dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
         fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(grad_r.contiguous()), *[_p(t) for t in lam],
            *[_p(t) for t in lmem], _p(scratch), *s18, _p(gf), _p(gca), _p(gcb), _p(gca_s),
-           _p(gcb_s), *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i), pb.rdz, pb.rdy,
-           pb.rdx, pb.dt, pb.nt, S, pb.nz, pb.ny, pb.nx, ctx.n_src, pb.n_rec, ctx.k, 0, 0,
-           ctx.shot_bytes, need_ca, need_cb, pb.batched, pb.batched, pb.batched, pb.nt, *pb.pml,
-           pb.src_comp, pb.rec_comp, 0, dev.index or 0, 0, stream, stream)
+           _p(gcb_s), *tail, need_ca, need_cb, *flags)
         nat.check("maxwell_3d born_backward")
         ctx.st = None
         return (gca if need_ca else None, gcb if need_cb else None,
-                gf if ctx.need_f and ctx.n_src > 0 else None, None)
+                gf if need[2] and ctx.n_src > 0 else None, None, None, None, None)
 
 
 def _born3d_prep(epsilon, sigma, mu, grid_spacing, dt, source_amplitude, source_location,
@@ -695,11 +726,16 @@ def born3d(
     names = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz") + MEM_NAMES
     bg_init = [state_and_unused.get(f"{n}_0") for n in names]
     sc_init = [state_and_unused.get(f"d{n}_0") for n in names]
-    epsilon, sigma, mu = epsilon.detach(), sigma.detach(), mu.detach()
+    mu = mu.detach()
     pert = (depsilon, dsigma) if parameterization == "epsilon_sigma" else (dca, dcb)
-    grad_on = torch.is_grad_enabled() and any(
-        t is not None and t.requires_grad for t in pert)
-    with torch.no_grad():
+    # the background model is differentiated (second order, through the joint
+    # adjoint) when it requires a gradient; otherwise it enters as values
+    bg_grad = torch.is_grad_enabled() and (epsilon.requires_grad or sigma.requires_grad)
+    if not bg_grad:
+        epsilon, sigma = epsilon.detach(), sigma.detach()
+    grad_on = bg_grad or (torch.is_grad_enabled() and any(
+        t is not None and t.requires_grad for t in pert))
+    with torch.set_grad_enabled(bg_grad):
         prep = _born3d_prep(epsilon, sigma, mu, grid_spacing, dt, source_amplitude,
                             source_location, receiver_location, stencil, pml_width, max_vel,
                             nt, model_gradient_sampling_interval, source_component,
@@ -750,7 +786,9 @@ def born3d(
                 *[_p(t) for t in sc_fields], *[_p(t) for t in sc_mem], _p(rr), _p(bg_r))
 
     if grad_on:
-        r = Born3DPropagate.apply(dca_p, dcb_p, df, {"pb": pb, "head": head, "n_src": n_src})
+        f0 = pb.f if n_src > 0 else torch.empty(0, device=dev, dtype=dtype)
+        r = Born3DPropagate.apply(dca_p, dcb_p, df, pb.ca, pb.cb, f0,
+                                  {"pb": pb, "head": head, "n_src": n_src})
     else:
         fn = nat.get_backend_function("maxwell_3d", "born_forward", pb.stencil, dtype, dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
