@@ -585,3 +585,25 @@ def test_born3d_second_order_gradient_vs_reference_golden(cuda_device):
         err = rel_l2(t.grad.cpu(), torch.from_numpy(h[f"{name}_s2"]))
         assert err < 1e-9, (name, err)
     assert nat.device_status(dev) == 0
+
+
+def test_maxwell3d_second_vjp_matches_central_difference_of_jvp(cuda_device):
+    """3-D: <second_vjp(v, w), u> = d/ds <w, J(m + s u) v> at s = 0 (FP64)."""
+    op, model, v = _operator3d(cuda_device)
+    lin = op.linearize(model)
+    w = torch.randn(lin.primal.receiver_data.shape, generator=torch.Generator().manual_seed(8),
+                    dtype=torch.float64).to(cuda_device)
+    g = lin.second_vjp(v, w)
+    gu = torch.Generator().manual_seed(10)
+    u_eps = (0.2 * torch.randn(model.epsilon.shape, generator=gu, dtype=torch.float64)).to(cuda_device)
+    u_sig = (1e-3 * torch.randn(model.sigma.shape, generator=gu, dtype=torch.float64)).to(cuda_device)
+    analytic = float((g.epsilon * u_eps).sum() + (g.sigma * u_sig).sum())
+    h = 1e-4
+
+    def jw(s):
+        m = tide.EMModel(model.epsilon + s * u_eps, model.sigma + s * u_sig, model.mu)
+        return float((op.linearize(m).jvp(v).receiver_data * w).sum())
+
+    fd = (jw(h) - jw(-h)) / (2 * h)
+    assert abs(fd) > 0
+    assert abs(analytic - fd) <= 1e-6 * abs(fd), (analytic, fd)

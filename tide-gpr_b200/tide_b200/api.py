@@ -524,17 +524,38 @@ class LinearizedMaxwell3D(LinearizedMaxwellTM):
         direction.validate_for(self.model)
         if direction.mu is not None:
             raise NotImplementedError("3-D tangent propagation for mu is not available.")
+        # the background enters as values; a direction that requires grad is
+        # differentiated through the Born pass
+        res = self._born(self.model.epsilon.detach(), self.model.sigma.detach(), direction,
+                         bg_receivers=True)
+        return TangentResult(res[-1], EM3DState.from_tensors(res[18:36]))
+
+    def _born(self, eps, sig, direction: EMDirection, bg_receivers: bool = False):
         op = self.operator
         d, e = op.discretization, op.experiment
-        res = em3d.born3d(
-            self.model.epsilon, self.model.sigma, self.model.mu, grid_spacing=d.spacing,
+        return em3d.born3d(
+            eps, sig, self.model.mu, grid_spacing=d.spacing,
             dt=d.dt, source_amplitude=e.source_amplitude,
             source_location=e.acquisition.source_location,
             receiver_location=e.acquisition.receiver_location,
-            bg_receiver_location=e.acquisition.receiver_location,
+            bg_receiver_location=e.acquisition.receiver_location if bg_receivers else None,
             depsilon=direction.epsilon, dsigma=direction.sigma, stencil=d.stencil,
             pml_width=d.boundary.width, max_vel=d.max_velocity, nt=e.nt,
             model_gradient_sampling_interval=op.model_gradient_sampling_interval,
             source_component=e.source_component, receiver_component=e.receiver_component,
         )
-        return TangentResult(res[-1], EM3DState.from_tensors(res[18:36]))
+
+    def second_vjp(self, direction: EMDirection, cotangent: torch.Tensor) -> EMGradient:
+        """Gradient of <cotangent, J(model) direction> with respect to the
+        linearization targets (linearization.py:125-146) through the 3-D
+        second-order Born adjoint (born_backward_bggrad)."""
+        direction.validate_for(self.model)
+        if direction.mu is not None:
+            raise NotImplementedError("3-D tangent propagation for mu is not available.")
+        r = self._born(self._inputs["epsilon"], self._inputs["sigma"], direction)[-1]
+        if cotangent.shape != r.shape:
+            raise ValueError("The cotangent's shape differs from the tangent receiver data's.")
+        ins = [self._inputs[t] for t in self.targets]
+        grads = torch.autograd.grad(r, ins, grad_outputs=cotangent, allow_unused=True)
+        g = dict(zip(self.targets, grads))
+        return EMGradient(epsilon=g.get("epsilon"), sigma=g.get("sigma"))
