@@ -373,7 +373,12 @@ def run_b200(args) -> None:
         serving = serve_bench(args)
     sweep = None
     if rank == 0 and world == 1 and args.serve_sweep_jobs > 0:
-        sweep = serve_sweep(args)
+        try:
+            sweep = serve_sweep(args)
+        except nat.NativeError as exc:  # reported in the line; the other legs still run
+            sweep = {"error": str(exc)}
+            torch.cuda.synchronize(dev)
+            torch.cuda.empty_cache()
     if rank == 0 and world == 1 and args.em3d_nt > 0:
         em3d_leg = em3d_bench(args)
     if rank == 0 and world == 1 and args.debye_nt > 0:

@@ -84,7 +84,19 @@ cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     kept.fetch_or(1ull << dev);
   }
-  return cudaMallocAsync(p, bytes, st);
+  e = cudaMallocAsync(p, bytes, st);
+  if (e == cudaErrorMemoryAllocation) {
+    // memory the pool keeps from earlier calls may be what is missing: wait
+    // for the stream's pending frees, return the pool's unused memory to the
+    // driver and try once more
+    cudaGetLastError();
+    cudaMemPool_t pool;
+    if (cudaStreamSynchronize(st) == cudaSuccess &&
+        cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+        cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+      e = cudaMallocAsync(p, bytes, st);
+  }
+  return e;
 }
 
 ProfileScope::ProfileScope(cudaStream_t st)

@@ -349,7 +349,7 @@ class TMServer:
     """Persistent request loop over the native serving engine (one GPU).
 
     memory_budget: device bytes for resident jobs (default 85 % of free
-    memory); max_slots: resident shot groups; chunk_steps: time steps per
+    memory less 2 GiB for the library's per-call scratch); max_slots: resident shot groups; chunk_steps: time steps per
     chunk (the continuous-batching granularity); use_graphs: replay a
     captured CUDA graph per chunk; storage_compression: BF16 snapshots for
     every gradient job of this server; history_limit / group_limit: planning
@@ -376,7 +376,7 @@ class TMServer:
         self.item = self.sdtype.itemsize
         if memory_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
-            memory_budget = int(0.85 * free)
+            memory_budget = int(0.85 * free) - (2 << 30)  # headroom for per-call scratch
         self.budget = int(memory_budget)
         self.history_limit = int(history_limit if history_limit is not None else self.budget // 8)
         self.group_limit = int(group_limit if group_limit is not None else self.budget // 4)
@@ -697,6 +697,9 @@ class TMServer:
             js.pending -= 1
             if js.pending == 0:
                 self.completed.append(self._assemble(js))
+                # a finished job's blocks go back to the driver, where the
+                # library's per-call scratch (stream-ordered pool) can use them
+                torch.cuda.empty_cache()
 
     def _assemble(self, js: _JobState) -> JobResult:
         job = js.job
