@@ -332,12 +332,22 @@ def run_b200(args) -> None:
     L.tide_b200_profile_enable(1 if args.profile_every > 0 else 0, max(1, args.profile_every))
     read_profile(L)
     launches0 = L.tide_b200_launch_count()
+    replays0 = nat.graph_replays()
     ms, _, _ = timed(args.steps, copy_in=False)
     launches = L.tide_b200_launch_count() - launches0
+    replays = nat.graph_replays() - replays0
     L.tide_b200_profile_enable(0, 1)
     prof = read_profile(L)
     clk = clocks.stop()
     e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)
+    # the same step with every time step launched from the host (no graphs)
+    eager_ms = None
+    if args.graphs_off_steps > 0:
+        prev = nat.set_step_graphs(False)
+        try:
+            eager_ms, _, _ = timed(args.graphs_off_steps, copy_in=False)
+        finally:
+            nat.set_step_graphs(prev)
 
     units = cell_updates(S_total, args.nt)  # the whole job; its shots are split over the ranks
     value = units * args.steps / (ms / 1e3)
@@ -363,6 +373,18 @@ def run_b200(args) -> None:
             "avg_launch_ms": avg_ms,
             "kernel_ms_share": {k: round(v / sum(shares.values()), 4) for k, v in shares.items()},
         }
+    # GPU busy time: sampled mean duration of each step kernel x its launches
+    # per step (nt per shot batch), against the measured step time
+    n_batches = -(-S_rank // batch)
+    kernel_ms = sum(prof[k][0] / prof[k][1] * args.nt * n_batches
+                    for k in ("fwd_h", "fwd_e", "adj_e", "adj_h") if prof.get(k, (0, 0))[1] > 0)
+    graphs = {
+        "replays": int(replays), "block_steps": 64,
+        "kernel_ms_per_step": round(kernel_ms, 2),
+        "kernel_share_of_step": round(kernel_ms / (ms / args.steps), 4) if kernel_ms else None,
+        "ms_per_step_graphs_off": (eager_ms / args.graphs_off_steps) if eager_ms else None,
+        "graphs_off_steps": args.graphs_off_steps,
+    }
 
     tma_leg = None
     if rank == 0 and world == 1 and args.tma_nt > 0:
@@ -401,7 +423,7 @@ def run_b200(args) -> None:
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(launches),
+            "gpu_launches": int(launches), "step_graphs": graphs,
             "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
             "tma_path": tma_leg,
             "serving": serving, "serving_sweep": sweep,
@@ -979,9 +1001,12 @@ def main() -> None:
     ap.add_argument("--parity-shots", type=int, default=2)
     ap.add_argument("--parity-nt", type=int, default=250,
                     help="steps of the config-2 accuracy sample (0: skip)")
-    ap.add_argument("--profile-every", type=int, default=32,
+    ap.add_argument("--profile-every", type=int, default=512,
                     help="time every n-th step's kernels with events in the timed region "
-                         "(0: off; the roofline needs it)")
+                         "(0: off; the roofline needs it); the 64-step block holding a timed "
+                         "step runs as ordinary launches, the others replay a CUDA graph")
+    ap.add_argument("--graphs-off-steps", type=int, default=1,
+                    help="steps timed again with the step graphs off (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=32,
                     help="jobs of the served mixed-size stream (0: skip the serving runs)")
     ap.add_argument("--serve-plain-jobs", type=int, default=32)

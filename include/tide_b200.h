@@ -664,6 +664,19 @@ int tide_b200_set_tma_mode(int mode);
  * bit-identical for every bound.  Returns the previous bound. */
 int tide_b200_set_tma_ctas(int max_ctas);
 
+/* Step blocks replayed from CUDA graphs (new; no reference counterpart): the
+ * TM2D forward, forward_with_storage and backward of the per-cell kernels,
+ * with the snapshot history on the device or none, run a call of at least
+ * three blocks (64 steps, or the next multiple of the even snapshot
+ * interval) as one captured graph replayed per block instead of two launches
+ * per step; the step-indexed pointers move with a device-side block counter.
+ * Results are bit-identical either way.  1 = on (default), 0 = off.  Returns
+ * the previous setting; process-wide, takes effect at the next call. */
+int tide_b200_set_step_graphs(int on);
+
+/* Graph replays issued so far by this process (each one block of steps). */
+int64_t tide_b200_graph_replays(void);
+
 #ifdef __cplusplus
 }
 #endif

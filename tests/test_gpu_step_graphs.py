@@ -1,0 +1,147 @@
+"""Step blocks replayed from CUDA graphs give the results of per-step launches.
+
+A TM2D call of at least three step blocks (64 steps, or the next multiple of
+the even snapshot interval) captures one block into a graph and replays it,
+the step-indexed pointers moving with a device-side block counter.  These
+tests run the same calls with the graphs off and on and require bit-identical
+receivers, snapshots, fields and gradients, plus the oracle on one case; the
+step counts leave a tail after the last whole block so both the replayed
+blocks and the tail are covered.
+"""
+
+from __future__ import annotations
+
+import pytest
+import torch
+
+from cases import clone_problem, random_problem
+from oracle_harness import set_grad_order
+from tide_b200 import _native as nat
+from tide_b200 import storage as stg
+from tide_b200 import tm2d
+
+pytestmark = pytest.mark.gpu
+
+
+def _zeros_r(pb, device="cpu"):
+    return torch.zeros((pb.nt, pb.n_shots, pb.n_rec), dtype=pb.dtype, device=device)
+
+
+class _Graphs:
+    """Sets the step-graph switch for a block and restores it afterwards."""
+
+    def __init__(self, on: bool):
+        self.on = on
+
+    def __enter__(self):
+        self.prev = nat.set_step_graphs(self.on)
+
+    def __exit__(self, *exc):
+        nat.set_step_graphs(self.prev)
+
+
+def _forward(pb, dev, on):
+    g = clone_problem(pb, dev)
+    r = _zeros_r(g, dev)
+    n0 = nat.graph_replays()
+    with _Graphs(on):
+        tm2d.native_forward(g, g.ca, g.cb, g.f, r, 0, g.nt)
+        torch.cuda.synchronize()
+    return [r] + [f.detach().clone() for f in g.fields], nat.graph_replays() - n0
+
+
+def _gradients(pb, dev, grad_r, on, fmt=0, k=1):
+    g = clone_problem(pb, dev)
+    g.grad_interval = k
+    S, ny, nx, nt = g.n_shots, g.ny, g.nx, g.nt
+    sdt = torch.bfloat16 if fmt else g.dtype
+    n_store = (nt + k - 1) // k
+    snaps = stg.allocate(stg.STORAGE_DEVICE, sdt, fmt, n_store, S, ny, nx, dev, True, True)
+    snaps.ey_dev.zero_()
+    snaps.curl_dev.zero_()
+    r = _zeros_r(g, dev)
+    n0 = nat.graph_replays()
+    with _Graphs(on):
+        tm2d._run_forward_storage(g, g.ca, g.cb, g.f, r, snaps, True, True, None, 0)
+        gca, gcb, gf = tm2d._run_backward(g, g.ca, g.cb, grad_r.to(dev), snaps, True, True,
+                                          True, {})
+        torch.cuda.synchronize()
+    out = [r, snaps.ey_dev.clone(), snaps.curl_dev.clone(), gca, gcb, gf]
+    return out, nat.graph_replays() - n0
+
+
+def _same(a, b, names):
+    for x, y, n in zip(a, b, names):
+        assert torch.equal(x.detach().cpu(), y.detach().cpu()), f"{n}: graph replay differs"
+
+
+@pytest.mark.parametrize("stencil", [2, 4])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_forward_graphs_bitwise(cuda_device, stencil, dtype):
+    pb = random_problem(300 + stencil, 41, 57, 3, 229, stencil=stencil, dtype=dtype)
+    eager, n_eager = _forward(pb, cuda_device, False)
+    graph, n_graph = _forward(pb, cuda_device, True)
+    assert n_eager == 0 and n_graph == 229 // 64 - 1  # blocks 1.. replayed, block 0 eager
+    _same(eager, graph, ("r", "Ey", "Hx", "Hz", "mEyx", "mEyz", "mHxz", "mHzx"))
+
+
+@pytest.mark.parametrize("fmt,k", [(0, 1), (1, 1), (0, 3), (1, 4)])
+def test_storage_and_backward_graphs_bitwise(cuda_device, fmt, k):
+    nt = 241
+    pb = random_problem(77 + k, 39, 51, 2, nt)
+    gen = torch.Generator().manual_seed(11)
+    grad_r = torch.randn((nt, pb.n_shots, pb.n_rec), generator=gen)
+    eager, n_eager = _gradients(pb, cuda_device, grad_r, False, fmt, k)
+    graph, n_graph = _gradients(pb, cuda_device, grad_r, True, fmt, k)
+    blk = {1: 64, 3: 66, 4: 64}[k]  # 64 rounded up to a multiple of lcm(2, k)
+    assert n_eager == 0 and n_graph == 2 * (nt // blk - 1)
+    _same(eager, graph, ("r", "Ey snapshots", "curl snapshots", "grad_ca", "grad_cb", "grad_f"))
+
+
+def test_backward_graphs_double_stencil8(cuda_device):
+    nt = 200
+    pb = random_problem(91, 40, 48, 2, nt, stencil=8, dtype=torch.float64)
+    grad_r = torch.randn((nt, pb.n_shots, pb.n_rec), generator=torch.Generator().manual_seed(4),
+                         dtype=torch.float64)
+    eager, _ = _gradients(pb, cuda_device, grad_r, False)
+    graph, n_graph = _gradients(pb, cuda_device, grad_r, True)
+    assert n_graph == 2 * (nt // 64 - 1)
+    _same(eager, graph, ("r", "Ey snapshots", "curl snapshots", "grad_ca", "grad_cb", "grad_f"))
+
+
+def test_graphs_vs_oracle(oracle, cuda_device):
+    """The replayed blocks against the CPU oracle (step-major gradient order)."""
+    nt = 200
+    pb = random_problem(93, 33, 45, 2, nt)
+    grad_r = torch.randn((nt, pb.n_shots, pb.n_rec), generator=torch.Generator().manual_seed(6))
+    graph, n_graph = _gradients(pb, cuda_device, grad_r, True)
+    assert n_graph > 0
+    qb = clone_problem(pb)
+    store = (torch.zeros((nt, 2, pb.ny, pb.nx)), torch.zeros((nt, 2, pb.ny, pb.nx)))
+    r_o = _zeros_r(qb)
+    oracle.forward(qb, qb.ca, qb.cb, qb.f, r_o, store=store, need_ca=True, need_cb=True)
+    set_grad_order(oracle, 1)
+    try:
+        oca, ocb, ogf, _ = oracle.backward(qb, qb.ca, qb.cb, grad_r, store)
+    finally:
+        set_grad_order(oracle, 0)
+    r, ey_s, cu_s, gca, gcb, gf = graph
+    _same([r, ey_s, cu_s, gca[0], gcb[0], gf.reshape(ogf.shape)],
+          [r_o, store[0], store[1], oca, ocb, ogf],
+          ("r", "Ey snapshots", "curl snapshots", "grad_ca", "grad_cb", "grad_f"))
+
+
+def test_profiled_blocks_run_eagerly(cuda_device):
+    """Blocks holding a profiled step run as launches; the rest replay."""
+    nt = 260
+    pb = random_problem(95, 36, 44, 2, nt)
+    lib = nat.load()
+    base, _ = _forward(pb, cuda_device, True)
+    lib.tide_b200_profile_enable(1, 128)
+    try:
+        prof, n_graph = _forward(pb, cuda_device, True)
+    finally:
+        lib.tide_b200_profile_enable(0, 1)
+    # blocks 1..3 of 64 steps; steps 128 (block 2) is profiled
+    assert n_graph == 2
+    _same(base, prof, ("r", "Ey", "Hx", "Hz", "mEyx", "mEyz", "mHxz", "mHzx"))

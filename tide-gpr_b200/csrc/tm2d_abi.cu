@@ -209,14 +209,14 @@ template <typename T, int ST, typename S>
 inline void launch_fwd_e(const Launch<T, ST> &L, cudaStream_t st, const T *ca, const T *cb,
                          const T *hx, const T *hz, T *ey, T *m_hx_z, T *m_hz_x, S *e_st,
                          S *c_st, const DebyeArgs<T> &db, const PointScratch &ps, const T *ft,
-                         T *rt) {
+                         T *rt, const StepShift &sh = StepShift{}) {
   if (ST == 2 && db.n_poles == 0)
     k2_fwd_e<T, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
-                                                         e_st, c_st, ps.src, ps.rec, ft, rt);
+                                                         e_st, c_st, ps.src, ps.rec, ft, rt, sh);
   else
     k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z,
                                                             m_hz_x, e_st, c_st, db, ps.src,
-                                                            ps.rec, ft, rt);
+                                                            ps.rec, ft, rt, sh);
 }
 
 template <typename T, int ST>
@@ -243,17 +243,110 @@ template <typename T, int ST, typename S>
 inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, const T *cq,
                          const T *lhx, const T *lhz, T *ley, const T *mex, const T *mez,
                          T *mex_n, T *mez_n, const PointScratch &ps, const T *grt, T *gft,
-                         const GradArgs<T, S> &ga) {
+                         const GradArgs<T, S> &ga, const StepShift &sh = StepShift{}) {
   if (ST == 2 && L.ah_by == 4)
     k2_adj_h<T, S, kRowsAH, 4><<<L.grid_ah, dim3(kTileX, 4, 1), 0, st>>>(
-        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga);
+        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga,
+        sh);
   else if (ST == 2)
     k2_adj_h<T, S, kRowsAH, kBlockY><<<L.grid_ah, L.block, 0, st>>>(
-        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga);
+        L.g, ca, cq, lhx, lhz, ley, mex, mez, mex_n, mez_n, ps.rec, ps.src, ps.rowf, grt, gft, ga,
+        sh);
   else
     k_adj_h<T, ST, S, kRowsAH><<<L.grid_ah, L.block, 0, st>>>(L.g, ca, cq, lhx, lhz, ley, mex,
                                                               mez, mex_n, mez_n, ps.rec, ps.src,
-                                                              grt, gft, ga);
+                                                              grt, gft, ga, sh);
+}
+
+// ---------------------------------------------------------------------------
+// Step blocks replayed from a CUDA graph.  A time step of the per-cell-kernel
+// paths is two launches of 25-50 us each, and every launch costs the host a
+// few microseconds; a host that falls behind leaves the GPU idle between
+// steps.  So a long call runs its first block of steps as ordinary launches,
+// captures the second block into a graph meanwhile (on a private stream:
+// nothing runs during the capture) and replays that graph for every later
+// block, one host call per block.  The step-indexed pointers of the captured
+// launches (source and receiver rows, snapshot slots) move with a device word
+// that the block's last launch advances (StepShift).  The block length is
+// even and a multiple of the snapshot interval, so the steps that store or
+// image a snapshot and the ping-pong state of the adjoint's CPML memories are
+// the same in every block.  Blocks that hold a profiled step, and the steps
+// after the last whole block, run as ordinary launches.
+std::atomic<int> g_step_graphs{1};          // tide_b200_set_step_graphs
+std::atomic<int64_t> g_graph_replays{0};    // tide_b200_graph_replays
+
+__global__ void k_block_advance(int64_t *blk) { *blk += 1; }
+
+// Steps per block when the step pattern repeats every `period` steps; 0: no
+// graph (a block would exceed 256 steps).
+inline int64_t graph_block_len(int64_t period) {
+  const int64_t p = period % 2 ? 2 * period : period;  // lcm(2, period)
+  if (p < 1 || p > 256) return 0;
+  return ((64 + p - 1) / p) * p;
+}
+
+struct GraphHold {
+  cudaStream_t st = nullptr, cs = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t *blk = nullptr;
+  ~GraphHold() {
+    if (exec) cudaGraphExecDestroy(exec);  // freed once its replays have run
+    if (cs) cudaStreamDestroy(cs);
+    if (blk) cudaFreeAsync(blk, st);
+  }
+};
+
+// Runs steps 0..n-1 of a call.  step(i, stream, blk, B) launches step i on
+// `stream`; blk != nullptr marks a captured launch (StepShift over blocks of B
+// steps, no profiling events).  sampled(i): step i is profiled.
+template <typename Step, typename Sampled>
+bool run_step_blocks(int64_t n, int64_t period, cudaStream_t st, Step &&step,
+                     Sampled &&sampled) {
+  const int64_t B = g_step_graphs.load() ? graph_block_len(period) : 0;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (B > 0 && n >= 3 * B && TB_CUDA(cudaStreamIsCapturing(st, &cap))) return false;
+  if (B == 0 || n < 3 * B || cap != cudaStreamCaptureStatusNone) {
+    for (int64_t i = 0; i < n; ++i)
+      if (!step(i, st, nullptr, B)) return false;
+    return true;
+  }
+  for (int64_t i = 0; i < B; ++i)  // block 0 runs while block 1 is captured
+    if (!step(i, st, nullptr, B)) return false;
+  GraphHold gh;
+  gh.st = st;
+  if (TB_CUDA(pool_malloc((void **)&gh.blk, sizeof(int64_t), st))) return false;
+  if (TB_CUDA(cudaMemsetAsync(gh.blk, 0, sizeof(int64_t), st))) return false;
+  if (TB_CUDA(cudaStreamCreateWithFlags(&gh.cs, cudaStreamNonBlocking))) return false;
+  if (TB_CUDA(cudaStreamBeginCapture(gh.cs, cudaStreamCaptureModeThreadLocal))) return false;
+  bool ok = true;
+  for (int64_t i = B; i < 2 * B && ok; ++i) ok = step(i, gh.cs, gh.blk, B);
+  if (ok) k_block_advance<<<1, 1, 0, gh.cs>>>(gh.blk);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(gh.cs, &graph);
+  if (!ok || TB_CUDA(ec)) {
+    if (graph) cudaGraphDestroy(graph);
+    return false;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&gh.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (TB_CUDA(ei)) return false;
+  const int64_t nb = n / B;
+  for (int64_t b = 1; b < nb; ++b) {
+    bool eager = false;
+    for (int64_t i = b * B; i < (b + 1) * B && !eager; ++i) eager = sampled(i);
+    if (!eager) {
+      if (TB_CUDA(cudaGraphLaunch(gh.exec, st))) return false;
+      g_graph_replays.fetch_add(1, std::memory_order_relaxed);
+      continue;
+    }
+    for (int64_t i = b * B; i < (b + 1) * B; ++i)
+      if (!step(i, st, nullptr, B)) return false;
+    k_block_advance<<<1, 1, 0, st>>>(gh.blk);
+  }
+  count_launches(nb - 1);  // block advances
+  for (int64_t i = nb * B; i < n; ++i)
+    if (!step(i, st, nullptr, B)) return false;
+  return !TB_CUDA(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------
@@ -682,18 +775,23 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
                     n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   ProfileScope prof(st);
-  for (int64_t t = start_t; t < start_t + nt; ++t) {
-    const bool smp = prof.sample(t);
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+    const int64_t t = start_t + i;
+    const bool smp = !blk && prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
-      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
       if (smp) prof.end(kKFwdH);
     }
     if (smp) prof.begin(kKFwdE);
-    launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, nullptr, nullptr, db, ps,
-                           f ? f + t * fs : nullptr, r ? r + t * rs : nullptr);
+    launch_fwd_e<T, ST, T>(L, s, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, nullptr, nullptr, db, ps,
+                           f ? f + t * fs : nullptr, r ? r + t * rs : nullptr,
+                           StepShift{blk, B * fs, B * rs, 0});
     if (smp) prof.end(kKFwdE);
-  }
+    return true;
+  };
+  if (!run_step_blocks(nt, 1, st, step, [&](int64_t i) { return prof.sample(start_t + i); }))
+    return;
   count_launches(nt * (L.has_domain ? 2 : 1));
   TB_CUDA(cudaGetLastError());
 }
@@ -749,6 +847,48 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
   const DebyeArgs<T> db{nullptr, nullptr, nullptr, nullptr, 0};
   const bool bf16 = sr.bf16;
   ProfileScope prof(st);
+  if (!qpath && !fused) {
+    // Per-cell kernels; with the history on the device the step blocks are
+    // replayed from a graph (run_step_blocks).
+    const int64_t snap = sr.want ? (int64_t)(sr.step_bytes / (bf16 ? 2 : sizeof(T))) : 0;
+    auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+      const int64_t t = start_t + i;
+      const bool smp = !blk && prof.sample(t);
+      const bool store_step = sr.stores(t);
+      char *dst[2];
+      if (!sr.begin(t, dst)) return false;
+      char *const e1 = dst[0], *const c1 = dst[1];
+      const T *ft = f ? f + t * fs : nullptr;
+      T *rt = r ? r + t * rs : nullptr;
+      const StepShift sh{blk, B * fs, B * rs, B / step_ratio * snap};
+      if (L.has_domain) {
+        if (smp) prof.begin(kKFwdH);
+        launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
+        if (smp) prof.end(kKFwdH);
+      }
+      if (smp) prof.begin(kKFwdE);
+      if (store_step && bf16)
+        launch_fwd_e<T, ST, __nv_bfloat16>(L, s, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
+                                           (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db, ps, ft,
+                                           rt, sh);
+      else
+        launch_fwd_e<T, ST, T>(L, s, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)e1, (T *)c1, db,
+                               ps, ft, rt, sh);
+      if (smp) prof.end(kKFwdE);
+      return sr.end(t, dst);
+    };
+    auto sampled = [&](int64_t i) { return prof.sample(start_t + i); };
+    if (sr.host_side) {
+      for (int64_t i = 0; i < nt; ++i)
+        if (!step(i, st, nullptr, 0)) return;
+    } else if (!run_step_blocks(nt, sr.want ? step_ratio : 1, st, step, sampled)) {
+      return;
+    }
+    count_launches(nt * (L.has_domain ? 2 : 1));
+    if (TB_CUDA(cudaGetLastError())) return;
+    sr.finish();
+    return;
+  }
   for (int64_t t = start_t; t < start_t + nt; ++t) {
     const bool smp = prof.sample(t);
     const bool store_step = sr.stores(t);
@@ -769,7 +909,7 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
         if (!ok) return;
       }
       if (smp) prof.end(kKFwdStep);
-    } else if (fused) {
+    } else {
       if (smp) prof.begin(kKFwdStep);
       if constexpr (is_float<T>()) {
         if (store_step && bf16)
@@ -778,25 +918,10 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
           pf.launch<float>(L.g, (float *)e1, (float *)c1, ps, ft, rt);
       }
       if (smp) prof.end(kKFwdStep);
-    } else {
-      if (L.has_domain) {
-        if (smp) prof.begin(kKFwdH);
-        launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
-        if (smp) prof.end(kKFwdH);
-      }
-      if (smp) prof.begin(kKFwdE);
-      if (store_step && bf16)
-        launch_fwd_e<T, ST, __nv_bfloat16>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
-                                           (__nv_bfloat16 *)e1, (__nv_bfloat16 *)c1, db, ps, ft,
-                                           rt);
-      else
-        launch_fwd_e<T, ST, T>(L, st, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, (T *)e1, (T *)c1, db,
-                               ps, ft, rt);
-      if (smp) prof.end(kKFwdE);
     }
     if (!sr.end(t, dst)) return;
   }
-  count_launches((fused || qpath) ? nt : nt * (L.has_domain ? 2 : 1));
+  count_launches(nt);
   if (TB_CUDA(cudaGetLastError())) return;
   if constexpr (is_float<T>()) {
     if (fused && !pf.finish()) return;
@@ -961,48 +1086,53 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
 
   ProfileScope prof(st);
-  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
-    const bool smp = prof.sample(t);
+  // One-sweep TMA steps.
+  for (int64_t t = start_t - 1; qpath && t >= start_t - nt; --t) {
     if constexpr (is_float<T>()) {
-      if (qpath) {
-        const bool grad_step = grads && t % step_ratio == 0;
-        const int64_t q = t / step_ratio;
-        const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
-                                              : (size_t)(q % kRing) * step_bytes;
-        if (grad_step && pipeline &&
-            TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0)))
-          return;
-        const char *es = grad_step && ca_requires_grad ? (const char *)ey_store_1 + off1 : nullptr;
-        const char *cs = grad_step && cb_requires_grad ? (const char *)curl_store_1 + off1 : nullptr;
-        const float *const mc[4] = {cur_hz_x, cur_hx_z, cur_ey_x, cur_ey_z};
-        float *const mn[4] = {nxt_hz_x, nxt_hx_z, nxt_ey_x, nxt_ey_z};
-        const float *grt = grad_r ? grad_r + t * rs : nullptr;
-        float *gft = grad_f ? grad_f + t * fs : nullptr;
-        if (smp) prof.begin(kKAdjStep);
-        const bool ok =
-            bf16 ? qr.template adj_step<__nv_bfloat16>(
-                       L.g, ps, grt, gft, mc, mn, (const __nv_bfloat16 *)es,
-                       (const __nv_bfloat16 *)cs, bg_shots, grad_ca, grad_cb, (float)step_ratio)
-                 : qr.template adj_step<float>(L.g, ps, grt, gft, mc, mn, (const float *)es,
-                                               (const float *)cs, bg_shots, grad_ca, grad_cb,
-                                               (float)step_ratio);
-        if (!ok) return;
-        if (smp) prof.end(kKAdjStep);
-        std::swap(cur_hx_z, nxt_hx_z);
-        std::swap(cur_hz_x, nxt_hz_x);
-        std::swap(cur_ey_x, nxt_ey_x);
-        std::swap(cur_ey_z, nxt_ey_z);
-        if (grad_step && host_side) {
-          ++next_q;
-          if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
-          if (!load(next_q + 1)) return;
-        }
-        continue;
+      const bool smp = prof.sample(t);
+      const bool grad_step = grads && t % step_ratio == 0;
+      const int64_t q = t / step_ratio;
+      const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
+                                            : (size_t)(q % kRing) * step_bytes;
+      if (grad_step && pipeline &&
+          TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0)))
+        return;
+      const char *es = grad_step && ca_requires_grad ? (const char *)ey_store_1 + off1 : nullptr;
+      const char *cs = grad_step && cb_requires_grad ? (const char *)curl_store_1 + off1 : nullptr;
+      const float *const mc[4] = {cur_hz_x, cur_hx_z, cur_ey_x, cur_ey_z};
+      float *const mn[4] = {nxt_hz_x, nxt_hx_z, nxt_ey_x, nxt_ey_z};
+      const float *grt = grad_r ? grad_r + t * rs : nullptr;
+      float *gft = grad_f ? grad_f + t * fs : nullptr;
+      if (smp) prof.begin(kKAdjStep);
+      const bool ok =
+          bf16 ? qr.template adj_step<__nv_bfloat16>(
+                     L.g, ps, grt, gft, mc, mn, (const __nv_bfloat16 *)es,
+                     (const __nv_bfloat16 *)cs, bg_shots, grad_ca, grad_cb, (float)step_ratio)
+               : qr.template adj_step<float>(L.g, ps, grt, gft, mc, mn, (const float *)es,
+                                             (const float *)cs, bg_shots, grad_ca, grad_cb,
+                                             (float)step_ratio);
+      if (!ok) return;
+      if (smp) prof.end(kKAdjStep);
+      std::swap(cur_hx_z, nxt_hx_z);
+      std::swap(cur_hz_x, nxt_hz_x);
+      std::swap(cur_ey_x, nxt_ey_x);
+      std::swap(cur_ey_z, nxt_ey_z);
+      if (grad_step && host_side) {
+        ++next_q;
+        if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
+        if (!load(next_q + 1)) return;
       }
     }
+  }
+  // Per-cell kernels; with the history on the device (or none) the step
+  // blocks are replayed from a graph (run_step_blocks).
+  const int64_t snap = grads ? (int64_t)(step_bytes / esz) : 0;
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+    const int64_t t = start_t - 1 - i;
+    const bool smp = !blk && prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKAdjE);
-      launch_adj_e<T, ST>(L, st, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x,
+      launch_adj_e<T, ST>(L, s, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x,
                           nxt_hx_z, nxt_hz_x);
       if (smp) prof.end(kKAdjE);
     }
@@ -1013,33 +1143,45 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
     const size_t off1 = storage_mode == 0 ? (size_t)q * step_bytes
                                           : (size_t)(q % kRing) * step_bytes;
     if (grad_step && pipeline &&
-        TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[(int)(q % kRing)], 0)))
-      return;
+        TB_CUDA(cudaStreamWaitEvent(s, loaded.ev[(int)(q % kRing)], 0)))
+      return false;
     const char *es = grad_step && ca_requires_grad ? (const char *)ey_store_1 + off1 : nullptr;
     const char *cs = grad_step && cb_requires_grad ? (const char *)curl_store_1 + off1 : nullptr;
     const T *grt = grad_r ? grad_r + t * rs : nullptr;
     T *gft = grad_f ? grad_f + t * fs : nullptr;
+    // the adjoint walks the steps backwards: pointers move down by a block
+    const StepShift sh{blk, -B * fs, -B * rs, -(B / step_ratio) * snap};
     if (smp) prof.begin(kKAdjH);
     if (bf16) {
       GradArgs<T, __nv_bfloat16> ga{(const __nv_bfloat16 *)es, (const __nv_bfloat16 *)cs,
                                     grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched,
                                     bg_shots};
-      launch_adj_h<T, ST, __nv_bfloat16>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey,
+      launch_adj_h<T, ST, __nv_bfloat16>(L, s, ca, cq, lambda_hx, lambda_hz, lambda_ey,
                                          cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft,
-                                         ga);
+                                         ga, sh);
     } else {
       GradArgs<T, T> ga{(const T *)es, (const T *)cs, grad_ca, grad_cb, (T)step_ratio,
                         ca_batched, cb_batched, bg_shots};
-      launch_adj_h<T, ST, T>(L, st, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x,
-                             cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft, ga);
+      launch_adj_h<T, ST, T>(L, s, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x,
+                             cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft, ga, sh);
     }
     if (smp) prof.end(kKAdjH);
     std::swap(cur_ey_x, nxt_ey_x);
     std::swap(cur_ey_z, nxt_ey_z);
     if (grad_step && host_side) {
       ++next_q;
-      if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], st))) return;
-      if (!load(next_q + 1)) return;
+      if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[(int)(q % kRing)], s))) return false;
+      if (!load(next_q + 1)) return false;
+    }
+    return true;
+  };
+  if (!qpath) {
+    if (host_side) {
+      for (int64_t i = 0; i < nt; ++i)
+        if (!step(i, st, nullptr, 0)) return;
+    } else if (!run_step_blocks(nt, grads ? step_ratio : 1, st, step,
+                                [&](int64_t i) { return prof.sample(start_t - 1 - i); })) {
+      return;
     }
   }
   // Leave the final adjoint memories in the caller's arrays
@@ -1131,6 +1273,8 @@ extern "C" int tide_b200_set_tma_ctas(int max_ctas) {
 extern "C" int tide_b200_set_tma_mode(int mode) {
   return tb::g_tma_mode.exchange(mode < 0 ? 0 : (mode > 2 ? 2 : mode));
 }
+extern "C" int tide_b200_set_step_graphs(int on) { return tb::g_step_graphs.exchange(on ? 1 : 0); }
+extern "C" int64_t tide_b200_graph_replays(void) { return tb::g_graph_replays.load(); }
 
 extern "C" int64_t tide_b200_set_fused_threshold(int64_t bytes) {
   return tb::g_fused_min_bytes.exchange(bytes < 0 ? -1 : bytes);

@@ -182,7 +182,7 @@ void debye_forward(const TideTMDebye &A) {
     k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(
         L.g, ca, cb, fld[1], fld[2], fld[0], fld[5], fld[6], static_cast<S *>(at(A.ey_store, SN)),
         static_cast<S *>(at(A.curl_store, SN)), db, ps.src, ps.rec, f ? f + t * fs : nullptr,
-        r ? r + t * rs : nullptr);
+        r ? r + t * rs : nullptr, StepShift{});
   }
   count_launches(2 * A.nt);
   TB_CUDA(cudaGetLastError());

@@ -56,6 +56,23 @@ template <> struct FD<8> {
   }
 };
 
+// Step-indexed pointers of a launch replayed from a captured block of time
+// steps.  The captured launch holds the pointers of the block it was
+// captured for; replay j (the device word *blk, advanced by the block's last
+// launch) moves each of them by j times its per-block advance, in elements.
+// blk == nullptr: an ordinary launch whose pointers are used as given.
+struct StepShift {
+  const int64_t *blk = nullptr;
+  int64_t src = 0;   // source amplitudes (forward) / their gradient (adjoint)
+  int64_t rec = 0;   // receiver records (forward) / their gradient (adjoint)
+  int64_t snap = 0;  // snapshot slots
+  __device__ __forceinline__ int64_t block() const { return blk ? *blk : 0; }
+};
+template <typename P>
+__device__ __forceinline__ P *shifted(P *p, int64_t adv, int64_t j) {
+  return (p && j) ? p + adv * j : p;
+}
+
 template <typename T> struct TMGeom {
   const T *ay, *by, *ayh, *byh, *ax, *bx, *axh, *bxh;
   const T *ky, *kyh, *kx, *kxh;
@@ -336,8 +353,15 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
         const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
         T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
         DebyeArgs<T> db, PointCSR src, PointCSR rec, const T *__restrict__ f_t,
-        T *__restrict__ r_t) {
+        T *__restrict__ r_t, StepShift sh) {
   constexpr int P = FD<ST>::P;
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    f_t = shifted(f_t, sh.src, jb);
+    r_t = shifted(r_t, sh.rec, jb);
+    ey_store = shifted(ey_store, sh.snap, jb);
+    curl_store = shifted(curl_store, sh.snap, jb);
+  }
   const int x = blockIdx.x * kTileX + threadIdx.x;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int s = blockIdx.z;
@@ -668,8 +692,15 @@ k_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
         const T *__restrict__ lam_hx, const T *__restrict__ lam_hz, T *__restrict__ lam_ey,
         const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
         T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src, const T *__restrict__ gr_t,
-        T *__restrict__ gf_t, GradArgs<T, S> ga) {
+        T *__restrict__ gf_t, GradArgs<T, S> ga, StepShift sh) {
   constexpr int P = FD<ST>::P;
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    gr_t = shifted(gr_t, sh.rec, jb);
+    gf_t = shifted(gf_t, sh.src, jb);
+    ga.ey_st = shifted(ga.ey_st, sh.snap, jb);
+    ga.cu_st = shifted(ga.cu_st, sh.snap, jb);
+  }
   const int x = blockIdx.x * kTileX + threadIdx.x;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int tile_xy = blockIdx.y * gridDim.x + blockIdx.x;

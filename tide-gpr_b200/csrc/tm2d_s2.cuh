@@ -257,7 +257,15 @@ __global__ void __launch_bounds__(256)
 k2_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
          const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
          T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
-         PointCSR src, PointCSR rec, const T *__restrict__ f_t, T *__restrict__ r_t) {
+         PointCSR src, PointCSR rec, const T *__restrict__ f_t, T *__restrict__ r_t,
+         StepShift sh) {
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    f_t = shifted(f_t, sh.src, jb);
+    r_t = shifted(r_t, sh.rec, jb);
+    ey_store = shifted(ey_store, sh.snap, jb);
+    curl_store = shifted(curl_store, sh.snap, jb);
+  }
   fwd_e_tile<T, S, R>(HwTile(), g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, ey_store, curl_store, src,
       rec, f_t, r_t);
 }
@@ -704,7 +712,14 @@ k2_adj_h(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cq,
          const T *__restrict__ m_ey_x, const T *__restrict__ m_ey_z, T *__restrict__ m_ey_x_n,
          T *__restrict__ m_ey_z_n, PointCSR rec, PointCSR src,
          const unsigned char *__restrict__ rowf, const T *__restrict__ gr_t,
-         T *__restrict__ gf_t, GradArgs<T, S> ga) {
+         T *__restrict__ gf_t, GradArgs<T, S> ga, StepShift sh) {
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    gr_t = shifted(gr_t, sh.rec, jb);
+    gf_t = shifted(gf_t, sh.src, jb);
+    ga.ey_st = shifted(ga.ey_st, sh.snap, jb);
+    ga.cu_st = shifted(ga.cu_st, sh.snap, jb);
+  }
   adj_h_tile<T, S, R, BY>(HwTile(), g, ca, cq, lam_hx, lam_hz, lam_ey, m_ey_x, m_ey_z, m_ey_x_n,
       m_ey_z_n, rec, src, rowf, gr_t, gf_t, ga);
 }

@@ -233,6 +233,22 @@ def set_tma_ctas(max_ctas: int) -> int:
     return int(lib.tide_b200_set_tma_ctas(int(max_ctas)))
 
 
+def set_step_graphs(on: bool) -> bool:
+    """Replay blocks of time steps from one captured CUDA graph (default on);
+    returns the previous setting."""
+    lib = load()
+    lib.tide_b200_set_step_graphs.argtypes = [ctypes.c_int]
+    lib.tide_b200_set_step_graphs.restype = ctypes.c_int
+    return bool(lib.tide_b200_set_step_graphs(1 if on else 0))
+
+
+def graph_replays() -> int:
+    """Step-block graph replays issued so far by this process."""
+    lib = load()
+    lib.tide_b200_graph_replays.restype = ctypes.c_int64
+    return int(lib.tide_b200_graph_replays())
+
+
 def ptr(t: torch.Tensor | None) -> int:
     if t is None or t.numel() == 0:
         return 0
@@ -273,6 +289,8 @@ def exported_symbols() -> list[str]:
         "tide_b200_set_fused_threshold",
         "tide_b200_set_tma_mode",
         "tide_b200_set_tma_ctas",
+        "tide_b200_set_step_graphs",
+        "tide_b200_graph_replays",
         "tide_b200_launch_count",
         "tide_b200_profile_enable",
         "tide_b200_profile_read",

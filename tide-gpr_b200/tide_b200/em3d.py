@@ -636,14 +636,19 @@ class Born3DPropagate(torch.autograd.Function):
             gf0 = torch.zeros(nf, device=dev, dtype=dt) if ctx.n_src > 0 else empty
             gdf = torch.zeros(nf, device=dev, dtype=dt) if ctx.n_src > 0 else empty
             dca, dcb, df = ctx.pert
+            # every work array stays referenced until the call is enqueued: a
+            # tensor dropped after taking its pointer would hand its block to
+            # the next allocation, and the arrays would alias
+            lam_eta = [z() for _ in range(36)]  # adjoint fields + memories, twice
+            scratch = torch.empty((24, *full), device=dev, dtype=dt)
+            work = [z() for _ in range(3)]
+            grad_r = grad_r.contiguous()
             fn = nat.get_backend_function("maxwell_3d", "born_backward_bggrad", pb.stencil, dt,
                                           dev)
-            fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(pb.f), _p(df),
-               _p(grad_r.contiguous()), *[_p(z()) for _ in range(18)],
-               *[_p(z()) for _ in range(18)], _p(torch.empty((24, *full), device=dev, dtype=dt)),
-               *s18, *[_p(t) for t in ctx.sc], _p(gf0), _p(gdf), _p(g[2]), _p(g[3]), _p(g[0]),
-               _p(g[1]), *[_p(t) for t in gs], *[_p(z()) for _ in range(3)], *tail, True, True,
-               True, True, *flags)
+            fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(dca), _p(dcb), _p(pb.f), _p(df), _p(grad_r),
+               *[_p(t) for t in lam_eta], _p(scratch), *s18, *[_p(t) for t in ctx.sc], _p(gf0),
+               _p(gdf), _p(g[2]), _p(g[3]), _p(g[0]), _p(g[1]), *[_p(t) for t in gs],
+               *[_p(t) for t in work], *tail, True, True, True, True, *flags)
             nat.check("maxwell_3d born_backward_bggrad")
             ctx.st = ctx.sc = None
             return (g[0], g[1], gdf if ctx.n_src > 0 else None, g[2], g[3],
@@ -657,8 +662,9 @@ class Born3DPropagate(torch.autograd.Function):
         gca_s = torch.empty(full, device=dev, dtype=dt) if need_ca and S > 1 else empty
         gcb_s = torch.empty(full, device=dev, dtype=dt) if need_cb and S > 1 else empty
         gf = torch.empty(nf, device=dev, dtype=dt) if need[2] and ctx.n_src > 0 else empty
+        grad_r = grad_r.contiguous()
         fn = nat.get_backend_function("maxwell_3d", "born_backward", pb.stencil, dt, dev)
-        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(grad_r.contiguous()), *[_p(t) for t in lam],
+        fn(_p(pb.ca), _p(pb.cb), _p(pb.cq), _p(grad_r), *[_p(t) for t in lam],
            *[_p(t) for t in lmem], _p(scratch), *s18, _p(gf), _p(gca), _p(gcb), _p(gca_s),
            _p(gcb_s), *tail, need_ca, need_cb, *flags)
         nat.check("maxwell_3d born_backward")
