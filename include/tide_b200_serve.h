@@ -101,6 +101,11 @@ int64_t tide_b200_serve_run(void *engine, int64_t chunk_steps, int64_t use_graph
  * tile walk; fused != 0 lets them use the fused forward step when planned
  * with TIDE_SERVE_FLAG_FUSED.  Defaults: 1 << 20 cells, fused on. */
 int64_t tide_b200_serve_configure(void *engine, int64_t direct_cells, int64_t fused);
+/* Streams the large slots bound from now on are spread over (1..8; default
+ * 8).  One stream runs the large slots of a chunk one after another, each
+ * with its fields in L2 between its kernels; more streams overlap them.
+ * Returns the previous count, or -1. */
+int64_t tide_b200_serve_set_direct_streams(void *engine, int64_t n);
 /* Kernel launches issued by the engine so far (graph replays count their nodes). */
 int64_t tide_b200_serve_launches(void *engine);
 

@@ -131,17 +131,45 @@ def test_graphs_vs_oracle(oracle, cuda_device):
           ("r", "Ey snapshots", "curl snapshots", "grad_ca", "grad_cb", "grad_f"))
 
 
-def test_profiled_blocks_run_eagerly(cuda_device):
-    """Blocks holding a profiled step run as launches; the rest replay."""
+def _read_profile(lib):
+    import ctypes
+
+    ms = (ctypes.c_double * 16)()
+    n = (ctypes.c_int64 * 16)()
+    lib.tide_b200_profile_read.restype = ctypes.c_int
+    k = lib.tide_b200_profile_read(ms, n, 16)
+    lib.tide_b200_profile_kind_name.restype = ctypes.c_char_p
+    return {lib.tide_b200_profile_kind_name(i).decode(): (ms[i], n[i]) for i in range(k)}
+
+
+def test_profiled_blocks_replay_a_timed_graph(cuda_device):
+    """Blocks holding a profiled step replay a second graph whose event-record
+    nodes time the kernels of its first step; results are unchanged."""
     nt = 260
     pb = random_problem(95, 36, 44, 2, nt)
     lib = nat.load()
     base, _ = _forward(pb, cuda_device, True)
     lib.tide_b200_profile_enable(1, 128)
+    _read_profile(lib)
     try:
         prof, n_graph = _forward(pb, cuda_device, True)
     finally:
         lib.tide_b200_profile_enable(0, 1)
-    # blocks 1..3 of 64 steps; steps 128 (block 2) is profiled
-    assert n_graph == 2
+    times = _read_profile(lib)
+    # blocks 1..3 of 64 steps replay (block 2, steps 128.., through the timed
+    # graph); the profiled steps 0 (block 0) and 256 (tail) run as ordinary
+    # launches and are not timed on this path
+    assert n_graph == 3
+    for kind in ("fwd_h", "fwd_e"):
+        ms, n = times[kind]
+        assert n == 1 and ms > 0, (kind, times[kind])
+    # a call too short for graphs times its profiled steps as launches
+    short = random_problem(96, 36, 44, 2, 150)
+    lib.tide_b200_profile_enable(1, 128)
+    try:
+        _, n_short = _forward(short, cuda_device, True)
+    finally:
+        lib.tide_b200_profile_enable(0, 1)
+    times = _read_profile(lib)
+    assert n_short == 0 and times["fwd_h"][1] == 2 and times["fwd_e"][1] == 2
     _same(base, prof, ("r", "Ey", "Hx", "Hz", "mEyx", "mEyz", "mHxz", "mHzx"))

@@ -133,3 +133,39 @@ def test_mixed_stream_is_seeded_and_in_range():
     assert arr == sorted(arr) and arr[0] > 0
     frac = sum(j.gradient for j in sv.mixed_stream(400, seed=3)) / 400
     assert 0.22 < frac < 0.38
+
+
+def test_load_defers_on_allocator_oom(monkeypatch):
+    """A load the byte budget admits but the fragmented allocator cannot place
+    is retried once after the cache goes back to the driver, then deferred
+    while other jobs are resident, and raised when none is."""
+    import torch
+
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    monkeypatch.setattr(torch.cuda, "empty_cache", lambda: None)
+
+    class Task:
+        def __init__(self):
+            self.out = {}
+
+    class Busy:
+        device = "cuda:0"
+
+        def __init__(self, resident, fail):
+            self.resident, self.fail, self.calls = resident, fail, 0
+            self.stats = {"deferred_oom": 0}
+
+        def _load(self, t):
+            self.calls += 1
+            t.out["partial"] = 1
+            if self.calls <= self.fail:
+                raise torch.OutOfMemoryError("fragmented")
+
+    s, t = Busy(["resident job"], fail=2), Task()
+    assert sv.TMServer._load_or_defer(s, t) is False
+    assert s.calls == 2 and s.stats["deferred_oom"] == 1 and t.out == {}
+    s = Busy([], fail=2)
+    with pytest.raises(torch.OutOfMemoryError):
+        sv.TMServer._load_or_defer(s, Task())
+    s = Busy(["resident job"], fail=1)
+    assert sv.TMServer._load_or_defer(s, Task()) is True and s.calls == 2

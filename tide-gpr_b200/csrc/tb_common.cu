@@ -104,33 +104,106 @@ ProfileScope::ProfileScope(cudaStream_t st)
 
 bool ProfileScope::sample(int64_t step) const { return on_ && (step % every_) == 0; }
 
-void ProfileScope::begin(int kind) {
-  if (!on_) return;
+bool ProfileScope::push(cudaEvent_t a, cudaEvent_t b, int kind) {
   if (n_ == cap_) {
     int nc = cap_ ? 2 * cap_ : 256;
     Pair *np = static_cast<Pair *>(realloc(pairs_, sizeof(Pair) * nc));
-    if (!np) return;
+    if (!np) return false;
     pairs_ = np;
     cap_ = nc;
   }
-  Pair &p = pairs_[n_];
-  p.a = take_event();
-  p.b = take_event();
-  p.kind = kind;
-  if (!p.a || !p.b) {
-    give_event(p.a);
-    give_event(p.b);
+  pairs_[n_++] = Pair{a, b, kind};
+  return true;
+}
+
+void ProfileScope::begin(int kind) {
+  if (!on_) return;
+  cudaEvent_t a = take_event(), b = take_event();
+  if (!a || !b) {
+    give_event(a);
+    give_event(b);
     return;
   }
-  cudaEventRecord(p.a, st_);
+  if (cs_) {  // an event-record node of the graph being captured
+    if (nt_ == tcap_) {
+      int nc = tcap_ ? 2 * tcap_ : 16;
+      NodePair *np = static_cast<NodePair *>(realloc(tmpl_, sizeof(NodePair) * nc));
+      if (!np) {
+        give_event(a);
+        give_event(b);
+        return;
+      }
+      tmpl_ = np;
+      tcap_ = nc;
+    }
+    tmpl_[nt_] = NodePair{a, b, nullptr, nullptr, kind};
+    cudaEventRecordWithFlags(a, cs_, cudaEventRecordExternal);
+  } else {
+    if (!push(a, b, kind)) {
+      give_event(a);
+      give_event(b);
+      return;
+    }
+    --n_;  // completed by end()
+    cudaEventRecord(a, st_);
+  }
   open_kind_ = kind;
 }
 
 void ProfileScope::end(int kind) {
   if (!on_ || open_kind_ != kind) return;
-  cudaEventRecord(pairs_[n_].b, st_);
-  ++n_;
+  if (cs_) {
+    cudaEventRecordWithFlags(tmpl_[nt_].b, cs_, cudaEventRecordExternal);
+    ++nt_;
+  } else {
+    cudaEventRecord(pairs_[n_].b, st_);
+    ++n_;
+  }
   open_kind_ = -1;
+}
+
+void ProfileScope::capture_begin(cudaStream_t cs) {
+  if (!on_) return;
+  cs_ = cs;
+  open_kind_ = -1;
+}
+
+void ProfileScope::capture_end() { cs_ = nullptr; }
+
+bool ProfileScope::bind(cudaGraph_t graph) {
+  if (!on_ || nt_ == 0) return false;
+  size_t n = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return false;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n == 0 || cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return false;
+  for (cudaGraphNode_t node : nodes) {
+    cudaGraphNodeType type;
+    cudaEvent_t ev = nullptr;
+    if (cudaGraphNodeGetType(node, &type) != cudaSuccess) return false;
+    if (type != cudaGraphNodeTypeEventRecord) continue;
+    if (cudaGraphEventRecordNodeGetEvent(node, &ev) != cudaSuccess) return false;
+    for (int i = 0; i < nt_; ++i) {
+      if (tmpl_[i].a == ev) tmpl_[i].na = node;
+      if (tmpl_[i].b == ev) tmpl_[i].nb = node;
+    }
+  }
+  for (int i = 0; i < nt_; ++i)
+    if (!tmpl_[i].na || !tmpl_[i].nb) return false;
+  return true;
+}
+
+bool ProfileScope::arm(cudaGraphExec_t exec) {
+  for (int i = 0; i < nt_; ++i) {
+    cudaEvent_t a = take_event(), b = take_event();
+    if (!a || !b || cudaGraphExecEventRecordNodeSetEvent(exec, tmpl_[i].na, a) != cudaSuccess ||
+        cudaGraphExecEventRecordNodeSetEvent(exec, tmpl_[i].nb, b) != cudaSuccess ||
+        !push(a, b, tmpl_[i].kind)) {
+      give_event(a);
+      give_event(b);
+      return false;
+    }
+  }
+  return true;
 }
 
 // Event pairs of closed scopes wait here until tide_b200_profile_read, so a
@@ -139,6 +212,11 @@ std::mutex g_pending_mu;
 std::vector<std::pair<std::pair<cudaEvent_t, cudaEvent_t>, int>> g_pending;
 
 ProfileScope::~ProfileScope() {
+  for (int i = 0; i < nt_; ++i) {  // placeholders: recorded by no replay
+    give_event(tmpl_[i].a);
+    give_event(tmpl_[i].b);
+  }
+  free(tmpl_);
   if (!on_) return;
   {
     std::lock_guard<std::mutex> lk(g_pending_mu);

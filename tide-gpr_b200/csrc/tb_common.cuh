@@ -51,13 +51,24 @@ cudaError_t pool_malloc(void **p, size_t bytes, cudaStream_t st);
 
 // Brackets sampled launches with events on one stream; accumulates into the
 // process-wide profile when the scope closes (after waiting for its events).
+//
+// Launches captured into a CUDA graph are timed by event-record nodes: between
+// capture_begin and capture_end, begin / end add such nodes on the capture
+// stream (their events are placeholders); bind maps them to the instantiated
+// graph's nodes, and arm gives those nodes fresh events before each timed
+// replay, so every replay's times are kept.
 class ProfileScope {
  public:
   explicit ProfileScope(cudaStream_t st);
   ~ProfileScope();
+  bool on() const { return on_; }
   bool sample(int64_t step) const;  // is this time step timed?
   void begin(int kind);
   void end(int kind);
+  void capture_begin(cudaStream_t cs);
+  void capture_end();
+  bool bind(cudaGraph_t graph);        // false: no timed nodes (or an error)
+  bool arm(cudaGraphExec_t exec);      // before each timed replay of `exec`
 
  private:
   cudaStream_t st_;
@@ -67,6 +78,12 @@ class ProfileScope {
   struct Pair { cudaEvent_t a, b; int kind; };
   Pair *pairs_ = nullptr;
   int n_ = 0, cap_ = 0;
+  bool push(cudaEvent_t a, cudaEvent_t b, int kind);
+  // graph timing: placeholder pairs recorded during capture and their nodes
+  cudaStream_t cs_ = nullptr;
+  struct NodePair { cudaEvent_t a, b; cudaGraphNode_t na, nb; int kind; };
+  NodePair *tmpl_ = nullptr;
+  int nt_ = 0, tcap_ = 0;
 };
 
 }  // namespace tb

@@ -270,8 +270,12 @@ inline void launch_adj_h(const Launch<T, ST> &L, cudaStream_t st, const T *ca, c
 // that the block's last launch advances (StepShift).  The block length is
 // even and a multiple of the snapshot interval, so the steps that store or
 // image a snapshot and the ping-pong state of the adjoint's CPML memories are
-// the same in every block.  Blocks that hold a profiled step, and the steps
-// after the last whole block, run as ordinary launches.
+// the same in every block.  The steps after the last whole block run as
+// ordinary launches.  With profiling on, a second graph of the block carries
+// event-record nodes around the kernels of its first step and replays for
+// the blocks that hold a profiled step (ProfileScope::arm gives it fresh
+// events each time), so the sampled kernel times are those of graph-launched
+// kernels; the ordinary launches of such a call are not sampled.
 std::atomic<int> g_step_graphs{1};          // tide_b200_set_step_graphs
 std::atomic<int64_t> g_graph_replays{0};    // tide_b200_graph_replays
 
@@ -287,67 +291,92 @@ inline int64_t graph_block_len(int64_t period) {
 
 struct GraphHold {
   cudaStream_t st = nullptr, cs = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t timed_graph = nullptr;  // kept: its event nodes are re-armed per replay
+  cudaGraphExec_t exec = nullptr, timed = nullptr;
   int64_t *blk = nullptr;
   ~GraphHold() {
     if (exec) cudaGraphExecDestroy(exec);  // freed once its replays have run
+    if (timed) cudaGraphExecDestroy(timed);
+    if (timed_graph) cudaGraphDestroy(timed_graph);
     if (cs) cudaStreamDestroy(cs);
     if (blk) cudaFreeAsync(blk, st);
   }
 };
 
-// Runs steps 0..n-1 of a call.  step(i, stream, blk, B) launches step i on
-// `stream`; blk != nullptr marks a captured launch (StepShift over blocks of B
-// steps, no profiling events).  sampled(i): step i is profiled.
-template <typename Step, typename Sampled>
-bool run_step_blocks(int64_t n, int64_t period, cudaStream_t st, Step &&step,
-                     Sampled &&sampled) {
+// Captures steps [B, 2B) and the block advance into a graph on gh.cs; with
+// `timed`, the first step's kernels are bracketed by the profile's
+// event-record nodes.
+template <typename Step>
+bool capture_block(GraphHold &gh, int64_t B, Step &step, ProfileScope &prof, bool timed,
+                   cudaGraph_t *graph) {
+  *graph = nullptr;
+  if (TB_CUDA(cudaStreamBeginCapture(gh.cs, cudaStreamCaptureModeThreadLocal))) return false;
+  if (timed) prof.capture_begin(gh.cs);
+  bool ok = true;
+  for (int64_t i = B; i < 2 * B && ok; ++i) ok = step(i, gh.cs, gh.blk, B, timed && i == B);
+  if (timed) prof.capture_end();
+  if (ok) k_block_advance<<<1, 1, 0, gh.cs>>>(gh.blk);
+  const cudaError_t ec = cudaStreamEndCapture(gh.cs, graph);
+  if (!ok || TB_CUDA(ec)) {
+    if (*graph) cudaGraphDestroy(*graph);
+    *graph = nullptr;
+    return false;
+  }
+  return true;
+}
+
+// Runs steps 0..n-1 of a call.  step(i, stream, blk, B, smp) launches step i
+// on `stream`, with profiling events when smp; blk != nullptr marks a
+// captured launch (StepShift over blocks of B steps).  A block is profiled
+// when prof samples one of its steps.
+template <typename Step>
+bool run_step_blocks(int64_t n, int64_t period, cudaStream_t st, ProfileScope &prof,
+                     int64_t (*t_of)(int64_t, int64_t), int64_t t_base, Step &&step) {
+  auto sampled = [&](int64_t i) { return prof.sample(t_of(t_base, i)); };
   const int64_t B = g_step_graphs.load() ? graph_block_len(period) : 0;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   if (B > 0 && n >= 3 * B && TB_CUDA(cudaStreamIsCapturing(st, &cap))) return false;
   if (B == 0 || n < 3 * B || cap != cudaStreamCaptureStatusNone) {
     for (int64_t i = 0; i < n; ++i)
-      if (!step(i, st, nullptr, B)) return false;
+      if (!step(i, st, nullptr, B, sampled(i))) return false;
     return true;
   }
-  for (int64_t i = 0; i < B; ++i)  // block 0 runs while block 1 is captured
-    if (!step(i, st, nullptr, B)) return false;
+  // Block 0 runs while block 1 is captured.  Profiled steps outside the
+  // replayed blocks (block 0, the tail) are not timed: only graph-launched
+  // kernels are sampled on this path.
+  for (int64_t i = 0; i < B; ++i)
+    if (!step(i, st, nullptr, B, false)) return false;
   GraphHold gh;
   gh.st = st;
   if (TB_CUDA(pool_malloc((void **)&gh.blk, sizeof(int64_t), st))) return false;
   if (TB_CUDA(cudaMemsetAsync(gh.blk, 0, sizeof(int64_t), st))) return false;
   if (TB_CUDA(cudaStreamCreateWithFlags(&gh.cs, cudaStreamNonBlocking))) return false;
-  if (TB_CUDA(cudaStreamBeginCapture(gh.cs, cudaStreamCaptureModeThreadLocal))) return false;
-  bool ok = true;
-  for (int64_t i = B; i < 2 * B && ok; ++i) ok = step(i, gh.cs, gh.blk, B);
-  if (ok) k_block_advance<<<1, 1, 0, gh.cs>>>(gh.blk);
   cudaGraph_t graph = nullptr;
-  const cudaError_t ec = cudaStreamEndCapture(gh.cs, &graph);
-  if (!ok || TB_CUDA(ec)) {
-    if (graph) cudaGraphDestroy(graph);
-    return false;
-  }
+  if (!capture_block(gh, B, step, prof, false, &graph)) return false;
   const cudaError_t ei = cudaGraphInstantiate(&gh.exec, graph, 0);
   cudaGraphDestroy(graph);
   if (TB_CUDA(ei)) return false;
+  if (prof.on()) {
+    if (!capture_block(gh, B, step, prof, true, &gh.timed_graph)) return false;
+    if (prof.bind(gh.timed_graph) &&
+        TB_CUDA(cudaGraphInstantiate(&gh.timed, gh.timed_graph, 0)))
+      return false;
+  }
   const int64_t nb = n / B;
   for (int64_t b = 1; b < nb; ++b) {
-    bool eager = false;
-    for (int64_t i = b * B; i < (b + 1) * B && !eager; ++i) eager = sampled(i);
-    if (!eager) {
-      if (TB_CUDA(cudaGraphLaunch(gh.exec, st))) return false;
-      g_graph_replays.fetch_add(1, std::memory_order_relaxed);
-      continue;
-    }
-    for (int64_t i = b * B; i < (b + 1) * B; ++i)
-      if (!step(i, st, nullptr, B)) return false;
-    k_block_advance<<<1, 1, 0, st>>>(gh.blk);
+    bool smp = false;
+    for (int64_t i = b * B; i < (b + 1) * B && !smp; ++i) smp = sampled(i);
+    const cudaGraphExec_t ge = smp && gh.timed && prof.arm(gh.timed) ? gh.timed : gh.exec;
+    if (TB_CUDA(cudaGraphLaunch(ge, st))) return false;
+    g_graph_replays.fetch_add(1, std::memory_order_relaxed);
   }
   count_launches(nb - 1);  // block advances
   for (int64_t i = nb * B; i < n; ++i)
-    if (!step(i, st, nullptr, B)) return false;
+    if (!step(i, st, nullptr, B, false)) return false;
   return !TB_CUDA(cudaGetLastError());
 }
+inline int64_t t_up(int64_t t0, int64_t i) { return t0 + i; }
+inline int64_t t_down(int64_t t0, int64_t i) { return t0 - 1 - i; }
 
 // ---------------------------------------------------------------------------
 // Fused stencil-2 FP32 forward (tm2d_fused.cuh) on a pitched internal copy of
@@ -775,9 +804,8 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
                     n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   ProfileScope prof(st);
-  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool smp) -> bool {
     const int64_t t = start_t + i;
-    const bool smp = !blk && prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKFwdH);
       launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
@@ -790,8 +818,7 @@ void tm_forward(TIDE_TM_FORWARD_ARGS(T)) {
     if (smp) prof.end(kKFwdE);
     return true;
   };
-  if (!run_step_blocks(nt, 1, st, step, [&](int64_t i) { return prof.sample(start_t + i); }))
-    return;
+  if (!run_step_blocks(nt, 1, st, prof, t_up, start_t, step)) return;
   count_launches(nt * (L.has_domain ? 2 : 1));
   TB_CUDA(cudaGetLastError());
 }
@@ -851,9 +878,8 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
     // Per-cell kernels; with the history on the device the step blocks are
     // replayed from a graph (run_step_blocks).
     const int64_t snap = sr.want ? (int64_t)(sr.step_bytes / (bf16 ? 2 : sizeof(T))) : 0;
-    auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+    auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool smp) -> bool {
       const int64_t t = start_t + i;
-      const bool smp = !blk && prof.sample(t);
       const bool store_step = sr.stores(t);
       char *dst[2];
       if (!sr.begin(t, dst)) return false;
@@ -877,11 +903,10 @@ void tm_forward_with_storage(TIDE_TM_FORWARD_WITH_STORAGE_ARGS(T)) {
       if (smp) prof.end(kKFwdE);
       return sr.end(t, dst);
     };
-    auto sampled = [&](int64_t i) { return prof.sample(start_t + i); };
     if (sr.host_side) {
       for (int64_t i = 0; i < nt; ++i)
-        if (!step(i, st, nullptr, 0)) return;
-    } else if (!run_step_blocks(nt, sr.want ? step_ratio : 1, st, step, sampled)) {
+        if (!step(i, st, nullptr, 0, prof.sample(start_t + i))) return;
+    } else if (!run_step_blocks(nt, sr.want ? step_ratio : 1, st, prof, t_up, start_t, step)) {
       return;
     }
     count_launches(nt * (L.has_domain ? 2 : 1));
@@ -1127,9 +1152,8 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
   // Per-cell kernels; with the history on the device (or none) the step
   // blocks are replayed from a graph (run_step_blocks).
   const int64_t snap = grads ? (int64_t)(step_bytes / esz) : 0;
-  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B) -> bool {
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool smp) -> bool {
     const int64_t t = start_t - 1 - i;
-    const bool smp = !blk && prof.sample(t);
     if (L.has_domain) {
       if (smp) prof.begin(kKAdjE);
       launch_adj_e<T, ST>(L, s, cb, lambda_ey, lambda_hx, lambda_hz, cur_hx_z, cur_hz_x,
@@ -1178,9 +1202,8 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
   if (!qpath) {
     if (host_side) {
       for (int64_t i = 0; i < nt; ++i)
-        if (!step(i, st, nullptr, 0)) return;
-    } else if (!run_step_blocks(nt, grads ? step_ratio : 1, st, step,
-                                [&](int64_t i) { return prof.sample(start_t - 1 - i); })) {
+        if (!step(i, st, nullptr, 0, prof.sample(start_t - 1 - i))) return;
+    } else if (!run_step_blocks(nt, grads ? step_ratio : 1, st, prof, t_down, start_t, step)) {
       return;
     }
   }

@@ -191,6 +191,7 @@ struct SrvEngine {
   int grid[4] = {0, 0, 0, 0};
   int64_t direct_cells = (int64_t)1 << 20;  // shots x cells of a large slot (< 0: none)
   bool fused = true;                        // fused forward step for eligible large slots
+  int n_pool = kSrvPool;  // streams the large slots are spread over (serve_set_direct_streams)
   cudaStream_t pool[kSrvPool] = {};
   cudaEvent_t ev_pool[kSrvPool] = {};
   std::vector<SrvHostSlot> slots;
@@ -470,7 +471,7 @@ int64_t tide_b200_serve_bind(void *engine, const TideServeJob *job, int64_t stre
   H.adjoint = adjoint;
   H.nt = J.nt;
   H.direct = E->direct_cells >= 0 && s.shot_cells >= E->direct_cells;
-  H.pool = slot % kSrvPool;
+  H.pool = slot % E->n_pool;
   H.L = L;
   H.src_i = J.n_src > 0 ? J.sources_i : nullptr;
   H.rec_i = J.n_rec > 0 ? J.receivers_i : nullptr;
@@ -709,6 +710,18 @@ int64_t tide_b200_serve_configure(void *engine, int64_t direct_cells, int64_t fu
   E->direct_cells = direct_cells;
   E->fused = fused != 0;
   return 0;
+}
+
+int64_t tide_b200_serve_set_direct_streams(void *engine, int64_t n) {
+  auto *E = static_cast<tb::SrvEngine *>(engine);
+  if (E == nullptr || n < 1 || n > tb::kSrvPool) {
+    tb::set_error(tb::kBadArgument, "serve set_direct_streams: null engine or n outside [1, %d]",
+                  tb::kSrvPool);
+    return -1;
+  }
+  const int prev = E->n_pool;
+  E->n_pool = (int)n;
+  return prev;
 }
 
 int64_t tide_b200_serve_launches(void *engine) {

@@ -304,5 +304,6 @@ def exported_symbols() -> list[str]:
         "tide_b200_serve_run",
         "tide_b200_serve_launches",
         "tide_b200_serve_configure",
+        "tide_b200_serve_set_direct_streams",
     ] + [f"tide_b200_tm_debye_{p}_{d}" for p in ("forward_with_storage", "backward")
          for d in ("float", "double")]

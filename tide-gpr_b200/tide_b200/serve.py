@@ -46,6 +46,7 @@ from . import tm2d
 IDLE, FORWARD, FORWARD_STORE, ADJOINT = 0, 1, 2, 3
 FLAG_FUSED = 1
 DIRECT_CELLS = 1 << 20  # shots x cells from which a group runs the per-call kernels
+DIRECT_STREAMS = 8  # streams of those groups
 
 
 class _CJob(ctypes.Structure):
@@ -80,6 +81,7 @@ def _lib():
             "tide_b200_serve_release": ([P, I], I),
             "tide_b200_serve_plan": ([P, I, I, I, I, P, P, I, I, I], I),
             "tide_b200_serve_configure": ([P, I, I], I),
+            "tide_b200_serve_set_direct_streams": ([P, I], I),
             "tide_b200_serve_run": ([P, I, I, I], I),
             "tide_b200_serve_launches": ([P], I),
         }
@@ -349,13 +351,16 @@ class TMServer:
     """Persistent request loop over the native serving engine (one GPU).
 
     memory_budget: device bytes for resident jobs (default 85 % of free
-    memory less 2 GiB for the library's per-call scratch); max_slots: resident shot groups; chunk_steps: time steps per
-    chunk (the continuous-batching granularity); use_graphs: replay a
-    captured CUDA graph per chunk; storage_compression: BF16 snapshots for
-    every gradient job of this server; history_limit / group_limit: planning
-    thresholds (default budget/8 and budget/4); direct_cells: shots x cells
-    from which a group runs the per-call kernels on its own stream (and, with
-    fused, the fused forward step) instead of the shared tile walk.
+    memory less 2 GiB for the library's per-call scratch); max_slots:
+    resident shot groups; chunk_steps: time steps per chunk (the
+    continuous-batching granularity); use_graphs: replay a captured CUDA
+    graph per chunk; storage_compression: BF16 snapshots for every gradient
+    job of this server; history_limit / group_limit: planning thresholds
+    (default budget/8 and budget/4); direct_cells: shots x cells from which a
+    group runs the per-call kernels on its own stream (and, with fused, the
+    fused forward step) instead of the shared tile walk; direct_streams: the
+    streams those groups are spread over (1: one after another, each with its
+    fields in L2 between its kernels).
     """
 
     def __init__(self, device: torch.device | str = "cuda", *, memory_budget: int | None = None,
@@ -363,7 +368,7 @@ class TMServer:
                  storage_compression: bool = False, history_limit: int | None = None,
                  group_limit: int | None = None, max_bypass: int = 8, depth: int = 2,
                  direct_cells: int = DIRECT_CELLS, fused: bool = True, priority: bool = True,
-                 max_weight: int = 4):
+                 max_weight: int = 4, direct_streams: int = DIRECT_STREAMS):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise nat.NativeError("TMServer runs on a CUDA device only")
@@ -392,6 +397,8 @@ class TMServer:
             raise nat.NativeError("serve create failed")
         self.lib.tide_b200_serve_configure(self.engine, int(direct_cells), int(fused))
         nat.check("serve configure")
+        if self.lib.tide_b200_serve_set_direct_streams(self.engine, int(direct_streams)) < 0:
+            nat.check("serve set_direct_streams")
         self.direct_cells = int(direct_cells)
         self.priority = bool(priority)
         self.max_weight = max(1, int(max_weight))
@@ -405,7 +412,8 @@ class TMServer:
         self.t0 = time.perf_counter()
         self.bypassed = 0
         self.chunks = 0
-        self.stats = {"admitted": 0, "chunks": 0, "max_resident": 0, "max_bytes": 0}
+        self.stats = {"admitted": 0, "chunks": 0, "max_resident": 0, "max_bytes": 0,
+                      "deferred_oom": 0}
 
     # -------------------------------------------------------------- public
 
@@ -498,10 +506,32 @@ class TMServer:
             [t.bytes for t in arrived], self.resident_bytes, len(self.resident), self.budget,
             self.max_slots, self.bypassed, self.max_bypass)
         for i in take:
-            self._load(arrived[i])
+            if not self._load_or_defer(arrived[i]):
+                break  # device memory is fragmented: the rest waits for a job to leave
             self.queue.remove(arrived[i])
         self.stats["max_resident"] = max(self.stats["max_resident"], len(self.resident))
         self.stats["max_bytes"] = max(self.stats["max_bytes"], self.resident_bytes)
+
+    def _load_or_defer(self, t: _Task) -> bool:
+        """Load a task admitted by the byte budget.  The budget counts bytes,
+        but torch's caching allocator can be too fragmented to place a large
+        block: then the cached blocks go back to the driver and the load is
+        tried once more; if it still fails the task stays queued while other
+        jobs are resident (False), and the error propagates when none is."""
+        for attempt in range(2):
+            try:
+                self._load(t)
+                return True
+            except torch.OutOfMemoryError:
+                t.out.clear()  # drop what the failed load allocated
+                torch.cuda.synchronize(self.device)
+                torch.cuda.empty_cache()
+                if attempt == 1 and self.resident:
+                    self.stats["deferred_oom"] += 1
+                    return False
+                if attempt == 1:
+                    raise
+        return False
 
     def _load(self, t: _Task) -> None:
         """Prepare a shot group on the device and bind it to a slot."""
