@@ -1001,7 +1001,7 @@ def main() -> None:
     ap.add_argument("--parity-shots", type=int, default=2)
     ap.add_argument("--parity-nt", type=int, default=250,
                     help="steps of the config-2 accuracy sample (0: skip)")
-    ap.add_argument("--profile-every", type=int, default=512,
+    ap.add_argument("--profile-every", type=int, default=2048,
                     help="time every n-th step's kernels with events in the timed region "
                          "(0: off; the roofline needs it); the 64-step block holding a timed "
                          "step runs as ordinary launches, the others replay a CUDA graph")

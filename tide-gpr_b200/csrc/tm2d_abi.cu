@@ -1152,6 +1152,9 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
   // Per-cell kernels; with the history on the device (or none) the step
   // blocks are replayed from a graph (run_step_blocks).
   const int64_t snap = grads ? (int64_t)(step_bytes / esz) : 0;
+  // one snapshot per shot: the kernel indexes snapshots by shot directly
+  // (GradArgs::snap_base skips its modulo)
+  const int ga_bg = bg_shots == n_shots ? 0 : bg_shots;
   auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool smp) -> bool {
     const int64_t t = start_t - 1 - i;
     if (L.has_domain) {
@@ -1179,13 +1182,13 @@ void tm_backward(TIDE_TM_BACKWARD_ARGS(T), int64_t background_n_shots) {
     if (bf16) {
       GradArgs<T, __nv_bfloat16> ga{(const __nv_bfloat16 *)es, (const __nv_bfloat16 *)cs,
                                     grad_ca, grad_cb, (T)step_ratio, ca_batched, cb_batched,
-                                    bg_shots};
+                                    ga_bg};
       launch_adj_h<T, ST, __nv_bfloat16>(L, s, ca, cq, lambda_hx, lambda_hz, lambda_ey,
                                          cur_ey_x, cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft,
                                          ga, sh);
     } else {
       GradArgs<T, T> ga{(const T *)es, (const T *)cs, grad_ca, grad_cb, (T)step_ratio,
-                        ca_batched, cb_batched, bg_shots};
+                        ca_batched, cb_batched, ga_bg};
       launch_adj_h<T, ST, T>(L, s, ca, cq, lambda_hx, lambda_hz, lambda_ey, cur_ey_x,
                              cur_ey_z, nxt_ey_x, nxt_ey_z, ps, grt, gft, ga, sh);
     }

@@ -727,9 +727,13 @@ class TMServer:
             js.pending -= 1
             if js.pending == 0:
                 self.completed.append(self._assemble(js))
-                # a finished job's blocks go back to the driver, where the
-                # library's per-call scratch (stream-ordered pool) can use them
-                torch.cuda.empty_cache()
+                # when torch's cache has grown past the budget (freed blocks
+                # kept by the caching allocator), a finished job's blocks go
+                # back to the driver, where the library's per-call scratch
+                # (stream-ordered pool) can use them; otherwise they stay
+                # cached (returning them synchronises the device)
+                if torch.cuda.memory_reserved(self.device) > self.budget:
+                    torch.cuda.empty_cache()
 
     def _assemble(self, js: _JobState) -> JobResult:
         job = js.job
