@@ -268,7 +268,8 @@ def run_b200(args) -> None:
     S_total = args.shots
     S_rank = int(tdist.rank_shot_indices(S_total, ctx=ctx, device="cpu").numel())
     batch = args.batch or shot_batches(S_rank, snap_bytes, dev)
-    compression = args.storage == "bf16"
+    # snapshot format and shot batch of the step (the BF16 leg switches them)
+    mode = {"compression": args.storage == "bf16", "batch": batch}
 
     # host (pinned) copies for the end-to-end leg, device copies for `value`
     host = {k: (v.pin_memory() if torch.is_tensor(v) else v) for k, v in cfg.items()}
@@ -285,14 +286,14 @@ def run_b200(args) -> None:
                 eps, sig, d["mu"], d["dx"], d["dt"], _shot_take(d["amp"], ids),
                 _shot_take(d["src"], ids), _shot_take(d["rec"], ids),
                 stencil=2, pml_width=d["pml"], storage_mode="device",
-                storage_compression=compression,
+                storage_compression=mode["compression"],
             )
             r = out[-1]
             loss = 0.5 * (r * r).sum()
             loss.backward()
             return loss.detach()
 
-        return sharded_gradient(d["eps"], d["sig"], S_total, batch, batch_fn, ctx)
+        return sharded_gradient(d["eps"], d["sig"], S_total, mode["batch"], batch_fn, ctx)
 
     def timed(n_steps, copy_in):
         if world > 1:
@@ -340,6 +341,47 @@ def run_b200(args) -> None:
     prof = read_profile(L)
     clk = clocks.stop()
     e2e_ms, h2d, d2h = timed(max(1, args.e2e_steps), copy_in=True)
+    # config 2's BF16 snapshot variant: the same step and shot batches with
+    # BF16 histories (half the snapshot bytes)
+    bf16_leg = None
+    if args.bf16_steps > 0 and args.storage == "fp32":
+        def fresh():  # the FP32 history goes back to the driver before the switch
+            torch.cuda.synchronize(dev)
+            stg.release_history_pool()
+            torch.cuda.empty_cache()
+
+        fresh()
+        mode.update(compression=True)
+        try:
+            step(dev_in, False)  # warm-up: allocates the BF16 history
+            torch.cuda.synchronize(dev)
+            L.tide_b200_profile_enable(1 if args.profile_every > 0 else 0,
+                                       max(1, args.profile_every))
+            read_profile(L)
+            b_ms, _, _ = timed(args.bf16_steps, copy_in=False)
+            L.tide_b200_profile_enable(0, 1)
+            bprof = read_profile(L)
+        except torch.OutOfMemoryError as exc:  # reported in the line; the rest still runs
+            L.tide_b200_profile_enable(0, 1)
+            bf16_leg = {"error": str(exc).splitlines()[0]}
+        finally:
+            mode.update(compression=False)
+            fresh()
+        if bf16_leg is None:
+            bk = {}
+            for k in ("fwd_h", "fwd_e", "adj_e", "adj_h"):
+                if bprof.get(k, (0, 0))[1] > 0:
+                    avg = bprof[k][0] / bprof[k][1]
+                    bpc = kernel_bytes_per_cell(k, batch, 2, 41 / PADDED[1], 41 / PADDED[0])
+                    gbs = bpc * batch * PADDED[0] * PADDED[1] / (avg / 1e3) / 1e9
+                    bk[k] = {"avg_launch_ms": round(avg, 5), "achieved_gbs": round(gbs, 1),
+                             "frac": round(gbs / hbm_peak()[0], 4)}
+            bf16_leg = {
+                "value": cell_updates(S_total, args.nt) * args.bf16_steps / (b_ms / 1e3),
+                "unit": UNIT, "steps": args.bf16_steps, "ms_per_step": b_ms / args.bf16_steps,
+                "shot_batch": batch, "kernels": bk,
+                "note": "same step and shot batches with BF16 snapshot histories; kernel "
+                        "fractions use 2-byte snapshots in the byte model"}
     # the same step with every time step launched from the host (no graphs)
     eager_ms = None
     if args.graphs_off_steps > 0:
@@ -425,7 +467,7 @@ def run_b200(args) -> None:
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "step_graphs": graphs,
             "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk,
-            "tma_path": tma_leg,
+            "tma_path": tma_leg, "bf16_snapshots": bf16_leg,
             "serving": serving, "serving_sweep": sweep,
             "em3d": em3d_leg, "debye": debye_leg,
         }
@@ -1005,6 +1047,9 @@ def main() -> None:
                     help="time every n-th step's kernels with events in the timed region "
                          "(0: off; the roofline needs it); the 64-step block holding a timed "
                          "step runs as ordinary launches, the others replay a CUDA graph")
+    ap.add_argument("--bf16-steps", type=int, default=2,
+                    help="steps timed with BF16 snapshot histories (config 2's BF16 variant; "
+                         "0: skip)")
     ap.add_argument("--graphs-off-steps", type=int, default=1,
                     help="steps timed again with the step graphs off (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=32,

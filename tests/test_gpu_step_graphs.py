@@ -173,3 +173,93 @@ def test_profiled_blocks_replay_a_timed_graph(cuda_device):
     times = _read_profile(lib)
     assert n_short == 0 and times["fwd_h"][1] == 2 and times["fwd_e"][1] == 2
     _same(base, prof, ("r", "Ey", "Hx", "Hz", "mEyx", "mEyz", "mHxz", "mHzx"))
+
+
+# ---------------------------------------------------------------- Born passes
+
+
+def _born_case(dev, nt=230, dtype=torch.float64, seed=21):
+    import tide_b200 as tide
+
+    g = torch.Generator().manual_seed(seed)
+    ny, nx, S = 32, 46, 2
+    eps = (2.0 + 4.0 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    sig = (0.005 * torch.rand((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev)
+    dx = 0.02
+    dt = 0.9 * dx / (tide.C0 / float(eps.min().sqrt()) * 2 ** 0.5)
+    return dict(
+        eps=eps, sig=sig, mu=torch.ones((ny, nx), device=dev, dtype=dtype), dx=dx, dt=dt,
+        amp=tide.ricker(500e6, nt, dt, dtype=dtype).view(1, 1, nt).repeat(S, 1, 1).to(dev),
+        src=torch.tensor([[[10, 12]], [[15, 30]]], device=dev),
+        rec=torch.tensor([[[5, 5 + 3 * j] for j in range(10)]] * S, device=dev),
+        deps=(0.3 * torch.randn((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev),
+        dsig=(1e-3 * torch.randn((ny, nx), generator=g, dtype=torch.float64)).to(dtype).to(dev),
+        w=torch.randn((nt, S, 10), generator=g, dtype=torch.float64).to(dtype).to(dev))
+
+
+def _borntm(c, deps, dsig, eps=None, sig=None):
+    import tide_b200 as tide
+
+    return tide.borntm(c["eps"] if eps is None else eps, c["sig"] if sig is None else sig,
+                       c["mu"], c["dx"], c["dt"], c["amp"], c["src"], c["rec"], c["rec"],
+                       depsilon=deps, dsigma=dsig, stencil=2, pml_width=8)
+
+
+def _with_graphs(on, fn):
+    n0 = nat.graph_replays()
+    with _Graphs(on):
+        out = fn()
+        torch.cuda.synchronize()
+    return out, nat.graph_replays() - n0
+
+
+def test_born_forward_graphs_bitwise(cuda_device):
+    c = _born_case(cuda_device)
+
+    def run():
+        with torch.no_grad():
+            return [t.clone() for t in _borntm(c, c["deps"], c["dsig"]) if t.numel()]
+
+    eager, n_eager = _with_graphs(False, run)
+    graph, n_graph = _with_graphs(True, run)
+    assert n_eager == 0 and n_graph == 230 // 64 - 1
+    _same(eager, graph, [f"born output {i}" for i in range(len(eager))])
+
+
+def test_born_storage_and_second_order_graphs_bitwise(cuda_device):
+    """Born forward with background and scattered histories (graph replay)
+    feeding the second-order adjoint: gradients in eps, sigma, deps, dsigma."""
+    c = _born_case(cuda_device)
+
+    def run():
+        leaves = [t.clone().requires_grad_() for t in (c["eps"], c["sig"], c["deps"], c["dsig"])]
+        r = _borntm(c, leaves[2], leaves[3], eps=leaves[0], sig=leaves[1])[-1]
+        (r * c["w"]).sum().backward()
+        return [r.detach()] + [t.grad for t in leaves]
+
+    eager, _ = _with_graphs(False, run)
+    graph, n_graph = _with_graphs(True, run)
+    assert n_graph >= 230 // 64 - 1  # the storing forward replays; adjoints as their paths allow
+    _same(eager, graph, ("r", "grad eps", "grad sigma", "grad deps", "grad dsigma"))
+
+
+def test_tangent_from_history_graphs_bitwise(cuda_device):
+    """MaxwellTM.linearize(...).jvp from the kept device history
+    (born_tangent_forward_with_storage) with and without graph replay."""
+    import tide_b200 as tide
+
+    c = _born_case(cuda_device)
+    op = tide.MaxwellTM(tide.Discretization(c["dx"], c["dt"], stencil=2, boundary=tide.CPML(8)),
+                        tide.Experiment(tide.Acquisition(c["src"], c["rec"]), c["amp"]))
+    v = tide.EMDirection(c["deps"], c["dsig"])
+
+    def run():
+        lin = op.linearize(tide.EMModel(c["eps"], c["sig"], c["mu"]))
+        out = lin._jvp_from_history(v)
+        assert out is not None
+        return [out.receiver_data.clone(), out.final_state.Ey.clone()]
+
+    eager, _ = _with_graphs(False, run)
+    graph, n_graph = _with_graphs(True, run)
+    assert n_graph >= 2 * (230 // 64 - 1)  # primal storing forward + tangent pass
+    _same(eager, graph, ("jvp receivers", "jvp final Ey"))

@@ -33,8 +33,19 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
          T *__restrict__ dey, T *__restrict__ dm_hx_z, T *__restrict__ dm_hz_x, PointCSR src,
          PointCSR rec, const T *__restrict__ f0_t, const T *__restrict__ df_t,
          T *__restrict__ r_t, T *__restrict__ bgr_t, S *__restrict__ es,
-         S *__restrict__ cs, S *__restrict__ des, S *__restrict__ dcs) {
+         S *__restrict__ cs, S *__restrict__ des, S *__restrict__ dcs, StepShift sh) {
   constexpr int P = FD<ST>::P;
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    f0_t = shifted(f0_t, sh.src, jb);
+    df_t = shifted(df_t, sh.src, jb);
+    r_t = shifted(r_t, sh.rec, jb);
+    bgr_t = shifted(bgr_t, sh.rec, jb);
+    es = shifted(es, sh.snap, jb);
+    cs = shifted(cs, sh.snap, jb);
+    des = shifted(des, sh.snap, jb);
+    dcs = shifted(dcs, sh.snap, jb);
+  }
   const int x = blockIdx.x * kTileX + threadIdx.x;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int s = blockIdx.z;
@@ -111,8 +122,17 @@ k_born_tangent_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb
                  T *__restrict__ dm_hx_z, T *__restrict__ dm_hz_x, const S *__restrict__ e_bg,
                  const S *__restrict__ c_bg, int bg_shots, PointCSR src, PointCSR rec,
                  const T *__restrict__ df_t, T *__restrict__ r_t, S *__restrict__ des,
-                 S *__restrict__ dcs) {
+                 S *__restrict__ dcs, StepShift sh) {
   constexpr int P = FD<ST>::P;
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    df_t = shifted(df_t, sh.src, jb);
+    r_t = shifted(r_t, sh.rec, jb);
+    e_bg = shifted(e_bg, sh.hist, jb);
+    c_bg = shifted(c_bg, sh.hist, jb);
+    des = shifted(des, sh.snap, jb);
+    dcs = shifted(dcs, sh.snap, jb);
+  }
   const int x = blockIdx.x * kTileX + threadIdx.x;
   const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
   const int s = blockIdx.z;
@@ -181,17 +201,21 @@ void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
                     sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
-  for (int64_t t = start_t; t < start_t + nt; ++t) {
+  ProfileScope prof(st);
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool) -> bool {
+    const int64_t t = start_t + i;
     if (L.has_domain) {
-      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
-      launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+      launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, s, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
     }
-    k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+    k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
         L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
         ps.src, ps.rec, f0 ? f0 + t * fs : nullptr, df ? df + t * fs : nullptr,
         r ? r + t * rs : nullptr, background_r ? background_r + t * rs : nullptr, nullptr,
-        nullptr, nullptr, nullptr);
-  }
+        nullptr, nullptr, nullptr, StepShift{blk, B * fs, B * rs, 0, 0});
+    return true;
+  };
+  if (!run_step_blocks(nt, 1, st, prof, t_up, start_t, step)) return;
   count_launches(nt * (L.has_domain ? 3 : 1));
   TB_CUDA(cudaGetLastError());
 }
@@ -227,9 +251,14 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
                     sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
-  for (int64_t t = start_t; t < start_t + nt; ++t) {
+  const int64_t snap =
+      sr.want ? (int64_t)(sr.step_bytes / (sr.bf16 ? sizeof(__nv_bfloat16) : sizeof(T))) : 0;
+  ProfileScope prof(st);
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool) -> bool {
+    const int64_t t = start_t + i;
+    const StepShift sh{blk, B * fs, B * rs, B / step_ratio * snap, 0};
     char *dst[2];
-    if (!sr.begin(t, dst)) return;
+    if (!sr.begin(t, dst)) return false;
     char *const e1 = dst[0], *const c1 = dst[1];
     // scattered history: device-resident, indexed by store index
     char *de1 = nullptr, *dc1 = nullptr;
@@ -239,22 +268,28 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
       if (dcurl_store) dc1 = (char *)dcurl_store + off;
     }
     if (L.has_domain) {
-      launch_fwd_h<T, ST>(L, st, cq, ey, hx, hz, m_ey_x, m_ey_z);
-      launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+      launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
+      launch_fwd_h<T, ST>(L, s, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
     }
     const T *f0t = f0 ? f0 + t * fs : nullptr, *dft = df ? df + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr, *bgt = background_r ? background_r + t * rs : nullptr;
     if (sr.stores(t) && sr.bf16) {
-      using B = __nv_bfloat16;
-      k_born_e<T, ST, B, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+      using BF = __nv_bfloat16;
+      k_born_e<T, ST, BF, kRowsE><<<L.grid_e, L.block, 0, s>>>(
           L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
-          ps.src, ps.rec, f0t, dft, rt, bgt, (B *)e1, (B *)c1, (B *)de1, (B *)dc1);
+          ps.src, ps.rec, f0t, dft, rt, bgt, (BF *)e1, (BF *)c1, (BF *)de1, (BF *)dc1, sh);
     } else {
-      k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
+      k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
           L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
-          ps.src, ps.rec, f0t, dft, rt, bgt, (T *)e1, (T *)c1, (T *)de1, (T *)dc1);
+          ps.src, ps.rec, f0t, dft, rt, bgt, (T *)e1, (T *)c1, (T *)de1, (T *)dc1, sh);
     }
-    if (!sr.end(t, dst)) return;
+    return sr.end(t, dst);
+  };
+  if (sr.host_side) {
+    for (int64_t i = 0; i < nt; ++i)
+      if (!step(i, st, nullptr, 0, false)) return;
+  } else if (!run_step_blocks(nt, sr.want ? step_ratio : 1, st, prof, t_up, start_t, step)) {
+    return;
   }
   count_launches(nt * (L.has_domain ? 3 : 1));
   if (TB_CUDA(cudaGetLastError())) return;
@@ -297,25 +332,32 @@ void tm_born_tangent_forward_with_storage(TIDE_TM_BORN_TANGENT_ARGS(T)) {
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   const int64_t bg_step = background_n_shots * ny * nx, sc_step = n_shots * ny * nx;
-  for (int64_t t = start_t; t < start_t + nt; ++t) {
-    if (L.has_domain) launch_fwd_h<T, ST>(L, st, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
+  ProfileScope prof(st);
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool) -> bool {
+    const int64_t t = start_t + i;
+    const StepShift sh{blk, B * fs, B * rs, B * sc_step, B * bg_step};
+    if (L.has_domain) launch_fwd_h<T, ST>(L, s, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
     const T *dft = df ? df + t * fs : nullptr;
     T *rt = r ? r + t * rs : nullptr;
     if (bf16) {
-      using B = __nv_bfloat16;
-      k_born_tangent_e<T, ST, B, kRowsE><<<L.grid_e, L.block, 0, st>>>(
-          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x, (const B *)ey_store + t * bg_step,
-          (const B *)curl_store + t * bg_step, (int)background_n_shots, ps.src, ps.rec, dft, rt,
-          dey_store ? (B *)dey_store + t * sc_step : nullptr,
-          dcurl_store ? (B *)dcurl_store + t * sc_step : nullptr);
+      using BF = __nv_bfloat16;
+      k_born_tangent_e<T, ST, BF, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x,
+          (const BF *)ey_store + t * bg_step, (const BF *)curl_store + t * bg_step,
+          (int)background_n_shots, ps.src, ps.rec, dft, rt,
+          dey_store ? (BF *)dey_store + t * sc_step : nullptr,
+          dcurl_store ? (BF *)dcurl_store + t * sc_step : nullptr, sh);
     } else {
-      k_born_tangent_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, st>>>(
-          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x, (const T *)ey_store + t * bg_step,
-          (const T *)curl_store + t * bg_step, (int)background_n_shots, ps.src, ps.rec, dft, rt,
+      k_born_tangent_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+          L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x,
+          (const T *)ey_store + t * bg_step, (const T *)curl_store + t * bg_step,
+          (int)background_n_shots, ps.src, ps.rec, dft, rt,
           dey_store ? (T *)dey_store + t * sc_step : nullptr,
-          dcurl_store ? (T *)dcurl_store + t * sc_step : nullptr);
+          dcurl_store ? (T *)dcurl_store + t * sc_step : nullptr, sh);
     }
-  }
+    return true;
+  };
+  if (!run_step_blocks(nt, 1, st, prof, t_up, start_t, step)) return;
   count_launches(nt * (L.has_domain ? 2 : 1));
   TB_CUDA(cudaGetLastError());
 }

@@ -66,6 +66,7 @@ struct StepShift {
   int64_t src = 0;   // source amplitudes (forward) / their gradient (adjoint)
   int64_t rec = 0;   // receiver records (forward) / their gradient (adjoint)
   int64_t snap = 0;  // snapshot slots
+  int64_t hist = 0;  // slots of a stored history the step reads (Born tangent)
   __device__ __forceinline__ int64_t block() const { return blk ? *blk : 0; }
 };
 template <typename P>
