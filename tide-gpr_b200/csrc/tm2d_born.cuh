@@ -430,7 +430,12 @@ __global__ void k_bg_prep(TMGeom<T> g, const T *__restrict__ ca, const T *__rest
 template <typename T, typename S>
 __global__ void k_image_bg(TMGeom<T> g, const T *__restrict__ lam, const S *__restrict__ e_st,
                            const S *__restrict__ c_st, T *__restrict__ gdca,
-                           T *__restrict__ gdcb, T kscale, int bg_shots, int p) {
+                           T *__restrict__ gdcb, T kscale, int bg_shots, int p, StepShift sh) {
+  if (sh.blk) {
+    const int64_t jb = sh.block();
+    e_st = shifted(e_st, sh.snap, jb);
+    c_st = shifted(c_st, sh.snap, jb);
+  }
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
   if (x < p || x >= g.nx - p + 1 || y < p || y >= g.ny - p + 1) return;
@@ -515,12 +520,20 @@ void tm_born_backward_bggrad(TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
   const size_t bstep = (size_t)shot_bytes_uncomp * (size_t)bg;       // background history step
   const size_t sstep = (size_t)shot_bytes_uncomp * (size_t)n_shots;  // scattered history step
+  const int64_t bsnap = (int64_t)(bstep / esz), ssnap = (int64_t)(sstep / esz);
   int64_t launches = 1;
-  for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
-    k_bg_prep<T><<<pgrid, pblk, 0, st>>>(L.g, ca, cb, dca, dcb, ey, dey, w, p);
+  ProfileScope prof(st);
+  // step i of the call (time step start_t - 1 - i); the block pointers move
+  // down (the adjoint walks the steps backwards)
+  auto step = [&](int64_t i, cudaStream_t s, const int64_t *blk, int64_t B, bool) -> bool {
+    const int64_t t = start_t - 1 - i;
+    const int64_t qb = -(B / step_ratio);
+    const StepShift sh_bg{blk, -B * fs, -B * rs, qb * bsnap, 0};
+    const StepShift sh_sc{blk, -B * fs, -B * rs, qb * ssnap, 0};
+    k_bg_prep<T><<<pgrid, pblk, 0, s>>>(L.g, ca, cb, dca, dcb, ey, dey, w, p);
     if (L.has_domain) {
-      launch_adj_e<T, ST>(L, st, cb, ey, hx, hz, lc[2], lc[3], ln[2], ln[3]);
-      launch_adj_e<T, ST>(L, st, ones, w, dhx, dhz, ec[2], ec[3], en[2], en[3]);
+      launch_adj_e<T, ST>(L, s, cb, ey, hx, hz, lc[2], lc[3], ln[2], ln[3]);
+      launch_adj_e<T, ST>(L, s, ones, w, dhx, dhz, ec[2], ec[3], en[2], en[3]);
     }
     for (int m = 2; m < 4; ++m) {
       std::swap(lc[m], ln[m]);
@@ -540,15 +553,16 @@ void tm_born_backward_bggrad(TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {
       using SN_T = decltype(tag);
       GradArgs<T, SN_T> ge{(const SN_T *)es, (const SN_T *)cs, grad_ca, grad_cb,
                            (T)step_ratio, ca_batched, cb_batched, bg};
-      launch_adj_h<T, ST, SN_T>(L, st, ones, cq, dhx, dhz, dey, ec[0], ec[1], en[0], en[1], ps,
-                                gbr, gf0, ge);
+      launch_adj_h<T, ST, SN_T>(L, s, ones, cq, dhx, dhz, dey, ec[0], ec[1], en[0], en[1], ps,
+                                gbr, gf0, ge, sh_bg);
       GradArgs<T, SN_T> gl{(const SN_T *)des, (const SN_T *)dcs, grad_ca, grad_cb,
                            (T)step_ratio, ca_batched, cb_batched, 0};
-      launch_adj_h<T, ST, SN_T>(L, st, ca, cq, hx, hz, ey, lc[0], lc[1], ln[0], ln[1], ps, grt,
-                                gdf, gl);
+      launch_adj_h<T, ST, SN_T>(L, s, ca, cq, hx, hz, ey, lc[0], lc[1], ln[0], ln[1], ps, grt,
+                                gdf, gl, sh_sc);
       if (grad_step)
-        k_image_bg<T, SN_T><<<igrid, pblk, 0, st>>>(L.g, ey, (const SN_T *)es, (const SN_T *)cs,
-                                                    grad_dca, grad_dcb, (T)step_ratio, bg, p);
+        k_image_bg<T, SN_T><<<igrid, pblk, 0, s>>>(L.g, ey, (const SN_T *)es, (const SN_T *)cs,
+                                                   grad_dca, grad_dcb, (T)step_ratio, bg, p,
+                                                   sh_bg);
     };
     if (bf16) both_h(__nv_bfloat16(0.f));
     else both_h(T(0));
@@ -556,8 +570,12 @@ void tm_born_backward_bggrad(TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {
       std::swap(lc[m], ln[m]);
       std::swap(ec[m], en[m]);
     }
-    launches += 3 + (L.has_domain ? 2 : 0) + (grad_step ? 1 : 0);
-  }
+    return true;
+  };
+  if (!run_step_blocks(nt, step_ratio, st, prof, t_down, start_t, step)) return;
+  // launches: 3 (+2 with a domain) per step and the image pass of each stored step
+  for (int64_t t = start_t - 1; t >= start_t - nt; --t)
+    launches += 3 + (L.has_domain ? 2 : 0) + (t % step_ratio == 0 ? 1 : 0);
   // leave the final memories in the caller's arrays
   const size_t nb = SN * sizeof(T);
   if (lc[0] != m_lambda_ey_x)
