@@ -666,7 +666,8 @@ int tide_b200_set_tma_ctas(int max_ctas);
 
 /* Step blocks replayed from CUDA graphs (new; no reference counterpart): the
  * TM2D forward, forward_with_storage and backward of the per-cell kernels and
- * the Born forward, born_forward_with_storage and tangent passes, with the
+ * the Born forward, born_forward_with_storage, tangent and
+ * born_backward_bggrad passes, with the
  * snapshot history on the device or none, run a call of at least
  * three blocks (64 steps, or the next multiple of the even snapshot
  * interval) as one captured graph replayed per block instead of two launches
