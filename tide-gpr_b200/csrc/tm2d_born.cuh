@@ -489,6 +489,7 @@ void tm_born_backward_bggrad(TIDE_TM_BORN_BACKWARD_BGGRAD_ARGS(T)) {
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
+  L.narrow_e();
   cudaStream_t st = as_stream(compute_stream);
   const size_t SN = (size_t)n_shots * (size_t)L.g.N;
   const int bg = (int)background_n_shots;

@@ -139,7 +139,7 @@ k2_fwd_h(TMGeom<T> g, const T *__restrict__ cq, const T *__restrict__ ey, T *__r
 
 // ---------------------------------------------------------------- forward E
 // Full-grid tiles (32 x 8R) so point entries outside the domain are served.
-template <typename T, typename S, int R, typename TL>
+template <typename T, typename S, int R, int BY = kBlockY, typename TL>
 __device__ __forceinline__ void fwd_e_tile(
     const TL tl, const TMGeom<T> &g,
     const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
@@ -148,7 +148,7 @@ __device__ __forceinline__ void fwd_e_tile(
     PointCSR src, PointCSR rec, const T *__restrict__ f_t, T *__restrict__ r_t) {
   const int nx = g.nx, ny = g.ny;
   const int x = tl.x() * kTileX + threadIdx.x;
-  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R;
+  const int y0 = (tl.y() * BY + threadIdx.y) * R;
   const int s = tl.z();
   const int tile = (s * tl.gy() + tl.y()) * tl.gx() + tl.x();
   if (y0 >= ny || x >= nx) return;
@@ -162,9 +162,9 @@ __device__ __forceinline__ void fwd_e_tile(
   const int j0 = y0 * nx + x;
   {
     // Interior tile (block-uniform): no strip cell, every cell in the domain.
-    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * kBlockY * R;
+    const int tx0 = tl.x() * kTileX, ty0 = tl.y() * BY * R;
     if (tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1 && ty0 >= g.pml_y0 &&
-        ty0 + kBlockY * R <= g.pml_y1) {
+        ty0 + BY * R <= g.pml_y1) {
       T vx[R + 1], vz[R], vzl[R], eo[R], a[R], b[R];
 #pragma unroll
       for (int r = 0; r <= R; ++r) vx[r] = ldg(hx + j0 + (r - 1) * nx);
@@ -252,8 +252,8 @@ __device__ __forceinline__ void fwd_e_tile(
     if (pts) point_record(rec, tile, j, r_t, e);
   }
 }
-template <typename T, typename S, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, typename S, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k2_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
          const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
          T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
@@ -266,15 +266,15 @@ k2_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const 
     ey_store = shifted(ey_store, sh.snap, jb);
     curl_store = shifted(curl_store, sh.snap, jb);
   }
-  fwd_e_tile<T, S, R>(HwTile(), g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, ey_store, curl_store, src,
-      rec, f_t, r_t);
+  fwd_e_tile<T, S, R, BY>(HwTile(), g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, ey_store, curl_store,
+      src, rec, f_t, r_t);
 }
 
 // ---------------------------------------------------------------- adjoint E
 // raw_x(x') = q (x' in [pml_x0, pml_x1)) or ax (bx m + q) + q / kx;
 // raw_y(y') = -q (y' in [pml_y0, pml_y1)) or ay (by m - q) - q / ky; both 0
 // outside the domain (maxwell_tm_cuda_inst.cu:954-994).
-template <typename T, int R, typename TL>
+template <typename T, int R, int BY = kBlockY, typename TL>
 __device__ __forceinline__ void adj_e_tile(
     const TL tl, const TMGeom<T> &g,
     const T *__restrict__ cb, const T *__restrict__ lam_ey,
@@ -282,7 +282,7 @@ __device__ __forceinline__ void adj_e_tile(
     const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
   const int nx = g.nx, ny = g.ny;
   const int x = tl.x() * kTileX + threadIdx.x + 1;
-  const int y0 = (tl.y() * kBlockY + threadIdx.y) * R + 1;
+  const int y0 = (tl.y() * BY + threadIdx.y) * R + 1;
   if (y0 >= ny || x >= nx) return;
   const int64_t base = (int64_t)tl.z() * g.N;
   lam_ey += base; lam_hx += base; lam_hz += base;
@@ -291,9 +291,9 @@ __device__ __forceinline__ void adj_e_tile(
   {
     // Interior tile (block-uniform): cells and their +1 neighbours outside
     // the strips, so raw_x = q and raw_y = -q throughout.
-    const int tx0 = tl.x() * kTileX + 1, ty0 = tl.y() * kBlockY * R + 1;
+    const int tx0 = tl.x() * kTileX + 1, ty0 = tl.y() * BY * R + 1;
     if (tx0 >= g.pml_x0 && tx0 + kTileX < g.pml_x1 && ty0 >= g.pml_y0 &&
-        ty0 + kBlockY * R < g.pml_y1) {
+        ty0 + BY * R < g.pml_y1) {
       const int j0 = y0 * nx + x;
       T lq[R + 1], cq_[R + 1], lr[R], cr[R], vx[R], vz[R];
 #pragma unroll
@@ -406,12 +406,13 @@ __device__ __forceinline__ void adj_e_tile(
     lam_hx[j] = vx[r] + ay_ * g.rdy;
   }
 }
-template <typename T, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k2_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
          T *__restrict__ lam_hx, T *__restrict__ lam_hz, const T *__restrict__ m_hx_z,
          const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
-  adj_e_tile<T, R>(HwTile(), g, cb, lam_ey, lam_hx, lam_hz, m_hx_z, m_hz_x, m_hx_z_n, m_hz_x_n);
+  adj_e_tile<T, R, BY>(HwTile(), g, cb, lam_ey, lam_hx, lam_hz, m_hx_z, m_hz_x, m_hx_z_n,
+      m_hz_x_n);
 }
 
 // ---------------------------------------------------------------- adjoint H
