@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import gc
 import json
 import math
 import os
@@ -347,6 +348,7 @@ def run_b200(args) -> None:
     if args.bf16_steps > 0 and args.storage == "fp32":
         def fresh():  # the FP32 history goes back to the driver before the switch
             torch.cuda.synchronize(dev)
+            gc.collect()
             stg.release_history_pool()
             torch.cuda.empty_cache()
 
@@ -432,7 +434,12 @@ def run_b200(args) -> None:
     if rank == 0 and world == 1 and args.tma_nt > 0:
         tma_leg = tma_bench(args, dev, batch, snap_bytes)
     serving = em3d_leg = debye_leg = None
-    stg.release_history_pool()  # the other legs budget device memory themselves
+    # the other legs budget device memory themselves: kept histories (some
+    # held only by reference cycles until a collection) go back to the driver
+    torch.cuda.synchronize(dev)
+    gc.collect()
+    stg.release_history_pool()
+    torch.cuda.empty_cache()
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         serving = serve_bench(args)
     sweep = None

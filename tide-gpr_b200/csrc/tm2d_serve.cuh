@@ -473,6 +473,7 @@ int64_t tide_b200_serve_bind(void *engine, const TideServeJob *job, int64_t stre
   H.direct = E->direct_cells >= 0 && s.shot_cells >= E->direct_cells;
   H.pool = slot % E->n_pool;
   H.L = L;
+  if (H.direct) H.L.narrow_e();  // the per-call E kernels' block shape
   H.src_i = J.n_src > 0 ? J.sources_i : nullptr;
   H.rec_i = J.n_rec > 0 ? J.receivers_i : nullptr;
   H.n_src = J.n_src;
@@ -489,8 +490,10 @@ int64_t tide_b200_serve_bind(void *engine, const TideServeJob *job, int64_t stre
     s.grad_ca = J.grad_ca;
     s.grad_cb = J.grad_cb;
   }
-  // Tile lists: E tiling (forward) and, for the adjoint, adjoint-H tiling.
-  const PointTiles pe{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0};
+  // Tile lists: E tiling (forward; the table walk's, or for a large slot that
+  // of the per-call E kernel) and, for the adjoint, adjoint-H tiling.
+  const PointTiles pe = H.direct ? H.L.e_tiles()
+                                 : PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0};
   const PointTiles ph = L.ah_tiles();  // 8-warp blocks: the table's tiling
   auto words = [&](const PointTiles &pt, int64_t per) -> size_t {
     if (per <= 0) return 0;

@@ -28,6 +28,7 @@ given); results are returned on the host.
 from __future__ import annotations
 
 import ctypes
+import gc
 import math
 import time
 from collections import deque
@@ -374,9 +375,14 @@ class TMServer:
             raise nat.NativeError("TMServer runs on a CUDA device only")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
-        # the server budgets device memory itself: a history kept for reuse by
-        # earlier gradient calls goes back to torch first
+        # the server budgets device memory itself from the free memory: the
+        # histories of earlier gradient calls (some held only by reference
+        # cycles until a collection) and torch's cached blocks go back to the
+        # driver first
+        gc.collect()
         stg.release_history_pool()
+        torch.cuda.synchronize(self.device)
+        torch.cuda.empty_cache()
         self.fmt, self.sdtype = stg.compression_format(storage_compression, torch.float32)
         self.item = self.sdtype.itemsize
         if memory_budget is None:
