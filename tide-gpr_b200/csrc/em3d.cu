@@ -26,6 +26,7 @@
 // update domain stay zero).
 #include <algorithm>
 #include <utility>
+#include <vector>
 
 #include <cuda_bf16.h>
 
@@ -1214,7 +1215,6 @@ void em3d_forward_with_storage(TIDE_3D_FORWARD_WITH_STORAGE_ARGS(T)) {
 template <typename T, int ST>
 void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   (void)n_threads;
-  (void)storage_stream;
   if (TB_CUDA(cudaSetDevice((int)device))) return;
   TB_REQUIRE(nt >= 0 && step_ratio >= 1, "3-D backward: bad nt/step_ratio");
   TB_REQUIRE(start_t - nt >= 0, "3-D backward: start_t - nt must be >= 0");
@@ -1313,6 +1313,62 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   const size_t step_bytes = (size_t)shot_bytes_uncomp * (size_t)n_shots;
   const int S_ = (int)n_shots;
   int64_t launches = 0;
+  // cpu / disk modes: stored step q comes back through device ring slot
+  // q % kStoreRing, loaded two stored steps ahead of its use.  With a storage
+  // stream of its own the host-to-device copies run there, overlapping the
+  // adjoint kernels: `loaded` orders a slot's reader after its copy and
+  // `consumed` the next copy into the slot after its reader.
+  const bool host_side = (need_ca || need_cb) && (storage_mode == 1 || storage_mode == 2);
+  cudaStream_t ss = stream_of(storage_stream);
+  const bool pipeline = host_side && ss != nullptr && ss != st;
+  std::vector<int64_t> qs;  // stored steps of this call, latest first
+  if (host_side)
+    for (int64_t t = start_t - 1; t >= start_t - nt; --t)
+      if (t % step_ratio == 0) qs.push_back(t / step_ratio);
+  EventRing loaded, consumed;
+  if (pipeline) {
+    if (!loaded.ok || !consumed.ok) {
+      set_error(kCudaError, "3-D: event creation failed");
+      return;
+    }
+    for (int k = 0; k < kStoreRing; ++k)
+      if (TB_CUDA(cudaEventRecord(consumed.ev[k], st))) return;
+  }
+  auto load = [&](size_t n) -> bool {
+    if (n >= qs.size()) return true;
+    const int64_t q = qs[n];
+    const int ring = (int)(q % kStoreRing);
+    cudaStream_t ls = pipeline ? ss : st;
+    if (pipeline && TB_CUDA(cudaStreamWaitEvent(ss, consumed.ev[ring], 0))) return false;
+    // disk mode: the staging slot is rewritten here, so its previous copy
+    // to the device must have run
+    if (storage_mode == 2 && staged_used[ring] && TB_CUDA(cudaEventSynchronize(staged.ev[ring])))
+      return false;
+    for (int c = 0; c < 6; ++c) {
+      if (!need[c]) continue;
+      char *slot = (char *)s1[c] + (size_t)ring * step_bytes;
+      const char *host = (const char *)s3[c] + (size_t)q * step_bytes;
+      if (storage_mode == 2) {
+        char *stage = (char *)s3[c] + (size_t)ring * step_bytes;
+        if (!disk[c]->read(stage, step_bytes, (int64_t)(q * step_bytes))) {
+          set_error(kCudaError, "3-D disk storage: %s", disk[c]->error().c_str());
+          return false;
+        }
+        host = stage;
+      }
+      if (TB_CUDA(cudaMemcpyAsync(slot, host, step_bytes, cudaMemcpyHostToDevice, ls)))
+        return false;
+    }
+    if (storage_mode == 2) {
+      if (TB_CUDA(cudaEventRecord(staged.ev[ring], ls))) return false;
+      staged_used[ring] = true;
+    }
+    return !(pipeline && TB_CUDA(cudaEventRecord(loaded.ev[ring], ss)));
+  };
+  size_t next_n = 0;
+  for (size_t n = 0; n < 2; ++n)
+    if (!load(n)) return;
+  int pending_ring = 0;
   ProfileScope ps(st);
   // The coefficient-gradient term of a stored step t reads lambda_E as it
   // stands after step t's receivers, which is what the adjoint E launch of
@@ -1347,10 +1403,16 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   for (int64_t t = start_t - 1; t >= start_t - nt; --t) {
     const bool smp = ps.sample(t);
     if (smp) ps.begin(kK3AdjE);
+    const bool consumes = has_pending;
     if (has_pending && bf16) launch_adj_e(__nv_bfloat16(0.f));
     else launch_adj_e(T(0));
     has_pending = false;
     if (smp) ps.end(kK3AdjE);
+    if (consumes && host_side) {  // the slot just read takes the history two stored steps on
+      if (pipeline && TB_CUDA(cudaEventRecord(consumed.ev[pending_ring], st))) return;
+      ++next_n;
+      if (!load(next_n + 1)) return;
+    }
     if (smp) ps.begin(kK3AdjH);
     if constexpr (ST == 2)
       k3_adj_h<T><<<L.grid, L.block, 0, st>>>(g, ca, cq, lambda_hx, lambda_hy, lambda_hz,
@@ -1376,39 +1438,14 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
     if ((need_ca || need_cb) && (t % step_ratio) == 0) {
       const int64_t q = t / step_ratio;
       const int ring = (int)(q % kStoreRing);
-      const char *src[6];
-      if (storage_mode == 2 && staged_used[ring]) {
-        // the staging slot is rewritten below: its previous copy must be done
-        if (TB_CUDA(cudaEventSynchronize(staged.ev[ring]))) return;
-      }
-      for (int c = 0; c < 6; ++c) {
-        src[c] = nullptr;
-        if (!need[c]) continue;
-        if (storage_mode == 1 || storage_mode == 2) {
-          // bring the host (cpu) or file (disk, through a staging slot)
-          // history back through a device ring slot
-          char *slot = (char *)s1[c] + (size_t)ring * step_bytes;
-          const char *host = (const char *)s3[c] + (size_t)q * step_bytes;
-          if (storage_mode == 2) {
-            char *stage = (char *)s3[c] + (size_t)ring * step_bytes;
-            if (!disk[c]->read(stage, step_bytes, (int64_t)(q * step_bytes))) {
-              set_error(kCudaError, "3-D disk storage: %s", disk[c]->error().c_str());
-              return;
-            }
-            host = stage;
-          }
-          if (TB_CUDA(cudaMemcpyAsync(slot, host, step_bytes, cudaMemcpyHostToDevice, st)))
-            return;
-          src[c] = slot;
-        } else {
-          src[c] = (const char *)s1[c] + (size_t)q * step_bytes;
-        }
-      }
-      if (storage_mode == 2) {
-        if (TB_CUDA(cudaEventRecord(staged.ev[ring], st))) return;
-        staged_used[ring] = true;
-      }
-      for (int c = 0; c < 6; ++c) pending[c] = src[c];
+      // host modes: the slot loaded for q (its copy ordered before the
+      // reader); device mode: the history itself
+      if (pipeline && TB_CUDA(cudaStreamWaitEvent(st, loaded.ev[ring], 0))) return;
+      for (int c = 0; c < 6; ++c)
+        pending[c] = !need[c]    ? nullptr
+                     : host_side ? (const char *)s1[c] + (size_t)ring * step_bytes
+                                 : (const char *)s1[c] + (size_t)q * step_bytes;
+      pending_ring = ring;
       has_pending = true;
     }
     std::swap(cur, nxt);
@@ -1455,8 +1492,11 @@ void em3d_backward(TIDE_3D_BACKWARD_ARGS(T), bool compact = true) {
   }
   count_launches(launches);
   if (TB_CUDA(cudaGetLastError())) return;
-  if ((need_ca || need_cb) && (storage_mode == 1 || storage_mode == 2))
+  if (host_side) {
+    // the caller's staging and host buffers are free once the copies ran
+    if (pipeline && TB_CUDA(cudaStreamSynchronize(ss))) return;
     TB_CUDA(cudaStreamSynchronize(st));
+  }
 }
 
 // Snapshot plan of born_forward_with_storage: device base pointers of the

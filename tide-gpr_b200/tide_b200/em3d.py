@@ -372,7 +372,8 @@ def native_backward(pb: EM3DProblem, ca, cb, grad_r, sn: Snapshots3D, need_ca: b
        _p(grad_cb), _p(grad_eps), _p(grad_sigma), _p(shot_ca), _p(shot_cb), False,
        *_profile_ptrs(pb), _p(pb.sources_i), _p(pb.receivers_i),
        *_tail(pb, nt, max(1, pb.grad_interval)), sn.mode, sn.fmt, sn.shot_bytes, need_ca,
-       need_cb, *_flags(pb, start_t), stream, stream)
+       need_cb, *_flags(pb, start_t), stream,
+       sn.side.cuda_stream if sn.side is not None else stream)
     nat.check("maxwell_3d backward")
     return grad_ca, grad_cb, grad_f
 
