@@ -210,6 +210,7 @@ void debye_backward(const TideTMDebye &A) {
     return;
   PointScratch ps;
   if constexpr (ST == 2) pick_adj_h_rows<T, T>(L);
+  L.narrow_e();  // 4-warp adjoint E blocks (the adjoint E kernel has no point lists)
   if (!build_points(ps, L, L.ah_tiles(), A.sources_i, A.n_src, A.receivers_i, A.n_rec, st))
     return;
   const T *ca = static_cast<const T *>(A.ca), *cb = static_cast<const T *>(A.cb);
