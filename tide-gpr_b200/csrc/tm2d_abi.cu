@@ -436,6 +436,18 @@ struct PitchedFwd {
                                       (size_t)nx * 4, (size_t)nrows, cudaMemcpyDeviceToDevice,
                                       st));
   }
+  // Device bytes of the pitched copy of geometry g (state, memories,
+  // coefficients, guard rows).
+  static size_t bytes_for(const TMGeom<float> &g) {
+    const F4Geom q = f4_geom(g);
+    const int64_t rows = (int64_t)g.n_shots * g.ny;
+    size_t total = 12 * (size_t)(rows + 2) * q.pitch;
+    const int64_t rc[3] = {(g.ca_b ? g.n_shots : 1) * (int64_t)g.ny,
+                           (g.cb_b ? g.n_shots : 1) * (int64_t)g.ny,
+                           (g.cq_b ? g.n_shots : 1) * (int64_t)g.ny};
+    for (int i = 0; i < 3; ++i) total += (size_t)(rc[i] + 2) * q.pitch;
+    return total * sizeof(float);
+  }
   bool init(const TMGeom<float> &g, float *const fields[7], const float *ca_u,
             const float *cb_u, const float *cq_u, cudaStream_t s) {
     st = s;
@@ -450,8 +462,7 @@ struct PitchedFwd {
                            (g.cb_b ? g.n_shots : 1) * (int64_t)g.ny,
                            (g.cq_b ? g.n_shots : 1) * (int64_t)g.ny};
     const size_t state = (size_t)(rows + 2) * q.pitch;
-    size_t total = 12 * state;
-    for (int i = 0; i < 3; ++i) total += (size_t)(rc[i] + 2) * q.pitch;
+    const size_t total = bytes_for(g) / sizeof(float);
     if (TB_CUDA(pool_malloc(&mem, total * sizeof(float), st))) return false;
     if (TB_CUDA(cudaMemsetAsync(mem, 0, total * sizeof(float), st))) return false;
     float *p = static_cast<float *>(mem);

@@ -270,7 +270,18 @@ bool srv_direct(SrvHostSlot &H, cudaStream_t st, bool fused_enabled, int64_t &la
   pe.src = s.src_e; pe.rec = s.rec_e;
   pa.src = s.src_ah; pa.rec = s.rec_ah; pa.rowf = s.rowf_ah;
   const bool fwd = s.phase == TIDE_SERVE_FORWARD || s.phase == TIDE_SERVE_FORWARD_STORE;
-  const bool fused = fwd && H.fused_ok && fused_enabled && fused_pays(s.g.n_shots, s.g.N);
+  bool fused = fwd && H.fused_ok && fused_enabled && fused_pays(s.g.n_shots, s.g.N);
+  if (fused && !H.pf) {
+    // entering the fused phase needs a pitched copy of the slot's state; when
+    // the free device memory cannot take it (the caller's allocator may hold
+    // the rest) the slot runs the per-call pair, which gives the same bits
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess ||
+        free_b < PitchedFwd::bytes_for(s.g) + ((size_t)1 << 30)) {
+      cudaGetLastError();
+      fused = false;
+    }
+  }
   if (H.pf && !fused) {
     // leaving the fused phase: fields back to the caller's layout when a
     // forward follows, then the pitched copy goes

@@ -675,6 +675,10 @@ class TMServer:
             planned.append((t, n))
         if not planned:
             return
+        # the engine's own scratch (pitched copies, tile lists) comes from the
+        # driver: torch's cached blocks go back when the driver runs short
+        if torch.cuda.mem_get_info(self.device)[0] < (4 << 30):
+            torch.cuda.empty_cache()
         rc = self.lib.tide_b200_serve_run(self.engine, C, int(self.use_graphs),
                                           self.stream.cuda_stream)
         nat.check("serve run")
