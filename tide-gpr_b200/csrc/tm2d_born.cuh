@@ -24,8 +24,8 @@ namespace {
 // entries outside the update domain are still served.  Non-null store
 // pointers (this step's slots, type S) receive Ey^n, curl H^n, dEy^n and
 // dcurl H^n of the update domain.
-template <typename T, int ST, typename S, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, int ST, typename S, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
          const T *__restrict__ dca, const T *__restrict__ dcb, const T *__restrict__ hx,
          const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
@@ -47,7 +47,7 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
     dcs = shifted(dcs, sh.snap, jb);
   }
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
+  const int y0 = (blockIdx.y * BY + threadIdx.y) * R;
   const int s = blockIdx.z;
   const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   const bool pts = !point_tile_empty(src, rec, tile);
@@ -114,8 +114,8 @@ k_born_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
 // (maxwell_tm_core.cuh:691-743): Ey^n and curl H^n of background shot
 // s % bg_shots are read from this step's slots e_bg / c_bg (type S) instead
 // of being recomputed; then the scattered sources and receivers.
-template <typename T, int ST, typename S, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, int ST, typename S, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k_born_tangent_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb,
                  const T *__restrict__ dca, const T *__restrict__ dcb,
                  const T *__restrict__ dhx, const T *__restrict__ dhz, T *__restrict__ dey,
@@ -134,7 +134,7 @@ k_born_tangent_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb
     dcs = shifted(dcs, sh.snap, jb);
   }
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
+  const int y0 = (blockIdx.y * BY + threadIdx.y) * R;
   const int s = blockIdx.z;
   const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   const bool pts = !point_tile_empty(src, rec, tile);
@@ -180,6 +180,25 @@ k_born_tangent_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb
   }
 }
 
+// Born E launches with the block shape of L (Launch::narrow_e: 4-warp blocks
+// for stencil 2, whose point lists then follow L.e_tiles()).
+template <typename T, int ST, typename S, typename... A>
+inline void launch_born_e(const Launch<T, ST> &L, cudaStream_t s, A... a) {
+  constexpr int NB = Launch<T, ST>::kNarrowBY;
+  if (L.e_by == NB)
+    k_born_e<T, ST, S, kRowsE, NB><<<L.grid_e_n, dim3(kTileX, NB, 1), 0, s>>>(a...);
+  else
+    k_born_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, s>>>(a...);
+}
+template <typename T, int ST, typename S, typename... A>
+inline void launch_born_tangent_e(const Launch<T, ST> &L, cudaStream_t s, A... a) {
+  constexpr int NB = Launch<T, ST>::kNarrowBY;
+  if (L.e_by == NB)
+    k_born_tangent_e<T, ST, S, kRowsE, NB><<<L.grid_e_n, dim3(kTileX, NB, 1), 0, s>>>(a...);
+  else
+    k_born_tangent_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, s>>>(a...);
+}
+
 template <typename T, int ST>
 void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
   (void)dt; (void)step_ratio; (void)n_threads;
@@ -197,7 +216,8 @@ void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
     return;
   cudaStream_t st = as_stream(compute_stream);
   PointScratch ps;
-  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+  L.narrow_e();
+  if (!build_points(ps, L, L.e_tiles(),
                     sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
@@ -208,7 +228,7 @@ void tm_born_forward(TIDE_TM_BORN_FORWARD_ARGS(T)) {
       launch_fwd_h<T, ST>(L, s, cq, ey, hx, hz, m_ey_x, m_ey_z);
       launch_fwd_h<T, ST>(L, s, cq, dey, dhx, dhz, dm_ey_x, dm_ey_z);
     }
-    k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+    launch_born_e<T, ST, T>(L, s,
         L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
         ps.src, ps.rec, f0 ? f0 + t * fs : nullptr, df ? df + t * fs : nullptr,
         r ? r + t * rs : nullptr, background_r ? background_r + t * rs : nullptr, nullptr,
@@ -247,7 +267,8 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
                    ny, nx, pml_y0, pml_x0, pml_y1, pml_x1, ca_batched, cb_batched, cq_batched))
     return;
   PointScratch ps;
-  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+  L.narrow_e();
+  if (!build_points(ps, L, L.e_tiles(),
                     sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
@@ -275,11 +296,11 @@ void tm_born_forward_with_storage(TIDE_TM_BORN_FORWARD_WITH_STORAGE_ARGS(T)) {
     T *rt = r ? r + t * rs : nullptr, *bgt = background_r ? background_r + t * rs : nullptr;
     if (sr.stores(t) && sr.bf16) {
       using BF = __nv_bfloat16;
-      k_born_e<T, ST, BF, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+      launch_born_e<T, ST, BF>(L, s,
           L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
           ps.src, ps.rec, f0t, dft, rt, bgt, (BF *)e1, (BF *)c1, (BF *)de1, (BF *)dc1, sh);
     } else {
-      k_born_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+      launch_born_e<T, ST, T>(L, s,
           L.g, ca, cb, dca, dcb, hx, hz, ey, m_hx_z, m_hz_x, dhx, dhz, dey, dm_hx_z, dm_hz_x,
           ps.src, ps.rec, f0t, dft, rt, bgt, (T *)e1, (T *)c1, (T *)de1, (T *)dc1, sh);
     }
@@ -327,7 +348,8 @@ void tm_born_tangent_forward_with_storage(TIDE_TM_BORN_TANGENT_ARGS(T)) {
     return;
   cudaStream_t st = as_stream(compute_stream);
   PointScratch ps;
-  if (!build_points(ps, L, PointTiles{L.tiles_x, L.tiles_y_e, kTileX, kBlockY * kRowsE, 0},
+  L.narrow_e();
+  if (!build_points(ps, L, L.e_tiles(),
                     sources_i, n_sources_per_shot, receivers_i, n_receivers_per_shot, st))
     return;
   const int64_t fs = n_shots * n_sources_per_shot, rs = n_shots * n_receivers_per_shot;
@@ -341,14 +363,14 @@ void tm_born_tangent_forward_with_storage(TIDE_TM_BORN_TANGENT_ARGS(T)) {
     T *rt = r ? r + t * rs : nullptr;
     if (bf16) {
       using BF = __nv_bfloat16;
-      k_born_tangent_e<T, ST, BF, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+      launch_born_tangent_e<T, ST, BF>(L, s,
           L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x,
           (const BF *)ey_store + t * bg_step, (const BF *)curl_store + t * bg_step,
           (int)background_n_shots, ps.src, ps.rec, dft, rt,
           dey_store ? (BF *)dey_store + t * sc_step : nullptr,
           dcurl_store ? (BF *)dcurl_store + t * sc_step : nullptr, sh);
     } else {
-      k_born_tangent_e<T, ST, T, kRowsE><<<L.grid_e, L.block, 0, s>>>(
+      launch_born_tangent_e<T, ST, T>(L, s,
           L.g, ca, cb, dca, dcb, dhx, dhz, dey, dm_hx_z, dm_hz_x,
           (const T *)ey_store + t * bg_step, (const T *)curl_store + t * bg_step,
           (int)background_n_shots, ps.src, ps.rec, dft, rt,
