@@ -641,6 +641,12 @@ const char *tide_b200_profile_kind_name(int kind);
 /* Total kernels this library has launched in this process (monotonic). */
 int64_t tide_b200_launch_count(void);
 
+/* Per-call scratch comes from the device's default stream-ordered memory
+ * pool, which keeps up to 4 GiB of freed memory for later calls.  This waits
+ * for the device and returns all of it to the driver (for a caller that
+ * budgets device memory itself).  0 on success, -1 (status set) on error. */
+int tide_b200_release_scratch(int64_t device);
+
 /* Selection between the two stencil-2 FP32 forward implementations (new; no
  * reference counterpart).  A call whose three field arrays (3 * n_shots * ny
  * * nx * 4 bytes) exceed `bytes` runs the fused one-launch-per-step kernel;

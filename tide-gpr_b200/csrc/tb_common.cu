@@ -326,6 +326,15 @@ const char *tide_b200_profile_kind_name(int kind) {
 
 int64_t tide_b200_launch_count(void) { return tb::g_launches.load(); }
 
+int tide_b200_release_scratch(int64_t device) {
+  cudaMemPool_t pool;
+  if (TB_CUDA(cudaSetDevice((int)device)) || TB_CUDA(cudaDeviceSynchronize()) ||
+      TB_CUDA(cudaDeviceGetDefaultMemPool(&pool, (int)device)) ||
+      TB_CUDA(cudaMemPoolTrimTo(pool, 0)))
+    return -1;
+  return 0;
+}
+
 
 const char *tide_cuda_arches(void) { return "100a"; }
 

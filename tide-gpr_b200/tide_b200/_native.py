@@ -242,6 +242,15 @@ def set_step_graphs(on: bool) -> bool:
     return bool(lib.tide_b200_set_step_graphs(1 if on else 0))
 
 
+def release_scratch(device: torch.device) -> None:
+    """Return the library's cached per-call scratch on `device` to the driver."""
+    lib = load()
+    lib.tide_b200_release_scratch.argtypes = [c_int64]
+    lib.tide_b200_release_scratch.restype = c_int
+    if lib.tide_b200_release_scratch(device.index or 0) != 0:
+        check("release_scratch")
+
+
 def graph_replays() -> int:
     """Step-block graph replays issued so far by this process."""
     lib = load()
@@ -292,6 +301,7 @@ def exported_symbols() -> list[str]:
         "tide_b200_set_step_graphs",
         "tide_b200_graph_replays",
         "tide_b200_launch_count",
+        "tide_b200_release_scratch",
         "tide_b200_profile_enable",
         "tide_b200_profile_read",
         "tide_b200_profile_kind_name",

@@ -383,6 +383,7 @@ class TMServer:
         stg.release_history_pool()
         torch.cuda.synchronize(self.device)
         torch.cuda.empty_cache()
+        nat.release_scratch(self.device)
         self.fmt, self.sdtype = stg.compression_format(storage_compression, torch.float32)
         self.item = self.sdtype.itemsize
         if memory_budget is None:
