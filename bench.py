@@ -209,7 +209,7 @@ def kernel_bytes_per_cell(kind: str, S: int, snap_bytes: int, rho_x: float, rho_
 # DRAM bytes per cell (one shot, one step) moved by each kernel in an ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) on the config-2 grid
 # with 8-shot launches; None where not captured.
-TRAFFIC_B_PER_CELL = {"adj_h": 23.7}
+TRAFFIC_B_PER_CELL = {"adj_h": 23.6}
 
 
 def shot_batches(shots: int, snap_bytes: int, device) -> int:
