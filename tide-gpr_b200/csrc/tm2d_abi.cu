@@ -66,20 +66,20 @@ template <typename T, int ST> struct Launch {
     tiles_y_ah = (int)cdiv(g.ny, by * kRowsAH);
     grid_ah = dim3((unsigned)tiles_x, (unsigned)tiles_y_ah, 1);
   }
-  // 4-warp blocks for the stencil-2 E kernels of a per-call loop: on the
-  // 553 x 1065 grid at 8 shots the forward E kernel runs 34.2 against 38.2 us
-  // per launch and the adjoint E kernel 26.5 against 28.5 (the H kernels are
-  // faster with 8 warps).  Only stencil 2 without Debye poles has these
-  // kernels; the point lists of a call follow e_tiles().
+  // 4-warp blocks for the E and adjoint E kernels of a per-call loop: on the
+  // 553 x 1065 grid at 8 shots the stencil-2 forward E kernel runs 34.2
+  // against 38.2 us per launch and the adjoint E kernel 26.5 against 28.5;
+  // at stencil 4 the generic kernels 44.1 / 65.8 against 45.1 / 69.9, at
+  // stencil 8 50.1 / 131 against 51.1 / 135 (the H kernels are faster with
+  // 8 warps).  The point lists of a call follow e_tiles(); callers with
+  // Debye poles keep the 8-warp forward E launch.
   void narrow_e() {
-    if constexpr (ST == 2) {
-      constexpr int P = FD<ST>::P;
-      e_by = ae_by = kNarrowBY;
-      tiles_y_e_n = (int)cdiv(g.ny, kNarrowBY * kRowsE);
-      grid_e_n = dim3((unsigned)tiles_x, (unsigned)tiles_y_e_n, (unsigned)g.n_shots);
-      grid_ae_n = dim3(cdiv(g.nx - 2 * P + 1, kTileX), cdiv(g.ny - 2 * P + 1, kNarrowBY * kRowsAE),
-                       (unsigned)g.n_shots);
-    }
+    constexpr int P = FD<ST>::P;
+    e_by = ae_by = kNarrowBY;
+    tiles_y_e_n = (int)cdiv(g.ny, kNarrowBY * kRowsE);
+    grid_e_n = dim3((unsigned)tiles_x, (unsigned)tiles_y_e_n, (unsigned)g.n_shots);
+    grid_ae_n = dim3(cdiv(g.nx - 2 * P + 1, kTileX), cdiv(g.ny - 2 * P + 1, kNarrowBY * kRowsAE),
+                     (unsigned)g.n_shots);
   }
   static constexpr int kNarrowBY = 4;
 };
@@ -243,6 +243,9 @@ inline void launch_fwd_e(const Launch<T, ST> &L, cudaStream_t st, const T *ca, c
   else if (ST == 2 && db.n_poles == 0)
     k2_fwd_e<T, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x,
                                                          e_st, c_st, ps.src, ps.rec, ft, rt, sh);
+  else if (L.e_by == NB)
+    k_fwd_e<T, ST, S, kRowsE, NB><<<L.grid_e_n, dim3(kTileX, NB, 1), 0, st>>>(
+        L.g, ca, cb, hx, hz, ey, m_hx_z, m_hz_x, e_st, c_st, db, ps.src, ps.rec, ft, rt, sh);
   else
     k_fwd_e<T, ST, S, kRowsE><<<L.grid_e, L.block, 0, st>>>(L.g, ca, cb, hx, hz, ey, m_hx_z,
                                                             m_hz_x, e_st, c_st, db, ps.src,
@@ -268,6 +271,10 @@ inline void launch_adj_e(const Launch<T, ST> &L, cudaStream_t st, const T *cb, c
   else if (ST == 2)
     k2_adj_e<T, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(L.g, cb, lam, lhx, lhz, mz, mx, mz_n,
                                                         mx_n);
+  else if (L.ae_by == NB)
+    k_adj_e<T, ST, kRowsAE, NB><<<L.grid_ae_n, dim3(kTileX, NB, 1), 0, st>>>(L.g, cb, lam, lhx,
+                                                                             lhz, mz, mx, mz_n,
+                                                                             mx_n);
   else
     k_adj_e<T, ST, kRowsAE><<<L.grid_ae, L.block, 0, st>>>(L.g, cb, lam, lhx, lhz, mz, mx, mz_n,
                                                            mx_n);

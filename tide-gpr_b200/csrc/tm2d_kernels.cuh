@@ -348,8 +348,8 @@ __device__ __forceinline__ void fwd_e_fast(const TMGeom<T> &g, const T *__restri
 // (maxwell_tm_core.cuh:504-599, maxwell_tm_cuda_inst.cu:382-457,
 // maxwell.cu:89-141).  Grid covers the full [0,ny)x[0,nx) grid (tiles of 32 x
 // 8R) so points outside the update domain are still injected and recorded.
-template <typename T, int ST, typename S, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, int ST, typename S, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T *__restrict__ hx,
         const T *__restrict__ hz, T *__restrict__ ey, T *__restrict__ m_hx_z,
         T *__restrict__ m_hz_x, S *__restrict__ ey_store, S *__restrict__ curl_store,
@@ -364,15 +364,15 @@ k_fwd_e(TMGeom<T> g, const T *__restrict__ ca, const T *__restrict__ cb, const T
     curl_store = shifted(curl_store, sh.snap, jb);
   }
   const int x = blockIdx.x * kTileX + threadIdx.x;
-  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R;
+  const int y0 = (blockIdx.y * BY + threadIdx.y) * R;
   const int s = blockIdx.z;
   const int tile = (s * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   const bool pts = !point_tile_empty(src, rec, tile);
   const int64_t base = (int64_t)s * g.N;
   if constexpr (ST == 2) {
-    const int tx0 = blockIdx.x * kTileX, ty0 = blockIdx.y * kBlockY * R;
+    const int tx0 = blockIdx.x * kTileX, ty0 = blockIdx.y * BY * R;
     if (db.n_poles == 0 && tx0 >= g.pml_x0 && tx0 + kTileX <= g.pml_x1 && ty0 >= g.pml_y0 &&
-        ty0 + kBlockY * R <= g.pml_y1) {
+        ty0 + BY * R <= g.pml_y1) {
       fwd_e_fast<T, S, R>(g, g.ca_b ? ca + base : ca, g.cb_b ? cb + base : cb, hx + base,
                           hz + base, ey + base, ey_store ? ey_store + base : nullptr,
                           curl_store ? curl_store + base : nullptr, pts, src, rec, tile, f_t,
@@ -507,20 +507,20 @@ __device__ __forceinline__ void adj_e_fast(const TMGeom<T> &g, const T *__restri
   }
 }
 
-template <typename T, int ST, int R>
-__global__ void __launch_bounds__(256)
+template <typename T, int ST, int R, int BY = kBlockY>
+__global__ void __launch_bounds__(32 * BY)
 k_adj_e(TMGeom<T> g, const T *__restrict__ cb, const T *__restrict__ lam_ey,
         T *__restrict__ lam_hx, T *__restrict__ lam_hz, const T *__restrict__ m_hx_z,
         const T *__restrict__ m_hz_x, T *__restrict__ m_hx_z_n, T *__restrict__ m_hz_x_n) {
   constexpr int P = FD<ST>::P;
   const int x = blockIdx.x * kTileX + threadIdx.x + P;
-  const int y0 = (blockIdx.y * kBlockY + threadIdx.y) * R + P;
+  const int y0 = (blockIdx.y * BY + threadIdx.y) * R + P;
   const int64_t base = (int64_t)blockIdx.z * g.N;
   if constexpr (ST == 2) {
     // Interior tile: cells and their +1 neighbours outside the strips.
-    const int tx0 = blockIdx.x * kTileX + P, ty0 = blockIdx.y * kBlockY * R + P;
+    const int tx0 = blockIdx.x * kTileX + P, ty0 = blockIdx.y * BY * R + P;
     if (tx0 >= g.pml_x0 && tx0 + kTileX < g.pml_x1 && ty0 >= g.pml_y0 &&
-        ty0 + kBlockY * R < g.pml_y1) {
+        ty0 + BY * R < g.pml_y1) {
       adj_e_fast<T, R>(g, g.cb_b ? cb + base : cb, lam_ey + base, lam_hx + base, lam_hz + base,
                        x, y0);
       return;
